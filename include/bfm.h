@@ -1,0 +1,141 @@
+/*
+ * bfm.h — C-ABI of the B200 BFM sweep engine (libbfm.so).
+ *
+ * Drop-in for pscbfm's GPU updater UpdaterGPUScBFM_AB_Type
+ * (reference: src/pscbfm/UpdaterGPUScBFM_AB_Type.h:316-358). Every entry point returns a status
+ * (BFM_OK or one of the error codes below) instead of throwing; bfm_last_error() returns the
+ * message the reference would have put into its exception. Plain pointers and sizes only.
+ *
+ * Ownership: the engine copies every input into its own host and device buffers; callers keep
+ * ownership of what they pass. Handles are independent (no global device state); one handle
+ * must not be used from two threads at once, distinct handles may.
+ *
+ * Draw stream: each sub-step draws a colour (draw % nColors) and a 32-bit seed, in that order
+ * (src/pscbfm/CRITICAL.cu:509-510). The default stream is counter-based: draw k of a system with
+ * seed S is the upper 32 bits of SplitMix64(SplitMix64(S) + (k+1) * 0x9E3779B97F4A7C15), sub-step
+ * t uses draws 2t and 2t+1. An external generator (e.g. LeMonADE's r250) can be plugged in with
+ * bfm_set_draw_callback.
+ */
+#ifndef BFM_H
+#define BFM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define BFM_OK 0
+#define BFM_ERR_INVALID_ARGUMENT 1 /* reference: std::invalid_argument */
+#define BFM_ERR_RUNTIME 2          /* reference: std::runtime_error */
+#define BFM_ERR_CUDA 3             /* reference: CUDA_ERROR -> exit(EXIT_FAILURE), cudacommon.hpp:31-46 */
+#define BFM_ERR_OUT_OF_RANGE 4     /* reference: std::out_of_range from vector::at */
+#define BFM_ERR_NULL_HANDLE 5
+#define BFM_ERR_BUDGET 6           /* server admission: job larger than the memory budget */
+#define BFM_ERR_BUSY 7             /* server: result not ready yet */
+
+/* engine paths (bfm_set_mode) */
+#define BFM_MODE_AUTO 0     /* resident if the system fits one CTA, else graph */
+#define BFM_MODE_LAUNCH 1   /* check + perform launch per sub-step (the reference's structure) */
+#define BFM_MODE_GRAPH 2    /* the same launches captured into CUDA graphs */
+#define BFM_MODE_RESIDENT 3 /* one CTA per system, lattice in shared memory (box <= 64^3) */
+
+typedef struct bfm_updater* bfm_handle;
+typedef struct bfm_batch* bfm_batch_handle;
+typedef uint32_t (*bfm_draw_fn)(void* ctx);
+
+/* Last error message of a handle (NULL handle: of the last failed call without a handle on this
+ * thread). Valid until the next call on that handle. */
+const char* bfm_last_error(bfm_handle h);
+
+/* ------------------------------------------------------------------ life cycle */
+/* Constructor + setGpu (UpdaterGPUScBFM_AB_Type.cu:416-450, :472-487). */
+int bfm_create(bfm_handle* out, int gpu);
+/* Destructor (UpdaterGPUScBFM_AB_Type.cu:467-470). */
+int bfm_destroy(bfm_handle h);
+/* setGpu (UpdaterGPUScBFM_AB_Type.cu:472-487); invalid_argument if the GPU does not exist. */
+int bfm_set_gpu(bfm_handle h, int gpu);
+/* cleanup (UpdaterGPUScBFM_AB_Type.cu:995-1001): frees the device state; the handle returns to
+ * its freshly created state so the setter sequence can be repeated. */
+int bfm_cleanup(bfm_handle h);
+
+/* ------------------------------------------------------------------ setters */
+/* setPeriodicity (UpdaterGPUScBFM_AB_Type.cu:728-753): only fully periodic boxes. */
+int bfm_set_periodicity(bfm_handle h, int px, int py, int pz);
+/* setNrOfAllMonomers (UpdaterGPUScBFM_AB_Type.cu:699-726); runtime error if already set. */
+int bfm_set_n_monomers(bfm_handle h, uint32_t n);
+/* setAttribute (UpdaterGPUScBFM_AB_Type.cu:755-758). */
+int bfm_set_attribute(bfm_handle h, uint32_t i, int32_t attribute);
+/* Bulk form of setAttribute for monomers 0..n-1. */
+int bfm_set_attributes_bulk(bfm_handle h, const int32_t* attributes, uint32_t n);
+/* setMonomerCoordinates (UpdaterGPUScBFM_AB_Type.cu:760-771), lower-left-front corner, unfolded. */
+int bfm_set_coords(bfm_handle h, uint32_t i, int32_t x, int32_t y, int32_t z);
+/* Bulk form of setMonomerCoordinates: xyz[3*i+a]. After bfm_initialize it uploads the new
+ * positions and rebuilds the occupancy lattice on the device. */
+int bfm_set_coords_bulk(bfm_handle h, const int32_t* xyz, uint32_t n);
+/* setConnectivity (UpdaterGPUScBFM_AB_Type.cu:777-795): directed, call once per direction.
+ * At most 16 neighbours per monomer (the reference's compile-time MAX_CONNECTIVITY is 4). */
+int bfm_add_bond(bfm_handle h, uint32_t a, uint32_t b);
+/* Bulk form: pairs[2*k] -> pairs[2*k+1] for k < n_pairs, in order (same as n_pairs calls). */
+int bfm_add_bonds_bulk(bfm_handle h, const uint32_t* pairs, uint32_t n_pairs);
+/* setLatticeSize (UpdaterGPUScBFM_AB_Type.cu:797-848): powers of two, 4..1024 per side. */
+int bfm_set_box(bfm_handle h, uint32_t bx, uint32_t by, uint32_t bz);
+/* copyBondSet (UpdaterGPUScBFM_AB_Type.cu:693-697): entry (dx&7)|(dy&7)<<3|(dz&7)<<6 of the
+ * 512-entry table; everything starts forbidden. */
+int bfm_set_bond_forbidden(bfm_handle h, int dx, int dy, int dz, int forbidden);
+/* Convenience: load the standard 108-vector set (GPUScBFM_AB_Type.h:120-127 with LeMonADE's
+ * default bond set). */
+int bfm_set_standard_bond_set(bfm_handle h);
+/* populateLattice (UpdaterGPUScBFM_AB_Type.cu:850-872). */
+int bfm_populate_lattice(bfm_handle h);
+/* Draw stream (replaces the RandomNumberGenerators member, UpdaterGPUScBFM_AB_Type.h:131). */
+int bfm_set_seed(bfm_handle h, uint64_t seed);
+int bfm_set_draw_callback(bfm_handle h, bfm_draw_fn fn, void* ctx);
+/* Engine path, BFM_MODE_*. */
+int bfm_set_mode(bfm_handle h, int mode);
+
+/* ------------------------------------------------------------------ simulation */
+/* initialize (UpdaterGPUScBFM_AB_Type.cu:490-690): bond-set check (exactly 108 allowed),
+ * colouring, per-colour groups, device upload. */
+int bfm_initialize(bfm_handle h);
+/* runSimulationOnGPU (CRITICAL.cu:414-698): nMCS Monte Carlo steps; returns when done. */
+int bfm_run(bfm_handle h, int32_t n_mcs);
+/* The same, returning as soon as the work is queued on the handle's stream. */
+int bfm_run_async(bfm_handle h, int32_t n_mcs);
+int bfm_synchronize(bfm_handle h);
+
+/* ------------------------------------------------------------------ read back */
+/* getMonomerPositionIn{X,Y,Z} (UpdaterGPUScBFM_AB_Type.cu:773-775); axis 0,1,2. */
+int bfm_get_coord(bfm_handle h, uint32_t i, int axis, int32_t* out);
+/* All positions, xyz[3*i+a], original monomer order. */
+int bfm_get_coords_bulk(bfm_handle h, int32_t* xyz, uint32_t n);
+/* Number of colour groups (mnElementsInGroup.size(), UpdaterGPUScBFM_AB_Type.cu:559-565) and
+ * their sizes (sizes may be NULL). */
+int bfm_n_colors(bfm_handle h, uint32_t* n_colors, uint32_t* sizes, uint32_t capacity);
+/* Counters since initialize: attempted moves, tentatively accepted (check passed), accepted,
+ * MCS done. */
+int bfm_get_stats(bfm_handle h, uint64_t out[4]);
+/* checkSystem (UpdaterGPUScBFM_AB_Type.cu:882-986): excluded volume and bond set on the host. */
+int bfm_validate(bfm_handle h);
+/* Device bytes held by the handle. */
+int bfm_device_bytes(bfm_handle h, uint64_t* out);
+
+/* ------------------------------------------------------------------ batch (no reference counterpart) */
+/* Advances many initialised handles on one GPU together; each keeps its own draw stream, so its
+ * trajectory equals a run alone. Handles stay owned by the caller and must outlive the batch. */
+int bfm_batch_create(bfm_batch_handle* out, int gpu, const bfm_handle* members, uint32_t n);
+int bfm_batch_destroy(bfm_batch_handle b);
+int bfm_batch_run(bfm_batch_handle b, int32_t n_mcs);        /* returns when done */
+int bfm_batch_run_async(bfm_batch_handle b, int32_t n_mcs);
+int bfm_batch_synchronize(bfm_batch_handle b);
+/* 0: every system on the grid path; 1 (default): small systems on the resident kernel. */
+int bfm_batch_set_resident(bfm_batch_handle b, int on);
+const char* bfm_batch_last_error(bfm_batch_handle b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BFM_H */

@@ -1,0 +1,149 @@
+"""ORACLE — TEST INFRASTRUCTURE ONLY.
+
+ctypes bindings of the CPU restatement of the reference sweep (oracle/bfm_oracle.cpp, built as
+oracle/liboracle.so) and of the reference updater compiled for sm_100a
+(oracle/_ref/libpscbfm_ref.so, GPU only). Only tests/, the smoke entry and the CPU-baseline leg of
+bench.py import this module; the engine in pscbfm_b200/ never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libpscbfm_ref.so")
+
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+
+_lib = None
+_ref = None
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        L.orc_hash.argtypes = [C.c_uint32]
+        L.orc_hash.restype = C.c_uint32
+        L.orc_counter_draw.argtypes = [C.c_uint64, C.c_uint64]
+        L.orc_counter_draw.restype = C.c_uint32
+        L.orc_counter_draws.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, _u32p]
+        L.orc_counter_draws.restype = None
+        L.orc_bond_index.argtypes = [C.c_int32] * 3
+        L.orc_bond_index.restype = C.c_uint32
+        L.orc_color.argtypes = [C.c_uint32, _u32p, _u32p, C.c_uint32, _u8p, C.c_char_p, C.c_int]
+        L.orc_color.restype = C.c_int
+        L.orc_run.argtypes = [C.c_uint32, _i32p, _u32p, _u32p, C.c_uint32, _u32p, _u8p, C.c_int,
+                              C.c_uint64, C.c_uint64, _u32p, C.c_uint64, C.c_uint32, _i32p, _u64p,
+                              C.c_char_p, C.c_int]
+        L.orc_run.restype = C.c_int
+        L.orc_seq_run.argtypes = [C.c_uint32, _i32p, _u32p, _u32p, C.c_uint32, _u32p, _u8p, C.c_uint64,
+                                  C.c_uint32, _i32p, _u64p, C.c_char_p, C.c_int]
+        L.orc_seq_run.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _arrs(sys):
+    xyz = np.ascontiguousarray(sys.xyz, dtype=np.int32).reshape(-1)
+    cnt = np.ascontiguousarray(sys.nbr_count, dtype=np.uint32)
+    ids = np.ascontiguousarray(sys.nbr_ids, dtype=np.uint32).reshape(-1)
+    box = np.ascontiguousarray(sys.box, dtype=np.uint32)
+    forb = np.ascontiguousarray(sys.forbidden, dtype=np.uint8)
+    return xyz, cnt, ids, box, forb
+
+
+def move_hash(a: int) -> int:
+    return int(lib().orc_hash(a))
+
+
+def counter_draws(seed: int, k0: int, count: int) -> np.ndarray:
+    out = np.zeros(count, dtype=np.uint32)
+    lib().orc_counter_draws(seed, k0, count, out)
+    return out
+
+
+def color(sys) -> np.ndarray:
+    xyz, cnt, ids, box, forb = _arrs(sys)
+    out = np.zeros(sys.n, dtype=np.uint8)
+    err = C.create_string_buffer(512)
+    nc = lib().orc_color(sys.n, cnt, ids, sys.maxc, out, err, 512)
+    if nc < 0:
+        raise RuntimeError(err.value.decode())
+    return out
+
+
+def run(sys, n_mcs: int, seed: int | None = None, substep0: int = 0, draws=None):
+    """Positions after n_mcs MCS of the parallel sweep, plus (attempted, tentative, accepted)."""
+    xyz, cnt, ids, box, forb = _arrs(sys)
+    out = np.zeros_like(xyz)
+    stats = np.zeros(3, dtype=np.uint64)
+    err = C.create_string_buffer(512)
+    if draws is None:
+        kind, dl = 0, np.zeros(1, np.uint32)
+        seed = sys.seed if seed is None else seed
+    else:
+        kind, dl = 1, np.ascontiguousarray(draws, dtype=np.uint32)
+        seed = 0
+    rc = lib().orc_run(sys.n, xyz, cnt, ids, sys.maxc, box, forb, kind, seed, substep0, dl,
+                       len(dl), n_mcs, out, stats, err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return out.reshape(-1, 3), tuple(int(s) for s in stats)
+
+
+def seq_run(sys, n_mcs: int, seed: int):
+    xyz, cnt, ids, box, forb = _arrs(sys)
+    out = np.zeros_like(xyz)
+    stats = np.zeros(2, dtype=np.uint64)
+    err = C.create_string_buffer(512)
+    rc = lib().orc_seq_run(sys.n, xyz, cnt, ids, sys.maxc, box, forb, seed, n_mcs, out, stats, err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return out.reshape(-1, 3), tuple(int(s) for s in stats)
+
+
+# ------------------------------------------------------------------ reference updater (GPU box)
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        R = C.CDLL(REF_LIB)
+        R.bfmref_run.argtypes = [C.c_int, C.c_uint32, _i32p, _u32p, _u32p, C.c_uint32, _u32p, _u8p,
+                                 _u32p, C.c_uint64, _u32p, C.c_uint32, _i32p, _u64p, C.c_char_p, C.c_int]
+        R.bfmref_run.restype = C.c_int
+        _ref = R
+    return _ref
+
+
+def ref_run(sys, draws, chunks, gpu: int = 0):
+    """Runs the reference updater (its own kernels) with the given draw list; chunks are the
+    nMCS of successive runSimulationOnGPU calls. Returns positions and the number of draws used."""
+    xyz, cnt, ids, box, forb = _arrs(sys)
+    out = np.zeros_like(xyz)
+    used = np.zeros(1, dtype=np.uint64)
+    err = C.create_string_buffer(1024)
+    d = np.ascontiguousarray(draws, dtype=np.uint32)
+    ch = np.ascontiguousarray(chunks, dtype=np.uint32)
+    rc = ref_lib().bfmref_run(gpu, sys.n, xyz, cnt, ids, sys.maxc, box, forb, d, len(d), ch, len(ch),
+                              out, used, err, 1024)
+    if rc != 0:
+        raise RuntimeError(f"reference updater failed ({rc}): {err.value.decode()}")
+    return out.reshape(-1, 3), int(used[0])

@@ -1,0 +1,223 @@
+// C-ABI of the engine (include/bfm.h): exceptions of the C++ layer become status codes.
+
+#include "../../include/bfm.h"
+
+#include <new>
+#include <stdexcept>
+#include <string>
+
+#include "bfm_engine.hpp"
+
+struct bfm_updater {
+    bfm::Updater u;
+    std::string err;
+    explicit bfm_updater(int gpu) : u(gpu) {}
+};
+
+struct bfm_batch {
+    bfm::Batch b;
+    std::string err;
+    bfm_batch(int gpu, bfm::Updater* const* m, uint32_t n) : b(gpu, m, n) {}
+};
+
+namespace {
+
+thread_local std::string gErr;
+
+template <typename F>
+int guarded(std::string* sink, F&& f)
+{
+    try {
+        f();
+        return BFM_OK;
+    } catch (bfm::CudaError const& e) {
+        (sink ? *sink : gErr) = e.what();
+        return BFM_ERR_CUDA;
+    } catch (std::out_of_range const& e) {
+        (sink ? *sink : gErr) = e.what();
+        return BFM_ERR_OUT_OF_RANGE;
+    } catch (std::invalid_argument const& e) {
+        (sink ? *sink : gErr) = e.what();
+        return BFM_ERR_INVALID_ARGUMENT;
+    } catch (std::bad_alloc const&) {
+        (sink ? *sink : gErr) = "host allocation failed";
+        return BFM_ERR_RUNTIME;
+    } catch (std::exception const& e) {
+        (sink ? *sink : gErr) = e.what();
+        return BFM_ERR_RUNTIME;
+    }
+}
+
+#define BFM_CALL(h, ...)                                          \
+    do {                                                          \
+        if (!(h)) {                                               \
+            gErr = "null handle";                                 \
+            return BFM_ERR_NULL_HANDLE;                           \
+        }                                                         \
+        return guarded(&(h)->err, [&] { __VA_ARGS__; });          \
+    } while (0)
+
+}  // namespace
+
+extern "C" {
+
+const char* bfm_last_error(bfm_handle h) { return h ? h->err.c_str() : gErr.c_str(); }
+
+int bfm_create(bfm_handle* out, int gpu)
+{
+    if (!out) {
+        gErr = "null output pointer";
+        return BFM_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    return guarded(nullptr, [&] { *out = new bfm_updater(gpu); });
+}
+
+int bfm_destroy(bfm_handle h)
+{
+    if (!h) return BFM_OK;
+    delete h;
+    return BFM_OK;
+}
+
+int bfm_set_gpu(bfm_handle h, int gpu) { BFM_CALL(h, h->u.setGpu(gpu)); }
+int bfm_cleanup(bfm_handle h) { BFM_CALL(h, h->u.cleanup()); }
+int bfm_set_periodicity(bfm_handle h, int px, int py, int pz) { BFM_CALL(h, h->u.setPeriodicity(px, py, pz)); }
+int bfm_set_n_monomers(bfm_handle h, uint32_t n) { BFM_CALL(h, h->u.setNrOfAllMonomers(n)); }
+int bfm_set_attribute(bfm_handle h, uint32_t i, int32_t a) { BFM_CALL(h, h->u.setAttribute(i, a)); }
+int bfm_set_coords(bfm_handle h, uint32_t i, int32_t x, int32_t y, int32_t z)
+{
+    BFM_CALL(h, h->u.setMonomerCoordinates(i, x, y, z));
+}
+int bfm_set_coords_bulk(bfm_handle h, const int32_t* xyz, uint32_t n)
+{
+    BFM_CALL(h, {
+        if (!xyz) throw std::invalid_argument("[bfm_set_coords_bulk] null buffer");
+        h->u.setCoordinates(xyz, n);
+    });
+}
+int bfm_add_bond(bfm_handle h, uint32_t a, uint32_t b) { BFM_CALL(h, h->u.setConnectivity(a, b)); }
+int bfm_add_bonds_bulk(bfm_handle h, const uint32_t* pairs, uint32_t n)
+{
+    BFM_CALL(h, {
+        if (!pairs && n) throw std::invalid_argument("[bfm_add_bonds_bulk] null buffer");
+        for (uint32_t k = 0; k < n; ++k) h->u.setConnectivity(pairs[2 * k], pairs[2 * k + 1]);
+    });
+}
+int bfm_set_attributes_bulk(bfm_handle h, const int32_t* a, uint32_t n)
+{
+    BFM_CALL(h, {
+        if (!a && n) throw std::invalid_argument("[bfm_set_attributes_bulk] null buffer");
+        for (uint32_t i = 0; i < n; ++i) h->u.setAttribute(i, a[i]);
+    });
+}
+int bfm_set_box(bfm_handle h, uint32_t bx, uint32_t by, uint32_t bz) { BFM_CALL(h, h->u.setLatticeSize(bx, by, bz)); }
+int bfm_set_bond_forbidden(bfm_handle h, int dx, int dy, int dz, int f)
+{
+    BFM_CALL(h, h->u.copyBondSet(dx, dy, dz, f != 0));
+}
+int bfm_set_standard_bond_set(bfm_handle h)
+{
+    BFM_CALL(h, {
+        // every sign/permutation of (2,0,0) (2,1,0) (2,1,1) (2,2,1) (3,0,0) (3,1,0)
+        static int const base[6][3] = {{2, 0, 0}, {2, 1, 0}, {2, 1, 1}, {2, 2, 1}, {3, 0, 0}, {3, 1, 0}};
+        static int const perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+        for (int dx = -4; dx < 4; ++dx)
+            for (int dy = -4; dy < 4; ++dy)
+                for (int dz = -4; dz < 4; ++dz) h->u.copyBondSet(dx, dy, dz, true);
+        for (auto const& b : base)
+            for (auto const& p : perm)
+                for (int s = 0; s < 8; ++s) {
+                    int const v[3] = {b[p[0]] * ((s & 1) ? -1 : 1), b[p[1]] * ((s & 2) ? -1 : 1),
+                                      b[p[2]] * ((s & 4) ? -1 : 1)};
+                    h->u.copyBondSet(v[0], v[1], v[2], false);
+                }
+    });
+}
+int bfm_populate_lattice(bfm_handle h) { BFM_CALL(h, h->u.populateLattice()); }
+int bfm_set_seed(bfm_handle h, uint64_t seed) { BFM_CALL(h, h->u.setDrawCounter(seed)); }
+int bfm_set_draw_callback(bfm_handle h, bfm_draw_fn fn, void* ctx) { BFM_CALL(h, h->u.setDrawCallback(fn, ctx)); }
+int bfm_set_mode(bfm_handle h, int mode) { BFM_CALL(h, h->u.setMode(mode)); }
+int bfm_initialize(bfm_handle h) { BFM_CALL(h, h->u.initialize()); }
+int bfm_run(bfm_handle h, int32_t n) { BFM_CALL(h, h->u.runSimulationOnGPU(n)); }
+int bfm_run_async(bfm_handle h, int32_t n) { BFM_CALL(h, h->u.run(n)); }
+int bfm_synchronize(bfm_handle h) { BFM_CALL(h, h->u.synchronize()); }
+int bfm_get_coord(bfm_handle h, uint32_t i, int axis, int32_t* out)
+{
+    BFM_CALL(h, {
+        if (!out) throw std::invalid_argument("[bfm_get_coord] null output");
+        *out = h->u.getMonomerPosition(i, axis);
+    });
+}
+int bfm_get_coords_bulk(bfm_handle h, int32_t* xyz, uint32_t n)
+{
+    BFM_CALL(h, {
+        if (!xyz) throw std::invalid_argument("[bfm_get_coords_bulk] null buffer");
+        h->u.getCoordinates(xyz, n);
+    });
+}
+int bfm_n_colors(bfm_handle h, uint32_t* nColors, uint32_t* sizes, uint32_t capacity)
+{
+    BFM_CALL(h, {
+        auto const g = h->u.groupSizes();
+        if (nColors) *nColors = (uint32_t)g.size();
+        if (sizes)
+            for (uint32_t c = 0; c < g.size() && c < capacity; ++c) sizes[c] = g[c];
+    });
+}
+int bfm_get_stats(bfm_handle h, uint64_t out[4])
+{
+    BFM_CALL(h, {
+        if (!out) throw std::invalid_argument("[bfm_get_stats] null output");
+        h->u.stats(out);
+    });
+}
+int bfm_validate(bfm_handle h) { BFM_CALL(h, h->u.validate()); }
+int bfm_device_bytes(bfm_handle h, uint64_t* out)
+{
+    BFM_CALL(h, {
+        if (!out) throw std::invalid_argument("[bfm_device_bytes] null output");
+        *out = h->u.deviceBytes();
+    });
+}
+
+// ---------------------------------------------------------------- batch
+
+const char* bfm_batch_last_error(bfm_batch_handle b) { return b ? b->err.c_str() : gErr.c_str(); }
+
+int bfm_batch_create(bfm_batch_handle* out, int gpu, const bfm_handle* members, uint32_t n)
+{
+    if (!out || (!members && n)) {
+        gErr = "null argument";
+        return BFM_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    return guarded(nullptr, [&] {
+        std::vector<bfm::Updater*> m(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            if (!members[i]) throw std::invalid_argument("[bfm_batch_create] null member handle");
+            m[i] = &members[i]->u;
+        }
+        *out = new bfm_batch(gpu, m.data(), n);
+    });
+}
+
+int bfm_batch_destroy(bfm_batch_handle b)
+{
+    if (!b) return BFM_OK;
+    delete b;
+    return BFM_OK;
+}
+
+int bfm_batch_run(bfm_batch_handle b, int32_t n)
+{
+    BFM_CALL(b, {
+        b->b.run(n);
+        b->b.synchronize();
+    });
+}
+int bfm_batch_run_async(bfm_batch_handle b, int32_t n) { BFM_CALL(b, b->b.run(n)); }
+int bfm_batch_synchronize(bfm_batch_handle b) { BFM_CALL(b, b->b.synchronize()); }
+int bfm_batch_set_resident(bfm_batch_handle b, int on) { BFM_CALL(b, b->b.setResidentEnabled(on != 0)); }
+
+}  // extern "C"

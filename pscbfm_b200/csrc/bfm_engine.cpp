@@ -1,0 +1,730 @@
+// Updater: host orchestration of one system (the drop-in for UpdaterGPUScBFM_AB_Type).
+//
+// initialize() follows src/pscbfm/UpdaterGPUScBFM_AB_Type.cu:490-690: bond-set check, colouring,
+// per-colour groups in stable original order, neighbour ids re-indexed to sorted slots, lattice
+// built from the positions. run() follows CRITICAL.cu:414-698: per MCS nColors sub-steps, each
+// drawing (colour, seed) on the host and advancing that colour group on the device.
+
+#include "bfm_engine.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <sstream>
+#include <string>
+
+namespace bfm {
+
+void cuda_check(cudaError_t e, char const* what)
+{
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw CudaError(std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+    }
+}
+
+namespace {
+
+constexpr uint32_t kStepCap = 8192;       // step entries staged per host->device copy
+constexpr uint32_t kGraphMcs = 32;        // MCS per captured graph chunk
+constexpr uint32_t kSlotAlign = 32;
+
+bool pow2(uint32_t v) { return v && !(v & (v - 1)); }
+
+uint32_t ilog2(uint32_t v)
+{
+    uint32_t l = 0;
+    while ((1u << l) < v) ++l;
+    return l;
+}
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+// Per-axis contributions of the brick coordinates to the brick index: the bits of the three
+// brick coordinates are interleaved x, y, z from the lowest level up (a Z-curve for a cubic box;
+// axes that run out of bits drop out of the rotation).
+std::vector<uint32_t> brick_tables(uint32_t const nb[3])
+{
+    uint32_t lb[3] = {ilog2(nb[0]), ilog2(nb[1]), ilog2(nb[2])};
+    uint32_t pos[3][32];
+    uint32_t next = 0;
+    for (uint32_t k = 0; k < 32; ++k)
+        for (int a = 0; a < 3; ++a)
+            if (k < lb[a]) pos[a][k] = next++;
+    std::vector<uint32_t> tab(nb[0] + nb[1] + nb[2]);
+    uint32_t base = 0;
+    for (int a = 0; a < 3; ++a) {
+        for (uint32_t b = 0; b < nb[a]; ++b) {
+            uint32_t w = 0;
+            for (uint32_t k = 0; k < lb[a]; ++k)
+                if ((b >> k) & 1u) w |= 1u << pos[a][k];
+            tab[base + b] = w;
+        }
+        base += nb[a];
+    }
+    return tab;
+}
+
+inline uint32_t host_brick_pos(uint32_t v, uint32_t a) { return ((v & 1u) | ((v & 2u) << 2)) << a; }
+
+}  // namespace
+
+// ============================================================================ construction
+
+Updater::Updater(int gpu)
+{
+    std::fill(forbidden_, forbidden_ + 512, true);
+    setGpu(gpu);
+}
+
+Updater::~Updater()
+{
+    try {
+        freeDevice();
+    } catch (...) {
+    }
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Updater::setGpu(int gpu)
+{
+    int count = 0;
+    cuda_check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    if (gpu < 0 || gpu >= count) {
+        std::ostringstream m;
+        m << "[UpdaterGPUScBFM_AB_Type::setGpu] GPU with ID " << gpu << " not present. Only " << count
+          << " GPUs are available.";
+        throw std::invalid_argument(m.str());
+    }
+    if (initialized() && gpu != gpu_) throw std::runtime_error("[setGpu] cannot move an initialized system to another GPU");
+    cuda_check(cudaSetDevice(gpu), "cudaSetDevice");
+    if (stream_ && gpu != gpu_) {
+        cudaStreamDestroy(stream_);
+        stream_ = nullptr;
+    }
+    gpu_ = gpu;
+    if (!stream_) cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+}
+
+void Updater::requireN(char const* who) const
+{
+    if (!nSet_) throw std::runtime_error(std::string("[") + who + "] setNrOfAllMonomers has not been called");
+}
+
+void Updater::requireInit(char const* who) const
+{
+    if (!initialized()) throw std::runtime_error(std::string("[") + who + "] initialize has not been called");
+}
+
+// ============================================================================ setters
+
+void Updater::setPeriodicity(bool px, bool py, bool pz)
+{
+    // UpdaterGPUScBFM_AB_Type.cu:728-753: the sweep is for fully periodic boxes only
+    if (!px || !py || !pz) {
+        std::ostringstream m;
+        m << "[UpdaterGPUScBFM_AB_Type::setPeriodicity] Simulation is intended to use completely periodic "
+             "boundary conditions, but setPeriodicity was called with ("
+          << px << "," << py << "," << pz << ")";
+        throw std::invalid_argument(m.str());
+    }
+}
+
+void Updater::setNrOfAllMonomers(uint32_t n)
+{
+    if (n_ != 0 || initialized()) {
+        std::ostringstream m;
+        m << "[UpdaterGPUScBFM_AB_Type::setNrOfAllMonomers] Number of Monomers already set to " << n_ << "!";
+        throw std::runtime_error(m.str());
+    }
+    n_ = n;
+    nSet_ = true;
+    xyz_.assign((size_t)n * 3, 0);
+    attr_.assign(n, 0);
+    nbrCnt_.assign(n, 0);
+    nbrIds_.assign((size_t)n * kMaxConn, 0);
+}
+
+void Updater::setAttribute(uint32_t i, int32_t a)
+{
+    requireN("setAttribute");
+    if (i >= n_) throw std::out_of_range("[setAttribute] monomer index out of range");
+    attr_[i] = a;
+}
+
+void Updater::setMonomerCoordinates(uint32_t i, int32_t x, int32_t y, int32_t z)
+{
+    requireN("setMonomerCoordinates");
+    if (i >= n_) throw std::out_of_range("[setMonomerCoordinates] monomer index out of range");
+    if (hostStale_) pullPositions();
+    xyz_[3 * (size_t)i] = x;
+    xyz_[3 * (size_t)i + 1] = y;
+    xyz_[3 * (size_t)i + 2] = z;
+    if (initialized()) setCoordinates(xyz_.data(), n_);
+}
+
+void Updater::setConnectivity(uint32_t a, uint32_t b)
+{
+    requireN("setConnectivity");
+    if (initialized()) throw std::runtime_error("[setConnectivity] bonds are fixed after initialize");
+    if (a >= n_ || b >= n_) throw std::out_of_range("[setConnectivity] monomer index out of range");
+    // UpdaterGPUScBFM_AB_Type.cu:777-795 (directed: call once per direction)
+    if (nbrCnt_[a] >= (uint32_t)kMaxConn) {
+        std::ostringstream m;
+        m << "[UpdaterGPUScBFM_AB_Type::setConnectivity] The maximum amount of bonds per monomer (" << kMaxConn
+          << ") has been exceeded!";
+        throw std::invalid_argument(m.str());
+    }
+    nbrIds_[(size_t)a * kMaxConn + nbrCnt_[a]++] = b;
+}
+
+void Updater::setLatticeSize(uint32_t bx, uint32_t by, uint32_t bz)
+{
+    if (box_[0] == bx && box_[1] == by && box_[2] == bz) return;
+    if (initialized()) throw std::runtime_error("[setLatticeSize] the box is fixed after initialize");
+    // UpdaterGPUScBFM_AB_Type.cu:797-848; positions are int32 here, boxes up to 1024 per side
+    if (bx > 1024 || by > 1024 || bz > 1024) {
+        std::ostringstream m;
+        m << "[UpdaterGPUScBFM_AB_Type::setLatticeSize] The box size (" << bx << "," << by << "," << bz
+          << ") is larger than supported (<= 1024 per side)";
+        throw std::invalid_argument(m.str());
+    }
+    if (!pow2(bx) || !pow2(by) || !pow2(bz) || bx < 4 || by < 4 || bz < 4) {
+        std::ostringstream m;
+        m << "[UpdaterGPUScBFM_AB_Type::setLatticeSize] Could not determine value for bit shift. Check whether "
+             "the box size is a power of 2 (and at least 4)! ( box="
+          << bx << "," << by << "," << bz << " )";
+        throw std::runtime_error(m.str());
+    }
+    box_[0] = bx;
+    box_[1] = by;
+    box_[2] = bz;
+}
+
+void Updater::copyBondSet(int dx, int dy, int dz, bool forbidden)
+{
+    // UpdaterGPUScBFM_AB_Type.cu:693-697 with the index of CRITICAL.cu:243-261
+    uint32_t const idx = (uint32_t(dx) & 7u) | ((uint32_t(dy) & 7u) << 3) | ((uint32_t(dz) & 7u) << 6);
+    forbidden_[idx] = forbidden;
+}
+
+void Updater::populateLattice()
+{
+    // UpdaterGPUScBFM_AB_Type.cu:850-872 fills the host lattice used by checkSystem; every
+    // coordinate maps into the periodic box, so only the preconditions are checked here.
+    requireN("populateLattice");
+    if (!box_[0]) throw std::runtime_error("[populateLattice] setLatticeSize has not been called");
+    latticePopulated_ = true;
+}
+
+void Updater::setDrawCounter(uint64_t seed)
+{
+    drawKind_ = kDrawCounter;
+    drawSeed_ = seed;
+    drawFn_ = nullptr;
+    drawCtx_ = nullptr;
+}
+
+void Updater::setDrawCallback(DrawFn fn, void* ctx)
+{
+    if (!fn) throw std::invalid_argument("[setDrawCallback] null callback");
+    drawKind_ = kDrawCallback;
+    drawFn_ = fn;
+    drawCtx_ = ctx;
+}
+
+void Updater::setMode(int mode)
+{
+    if (mode < kModeAuto || mode > kModeResident) throw std::invalid_argument("[setMode] unknown mode");
+    if (mode == kModeResident && initialized() && !residentEligible())
+        throw std::invalid_argument("[setMode] this system does not fit the resident kernel");
+    mode_ = mode;
+}
+
+// ============================================================================ initialize
+
+void Updater::initialize()
+{
+    if (initialized())
+        throw std::runtime_error(
+            "[UpdaterGPUScBFM_AB_Type::initialize] Initialize was already called and may not be called again until "
+            "cleanup was called!");
+    requireN("initialize");
+    if (n_ == 0) throw std::runtime_error("[initialize] the system has no monomers");
+    if (!box_[0]) throw std::runtime_error("[initialize] setLatticeSize has not been called");
+    uint32_t nAllowed = 0;
+    for (bool f : forbidden_) nAllowed += f ? 0 : 1;
+    if (nAllowed != 108) {
+        std::ostringstream m;
+        m << "[UpdaterGPUScBFM_AB_Type::initialize] Wrong bond-set! Expected 108 allowed bonds, but got " << nAllowed;
+        throw std::runtime_error(m.str());
+    }
+    cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
+
+    // colouring and groups (UpdaterGPUScBFM_AB_Type.cu:549-608)
+    colour_ = colour_bond_graph(n_, nbrCnt_.data(), nbrIds_.data(), kMaxConn);
+    uint32_t nC = 0;
+    for (uint8_t c : colour_) nC = std::max(nC, (uint32_t)c + 1);
+    grpSize_.assign(nC, 0);
+    for (uint8_t c : colour_) ++grpSize_[c];
+    grpOff_.assign(nC, 0);
+    uint32_t acc = 0;
+    maxGroup_ = 0;
+    for (uint32_t c = 0; c < nC; ++c) {
+        grpOff_[c] = acc;
+        acc += (grpSize_[c] + kSlotAlign - 1) / kSlotAlign * kSlotAlign;
+        maxGroup_ = std::max(maxGroup_, grpSize_[c]);
+    }
+    npad_ = std::max(acc, kSlotAlign);
+    oldToNew_.assign(n_, 0);
+    {
+        std::vector<uint32_t> next = grpOff_;
+        for (uint32_t i = 0; i < n_; ++i) oldToNew_[i] = next[colour_[i]]++;
+    }
+    maxc_ = 1;
+    for (uint32_t i = 0; i < n_; ++i) maxc_ = std::max(maxc_, nbrCnt_[i]);
+
+    // host images
+    uint32_t nb[3] = {box_[0] / 4, box_[1] / 4, box_[2] / 4};
+    uint32_t const nwords = nb[0] * nb[1] * nb[2];
+    std::vector<uint32_t> tab = brick_tables(nb);
+    std::vector<int32_t> hx(npad_, kPadCoord), hy(npad_, 0), hz(npad_, 0);
+    std::vector<uint32_t> hnbr((size_t)maxc_ * npad_, 0);
+    std::vector<uint8_t> hnnb(npad_, 0);
+    std::vector<unsigned long long> hlat(nwords, 0ull);
+    for (uint32_t i = 0; i < n_; ++i) {
+        uint32_t const s = oldToNew_[i];
+        int32_t const x = xyz_[3 * (size_t)i], y = xyz_[3 * (size_t)i + 1], z = xyz_[3 * (size_t)i + 2];
+        hx[s] = x;
+        hy[s] = y;
+        hz[s] = z;
+        hnnb[s] = (uint8_t)nbrCnt_[i];
+        for (uint32_t k = 0; k < nbrCnt_[i]; ++k)
+            hnbr[(size_t)k * npad_ + s] = oldToNew_[nbrIds_[(size_t)i * kMaxConn + k]];
+        uint32_t const mx = uint32_t(x) & (box_[0] - 1), my = uint32_t(y) & (box_[1] - 1),
+                       mz = uint32_t(z) & (box_[2] - 1);
+        uint32_t const w = tab[mx >> 2] + tab[nb[0] + (my >> 2)] + tab[nb[0] + nb[1] + (mz >> 2)];
+        uint32_t const b = host_brick_pos(mx & 3, 0) | host_brick_pos(my & 3, 1) | host_brick_pos(mz & 3, 2);
+        hlat[w] |= 1ull << b;
+    }
+    std::vector<uint32_t> hgrp(2 * (size_t)nC);
+    for (uint32_t c = 0; c < nC; ++c) {
+        hgrp[2 * c] = grpOff_[c];
+        hgrp[2 * c + 1] = grpSize_[c];
+    }
+
+    // one arena for every device array of this system
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t const o = off;
+        off = align256(off + bytes);
+        return o;
+    };
+    size_t const oX = take(4ull * npad_), oY = take(4ull * npad_), oZ = take(4ull * npad_);
+    size_t const oNbr = take(4ull * maxc_ * npad_), oNnb = take(npad_), oFlags = take(npad_);
+    size_t const oMark = take(8ull * npad_), oLat = take(8ull * nwords), oTmp = take(16ull * nwords);
+    size_t const oTab = take(4ull * tab.size()), oGrp = take(4ull * hgrp.size()), oStats = take(32);
+    size_t const oDesc = take(sizeof(SysDev)), oSteps = take(sizeof(StepEntry) * kStepCap), oList = take(4);
+    Device d;
+    d.bytes = off;
+    cuda_check(cudaMalloc(&d.arena, off), "cudaMalloc(system arena)");
+    char* base = static_cast<char*>(d.arena);
+    dev_ = d;
+    SysDev& h = dev_.h;
+    h.x = reinterpret_cast<int32_t*>(base + oX);
+    h.y = reinterpret_cast<int32_t*>(base + oY);
+    h.z = reinterpret_cast<int32_t*>(base + oZ);
+    h.nbr = reinterpret_cast<uint32_t*>(base + oNbr);
+    h.nnb = reinterpret_cast<uint8_t*>(base + oNnb);
+    h.flags = reinterpret_cast<uint8_t*>(base + oFlags);
+    h.tmark = reinterpret_cast<uint32_t*>(base + oMark);
+    h.lat = reinterpret_cast<unsigned long long*>(base + oLat);
+    h.tmp = reinterpret_cast<unsigned long long*>(base + oTmp);
+    h.brickTab = reinterpret_cast<uint32_t*>(base + oTab);
+    h.grp = reinterpret_cast<uint32_t*>(base + oGrp);
+    h.stats = reinterpret_cast<unsigned long long*>(base + oStats);
+    h.npad = npad_;
+    h.nwords = nwords;
+    h.maxc = maxc_;
+    h.nColors = nC;
+    for (int a = 0; a < 3; ++a) {
+        h.mask[a] = box_[a] - 1;
+        h.nb[a] = nb[a];
+    }
+    std::memset(h.forbid, 0, sizeof(h.forbid));
+    for (uint32_t i = 0; i < 512; ++i)
+        if (forbidden_[i]) h.forbid[i >> 5] |= 1u << (i & 31);
+    dev_.dDesc = reinterpret_cast<SysDev*>(base + oDesc);
+    dev_.dSteps = reinterpret_cast<StepEntry*>(base + oSteps);
+    dev_.stepCap = kStepCap;
+    dev_.dList = reinterpret_cast<uint32_t*>(base + oList);
+
+    cudaStream_t s = stream_;
+    cuda_check(cudaMemcpyAsync(h.x, hx.data(), 4ull * npad_, cudaMemcpyHostToDevice, s), "upload x");
+    cuda_check(cudaMemcpyAsync(h.y, hy.data(), 4ull * npad_, cudaMemcpyHostToDevice, s), "upload y");
+    cuda_check(cudaMemcpyAsync(h.z, hz.data(), 4ull * npad_, cudaMemcpyHostToDevice, s), "upload z");
+    cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(h.nbr), hnbr.data(), 4ull * maxc_ * npad_,
+                               cudaMemcpyHostToDevice, s), "upload nbr");
+    cuda_check(cudaMemcpyAsync(const_cast<uint8_t*>(h.nnb), hnnb.data(), npad_, cudaMemcpyHostToDevice, s),
+               "upload nnb");
+    cuda_check(cudaMemsetAsync(h.flags, 0, npad_, s), "memset flags");
+    cuda_check(cudaMemsetAsync(h.tmark, 0xFF, 8ull * npad_, s), "memset tmark");
+    cuda_check(cudaMemcpyAsync(h.lat, hlat.data(), 8ull * nwords, cudaMemcpyHostToDevice, s), "upload lattice");
+    cuda_check(cudaMemsetAsync(h.tmp, 0, 16ull * nwords, s), "memset tmp");
+    cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(h.brickTab), tab.data(), 4ull * tab.size(),
+                               cudaMemcpyHostToDevice, s), "upload brick table");
+    cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(h.grp), hgrp.data(), 4ull * hgrp.size(),
+                               cudaMemcpyHostToDevice, s), "upload groups");
+    cuda_check(cudaMemsetAsync(h.stats, 0, 32, s), "memset stats");
+    cuda_check(cudaMemcpyAsync(dev_.dDesc, &h, sizeof(SysDev), cudaMemcpyHostToDevice, s), "upload descriptor");
+    cuda_check(cudaMemsetAsync(dev_.dList, 0, 4, s), "memset list");
+    if (!hSteps_) {
+        cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * kStepCap), "cudaMallocHost(steps)");
+        hStepCap_ = kStepCap;
+    }
+    if (!stepsFree_) cuda_check(cudaEventCreateWithFlags(&stepsFree_, cudaEventDisableTiming), "cudaEventCreate");
+    cuda_check(cudaStreamSynchronize(s), "initialize");
+    subStep_ = 0;
+    mcsDone_ = 0;
+    lastColor_ = kNoColor;
+    hostStale_ = false;
+}
+
+bool Updater::residentEligible() const
+{
+    if (!initialized()) return false;
+    uint32_t const ntab = dev_.h.nb[0] + dev_.h.nb[1] + dev_.h.nb[2];
+    return resident_smem_bytes(dev_.h.nwords, ntab) <= kResidentMaxSmem && maxGroup_ <= 16u * kResidentBlock;
+}
+
+// ============================================================================ run
+
+StepEntry Updater::nextStep()
+{
+    uint32_t const nC = (uint32_t)grpSize_.size();
+    uint32_t d0, d1;
+    if (drawKind_ == kDrawCounter) {
+        d0 = counter_draw(drawSeed_, 2 * subStep_);
+        d1 = counter_draw(drawSeed_, 2 * subStep_ + 1);
+    } else {
+        d0 = drawFn_(drawCtx_);
+        d1 = drawFn_(drawCtx_);
+    }
+    StepEntry e;
+    e.color = d0 % nC;
+    e.seed = d1;
+    e.parity = (uint32_t)(subStep_ & 1u);
+    e.prevColor = lastColor_;
+    lastColor_ = e.color;
+    ++subStep_;
+    return e;
+}
+
+void Updater::fillSteps(uint32_t nSteps, StepEntry* buf, bool)
+{
+    for (uint32_t t = 0; t < nSteps; ++t) buf[t] = nextStep();
+}
+
+void Updater::scrubPending(cudaStream_t s)
+{
+    if (lastColor_ == kNoColor) return;
+    // a perform launch with no current colour only zeroes the previous sub-step's marks
+    cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
+    hSteps_[0] = StepEntry{kNoColor, 0u, (uint32_t)(subStep_ & 1u), lastColor_};
+    cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry), cudaMemcpyHostToDevice, s), "steps H2D");
+    cuda_check(cudaEventRecord(stepsFree_, s), "event");
+    uint32_t const tiles = (maxGroup_ + kGridBlock - 1) / kGridBlock;
+    cuda_check(launch_perform(dev_.dDesc, nullptr, std::max(tiles, 1u), kGridBlock, dev_.dSteps, s), "scrub");
+    lastColor_ = kNoColor;
+}
+
+void Updater::noteExternalRun(uint64_t subSteps, uint64_t mcs, bool pendingMarks, uint32_t lastColor)
+{
+    (void)subSteps;
+    mcsDone_ += mcs;
+    hostStale_ = true;
+    lastColor_ = pendingMarks ? lastColor : kNoColor;
+}
+
+void Updater::enqueueLaunch(uint32_t nSteps)
+{
+    uint32_t const tiles = std::max((maxGroup_ + kGridBlock - 1) / kGridBlock, 1u);
+    for (uint32_t done = 0; done < nSteps;) {
+        uint32_t const chunk = std::min(nSteps - done, hStepCap_);
+        cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
+        fillSteps(chunk, hSteps_, false);
+        cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
+                   "steps H2D");
+        cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
+        for (uint32_t t = 0; t < chunk; ++t) {
+            cuda_check(launch_check(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_), "check");
+            cuda_check(launch_perform(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_), "perform");
+        }
+        done += chunk;
+    }
+}
+
+void Updater::enqueueGraph(uint32_t nSteps)
+{
+    uint32_t const nC = (uint32_t)grpSize_.size();
+    uint32_t const G = std::min(kGraphMcs * nC, hStepCap_);
+    uint32_t const tiles = std::max((maxGroup_ + kGridBlock - 1) / kGridBlock, 1u);
+    if (nSteps < G) {
+        enqueueLaunch(nSteps);
+        return;
+    }
+    if (!graph_ || graphSteps_ != G) {
+        if (graph_) cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+        cudaGraph_t g;
+        cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+        cudaError_t err = cudaSuccess;
+        for (uint32_t t = 0; t < G && err == cudaSuccess; ++t) {
+            err = launch_check(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_);
+            if (err == cudaSuccess) err = launch_perform(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_);
+        }
+        cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
+        cuda_check(err, "capture launches");
+        cuda_check(endErr, "end capture");
+        cudaError_t const instErr = cudaGraphInstantiate(&graph_, g, 0);
+        cudaGraphDestroy(g);
+        cuda_check(instErr, "graph instantiate");
+        graphSteps_ = G;
+    }
+    uint32_t done = 0;
+    for (; done + G <= nSteps; done += G) {
+        cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
+        fillSteps(G, hSteps_, false);
+        cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * G, cudaMemcpyHostToDevice, stream_),
+                   "steps H2D");
+        cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
+        cuda_check(cudaGraphLaunch(graph_, stream_), "graph launch");
+    }
+    if (done < nSteps) enqueueLaunch(nSteps - done);
+}
+
+void Updater::enqueueResident(uint32_t nSteps)
+{
+    scrubPending(stream_);
+    uint32_t const ntab = dev_.h.nb[0] + dev_.h.nb[1] + dev_.h.nb[2];
+    size_t const smem = resident_smem_bytes(dev_.h.nwords, ntab);
+    uint32_t per = 1;
+    while (per * kResidentBlock < maxGroup_) per *= 2;
+    for (uint32_t done = 0; done < nSteps;) {
+        uint32_t const chunk = std::min(nSteps - done, hStepCap_);
+        cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
+        fillSteps(chunk, hSteps_, true);
+        cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
+                   "steps H2D");
+        cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
+        cuda_check(launch_resident(dev_.dDesc, dev_.dList, 1, per, dev_.dSteps, 1, chunk, smem, stream_), "resident");
+        done += chunk;
+    }
+    lastColor_ = kNoColor;   // the resident kernel leaves no marks in the global temporary lattices
+}
+
+void Updater::run(int32_t nMcs)
+{
+    requireInit("runSimulationOnGPU");
+    if (nMcs <= 0) return;
+    cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
+    uint64_t const total = (uint64_t)nMcs * grpSize_.size();
+    if (total > 0xFFFFFFFFull) throw std::invalid_argument("[runSimulationOnGPU] too many sub-steps in one call");
+    uint32_t const nSteps = (uint32_t)total;
+    int m = mode_;
+    if (m == kModeAuto) m = residentEligible() ? kModeResident : kModeGraph;
+    if (m == kModeResident && !residentEligible()) m = kModeGraph;
+    if (m == kModeResident) enqueueResident(nSteps);
+    else if (m == kModeGraph) enqueueGraph(nSteps);
+    else enqueueLaunch(nSteps);
+    mcsDone_ += (uint64_t)nMcs;
+    hostStale_ = true;
+}
+
+void Updater::runSimulationOnGPU(int32_t nMcs)
+{
+    run(nMcs);
+    synchronize();
+}
+
+void Updater::streamWait(cudaEvent_t e)
+{
+    cuda_check(cudaStreamWaitEvent(stream_, e, 0), "cudaStreamWaitEvent");
+}
+
+void Updater::synchronize()
+{
+    if (stream_) cuda_check(cudaStreamSynchronize(stream_), "sweep");
+}
+
+// ============================================================================ read back
+
+void Updater::pullPositions()
+{
+    if (!hostStale_ || !initialized()) return;
+    std::vector<int32_t> hx(npad_), hy(npad_), hz(npad_);
+    cuda_check(cudaMemcpyAsync(hx.data(), dev_.h.x, 4ull * npad_, cudaMemcpyDeviceToHost, stream_), "download x");
+    cuda_check(cudaMemcpyAsync(hy.data(), dev_.h.y, 4ull * npad_, cudaMemcpyDeviceToHost, stream_), "download y");
+    cuda_check(cudaMemcpyAsync(hz.data(), dev_.h.z, 4ull * npad_, cudaMemcpyDeviceToHost, stream_), "download z");
+    cuda_check(cudaStreamSynchronize(stream_), "download positions");
+    for (uint32_t i = 0; i < n_; ++i) {
+        uint32_t const s = oldToNew_[i];
+        xyz_[3 * (size_t)i] = hx[s];
+        xyz_[3 * (size_t)i + 1] = hy[s];
+        xyz_[3 * (size_t)i + 2] = hz[s];
+    }
+    hostStale_ = false;
+}
+
+int32_t Updater::getMonomerPosition(uint32_t i, int axis)
+{
+    requireN("getMonomerPosition");
+    if (i >= n_ || axis < 0 || axis > 2) throw std::out_of_range("[getMonomerPosition] index out of range");
+    pullPositions();
+    return xyz_[3 * (size_t)i + axis];
+}
+
+void Updater::getCoordinates(int32_t* xyz, uint32_t n)
+{
+    requireN("getCoordinates");
+    if (n != n_) throw std::invalid_argument("[getCoordinates] wrong monomer count");
+    pullPositions();
+    std::memcpy(xyz, xyz_.data(), sizeof(int32_t) * 3 * (size_t)n_);
+}
+
+void Updater::setCoordinates(int32_t const* xyz, uint32_t n)
+{
+    requireN("setCoordinates");
+    if (n != n_) throw std::invalid_argument("[setCoordinates] wrong monomer count");
+    if (xyz != xyz_.data()) std::memcpy(xyz_.data(), xyz, sizeof(int32_t) * 3 * (size_t)n_);
+    hostStale_ = false;
+    if (!initialized()) return;
+    // re-upload positions in sorted order and rebuild the occupancy lattice on the device
+    synchronize();
+    std::vector<int32_t> hx(npad_, kPadCoord), hy(npad_, 0), hz(npad_, 0);
+    for (uint32_t i = 0; i < n_; ++i) {
+        uint32_t const s = oldToNew_[i];
+        hx[s] = xyz_[3 * (size_t)i];
+        hy[s] = xyz_[3 * (size_t)i + 1];
+        hz[s] = xyz_[3 * (size_t)i + 2];
+    }
+    scrubPending(stream_);
+    cuda_check(cudaMemcpyAsync(dev_.h.x, hx.data(), 4ull * npad_, cudaMemcpyHostToDevice, stream_), "upload x");
+    cuda_check(cudaMemcpyAsync(dev_.h.y, hy.data(), 4ull * npad_, cudaMemcpyHostToDevice, stream_), "upload y");
+    cuda_check(cudaMemcpyAsync(dev_.h.z, hz.data(), 4ull * npad_, cudaMemcpyHostToDevice, stream_), "upload z");
+    cuda_check(cudaMemsetAsync(dev_.h.lat, 0, 8ull * dev_.h.nwords, stream_), "clear lattice");
+    cuda_check(launch_build_lattice(dev_.dDesc, npad_, stream_), "build lattice");
+    cuda_check(cudaStreamSynchronize(stream_), "setCoordinates");
+}
+
+uint32_t Updater::nColors() const
+{
+    requireInit("nColors");
+    return (uint32_t)grpSize_.size();
+}
+
+std::vector<uint32_t> Updater::groupSizes() const
+{
+    requireInit("groupSizes");
+    return grpSize_;
+}
+
+void Updater::stats(uint64_t out[4])
+{
+    requireInit("stats");
+    unsigned long long h[4];
+    cuda_check(cudaMemcpyAsync(h, dev_.h.stats, 32, cudaMemcpyDeviceToHost, stream_), "stats");
+    cuda_check(cudaStreamSynchronize(stream_), "stats");
+    out[0] = h[0];
+    out[1] = h[1];
+    out[2] = h[2];
+    out[3] = mcsDone_;
+}
+
+void Updater::validate()
+{
+    // checkSystem, UpdaterGPUScBFM_AB_Type.cu:882-986: 8 cells per monomer without overlap, and
+    // every bond in the allowed set (looked up with the kernel's 3-bit component index).
+    requireN("validate");
+    pullPositions();
+    uint64_t const V = (uint64_t)box_[0] * box_[1] * box_[2];
+    std::vector<uint8_t> cells(V, 0);
+    uint64_t occupied = 0;
+    for (uint32_t i = 0; i < n_; ++i)
+        for (int c = 0; c < 8; ++c) {
+            uint32_t const x = uint32_t(xyz_[3 * (size_t)i] + (c & 1)) & (box_[0] - 1);
+            uint32_t const y = uint32_t(xyz_[3 * (size_t)i + 1] + ((c >> 1) & 1)) & (box_[1] - 1);
+            uint32_t const z = uint32_t(xyz_[3 * (size_t)i + 2] + ((c >> 2) & 1)) & (box_[2] - 1);
+            uint8_t& cell = cells[x + (uint64_t)box_[0] * (y + (uint64_t)box_[1] * z)];
+            occupied += cell ? 0 : 1;
+            cell = 1;
+        }
+    if (occupied != 8ull * n_) {
+        std::ostringstream m;
+        m << "[checkSystem] Occupation count in the lattice is wrong! Expected 8*nMonomers=" << 8ull * n_
+          << " occupied cells, but got " << occupied;
+        throw std::runtime_error(m.str());
+    }
+    for (uint32_t i = 0; i < n_; ++i)
+        for (uint32_t k = 0; k < nbrCnt_[i]; ++k) {
+            uint32_t const j = nbrIds_[(size_t)i * kMaxConn + k];
+            int32_t const dx = xyz_[3 * (size_t)j] - xyz_[3 * (size_t)i];
+            int32_t const dy = xyz_[3 * (size_t)j + 1] - xyz_[3 * (size_t)i + 1];
+            int32_t const dz = xyz_[3 * (size_t)j + 2] - xyz_[3 * (size_t)i + 2];
+            uint32_t const idx = (uint32_t(dx) & 7u) | ((uint32_t(dy) & 7u) << 3) | ((uint32_t(dz) & 7u) << 6);
+            if (forbidden_[idx]) {
+                std::ostringstream m;
+                m << "[checkSystem] This particular bond is forbidden: (" << dx << "," << dy << "," << dz
+                  << ") between monomer " << i + 1 << " and monomer " << j + 1;
+                throw std::runtime_error(m.str());
+            }
+        }
+}
+
+// ============================================================================ teardown
+
+void Updater::freeDevice()
+{
+    if (graph_) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+        graphSteps_ = 0;
+    }
+    if (dev_.arena) {
+        cudaSetDevice(gpu_);
+        if (stream_) cudaStreamSynchronize(stream_);
+        cudaFree(dev_.arena);
+    }
+    dev_ = Device{};
+    if (hSteps_) {
+        cudaFreeHost(hSteps_);
+        hSteps_ = nullptr;
+        hStepCap_ = 0;
+    }
+    if (stepsFree_) {
+        cudaEventDestroy(stepsFree_);
+        stepsFree_ = nullptr;
+    }
+}
+
+void Updater::cleanup()
+{
+    // UpdaterGPUScBFM_AB_Type.cu:995-1001 frees everything initialize and the setters allocated;
+    // here the system returns to its freshly constructed state so the setter sequence can repeat.
+    freeDevice();
+    n_ = 0;
+    nSet_ = false;
+    xyz_.clear();
+    attr_.clear();
+    nbrCnt_.clear();
+    nbrIds_.clear();
+    colour_.clear();
+    grpOff_.clear();
+    grpSize_.clear();
+    oldToNew_.clear();
+    latticePopulated_ = false;
+    subStep_ = mcsDone_ = 0;
+    lastColor_ = kNoColor;
+    hostStale_ = false;
+}
+
+}  // namespace bfm

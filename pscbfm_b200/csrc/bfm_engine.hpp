@@ -1,0 +1,208 @@
+// Host side of the BFM sweep engine: the updater behind the reference's API
+// (src/pscbfm/UpdaterGPUScBFM_AB_Type.h:316-358), a batch of updaters advanced together, and the
+// pieces they share. Everything here is plain C++ over the CUDA runtime; the C-ABI in
+// bfm_capi.cpp is a thin exception-to-status layer on top.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "bfm_device.cuh"
+#include "bfm_kernels.hpp"
+
+namespace bfm {
+
+// Error classes, mapped to status codes by the C-ABI. The reference throws std::invalid_argument
+// and std::runtime_error for misuse and calls exit() on CUDA errors
+// (src/pscbfm/cudacommon.hpp:31-46); here CUDA errors become CudaError.
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void cuda_check(cudaError_t e, char const* what);
+
+std::vector<uint8_t> colour_bond_graph(uint32_t n, uint32_t const* cnt, uint32_t const* ids, uint32_t stride);
+
+// Host draw stream: per sub-step one draw for the colour (draw % nColors) and one for the seed,
+// in that order (src/pscbfm/CRITICAL.cu:509-510).
+enum DrawKind : int { kDrawCounter = 0, kDrawCallback = 1 };
+using DrawFn = uint32_t (*)(void*);
+
+// SplitMix64 finaliser (Steele, Lea & Flood 2014), keyed counter stream.
+inline uint64_t sm64_mix(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+inline uint32_t counter_draw(uint64_t seed, uint64_t k)
+{
+    return (uint32_t)(sm64_mix(sm64_mix(seed) + (k + 1) * 0x9E3779B97F4A7C15ull) >> 32);
+}
+
+// Engine path of one updater's run().
+enum Mode : int {
+    kModeAuto = 0,      // resident if the system fits one CTA, else graph
+    kModeLaunch = 1,    // two kernel launches per sub-step, like the reference
+    kModeGraph = 2,     // the same kernels captured into a CUDA graph per chunk of sub-steps
+    kModeResident = 3,  // one CTA runs the whole chunk, lattice in shared memory
+};
+
+class Updater {
+public:
+    explicit Updater(int gpu);
+    ~Updater();
+    Updater(Updater const&) = delete;
+    Updater& operator=(Updater const&) = delete;
+
+    // ---- reference setter API (UpdaterGPUScBFM_AB_Type.h:340-358)
+    void setGpu(int gpu);
+    void setPeriodicity(bool px, bool py, bool pz);
+    void setNrOfAllMonomers(uint32_t n);
+    void setAttribute(uint32_t i, int32_t a);
+    void setMonomerCoordinates(uint32_t i, int32_t x, int32_t y, int32_t z);
+    void setConnectivity(uint32_t a, uint32_t b);
+    void setLatticeSize(uint32_t bx, uint32_t by, uint32_t bz);
+    void copyBondSet(int dx, int dy, int dz, bool forbidden);
+    void populateLattice();
+    void initialize();
+    void runSimulationOnGPU(int32_t nMcs);   // enqueue + wait, like the reference
+    int32_t getMonomerPosition(uint32_t i, int axis);
+    void cleanup();
+
+    // ---- engine extensions
+    void setCoordinates(int32_t const* xyz, uint32_t n);
+    void getCoordinates(int32_t* xyz, uint32_t n);
+    void setDrawCounter(uint64_t seed);
+    void setDrawCallback(DrawFn fn, void* ctx);
+    void setMode(int mode);
+    int mode() const { return mode_; }
+    void run(int32_t nMcs);                  // enqueue only
+    void synchronize();
+    uint32_t nColors() const;
+    std::vector<uint32_t> groupSizes() const;
+    void stats(uint64_t out[4]);             // attempted, tentative, accepted, MCS done
+    uint64_t substep() const { return subStep_; }
+    uint64_t mcsDone() const { return mcsDone_; }
+    cudaStream_t stream() const { return stream_; }
+    bool initialized() const { return dev_.arena != nullptr; }
+    uint32_t nMonomers() const { return n_; }
+    size_t deviceBytes() const { return dev_.bytes; }
+    uint32_t maxGroup() const { return maxGroup_; }
+    bool residentEligible() const;
+    int gpu() const { return gpu_; }
+    void validate();                         // host-side EV and bond-set check (checkSystem)
+
+    // pieces used by Batch
+    SysDev const& desc() const { return dev_.h; }
+    SysDev* deviceDesc() const { return dev_.dDesc; }
+    uint32_t const* sortedSlot() const { return oldToNew_.data(); }
+    StepEntry nextStep();                    // consumes the draws of one sub-step
+    void scrubPending(cudaStream_t s);       // clears the temporary marks of the last sub-step
+    void noteExternalRun(uint64_t subSteps, uint64_t mcs, bool pendingMarks, uint32_t lastColor);
+    uint32_t lastColor() const { return lastColor_; }
+    void streamWait(cudaEvent_t e);          // orders this system's later work after e
+
+private:
+    struct Device {
+        void* arena = nullptr;
+        size_t bytes = 0;
+        SysDev h{};
+        SysDev* dDesc = nullptr;
+        StepEntry* dSteps = nullptr;
+        uint32_t stepCap = 0;
+        uint32_t* dList = nullptr;     // resident kernel system list (one entry: 0)
+    };
+    void requireN(char const* who) const;
+    void requireInit(char const* who) const;
+    void pullPositions();
+    void enqueueLaunch(uint32_t nSteps);
+    void enqueueGraph(uint32_t nSteps);
+    void enqueueResident(uint32_t nSteps);
+    void fillSteps(uint32_t nSteps, StepEntry* hostBuf, bool residentParity);
+    void freeDevice();
+
+    int gpu_ = 0;
+    cudaStream_t stream_ = nullptr;
+    uint32_t n_ = 0;
+    bool nSet_ = false;
+    std::vector<int32_t> xyz_;                 // host copy, original order
+    std::vector<int32_t> attr_;
+    std::vector<uint32_t> nbrCnt_;
+    std::vector<uint32_t> nbrIds_;             // [n][kMaxConn]
+    uint32_t box_[3] = {0, 0, 0};
+    bool forbidden_[512];
+    bool latticePopulated_ = false;
+
+    int drawKind_ = kDrawCounter;
+    uint64_t drawSeed_ = 0;
+    DrawFn drawFn_ = nullptr;
+    void* drawCtx_ = nullptr;
+    int mode_ = kModeAuto;
+
+    // after initialize
+    std::vector<uint8_t> colour_;
+    std::vector<uint32_t> grpOff_, grpSize_;
+    std::vector<uint32_t> oldToNew_;
+    uint32_t npad_ = 0, maxc_ = 1, maxGroup_ = 0;
+    uint64_t subStep_ = 0, mcsDone_ = 0;
+    uint32_t lastColor_ = kNoColor;            // colour whose marks are still in tmp[(subStep-1)&1]
+    bool hostStale_ = false;
+    Device dev_;
+    StepEntry* hSteps_ = nullptr;              // pinned staging for step entries
+    uint32_t hStepCap_ = 0;
+    cudaGraphExec_t graph_ = nullptr;
+    uint32_t graphSteps_ = 0;
+    cudaEvent_t stepsFree_ = nullptr;          // host staging may be rewritten after this event
+};
+
+// A set of initialised updaters on one GPU advanced together: systems that fit one CTA run in the
+// resident kernel (one launch per chunk), the others share one grid-phase launch per phase and
+// sub-step, captured into a CUDA graph. Every system keeps its own draw stream, so its
+// trajectory is identical to running it alone.
+class Batch {
+public:
+    Batch(int gpu, Updater* const* members, uint32_t n);
+    ~Batch();
+    void run(int32_t nMcs);     // enqueue
+    void synchronize();
+    uint32_t size() const { return (uint32_t)members_.size(); }
+    Updater* member(uint32_t i) const { return members_.at(i); }
+    void setResidentEnabled(bool on)
+    {
+        if (on != residentOn_) built_ = false;
+        residentOn_ = on;
+    }
+    cudaStream_t stream() const { return stream_; }
+    uint32_t gridTiles() const { return (uint32_t)tiles_.size(); }
+    uint32_t residentCount() const { return (uint32_t)resident_.size(); }
+
+private:
+    void rebuild();
+    int gpu_;
+    std::vector<Updater*> members_;
+    std::vector<uint32_t> resident_, grid_;    // member indices per path
+    std::vector<TileRef> tiles_;
+    bool residentOn_ = true;
+    bool built_ = false;
+    cudaStream_t stream_ = nullptr, stream2_ = nullptr;
+    cudaEvent_t join_ = nullptr, fork_ = nullptr;
+    SysDev* dSys_ = nullptr;                   // descriptors of all members
+    TileRef* dTiles_ = nullptr;
+    uint32_t* dResList_ = nullptr;
+    StepEntry* dSteps_ = nullptr;              // [cap][members]
+    StepEntry* hSteps_ = nullptr;
+    size_t stepCap_ = 0;
+    uint32_t residentPerThread_ = 1;
+    size_t residentSmem_ = 0;
+    cudaEvent_t stepsFree_ = nullptr;
+    cudaEvent_t done_ = nullptr;
+    cudaGraphExec_t graph_ = nullptr;
+};
+
+}  // namespace bfm

@@ -1,0 +1,41 @@
+// Host-callable launchers of the sweep kernels (bfm_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "bfm_device.cuh"
+
+namespace bfm {
+
+constexpr uint32_t kGridBlock = 256;          // threads per CTA of the grid-phase kernels
+constexpr uint32_t kResidentBlock = 1024;     // threads per CTA of the resident kernel
+// dynamic shared memory of the resident kernel: the 227 KB opt-in limit minus room for its
+// static shared memory (the copied system descriptor)
+constexpr size_t kResidentMaxSmem = 226 * 1024;
+constexpr int32_t kPadCoord = INT32_MIN;      // x of an unused (padding) slot
+
+// One CTA of a grid-phase launch: system index and first in-colour index it covers.
+struct TileRef {
+    uint32_t sys;
+    uint32_t start;
+};
+
+// dTiles == nullptr: single system 0, CTA b covers [b*tileSpan, (b+1)*tileSpan).
+cudaError_t launch_check(SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles, uint32_t tileSpan,
+                         StepEntry const* dSteps, cudaStream_t s);
+cudaError_t launch_perform(SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles, uint32_t tileSpan,
+                           StepEntry const* dSteps, cudaStream_t s);
+
+// Resident kernel: CTA b runs system dList[b] through sub-steps 0..nSteps-1 of dSteps
+// ([nSteps][nSys] entries). perThread = ceil(largest colour group / kResidentBlock), in {1,2,4,8,16}.
+size_t resident_smem_bytes(uint32_t nwords, uint32_t ntab);
+cudaError_t launch_resident(SysDev const* dSys, uint32_t const* dList, uint32_t nCta, uint32_t perThread,
+                            StepEntry const* dSteps, uint32_t nSys, uint32_t nSteps, size_t smem, cudaStream_t s);
+
+// Sets the occupancy bit of every non-padding slot of system dSys[0] (lat must be zeroed).
+cudaError_t launch_build_lattice(SysDev const* dSys, uint32_t npad, cudaStream_t s);
+
+}  // namespace bfm

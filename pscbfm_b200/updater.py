@@ -1,0 +1,232 @@
+"""Python mirror of the reference updater interface over the C-ABI.
+
+``UpdaterGPUScBFM_AB_Type`` keeps the method names, argument meaning and call order of
+src/pscbfm/UpdaterGPUScBFM_AB_Type.h:316-358; errors raise the Python counterpart of the
+reference's exception (std::invalid_argument -> ValueError, std::runtime_error -> RuntimeError,
+std::out_of_range -> IndexError, CUDA errors -> BfmCudaError). ``Batch`` advances many updaters
+together (no reference counterpart).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import MODE_AUTO, MODE_GRAPH, MODE_LAUNCH, MODE_RESIDENT  # noqa: F401
+
+
+class UpdaterGPUScBFM_AB_Type:
+    def __init__(self, gpu: int = 0):
+        self._L = _lib.load()
+        h = C.c_void_p()
+        self._check(self._L.bfm_create(C.byref(h), gpu), None)
+        self._h = h
+        self._draw_cb = None
+
+    # ---------------------------------------------------------------- plumbing
+    def _check(self, status, h="self"):
+        if status != _lib.BFM_OK:
+            handle = self._h if h == "self" else None
+            _lib.raise_for(status, self._L.bfm_last_error(handle).decode())
+
+    def _call(self, name, *args):
+        self._check(getattr(self._L, name)(self._h, *args))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.bfm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---------------------------------------------------------------- reference API
+    def setGpu(self, gpu: int):
+        self._call("bfm_set_gpu", gpu)
+
+    def setPeriodicity(self, px: bool, py: bool, pz: bool):
+        self._call("bfm_set_periodicity", int(px), int(py), int(pz))
+
+    def setNrOfAllMonomers(self, n: int):
+        self._call("bfm_set_n_monomers", n)
+        self.n_monomers = n
+
+    def setAttribute(self, i: int, attribute: int):
+        self._call("bfm_set_attribute", i, attribute)
+
+    def setMonomerCoordinates(self, i: int, x: int, y: int, z: int):
+        self._call("bfm_set_coords", i, x, y, z)
+
+    def setConnectivity(self, a: int, b: int):
+        self._call("bfm_add_bond", a, b)
+
+    def setLatticeSize(self, bx: int, by: int, bz: int):
+        self._call("bfm_set_box", bx, by, bz)
+
+    def copyBondSet(self, dx: int, dy: int, dz: int, forbidden: bool):
+        self._call("bfm_set_bond_forbidden", dx, dy, dz, int(forbidden))
+
+    def populateLattice(self):
+        self._call("bfm_populate_lattice")
+
+    def initialize(self):
+        self._call("bfm_initialize")
+
+    def execute(self) -> bool:
+        return True
+
+    def runSimulationOnGPU(self, n_mcs: int):
+        self._call("bfm_run", n_mcs)
+
+    def getMonomerPositionInX(self, i: int) -> int:
+        return self._coord(i, 0)
+
+    def getMonomerPositionInY(self, i: int) -> int:
+        return self._coord(i, 1)
+
+    def getMonomerPositionInZ(self, i: int) -> int:
+        return self._coord(i, 2)
+
+    def cleanup(self):
+        self._call("bfm_cleanup")
+
+    def _coord(self, i, axis):
+        out = C.c_int32()
+        self._call("bfm_get_coord", i, axis, C.byref(out))
+        return out.value
+
+    # ---------------------------------------------------------------- engine extensions
+    def set_seed(self, seed: int):
+        self._call("bfm_set_seed", seed)
+
+    def set_draw_callback(self, fn):
+        """fn() -> int: an external host generator consumed twice per sub-step (colour, seed)."""
+        cb = _lib.DRAW_FN(lambda _ctx: int(fn()) & 0xFFFFFFFF)
+        self._draw_cb = cb
+        self._call("bfm_set_draw_callback", cb, None)
+
+    def set_mode(self, mode: int):
+        self._call("bfm_set_mode", mode)
+
+    def set_standard_bond_set(self):
+        self._call("bfm_set_standard_bond_set")
+
+    def set_coords(self, xyz: np.ndarray):
+        a = np.ascontiguousarray(xyz, dtype=np.int32).reshape(-1)
+        self._call("bfm_set_coords_bulk", a, a.size // 3)
+
+    def get_coords(self, out: np.ndarray | None = None) -> np.ndarray:
+        n = self.n_monomers
+        if out is None:
+            out = np.empty((n, 3), dtype=np.int32)
+        self._call("bfm_get_coords_bulk", out.reshape(-1), n)
+        return out
+
+    def run_async(self, n_mcs: int):
+        self._call("bfm_run_async", n_mcs)
+
+    def synchronize(self):
+        self._call("bfm_synchronize")
+
+    def n_colors(self):
+        n = C.c_uint32()
+        self._call("bfm_n_colors", C.byref(n), None, 0)
+        sizes = np.zeros(n.value, dtype=np.uint32)
+        self._call("bfm_n_colors", C.byref(n), sizes.ctypes.data_as(C.c_void_p), n.value)
+        return n.value, sizes
+
+    def stats(self):
+        out = np.zeros(4, dtype=np.uint64)
+        self._call("bfm_get_stats", out)
+        return {"attempted": int(out[0]), "tentative": int(out[1]), "accepted": int(out[2]), "mcs": int(out[3])}
+
+    def validate(self):
+        self._call("bfm_validate")
+
+    def device_bytes(self) -> int:
+        v = C.c_uint64()
+        self._call("bfm_device_bytes", C.byref(v))
+        return v.value
+
+    n_monomers = 0
+
+    def load_system(self, system, seed: int | None = None, mode: int | None = None, initialize: bool = True):
+        """Feeds a systems.BfmSystem through the setter API in the adapter's order
+        (src/pscbfm/GPUScBFM_AB_Type.h:83-130), then initializes."""
+        self.setPeriodicity(True, True, True)
+        self.setNrOfAllMonomers(system.n)
+        self.set_coords(system.xyz)
+        attrs = np.ascontiguousarray(system.attributes, dtype=np.int32)
+        self._call("bfm_set_attributes_bulk", attrs, system.n)
+        rows, cols = system.bonds()
+        pairs = np.ascontiguousarray(np.stack([rows, cols], axis=1), dtype=np.uint32).reshape(-1)
+        self._call("bfm_add_bonds_bulk", pairs, pairs.size // 2)
+        self.setLatticeSize(*system.box)
+        self.populateLattice()
+        forb = system.forbidden
+        for dx in range(-4, 4):
+            for dy in range(-4, 4):
+                for dz in range(-4, 4):
+                    idx = (dx & 7) | ((dy & 7) << 3) | ((dz & 7) << 6)
+                    self._L.bfm_set_bond_forbidden(self._h, dx, dy, dz, int(forb[idx]))
+        self.set_seed(system.seed if seed is None else seed)
+        if mode is not None:
+            self.set_mode(mode)
+        if initialize:
+            self.initialize()
+        return self
+
+
+class Batch:
+    """Many initialised updaters on one GPU advanced together (include/bfm.h, bfm_batch_*)."""
+
+    def __init__(self, members, gpu: int = 0, resident: bool = True):
+        self._L = _lib.load()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m.handle for m in self.members])
+        h = C.c_void_p()
+        st = self._L.bfm_batch_create(C.byref(h), gpu, arr, len(self.members))
+        if st != _lib.BFM_OK:
+            _lib.raise_for(st, self._L.bfm_batch_last_error(None).decode())
+        self._h = h
+        if not resident:
+            self._call("bfm_batch_set_resident", 0)
+
+    def _call(self, name, *args):
+        st = getattr(self._L, name)(self._h, *args)
+        if st != _lib.BFM_OK:
+            _lib.raise_for(st, self._L.bfm_batch_last_error(self._h).decode())
+
+    def run(self, n_mcs: int):
+        self._call("bfm_batch_run", n_mcs)
+
+    def run_async(self, n_mcs: int):
+        self._call("bfm_batch_run_async", n_mcs)
+
+    def synchronize(self):
+        self._call("bfm_batch_synchronize")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.bfm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
