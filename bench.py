@@ -1,0 +1,415 @@
+#!/usr/bin/env python
+"""Benchmark of the BFM sweep engine: attempted monomer moves/s (MCS x N / t) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+A step is one Monte Carlo step (every colour group once) of the workload's system(s), inputs
+resident in HBM. Workloads (synthetic, generated from their sizes; no dataset is involved):
+  dense_melt  (default) periodic 256^3, 16,384 chains x 64 (N = 1,048,576, phi = 0.5), seed 7
+  small       periodic 64^3, 256 chains x 32 (N = 8192, phi = 0.25), seed 42
+  network     periodic 128^3, 512 six-functional nodes + 1536 strands of 7 (N = 11,264), seed 3
+  ensemble    256 systems, box {32,64,128}, chains {16..256}, phi U[0.1,0.5], batched
+Timing: W untimed warm-up steps, then K steps each bracketed by CUDA events on the engine's
+stream, with the L2 flushed (a 256 MiB write) before every step; max over ranks. One process per
+GPU under torchrun; a single system does not shard, so N GPUs run N replicas (weak scaling).
+
+--impl reference times the reference's algorithm on the host cores: the CPU restatement of the
+reference sweep (oracle/), one replica per core, same metric and workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["dense_melt", "small", "network", "ensemble"], default="dense_melt")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched-vs-plain side measurement")
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)
+    return a
+
+
+# ------------------------------------------------------------------ workloads
+
+def build_workload(name):
+    from pscbfm_b200 import systems as S
+    if name == "dense_melt":
+        return [S.dense_melt()]
+    if name == "small":
+        return [S.small_chains()]
+    if name == "network":
+        return [S.crosslinked_network()]
+    return S.ensemble()
+
+
+def workload_config(name, systems):
+    if name == "dense_melt":
+        return {"workload": "dense_melt_256^3_16384x64_phi0.5", "box": 256, "chains": 16384, "chain_length": 64,
+                "monomers": systems[0].n, "seed": 7}
+    if name == "small":
+        return {"workload": "chains_64^3_256x32_phi0.25", "box": 64, "chains": 256, "chain_length": 32,
+                "monomers": systems[0].n, "seed": 42}
+    if name == "network":
+        return {"workload": "network_128^3_512x6func_strands7", "box": 128, "monomers": systems[0].n, "seed": 3}
+    return {"workload": "ensemble_256_systems", "systems": len(systems), "monomers": sum(s.n for s in systems),
+            "seeds": "1000+i", "generator_seed": 20240611}
+
+
+# ------------------------------------------------------------------ algorithmic bytes (roofline)
+
+def check_bytes_per_move(systems, p_chk):
+    """Algorithmic bytes of one attempted move in the check kernel: own xyz 12 B, per neighbour
+    4 B id + 12 B xyz, neighbour count 1 B, flag write 1 B, 9 occupancy bits, one temporary bit
+    for a tentative move."""
+    n = sum(s.n for s in systems)
+    kbar = sum(int(s.nbr_count.sum()) for s in systems) / n
+    return 12 + 16 * kbar + 1 + 1 + 9 / 8 + p_chk / 8, kbar
+
+
+def sweep_bytes_per_move(kbar, p_chk, p_acc):
+    """Whole sub-step (check + perform): 12 + 16 kbar + 2 + 2.25 + 24 p_acc + 0.25 p_acc + 0.125 p_chk."""
+    return 12 + 16 * kbar + 2 + 2.25 + 24.25 * p_acc + 0.125 * p_chk
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel_key):
+    """dram bytes per launch recorded from an ncu capture in profiles/<kernel_key>.md, if present."""
+    p = os.path.join(ROOT, "profiles", kernel_key + ".md")
+    if not os.path.exists(p):
+        return None
+    for ln in open(p):
+        if ln.strip().startswith("dram_bytes_per_launch:"):
+            try:
+                return float(ln.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + ",".join(self.FIELDS),
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [ln.split(", ") for ln in open(self.f.name).read().splitlines() if ln.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip() == "Active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU legs (oracle, spawned)
+
+def _cpu_worker(args):
+    kind, workload, steps, warmup = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    systems = build_workload(workload)
+    s = systems[0] if workload != "ensemble" else max(systems, key=lambda q: q.n)
+    attempted = 0
+    t_total = 0.0
+    seed = s.seed
+    for k in range(warmup + steps):
+        t0 = time.perf_counter()
+        if kind == "sequential":
+            _, st = O.seq_run(s, 1, seed=seed + k)
+            att = st[0]
+        else:
+            nc = int(O.color(s).max()) + 1
+            _, st = O.run(s, 1, substep0=k * nc)
+            att = st[0]
+        dt = time.perf_counter() - t0
+        if k >= warmup:
+            attempted += att
+            t_total += dt
+    return attempted, t_total, s.n
+
+
+def cpu_replicas(kind, workload, steps, warmup):
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_cpu_worker, [(kind, workload, steps, warmup)] * cores)
+    rate = sum(a / t for a, t, _ in res)
+    return rate, cores, res[0][2]
+
+
+# ------------------------------------------------------------------ main arm
+
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def reduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def gpu_index(local):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        parts = [p for p in vis.split(",") if p]
+        if local < len(parts):
+            return parts[local]
+    return str(local)
+
+
+def run_ours(args):
+    import torch
+    import pscbfm_b200 as P
+    rank, world, local = dist_setup(args)
+    systems = build_workload(args.workload)
+    config = workload_config(args.workload, systems)
+    n_total = sum(s.n for s in systems)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    members = [P.UpdaterGPUScBFM_AB_Type(local).load_system(s) for s in systems]
+    batch = P.Batch(members, gpu=local) if len(members) > 1 else None
+    u0 = members[0]
+
+    def step_timed(n):
+        return u0.run_timed(n) if batch is None else batch.run_timed(n)
+
+    for _ in range(args.warmup):
+        step_timed(1)
+    launches0 = sum(m.launch_count() for m in members)
+    stats0 = [m.stats() for m in members]
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(gpu_index(local))
+    ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ms += step_timed(1)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier(world)
+    launches = sum(m.launch_count() for m in members) - launches0
+    stats1 = [m.stats() for m in members]
+    attempted = sum(b["attempted"] - a["attempted"] for a, b in zip(stats0, stats1))
+    tentative = sum(b["tentative"] - a["tentative"] for a, b in zip(stats0, stats1))
+    accepted = sum(b["accepted"] - a["accepted"] for a, b in zip(stats0, stats1))
+    t_max = reduce_max(ms / 1e3, world)
+    moves = args.steps * n_total
+    value = world * moves / t_max
+    p_chk, p_acc = tentative / max(attempted, 1), accepted / max(attempted, 1)
+
+    # warm-L2 back-to-back number (no flush), for reference
+    warm_ms = step_timed(args.steps)
+    value_warm = world * moves / reduce_max(warm_ms / 1e3, world)
+
+    # roofline of the dominant kernel
+    hbm_peak, peak_kind = measured_peaks()
+    roofline = None
+    if batch is None:
+        kt = u0.time_kernels(max(4, min(args.steps, 40)))
+        nC = u0.n_colors()[0]
+        att_per_launch = systems[0].n / nC
+        b_check, kbar = check_bytes_per_move(systems, p_chk)
+        avg_check = kt["check_ms"] / kt["check_launches"]
+        avg_perform = kt["perform_ms"] / kt["perform_launches"]
+        achieved = b_check * att_per_launch / (avg_check / 1e3) / 1e9
+        key = {"dense_melt": "k_check_dense_melt256", "small": "k_check_chains64",
+               "network": "k_check_network128"}[args.workload]
+        traffic = profiled_traffic(key)
+        roofline = {"kernel": "bfm::k_check", "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
+                    "unit": "GB/s", "frac": round(achieved / hbm_peak, 4), "peak_kind": peak_kind,
+                    "traffic": traffic, "algorithmic_bytes_per_launch": round(b_check * att_per_launch),
+                    "bytes_per_attempted_move": round(b_check, 3), "kbar": round(kbar, 5),
+                    "avg_launch_us": round(avg_check * 1e3, 2), "perform_avg_launch_us": round(avg_perform * 1e3, 2),
+                    "sweep_bytes_per_attempted_move": round(sweep_bytes_per_move(kbar, p_chk, p_acc), 3),
+                    "note": "state is L2-resident between sub-steps; frac is against HBM copy bandwidth"}
+
+    # e2e through the C-ABI with host buffers: per step one bfm_run (host draws uploaded from
+    # pinned memory) and a read of the step's counters; positions copied back at the end
+    import numpy as np
+    host_xyz = np.empty((systems[0].n, 3), dtype=np.int32)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        if batch is None:
+            u0.runSimulationOnGPU(1)
+        else:
+            batch.run(1)
+        u0.stats()
+    u0.get_coords(host_xyz)
+    e2e_s = time.perf_counter() - t
+    nC0 = u0.n_colors()[0]
+    e2e_value = world * moves / reduce_max(e2e_s, world)
+    e2e = {"value": e2e_value, "unit": "attempted moves/s",
+           "h2d_bytes_per_step": 16 * sum(m.n_colors()[0] for m in members),
+           "d2h_bytes_per_step": 32 * (1 if batch is None else 1) + round(12 * systems[0].n / args.steps),
+           "calls": "bfm_run(1) + bfm_get_stats per step, bfm_get_coords_bulk once"}
+
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras and args.workload != "ensemble":
+        extras["batched_vs_plain"] = batched_vs_plain()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, _ = cpu_replicas("sequential", args.workload, steps=3 if n_total > 100000 else 40, warmup=1)
+        cpu = {"value": rate, "unit": "attempted moves/s", "cores": cores, "kind": "port",
+               "sample": ("random-sequential single-monomer BFM (LeMonADE serial-updater scheme), one replica of "
+                          "the workload system per core, " + ("3" if n_total > 100000 else "40") + " MCS each")}
+    launches_total = reduce_sum(float(launches), world)
+    for m in members:
+        m.validate()
+    if rank == 0:
+        line = {"metric": "attempted monomer moves/s", "value": value, "unit": "attempted moves/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                "config": dict(config, l2="flushed (256 MiB write) before every timed step",
+                               path="auto" if batch is None else "batch", parallelism=f"replicas x{world}"),
+                "value_warm_l2": value_warm, "p_chk": p_chk, "p_acc": p_acc,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches_total),
+                "clocks": clocks}
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def batched_vs_plain(n_systems=64, mcs=20):
+    """The first n_systems of the ensemble: the batch (one launch sequence for all) against the
+    plain path (each system alone through the per-sub-step launch path), same MCS."""
+    import pscbfm_b200 as P
+    from pscbfm_b200 import systems as S
+    systems = S.ensemble(n_systems=n_systems)
+    n = sum(s.n for s in systems)
+    members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
+    b = P.Batch(members)
+    b.run(2)
+    batched = n * mcs / (b.run_timed(mcs) / 1e3)
+    b.close()
+    plain_t = 0.0
+    for m in members:
+        m.set_mode(P.MODE_LAUNCH)
+        m.run_timed(1)
+        plain_t += m.run_timed(mcs) / 1e3
+    plain = n * mcs / plain_t
+    for m in members:
+        m.close()
+    return {"systems": n_systems, "monomers": n, "mcs": mcs, "batched": batched, "plain": plain,
+            "ratio": batched / plain, "plain_path": "BFM_MODE_LAUNCH, one system at a time"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    systems = build_workload(args.workload)
+    config = workload_config(args.workload, systems)
+    steps = min(args.steps, 5 if sum(s.n for s in systems) > 100000 else 50)
+    rate, cores, n = cpu_replicas("parallel", args.workload, steps=steps, warmup=min(args.warmup, 1))
+    sample = (f"CPU restatement of the reference's colour-by-colour sweep (oracle/bfm_oracle.cpp), one "
+              f"replica per core, {steps} MCS each after 1 warm-up MCS")
+    line = {"impl": "reference", "metric": "attempted monomer moves/s", "value": rate, "unit": "attempted moves/s",
+            "n_gpus": args.gpus, "steps": steps, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic", "config": config,
+            "cpu_baseline": {"value": rate, "unit": "attempted moves/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": "attempted moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -122,6 +122,24 @@ int bfm_validate(bfm_handle h);
 /* Device bytes held by the handle. */
 int bfm_device_bytes(bfm_handle h, uint64_t* out);
 
+/* ------------------------------------------------------------------ measurement (no reference counterpart) */
+/* bfm_run bracketed by CUDA events on the handle's stream; *ms = device time of the n_mcs MCS. */
+int bfm_run_timed(bfm_handle h, int32_t n_mcs, float* ms);
+/* Runs n_mcs MCS on the grid-phase kernels one launch at a time, each bracketed by CUDA events:
+ * out = {check ms total, perform ms total, check launches, perform launches}. */
+int bfm_time_kernels(bfm_handle h, int32_t n_mcs, double out[4]);
+/* Kernels this handle has launched so far (graph replays counted per kernel). */
+int bfm_launch_count(bfm_handle h, uint64_t* out);
+
+/* ------------------------------------------------------------------ host-only helpers (no GPU needed) */
+/* The colouring step of initialize (graphColoring.tpp:77-293 with uniform rebalancing,
+ * UpdaterGPUScBFM_AB_Type.cu:549-555): colours_out[i] for monomer i; returns the status and
+ * writes the colour count. ids[i*stride + k] is neighbour k of monomer i. */
+int bfm_color_graph(uint32_t n, const uint32_t* counts, const uint32_t* ids, uint32_t stride,
+                    uint8_t* colours_out, uint32_t* n_colors);
+/* Draw k of the counter stream with the given seed. */
+uint32_t bfm_counter_draw(uint64_t seed, uint64_t k);
+
 /* ------------------------------------------------------------------ batch (no reference counterpart) */
 /* Advances many initialised handles on one GPU together; each keeps its own draw stream, so its
  * trajectory equals a run alone. Handles stay owned by the caller and must outlive the batch. */
@@ -129,6 +147,8 @@ int bfm_batch_create(bfm_batch_handle* out, int gpu, const bfm_handle* members, 
 int bfm_batch_destroy(bfm_batch_handle b);
 int bfm_batch_run(bfm_batch_handle b, int32_t n_mcs);        /* returns when done */
 int bfm_batch_run_async(bfm_batch_handle b, int32_t n_mcs);
+/* bfm_batch_run bracketed by CUDA events on the batch stream; *ms = device time. */
+int bfm_batch_run_timed(bfm_batch_handle b, int32_t n_mcs, float* ms);
 int bfm_batch_synchronize(bfm_batch_handle b);
 /* 0: every system on the grid path; 1 (default): small systems on the resident kernel. */
 int bfm_batch_set_resident(bfm_batch_handle b, int on);

@@ -76,15 +76,21 @@ _SIGS = {
     "bfm_get_stats": [H, _u64p],
     "bfm_validate": [H],
     "bfm_device_bytes": [H, C.POINTER(C.c_uint64)],
+    "bfm_run_timed": [H, C.c_int32, C.POINTER(C.c_float)],
+    "bfm_time_kernels": [H, C.c_int32, _f64p],
+    "bfm_launch_count": [H, C.POINTER(C.c_uint64)],
     "bfm_batch_create": [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p), C.c_uint32],
     "bfm_batch_destroy": [H],
     "bfm_batch_run": [H, C.c_int32],
     "bfm_batch_run_async": [H, C.c_int32],
+    "bfm_batch_run_timed": [H, C.c_int32, C.POINTER(C.c_float)],
     "bfm_batch_synchronize": [H],
     "bfm_batch_set_resident": [H, C.c_int],
+    "bfm_color_graph": [C.c_uint32, _u32p, _u32p, C.c_uint32,
+                        np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS"), C.POINTER(C.c_uint32)],
 }
-_RET = {"bfm_last_error": C.c_char_p, "bfm_batch_last_error": C.c_char_p}
-_RET_ARGS = {"bfm_last_error": [H], "bfm_batch_last_error": [H]}
+_RET = {"bfm_last_error": C.c_char_p, "bfm_batch_last_error": C.c_char_p, "bfm_counter_draw": C.c_uint32}
+_RET_ARGS = {"bfm_last_error": [H], "bfm_batch_last_error": [H], "bfm_counter_draw": [C.c_uint64, C.c_uint64]}
 
 _lib = None
 

@@ -189,6 +189,24 @@ void Batch::run(int32_t nMcs)
     }
 }
 
+float Batch::runTimed(int32_t nMcs)
+{
+    cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
+    for (Updater* u : members_) u->synchronize();
+    cudaEvent_t a, b;
+    cuda_check(cudaEventCreate(&a), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&b), "cudaEventCreate");
+    cuda_check(cudaEventRecord(a, stream_), "event");
+    run(nMcs);   // the resident stream joins stream_ before run() returns
+    cuda_check(cudaEventRecord(b, stream_), "event");
+    cuda_check(cudaEventSynchronize(b), "timed batch");
+    float ms = 0.f;
+    cuda_check(cudaEventElapsedTime(&ms, a, b), "elapsed");
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms;
+}
+
 void Batch::synchronize()
 {
     cuda_check(cudaStreamSynchronize(stream_), "batch");

@@ -181,6 +181,53 @@ int bfm_device_bytes(bfm_handle h, uint64_t* out)
     });
 }
 
+int bfm_run_timed(bfm_handle h, int32_t n, float* ms)
+{
+    BFM_CALL(h, {
+        if (!ms) throw std::invalid_argument("[bfm_run_timed] null output");
+        *ms = h->u.runTimed(n);
+    });
+}
+int bfm_time_kernels(bfm_handle h, int32_t n, double out[4])
+{
+    BFM_CALL(h, {
+        if (!out) throw std::invalid_argument("[bfm_time_kernels] null output");
+        h->u.timeKernels(n, out);
+    });
+}
+int bfm_launch_count(bfm_handle h, uint64_t* out)
+{
+    BFM_CALL(h, {
+        if (!out) throw std::invalid_argument("[bfm_launch_count] null output");
+        *out = h->u.launches();
+    });
+}
+
+// ---------------------------------------------------------------- host-only helpers
+
+int bfm_color_graph(uint32_t n, const uint32_t* counts, const uint32_t* ids, uint32_t stride, uint8_t* out,
+                    uint32_t* nColors)
+{
+    return guarded(nullptr, [&] {
+        if (n == 0) throw std::invalid_argument("[bfm_color_graph] no monomers");
+        if (!counts || !ids || !out) throw std::invalid_argument("[bfm_color_graph] null buffer");
+        for (uint32_t i = 0; i < n; ++i) {
+            if (counts[i] > stride) throw std::invalid_argument("[bfm_color_graph] count exceeds stride");
+            for (uint32_t k = 0; k < counts[i]; ++k)
+                if (ids[(size_t)i * stride + k] >= n) throw std::out_of_range("[bfm_color_graph] neighbour id out of range");
+        }
+        auto const c = bfm::colour_bond_graph(n, counts, ids, stride);
+        uint32_t nc = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            out[i] = c[i];
+            if ((uint32_t)c[i] + 1 > nc) nc = c[i] + 1u;
+        }
+        if (nColors) *nColors = nc;
+    });
+}
+
+uint32_t bfm_counter_draw(uint64_t seed, uint64_t k) { return bfm::counter_draw(seed, k); }
+
 // ---------------------------------------------------------------- batch
 
 const char* bfm_batch_last_error(bfm_batch_handle b) { return b ? b->err.c_str() : gErr.c_str(); }
@@ -217,6 +264,13 @@ int bfm_batch_run(bfm_batch_handle b, int32_t n)
     });
 }
 int bfm_batch_run_async(bfm_batch_handle b, int32_t n) { BFM_CALL(b, b->b.run(n)); }
+int bfm_batch_run_timed(bfm_batch_handle b, int32_t n, float* ms)
+{
+    BFM_CALL(b, {
+        if (!ms) throw std::invalid_argument("[bfm_batch_run_timed] null output");
+        *ms = b->b.runTimed(n);
+    });
+}
 int bfm_batch_synchronize(bfm_batch_handle b) { BFM_CALL(b, b->b.synchronize()); }
 int bfm_batch_set_resident(bfm_batch_handle b, int on) { BFM_CALL(b, b->b.setResidentEnabled(on != 0)); }
 

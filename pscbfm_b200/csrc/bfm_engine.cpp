@@ -434,6 +434,7 @@ void Updater::scrubPending(cudaStream_t s)
     cuda_check(cudaEventRecord(stepsFree_, s), "event");
     uint32_t const tiles = (maxGroup_ + kGridBlock - 1) / kGridBlock;
     cuda_check(launch_perform(dev_.dDesc, nullptr, std::max(tiles, 1u), kGridBlock, dev_.dSteps, s), "scrub");
+    ++launches_;
     lastColor_ = kNoColor;
 }
 
@@ -459,47 +460,115 @@ void Updater::enqueueLaunch(uint32_t nSteps)
             cuda_check(launch_check(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_), "check");
             cuda_check(launch_perform(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_), "perform");
         }
+        launches_ += 2ull * chunk;
         done += chunk;
     }
 }
 
+cudaGraphExec_t Updater::graphFor(uint32_t nSteps, uint32_t tiles)
+{
+    for (auto const& g : graphs_)
+        if (g.first == nSteps) return g.second;
+    cudaGraph_t g;
+    cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t err = cudaSuccess;
+    for (uint32_t t = 0; t < nSteps && err == cudaSuccess; ++t) {
+        err = launch_check(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_);
+        if (err == cudaSuccess) err = launch_perform(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_);
+    }
+    cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
+    cuda_check(err, "capture launches");
+    cuda_check(endErr, "end capture");
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t const instErr = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    cuda_check(instErr, "graph instantiate");
+    graphs_.emplace_back(nSteps, exec);
+    return exec;
+}
+
 void Updater::enqueueGraph(uint32_t nSteps)
 {
+    // full chunks of kGraphMcs MCS replay one graph; a shorter tail (or a short run) replays a
+    // graph of its own length, captured once and kept
     uint32_t const nC = (uint32_t)grpSize_.size();
     uint32_t const G = std::min(kGraphMcs * nC, hStepCap_);
     uint32_t const tiles = std::max((maxGroup_ + kGridBlock - 1) / kGridBlock, 1u);
-    if (nSteps < G) {
-        enqueueLaunch(nSteps);
-        return;
-    }
-    if (!graph_ || graphSteps_ != G) {
-        if (graph_) cudaGraphExecDestroy(graph_);
-        graph_ = nullptr;
-        cudaGraph_t g;
-        cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
-        cudaError_t err = cudaSuccess;
-        for (uint32_t t = 0; t < G && err == cudaSuccess; ++t) {
-            err = launch_check(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_);
-            if (err == cudaSuccess) err = launch_perform(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_);
-        }
-        cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
-        cuda_check(err, "capture launches");
-        cuda_check(endErr, "end capture");
-        cudaError_t const instErr = cudaGraphInstantiate(&graph_, g, 0);
-        cudaGraphDestroy(g);
-        cuda_check(instErr, "graph instantiate");
-        graphSteps_ = G;
-    }
-    uint32_t done = 0;
-    for (; done + G <= nSteps; done += G) {
+    for (uint32_t done = 0; done < nSteps;) {
+        uint32_t const chunk = std::min(G, nSteps - done);
+        cudaGraphExec_t const exec = graphFor(chunk, tiles);
         cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
-        fillSteps(G, hSteps_, false);
-        cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * G, cudaMemcpyHostToDevice, stream_),
+        fillSteps(chunk, hSteps_, false);
+        cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
                    "steps H2D");
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
-        cuda_check(cudaGraphLaunch(graph_, stream_), "graph launch");
+        cuda_check(cudaGraphLaunch(exec, stream_), "graph launch");
+        launches_ += 2ull * chunk;
+        done += chunk;
     }
-    if (done < nSteps) enqueueLaunch(nSteps - done);
+}
+
+float Updater::runTimed(int32_t nMcs)
+{
+    requireInit("runTimed");
+    cudaEvent_t a, b;
+    cuda_check(cudaEventCreate(&a), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&b), "cudaEventCreate");
+    cuda_check(cudaEventRecord(a, stream_), "event");
+    run(nMcs);
+    cuda_check(cudaEventRecord(b, stream_), "event");
+    cuda_check(cudaEventSynchronize(b), "timed run");
+    float ms = 0.f;
+    cuda_check(cudaEventElapsedTime(&ms, a, b), "elapsed");
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms;
+}
+
+void Updater::timeKernels(int32_t nMcs, double out[4])
+{
+    // the grid-phase kernels one launch at a time, each bracketed by CUDA events on the stream
+    // it runs on; sums per kernel
+    requireInit("timeKernels");
+    cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
+    scrubPending(stream_);
+    uint32_t const nSteps = (uint32_t)nMcs * (uint32_t)grpSize_.size();
+    uint32_t const tiles = std::max((maxGroup_ + kGridBlock - 1) / kGridBlock, 1u);
+    std::vector<cudaEvent_t> ev(3);
+    for (auto& e : ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+    double check = 0, perform = 0;
+    uint64_t n = 0;
+    for (uint32_t done = 0; done < nSteps;) {
+        uint32_t const chunk = std::min(nSteps - done, hStepCap_);
+        cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
+        fillSteps(chunk, hSteps_, false);
+        cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
+                   "steps H2D");
+        cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
+        for (uint32_t t = 0; t < chunk; ++t) {
+            cuda_check(cudaEventRecord(ev[0], stream_), "event");
+            cuda_check(launch_check(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_), "check");
+            cuda_check(cudaEventRecord(ev[1], stream_), "event");
+            cuda_check(launch_perform(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_), "perform");
+            cuda_check(cudaEventRecord(ev[2], stream_), "event");
+            cuda_check(cudaEventSynchronize(ev[2]), "timed kernels");
+            float a = 0, b = 0;
+            cuda_check(cudaEventElapsedTime(&a, ev[0], ev[1]), "elapsed");
+            cuda_check(cudaEventElapsedTime(&b, ev[1], ev[2]), "elapsed");
+            check += a;
+            perform += b;
+            ++n;
+        }
+        done += chunk;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    launches_ += 2 * n;
+    mcsDone_ += (uint64_t)nMcs;
+    hostStale_ = true;
+    out[0] = check;
+    out[1] = perform;
+    out[2] = (double)n;
+    out[3] = (double)n;
 }
 
 void Updater::enqueueResident(uint32_t nSteps)
@@ -517,6 +586,7 @@ void Updater::enqueueResident(uint32_t nSteps)
                    "steps H2D");
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         cuda_check(launch_resident(dev_.dDesc, dev_.dList, 1, per, dev_.dSteps, 1, chunk, smem, stream_), "resident");
+        ++launches_;
         done += chunk;
     }
     lastColor_ = kNoColor;   // the resident kernel leaves no marks in the global temporary lattices
@@ -684,11 +754,8 @@ void Updater::validate()
 
 void Updater::freeDevice()
 {
-    if (graph_) {
-        cudaGraphExecDestroy(graph_);
-        graph_ = nullptr;
-        graphSteps_ = 0;
-    }
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.second);
+    graphs_.clear();
     if (dev_.arena) {
         cudaSetDevice(gpu_);
         if (stream_) cudaStreamSynchronize(stream_);

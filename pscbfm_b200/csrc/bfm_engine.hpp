@@ -108,6 +108,12 @@ public:
     uint32_t lastColor() const { return lastColor_; }
     void streamWait(cudaEvent_t e);          // orders this system's later work after e
 
+    // measurement
+    float runTimed(int32_t nMcs);            // run + CUDA-event time on the handle's stream (ms)
+    void timeKernels(int32_t nMcs, double out[4]);   // check ms, perform ms, launches of each
+    uint64_t launches() const { return launches_; }  // kernels launched by this handle so far
+    void addLaunches(uint64_t n) { launches_ += n; }
+
 private:
     struct Device {
         void* arena = nullptr;
@@ -156,9 +162,10 @@ private:
     Device dev_;
     StepEntry* hSteps_ = nullptr;              // pinned staging for step entries
     uint32_t hStepCap_ = 0;
-    cudaGraphExec_t graph_ = nullptr;
-    uint32_t graphSteps_ = 0;
+    std::vector<std::pair<uint32_t, cudaGraphExec_t>> graphs_;   // captured chunk length -> graph
     cudaEvent_t stepsFree_ = nullptr;          // host staging may be rewritten after this event
+    uint64_t launches_ = 0;
+    cudaGraphExec_t graphFor(uint32_t nSteps, uint32_t tiles);
 };
 
 // A set of initialised updaters on one GPU advanced together: systems that fit one CTA run in the
@@ -170,6 +177,7 @@ public:
     Batch(int gpu, Updater* const* members, uint32_t n);
     ~Batch();
     void run(int32_t nMcs);     // enqueue
+    float runTimed(int32_t nMcs);   // run + CUDA-event time on the batch stream (ms)
     void synchronize();
     uint32_t size() const { return (uint32_t)members_.size(); }
     Updater* member(uint32_t i) const { return members_.at(i); }

@@ -199,6 +199,58 @@ def serpentine_chains(L: int, chain_len: int, phi: float, name: str = "", seed: 
     return from_bonds((L, L, L), xyz, bonds, name=name or f"serp{L}_{n_chains}x{chain_len}", seed=seed)
 
 
+_RING3 = [(0, 0, 0), (2, 0, 0), (1, 2, 0)]
+_RING5 = [(0, 0, 0), (2, 0, 0), (3, 2, 0), (1, 3, 0), (-1, 2, 0)]
+
+
+def rings_and_free(L: int = 32, spacing: int = 8, free_per_cell: int = 1, seed: int = 11) -> BfmSystem:
+    """Odd rings (3 and 5 monomers, which need three colours) on a grid of cells with the given
+    spacing, alternating per cell, plus `free_per_cell` unbonded monomers per cell (these let the
+    uniform colour pass move monomers between colours)."""
+    xyz, bonds, attrs = [], [], []
+    g = L // spacing
+    cell = 0
+    for i in range(g):
+        for j in range(g):
+            for k in range(g):
+                base = np.array([i, j, k]) * spacing + 1
+                ring = _RING3 if cell % 2 == 0 else _RING5
+                start = len(xyz)
+                for p in ring:
+                    xyz.append(base + np.array(p) + np.array([1, 0, 0]))
+                    attrs.append(1)
+                for m in range(len(ring)):
+                    bonds.append((start + m, start + (m + 1) % len(ring)))
+                for f in range(free_per_cell):
+                    xyz.append(base + np.array([0, 5, 2 + 2 * f]))
+                    attrs.append(2)
+                cell += 1
+    return from_bonds((L, L, L), np.array(xyz), bonds, attributes=np.array(attrs), name=f"rings{L}", seed=seed)
+
+
+def square_network(L: int = 64, spacing: int = 16, strand: int = 7, seed: int = 5) -> BfmSystem:
+    """Four-functional network: nodes on a (L/spacing)^3 grid linked along +x and +y (periodic) by
+    strands of `strand` monomers with axis bonds of length 2 (spacing = 2 (strand + 1))."""
+    assert spacing == 2 * (strand + 1)
+    G = L // spacing
+    nodes = [(i, j, k) for i in range(G) for j in range(G) for k in range(G)]
+    nid = {n: t for t, n in enumerate(nodes)}
+    xyz = [np.array(n) * spacing for n in nodes]
+    bonds = []
+    for n in nodes:
+        for a in range(2):
+            step = np.zeros(3, dtype=np.int64)
+            step[a] = 2
+            start = len(xyz)
+            for m in range(strand):
+                xyz.append(np.array(n) * spacing + step * (m + 1))
+            nxt = list(n)
+            nxt[a] = (nxt[a] + 1) % G
+            chain = [nid[n]] + list(range(start, start + strand)) + [nid[tuple(nxt)]]
+            bonds.extend(zip(chain[:-1], chain[1:]))
+    return from_bonds((L, L, L), np.array(xyz) % L, bonds, name=f"sqnet{L}", seed=seed)
+
+
 def ensemble_params(n_systems: int = 256, gen_seed: int = 20240611):
     """Per-system (L, chain_len, phi) draws of the batched ensemble: L uniform on {32, 64, 128},
     chain length uniform on {16, 32, 64, 128, 256}, phi uniform on [0.1, 0.5]."""

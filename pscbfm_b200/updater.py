@@ -16,6 +16,23 @@ from . import _lib
 from ._lib import MODE_AUTO, MODE_GRAPH, MODE_LAUNCH, MODE_RESIDENT  # noqa: F401
 
 
+def color_graph(system) -> np.ndarray:
+    """Colours of the system's monomers as initialize() computes them (host only, no GPU)."""
+    L = _lib.load()
+    cnt = np.ascontiguousarray(system.nbr_count, dtype=np.uint32)
+    ids = np.ascontiguousarray(system.nbr_ids, dtype=np.uint32).reshape(-1)
+    out = np.zeros(system.n, dtype=np.uint8)
+    nc = C.c_uint32()
+    st = L.bfm_color_graph(system.n, cnt, ids, system.maxc, out, C.byref(nc))
+    if st != _lib.BFM_OK:
+        _lib.raise_for(st, L.bfm_last_error(None).decode())
+    return out
+
+
+def counter_draw(seed: int, k: int) -> int:
+    return int(_lib.load().bfm_counter_draw(seed, k))
+
+
 class UpdaterGPUScBFM_AB_Type:
     def __init__(self, gpu: int = 0):
         self._L = _lib.load()
@@ -162,6 +179,23 @@ class UpdaterGPUScBFM_AB_Type:
         self._call("bfm_device_bytes", C.byref(v))
         return v.value
 
+    def run_timed(self, n_mcs: int) -> float:
+        """Runs n_mcs MCS; returns their device time in ms (CUDA events on the engine's stream)."""
+        ms = C.c_float()
+        self._call("bfm_run_timed", n_mcs, C.byref(ms))
+        return ms.value
+
+    def time_kernels(self, n_mcs: int):
+        out = np.zeros(4, dtype=np.float64)
+        self._call("bfm_time_kernels", n_mcs, out)
+        return {"check_ms": out[0], "perform_ms": out[1], "check_launches": int(out[2]),
+                "perform_launches": int(out[3])}
+
+    def launch_count(self) -> int:
+        v = C.c_uint64()
+        self._call("bfm_launch_count", C.byref(v))
+        return v.value
+
     n_monomers = 0
 
     def load_system(self, system, seed: int | None = None, mode: int | None = None, initialize: bool = True):
@@ -216,6 +250,11 @@ class Batch:
 
     def run_async(self, n_mcs: int):
         self._call("bfm_batch_run_async", n_mcs)
+
+    def run_timed(self, n_mcs: int) -> float:
+        ms = C.c_float()
+        self._call("bfm_batch_run_timed", n_mcs, C.byref(ms))
+        return ms.value
 
     def synchronize(self):
         self._call("bfm_batch_synchronize")

@@ -1,0 +1,70 @@
+"""The C-ABI library: it loads, exports every symbol include/bfm.h declares, the Python binding
+declares a signature for each, and without a GPU it fails loudly (no CPU fallback)."""
+import ctypes as C
+import subprocess
+
+import numpy as np
+import pytest
+
+from pscbfm_b200 import _lib
+from pscbfm_b200 import systems as S
+from pscbfm_b200.updater import color_graph, counter_draw
+
+
+def test_exports_every_declared_symbol():
+    L = _lib.load()
+    declared = _lib.declared_symbols()
+    assert len(declared) >= 35
+    for name in declared:
+        assert hasattr(L, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    assert set(declared) <= exported
+
+
+def test_binding_covers_header():
+    declared = set(_lib.declared_symbols())
+    bound = set(_lib._SIGS) | set(_lib._RET)
+    assert declared == bound, (declared ^ bound)
+
+
+def test_null_handle_and_null_buffers():
+    L = _lib.load()
+    assert L.bfm_run(None, 1) == _lib.BFM_ERR_NULL_HANDLE
+    assert L.bfm_destroy(None) == _lib.BFM_OK
+    assert L.bfm_create(None, 0) == _lib.BFM_ERR_INVALID_ARGUMENT
+
+
+def test_no_gpu_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    L = _lib.load()
+    h = C.c_void_p()
+    st = L.bfm_create(C.byref(h), 0)
+    assert st == _lib.BFM_ERR_CUDA
+    assert b"cuda" in L.bfm_last_error(None).lower()
+
+
+def test_host_colouring_matches_oracle():
+    from oracle import oracle as O
+    for s in [S.small_chains(), S.rings_and_free(), S.square_network(), S.crosslinked_network(),
+              S.serpentine_chains(64, 128, 0.4)]:
+        assert np.array_equal(color_graph(s), O.color(s)), s.name
+
+
+def test_counter_stream_matches_oracle():
+    from oracle import oracle as O
+    ref = O.counter_draws(42, 0, 64)
+    assert [counter_draw(42, k) for k in range(64)] == ref.tolist()
+    assert counter_draw(7, 0) != counter_draw(8, 0)
+
+
+def test_colour_errors():
+    L = _lib.load()
+    cnt = np.array([1], np.uint32)
+    ids = np.array([5], np.uint32)
+    out = np.zeros(1, np.uint8)
+    nc = C.c_uint32()
+    assert L.bfm_color_graph(1, cnt, ids, 1, out, C.byref(nc)) == _lib.BFM_ERR_OUT_OF_RANGE
+    assert L.bfm_color_graph(0, cnt, ids, 1, out, C.byref(nc)) == _lib.BFM_ERR_INVALID_ARGUMENT

@@ -1,0 +1,100 @@
+"""Error behaviour of the drop-in API mirrors the reference's exceptions
+(src/pscbfm/UpdaterGPUScBFM_AB_Type.cu: invalid_argument / runtime_error / out_of_range)."""
+import pytest
+
+import pscbfm_b200 as P
+from pscbfm_b200 import systems as S
+
+pytestmark = pytest.mark.gpu
+
+
+def fresh():
+    return P.UpdaterGPUScBFM_AB_Type(0)
+
+
+def test_set_gpu_out_of_range():
+    u = fresh()
+    with pytest.raises(ValueError, match="not present"):
+        u.setGpu(999)
+
+
+def test_non_periodic_rejected():
+    with pytest.raises(ValueError, match="periodic"):
+        fresh().setPeriodicity(True, False, True)
+
+
+def test_monomer_count_set_twice():
+    u = fresh()
+    u.setNrOfAllMonomers(4)
+    with pytest.raises(RuntimeError, match="already set"):
+        u.setNrOfAllMonomers(5)
+
+
+def test_box_must_be_power_of_two():
+    with pytest.raises(RuntimeError, match="power of 2"):
+        fresh().setLatticeSize(48, 64, 64)
+    with pytest.raises(ValueError):
+        fresh().setLatticeSize(2048, 64, 64)
+
+
+def test_too_many_bonds():
+    u = fresh()
+    u.setNrOfAllMonomers(20)
+    for j in range(1, 17):
+        u.setConnectivity(0, j)
+    with pytest.raises(ValueError, match="maximum amount of bonds"):
+        u.setConnectivity(0, 17)
+
+
+def test_index_errors():
+    u = fresh()
+    u.setNrOfAllMonomers(3)
+    with pytest.raises(IndexError):
+        u.setMonomerCoordinates(3, 0, 0, 0)
+    with pytest.raises(IndexError):
+        u.setConnectivity(0, 7)
+
+
+def test_wrong_bond_set_and_double_initialize():
+    s = S.small_chains()
+    u = fresh()
+    u.load_system(s, initialize=False)
+    u.copyBondSet(3, 1, 0, True)
+    with pytest.raises(RuntimeError, match="Expected 108 allowed bonds, but got 107"):
+        u.initialize()
+    u.copyBondSet(3, 1, 0, False)
+    u.initialize()
+    with pytest.raises(RuntimeError, match="Initialize was already called"):
+        u.initialize()
+
+
+def test_run_before_initialize():
+    u = fresh()
+    u.setNrOfAllMonomers(2)
+    with pytest.raises(RuntimeError, match="initialize"):
+        u.runSimulationOnGPU(1)
+
+
+def test_cleanup_allows_repeat():
+    s = S.small_chains()
+    u = fresh()
+    u.load_system(s)
+    u.runSimulationOnGPU(5)
+    a = u.get_coords().copy()
+    u.cleanup()
+    u.load_system(s)
+    u.runSimulationOnGPU(5)
+    assert (u.get_coords() == a).all()
+
+
+def test_reference_getters_and_colours():
+    s = S.rings_and_free()
+    u = fresh()
+    u.load_system(s)
+    assert u.getMonomerPositionInX(0) == s.xyz[0, 0]
+    assert u.getMonomerPositionInY(1) == s.xyz[1, 1]
+    assert u.getMonomerPositionInZ(2) == s.xyz[2, 2]
+    n, sizes = u.n_colors()
+    assert n == 3 and sizes.sum() == s.n
+    assert u.execute() is True
+    assert u.device_bytes() > 0

@@ -1,0 +1,156 @@
+"""Parity of the CUDA engine (through the C-ABI) with the reference and the oracle: bit-exact
+final positions, for every engine path, at the configs' sizes and on ragged / odd cases."""
+import json
+
+import numpy as np
+import pytest
+
+import pscbfm_b200 as P
+from cases import CASES, GOLDEN_JSON, positions_digest
+from oracle import oracle as O
+from pscbfm_b200 import systems as S
+
+pytestmark = pytest.mark.gpu
+
+MODES = {"launch": P.MODE_LAUNCH, "graph": P.MODE_GRAPH, "resident": P.MODE_RESIDENT, "auto": P.MODE_AUTO}
+
+
+def run_engine(s, chunks, mode=P.MODE_AUTO, seed=None):
+    u = P.UpdaterGPUScBFM_AB_Type(0)
+    u.load_system(s, seed=seed, mode=mode)
+    for c in chunks:
+        u.runSimulationOnGPU(c)
+    xyz = u.get_coords().copy()
+    st = u.stats()
+    u.validate()
+    u.close()
+    return xyz, st
+
+
+def _resident_ok(s):
+    return max(s.box) <= 64
+
+
+@pytest.mark.parametrize("mode", ["launch", "graph", "resident"])
+@pytest.mark.parametrize("name", list(CASES))
+def test_engine_reproduces_reference_updater(name, mode):
+    g = json.load(open(GOLDEN_JSON))["cases"][name]
+    build, chunks = CASES[name]
+    s = build()
+    if mode == "resident" and not _resident_ok(s):
+        pytest.skip("box larger than the resident kernel holds")
+    xyz, st = run_engine(s, chunks, MODES[mode])
+    assert positions_digest(xyz) == g["sha256"]
+    assert st["mcs"] == sum(chunks)
+
+
+def test_engine_matches_live_reference_updater():
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    s = S.small_chains()
+    draws = O.counter_draws(s.seed, 0, 2 * 2 * 300)
+    ref, used = O.ref_run(s, draws, [100, 200])
+    assert used == len(draws)
+    xyz, _ = run_engine(s, [300])
+    assert np.array_equal(xyz, ref)
+
+
+@pytest.mark.parametrize("mode", ["launch", "graph"])
+def test_six_functional_network_vs_oracle(mode):
+    # the reference is compiled with MAX_CONNECTIVITY 4, so this case is pinned by the oracle only
+    s = S.crosslinked_network()
+    ref, ost = O.run(s, 1000)
+    xyz, st = run_engine(s, [400, 600], MODES[mode])
+    assert np.array_equal(xyz, ref)
+    assert (st["attempted"], st["tentative"], st["accepted"]) == ost
+
+
+def test_dense_melt_full_config():
+    """256^3 melt at phi = 0.5: the full 10^4 MCS of the config, split across calls and modes,
+    equals one uninterrupted run; invariants hold; the first MCS match the oracle."""
+    s = S.dense_melt()
+    ref, _ = O.run(s, 4)
+    xyz4, _ = run_engine(s, [4], P.MODE_GRAPH)
+    assert np.array_equal(xyz4, ref)
+    a, sa = run_engine(s, [10000], P.MODE_GRAPH)
+    u = P.UpdaterGPUScBFM_AB_Type(0)
+    u.load_system(s, mode=P.MODE_LAUNCH)
+    u.runSimulationOnGPU(3000)
+    u.set_mode(P.MODE_GRAPH)
+    u.runSimulationOnGPU(7000)
+    b = u.get_coords().copy()
+    u.validate()
+    u.close()
+    assert np.array_equal(a, b)
+    assert sa["attempted"] == 10000 * s.n
+
+
+def test_mode_switches_mid_run():
+    s = S.serpentine_chains(64, 32, 0.35, seed=21)
+    ref, _ = O.run(s, 90)
+    u = P.UpdaterGPUScBFM_AB_Type(0)
+    u.load_system(s, mode=P.MODE_LAUNCH)
+    u.runSimulationOnGPU(30)
+    u.set_mode(P.MODE_RESIDENT)
+    u.runSimulationOnGPU(30)
+    u.set_mode(P.MODE_GRAPH)
+    u.runSimulationOnGPU(30)
+    assert np.array_equal(u.get_coords(), ref)
+    u.close()
+
+
+def test_callback_stream_equals_counter_stream():
+    s = S.rings_and_free()
+    k = iter(range(10 ** 9))
+    u = P.UpdaterGPUScBFM_AB_Type(0)
+    u.load_system(s)
+    u.set_draw_callback(lambda: P.updater.counter_draw(s.seed, next(k)))
+    u.runSimulationOnGPU(200)
+    xyz = u.get_coords().copy()
+    u.close()
+    ref, _ = O.run(s, 200)
+    assert np.array_equal(xyz, ref)
+
+
+def test_set_coords_after_initialize():
+    s = S.small_chains()
+    mid, _ = O.run(s, 25)
+    u = P.UpdaterGPUScBFM_AB_Type(0)
+    u.load_system(s)
+    u.runSimulationOnGPU(10)
+    u.set_coords(mid)   # replaces the state; the draw stream continues at sub-step 20
+    u.runSimulationOnGPU(15)
+    got = u.get_coords().copy()
+    u.close()
+    s2 = S.BfmSystem(s.box, mid.astype(np.int32), s.nbr_count, s.nbr_ids, s.attributes, s.forbidden, seed=s.seed)
+    ref, _ = O.run(s2, 15, substep0=20)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("resident", [True, False])
+def test_batch_equals_each_system_alone(resident):
+    systems = S.ensemble(n_systems=20)
+    systems.append(S.rings_and_free())         # three colours in the mix
+    members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
+    b = P.Batch(members, resident=resident)
+    b.run(60)
+    b.run(40)
+    for s, m in zip(systems, members):
+        ref, _ = O.run(s, 100)
+        assert np.array_equal(m.get_coords(), ref), s.name
+        m.validate()
+    b.close()
+    for m in members:
+        m.close()
+
+
+def test_single_monomer_and_ragged_groups():
+    # one free monomer, and a 33-monomer chain (groups of 17 and 16: ragged tiles)
+    one = S.from_bonds((8, 8, 8), np.array([[1, 1, 1]]), np.zeros((0, 2)), seed=4)
+    xyz = np.array([[2 * j, 0, 0] for j in range(33)])
+    chain = S.from_bonds((128, 128, 128), xyz, [(j, j + 1) for j in range(32)], seed=5)
+    for s in (one, chain):
+        for mode in ("launch", "graph", "resident"):
+            ref, _ = O.run(s, 120)
+            got, _ = run_engine(s, [120], MODES[mode])
+            assert np.array_equal(got, ref), (s.name, mode)
