@@ -68,3 +68,42 @@ def test_colour_errors():
     nc = C.c_uint32()
     assert L.bfm_color_graph(1, cnt, ids, 1, out, C.byref(nc)) == _lib.BFM_ERR_OUT_OF_RANGE
     assert L.bfm_color_graph(0, cnt, ids, 1, out, C.byref(nc)) == _lib.BFM_ERR_INVALID_ARGUMENT
+
+
+def test_cpp_wrapper_compiles_for_reference_style_callers(tmp_path):
+    """A caller written like GPUScBFM_AB_Type::initialize/execute compiles and links against
+    include/bfm_updater.hpp + libbfm.so."""
+    import os
+    src = tmp_path / "caller.cpp"
+    src.write_text(r'''
+#include "bfm_updater.hpp"
+#include <cstdio>
+int main() {
+    try {
+        UpdaterGPUScBFM_AB_Type u;
+        u.setGpu(0);
+        u.setPeriodicity(true, true, true);
+        u.setNrOfAllMonomers(2);
+        u.setMonomerCoordinates(0, 0, 0, 0);
+        u.setMonomerCoordinates(1, 2, 0, 0);
+        u.setAttribute(0, 1);
+        u.setConnectivity(0, 1);
+        u.setConnectivity(1, 0);
+        u.setLatticeSize(8, 8, 8);
+        u.populateLattice();
+        for (int dx = -4; dx < 4; ++dx) for (int dy = -4; dy < 4; ++dy) for (int dz = -4; dz < 4; ++dz)
+            u.copyBondSet(dx, dy, dz, true);
+        u.initialize();
+        u.runSimulationOnGPU(10);
+        std::printf("%d\n", u.getMonomerPositionInX(1));
+        u.cleanup();
+    } catch (std::exception const& e) { std::printf("error: %s\n", e.what()); return 1; }
+    return 0;
+}
+''')
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = tmp_path / "caller"
+    r = subprocess.run(["g++", "-std=c++14", "-I", os.path.join(root, "include"), str(src), "-o", str(out),
+                        "-L", os.path.join(root, "pscbfm_b200"), "-lbfm",
+                        "-Wl,-rpath," + os.path.join(root, "pscbfm_b200")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
