@@ -154,6 +154,36 @@ int bfm_batch_synchronize(bfm_batch_handle b);
 int bfm_batch_set_resident(bfm_batch_handle b, int on);
 const char* bfm_batch_last_error(bfm_batch_handle b);
 
+/* ------------------------------------------------------------------ sweep without allocation */
+/* No counterpart in the reference. For callers that must not have the library allocate device
+ * memory: programs that reserved the GPU's memory for their own pool, and latency-sensitive
+ * loops where cudaMalloc/cudaFree would synchronise the device. The caller owns every input and
+ * output buffer; the engine's scratch is one fixed 32 MiB device array inside the library, held by
+ * every GPU that loads it until the process exits. Systems needing more scratch than that
+ * (roughly npad * 9 B + box volume / 4 B) are rejected with BFM_ERR_INVALID_ARGUMENT. The first
+ * call on a device performs a one-time set-up (the scratch's device address) and should come
+ * before any stream capture. All calls share the scratch: calls that overlap on the GPU race. */
+typedef struct bfm_noalloc_system {
+    int32_t* x;                   /* device, npad, in/out: colour-sorted corner positions;  */
+    int32_t* y;                   /*   padding slots have x = INT32_MIN                      */
+    int32_t* z;
+    const uint32_t* nbr;          /* device, maxc * npad: neighbour k of slot g at k*npad + g */
+    const uint8_t* nnb;           /* device, npad: neighbour count of each slot */
+    uint32_t npad;                /* slots, padding included */
+    uint32_t maxc;                /* neighbour slots per monomer, 1..16 */
+    uint32_t box[3];              /* powers of two, 4..1024 */
+    uint32_t n_colors;            /* colour groups (bfm_color_graph) */
+    const uint32_t* group_offset; /* host, n_colors: first slot of each colour group */
+    const uint32_t* group_size;   /* host, n_colors: monomers of each group (in-colour index order) */
+    const uint8_t* forbidden;     /* host, 512: bond table, 1 = forbidden */
+} bfm_noalloc_system;
+/* n_mcs MCS of the counter draw stream (seed) starting at sub-step substep0, on `stream` (a
+ * cudaStream_t, may be NULL), with the same kernels and results as bfm_run. Calls no
+ * cudaMalloc/cudaFree and allocates no host memory; returns once the work is queued. On error,
+ * a message goes to err (err_len bytes) if err is not NULL. */
+int bfm_sweep_noalloc(const bfm_noalloc_system* s, int32_t n_mcs, uint64_t seed, uint64_t substep0, void* stream,
+                      char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

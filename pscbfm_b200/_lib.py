@@ -37,6 +37,13 @@ class BfmBusy(RuntimeError):
     """A server result is not ready yet."""
 
 
+class NoallocSystem(C.Structure):
+    """bfm_noalloc_system of include/bfm.h."""
+    _fields_ = [("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p), ("nbr", C.c_void_p), ("nnb", C.c_void_p),
+                ("npad", C.c_uint32), ("maxc", C.c_uint32), ("box", C.c_uint32 * 3), ("n_colors", C.c_uint32),
+                ("group_offset", C.c_void_p), ("group_size", C.c_void_p), ("forbidden", C.c_void_p)]
+
+
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
@@ -86,6 +93,7 @@ _SIGS = {
     "bfm_batch_run_timed": [H, C.c_int32, C.POINTER(C.c_float)],
     "bfm_batch_synchronize": [H],
     "bfm_batch_set_resident": [H, C.c_int],
+    "bfm_sweep_noalloc": [C.c_void_p, C.c_int32, C.c_uint64, C.c_uint64, C.c_void_p, C.c_char_p, C.c_size_t],
     "bfm_color_graph": [C.c_uint32, _u32p, _u32p, C.c_uint32,
                         np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS"), C.POINTER(C.c_uint32)],
 }
