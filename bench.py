@@ -258,9 +258,12 @@ def run_ours(args):
     def step_timed(n):
         return u0.run_timed(n) if batch is None else batch.run_timed(n)
 
+    def launch_count():
+        return u0.launch_count() if batch is None else batch.launch_count()
+
     for _ in range(args.warmup):
         step_timed(1)
-    launches0 = sum(m.launch_count() for m in members)
+    launches0 = launch_count()
     stats0 = [m.stats() for m in members]
     barrier(world)
     torch.cuda.synchronize()
@@ -273,7 +276,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     clocks = sampler.stop()
     barrier(world)
-    launches = sum(m.launch_count() for m in members) - launches0
+    launches = launch_count() - launches0
     stats1 = [m.stats() for m in members]
     attempted = sum(b["attempted"] - a["attempted"] for a, b in zip(stats0, stats1))
     tentative = sum(b["tentative"] - a["tentative"] for a, b in zip(stats0, stats1))

@@ -95,6 +95,16 @@ int bfm_set_seed(bfm_handle h, uint64_t seed);
 int bfm_set_draw_callback(bfm_handle h, bfm_draw_fn fn, void* ctx);
 /* Engine path, BFM_MODE_*. */
 int bfm_set_mode(bfm_handle h, int mode);
+/* Device representation of the bonds, chosen before bfm_initialize: BFM_REPR_AUTO (bond codes —
+ * each monomer keeps the table indices of its bonds, updated exactly when it or a neighbour moves
+ * — when every bond is listed in both directions and no monomer has more than 6; otherwise the
+ * neighbours' positions are gathered like the reference does) or BFM_REPR_GATHER. Results are
+ * identical; only speed differs. */
+#define BFM_REPR_AUTO 0
+#define BFM_REPR_GATHER 1
+int bfm_set_representation(bfm_handle h, int repr);
+/* The representation initialize chose: 0 gather, 1 bond codes (32-bit), 2 bond codes (64-bit). */
+int bfm_get_representation(bfm_handle h, int* out);
 
 /* ------------------------------------------------------------------ simulation */
 /* initialize (UpdaterGPUScBFM_AB_Type.cu:490-690): bond-set check (exactly 108 allowed),
@@ -149,6 +159,8 @@ int bfm_batch_run(bfm_batch_handle b, int32_t n_mcs);        /* returns when don
 int bfm_batch_run_async(bfm_batch_handle b, int32_t n_mcs);
 /* bfm_batch_run bracketed by CUDA events on the batch stream; *ms = device time. */
 int bfm_batch_run_timed(bfm_batch_handle b, int32_t n_mcs, float* ms);
+/* Kernels the batch has launched so far (graph replays counted per kernel). */
+int bfm_batch_launch_count(bfm_batch_handle b, uint64_t* out);
 int bfm_batch_synchronize(bfm_batch_handle b);
 /* 0: every system on the grid path; 1 (default): small systems on the resident kernel. */
 int bfm_batch_set_resident(bfm_batch_handle b, int on);

@@ -73,6 +73,9 @@ _SIGS = {
     "bfm_set_seed": [H, C.c_uint64],
     "bfm_set_draw_callback": [H, DRAW_FN, C.c_void_p],
     "bfm_set_mode": [H, C.c_int],
+    "bfm_set_representation": [H, C.c_int],
+    "bfm_get_representation": [H, C.POINTER(C.c_int)],
+    "bfm_batch_launch_count": [H, C.POINTER(C.c_uint64)],
     "bfm_initialize": [H],
     "bfm_run": [H, C.c_int32],
     "bfm_run_async": [H, C.c_int32],

@@ -1,11 +1,12 @@
 // Batch: many independent systems advanced together on one GPU.
 //
-// Systems whose three occupancy lattices fit one CTA's shared memory run in the resident kernel,
-// one CTA per system, one launch per chunk of sub-steps. The other systems share the grid-phase
-// kernels: one check and one perform launch per sub-step cover the active colour group of every
-// such system at once, and a chunk of those launches is captured into a CUDA graph once and
-// replayed. The two paths run concurrently on two streams. Each system draws its own sub-steps
-// from its own stream exactly as it would alone, so its trajectory is unchanged by batching.
+// Systems whose lattices (and, in the bond-code representation, packed coordinates and bond
+// codes) fit one CTA's shared memory run in the resident kernel, one CTA per system, one launch
+// per chunk of sub-steps. The other systems share the grid-phase kernels: one check and one
+// perform launch per sub-step and representation cover the active colour group of every such
+// system at once, and a chunk of those launches is captured into a CUDA graph once and replayed.
+// The two paths run concurrently on two streams. Each system draws its own sub-steps from its own
+// stream exactly as it would alone, so its trajectory is unchanged by batching.
 
 #include <algorithm>
 #include <cstring>
@@ -17,7 +18,8 @@ namespace bfm {
 
 namespace {
 constexpr uint32_t kBatchChunk = 64;      // sub-steps per staged chunk / per captured graph
-}
+size_t up256(size_t v) { return (v + 255) & ~size_t(255); }
+}  // namespace
 
 Batch::Batch(int gpu, Updater* const* members, uint32_t n) : gpu_(gpu)
 {
@@ -46,67 +48,105 @@ Batch::~Batch()
     if (stream_) cudaStreamSynchronize(stream_);
     if (stream2_) cudaStreamSynchronize(stream2_);
     if (graph_) cudaGraphExecDestroy(graph_);
-    cudaFree(dSys_);
+    cudaFree(arena_);
     cudaFreeHost(hSteps_);
-    if (join_) cudaEventDestroy(join_);
-    if (fork_) cudaEventDestroy(fork_);
-    if (stepsFree_) cudaEventDestroy(stepsFree_);
-    if (done_) cudaEventDestroy(done_);
+    for (cudaEvent_t e : {join_, fork_, stepsFree_, done_})
+        if (e) cudaEventDestroy(e);
     if (stream_) cudaStreamDestroy(stream_);
     if (stream2_) cudaStreamDestroy(stream2_);
+}
+
+uint32_t Batch::residentCount() const
+{
+    uint32_t n = 0;
+    for (auto const& g : resident_) n += (uint32_t)g.members.size();
+    return n;
 }
 
 void Batch::rebuild()
 {
     uint32_t const M = (uint32_t)members_.size();
-    resident_.clear();
     grid_.clear();
-    tiles_.clear();
-    residentPerThread_ = 1;
-    residentSmem_ = 0;
+    resident_.clear();
+    isResident_.assign(M, 0);
+    auto gridGroup = [&](uint32_t mode) -> GridGroup& {
+        for (auto& g : grid_)
+            if (g.codeMode == mode) return g;
+        grid_.push_back(GridGroup{mode, {}, nullptr});
+        return grid_.back();
+    };
+    auto resGroup = [&](uint32_t mode) -> ResidentGroup& {
+        for (auto& g : resident_)
+            if (g.codeMode == mode) return g;
+        resident_.push_back(ResidentGroup{mode, {}, nullptr, 1, 0});
+        return resident_.back();
+    };
     for (uint32_t m = 0; m < M; ++m) {
         Updater* u = members_[m];
         if (residentOn_ && u->residentEligible()) {
-            resident_.push_back(m);
-            SysDev const& d = u->desc();
-            residentSmem_ = std::max(residentSmem_, resident_smem_bytes(d.nwords, d.nb[0] + d.nb[1] + d.nb[2]));
-            while (residentPerThread_ * kResidentBlock < u->maxGroup()) residentPerThread_ *= 2;
+            ResidentGroup& g = resGroup(u->codeMode());
+            g.members.push_back(m);
+            g.smem = std::max(g.smem, u->residentSmem());
+            while (g.perThread * kResidentBlock < u->maxGroup()) g.perThread *= 2;
+            isResident_[m] = 1;
         } else {
-            grid_.push_back(m);
-            uint32_t const t = std::max((u->maxGroup() + kGridBlock - 1) / kGridBlock, 1u);
-            for (uint32_t k = 0; k < t; ++k) tiles_.push_back(TileRef{m, k * kGridBlock});
+            GridGroup& g = gridGroup(u->codeMode());
+            uint32_t const span = u->codeMode() == kCodeNone ? kGridBlock : kBcTileSpan;
+            uint32_t const t = u->gridTiles();
+            for (uint32_t k = 0; k < t; ++k) g.tiles.push_back(TileRef{m, k * span});
         }
     }
     stepCap_ = kBatchChunk;
-    size_t const stepsBytes = sizeof(StepEntry) * stepCap_ * M;
-    size_t const sysBytes = (sizeof(SysDev) * M + 255) & ~size_t(255);
-    size_t const tileBytes = (sizeof(TileRef) * std::max<size_t>(tiles_.size(), 1) + 255) & ~size_t(255);
-    size_t const listBytes = (sizeof(uint32_t) * std::max<size_t>(resident_.size(), 1) + 255) & ~size_t(255);
-    cudaFree(dSys_);
-    void* p = nullptr;
-    cuda_check(cudaMalloc(&p, sysBytes + tileBytes + listBytes + stepsBytes), "cudaMalloc(batch)");
-    char* base = static_cast<char*>(p);
-    dSys_ = reinterpret_cast<SysDev*>(base);
-    dTiles_ = reinterpret_cast<TileRef*>(base + sysBytes);
-    dResList_ = reinterpret_cast<uint32_t*>(base + sysBytes + tileBytes);
-    dSteps_ = reinterpret_cast<StepEntry*>(base + sysBytes + tileBytes + listBytes);
+    size_t total = up256(sizeof(SysDev) * M) + up256(sizeof(StepEntry) * stepCap_ * M);
+    for (auto const& g : grid_) total += up256(sizeof(TileRef) * g.tiles.size());
+    for (auto const& g : resident_) total += up256(sizeof(uint32_t) * g.members.size());
+    cudaFree(arena_);
+    arena_ = nullptr;
+    cuda_check(cudaMalloc(&arena_, total), "cudaMalloc(batch)");
+    char* p = static_cast<char*>(arena_);
+    dSys_ = reinterpret_cast<SysDev*>(p);
+    p += up256(sizeof(SysDev) * M);
+    dSteps_ = reinterpret_cast<StepEntry*>(p);
+    p += up256(sizeof(StepEntry) * stepCap_ * M);
     std::vector<SysDev> descs(M);
     for (uint32_t m = 0; m < M; ++m) descs[m] = members_[m]->desc();
     cuda_check(cudaMemcpy(dSys_, descs.data(), sizeof(SysDev) * M, cudaMemcpyHostToDevice), "upload descriptors");
-    if (!tiles_.empty())
-        cuda_check(cudaMemcpy(dTiles_, tiles_.data(), sizeof(TileRef) * tiles_.size(), cudaMemcpyHostToDevice),
+    for (auto& g : grid_) {
+        g.dTiles = reinterpret_cast<TileRef*>(p);
+        p += up256(sizeof(TileRef) * g.tiles.size());
+        cuda_check(cudaMemcpy(g.dTiles, g.tiles.data(), sizeof(TileRef) * g.tiles.size(), cudaMemcpyHostToDevice),
                    "upload tiles");
-    if (!resident_.empty())
-        cuda_check(cudaMemcpy(dResList_, resident_.data(), sizeof(uint32_t) * resident_.size(), cudaMemcpyHostToDevice),
+    }
+    for (auto& g : resident_) {
+        g.dList = reinterpret_cast<uint32_t*>(p);
+        p += up256(sizeof(uint32_t) * g.members.size());
+        cuda_check(cudaMemcpy(g.dList, g.members.data(), sizeof(uint32_t) * g.members.size(), cudaMemcpyHostToDevice),
                    "upload resident list");
+    }
     cudaFreeHost(hSteps_);
     hSteps_ = nullptr;
-    cuda_check(cudaMallocHost(&hSteps_, stepsBytes), "cudaMallocHost(batch steps)");
+    cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * stepCap_ * M), "cudaMallocHost(batch steps)");
     if (graph_) {
         cudaGraphExecDestroy(graph_);
         graph_ = nullptr;
     }
     built_ = true;
+}
+
+cudaError_t Batch::launchGrid(uint32_t t, uint32_t M)
+{
+    StepEntry const* e = dSteps_ + (size_t)t * M;
+    SysDev const unused{};   // multi-system launches read each CTA's descriptor from dSys_
+    for (auto const& g : grid_) {
+        uint32_t const n = (uint32_t)g.tiles.size();
+        cudaError_t err = g.codeMode == kCodeNone ? launch_check(dSys_, g.dTiles, n, kGridBlock, e, stream_)
+                                                  : launch_check_bc(unused, dSys_, g.dTiles, n, e, g.codeMode, stream_);
+        if (err != cudaSuccess) return err;
+        err = g.codeMode == kCodeNone ? launch_perform(dSys_, g.dTiles, n, kGridBlock, e, stream_)
+                                      : launch_perform_bc(unused, dSys_, g.dTiles, n, e, g.codeMode, stream_);
+        if (err != cudaSuccess) return err;
+    }
+    return cudaSuccess;
 }
 
 void Batch::run(int32_t nMcs)
@@ -118,8 +158,10 @@ void Batch::run(int32_t nMcs)
     // run resident must be cleared first
     for (Updater* u : members_) u->synchronize();
     if (!built_) rebuild();
-    for (uint32_t m : resident_) members_[m]->scrubPending(members_[m]->stream());
-    for (uint32_t m : resident_) members_[m]->synchronize();
+    for (uint32_t m = 0; m < M; ++m)
+        if (isResident_[m]) members_[m]->scrubPending(members_[m]->stream());
+    for (uint32_t m = 0; m < M; ++m)
+        if (isResident_[m]) members_[m]->synchronize();
 
     std::vector<uint64_t> need(M);
     uint64_t T = 0;
@@ -127,7 +169,6 @@ void Batch::run(int32_t nMcs)
         need[m] = (uint64_t)nMcs * members_[m]->nColors();
         T = std::max(T, need[m]);
     }
-    uint32_t const nGridTiles = (uint32_t)tiles_.size();
     for (uint64_t t0 = 0; t0 < T; t0 += stepCap_) {
         uint32_t const chunk = (uint32_t)std::min<uint64_t>(stepCap_, T - t0);
         cuda_check(cudaEventSynchronize(stepsFree_), "batch staging");
@@ -135,7 +176,7 @@ void Batch::run(int32_t nMcs)
             for (uint32_t m = 0; m < M; ++m) {
                 StepEntry& e = hSteps_[(size_t)t * M + m];
                 if (t0 + t < need[m]) e = members_[m]->nextStep();
-                else e = StepEntry{kNoColor, 0u, 0u, kNoColor};
+                else e = StepEntry{kNoColor, 0u, 0u, kNoColor, 0u, 0u, 0u, 0u};
             }
         cuda_check(cudaMemcpyAsync(dSteps_, hSteps_, sizeof(StepEntry) * chunk * M, cudaMemcpyHostToDevice, stream_),
                    "batch steps H2D");
@@ -143,21 +184,23 @@ void Batch::run(int32_t nMcs)
         if (!resident_.empty()) {
             cuda_check(cudaEventRecord(fork_, stream_), "event");
             cuda_check(cudaStreamWaitEvent(stream2_, fork_, 0), "wait");
-            cuda_check(launch_resident(dSys_, dResList_, (uint32_t)resident_.size(), residentPerThread_, dSteps_, M,
-                                       chunk, residentSmem_, stream2_),
-                       "batch resident");
+            for (auto const& g : resident_) {
+                cuda_check(g.codeMode == kCodeNone
+                               ? launch_resident(dSys_, g.dList, (uint32_t)g.members.size(), g.perThread, dSteps_, M,
+                                                 chunk, g.smem, stream2_)
+                               : launch_resident_bc(dSys_, g.dList, (uint32_t)g.members.size(), g.perThread, dSteps_,
+                                                    M, chunk, g.smem, g.codeMode, stream2_),
+                           "batch resident");
+                ++launches_;
+            }
         }
-        if (nGridTiles) {
+        if (!grid_.empty()) {
             if (chunk == stepCap_) {
                 if (!graph_) {
                     cudaGraph_t g;
                     cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
                     cudaError_t err = cudaSuccess;
-                    for (uint32_t t = 0; t < stepCap_ && err == cudaSuccess; ++t) {
-                        err = launch_check(dSys_, dTiles_, nGridTiles, kGridBlock, dSteps_ + (size_t)t * M, stream_);
-                        if (err == cudaSuccess)
-                            err = launch_perform(dSys_, dTiles_, nGridTiles, kGridBlock, dSteps_ + (size_t)t * M, stream_);
-                    }
+                    for (uint32_t t = 0; t < stepCap_ && err == cudaSuccess; ++t) err = launchGrid(t, M);
                     cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
                     cuda_check(err, "capture batch launches");
                     cuda_check(endErr, "end capture");
@@ -167,24 +210,18 @@ void Batch::run(int32_t nMcs)
                 }
                 cuda_check(cudaGraphLaunch(graph_, stream_), "batch graph launch");
             } else {
-                for (uint32_t t = 0; t < chunk; ++t) {
-                    cuda_check(launch_check(dSys_, dTiles_, nGridTiles, kGridBlock, dSteps_ + (size_t)t * M, stream_),
-                               "batch check");
-                    cuda_check(launch_perform(dSys_, dTiles_, nGridTiles, kGridBlock, dSteps_ + (size_t)t * M, stream_),
-                               "batch perform");
-                }
+                for (uint32_t t = 0; t < chunk; ++t) cuda_check(launchGrid(t, M), "batch grid launch");
             }
+            launches_ += 2ull * chunk * grid_.size();
         }
         if (!resident_.empty()) {
             cuda_check(cudaEventRecord(join_, stream2_), "event");
             cuda_check(cudaStreamWaitEvent(stream_, join_, 0), "wait");
         }
     }
-    std::vector<char> isRes(M, 0);
-    for (uint32_t m : resident_) isRes[m] = 1;
     cuda_check(cudaEventRecord(done_, stream_), "event");
     for (uint32_t m = 0; m < M; ++m) {
-        members_[m]->noteExternalRun(need[m], (uint64_t)nMcs, !isRes[m], members_[m]->lastColor());
+        members_[m]->noteExternalRun(need[m], (uint64_t)nMcs, !isResident_[m], members_[m]->lastColor());
         members_[m]->streamWait(done_);
     }
 }
@@ -193,6 +230,7 @@ float Batch::runTimed(int32_t nMcs)
 {
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
     for (Updater* u : members_) u->synchronize();
+    if (!built_) rebuild();
     cudaEvent_t a, b;
     cuda_check(cudaEventCreate(&a), "cudaEventCreate");
     cuda_check(cudaEventCreate(&b), "cudaEventCreate");

@@ -138,6 +138,14 @@ int bfm_populate_lattice(bfm_handle h) { BFM_CALL(h, h->u.populateLattice()); }
 int bfm_set_seed(bfm_handle h, uint64_t seed) { BFM_CALL(h, h->u.setDrawCounter(seed)); }
 int bfm_set_draw_callback(bfm_handle h, bfm_draw_fn fn, void* ctx) { BFM_CALL(h, h->u.setDrawCallback(fn, ctx)); }
 int bfm_set_mode(bfm_handle h, int mode) { BFM_CALL(h, h->u.setMode(mode)); }
+int bfm_set_representation(bfm_handle h, int r) { BFM_CALL(h, h->u.setRepresentation(r)); }
+int bfm_get_representation(bfm_handle h, int* out)
+{
+    BFM_CALL(h, {
+        if (!out) throw std::invalid_argument("[bfm_get_representation] null output");
+        *out = (int)h->u.codeMode();
+    });
+}
 int bfm_initialize(bfm_handle h) { BFM_CALL(h, h->u.initialize()); }
 int bfm_run(bfm_handle h, int32_t n) { BFM_CALL(h, h->u.runSimulationOnGPU(n)); }
 int bfm_run_async(bfm_handle h, int32_t n) { BFM_CALL(h, h->u.run(n)); }
@@ -272,6 +280,13 @@ int bfm_batch_run_timed(bfm_batch_handle b, int32_t n, float* ms)
     });
 }
 int bfm_batch_synchronize(bfm_batch_handle b) { BFM_CALL(b, b->b.synchronize()); }
+int bfm_batch_launch_count(bfm_batch_handle b, uint64_t* out)
+{
+    BFM_CALL(b, {
+        if (!out) throw std::invalid_argument("[bfm_batch_launch_count] null output");
+        *out = b->b.launches();
+    });
+}
 int bfm_batch_set_resident(bfm_batch_handle b, int on) { BFM_CALL(b, b->b.setResidentEnabled(on != 0)); }
 
 }  // extern "C"

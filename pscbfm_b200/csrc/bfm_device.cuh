@@ -22,6 +22,22 @@ namespace bfm {
 constexpr uint32_t kNoMark = 0xFFFFFFFFu;
 constexpr uint32_t kNoColor = 0xFFFFFFFFu;
 constexpr int kMaxConn = 16;
+// Move counters: stats[c * kStatSlots + s], c = 0 attempted, 1 tentative, 2 accepted; each CTA
+// adds its tally to slot blockIdx.x % kStatSlots, so no single address takes more than a few
+// dozen atomics per launch. Readers sum the slots.
+constexpr uint32_t kStatSlots = 64;
+constexpr size_t kStatBytes = 3 * kStatSlots * sizeof(unsigned long long);
+
+// Per-CTA tally: one shared-memory atomic per warp, one global atomic per CTA.
+__device__ __forceinline__ void tally_warp(bool pred, uint32_t* ctaTally)
+{
+    uint32_t const b = __ballot_sync(0xffffffffu, pred);
+    if ((threadIdx.x & 31u) == 0 && b) atomicAdd(ctaTally, (uint32_t)__popc(b));
+}
+__device__ __forceinline__ void tally_flush(uint32_t count, unsigned long long* stats, uint32_t which)
+{
+    if (count) atomicAdd(stats + which * kStatSlots + (blockIdx.x % kStatSlots), (unsigned long long)count);
+}
 
 struct SysDev {
     int32_t* x;
@@ -29,27 +45,55 @@ struct SysDev {
     int32_t* z;
     uint32_t const* nbr;
     uint8_t const* nnb;
-    uint8_t* flags;
-    uint32_t* tmark;                 // [2][npad]
+    uint8_t* flags;                  // [2][npad]; the gather kernels use the first npad
+    uint32_t* tmark;                 // [2][npad] (gather kernels)
     unsigned long long* lat;
     unsigned long long* tmp;         // [2][nwords]
     uint32_t const* brickTab;        // [nb0 + nb1 + nb2]
     uint32_t const* grp;             // [2 * nColors]: offset, size
     unsigned long long* stats;       // [4]: attempted, tentative, accepted, spare
+    // bond-code representation (codeMode != kCodeNone)
+    uint32_t* pk;                    // [npad] packed lattice coordinates x | y << 10 | z << 20 (masked)
+    void* code;                      // [npad] uint32 (3 slots) or uint64 (6 slots) bond codes
+    uint32_t const* nbrr;            // [maxc][npad] neighbour slot | reverse slot << 28
+    unsigned long long const* planeTab;   // [3][4][4][4][4] front-plane masks (see plane_table_fill)
+    uint8_t const* moveOk;           // [512] bit d: a bond with this index stays allowed after move d
+    uint32_t codeMode;               // kCodeNone, kCode32, kCode64
     uint32_t npad, nwords, maxc, nColors;
     uint32_t mask[3];                // box side - 1 (power-of-two box)
     uint32_t nb[3];                  // bricks per axis
+    uint32_t mb, hx, hy;             // brick_index parameters
     uint32_t forbid[16];             // bit i set <=> bond index i is forbidden
 };
 
+// Bond codes: field k (9 bits at 9k) of a monomer's code word is the bond index of
+// (neighbour k - monomer), i.e. the reference's table index (CRITICAL.cu:243-261) of that bond;
+// the count of fields sits above them. Valid only with symmetric neighbour lists, where the
+// reverse slot of every bond exists and bonded monomers never share a colour.
+constexpr uint32_t kCodeNone = 0, kCode32 = 1, kCode64 = 2;
+template <typename W>
+struct CodeWord;
+template <>
+struct CodeWord<uint32_t> {
+    static constexpr uint32_t kSlots = 3, kCountShift = 27;
+};
+template <>
+struct CodeWord<unsigned long long> {
+    static constexpr uint32_t kSlots = 6, kCountShift = 54;
+};
+constexpr uint32_t kSlotShift = 28;          // nbrr: reverse slot in the top 4 bits
+constexpr uint32_t kSlotMask = (1u << kSlotShift) - 1u;
+
 // One sub-step of one system inside a launch. color == kNoColor: the system idles.
 // prevColor: colour group whose temporary-lattice marks (parity ^ 1) are scrubbed in this
-// sub-step's perform phase (kNoColor: nothing to scrub).
+// sub-step (kNoColor: nothing to scrub). off/cnt and poff/pcnt: first slot and size of the
+// current and of the previous colour group (0 when absent).
 struct StepEntry {
     uint32_t color;
     uint32_t seed;
     uint32_t parity;
     uint32_t prevColor;
+    uint32_t off, cnt, poff, pcnt;
 };
 
 // Move-direction hash, src/pscbfm/CRITICAL.cu:2-11 (Jenkins' 6-shift 32-bit integer hash).
@@ -72,25 +116,120 @@ __device__ __forceinline__ uint32_t move_dir(uint32_t iLocal, uint32_t seed)
     return move_hash(move_hash(iLocal) ^ seed) % 6u;
 }
 
-// Position of value v (0..3) of axis a inside a brick word.
-__device__ __forceinline__ uint32_t brick_pos(uint32_t v, uint32_t a)
+// Position of value v (0..3) of axis a inside a brick word: bit = x + 4 y + 16 z.
+__host__ __device__ __forceinline__ uint32_t brick_pos(uint32_t v, uint32_t a)
 {
-    return ((v & 1u) | ((v & 2u) << 2)) << a;
+    return v << (2u * a);
 }
 
-__device__ __forceinline__ uint32_t brick_bit(uint32_t x, uint32_t y, uint32_t z)
+__host__ __device__ __forceinline__ uint32_t brick_bit(uint32_t x, uint32_t y, uint32_t z)
 {
-    return brick_pos(x & 3u, 0) | brick_pos(y & 3u, 1) | brick_pos(z & 3u, 2);
+    return (x & 3u) | ((y & 3u) << 2) | ((z & 3u) << 4);
 }
 
-// Mask of the cells with axis-a value in [lo, hi] (and the other two axes at 0).
+// Mask of the cells with axis-a value in [lo, hi] (and the other two axes at 0): a run of
+// hi-lo+1 ones with stride 4^a, shifted to lo.
 __device__ __forceinline__ unsigned long long range_mask(uint32_t lo, uint32_t hi, uint32_t a)
 {
-    unsigned long long m = 0;
-#pragma unroll
-    for (uint32_t v = 0; v < 4; ++v)
-        if (v >= lo && v <= hi) m |= 1ull << brick_pos(v, a);
-    return m;
+    uint32_t const n = hi - lo;   // 0..2
+    unsigned long long const rep = a == 0 ? (n == 0 ? 0x1ull : n == 1 ? 0x3ull : 0x7ull)
+                                 : a == 1 ? (n == 0 ? 0x1ull : n == 1 ? 0x11ull : 0x111ull)
+                                          : (n == 0 ? 0x1ull : n == 1 ? 0x10001ull : 0x100010001ull);
+    return rep << (lo << (2u * a));
+}
+
+// Spreads the low 8 bits of v to every third bit (published "Part1By2" bit-interleave masks).
+__host__ __device__ __forceinline__ uint32_t dilate3(uint32_t v)
+{
+    v &= 0xFFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+// Brick (word) index of brick coordinates (bx, by, bz): the low `mb` bits of the three
+// coordinates interleaved as a Z-curve, the remaining high bits (non-cubic boxes) appended in
+// x-fastest order; hx, hy are the high-part extents in x and y.
+__host__ __device__ __forceinline__ uint32_t brick_index(uint32_t bx, uint32_t by, uint32_t bz, uint32_t mb,
+                                                         uint32_t hx, uint32_t hy)
+{
+    uint32_t const lm = (1u << mb) - 1u;
+    uint32_t const lo = dilate3(bx & lm) | (dilate3(by & lm) << 1) | (dilate3(bz & lm) << 2);
+    uint32_t const hi = (bx >> mb) + hx * ((by >> mb) + hy * (bz >> mb));
+    return lo | (hi << (3u * mb));
+}
+
+// Host: brick_index parameters of a box with nb[a] bricks per axis (powers of two), and the
+// per-axis contributions to it (tab[0..nb0) for x, then y, then z; the index of a brick is the
+// sum of its three contributions). The table-driven kernels and the arithmetic ones agree.
+inline void brick_params(uint32_t const nb[3], uint32_t& mb, uint32_t& hx, uint32_t& hy)
+{
+    uint32_t lb[3];
+    for (int a = 0; a < 3; ++a) {
+        lb[a] = 0;
+        while ((1u << lb[a]) < nb[a]) ++lb[a];
+    }
+    mb = lb[0] < lb[1] ? (lb[0] < lb[2] ? lb[0] : lb[2]) : (lb[1] < lb[2] ? lb[1] : lb[2]);
+    hx = nb[0] >> mb;
+    hy = nb[1] >> mb;
+}
+
+inline void brick_tables_fill(uint32_t const nb[3], uint32_t* tab)
+{
+    uint32_t mb, hx, hy;
+    brick_params(nb, mb, hx, hy);
+    for (uint32_t b = 0; b < nb[0]; ++b) tab[b] = brick_index(b, 0, 0, mb, hx, hy);
+    for (uint32_t b = 0; b < nb[1]; ++b) tab[nb[0] + b] = brick_index(0, b, 0, mb, hx, hy);
+    for (uint32_t b = 0; b < nb[2]; ++b) tab[nb[0] + nb[1] + b] = brick_index(0, 0, b, mb, hx, hy);
+}
+
+// Host: masks of the front plane inside the (at most 2x2) bricks it touches. Entry
+// ((((a*4 + fo)*4 + lu)*4 + lv)*4 + k) for a move along axis a: fo = in-brick coordinate of the
+// plane along a, lu / lv = in-brick coordinate of the first of the three cells along the two other
+// axes u < v; k = 2*i + j selects the brick (i: u-brick 0 or 1, j: v-brick 0 or 1). A run that
+// starts at 2 or 3 spills into the next brick; a zero mask means that brick is not touched.
+inline void plane_table_fill(unsigned long long* t)
+{
+    auto run = [](uint32_t ax, uint32_t lo, uint32_t hi) {
+        unsigned long long m = 0;
+        for (uint32_t v = lo; v <= hi; ++v) m |= 1ull << brick_pos(v, ax);
+        return m;
+    };
+    for (uint32_t a = 0; a < 3; ++a) {
+        uint32_t const u = a == 0 ? 1u : 0u, v = a == 2 ? 1u : 2u;
+        for (uint32_t fo = 0; fo < 4; ++fo)
+            for (uint32_t lu = 0; lu < 4; ++lu)
+                for (uint32_t lv = 0; lv < 4; ++lv) {
+                    unsigned long long const mu0 = lu <= 1 ? run(u, lu, lu + 2) : run(u, lu, 3);
+                    unsigned long long const mu1 = lu <= 1 ? 0ull : run(u, 0, lu - 2);
+                    unsigned long long const mv0 = lv <= 1 ? run(v, lv, lv + 2) : run(v, lv, 3);
+                    unsigned long long const mv1 = lv <= 1 ? 0ull : run(v, 0, lv - 2);
+                    uint32_t const sh = brick_pos(fo, a);
+                    unsigned long long* e = t + ((((a * 4 + fo) * 4 + lu) * 4 + lv) * 4);
+                    e[0] = (mu0 * mv0) << sh;
+                    e[1] = (mu0 * mv1) << sh;
+                    e[2] = (mu1 * mv0) << sh;
+                    e[3] = (mu1 * mv1) << sh;
+                }
+    }
+}
+
+// Host: bit d of ok[idx] is set when the bond with table index idx (neighbour - monomer, every
+// component mod 8) is still allowed after the monomer moves along direction d.
+inline void move_ok_fill(bool const* forbidden512, uint8_t* ok)
+{
+    for (uint32_t idx = 0; idx < 512; ++idx) {
+        uint8_t m = 0;
+        for (uint32_t d = 0; d < 6; ++d) {
+            uint32_t const a = d >> 1;
+            uint32_t const c = (idx >> (3 * a)) & 7u;
+            uint32_t const nc = (c + ((d & 1u) ? 7u : 1u)) & 7u;   // neighbour - (monomer + d)
+            uint32_t const j = (idx & ~(7u << (3 * a))) | (nc << (3 * a));
+            if (!forbidden512[j]) m |= (uint8_t)(1u << d);
+        }
+        ok[idx] = m;
+    }
 }
 
 // Bond-set lookup, CRITICAL.cu:243-261 + :350: index of (dx,dy,dz) with every component masked
@@ -103,6 +242,50 @@ __device__ __forceinline__ uint32_t bond_index(int32_t dx, int32_t dy, int32_t d
 __device__ __forceinline__ bool forbidden(uint32_t const* tbl, uint32_t idx)
 {
     return (tbl[idx >> 5] >> (idx & 31u)) & 1u;
+}
+
+// Shifts component `axis` of every bond field of a code word by `delta` (mod 8). The monomer's
+// own bonds change by -d when it moves by d, the reverse bond of a neighbour by +d.
+template <typename W>
+__device__ __forceinline__ W code_shift(W code, uint32_t axis, int32_t delta)
+{
+    uint32_t const n = uint32_t(code >> CodeWord<W>::kCountShift) & 7u;
+    W out = code;
+#pragma unroll
+    for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k) {
+        if (k < n) {
+            uint32_t const sh = 9u * k + 3u * axis;
+            uint32_t const c = uint32_t(code >> sh) & 7u;
+            uint32_t const nc = uint32_t(int32_t(c) + delta) & 7u;
+            out ^= W(c ^ nc) << sh;
+        }
+    }
+    return out;
+}
+
+// True if every bond of the code word stays in the allowed set after a move along dir.
+template <typename W>
+__device__ __forceinline__ bool code_bonds_ok(W code, uint32_t dir, uint32_t const* tbl)
+{
+    uint32_t const n = uint32_t(code >> CodeWord<W>::kCountShift) & 7u;
+    uint32_t const axis = dir >> 1;
+    int32_t const delta = (dir & 1u) ? -1 : 1;   // neighbour - (self + d)
+    bool ok = true;
+#pragma unroll
+    for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k) {
+        if (k < n) {
+            uint32_t f = uint32_t(code >> (9u * k)) & 511u;
+            uint32_t const c = (f >> (3u * axis)) & 7u;
+            f ^= ((c ^ (uint32_t(int32_t(c) + delta) & 7u)) << (3u * axis));
+            ok = ok && !forbidden(tbl, f);
+        }
+    }
+    return ok;
+}
+
+__device__ __forceinline__ uint32_t pack_coord(uint32_t x, uint32_t y, uint32_t z)
+{
+    return x | (y << 10) | (z << 20);
 }
 
 // Word index of the brick containing cell (x,y,z) (coordinates already masked into the box).

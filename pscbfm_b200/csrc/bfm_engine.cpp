@@ -44,27 +44,12 @@ size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 // axes that run out of bits drop out of the rotation).
 std::vector<uint32_t> brick_tables(uint32_t const nb[3])
 {
-    uint32_t lb[3] = {ilog2(nb[0]), ilog2(nb[1]), ilog2(nb[2])};
-    uint32_t pos[3][32];
-    uint32_t next = 0;
-    for (uint32_t k = 0; k < 32; ++k)
-        for (int a = 0; a < 3; ++a)
-            if (k < lb[a]) pos[a][k] = next++;
     std::vector<uint32_t> tab(nb[0] + nb[1] + nb[2]);
-    uint32_t base = 0;
-    for (int a = 0; a < 3; ++a) {
-        for (uint32_t b = 0; b < nb[a]; ++b) {
-            uint32_t w = 0;
-            for (uint32_t k = 0; k < lb[a]; ++k)
-                if ((b >> k) & 1u) w |= 1u << pos[a][k];
-            tab[base + b] = w;
-        }
-        base += nb[a];
-    }
+    brick_tables_fill(nb, tab.data());
     return tab;
 }
 
-inline uint32_t host_brick_pos(uint32_t v, uint32_t a) { return ((v & 1u) | ((v & 2u) << 2)) << a; }
+inline uint32_t host_brick_pos(uint32_t v, uint32_t a) { return brick_pos(v, a); }
 
 }  // namespace
 
@@ -311,6 +296,27 @@ void Updater::initialize()
         hgrp[2 * c] = grpOff_[c];
         hgrp[2 * c + 1] = grpSize_[c];
     }
+    // bond-code representation: symmetric neighbour lists (every i->j has a j->i partner, the
+    // m-th occurrence of j in i's list pairing with the m-th occurrence of i in j's) and <= 6
+    // bonds per monomer
+    codeMode_ = kCodeNone;
+    if (repr_ == kReprAuto && maxc_ <= 6) {
+        bool sym = true;
+        for (uint32_t i = 0; i < n_ && sym; ++i)
+            for (uint32_t k = 0; k < nbrCnt_[i] && sym; ++k) {
+                uint32_t const j = nbrIds_[(size_t)i * kMaxConn + k];
+                uint32_t occ = 0, want = 0, seen = 0;
+                for (uint32_t q = 0; q < k; ++q) occ += nbrIds_[(size_t)i * kMaxConn + q] == j ? 1 : 0;
+                for (uint32_t q = 0; q < nbrCnt_[j]; ++q) want += nbrIds_[(size_t)j * kMaxConn + q] == i ? 1 : 0;
+                for (uint32_t q = 0; q < nbrCnt_[i]; ++q) seen += nbrIds_[(size_t)i * kMaxConn + q] == j ? 1 : 0;
+                sym = want == seen && occ < want;
+            }
+        if (sym) codeMode_ = maxc_ <= 3 ? kCode32 : kCode64;
+    }
+    std::vector<uint32_t> hpk;
+    std::vector<uint8_t> hcode;
+    std::vector<uint32_t> hnbrr;
+    size_t const codeBytes = codeMode_ == kCode64 ? 8 : 4;
 
     // one arena for every device array of this system
     size_t off = 0;
@@ -320,10 +326,12 @@ void Updater::initialize()
         return o;
     };
     size_t const oX = take(4ull * npad_), oY = take(4ull * npad_), oZ = take(4ull * npad_);
-    size_t const oNbr = take(4ull * maxc_ * npad_), oNnb = take(npad_), oFlags = take(npad_);
+    size_t const oNbr = take(4ull * maxc_ * npad_), oNnb = take(npad_), oFlags = take(2ull * npad_);
     size_t const oMark = take(8ull * npad_), oLat = take(8ull * nwords), oTmp = take(16ull * nwords);
-    size_t const oTab = take(4ull * tab.size()), oGrp = take(4ull * hgrp.size()), oStats = take(32);
+    size_t const oTab = take(4ull * tab.size()), oGrp = take(4ull * hgrp.size()), oStats = take(kStatBytes);
     size_t const oDesc = take(sizeof(SysDev)), oSteps = take(sizeof(StepEntry) * kStepCap), oList = take(4);
+    size_t const oPk = take(4ull * npad_), oCode = take(codeBytes * npad_), oNbrr = take(4ull * maxc_ * npad_);
+    size_t const oPlane = take(8ull * 768), oMoveOk = take(512);
     Device d;
     d.bytes = off;
     cuda_check(cudaMalloc(&d.arena, off), "cudaMalloc(system arena)");
@@ -350,6 +358,7 @@ void Updater::initialize()
         h.mask[a] = box_[a] - 1;
         h.nb[a] = nb[a];
     }
+    brick_params(nb, h.mb, h.hx, h.hy);
     std::memset(h.forbid, 0, sizeof(h.forbid));
     for (uint32_t i = 0; i < 512; ++i)
         if (forbidden_[i]) h.forbid[i >> 5] |= 1u << (i & 31);
@@ -357,8 +366,29 @@ void Updater::initialize()
     dev_.dSteps = reinterpret_cast<StepEntry*>(base + oSteps);
     dev_.stepCap = kStepCap;
     dev_.dList = reinterpret_cast<uint32_t*>(base + oList);
+    h.pk = reinterpret_cast<uint32_t*>(base + oPk);
+    h.code = base + oCode;
+    h.nbrr = reinterpret_cast<uint32_t*>(base + oNbrr);
+    h.planeTab = reinterpret_cast<unsigned long long*>(base + oPlane);
+    h.moveOk = reinterpret_cast<uint8_t*>(base + oMoveOk);
+    h.codeMode = codeMode_;
 
     cudaStream_t s = stream_;
+    std::vector<unsigned long long> hplane(768);
+    plane_table_fill(hplane.data());
+    std::vector<uint8_t> hmove(512);
+    move_ok_fill(forbidden_, hmove.data());
+    cuda_check(cudaMemcpyAsync(const_cast<unsigned long long*>(h.planeTab), hplane.data(), 8ull * 768,
+                               cudaMemcpyHostToDevice, s), "upload plane table");
+    cuda_check(cudaMemcpyAsync(const_cast<uint8_t*>(h.moveOk), hmove.data(), 512, cudaMemcpyHostToDevice, s),
+               "upload move table");
+    if (codeMode_ != kCodeNone) {
+        hostCodes(hpk, hcode, hnbrr);
+        cuda_check(cudaMemcpyAsync(h.pk, hpk.data(), 4ull * npad_, cudaMemcpyHostToDevice, s), "upload pk");
+        cuda_check(cudaMemcpyAsync(h.code, hcode.data(), hcode.size(), cudaMemcpyHostToDevice, s), "upload codes");
+        cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(h.nbrr), hnbrr.data(), 4ull * hnbrr.size(),
+                                   cudaMemcpyHostToDevice, s), "upload nbrr");
+    }
     cuda_check(cudaMemcpyAsync(h.x, hx.data(), 4ull * npad_, cudaMemcpyHostToDevice, s), "upload x");
     cuda_check(cudaMemcpyAsync(h.y, hy.data(), 4ull * npad_, cudaMemcpyHostToDevice, s), "upload y");
     cuda_check(cudaMemcpyAsync(h.z, hz.data(), 4ull * npad_, cudaMemcpyHostToDevice, s), "upload z");
@@ -366,7 +396,7 @@ void Updater::initialize()
                                cudaMemcpyHostToDevice, s), "upload nbr");
     cuda_check(cudaMemcpyAsync(const_cast<uint8_t*>(h.nnb), hnnb.data(), npad_, cudaMemcpyHostToDevice, s),
                "upload nnb");
-    cuda_check(cudaMemsetAsync(h.flags, 0, npad_, s), "memset flags");
+    cuda_check(cudaMemsetAsync(h.flags, 0, 2ull * npad_, s), "memset flags");
     cuda_check(cudaMemsetAsync(h.tmark, 0xFF, 8ull * npad_, s), "memset tmark");
     cuda_check(cudaMemcpyAsync(h.lat, hlat.data(), 8ull * nwords, cudaMemcpyHostToDevice, s), "upload lattice");
     cuda_check(cudaMemsetAsync(h.tmp, 0, 16ull * nwords, s), "memset tmp");
@@ -374,7 +404,7 @@ void Updater::initialize()
                                cudaMemcpyHostToDevice, s), "upload brick table");
     cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(h.grp), hgrp.data(), 4ull * hgrp.size(),
                                cudaMemcpyHostToDevice, s), "upload groups");
-    cuda_check(cudaMemsetAsync(h.stats, 0, 32, s), "memset stats");
+    cuda_check(cudaMemsetAsync(h.stats, 0, kStatBytes, s), "memset stats");
     cuda_check(cudaMemcpyAsync(dev_.dDesc, &h, sizeof(SysDev), cudaMemcpyHostToDevice, s), "upload descriptor");
     cuda_check(cudaMemsetAsync(dev_.dList, 0, 4, s), "memset list");
     if (!hSteps_) {
@@ -389,11 +419,81 @@ void Updater::initialize()
     hostStale_ = false;
 }
 
+void Updater::hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, std::vector<uint32_t>& nbrr) const
+{
+    // packed lattice coordinates, bond-code words and neighbour slots with their reverse slot,
+    // all in sorted order, from the host positions
+    pk.assign(npad_, 0u);
+    size_t const w = codeMode_ == kCode64 ? 8 : 4;
+    uint32_t const countShift = codeMode_ == kCode64 ? 54 : 27;
+    code.assign(w * npad_, 0);
+    nbrr.assign((size_t)maxc_ * npad_, 0u);
+    for (uint32_t i = 0; i < n_; ++i) {
+        uint32_t const s = oldToNew_[i];
+        int32_t const* p = &xyz_[3 * (size_t)i];
+        pk[s] = (uint32_t(p[0]) & (box_[0] - 1)) | ((uint32_t(p[1]) & (box_[1] - 1)) << 10) |
+                ((uint32_t(p[2]) & (box_[2] - 1)) << 20);
+        uint64_t c = (uint64_t)nbrCnt_[i] << countShift;
+        for (uint32_t k = 0; k < nbrCnt_[i]; ++k) {
+            uint32_t const j = nbrIds_[(size_t)i * kMaxConn + k];
+            int32_t const* q = &xyz_[3 * (size_t)j];
+            uint64_t const f = (uint32_t(q[0] - p[0]) & 7u) | ((uint32_t(q[1] - p[1]) & 7u) << 3) |
+                               ((uint32_t(q[2] - p[2]) & 7u) << 6);
+            c |= f << (9 * k);
+            // reverse slot: the occurrence of i in j's list with the same rank as this j in i's
+            uint32_t occ = 0;
+            for (uint32_t m = 0; m < k; ++m) occ += nbrIds_[(size_t)i * kMaxConn + m] == j ? 1 : 0;
+            uint32_t r = 0;
+            for (uint32_t m = 0; m < nbrCnt_[j]; ++m)
+                if (nbrIds_[(size_t)j * kMaxConn + m] == i) {
+                    if (occ == 0) {
+                        r = m;
+                        break;
+                    }
+                    --occ;
+                }
+            nbrr[(size_t)k * npad_ + s] = oldToNew_[j] | (r << kSlotShift);
+        }
+        std::memcpy(&code[w * s], &c, w);
+    }
+}
+
+void Updater::setRepresentation(int r)
+{
+    if (r != kReprAuto && r != kReprGather) throw std::invalid_argument("[setRepresentation] unknown representation");
+    if (initialized()) throw std::runtime_error("[setRepresentation] must be chosen before initialize");
+    repr_ = r;
+}
+
+uint32_t Updater::gridTiles() const
+{
+    uint32_t const span = codeMode_ == kCodeNone ? kGridBlock : kBcTileSpan;
+    return std::max((maxGroup_ + span - 1) / span, 1u);
+}
+
+cudaError_t Updater::launchCheck(StepEntry const* e, cudaStream_t s) const
+{
+    if (codeMode_ == kCodeNone) return launch_check(dev_.dDesc, nullptr, gridTiles(), kGridBlock, e, s);
+    return launch_check_bc(dev_.h, dev_.dDesc, nullptr, gridTiles(), e, codeMode_, s);
+}
+
+cudaError_t Updater::launchPerform(StepEntry const* e, cudaStream_t s) const
+{
+    if (codeMode_ == kCodeNone) return launch_perform(dev_.dDesc, nullptr, gridTiles(), kGridBlock, e, s);
+    return launch_perform_bc(dev_.h, dev_.dDesc, nullptr, gridTiles(), e, codeMode_, s);
+}
+
+size_t Updater::residentSmem() const
+{
+    uint32_t const ntab = dev_.h.nb[0] + dev_.h.nb[1] + dev_.h.nb[2];
+    return codeMode_ == kCodeNone ? resident_smem_bytes(dev_.h.nwords, ntab)
+                                  : resident_bc_smem_bytes(dev_.h.nwords, ntab, npad_, maxGroup_, codeMode_);
+}
+
 bool Updater::residentEligible() const
 {
     if (!initialized()) return false;
-    uint32_t const ntab = dev_.h.nb[0] + dev_.h.nb[1] + dev_.h.nb[2];
-    return resident_smem_bytes(dev_.h.nwords, ntab) <= kResidentMaxSmem && maxGroup_ <= 16u * kResidentBlock;
+    return residentSmem() <= kResidentMaxSmem && maxGroup_ <= 16u * kResidentBlock;
 }
 
 // ============================================================================ run
@@ -414,6 +514,10 @@ StepEntry Updater::nextStep()
     e.seed = d1;
     e.parity = (uint32_t)(subStep_ & 1u);
     e.prevColor = lastColor_;
+    e.off = grpOff_[e.color];
+    e.cnt = grpSize_[e.color];
+    e.poff = lastColor_ == kNoColor ? 0u : grpOff_[lastColor_];
+    e.pcnt = lastColor_ == kNoColor ? 0u : grpSize_[lastColor_];
     lastColor_ = e.color;
     ++subStep_;
     return e;
@@ -429,11 +533,12 @@ void Updater::scrubPending(cudaStream_t s)
     if (lastColor_ == kNoColor) return;
     // a perform launch with no current colour only zeroes the previous sub-step's marks
     cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
-    hSteps_[0] = StepEntry{kNoColor, 0u, (uint32_t)(subStep_ & 1u), lastColor_};
+    hSteps_[0] = StepEntry{kNoColor, 0u, (uint32_t)(subStep_ & 1u), lastColor_, 0u, 0u, grpOff_[lastColor_],
+                           grpSize_[lastColor_]};
     cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry), cudaMemcpyHostToDevice, s), "steps H2D");
     cuda_check(cudaEventRecord(stepsFree_, s), "event");
-    uint32_t const tiles = (maxGroup_ + kGridBlock - 1) / kGridBlock;
-    cuda_check(launch_perform(dev_.dDesc, nullptr, std::max(tiles, 1u), kGridBlock, dev_.dSteps, s), "scrub");
+    // gather kernels scrub in the perform, bond-code kernels in the check
+    cuda_check(codeMode_ == kCodeNone ? launchPerform(dev_.dSteps, s) : launchCheck(dev_.dSteps, s), "scrub");
     ++launches_;
     lastColor_ = kNoColor;
 }
@@ -448,7 +553,6 @@ void Updater::noteExternalRun(uint64_t subSteps, uint64_t mcs, bool pendingMarks
 
 void Updater::enqueueLaunch(uint32_t nSteps)
 {
-    uint32_t const tiles = std::max((maxGroup_ + kGridBlock - 1) / kGridBlock, 1u);
     for (uint32_t done = 0; done < nSteps;) {
         uint32_t const chunk = std::min(nSteps - done, hStepCap_);
         cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
@@ -457,15 +561,15 @@ void Updater::enqueueLaunch(uint32_t nSteps)
                    "steps H2D");
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         for (uint32_t t = 0; t < chunk; ++t) {
-            cuda_check(launch_check(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_), "check");
-            cuda_check(launch_perform(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_), "perform");
+            cuda_check(launchCheck(dev_.dSteps + t, stream_), "check");
+            cuda_check(launchPerform(dev_.dSteps + t, stream_), "perform");
         }
         launches_ += 2ull * chunk;
         done += chunk;
     }
 }
 
-cudaGraphExec_t Updater::graphFor(uint32_t nSteps, uint32_t tiles)
+cudaGraphExec_t Updater::graphFor(uint32_t nSteps)
 {
     for (auto const& g : graphs_)
         if (g.first == nSteps) return g.second;
@@ -473,8 +577,8 @@ cudaGraphExec_t Updater::graphFor(uint32_t nSteps, uint32_t tiles)
     cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t err = cudaSuccess;
     for (uint32_t t = 0; t < nSteps && err == cudaSuccess; ++t) {
-        err = launch_check(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_);
-        if (err == cudaSuccess) err = launch_perform(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_);
+        err = launchCheck(dev_.dSteps + t, stream_);
+        if (err == cudaSuccess) err = launchPerform(dev_.dSteps + t, stream_);
     }
     cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
     cuda_check(err, "capture launches");
@@ -493,10 +597,9 @@ void Updater::enqueueGraph(uint32_t nSteps)
     // graph of its own length, captured once and kept
     uint32_t const nC = (uint32_t)grpSize_.size();
     uint32_t const G = std::min(kGraphMcs * nC, hStepCap_);
-    uint32_t const tiles = std::max((maxGroup_ + kGridBlock - 1) / kGridBlock, 1u);
     for (uint32_t done = 0; done < nSteps;) {
         uint32_t const chunk = std::min(G, nSteps - done);
-        cudaGraphExec_t const exec = graphFor(chunk, tiles);
+        cudaGraphExec_t const exec = graphFor(chunk);
         cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
         fillSteps(chunk, hSteps_, false);
         cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
@@ -533,7 +636,6 @@ void Updater::timeKernels(int32_t nMcs, double out[4])
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
     scrubPending(stream_);
     uint32_t const nSteps = (uint32_t)nMcs * (uint32_t)grpSize_.size();
-    uint32_t const tiles = std::max((maxGroup_ + kGridBlock - 1) / kGridBlock, 1u);
     std::vector<cudaEvent_t> ev(3);
     for (auto& e : ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
     double check = 0, perform = 0;
@@ -547,9 +649,9 @@ void Updater::timeKernels(int32_t nMcs, double out[4])
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         for (uint32_t t = 0; t < chunk; ++t) {
             cuda_check(cudaEventRecord(ev[0], stream_), "event");
-            cuda_check(launch_check(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_), "check");
+            cuda_check(launchCheck(dev_.dSteps + t, stream_), "check");
             cuda_check(cudaEventRecord(ev[1], stream_), "event");
-            cuda_check(launch_perform(dev_.dDesc, nullptr, tiles, kGridBlock, dev_.dSteps + t, stream_), "perform");
+            cuda_check(launchPerform(dev_.dSteps + t, stream_), "perform");
             cuda_check(cudaEventRecord(ev[2], stream_), "event");
             cuda_check(cudaEventSynchronize(ev[2]), "timed kernels");
             float a = 0, b = 0;
@@ -574,8 +676,7 @@ void Updater::timeKernels(int32_t nMcs, double out[4])
 void Updater::enqueueResident(uint32_t nSteps)
 {
     scrubPending(stream_);
-    uint32_t const ntab = dev_.h.nb[0] + dev_.h.nb[1] + dev_.h.nb[2];
-    size_t const smem = resident_smem_bytes(dev_.h.nwords, ntab);
+    size_t const smem = residentSmem();
     uint32_t per = 1;
     while (per * kResidentBlock < maxGroup_) per *= 2;
     for (uint32_t done = 0; done < nSteps;) {
@@ -585,7 +686,11 @@ void Updater::enqueueResident(uint32_t nSteps)
         cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
                    "steps H2D");
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
-        cuda_check(launch_resident(dev_.dDesc, dev_.dList, 1, per, dev_.dSteps, 1, chunk, smem, stream_), "resident");
+        cuda_check(codeMode_ == kCodeNone
+                       ? launch_resident(dev_.dDesc, dev_.dList, 1, per, dev_.dSteps, 1, chunk, smem, stream_)
+                       : launch_resident_bc(dev_.dDesc, dev_.dList, 1, per, dev_.dSteps, 1, chunk, smem, codeMode_,
+                                            stream_),
+                   "resident");
         ++launches_;
         done += chunk;
     }
@@ -683,6 +788,14 @@ void Updater::setCoordinates(int32_t const* xyz, uint32_t n)
     cuda_check(cudaMemcpyAsync(dev_.h.z, hz.data(), 4ull * npad_, cudaMemcpyHostToDevice, stream_), "upload z");
     cuda_check(cudaMemsetAsync(dev_.h.lat, 0, 8ull * dev_.h.nwords, stream_), "clear lattice");
     cuda_check(launch_build_lattice(dev_.dDesc, npad_, stream_), "build lattice");
+    std::vector<uint32_t> hpk, hnbrr;
+    std::vector<uint8_t> hcode;
+    if (codeMode_ != kCodeNone) {
+        hostCodes(hpk, hcode, hnbrr);
+        cuda_check(cudaMemcpyAsync(dev_.h.pk, hpk.data(), 4ull * npad_, cudaMemcpyHostToDevice, stream_), "upload pk");
+        cuda_check(cudaMemcpyAsync(dev_.h.code, hcode.data(), hcode.size(), cudaMemcpyHostToDevice, stream_),
+                   "upload codes");
+    }
     cuda_check(cudaStreamSynchronize(stream_), "setCoordinates");
 }
 
@@ -701,12 +814,13 @@ std::vector<uint32_t> Updater::groupSizes() const
 void Updater::stats(uint64_t out[4])
 {
     requireInit("stats");
-    unsigned long long h[4];
-    cuda_check(cudaMemcpyAsync(h, dev_.h.stats, 32, cudaMemcpyDeviceToHost, stream_), "stats");
+    unsigned long long slots[3 * kStatSlots];
+    cuda_check(cudaMemcpyAsync(slots, dev_.h.stats, kStatBytes, cudaMemcpyDeviceToHost, stream_), "stats");
     cuda_check(cudaStreamSynchronize(stream_), "stats");
-    out[0] = h[0];
-    out[1] = h[1];
-    out[2] = h[2];
+    for (uint32_t c = 0; c < 3; ++c) {
+        out[c] = 0;
+        for (uint32_t s = 0; s < kStatSlots; ++s) out[c] += slots[c * kStatSlots + s];
+    }
     out[3] = mcsDone_;
 }
 
@@ -748,6 +862,33 @@ void Updater::validate()
                 throw std::runtime_error(m.str());
             }
         }
+    // device-side consistency: the occupancy lattice, and in the bond-code representation the
+    // packed coordinates and bond codes, must equal what the positions imply
+    if (initialized()) {
+        synchronize();
+        std::vector<unsigned long long> lat(dev_.h.nwords);
+        cuda_check(cudaMemcpy(lat.data(), dev_.h.lat, 8ull * lat.size(), cudaMemcpyDeviceToHost), "download lattice");
+        std::vector<uint32_t> tab = brick_tables(dev_.h.nb);
+        std::vector<unsigned long long> want(dev_.h.nwords, 0ull);
+        for (uint32_t i = 0; i < n_; ++i) {
+            uint32_t const mx = uint32_t(xyz_[3 * (size_t)i]) & (box_[0] - 1);
+            uint32_t const my = uint32_t(xyz_[3 * (size_t)i + 1]) & (box_[1] - 1);
+            uint32_t const mz = uint32_t(xyz_[3 * (size_t)i + 2]) & (box_[2] - 1);
+            uint32_t const w = tab[mx >> 2] + tab[dev_.h.nb[0] + (my >> 2)] + tab[dev_.h.nb[0] + dev_.h.nb[1] + (mz >> 2)];
+            want[w] |= 1ull << (host_brick_pos(mx & 3, 0) | host_brick_pos(my & 3, 1) | host_brick_pos(mz & 3, 2));
+        }
+        if (lat != want) throw std::runtime_error("[checkSystem] device occupancy lattice disagrees with the positions");
+        if (codeMode_ != kCodeNone) {
+            std::vector<uint32_t> hpk, hnbrr, dpk(npad_);
+            std::vector<uint8_t> hcode, dcode;
+            hostCodes(hpk, hcode, hnbrr);
+            dcode.resize(hcode.size());
+            cuda_check(cudaMemcpy(dpk.data(), dev_.h.pk, 4ull * npad_, cudaMemcpyDeviceToHost), "download pk");
+            cuda_check(cudaMemcpy(dcode.data(), dev_.h.code, dcode.size(), cudaMemcpyDeviceToHost), "download codes");
+            if (dpk != hpk) throw std::runtime_error("[checkSystem] packed coordinates disagree with the positions");
+            if (dcode != hcode) throw std::runtime_error("[checkSystem] bond codes disagree with the positions");
+        }
+    }
 }
 
 // ============================================================================ teardown

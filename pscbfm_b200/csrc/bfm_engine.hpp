@@ -165,7 +165,21 @@ private:
     std::vector<std::pair<uint32_t, cudaGraphExec_t>> graphs_;   // captured chunk length -> graph
     cudaEvent_t stepsFree_ = nullptr;          // host staging may be rewritten after this event
     uint64_t launches_ = 0;
-    cudaGraphExec_t graphFor(uint32_t nSteps, uint32_t tiles);
+    int repr_ = 0;
+    uint32_t codeMode_ = kCodeNone;
+    cudaGraphExec_t graphFor(uint32_t nSteps);
+    void hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, std::vector<uint32_t>& nbrr) const;
+
+public:
+    // representation of the bonds on the device: auto (bond codes when the neighbour lists are
+    // symmetric and <= 6 per monomer, else neighbour positions) or forced neighbour positions
+    static constexpr int kReprAuto = 0, kReprGather = 1;
+    void setRepresentation(int r);
+    uint32_t codeMode() const { return codeMode_; }
+    uint32_t gridTiles() const;                               // CTAs of one grid-phase launch
+    cudaError_t launchCheck(StepEntry const* e, cudaStream_t s) const;
+    cudaError_t launchPerform(StepEntry const* e, cudaStream_t s) const;
+    size_t residentSmem() const;
 };
 
 // A set of initialised updaters on one GPU advanced together: systems that fit one CTA run in the
@@ -187,30 +201,43 @@ public:
         residentOn_ = on;
     }
     cudaStream_t stream() const { return stream_; }
-    uint32_t gridTiles() const { return (uint32_t)tiles_.size(); }
-    uint32_t residentCount() const { return (uint32_t)resident_.size(); }
+    uint32_t residentCount() const;
+    uint64_t launches() const { return launches_; }
 
 private:
+    // members of one representation (codeMode) on one path
+    struct GridGroup {
+        uint32_t codeMode;
+        std::vector<TileRef> tiles;
+        TileRef* dTiles = nullptr;
+    };
+    struct ResidentGroup {
+        uint32_t codeMode;
+        std::vector<uint32_t> members;
+        uint32_t* dList = nullptr;
+        uint32_t perThread = 1;
+        size_t smem = 0;
+    };
     void rebuild();
+    cudaError_t launchGrid(uint32_t t, uint32_t M);
     int gpu_;
     std::vector<Updater*> members_;
-    std::vector<uint32_t> resident_, grid_;    // member indices per path
-    std::vector<TileRef> tiles_;
+    std::vector<char> isResident_;
+    std::vector<GridGroup> grid_;
+    std::vector<ResidentGroup> resident_;
     bool residentOn_ = true;
     bool built_ = false;
     cudaStream_t stream_ = nullptr, stream2_ = nullptr;
     cudaEvent_t join_ = nullptr, fork_ = nullptr;
+    void* arena_ = nullptr;                    // descriptors, tiles, lists, step entries
     SysDev* dSys_ = nullptr;                   // descriptors of all members
-    TileRef* dTiles_ = nullptr;
-    uint32_t* dResList_ = nullptr;
     StepEntry* dSteps_ = nullptr;              // [cap][members]
     StepEntry* hSteps_ = nullptr;
     size_t stepCap_ = 0;
-    uint32_t residentPerThread_ = 1;
-    size_t residentSmem_ = 0;
     cudaEvent_t stepsFree_ = nullptr;
     cudaEvent_t done_ = nullptr;
     cudaGraphExec_t graph_ = nullptr;
+    uint64_t launches_ = 0;
 };
 
 }  // namespace bfm

@@ -44,12 +44,6 @@ __device__ __forceinline__ void load_sys(SysDev& dst, SysDev const* src)
     for (uint32_t w = threadIdx.x; w < sizeof(SysDev) / 4; w += blockDim.x) d[w] = s[w];
 }
 
-__device__ __forceinline__ void warp_count(bool pred, unsigned long long* counter)
-{
-    uint32_t const b = __ballot_sync(0xffffffffu, pred);
-    if ((threadIdx.x & 31u) == 0 && b) atomicAdd(counter, (unsigned long long)__popc(b));
-}
-
 }  // namespace
 
 // ------------------------------------------------------------------------ grid phase: check
@@ -59,10 +53,12 @@ __global__ void __launch_bounds__(kGridBlock) k_check(SysDev const* __restrict__
                                                       StepEntry const* __restrict__ steps)
 {
     __shared__ SysDev S;
+    __shared__ uint32_t tally;
     TileRef const tr = tiles ? tiles[blockIdx.x] : TileRef{0u, blockIdx.x * tileSpan};
     StepEntry const st = steps[tr.sys];
     if (st.color == kNoColor) return;
     load_sys(S, sysv + tr.sys);
+    if (threadIdx.x == 0) tally = 0;
     __syncthreads();
 
     uint32_t const off = S.grp[2 * st.color], cnt = S.grp[2 * st.color + 1];
@@ -103,9 +99,13 @@ __global__ void __launch_bounds__(kGridBlock) k_check(SysDev const* __restrict__
             S.flags[g] = f;
             markCur[g] = mark;
         }
-        warp_count(ok, S.stats + 1);
+        tally_warp(ok, &tally);
     }
-    if (threadIdx.x == 0 && tr.start == 0) atomicAdd(S.stats + 0, (unsigned long long)cnt);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        tally_flush(tally, S.stats, 1);
+        if (tr.start == 0) tally_flush(cnt, S.stats, 0);
+    }
 }
 
 // ------------------------------------------------------------------------ grid phase: perform
@@ -115,10 +115,12 @@ __global__ void __launch_bounds__(kGridBlock) k_perform(SysDev const* __restrict
                                                         StepEntry const* __restrict__ steps)
 {
     __shared__ SysDev S;
+    __shared__ uint32_t tally;
     TileRef const tr = tiles ? tiles[blockIdx.x] : TileRef{0u, blockIdx.x * tileSpan};
     StepEntry const st = steps[tr.sys];
     if (st.color == kNoColor && st.prevColor == kNoColor) return;
     load_sys(S, sysv + tr.sys);
+    if (threadIdx.x == 0) tally = 0;
     __syncthreads();
 
     // scrub the marks of the previous sub-step of this system (other parity)
@@ -172,8 +174,10 @@ __global__ void __launch_bounds__(kGridBlock) k_perform(SysDev const* __restrict
                 }
             }
         }
-        warp_count(moved, S.stats + 2);
+        tally_warp(moved, &tally);
     }
+    __syncthreads();
+    if (threadIdx.x == 0) tally_flush(tally, S.stats, 2);
 }
 
 // ------------------------------------------------------------------------ resident (1 CTA / system)
@@ -286,10 +290,10 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident(SysDev const* __
     uint32_t tsum = __reduce_add_sync(0xffffffffu, nTent);
     uint32_t asum = __reduce_add_sync(0xffffffffu, nAcc);
     if ((threadIdx.x & 31u) == 0) {
-        atomicAdd(S.stats + 1, (unsigned long long)tsum);
-        atomicAdd(S.stats + 2, (unsigned long long)asum);
+        tally_flush(tsum, S.stats, 1);
+        tally_flush(asum, S.stats, 2);
     }
-    if (threadIdx.x == 0) atomicAdd(S.stats + 0, nAtt);
+    if (threadIdx.x == 0 && nAtt) atomicAdd(S.stats + (blockIdx.x % kStatSlots), nAtt);
 }
 
 // ------------------------------------------------------------------------ lattice build

@@ -35,6 +35,22 @@ size_t resident_smem_bytes(uint32_t nwords, uint32_t ntab);
 cudaError_t launch_resident(SysDev const* dSys, uint32_t const* dList, uint32_t nCta, uint32_t perThread,
                             StepEntry const* dSteps, uint32_t nSys, uint32_t nSteps, size_t smem, cudaStream_t s);
 
+// Bond-code kernels (SysDev::codeMode kCode32 / kCode64). Tiles span kBcTileSpan in-colour
+// indices. In this representation the check zeroes the previous sub-step's marks, so a
+// stand-alone scrub is a check launch whose entry has color == kNoColor.
+constexpr int kCheckMpt = 2;                                   // monomers per thread per pass
+constexpr uint32_t kBcTileSpan = kGridBlock * kCheckMpt;
+// dTiles == nullptr: single system, descriptor passed by value (hostDesc); otherwise the tile
+// list selects the system per CTA from dSys and hostDesc is unused.
+cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
+                            StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s);
+cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
+                              StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s);
+size_t resident_bc_smem_bytes(uint32_t nwords, uint32_t ntab, uint32_t npad, uint32_t maxGroup, uint32_t codeMode);
+cudaError_t launch_resident_bc(SysDev const* dSys, uint32_t const* dList, uint32_t nCta, uint32_t perThread,
+                               StepEntry const* dSteps, uint32_t nSys, uint32_t nSteps, size_t smem, uint32_t codeMode,
+                               cudaStream_t s);
+
 // Sets the occupancy bit of every non-padding slot of system dSys[0] (lat must be zeroed).
 cudaError_t launch_build_lattice(SysDev const* dSys, uint32_t npad, cudaStream_t s);
 

@@ -1,0 +1,591 @@
+// Bond-code kernels of the BFM sweep (sm_100a).
+//
+// The same sub-step as the gather kernels (check: CRITICAL.cu:298-374, perform + apply:
+// CRITICAL.cu:376-411, clear: :561-573), on a different state: each monomer keeps its packed
+// lattice coordinates (pk) and a bond-code word whose 9-bit fields are the reference's bond-table
+// indices of its bonds, so the check needs no neighbour positions. When a monomer moves by d, its
+// own fields change by -d and the reverse field of every neighbour by +d; the reverse field's old
+// value is the negation (mod 8) of the monomer's own field, so the update needs no extra load.
+//
+// Grid phase (k_check_bc, k_perform_bc): flags are double-buffered by sub-step parity, so the
+// check of sub-step t also zeroes the temporary-lattice words marked at t-1 (found from
+// flags[parity^1] and pk, both read-only during the check). Every independent load of a pass is
+// issued before any dependent one; a single-system launch takes the descriptor as a grid-constant
+// parameter.
+//
+// Resident (k_resident_bc): one CTA owns a small system for a chunk of sub-steps; lattice, one
+// temporary lattice, pk and bond codes in shared memory; the check appends tentative movers to a
+// shared list (warp ballot + one atomic per warp), so the perform runs with full warps.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "bfm_device.cuh"
+#include "bfm_kernels.hpp"
+
+namespace bfm {
+
+namespace {
+
+constexpr uint32_t kMaxTab = 768;   // brick-table entries for boxes up to 1024 per side
+
+__device__ __forceinline__ void copy_desc(SysDev& dst, SysDev const* src)
+{
+    static_assert(sizeof(SysDev) % 4 == 0, "SysDev is copied word by word");
+    uint32_t const* s = reinterpret_cast<uint32_t const*>(src);
+    uint32_t* d = reinterpret_cast<uint32_t*>(&dst);
+    for (uint32_t w = threadIdx.x; w < sizeof(SysDev) / 4; w += blockDim.x) d[w] = s[w];
+}
+
+struct Plane {
+    uint32_t w[4];
+    unsigned long long m[4];
+};
+
+// The <= 2x2 brick words of the front plane at pk + 2 d (perpendicular +-1) and their masks; the
+// masks come from the plane table (ptab: global memory through L1, or shared memory).
+template <bool kSharedTables>
+__device__ __forceinline__ void front_plane(Plane& p, uint32_t const* tab, unsigned long long const* ptab,
+                                            SysDev const& S, uint32_t pk, uint32_t dir)
+{
+    uint32_t const c0 = pk & 1023u, c1 = (pk >> 10) & 1023u, c2 = pk >> 20;
+    uint32_t const a = dir >> 1;
+    // coordinate, box mask, brick count and table offset of the move axis a and of the two
+    // perpendicular axes u < v
+    uint32_t const ca = a == 0 ? c0 : (a == 1 ? c1 : c2);
+    uint32_t const cu = a == 0 ? c1 : c0;
+    uint32_t const cv = a == 2 ? c1 : c2;
+    uint32_t const ma = a == 0 ? S.mask[0] : (a == 1 ? S.mask[1] : S.mask[2]);
+    uint32_t const mu = a == 0 ? S.mask[1] : S.mask[0];
+    uint32_t const mv = a == 2 ? S.mask[1] : S.mask[2];
+    uint32_t const nbu = a == 0 ? S.nb[1] : S.nb[0];
+    uint32_t const nbv = a == 2 ? S.nb[1] : S.nb[2];
+    uint32_t const oa = a == 0 ? 0u : (a == 1 ? S.nb[0] : S.nb[0] + S.nb[1]);
+    uint32_t const ou = a == 0 ? S.nb[0] : 0u;
+    uint32_t const ov = a == 2 ? S.nb[0] : S.nb[0] + S.nb[1];
+    uint32_t const f = (ca + ((dir & 1u) ? 2u : 0xFFFFFFFEu)) & ma;
+    uint32_t const pu = (cu - 1u) & mu, pv = (cv - 1u) & mv;
+    uint32_t const ti = ((((a * 4u + (f & 3u)) * 4u + (pu & 3u)) * 4u + (pv & 3u)) * 4u);
+    ulonglong2 m01, m23;
+    if (kSharedTables) {
+        m01 = *reinterpret_cast<ulonglong2 const*>(ptab + ti);
+        m23 = *reinterpret_cast<ulonglong2 const*>(ptab + ti + 2);
+    } else {
+        m01 = __ldg(reinterpret_cast<ulonglong2 const*>(ptab + ti));
+        m23 = __ldg(reinterpret_cast<ulonglong2 const*>(ptab + ti + 2));
+    }
+    uint32_t const bu0 = pu >> 2, bv0 = pv >> 2;
+    uint32_t const wa = tab[oa + (f >> 2)];
+    uint32_t const wu0 = tab[ou + bu0], wu1 = tab[ou + ((bu0 + 1u) & (nbu - 1u))];
+    uint32_t const wv0 = tab[ov + bv0], wv1 = tab[ov + ((bv0 + 1u) & (nbv - 1u))];
+    p.w[0] = wa + wu0 + wv0;
+    p.m[0] = m01.x;
+    p.w[1] = wa + wu0 + wv1;
+    p.m[1] = m01.y;
+    p.w[2] = wa + wu1 + wv0;
+    p.m[2] = m23.x;
+    p.w[3] = wa + wu1 + wv1;
+    p.m[3] = m23.y;
+}
+
+// True if every bond of the code word stays allowed after the move along dir (move table).
+template <typename W, bool kSharedTables>
+__device__ __forceinline__ bool bonds_ok(W code, uint32_t dir, uint8_t const* ok)
+{
+    uint32_t const n = uint32_t(code >> CodeWord<W>::kCountShift) & 7u;
+    bool r = true;
+#pragma unroll
+    for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k) {
+        if (k < n) {
+            uint32_t const idx = uint32_t(code >> (9u * k)) & 511u;
+            uint32_t const m = kSharedTables ? ok[idx] : __ldg(ok + idx);
+            r = r && ((m >> dir) & 1u);
+        }
+    }
+    return r;
+}
+
+__device__ __forceinline__ uint32_t step_pk(uint32_t pk, uint32_t dir, uint32_t const* mask)
+{
+    uint32_t const a = dir >> 1;
+    uint32_t const sh = 10u * a;
+    uint32_t const c = (pk >> sh) & 1023u;
+    uint32_t const nc = (c + ((dir & 1u) ? 1u : 0xFFFFFFFFu)) & mask[a];
+    return (pk & ~(1023u << sh)) | (nc << sh);
+}
+
+__device__ __forceinline__ void cell_of(uint32_t pk, uint32_t const* tab, SysDev const& S, uint32_t& w, uint32_t& b)
+{
+    uint32_t const x = pk & 1023u, y = (pk >> 10) & 1023u, z = pk >> 20;
+    w = tab[x >> 2] + tab[S.nb[0] + (y >> 2)] + tab[S.nb[0] + S.nb[1] + (z >> 2)];
+    b = brick_bit(x, y, z);
+}
+
+// ---------------------------------------------------------------------------------- check
+
+template <typename W, int MPT>
+__device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab, StepEntry const& st, uint32_t start,
+                                           uint32_t* tally)
+{
+    uint32_t const B = blockDim.x, tid = threadIdx.x;
+    uint32_t const* const PK = S.pk;
+    W const* const CODE = static_cast<W const*>(S.code);
+    uint8_t const* const fprev = S.flags + (size_t)(st.parity ^ 1u) * S.npad;
+    unsigned long long* const tprev = S.tmp + (size_t)(st.parity ^ 1u) * S.nwords;
+    uint8_t* const fcur = S.flags + (size_t)st.parity * S.npad;
+    unsigned long long* const tcur = S.tmp + (size_t)st.parity * S.nwords;
+    bool const active = st.color != kNoColor;
+
+    // stage 1: every independent load of the pass
+    uint32_t pk[MPT], pkb[MPT];
+    W code[MPT];
+    uint8_t fb[MPT];
+#pragma unroll
+    for (int q = 0; q < MPT; ++q) {
+        uint32_t const i = start + tid + (uint32_t)q * B;
+        bool const a = active && i < st.cnt;
+        bool const b = i < st.pcnt;   // pcnt is 0 when there is nothing to scrub
+        pk[q] = a ? __ldg(PK + st.off + i) : 0u;
+        code[q] = a ? __ldg(CODE + st.off + i) : W(0);
+        fb[q] = b ? __ldg(fprev + st.poff + i) : (uint8_t)0;
+        pkb[q] = b ? __ldg(PK + st.poff + i) : 0u;
+    }
+    // scrub of the previous sub-step: every set bit of tmp[parity^1] belongs to one of its
+    // tentative movers, so zeroing a whole marked word only clears bits that are due
+#pragma unroll
+    for (int q = 0; q < MPT; ++q) {
+        if (fb[q] & 1u) {
+            uint32_t const target = (fb[q] & 2u) ? pkb[q] : step_pk(pkb[q], (fb[q] >> 2) & 7u, S.mask);
+            uint32_t w, b;
+            cell_of(target, tab, S, w, b);
+            tprev[w] = 0ull;
+        }
+    }
+    if (!active) return;
+    // stage 2: direction, bonds, front-plane words
+    uint32_t dir[MPT];
+    bool ok[MPT];
+    Plane pl[MPT];
+#pragma unroll
+    for (int q = 0; q < MPT; ++q) {
+        uint32_t const i = start + tid + (uint32_t)q * B;
+        dir[q] = move_dir(i, st.seed);
+        ok[q] = i < st.cnt && bonds_ok<W, false>(code[q], dir[q], S.moveOk);
+        front_plane<false>(pl[q], tab, S.planeTab, S, pk[q], dir[q]);
+    }
+    // stage 3: occupancy words
+    unsigned long long hit[MPT];
+#pragma unroll
+    for (int q = 0; q < MPT; ++q) {
+        hit[q] = 0ull;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if (ok[q] && pl[q].m[r]) hit[q] |= __ldg(S.lat + pl[q].w[r]) & pl[q].m[r];
+    }
+    // stage 4: decisions
+#pragma unroll
+    for (int q = 0; q < MPT; ++q) {
+        uint32_t const i = start + tid + (uint32_t)q * B;
+        bool const go = ok[q] && hit[q] == 0ull;
+        if (i < st.cnt) {
+            uint8_t f = 0;
+            if (go) {
+                uint32_t w, b;
+                cell_of(step_pk(pk[q], dir[q], S.mask), tab, S, w, b);
+                atomicOr(tcur + w, 1ull << b);
+                f = (uint8_t)((dir[q] << 2) | 1u);
+            }
+            fcur[st.off + i] = f;
+        }
+        tally_warp(go, tally);
+    }
+}
+
+// ---------------------------------------------------------------------------------- perform
+
+template <typename W, int MPT>
+__device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* tab, StepEntry const& st,
+                                             uint32_t start, uint32_t* tally)
+{
+    uint32_t const B = blockDim.x, tid = threadIdx.x;
+    uint32_t* const PK = S.pk;
+    W* const CODE = static_cast<W*>(S.code);
+    uint8_t* const fcur = S.flags + (size_t)st.parity * S.npad;
+    unsigned long long const* const tcur = S.tmp + (size_t)st.parity * S.nwords;
+
+    uint8_t f[MPT];
+    uint32_t pk[MPT];
+#pragma unroll
+    for (int q = 0; q < MPT; ++q) {
+        uint32_t const i = start + tid + (uint32_t)q * B;
+        bool const a = i < st.cnt;
+        f[q] = a ? fcur[st.off + i] : (uint8_t)0;
+        pk[q] = a ? PK[st.off + i] : 0u;
+    }
+    Plane pl[MPT];
+    W code[MPT];
+    uint32_t nbr[MPT][CodeWord<W>::kSlots];
+#pragma unroll
+    for (int q = 0; q < MPT; ++q) {
+        uint32_t const g = st.off + start + tid + (uint32_t)q * B;
+        bool const t = f[q] & 1u;
+        front_plane<false>(pl[q], tab, S.planeTab, S, pk[q], (f[q] >> 2) & 7u);
+        code[q] = t ? CODE[g] : W(0);
+#pragma unroll
+        for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k)
+            nbr[q][k] = (t && k < S.maxc) ? __ldg(S.nbrr + (size_t)k * S.npad + g) : 0u;
+    }
+    unsigned long long hit[MPT];
+#pragma unroll
+    for (int q = 0; q < MPT; ++q) {
+        hit[q] = 0ull;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if ((f[q] & 1u) && pl[q].m[r]) hit[q] |= __ldg(tcur + pl[q].w[r]) & pl[q].m[r];
+    }
+#pragma unroll
+    for (int q = 0; q < MPT; ++q) {
+        uint32_t const g = st.off + start + tid + (uint32_t)q * B;
+        bool const go = (f[q] & 1u) && hit[q] == 0ull;
+        if (go) {
+            uint32_t const dir = (f[q] >> 2) & 7u;
+            uint32_t const a = dir >> 1;
+            int32_t const s = (dir & 1u) ? 1 : -1;
+            uint32_t const pk1 = step_pk(pk[q], dir, S.mask);
+            uint32_t w0, b0, w1, b1;
+            cell_of(pk[q], tab, S, w0, b0);
+            cell_of(pk1, tab, S, w1, b1);
+            if (w0 == w1) {
+                atomicXor(S.lat + w0, (1ull << b0) | (1ull << b1));
+            } else {
+                atomicXor(S.lat + w0, 1ull << b0);
+                atomicXor(S.lat + w1, 1ull << b1);
+            }
+            PK[g] = pk1;
+            atomicAdd((a == 0 ? S.x : (a == 1 ? S.y : S.z)) + g, s);
+            fcur[g] = (uint8_t)(f[q] | 2u);
+            W const own = code[q];
+            CODE[g] = code_shift(own, a, -s);
+            uint32_t const n = uint32_t(own >> CodeWord<W>::kCountShift) & 7u;
+#pragma unroll
+            for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k) {
+                if (k < n) {
+                    uint32_t const e = nbr[q][k];
+                    uint32_t const c = (0u - (uint32_t(own >> (9u * k + 3u * a)) & 7u)) & 7u;   // reverse field
+                    uint32_t const nc = uint32_t(int32_t(c) + s) & 7u;
+                    atomicXor(CODE + (e & kSlotMask), W(c ^ nc) << (9u * (e >> kSlotShift) + 3u * a));
+                }
+            }
+        }
+        tally_warp(go, tally);
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------- kernels
+
+template <typename W, int MPT, bool kMulti>
+__global__ void __launch_bounds__(kGridBlock) k_check_bc(const __grid_constant__ SysDev S1,
+                                                         SysDev const* __restrict__ sysv,
+                                                         TileRef const* __restrict__ tiles,
+                                                         StepEntry const* __restrict__ steps)
+{
+    __shared__ SysDev Sm;
+    __shared__ uint32_t tab[kMaxTab];
+    uint32_t sys = 0, start = blockIdx.x * (kGridBlock * MPT);
+    if (kMulti) {
+        TileRef const tr = tiles[blockIdx.x];
+        sys = tr.sys;
+        start = tr.start;
+    }
+    StepEntry const st = steps[sys];
+    if (st.color == kNoColor && st.prevColor == kNoColor) return;
+    if (start >= st.cnt && start >= st.pcnt) return;
+    if (kMulti) {
+        copy_desc(Sm, sysv + sys);
+        __syncthreads();
+    }
+    SysDev const& S = kMulti ? Sm : S1;
+    __shared__ uint32_t tally;
+    uint32_t const ntab = S.nb[0] + S.nb[1] + S.nb[2];
+    for (uint32_t w = threadIdx.x; w < ntab; w += blockDim.x) tab[w] = S.brickTab[w];
+    if (threadIdx.x == 0) tally = 0;
+    __syncthreads();
+    check_body<W, MPT>(S, tab, st, start, &tally);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        tally_flush(tally, S.stats, 1);
+        if (start == 0 && st.color != kNoColor) tally_flush(st.cnt, S.stats, 0);
+    }
+}
+
+template <typename W, int MPT, bool kMulti>
+__global__ void __launch_bounds__(kGridBlock) k_perform_bc(const __grid_constant__ SysDev S1,
+                                                           SysDev const* __restrict__ sysv,
+                                                           TileRef const* __restrict__ tiles,
+                                                           StepEntry const* __restrict__ steps)
+{
+    __shared__ SysDev Sm;
+    __shared__ uint32_t tab[kMaxTab];
+    uint32_t sys = 0, start = blockIdx.x * (kGridBlock * MPT);
+    if (kMulti) {
+        TileRef const tr = tiles[blockIdx.x];
+        sys = tr.sys;
+        start = tr.start;
+    }
+    StepEntry const st = steps[sys];
+    if (st.color == kNoColor || start >= st.cnt) return;
+    if (kMulti) {
+        copy_desc(Sm, sysv + sys);
+        __syncthreads();
+    }
+    SysDev const& S = kMulti ? Sm : S1;
+    __shared__ uint32_t tally;
+    uint32_t const ntab = S.nb[0] + S.nb[1] + S.nb[2];
+    for (uint32_t w = threadIdx.x; w < ntab; w += blockDim.x) tab[w] = S.brickTab[w];
+    if (threadIdx.x == 0) tally = 0;
+    __syncthreads();
+    perform_body<W, MPT>(S, tab, st, start, &tally);
+    __syncthreads();
+    if (threadIdx.x == 0) tally_flush(tally, S.stats, 2);
+}
+
+// ---------------------------------------------------------------------------------- resident
+
+template <typename W, int K>
+__global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const* __restrict__ sysv,
+                                                                    uint32_t const* __restrict__ sysList,
+                                                                    StepEntry const* __restrict__ steps,
+                                                                    uint32_t nSys, uint32_t nSteps)
+{
+    __shared__ SysDev S;
+    __shared__ uint32_t listCount;
+    extern __shared__ unsigned long long smem[];
+    uint32_t const sysId = sysList[blockIdx.x];
+    copy_desc(S, sysv + sysId);
+    __syncthreads();
+    uint32_t const nw = S.nwords, np = S.npad;
+    uint32_t const B = blockDim.x, tid = threadIdx.x, lane = tid & 31u;
+    unsigned long long* const ptab = smem;                  // 768 plane masks
+    unsigned long long* const lat = smem + 768;
+    unsigned long long* const tmp = lat + nw;
+    W* const code = reinterpret_cast<W*>(tmp + nw);
+    uint32_t* const pk = reinterpret_cast<uint32_t*>(code + np);
+    uint32_t* const tab = pk + np;
+    uint32_t const ntab = S.nb[0] + S.nb[1] + S.nb[2];
+    uint8_t* const mok = reinterpret_cast<uint8_t*>(tab + ((ntab + 3u) & ~3u));   // 512 move-table bytes
+    uint32_t* const list = reinterpret_cast<uint32_t*>(mok + 512);
+    W const* const gcode = static_cast<W const*>(S.code);
+    for (uint32_t w = tid; w < 768; w += B) ptab[w] = S.planeTab[w];
+    for (uint32_t w = tid; w < 512; w += B) mok[w] = S.moveOk[w];
+    for (uint32_t w = tid; w < nw; w += B) {
+        lat[w] = S.lat[w];
+        tmp[w] = 0ull;
+    }
+    for (uint32_t g = tid; g < np; g += B) {
+        code[g] = gcode[g];
+        pk[g] = S.pk[g];
+    }
+    for (uint32_t w = tid; w < ntab; w += B) tab[w] = S.brickTab[w];
+    if (tid == 0) listCount = 0;
+    uint32_t nTent = 0, nAcc = 0;
+    unsigned long long nAtt = 0;
+    StepEntry next = nSteps ? steps[sysId] : StepEntry{};
+    __syncthreads();
+
+    for (uint32_t t = 0; t < nSteps; ++t) {
+        StepEntry const st = next;
+        if (t + 1 < nSteps) next = steps[(size_t)(t + 1) * nSys + sysId];   // prefetch
+        if (st.color == kNoColor) continue;
+        nAtt += st.cnt;
+        // check: tentative movers -> tmp bit + shared list (one atomic per warp)
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            uint32_t const i = tid + (uint32_t)k * B;
+            bool go = false;
+            uint32_t entry = 0;
+            if (i < st.cnt) {
+                uint32_t const g = st.off + i;
+                uint32_t const dir = move_dir(i, st.seed);
+                if (bonds_ok<W, true>(code[g], dir, mok)) {
+                    Plane pl;
+                    front_plane<true>(pl, tab, ptab, S, pk[g], dir);
+                    unsigned long long hit = 0ull;
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+                        if (pl.m[r]) hit |= lat[pl.w[r]] & pl.m[r];
+                    if (hit == 0ull) {
+                        uint32_t w, b;
+                        cell_of(step_pk(pk[g], dir, S.mask), tab, S, w, b);
+                        atomicOr(tmp + w, 1ull << b);
+                        go = true;
+                        entry = g | (dir << kSlotShift);
+                    }
+                }
+            }
+            uint32_t const bal = __ballot_sync(0xffffffffu, go);
+            if (bal) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(&listCount, (uint32_t)__popc(bal));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (go) list[base + __popc(bal & ((1u << lane) - 1u))] = entry;
+                nTent += lane == 0 ? (uint32_t)__popc(bal) : 0u;
+            }
+        }
+        __syncthreads();
+        // perform over the compact list
+        uint32_t const nList = listCount;
+        for (uint32_t e = tid; e < nList; e += B) {
+            uint32_t const g = list[e] & kSlotMask, dir = list[e] >> kSlotShift;
+            uint32_t const p = pk[g];
+            Plane pl;
+            front_plane<true>(pl, tab, ptab, S, p, dir);
+            unsigned long long hit = 0ull;
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (pl.m[r]) hit |= tmp[pl.w[r]] & pl.m[r];
+            if (hit != 0ull) continue;
+            uint32_t const a = dir >> 1;
+            int32_t const s = (dir & 1u) ? 1 : -1;
+            uint32_t const p1 = step_pk(p, dir, S.mask);
+            uint32_t w0, b0, w1, b1;
+            cell_of(p, tab, S, w0, b0);
+            cell_of(p1, tab, S, w1, b1);
+            if (w0 == w1) {
+                atomicXor(lat + w0, (1ull << b0) | (1ull << b1));
+            } else {
+                atomicXor(lat + w0, 1ull << b0);
+                atomicXor(lat + w1, 1ull << b1);
+            }
+            pk[g] = p1;
+            atomicAdd((a == 0 ? S.x : (a == 1 ? S.y : S.z)) + g, s);
+            W const own = code[g];
+            code[g] = code_shift(own, a, -s);
+            uint32_t const n = uint32_t(own >> CodeWord<W>::kCountShift) & 7u;
+            for (uint32_t q = 0; q < n; ++q) {
+                uint32_t const ent = __ldg(S.nbrr + (size_t)q * np + g);
+                uint32_t const c = (0u - (uint32_t(own >> (9u * q + 3u * a)) & 7u)) & 7u;
+                uint32_t const nc = uint32_t(int32_t(c) + s) & 7u;
+                atomicXor(code + (ent & kSlotMask), W(c ^ nc) << (9u * (ent >> kSlotShift) + 3u * a));
+            }
+            ++nAcc;
+        }
+        __syncthreads();
+        for (uint32_t w = tid; w < nw; w += B) tmp[w] = 0ull;
+        if (tid == 0) listCount = 0;
+        __syncthreads();
+    }
+    W* const gcodeOut = static_cast<W*>(S.code);
+    for (uint32_t w = tid; w < nw; w += B) S.lat[w] = lat[w];
+    for (uint32_t g = tid; g < np; g += B) {
+        gcodeOut[g] = code[g];
+        S.pk[g] = pk[g];
+    }
+    uint32_t const tsum = __reduce_add_sync(0xffffffffu, nTent);
+    uint32_t const asum = __reduce_add_sync(0xffffffffu, nAcc);
+    if (lane == 0) {
+        tally_flush(tsum, S.stats, 1);
+        tally_flush(asum, S.stats, 2);
+    }
+    if (tid == 0 && nAtt) atomicAdd(S.stats + (blockIdx.x % kStatSlots), nAtt);
+}
+
+// ---------------------------------------------------------------------------------- launchers
+
+namespace {
+
+template <typename W>
+cudaError_t launch_grid_bc(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
+                           uint32_t nTiles, StepEntry const* dSteps, cudaStream_t s)
+{
+    if (dTiles) {
+        if (check) k_check_bc<W, kCheckMpt, true><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
+        else k_perform_bc<W, kCheckMpt, true><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
+    } else {
+        if (check) k_check_bc<W, kCheckMpt, false><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
+        else k_perform_bc<W, kCheckMpt, false><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
+                            StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s)
+{
+    if (nTiles == 0) return cudaSuccess;
+    if (codeMode == kCode32) return launch_grid_bc<uint32_t>(true, hostDesc, dSys, dTiles, nTiles, dSteps, s);
+    if (codeMode == kCode64)
+        return launch_grid_bc<unsigned long long>(true, hostDesc, dSys, dTiles, nTiles, dSteps, s);
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
+                              StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s)
+{
+    if (nTiles == 0) return cudaSuccess;
+    if (codeMode == kCode32) return launch_grid_bc<uint32_t>(false, hostDesc, dSys, dTiles, nTiles, dSteps, s);
+    if (codeMode == kCode64)
+        return launch_grid_bc<unsigned long long>(false, hostDesc, dSys, dTiles, nTiles, dSteps, s);
+    return cudaErrorInvalidValue;
+}
+
+size_t resident_bc_smem_bytes(uint32_t nwords, uint32_t ntab, uint32_t npad, uint32_t maxGroup, uint32_t codeMode)
+{
+    size_t const w = codeMode == kCode64 ? 8 : 4;
+    return 768 * 8 + (size_t)nwords * 2 * 8 + (size_t)npad * (w + 4) + (size_t)((ntab + 3u) & ~3u) * 4 + 512 +
+           (size_t)maxGroup * 4;
+}
+
+namespace {
+
+template <typename W, int K>
+cudaError_t launch_resident_bc_k(SysDev const* dSys, uint32_t const* dList, uint32_t nCta, StepEntry const* dSteps,
+                                 uint32_t nSys, uint32_t nSteps, size_t smem, cudaStream_t s)
+{
+    static thread_local size_t attrSet[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    size_t& have = attrSet[dev & 63];
+    if (smem > have) {
+        e = cudaFuncSetAttribute(k_resident_bc<W, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        have = smem;
+    }
+    k_resident_bc<W, K><<<nCta, kResidentBlock, smem, s>>>(dSys, dList, dSteps, nSys, nSteps);
+    return cudaGetLastError();
+}
+
+template <typename W>
+cudaError_t launch_resident_bc_w(SysDev const* dSys, uint32_t const* dList, uint32_t nCta, uint32_t perThread,
+                                 StepEntry const* dSteps, uint32_t nSys, uint32_t nSteps, size_t smem, cudaStream_t s)
+{
+    switch (perThread) {
+    case 1: return launch_resident_bc_k<W, 1>(dSys, dList, nCta, dSteps, nSys, nSteps, smem, s);
+    case 2: return launch_resident_bc_k<W, 2>(dSys, dList, nCta, dSteps, nSys, nSteps, smem, s);
+    case 4: return launch_resident_bc_k<W, 4>(dSys, dList, nCta, dSteps, nSys, nSteps, smem, s);
+    case 8: return launch_resident_bc_k<W, 8>(dSys, dList, nCta, dSteps, nSys, nSteps, smem, s);
+    case 16: return launch_resident_bc_k<W, 16>(dSys, dList, nCta, dSteps, nSys, nSteps, smem, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_resident_bc(SysDev const* dSys, uint32_t const* dList, uint32_t nCta, uint32_t perThread,
+                               StepEntry const* dSteps, uint32_t nSys, uint32_t nSteps, size_t smem, uint32_t codeMode,
+                               cudaStream_t s)
+{
+    if (nCta == 0 || nSteps == 0) return cudaSuccess;
+    if (smem > kResidentMaxSmem) return cudaErrorInvalidValue;
+    if (codeMode == kCode32)
+        return launch_resident_bc_w<uint32_t>(dSys, dList, nCta, perThread, dSteps, nSys, nSteps, smem, s);
+    if (codeMode == kCode64)
+        return launch_resident_bc_w<unsigned long long>(dSys, dList, nCta, perThread, dSteps, nSys, nSteps, smem, s);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace bfm

@@ -96,7 +96,7 @@ extern "C" int bfm_sweep_noalloc(const bfm_noalloc_system* s, int32_t n_mcs, uin
     size_t const oGrp = up256(oSteps + sizeof(StepEntry) * kStepRing);
     size_t const oTab = up256(oGrp + sizeof(uint32_t) * 2 * 255);
     size_t const oStats = up256(oTab + sizeof(uint32_t) * 3 * kMaxBricksPerAxis);
-    size_t const oFlags = up256(oStats + 4 * sizeof(unsigned long long));
+    size_t const oFlags = up256(oStats + kStatBytes);
     size_t const oMark = up256(oFlags + (size_t)s->npad);
     size_t const oLat = up256(oMark + 8ull * s->npad);
     size_t const oTmp = up256(oLat + 8ull * nwords);
@@ -158,26 +158,8 @@ extern "C" int bfm_sweep_noalloc(const bfm_noalloc_system* s, int32_t n_mcs, uin
         grp[2 * c + 1] = s->group_size[c];
     }
     uint32_t tab[3 * kMaxBricksPerAxis];
-    {
-        uint32_t lb[3], pos[3][32], next = 0;
-        for (int a = 0; a < 3; ++a) {
-            lb[a] = 0;
-            while ((1u << lb[a]) < nb[a]) ++lb[a];
-        }
-        for (uint32_t k = 0; k < 32; ++k)
-            for (int a = 0; a < 3; ++a)
-                if (k < lb[a]) pos[a][k] = next++;
-        uint32_t o = 0;
-        for (int a = 0; a < 3; ++a) {
-            for (uint32_t b = 0; b < nb[a]; ++b) {
-                uint32_t w = 0;
-                for (uint32_t k = 0; k < lb[a]; ++k)
-                    if ((b >> k) & 1u) w |= 1u << pos[a][k];
-                tab[o + b] = w;
-            }
-            o += nb[a];
-        }
-    }
+    brick_tables_fill(nb, tab);
+    brick_params(nb, d.mb, d.hx, d.hy);
     SysDev* const dDesc = reinterpret_cast<SysDev*>(B + oDesc);
     StepEntry* const dSteps = reinterpret_cast<StepEntry*>(B + oSteps);
 #define NOALLOC_CHECK(call, what)                                                                      \
@@ -194,7 +176,7 @@ extern "C" int bfm_sweep_noalloc(const bfm_noalloc_system* s, int32_t n_mcs, uin
     NOALLOC_CHECK(cudaMemcpyAsync(B + oTab, tab, sizeof(uint32_t) * ntab, cudaMemcpyHostToDevice, st), "brick table copy");
     // what must start at zero: counters, both temporary lattices, the occupancy lattice (rebuilt
     // from the caller's positions)
-    NOALLOC_CHECK(cudaMemsetAsync(B + oStats, 0, 4 * sizeof(unsigned long long), st), "clear counters");
+    NOALLOC_CHECK(cudaMemsetAsync(B + oStats, 0, kStatBytes, st), "clear counters");
     NOALLOC_CHECK(cudaMemsetAsync(B + oTmp, 0, 16ull * nwords, st), "clear temporary lattices");
     NOALLOC_CHECK(cudaMemsetAsync(B + oLat, 0, 8ull * nwords, st), "clear lattice");
     NOALLOC_CHECK(launch_build_lattice(dDesc, s->npad, st), "build lattice");
@@ -218,6 +200,10 @@ extern "C" int bfm_sweep_noalloc(const bfm_noalloc_system* s, int32_t n_mcs, uin
             q.seed = draw(seed, 2 * sub + 1);
             q.parity = (uint32_t)(sub & 1u);
             q.prevColor = last;
+            q.off = s->group_offset[q.color];
+            q.cnt = s->group_size[q.color];
+            q.poff = last == kNoColor ? 0u : s->group_offset[last];
+            q.pcnt = last == kNoColor ? 0u : s->group_size[last];
             last = q.color;
         }
         NOALLOC_CHECK(cudaMemcpyAsync(dSteps + ring, chunk, sizeof(StepEntry) * m, cudaMemcpyHostToDevice, st),

@@ -15,6 +15,8 @@ import numpy as np
 from . import _lib
 from ._lib import MODE_AUTO, MODE_GRAPH, MODE_LAUNCH, MODE_RESIDENT  # noqa: F401
 
+REPR_AUTO, REPR_GATHER = 0, 1
+
 
 def color_graph(system) -> np.ndarray:
     """Colours of the system's monomers as initialize() computes them (host only, no GPU)."""
@@ -198,9 +200,21 @@ class UpdaterGPUScBFM_AB_Type:
 
     n_monomers = 0
 
-    def load_system(self, system, seed: int | None = None, mode: int | None = None, initialize: bool = True):
+    def set_representation(self, repr_: int):
+        """REPR_AUTO (bond codes where possible) or REPR_GATHER; before initialize()."""
+        self._call("bfm_set_representation", repr_)
+
+    def representation(self) -> int:
+        v = C.c_int()
+        self._call("bfm_get_representation", C.byref(v))
+        return v.value
+
+    def load_system(self, system, seed: int | None = None, mode: int | None = None, initialize: bool = True,
+                    representation: int | None = None):
         """Feeds a systems.BfmSystem through the setter API in the adapter's order
         (src/pscbfm/GPUScBFM_AB_Type.h:83-130), then initializes."""
+        if representation is not None:
+            self.set_representation(representation)
         self.setPeriodicity(True, True, True)
         self.setNrOfAllMonomers(system.n)
         self.set_coords(system.xyz)
@@ -255,6 +269,11 @@ class Batch:
         ms = C.c_float()
         self._call("bfm_batch_run_timed", n_mcs, C.byref(ms))
         return ms.value
+
+    def launch_count(self) -> int:
+        v = C.c_uint64()
+        self._call("bfm_batch_launch_count", C.byref(v))
+        return v.value
 
     def synchronize(self):
         self._call("bfm_batch_synchronize")

@@ -13,11 +13,14 @@ from pscbfm_b200 import systems as S
 pytestmark = pytest.mark.gpu
 
 MODES = {"launch": P.MODE_LAUNCH, "graph": P.MODE_GRAPH, "resident": P.MODE_RESIDENT, "auto": P.MODE_AUTO}
+REPRS = {"codes": P.REPR_AUTO, "gather": P.REPR_GATHER}
 
 
-def run_engine(s, chunks, mode=P.MODE_AUTO, seed=None):
+def run_engine(s, chunks, mode=P.MODE_AUTO, seed=None, repr_=P.REPR_AUTO):
     u = P.UpdaterGPUScBFM_AB_Type(0)
-    u.load_system(s, seed=seed, mode=mode)
+    u.load_system(s, seed=seed, mode=mode, representation=repr_)
+    if repr_ == P.REPR_AUTO:
+        assert u.representation() != 0, "symmetric systems with <= 6 bonds use bond codes"
     for c in chunks:
         u.runSimulationOnGPU(c)
     xyz = u.get_coords().copy()
@@ -31,17 +34,33 @@ def _resident_ok(s):
     return max(s.box) <= 64
 
 
+@pytest.mark.parametrize("repr_", ["codes", "gather"])
 @pytest.mark.parametrize("mode", ["launch", "graph", "resident"])
 @pytest.mark.parametrize("name", list(CASES))
-def test_engine_reproduces_reference_updater(name, mode):
+def test_engine_reproduces_reference_updater(name, mode, repr_):
     g = json.load(open(GOLDEN_JSON))["cases"][name]
     build, chunks = CASES[name]
     s = build()
     if mode == "resident" and not _resident_ok(s):
         pytest.skip("box larger than the resident kernel holds")
-    xyz, st = run_engine(s, chunks, MODES[mode])
+    xyz, st = run_engine(s, chunks, MODES[mode], repr_=REPRS[repr_])
     assert positions_digest(xyz) == g["sha256"]
     assert st["mcs"] == sum(chunks)
+
+
+def test_asymmetric_lists_fall_back_to_gather():
+    # a bond listed in one direction only: the reference checks it from one side only
+    xyz = np.array([[2 * j, 0, 0] for j in range(16)])
+    s = S.from_bonds((32, 32, 32), xyz, [(j, j + 1) for j in range(15)], seed=8)
+    s.nbr_count = s.nbr_count.copy()
+    s.nbr_count[5] = 1       # monomer 5 forgets its second neighbour (6); 6 still lists 5
+    ref, _ = O.run(s, 150)
+    u = P.UpdaterGPUScBFM_AB_Type(0)
+    u.load_system(s)
+    assert u.representation() == 0
+    u.runSimulationOnGPU(150)
+    assert np.array_equal(u.get_coords(), ref)
+    u.close()
 
 
 def test_engine_matches_live_reference_updater():
@@ -55,12 +74,13 @@ def test_engine_matches_live_reference_updater():
     assert np.array_equal(xyz, ref)
 
 
+@pytest.mark.parametrize("repr_", ["codes", "gather"])
 @pytest.mark.parametrize("mode", ["launch", "graph"])
-def test_six_functional_network_vs_oracle(mode):
+def test_six_functional_network_vs_oracle(mode, repr_):
     # the reference is compiled with MAX_CONNECTIVITY 4, so this case is pinned by the oracle only
     s = S.crosslinked_network()
     ref, ost = O.run(s, 1000)
-    xyz, st = run_engine(s, [400, 600], MODES[mode])
+    xyz, st = run_engine(s, [400, 600], MODES[mode], repr_=REPRS[repr_])
     assert np.array_equal(xyz, ref)
     assert (st["attempted"], st["tentative"], st["accepted"]) == ost
 
@@ -131,7 +151,12 @@ def test_set_coords_after_initialize():
 def test_batch_equals_each_system_alone(resident):
     systems = S.ensemble(n_systems=20)
     systems.append(S.rings_and_free())         # three colours in the mix
+    systems.append(S.crosslinked_network())    # 64-bit bond codes in the mix
     members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
+    # and two systems forced onto the gather representation
+    for s in systems[:2]:
+        members.append(P.UpdaterGPUScBFM_AB_Type(0).load_system(s, representation=P.REPR_GATHER))
+    systems = systems + systems[:2]
     b = P.Batch(members, resident=resident)
     b.run(60)
     b.run(40)
