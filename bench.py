@@ -36,7 +36,7 @@ L2_FLUSH_BYTES = 256 << 20
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["dense_melt", "small", "network", "ensemble"], default="dense_melt")
@@ -112,6 +112,58 @@ def profiled_traffic(kernel_key):
 
 
 # ------------------------------------------------------------------ clocks
+
+class NvmlClockSampler:
+    """SM clock and throttle reasons read through NVML every 20 ms on a background thread (read
+    only; nothing is set)."""
+
+    REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
+
+    def __init__(self, gpu_index):
+        import threading
+        import pynvml
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        self.h = pynvml.nvmlDeviceGetHandleByIndex(int(gpu_index))
+        self.max = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        self.samples, self.reasons = [], set()
+        self.stop_flag = threading.Event()
+        self.t = threading.Thread(target=self._loop, daemon=True)
+        self.t.start()
+
+    def _loop(self):
+        nv = self.nv
+        while not self.stop_flag.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, const in self.REASONS.items():
+                    if bits & getattr(nv, const):
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self.stop_flag.wait(0.02)
+
+    def stop(self):
+        self.stop_flag.set()
+        self.t.join(timeout=2)
+        try:
+            self.nv.nvmlShutdown()
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.max,
+                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "nvml, 20 ms"}
+
+
+def clock_sampler(gpu_index):
+    try:
+        return NvmlClockSampler(gpu_index)
+    except Exception:
+        return ClockSampler(gpu_index)
+
 
 class ClockSampler:
     FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
@@ -267,7 +319,7 @@ def run_ours(args):
     stats0 = [m.stats() for m in members]
     barrier(world)
     torch.cuda.synchronize()
-    sampler = ClockSampler(gpu_index(local))
+    sampler = clock_sampler(gpu_index(local))
     ms = 0.0
     for _ in range(args.steps):
         flush.zero_()

@@ -132,6 +132,19 @@ int bfm_validate(bfm_handle h);
 /* Device bytes held by the handle. */
 int bfm_device_bytes(bfm_handle h, uint64_t* out);
 
+/* ------------------------------------------------------------------ observables (no reference counterpart) */
+/* Molecules are the connected components of the bonds, numbered by their lowest monomer id. */
+int bfm_n_molecules(bfm_handle h, uint32_t* n_mol);
+int bfm_molecule_sizes(bfm_handle h, uint32_t* sizes, uint32_t capacity);
+/* Exact int64 observables of the current configuration, 5*n_mol + 513 words:
+ *   [4m .. 4m+3]      molecule m: sum x, sum y, sum z, sum (x^2+y^2+z^2)  (Rg^2 = S2/n - |S1|^2/n^2)
+ *   [4 n_mol + m]     molecule m: |r_last - r_first|^2 (lowest and highest monomer id)
+ *   [5 n_mol + idx]   bond-vector histogram by table index (dx&7)|(dy&7)<<3|(dz&7)<<6, every listed bond
+ *   [5 n_mol + 512]   sum over monomers of |r - r_ref|^2 (r_ref: positions at initialize or last reset) */
+int bfm_observables(bfm_handle h, int64_t* out, uint64_t capacity_words);
+/* Makes the current positions the reference of the displacement sum. */
+int bfm_reset_msd_reference(bfm_handle h);
+
 /* ------------------------------------------------------------------ measurement (no reference counterpart) */
 /* bfm_run bracketed by CUDA events on the handle's stream; *ms = device time of the n_mcs MCS. */
 int bfm_run_timed(bfm_handle h, int32_t n_mcs, float* ms);
@@ -165,6 +178,41 @@ int bfm_batch_synchronize(bfm_batch_handle b);
 /* 0: every system on the grid path; 1 (default): small systems on the resident kernel. */
 int bfm_batch_set_resident(bfm_batch_handle b, int on);
 const char* bfm_batch_last_error(bfm_batch_handle b);
+
+/* ------------------------------------------------------------------ server (no reference counterpart) */
+/* Continuous batching of jobs "run this system for n_mcs MCS, sample observables every k MCS".
+ * A worker thread admits jobs in arrival order while their estimated device bytes fit the budget,
+ * sets new jobs up while running ones compute, and advances all running jobs together; a job's
+ * result equals running it alone. Job states: */
+#define BFM_JOB_PENDING 0
+#define BFM_JOB_RUNNING 1
+#define BFM_JOB_DONE 2
+#define BFM_JOB_CANCELLED 3
+#define BFM_JOB_FAILED 4
+typedef struct bfm_server* bfm_server_handle;
+int bfm_server_create(bfm_server_handle* out, int gpu, uint64_t budget_bytes, uint32_t max_jobs);
+/* Stops the worker (running jobs are dropped) and frees everything. */
+int bfm_server_destroy(bfm_server_handle s);
+/* The job's system is the setter state of `setup` (a handle that has NOT been initialised; it is
+ * copied, the caller keeps it). BFM_ERR_BUDGET if the job alone exceeds the budget. */
+int bfm_server_submit(bfm_server_handle s, bfm_handle setup, int32_t n_mcs, int32_t sample_every, uint64_t* job);
+/* The device bytes admission charges for a job built from `setup` (not initialised). */
+int bfm_server_estimate_bytes(bfm_handle setup, uint64_t* bytes);
+int bfm_server_status(bfm_server_handle s, uint64_t job, int* state);
+int bfm_server_cancel(bfm_server_handle s, uint64_t job);
+/* Waits up to timeout_s for a final state; BFM_ERR_BUSY on timeout. */
+int bfm_server_wait(bfm_server_handle s, uint64_t job, double timeout_s);
+/* Final positions (n monomers, may be NULL), the observable samples (ceil(n_mcs/k) records of
+ * 5*n_mol+513 int64 words, may be NULL) and the latency from submit to completion.
+ * BFM_ERR_BUSY if the job has not finished. */
+int bfm_server_result(bfm_server_handle s, uint64_t job, int32_t* xyz, uint32_t n, int64_t* samples,
+                      uint64_t capacity_words, uint32_t* n_samples, double* latency_s);
+/* out = {completed, failed, attempted moves of completed jobs, p50 latency s, p99 latency s,
+ *        mean latency s, resident device bytes, seconds since create} */
+int bfm_server_stats(bfm_server_handle s, double out[8]);
+/* Test hook: kind 1 makes the worker thread throw at its next loop (simulated worker death). */
+int bfm_server_inject_fault(bfm_server_handle s, int kind);
+const char* bfm_server_last_error(bfm_server_handle s);
 
 /* ------------------------------------------------------------------ sweep without allocation */
 /* No counterpart in the reference. For callers that must not have the library allocate device

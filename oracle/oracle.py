@@ -147,3 +147,52 @@ def ref_run(sys, draws, chunks, gpu: int = 0):
     if rc != 0:
         raise RuntimeError(f"reference updater failed ({rc}): {err.value.decode()}")
     return out.reshape(-1, 3), int(used[0])
+
+
+# ------------------------------------------------------------------ observables (int64 recomputation)
+
+def molecules(sys):
+    """Connected components of the bond graph, numbered by their lowest monomer id."""
+    parent = list(range(sys.n))
+
+    def find(a):
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = parent[a]
+        return a
+    rows, cols = sys.bonds()
+    for a, b in zip(rows.tolist(), cols.tolist()):
+        ra, rb = find(a), find(b)
+        if ra != rb:
+            parent[max(ra, rb)] = min(ra, rb)
+    roots = np.array([find(i) for i in range(sys.n)])
+    _, first_idx, mol = np.unique(roots, return_index=True, return_inverse=True)
+    # np.unique sorts by root id = lowest member id, which is the required numbering
+    return mol.astype(np.int64)
+
+
+def observables(sys, xyz, xyz_ref):
+    """The int64 words of bfm_observables, recomputed from positions with numpy (exact int64)."""
+    xyz = np.asarray(xyz, dtype=np.int64)
+    ref = np.asarray(xyz_ref, dtype=np.int64)
+    mol = molecules(sys)
+    m = int(mol.max()) + 1
+    out = np.zeros(5 * m + 513, dtype=np.int64)
+    mom = np.zeros((m, 4), dtype=np.int64)
+    for a in range(3):
+        np.add.at(mom[:, a], mol, xyz[:, a])
+    np.add.at(mom[:, 3], mol, (xyz ** 2).sum(axis=1))
+    out[:4 * m] = mom.reshape(-1)
+    idx = np.arange(sys.n)
+    first = np.full(m, sys.n, dtype=np.int64)
+    last = np.full(m, -1, dtype=np.int64)
+    np.minimum.at(first, mol, idx)
+    np.maximum.at(last, mol, idx)
+    d = xyz[last] - xyz[first]
+    out[4 * m:5 * m] = (d ** 2).sum(axis=1)
+    rows, cols = sys.bonds()
+    bi = (xyz[cols] - xyz[rows]) & 7
+    code = bi[:, 0] | (bi[:, 1] << 3) | (bi[:, 2] << 6)
+    out[5 * m:5 * m + 512] = np.bincount(code, minlength=512)
+    out[5 * m + 512] = ((xyz - ref) ** 2).sum()
+    return out

@@ -87,6 +87,10 @@ _SIGS = {
     "bfm_validate": [H],
     "bfm_device_bytes": [H, C.POINTER(C.c_uint64)],
     "bfm_run_timed": [H, C.c_int32, C.POINTER(C.c_float)],
+    "bfm_n_molecules": [H, C.POINTER(C.c_uint32)],
+    "bfm_molecule_sizes": [H, _u32p, C.c_uint32],
+    "bfm_observables": [H, _i64p, C.c_uint64],
+    "bfm_reset_msd_reference": [H],
     "bfm_time_kernels": [H, C.c_int32, _f64p],
     "bfm_launch_count": [H, C.POINTER(C.c_uint64)],
     "bfm_batch_create": [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p), C.c_uint32],
@@ -97,11 +101,24 @@ _SIGS = {
     "bfm_batch_synchronize": [H],
     "bfm_batch_set_resident": [H, C.c_int],
     "bfm_sweep_noalloc": [C.c_void_p, C.c_int32, C.c_uint64, C.c_uint64, C.c_void_p, C.c_char_p, C.c_size_t],
+    "bfm_server_create": [C.POINTER(C.c_void_p), C.c_int, C.c_uint64, C.c_uint32],
+    "bfm_server_destroy": [H],
+    "bfm_server_submit": [H, H, C.c_int32, C.c_int32, C.POINTER(C.c_uint64)],
+    "bfm_server_estimate_bytes": [H, C.POINTER(C.c_uint64)],
+    "bfm_server_status": [H, C.c_uint64, C.POINTER(C.c_int)],
+    "bfm_server_cancel": [H, C.c_uint64],
+    "bfm_server_wait": [H, C.c_uint64, C.c_double],
+    "bfm_server_result": [H, C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint32),
+                          C.POINTER(C.c_double)],
+    "bfm_server_stats": [H, _f64p],
+    "bfm_server_inject_fault": [H, C.c_int],
     "bfm_color_graph": [C.c_uint32, _u32p, _u32p, C.c_uint32,
                         np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS"), C.POINTER(C.c_uint32)],
 }
-_RET = {"bfm_last_error": C.c_char_p, "bfm_batch_last_error": C.c_char_p, "bfm_counter_draw": C.c_uint32}
-_RET_ARGS = {"bfm_last_error": [H], "bfm_batch_last_error": [H], "bfm_counter_draw": [C.c_uint64, C.c_uint64]}
+_RET = {"bfm_last_error": C.c_char_p, "bfm_batch_last_error": C.c_char_p, "bfm_counter_draw": C.c_uint32,
+        "bfm_server_last_error": C.c_char_p}
+_RET_ARGS = {"bfm_last_error": [H], "bfm_batch_last_error": [H], "bfm_counter_draw": [C.c_uint64, C.c_uint64],
+             "bfm_server_last_error": [H]}
 
 _lib = None
 

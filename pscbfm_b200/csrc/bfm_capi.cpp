@@ -7,6 +7,13 @@
 #include <string>
 
 #include "bfm_engine.hpp"
+#include "bfm_server.hpp"
+
+struct bfm_server {
+    bfm::Server s;
+    std::string err;
+    bfm_server(int gpu, size_t budget, uint32_t maxJobs) : s(gpu, budget, maxJobs) {}
+};
 
 struct bfm_updater {
     bfm::Updater u;
@@ -42,6 +49,12 @@ int guarded(std::string* sink, F&& f)
     } catch (std::bad_alloc const&) {
         (sink ? *sink : gErr) = "host allocation failed";
         return BFM_ERR_RUNTIME;
+    } catch (bfm::BudgetError const& e) {
+        (sink ? *sink : gErr) = e.what();
+        return BFM_ERR_BUDGET;
+    } catch (bfm::BusyError const& e) {
+        (sink ? *sink : gErr) = e.what();
+        return BFM_ERR_BUSY;
     } catch (std::exception const& e) {
         (sink ? *sink : gErr) = e.what();
         return BFM_ERR_RUNTIME;
@@ -189,6 +202,34 @@ int bfm_device_bytes(bfm_handle h, uint64_t* out)
     });
 }
 
+int bfm_n_molecules(bfm_handle h, uint32_t* n)
+{
+    BFM_CALL(h, {
+        if (!n) throw std::invalid_argument("[bfm_n_molecules] null output");
+        h->u.moleculeSizes();   // requires initialize
+        *n = h->u.nMolecules();
+    });
+}
+int bfm_molecule_sizes(bfm_handle h, uint32_t* sizes, uint32_t cap)
+{
+    BFM_CALL(h, {
+        auto const m = h->u.moleculeSizes();
+        if (!sizes && cap) throw std::invalid_argument("[bfm_molecule_sizes] null output");
+        for (uint32_t i = 0; i < m.size() && i < cap; ++i) sizes[i] = m[i];
+    });
+}
+int bfm_observables(bfm_handle h, int64_t* out, uint64_t cap)
+{
+    BFM_CALL(h, {
+        if (!out) throw std::invalid_argument("[bfm_observables] null output");
+        h->u.moleculeSizes();
+        if (cap < bfm::obs_words(h->u.nMolecules()))
+            throw std::invalid_argument("[bfm_observables] output holds fewer than 5*n_mol+513 words");
+        h->u.observables(reinterpret_cast<long long*>(out));
+    });
+}
+int bfm_reset_msd_reference(bfm_handle h) { BFM_CALL(h, h->u.resetReference()); }
+
 int bfm_run_timed(bfm_handle h, int32_t n, float* ms)
 {
     BFM_CALL(h, {
@@ -210,6 +251,70 @@ int bfm_launch_count(bfm_handle h, uint64_t* out)
         *out = h->u.launches();
     });
 }
+
+// ---------------------------------------------------------------- server
+
+const char* bfm_server_last_error(bfm_server_handle s) { return s ? s->err.c_str() : gErr.c_str(); }
+
+int bfm_server_create(bfm_server_handle* out, int gpu, uint64_t budget, uint32_t maxJobs)
+{
+    if (!out) {
+        gErr = "null output pointer";
+        return BFM_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    return guarded(nullptr, [&] { *out = new bfm_server(gpu, (size_t)budget, maxJobs); });
+}
+
+int bfm_server_destroy(bfm_server_handle s)
+{
+    if (!s) return BFM_OK;
+    delete s;
+    return BFM_OK;
+}
+
+int bfm_server_submit(bfm_server_handle s, bfm_handle setup, int32_t nMcs, int32_t every, uint64_t* job)
+{
+    BFM_CALL(s, {
+        if (!setup || !job) throw std::invalid_argument("[bfm_server_submit] null argument");
+        *job = s->s.submit(setup->u, nMcs, every);
+    });
+}
+int bfm_server_estimate_bytes(bfm_handle setup, uint64_t* bytes)
+{
+    BFM_CALL(setup, {
+        if (!bytes) throw std::invalid_argument("[bfm_server_estimate_bytes] null output");
+        setup->u.checkSetup();
+        *bytes = bfm::Server::estimateBytes(setup->u);
+    });
+}
+int bfm_server_status(bfm_server_handle s, uint64_t job, int* state)
+{
+    BFM_CALL(s, {
+        if (!state) throw std::invalid_argument("[bfm_server_status] null output");
+        *state = s->s.status(job);
+    });
+}
+int bfm_server_cancel(bfm_server_handle s, uint64_t job) { BFM_CALL(s, s->s.cancel(job)); }
+int bfm_server_wait(bfm_server_handle s, uint64_t job, double timeout)
+{
+    BFM_CALL(s, {
+        if (!s->s.wait(job, timeout)) throw bfm::BusyError("[bfm_server_wait] timed out");
+    });
+}
+int bfm_server_result(bfm_server_handle s, uint64_t job, int32_t* xyz, uint32_t n, int64_t* samples, uint64_t cap,
+                      uint32_t* nSamples, double* latency)
+{
+    BFM_CALL(s, s->s.result(job, xyz, n, reinterpret_cast<long long*>(samples), cap, nSamples, latency));
+}
+int bfm_server_stats(bfm_server_handle s, double out[8])
+{
+    BFM_CALL(s, {
+        if (!out) throw std::invalid_argument("[bfm_server_stats] null output");
+        s->s.stats(out);
+    });
+}
+int bfm_server_inject_fault(bfm_server_handle s, int kind) { BFM_CALL(s, s->s.injectFault(kind)); }
 
 // ---------------------------------------------------------------- host-only helpers
 

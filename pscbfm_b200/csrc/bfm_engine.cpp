@@ -413,6 +413,7 @@ void Updater::initialize()
     }
     if (!stepsFree_) cuda_check(cudaEventCreateWithFlags(&stepsFree_, cudaEventDisableTiming), "cudaEventCreate");
     cuda_check(cudaStreamSynchronize(s), "initialize");
+    buildObservables();
     subStep_ = 0;
     mcsDone_ = 0;
     lastColor_ = kNoColor;
@@ -456,6 +457,142 @@ void Updater::hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, s
         }
         std::memcpy(&code[w * s], &c, w);
     }
+}
+
+void Updater::buildObservables()
+{
+    // molecules: connected components of the bond graph, numbered by their lowest monomer id
+    std::vector<uint32_t> parent(n_);
+    for (uint32_t i = 0; i < n_; ++i) parent[i] = i;
+    auto find = [&](uint32_t a) {
+        while (parent[a] != a) a = parent[a] = parent[parent[a]];
+        return a;
+    };
+    for (uint32_t i = 0; i < n_; ++i)
+        for (uint32_t k = 0; k < nbrCnt_[i]; ++k) {
+            uint32_t a = find(i), b = find(nbrIds_[(size_t)i * kMaxConn + k]);
+            if (a != b) parent[a < b ? b : a] = a < b ? a : b;
+        }
+    std::vector<uint32_t> molOf(n_), rootMol(n_, kNoColor);
+    nMol_ = 0;
+    molSize_.clear();
+    std::vector<uint32_t> first, last;
+    for (uint32_t i = 0; i < n_; ++i) {
+        uint32_t const r = find(i);
+        if (rootMol[r] == kNoColor) {
+            rootMol[r] = nMol_++;
+            molSize_.push_back(0);
+            first.push_back(i);
+            last.push_back(i);
+        }
+        uint32_t const m = rootMol[r];
+        molOf[i] = m;
+        ++molSize_[m];
+        last[m] = i;
+    }
+    std::vector<uint32_t> molOfSlot(npad_, kNoColor), ends(2ull * nMol_);
+    for (uint32_t i = 0; i < n_; ++i) molOfSlot[oldToNew_[i]] = molOf[i];
+    for (uint32_t m = 0; m < nMol_; ++m) {
+        ends[2 * m] = oldToNew_[first[m]];
+        ends[2 * m + 1] = oldToNew_[last[m]];
+    }
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t const o = off;
+        off = align256(off + bytes);
+        return o;
+    };
+    size_t const oMol = take(4ull * npad_), oEnds = take(8ull * nMol_), oR = take(12ull * npad_);
+    size_t const oOut = take(sizeof(long long) * obs_words(nMol_));
+    cuda_check(cudaMalloc(&obsArena_, off), "cudaMalloc(observables)");
+    char* base = static_cast<char*>(obsArena_);
+    obs_.molOfSlot = reinterpret_cast<uint32_t*>(base + oMol);
+    obs_.ends = reinterpret_cast<uint32_t*>(base + oEnds);
+    obs_.rx = reinterpret_cast<int32_t*>(base + oR);
+    obs_.ry = obs_.rx + npad_;
+    obs_.rz = obs_.ry + npad_;
+    obs_.nMol = nMol_;
+    dObsOut_ = reinterpret_cast<long long*>(base + oOut);
+    cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(obs_.molOfSlot), molOfSlot.data(), 4ull * npad_,
+                               cudaMemcpyHostToDevice, stream_), "upload molecules");
+    cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(obs_.ends), ends.data(), 8ull * nMol_, cudaMemcpyHostToDevice,
+                               stream_), "upload molecule ends");
+    cuda_check(cudaStreamSynchronize(stream_), "observables set-up");
+    resetReference();
+}
+
+std::vector<uint32_t> Updater::moleculeSizes() const
+{
+    requireInit("moleculeSizes");
+    return molSize_;
+}
+
+void Updater::resetReference()
+{
+    requireInit("resetReference");
+    cuda_check(cudaMemcpyAsync(const_cast<int32_t*>(obs_.rx), dev_.h.x, 4ull * npad_, cudaMemcpyDeviceToDevice, stream_),
+               "reference x");
+    cuda_check(cudaMemcpyAsync(const_cast<int32_t*>(obs_.ry), dev_.h.y, 4ull * npad_, cudaMemcpyDeviceToDevice, stream_),
+               "reference y");
+    cuda_check(cudaMemcpyAsync(const_cast<int32_t*>(obs_.rz), dev_.h.z, 4ull * npad_, cudaMemcpyDeviceToDevice, stream_),
+               "reference z");
+}
+
+void Updater::enqueueObservables(long long* dOut, cudaStream_t s)
+{
+    requireInit("observables");
+    cuda_check(launch_observables(dev_.dDesc, obs_, dOut, npad_, s), "observables");
+    ++launches_;
+}
+
+void Updater::observables(long long* out)
+{
+    enqueueObservables(dObsOut_, stream_);
+    cuda_check(cudaMemcpyAsync(out, dObsOut_, sizeof(long long) * obs_words(nMol_), cudaMemcpyDeviceToHost, stream_),
+               "download observables");
+    cuda_check(cudaStreamSynchronize(stream_), "observables");
+}
+
+void Updater::checkSetup() const
+{
+    requireN("initialize");
+    if (n_ == 0) throw std::runtime_error("[initialize] the system has no monomers");
+    if (!box_[0]) throw std::runtime_error("[initialize] setLatticeSize has not been called");
+    uint32_t nAllowed = 0;
+    for (bool f : forbidden_) nAllowed += f ? 0 : 1;
+    if (nAllowed != 108) {
+        std::ostringstream m;
+        m << "[UpdaterGPUScBFM_AB_Type::initialize] Wrong bond-set! Expected 108 allowed bonds, but got " << nAllowed;
+        throw std::runtime_error(m.str());
+    }
+}
+
+void Updater::copySetup(Updater const& o)
+{
+    if (initialized()) throw std::runtime_error("[copySetup] target already initialized");
+    n_ = o.n_;
+    nSet_ = o.nSet_;
+    if (o.hostStale_) throw std::runtime_error("[copySetup] source positions are on the device");
+    xyz_ = o.xyz_;
+    attr_ = o.attr_;
+    nbrCnt_ = o.nbrCnt_;
+    nbrIds_ = o.nbrIds_;
+    for (int a = 0; a < 3; ++a) box_[a] = o.box_[a];
+    std::copy(o.forbidden_, o.forbidden_ + 512, forbidden_);
+    latticePopulated_ = o.latticePopulated_;
+    drawKind_ = o.drawKind_;
+    drawSeed_ = o.drawSeed_;
+    drawFn_ = o.drawFn_;
+    drawCtx_ = o.drawCtx_;
+    mode_ = o.mode_;
+    repr_ = o.repr_;
+}
+
+uint32_t Updater::maxNeighbours() const
+{
+    uint32_t m = 0;
+    for (uint32_t c : nbrCnt_) m = std::max(m, c);
+    return m;
 }
 
 void Updater::setRepresentation(int r)
@@ -903,6 +1040,12 @@ void Updater::freeDevice()
         cudaFree(dev_.arena);
     }
     dev_ = Device{};
+    if (obsArena_) cudaFree(obsArena_);
+    obsArena_ = nullptr;
+    obs_ = ObsDev{};
+    dObsOut_ = nullptr;
+    nMol_ = 0;
+    molSize_.clear();
     if (hSteps_) {
         cudaFreeHost(hSteps_);
         hSteps_ = nullptr;

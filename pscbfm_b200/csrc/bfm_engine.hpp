@@ -76,6 +76,10 @@ public:
     void cleanup();
 
     // ---- engine extensions
+    void checkSetup() const;                 // the checks initialize() makes before touching the GPU
+    void copySetup(Updater const& other);    // setter state of another (uninitialised) updater
+    uint32_t maxNeighbours() const;
+    uint64_t boxVolume() const { return (uint64_t)box_[0] * box_[1] * box_[2]; }
     void setCoordinates(int32_t const* xyz, uint32_t n);
     void getCoordinates(int32_t* xyz, uint32_t n);
     void setDrawCounter(uint64_t seed);
@@ -107,6 +111,13 @@ public:
     void noteExternalRun(uint64_t subSteps, uint64_t mcs, bool pendingMarks, uint32_t lastColor);
     uint32_t lastColor() const { return lastColor_; }
     void streamWait(cudaEvent_t e);          // orders this system's later work after e
+
+    // observables (bfm_observables.cu layout; molecules = connected components of the bonds)
+    uint32_t nMolecules() const { return nMol_; }
+    std::vector<uint32_t> moleculeSizes() const;
+    void observables(long long* out);         // computes now, copies obs_words(nMol) int64
+    void enqueueObservables(long long* dOut, cudaStream_t s);   // device buffer, no sync
+    void resetReference();                    // MSD reference := current positions
 
     // measurement
     float runTimed(int32_t nMcs);            // run + CUDA-event time on the handle's stream (ms)
@@ -167,6 +178,12 @@ private:
     uint64_t launches_ = 0;
     int repr_ = 0;
     uint32_t codeMode_ = kCodeNone;
+    uint32_t nMol_ = 0;
+    std::vector<uint32_t> molSize_;
+    void* obsArena_ = nullptr;
+    ObsDev obs_{};
+    long long* dObsOut_ = nullptr;
+    void buildObservables();
     cudaGraphExec_t graphFor(uint32_t nSteps);
     void hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, std::vector<uint32_t>& nbrr) const;
 

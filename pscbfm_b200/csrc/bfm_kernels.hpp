@@ -51,6 +51,19 @@ cudaError_t launch_resident_bc(SysDev const* dSys, uint32_t const* dList, uint32
                                StepEntry const* dSteps, uint32_t nSys, uint32_t nSteps, size_t smem, uint32_t codeMode,
                                cudaStream_t s);
 
+// Observables (bfm_observables.cu). Molecule of every slot (kNoColor for padding), first and last
+// slot of every molecule, and the reference positions for the mean squared displacement.
+struct ObsDev {
+    uint32_t const* molOfSlot;
+    uint32_t const* ends;       // [2 * nMol]
+    int32_t const* rx;
+    int32_t const* ry;
+    int32_t const* rz;
+    uint32_t nMol;
+};
+inline size_t obs_words(uint32_t nMol) { return 5ull * nMol + 512 + 1; }
+cudaError_t launch_observables(SysDev const* dSys, ObsDev const& o, long long* dOut, uint32_t npad, cudaStream_t s);
+
 // Sets the occupancy bit of every non-padding slot of system dSys[0] (lat must be zeroed).
 cudaError_t launch_build_lattice(SysDev const* dSys, uint32_t npad, cudaStream_t s);
 

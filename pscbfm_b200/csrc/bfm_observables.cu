@@ -1,0 +1,75 @@
+// int64 observables of one system, exact (no floating point on the device).
+//
+// Output layout (int64, nMol molecules = connected components of the bond graph, numbered in
+// order of their lowest monomer id):
+//   [0, 4 nMol)            per molecule: sum x, sum y, sum z, sum (x^2 + y^2 + z^2)
+//   [4 nMol, 5 nMol)       per molecule: |r_last - r_first|^2 (lowest and highest monomer id)
+//   [5 nMol, 5 nMol + 512) bond-vector histogram by bond-table index (every listed bond entry)
+//   [5 nMol + 512]         sum over monomers of |r - r_ref|^2 (r_ref: positions at the last reset)
+// Rg^2 of molecule m with n_m monomers = S2/n_m - |S1|^2/n_m^2; the host converts.
+// The reference has no observables on the device (analysis lived in LeMonADE); the CPU oracle is a
+// plain int64 recomputation from the positions.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "bfm_device.cuh"
+#include "bfm_kernels.hpp"
+
+namespace bfm {
+
+__global__ void __launch_bounds__(256) k_observables(SysDev const* __restrict__ sysv, ObsDev const o,
+                                                     long long* __restrict__ out)
+{
+    __shared__ unsigned int hist[512];
+    __shared__ long long msd;
+    SysDev const& S = sysv[0];
+    for (uint32_t b = threadIdx.x; b < 512; b += blockDim.x) hist[b] = 0;
+    if (threadIdx.x == 0) msd = 0;
+    __syncthreads();
+    long long* const mom = out;
+    long long* const ree = out + 4ull * o.nMol;
+    long long* const gh = out + 5ull * o.nMol;
+    long long* const gmsd = gh + 512;
+    long long myMsd = 0;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < S.npad; g += gridDim.x * blockDim.x) {
+        uint32_t const m = o.molOfSlot[g];
+        if (m == kNoColor) continue;   // padding slot
+        long long const x = S.x[g], y = S.y[g], z = S.z[g];
+        atomicAdd(reinterpret_cast<unsigned long long*>(mom + 4ull * m + 0), (unsigned long long)x);
+        atomicAdd(reinterpret_cast<unsigned long long*>(mom + 4ull * m + 1), (unsigned long long)y);
+        atomicAdd(reinterpret_cast<unsigned long long*>(mom + 4ull * m + 2), (unsigned long long)z);
+        atomicAdd(reinterpret_cast<unsigned long long*>(mom + 4ull * m + 3), (unsigned long long)(x * x + y * y + z * z));
+        long long const dx = x - o.rx[g], dy = y - o.ry[g], dz = z - o.rz[g];
+        myMsd += dx * dx + dy * dy + dz * dz;
+        uint32_t const nn = S.nnb[g];
+        for (uint32_t k = 0; k < nn; ++k) {
+            uint32_t const j = S.nbr[(size_t)k * S.npad + g];
+            atomicAdd(&hist[bond_index(S.x[j] - (int32_t)x, S.y[j] - (int32_t)y, S.z[j] - (int32_t)z)], 1u);
+        }
+    }
+    for (int sh = 16; sh > 0; sh >>= 1) myMsd += __shfl_down_sync(0xffffffffu, myMsd, sh);
+    if ((threadIdx.x & 31u) == 0 && myMsd) atomicAdd(reinterpret_cast<unsigned long long*>(&msd), (unsigned long long)myMsd);
+    // end-to-end vectors, one thread per molecule
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < o.nMol; m += gridDim.x * blockDim.x) {
+        uint32_t const a = o.ends[2 * m], b = o.ends[2 * m + 1];
+        long long const dx = (long long)S.x[b] - S.x[a], dy = (long long)S.y[b] - S.y[a], dz = (long long)S.z[b] - S.z[a];
+        ree[m] = dx * dx + dy * dy + dz * dz;
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < 512; b += blockDim.x)
+        if (hist[b]) atomicAdd(reinterpret_cast<unsigned long long*>(gh + b), (unsigned long long)hist[b]);
+    if (threadIdx.x == 0 && msd) atomicAdd(reinterpret_cast<unsigned long long*>(gmsd), (unsigned long long)msd);
+}
+
+cudaError_t launch_observables(SysDev const* dSys, ObsDev const& o, long long* dOut, uint32_t npad, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(dOut, 0, sizeof(long long) * obs_words(o.nMol), s);
+    if (e != cudaSuccess) return e;
+    uint32_t const grid = (npad + 255) / 256 < 1184 ? (npad + 255) / 256 : 1184;
+    k_observables<<<grid ? grid : 1, 256, 0, s>>>(dSys, o, dOut);
+    return cudaGetLastError();
+}
+
+}  // namespace bfm

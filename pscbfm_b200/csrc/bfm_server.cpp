@@ -1,0 +1,326 @@
+// Server: continuous batching of "run this system for M MCS, sample observables every k" jobs.
+//
+// Jobs are submitted from any host thread (the system is described by a handle configured with
+// the setter API; the server copies that description). A worker thread admits pending jobs in
+// arrival order while their estimated device bytes fit the budget, initialises them (colouring,
+// upload) while the current chunk of the batch runs on the GPU, and advances every running job
+// with one Batch launch sequence per chunk. A chunk ends at the nearest sample point or job end
+// of any running job, so every job samples exactly at its multiples of k; finished and cancelled
+// jobs leave between chunks and their memory is freed. Each job keeps its own draw stream, so its
+// result equals running it alone.
+//
+// Failure handling stays on the host: a malformed job fails at submit, a job larger than the
+// budget is refused, a job whose set-up throws is marked failed, and a worker that dies marks
+// every job failed and makes later calls return an error instead of hanging. No wait is unbounded.
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "bfm_engine.hpp"
+#include "bfm_server.hpp"
+
+namespace bfm {
+
+using Clock = std::chrono::steady_clock;
+
+// longest stretch of MCS the running jobs advance between two admission points
+constexpr int32_t kMaxChunkMcs = 256;
+
+struct Server::Job {
+    uint64_t id = 0;
+    int state = kJobPending;
+    std::unique_ptr<Updater> u;
+    int32_t nMcs = 0, every = 0, done = 0;
+    size_t bytes = 0;
+    Clock::time_point arrival, start, finish;
+    std::vector<long long> samples;
+    std::vector<int32_t> xyz;
+    std::string error;
+    bool cancel = false;
+};
+
+size_t Server::estimateBytes(Updater const& setup)
+{
+    // mirrors the arena of Updater::initialize (with colour-group padding slack) plus the
+    // observables arena and the step staging
+    uint64_t const n = setup.nMonomers() + 32ull * 8;
+    uint64_t const maxc = std::max<uint64_t>(setup.maxNeighbours(), 1);
+    uint64_t const V = setup.boxVolume();
+    uint64_t const perMonomer = 12 + 4 * maxc + 1 + 2 + 8 + 4 + 8 + 4 * maxc + 4 + 12;
+    return (size_t)(n * perMonomer + 3 * V / 8 + 64 * 1024 + 16 * 1024);
+}
+
+Server::Server(int gpu, size_t budgetBytes, uint32_t maxJobs) : gpu_(gpu), budget_(budgetBytes), maxJobs_(maxJobs)
+{
+    if (budgetBytes == 0) throw std::invalid_argument("[Server] zero memory budget");
+    if (maxJobs == 0) throw std::invalid_argument("[Server] zero job slots");
+    cuda_check(cudaSetDevice(gpu), "cudaSetDevice");
+    t0_ = Clock::now();
+    worker_ = std::thread([this] { workerMain(); });
+}
+
+Server::~Server()
+{
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        stop_ = true;
+    }
+    cv_.notify_all();
+    if (worker_.joinable()) worker_.join();
+}
+
+uint64_t Server::submit(Updater const& setup, int32_t nMcs, int32_t every)
+{
+    if (nMcs <= 0) throw std::invalid_argument("[Server::submit] the job needs at least one MCS");
+    if (every <= 0) throw std::invalid_argument("[Server::submit] the sample interval must be positive");
+    setup.checkSetup();   // malformed systems fail here, on the caller's thread
+    auto job = std::make_shared<Job>();
+    job->nMcs = nMcs;
+    job->every = every;
+    job->bytes = estimateBytes(setup);
+    if (job->bytes > budget_)
+        throw BudgetError("[Server::submit] the job needs about " + std::to_string(job->bytes) +
+                          " device bytes, more than the whole budget of " + std::to_string(budget_));
+    job->u.reset(new Updater(gpu_));
+    job->u->copySetup(setup);
+    std::lock_guard<std::mutex> lk(mu_);
+    if (dead_) throw std::runtime_error("[Server::submit] the server worker has stopped: " + deathReason_);
+    if (stop_) throw std::runtime_error("[Server::submit] the server is shutting down");
+    job->id = nextId_++;
+    job->arrival = Clock::now();
+    jobs_[job->id] = job;
+    pending_.push_back(job);
+    cv_.notify_all();
+    return job->id;
+}
+
+int Server::status(uint64_t id)
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    return find(id)->state;
+}
+
+void Server::cancel(uint64_t id)
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    auto j = find(id);
+    if (j->state == kJobPending) {
+        pending_.erase(std::remove(pending_.begin(), pending_.end(), j), pending_.end());
+        j->state = kJobCancelled;
+        j->u.reset();
+        j->finish = Clock::now();
+        doneCv_.notify_all();
+    } else if (j->state == kJobRunning) {
+        j->cancel = true;   // the worker removes it between chunks
+    }
+}
+
+bool Server::wait(uint64_t id, double timeoutS)
+{
+    std::unique_lock<std::mutex> lk(mu_);
+    auto j = find(id);
+    auto const deadline = Clock::now() + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(timeoutS));
+    return doneCv_.wait_until(lk, deadline, [&] { return j->state >= kJobDone; });
+}
+
+void Server::result(uint64_t id, int32_t* xyz, uint32_t n, long long* samples, uint64_t capWords, uint32_t* nSamples,
+                    double* latencyS)
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    auto j = find(id);
+    if (j->state == kJobFailed) throw std::runtime_error("[Server::result] job failed: " + j->error);
+    if (j->state == kJobCancelled) throw std::runtime_error("[Server::result] job was cancelled");
+    if (j->state != kJobDone) throw BusyError("[Server::result] job not finished");
+    if (xyz) {
+        if (n != j->xyz.size() / 3) throw std::invalid_argument("[Server::result] wrong monomer count");
+        std::memcpy(xyz, j->xyz.data(), j->xyz.size() * sizeof(int32_t));
+    }
+    if (samples) {
+        if (capWords < j->samples.size()) throw std::invalid_argument("[Server::result] sample buffer too small");
+        std::memcpy(samples, j->samples.data(), j->samples.size() * sizeof(long long));
+    }
+    if (nSamples) *nSamples = (uint32_t)(j->nMcs / j->every + (j->nMcs % j->every ? 1 : 0));
+    if (latencyS) *latencyS = std::chrono::duration<double>(j->finish - j->arrival).count();
+}
+
+void Server::stats(double out[8])
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    std::vector<double> lat;
+    double failed = 0, moves = 0;
+    for (auto const& kv : jobs_) {
+        auto const& j = kv.second;
+        if (j->state == kJobDone) {
+            lat.push_back(std::chrono::duration<double>(j->finish - j->arrival).count());
+            moves += (double)j->nMcs * (double)(j->xyz.size() / 3);
+        }
+        if (j->state == kJobFailed) failed += 1;
+    }
+    std::sort(lat.begin(), lat.end());
+    auto pct = [&](double p) {
+        if (lat.empty()) return 0.0;
+        size_t const i = std::min(lat.size() - 1, (size_t)(p * (double)lat.size()));
+        return lat[i];
+    };
+    double mean = 0;
+    for (double v : lat) mean += v;
+    out[0] = (double)lat.size();
+    out[1] = failed;
+    out[2] = moves;
+    out[3] = pct(0.50);
+    out[4] = pct(0.99);
+    out[5] = lat.empty() ? 0.0 : mean / (double)lat.size();
+    out[6] = (double)residentBytes_;
+    out[7] = std::chrono::duration<double>(Clock::now() - t0_).count();
+}
+
+void Server::injectFault(int kind)
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    fault_ = kind;
+    cv_.notify_all();
+}
+
+bool Server::dead()
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    return dead_;
+}
+
+std::shared_ptr<Server::Job> Server::find(uint64_t id)
+{
+    auto it = jobs_.find(id);
+    if (it == jobs_.end()) throw std::out_of_range("[Server] unknown job id");
+    return it->second;
+}
+
+// ------------------------------------------------------------------------------------ worker
+
+void Server::workerMain()
+{
+    try {
+        cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
+        std::vector<std::shared_ptr<Job>> active;
+        std::unique_ptr<Batch> batch;
+        bool changed = false;
+
+        auto admit = [&]() {
+            // take pending jobs in arrival order while they fit; set them up outside the lock
+            for (;;) {
+                std::shared_ptr<Job> j;
+                {
+                    std::lock_guard<std::mutex> lk(mu_);
+                    if (pending_.empty() || active.size() >= maxJobs_) return;
+                    auto const& head = pending_.front();
+                    if (residentBytes_ + head->bytes > budget_) return;
+                    j = head;
+                    pending_.pop_front();
+                    residentBytes_ += j->bytes;
+                    j->state = kJobRunning;
+                    j->start = Clock::now();
+                }
+                try {
+                    j->u->initialize();
+                    active.push_back(j);
+                    changed = true;
+                } catch (std::exception const& e) {
+                    std::lock_guard<std::mutex> lk(mu_);
+                    j->state = kJobFailed;
+                    j->error = e.what();
+                    j->finish = Clock::now();
+                    residentBytes_ -= j->bytes;
+                    j->u.reset();
+                    doneCv_.notify_all();
+                }
+            }
+        };
+
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                if (fault_ == 1) throw std::runtime_error("injected worker fault");
+                if (stop_) break;
+                if (active.empty() && pending_.empty())
+                    cv_.wait_for(lk, std::chrono::milliseconds(5));
+                if (stop_) break;
+            }
+            admit();
+            if (active.empty()) continue;
+            if (changed || !batch) {
+                std::vector<Updater*> members;
+                for (auto const& j : active) members.push_back(j->u.get());
+                batch.reset();
+                batch.reset(new Batch(gpu_, members.data(), (uint32_t)members.size()));
+                changed = false;
+            }
+            // chunks are also capped so that arrivals join and cancels take effect within a
+            // bounded amount of work
+            int32_t chunk = kMaxChunkMcs;
+            for (auto const& j : active)
+                chunk = std::min(chunk, std::min(j->every - j->done % j->every, j->nMcs - j->done));
+            batch->run(chunk);
+            admit();   // new jobs are set up on their own streams while the chunk runs
+            batch->synchronize();
+            std::vector<std::shared_ptr<Job>> keep;
+            for (auto const& j : active) {
+                j->done += chunk;
+                if (j->done % j->every == 0 || j->done == j->nMcs) {
+                    size_t const w = obs_words(j->u->nMolecules());
+                    size_t const off = j->samples.size();
+                    j->samples.resize(off + w);
+                    j->u->observables(j->samples.data() + off);
+                }
+                bool cancelled;
+                {
+                    std::lock_guard<std::mutex> lk(mu_);
+                    cancelled = j->cancel;
+                }
+                if (j->done == j->nMcs || cancelled) {
+                    std::vector<int32_t> xyz;
+                    if (!cancelled) {
+                        xyz.resize(3ull * j->u->nMonomers());
+                        j->u->getCoordinates(xyz.data(), j->u->nMonomers());
+                    }
+                    batch.reset();   // the batch references this job's device state
+                    changed = true;
+                    std::lock_guard<std::mutex> lk(mu_);
+                    j->xyz.swap(xyz);
+                    j->state = cancelled ? kJobCancelled : kJobDone;
+                    j->finish = Clock::now();
+                    residentBytes_ -= j->bytes;
+                    j->u.reset();
+                    doneCv_.notify_all();
+                } else {
+                    keep.push_back(j);
+                }
+            }
+            active.swap(keep);
+        }
+        batch.reset();
+        for (auto const& j : active) j->u.reset();
+    } catch (std::exception const& e) {
+        std::lock_guard<std::mutex> lk(mu_);
+        dead_ = true;
+        deathReason_ = e.what();
+        for (auto& kv : jobs_)
+            if (kv.second->state < kJobDone) {
+                kv.second->state = kJobFailed;
+                kv.second->error = std::string("server worker stopped: ") + e.what();
+                kv.second->finish = Clock::now();
+            }
+        pending_.clear();
+        doneCv_.notify_all();
+    }
+}
+
+}  // namespace bfm

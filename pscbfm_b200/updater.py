@@ -35,6 +35,21 @@ def counter_draw(seed: int, k: int) -> int:
     return int(_lib.load().bfm_counter_draw(seed, k))
 
 
+def decode_observables(raw: np.ndarray, sizes: np.ndarray) -> dict:
+    """Splits the int64 words of bfm_observables and derives the float observables on the host."""
+    m = len(sizes)
+    mom = raw[:4 * m].reshape(m, 4)
+    s1, s2 = mom[:, :3], mom[:, 3]
+    ree2 = raw[4 * m:5 * m]
+    hist = raw[5 * m:5 * m + 512]
+    msd_sum = int(raw[5 * m + 512])
+    n = sizes.astype(np.float64)
+    rg2 = s2 / n - (s1.astype(np.float64) ** 2).sum(axis=1) / n ** 2
+    return {"sum_r": s1, "sum_r2": s2, "ree2": ree2, "bond_hist": hist, "msd_sum": msd_sum, "sizes": sizes,
+            "rg2": rg2, "rg2_mean": float(rg2.mean()), "ree2_mean": float(ree2.mean()),
+            "msd": msd_sum / float(sizes.sum())}
+
+
 class UpdaterGPUScBFM_AB_Type:
     def __init__(self, gpu: int = 0):
         self._L = _lib.load()
@@ -181,6 +196,28 @@ class UpdaterGPUScBFM_AB_Type:
         self._call("bfm_device_bytes", C.byref(v))
         return v.value
 
+    def molecule_sizes(self) -> np.ndarray:
+        n = C.c_uint32()
+        self._call("bfm_n_molecules", C.byref(n))
+        out = np.zeros(n.value, dtype=np.uint32)
+        self._call("bfm_molecule_sizes", out, n.value)
+        return out
+
+    def observables_raw(self) -> np.ndarray:
+        """The exact int64 words of bfm_observables (layout in include/bfm.h)."""
+        n = C.c_uint32()
+        self._call("bfm_n_molecules", C.byref(n))
+        out = np.zeros(5 * n.value + 513, dtype=np.int64)
+        self._call("bfm_observables", out, out.size)
+        return out
+
+    def observables(self) -> dict:
+        """Exact sums plus the derived per-molecule Rg^2, Ree^2 and the mean squared displacement."""
+        return decode_observables(self.observables_raw(), self.molecule_sizes())
+
+    def reset_msd_reference(self):
+        self._call("bfm_reset_msd_reference")
+
     def run_timed(self, n_mcs: int) -> float:
         """Runs n_mcs MCS; returns their device time in ms (CUDA events on the engine's stream)."""
         ms = C.c_float()
@@ -281,6 +318,91 @@ class Batch:
     def close(self):
         if getattr(self, "_h", None):
             self._L.bfm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching job server (include/bfm.h, bfm_server_*)."""
+
+    PENDING, RUNNING, DONE, CANCELLED, FAILED = 0, 1, 2, 3, 4
+
+    def __init__(self, gpu: int = 0, budget_bytes: int = 150 << 30, max_jobs: int = 1024):
+        self._L = _lib.load()
+        h = C.c_void_p()
+        st = self._L.bfm_server_create(C.byref(h), gpu, budget_bytes, max_jobs)
+        if st != _lib.BFM_OK:
+            _lib.raise_for(st, self._L.bfm_server_last_error(None).decode())
+        self._h = h
+        self._sizes = {}
+
+    def _call(self, name, *args):
+        st = getattr(self._L, name)(self._h, *args)
+        if st != _lib.BFM_OK:
+            _lib.raise_for(st, self._L.bfm_server_last_error(self._h).decode())
+
+    def submit(self, system, n_mcs: int, every: int, seed: int | None = None) -> int:
+        """Queues system (a systems.BfmSystem) for n_mcs MCS with observables every `every` MCS."""
+        setup = UpdaterGPUScBFM_AB_Type(0)
+        setup.load_system(system, seed=seed, initialize=False)
+        return self.submit_setup(setup, n_mcs, every, n=system.n)
+
+    def submit_setup(self, setup: "UpdaterGPUScBFM_AB_Type", n_mcs: int, every: int, n: int) -> int:
+        job = C.c_uint64()
+        self._call("bfm_server_submit", setup.handle, n_mcs, every, C.byref(job))
+        self._sizes[job.value] = (n, n_mcs, every)
+        return job.value
+
+    @staticmethod
+    def estimate_bytes(system) -> int:
+        """Device bytes admission charges for a job on `system` (a systems.BfmSystem)."""
+        setup = UpdaterGPUScBFM_AB_Type(0)
+        setup.load_system(system, initialize=False)
+        v = C.c_uint64()
+        setup._call("bfm_server_estimate_bytes", C.byref(v))
+        setup.close()
+        return v.value
+
+    def status(self, job: int) -> int:
+        v = C.c_int()
+        self._call("bfm_server_status", job, C.byref(v))
+        return v.value
+
+    def cancel(self, job: int):
+        self._call("bfm_server_cancel", job)
+
+    def wait(self, job: int, timeout: float = 600.0):
+        self._call("bfm_server_wait", job, timeout)
+
+    def result(self, job: int, n_mol: int | None = None):
+        n, n_mcs, every = self._sizes[job]
+        xyz = np.zeros((n, 3), dtype=np.int32)
+        ns = C.c_uint32()
+        lat = C.c_double()
+        self._call("bfm_server_result", job, xyz.ctypes.data, n, None, 0, C.byref(ns), C.byref(lat))
+        samples = None
+        if n_mol is not None:
+            samples = np.zeros((ns.value, 5 * n_mol + 513), dtype=np.int64)
+            self._call("bfm_server_result", job, None, 0, samples.ctypes.data, samples.size, C.byref(ns), C.byref(lat))
+        return xyz, samples, lat.value
+
+    def stats(self) -> dict:
+        out = np.zeros(8, dtype=np.float64)
+        self._call("bfm_server_stats", out)
+        keys = ["completed", "failed", "moves", "p50_s", "p99_s", "mean_s", "resident_bytes", "elapsed_s"]
+        return dict(zip(keys, out.tolist()))
+
+    def inject_fault(self, kind: int = 1):
+        self._call("bfm_server_inject_fault", kind)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.bfm_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -224,3 +224,14 @@ def test_sequential_baseline_invariants():
     xyz, (att, acc) = O.seq_run(s, 50, seed=1)
     assert att == 50 * s.n and 0 < acc < att
     assert _ev_ok(xyz, s.box) and _bonds_ok(s, xyz)
+
+
+def test_oracle_observables_basics():
+    s = S.small_chains()
+    raw = O.observables(s, s.xyz, s.xyz)
+    m = 256
+    assert raw.size == 5 * m + 513
+    assert raw[5 * m + 512] == 0                       # no displacement
+    assert raw[5 * m:5 * m + 512].sum() == s.nbr_count.sum()
+    # straight chains of 32 with bond (2,0,0): Ree^2 = 62^2
+    assert (raw[4 * m:5 * m] == 62 ** 2).all()
