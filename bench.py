@@ -75,18 +75,35 @@ def workload_config(name, systems):
 
 # ------------------------------------------------------------------ algorithmic bytes (roofline)
 
-def check_bytes_per_move(systems, p_chk):
-    """Algorithmic bytes of one attempted move in the check kernel: own xyz 12 B, per neighbour
-    4 B id + 12 B xyz, neighbour count 1 B, flag write 1 B, 9 occupancy bits, one temporary bit
-    for a tentative move."""
+def check_bytes_per_move(systems, p_chk, code_mode):
+    """Algorithmic bytes of one attempted move in the check kernel.
+
+    Gather representation (code_mode 0): own xyz 12 B, per neighbour 4 B id + 12 B xyz, neighbour
+    count 1 B, flag write 1 B, 9 occupancy bits, one temporary bit per tentative move.
+    Bond codes (code_mode 1: 4 B words, 2: 8 B words): packed coordinate 4 B + code word, flag
+    write 1 B, the previous colour group's flag 1 B + packed coordinate 4 B (the scrub; the groups
+    are of equal size up to one monomer), 9 occupancy bits, one temporary bit set per tentative
+    move and one cleared per previous tentative move."""
     n = sum(s.n for s in systems)
     kbar = sum(int(s.nbr_count.sum()) for s in systems) / n
-    return 12 + 16 * kbar + 1 + 1 + 9 / 8 + p_chk / 8, kbar
+    if code_mode == 0:
+        return 12 + 16 * kbar + 1 + 1 + 9 / 8 + p_chk / 8, kbar
+    w = 4 if code_mode == 1 else 8
+    return 4 + w + 1 + 5 + 9 / 8 + 2 * p_chk / 8, kbar
 
 
-def sweep_bytes_per_move(kbar, p_chk, p_acc):
-    """Whole sub-step (check + perform): 12 + 16 kbar + 2 + 2.25 + 24 p_acc + 0.25 p_acc + 0.125 p_chk."""
-    return 12 + 16 * kbar + 2 + 2.25 + 24.25 * p_acc + 0.125 * p_chk
+def perform_bytes_per_move(kbar, p_chk, p_acc, code_mode):
+    """Algorithmic bytes of one attempted move in the perform kernel (bond codes): flag 1 B and
+    packed coordinate 4 B; per tentative move the code word, kbar neighbour references (4 B) and
+    9 temporary-lattice bits; per accepted move 2 lattice bits read and written, packed coordinate
+    4 B, one coordinate read+write 8 B, flag 1 B, own code word and kbar neighbour code words read
+    and written. Gather representation (code_mode 0): flag 1 B, per tentative move xyz 12 B and
+    9 temporary bits, per accepted move 2 lattice bits read and written, one coordinate 8 B, flag
+    1 B."""
+    if code_mode == 0:
+        return 1 + p_chk * (12 + 9 / 8) + p_acc * (0.5 + 8 + 1)
+    w = 4 if code_mode == 1 else 8
+    return 5 + p_chk * (w + 4 * kbar + 9 / 8) + p_acc * (0.5 + 4 + 8 + 1 + w + 2 * w * kbar)
 
 
 def measured_peaks():
@@ -347,22 +364,33 @@ def run_ours(args):
     roofline = None
     if batch is None:
         kt = u0.time_kernels(max(4, min(args.steps, 40)))
+        code_mode = u0.representation()
         nC = u0.n_colors()[0]
         att_per_launch = systems[0].n / nC
-        b_check, kbar = check_bytes_per_move(systems, p_chk)
+        b_check, kbar = check_bytes_per_move(systems, p_chk, code_mode)
+        b_perf = perform_bytes_per_move(kbar, p_chk, p_acc, code_mode)
         avg_check = kt["check_ms"] / kt["check_launches"]
         avg_perform = kt["perform_ms"] / kt["perform_launches"]
         achieved = b_check * att_per_launch / (avg_check / 1e3) / 1e9
-        key = {"dense_melt": "k_check_dense_melt256", "small": "k_check_chains64",
-               "network": "k_check_network128"}[args.workload]
+        achieved_perf = b_perf * att_per_launch / (avg_perform / 1e3) / 1e9
+        kname = "k_check" if code_mode == 0 else "k_check_bc"
+        key = kname + "_" + {"dense_melt": "dense_melt256", "small": "chains64",
+                             "network": "network128"}[args.workload]
         traffic = profiled_traffic(key)
-        roofline = {"kernel": "bfm::k_check", "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
+        roofline = {"kernel": "bfm::" + kname, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
                     "unit": "GB/s", "frac": round(achieved / hbm_peak, 4), "peak_kind": peak_kind,
                     "traffic": traffic, "algorithmic_bytes_per_launch": round(b_check * att_per_launch),
                     "bytes_per_attempted_move": round(b_check, 3), "kbar": round(kbar, 5),
-                    "avg_launch_us": round(avg_check * 1e3, 2), "perform_avg_launch_us": round(avg_perform * 1e3, 2),
-                    "sweep_bytes_per_attempted_move": round(sweep_bytes_per_move(kbar, p_chk, p_acc), 3),
-                    "note": "state is L2-resident between sub-steps; frac is against HBM copy bandwidth"}
+                    "representation": ["gather", "bond codes 32-bit", "bond codes 64-bit"][code_mode],
+                    "avg_launch_us": round(avg_check * 1e3, 2),
+                    "perform": {"kernel": "bfm::k_perform" + ("" if code_mode == 0 else "_bc"),
+                                "avg_launch_us": round(avg_perform * 1e3, 2),
+                                "bytes_per_attempted_move": round(b_perf, 3),
+                                "achieved": round(achieved_perf, 1), "frac": round(achieved_perf / hbm_peak, 4)},
+                    "timing": "CUDA events around each launch on the engine stream, one sub-step at a time",
+                    "note": ("the state (about 36 B per monomer) stays in the 126 MB L2 between launches, so "
+                             "the HBM fraction is low by construction; the kernels are bound by instruction "
+                             "issue and dependent-load latency")}
 
     # e2e through the C-ABI with host buffers: per step one bfm_run (host draws uploaded from
     # pinned memory) and a read of the step's counters; positions copied back at the end
@@ -385,9 +413,17 @@ def run_ours(args):
            "d2h_bytes_per_step": 32 * (1 if batch is None else 1) + round(12 * systems[0].n / args.steps),
            "calls": "bfm_run(1) + bfm_get_stats per step, bfm_get_coords_bulk once"}
 
+    for m in members:
+        m.validate()   # excluded volume, bonds and the device lattice after the timed run
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras and args.workload != "ensemble":
-        extras["batched_vs_plain"] = batched_vs_plain()
+        if batch is not None:
+            batch.close()
+        for m in members:
+            m.close()
+        members, batch = [], None
+        extras["batched"] = batched_vs_plain()
+        extras["served"] = served(local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -396,8 +432,6 @@ def run_ours(args):
                "sample": ("random-sequential single-monomer BFM (LeMonADE serial-updater scheme), one replica of "
                           "the workload system per core, " + ("3" if n_total > 100000 else "40") + " MCS each")}
     launches_total = reduce_sum(float(launches), world)
-    for m in members:
-        m.validate()
     if rank == 0:
         line = {"metric": "attempted monomer moves/s", "value": value, "unit": "attempted moves/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -415,28 +449,106 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def batched_vs_plain(n_systems=64, mcs=20):
-    """The first n_systems of the ensemble: the batch (one launch sequence for all) against the
-    plain path (each system alone through the per-sub-step launch path), same MCS."""
+def batched_vs_plain(n_systems=256, mcs=100, plain_mcs=20):
+    """The batched ensemble (256 systems, own seeds): the batch (one launch sequence per chunk for
+    all systems) against the plain path (each system alone through the per-sub-step launch path).
+    Both timed with CUDA events; the plain time is per system over plain_mcs MCS, scaled to mcs."""
     import pscbfm_b200 as P
     from pscbfm_b200 import systems as S
     systems = S.ensemble(n_systems=n_systems)
     n = sum(s.n for s in systems)
     members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
     b = P.Batch(members)
-    b.run(2)
-    batched = n * mcs / (b.run_timed(mcs) / 1e3)
+    b.run(3)
+    batched_ms = b.run_timed(mcs)
+    launches0 = b.launch_count()
+    b.run_timed(1)
+    launches_per_mcs = b.launch_count() - launches0
     b.close()
-    plain_t = 0.0
+    plain_ms = 0.0
     for m in members:
         m.set_mode(P.MODE_LAUNCH)
         m.run_timed(1)
-        plain_t += m.run_timed(mcs) / 1e3
-    plain = n * mcs / plain_t
+        plain_ms += m.run_timed(plain_mcs) * (mcs / plain_mcs)
     for m in members:
+        m.validate()
         m.close()
-    return {"systems": n_systems, "monomers": n, "mcs": mcs, "batched": batched, "plain": plain,
-            "ratio": batched / plain, "plain_path": "BFM_MODE_LAUNCH, one system at a time"}
+    return {"workload": "ensemble_256_systems", "systems": n_systems, "monomers": n, "mcs": mcs,
+            "batched": n * mcs / (batched_ms / 1e3), "plain": n * mcs / (plain_ms / 1e3),
+            "ratio": plain_ms / batched_ms, "batched_launches_per_mcs": launches_per_mcs,
+            "plain_path": f"BFM_MODE_LAUNCH, one system at a time, {plain_mcs} MCS each scaled to {mcs}",
+            "unit": "attempted moves/s"}
+
+
+SERVED_RATES = (10, 30, 100, 300, 1000)
+
+
+def served_jobs(n_jobs, seed=777):
+    """The served job set: systems drawn like the batched ensemble (own seeds), MCS log-uniform on
+    [1e3, 1e5], observables every 100 MCS."""
+    import numpy as np
+    from pscbfm_b200 import systems as S
+    systems = S.ensemble(n_systems=n_jobs, base_seed=50000, gen_seed=seed)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    mcs = np.exp(rng.uniform(np.log(1e3), np.log(1e5), n_jobs)).astype(np.int64)
+    return systems, [int(m) for m in mcs]
+
+
+def served(gpu=0, n_jobs=32, rates=SERVED_RATES, budget=150 << 30, every=100, plain_mcs=300):
+    """Poisson arrivals at each rate lambda into the job server (HBM budget 150 GB, observables every
+    100 MCS); latency = submit to completion on the host clock. The plain reference point runs the
+    same jobs one at a time through the per-sub-step launch path with the same observable sampling
+    (each job timed over min(MCS, plain_mcs) MCS and scaled to its MCS)."""
+    import numpy as np
+    import pscbfm_b200 as P
+    systems, mcs = served_jobs(n_jobs)
+    work = sum(s.n * m for s, m in zip(systems, mcs))
+    setups = [P.UpdaterGPUScBFM_AB_Type(gpu).load_system(s, initialize=False) for s in systems]
+    # plain: one job at a time
+    plain_s = 0.0
+    for s, m in zip(systems, mcs):
+        u = P.UpdaterGPUScBFM_AB_Type(gpu).load_system(s, mode=P.MODE_LAUNCH)
+        u.runSimulationOnGPU(1)
+        k = min(m, plain_mcs)
+        t = time.perf_counter()
+        done = 0
+        while done < k:
+            step = min(every - done % every, k - done)
+            u.runSimulationOnGPU(step)
+            done += step
+            if done % every == 0:
+                u.observables_raw()
+        plain_s += (time.perf_counter() - t) * m / k
+        u.close()
+    rows = []
+    for lam in rates:
+        rng = np.random.Generator(np.random.PCG64(int(lam)))
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, n_jobs))
+        srv = P.Server(gpu, budget_bytes=budget)
+        t0 = time.perf_counter()
+        jobs = []
+        for a, u, s, m in zip(arrivals, setups, systems, mcs):
+            dt = t0 + a - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            jobs.append(srv.submit_setup(u, m, every, n=s.n))
+        for j in jobs:
+            srv.wait(j, 900)
+        makespan = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        if st["completed"] != n_jobs:
+            raise RuntimeError(f"served: {st['completed']} of {n_jobs} jobs completed")
+        rows.append({"lambda_jobs_per_s": lam, "p50_s": round(st["p50_s"], 4), "p99_s": round(st["p99_s"], 4),
+                     "mean_s": round(st["mean_s"], 4), "makespan_s": round(makespan, 3),
+                     "moves_per_s": work / makespan, "ratio_vs_plain": plain_s / makespan})
+    for u in setups:
+        u.close()
+    return {"jobs_per_rate": n_jobs, "monomers_x_mcs": work, "every": every, "budget_bytes": budget,
+            "plain_one_at_a_time_s": plain_s, "plain_moves_per_s": work / plain_s, "rates": rows,
+            "unit": "attempted moves/s", "clock": "host wall clock, submit to completion",
+            "plain_path": f"BFM_MODE_LAUNCH one job at a time with observables every {every} MCS, "
+                          f"min(MCS, {plain_mcs}) MCS timed per job and scaled to its MCS"}
 
 
 def run_reference(args):

@@ -177,6 +177,8 @@ int bfm_batch_launch_count(bfm_batch_handle b, uint64_t* out);
 int bfm_batch_synchronize(bfm_batch_handle b);
 /* 0: every system on the grid path; 1 (default): small systems on the resident kernel. */
 int bfm_batch_set_resident(bfm_batch_handle b, int on);
+/* Member i advances mcs[i] MCS (0 = it idles); one launch sequence for all, like bfm_batch_run. */
+int bfm_batch_run_each(bfm_batch_handle b, const int32_t* mcs);
 const char* bfm_batch_last_error(bfm_batch_handle b);
 
 /* ------------------------------------------------------------------ server (no reference counterpart) */
@@ -207,6 +209,9 @@ int bfm_server_wait(bfm_server_handle s, uint64_t job, double timeout_s);
  * BFM_ERR_BUSY if the job has not finished. */
 int bfm_server_result(bfm_server_handle s, uint64_t job, int32_t* xyz, uint32_t n, int64_t* samples,
                       uint64_t capacity_words, uint32_t* n_samples, double* latency_s);
+/* out = {arrival, admission, completion} in seconds since bfm_server_create; a time not reached
+ * yet is -1. */
+int bfm_server_job_times(bfm_server_handle s, uint64_t job, double out[3]);
 /* out = {completed, failed, attempted moves of completed jobs, p50 latency s, p99 latency s,
  *        mean latency s, resident device bytes, seconds since create} */
 int bfm_server_stats(bfm_server_handle s, double out[8]);

@@ -97,6 +97,7 @@ _SIGS = {
     "bfm_batch_destroy": [H],
     "bfm_batch_run": [H, C.c_int32],
     "bfm_batch_run_async": [H, C.c_int32],
+    "bfm_batch_run_each": [H, _i32p],
     "bfm_batch_run_timed": [H, C.c_int32, C.POINTER(C.c_float)],
     "bfm_batch_synchronize": [H],
     "bfm_batch_set_resident": [H, C.c_int],
@@ -111,6 +112,7 @@ _SIGS = {
     "bfm_server_result": [H, C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint32),
                           C.POINTER(C.c_double)],
     "bfm_server_stats": [H, _f64p],
+    "bfm_server_job_times": [H, C.c_uint64, _f64p],
     "bfm_server_inject_fault": [H, C.c_int],
     "bfm_color_graph": [C.c_uint32, _u32p, _u32p, C.c_uint32,
                         np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS"), C.POINTER(C.c_uint32)],

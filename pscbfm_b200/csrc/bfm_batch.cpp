@@ -23,16 +23,8 @@ size_t up256(size_t v) { return (v + 255) & ~size_t(255); }
 
 Batch::Batch(int gpu, Updater* const* members, uint32_t n) : gpu_(gpu)
 {
-    if (n == 0) throw std::invalid_argument("[Batch] no systems");
-    for (uint32_t i = 0; i < n; ++i) {
-        Updater* u = members[i];
-        if (!u) throw std::invalid_argument("[Batch] null system");
-        if (!u->initialized()) throw std::runtime_error("[Batch] every system must be initialized");
-        if (u->gpu() != gpu) throw std::invalid_argument("[Batch] every system must live on the batch GPU");
-        for (uint32_t j = 0; j < i; ++j)
-            if (members[j] == u) throw std::invalid_argument("[Batch] a system appears twice");
-        members_.push_back(u);
-    }
+    validateMembers(members, n);
+    members_.assign(members, members + n);
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -63,8 +55,31 @@ uint32_t Batch::residentCount() const
     return n;
 }
 
+void Batch::setMembers(Updater* const* members, uint32_t n)
+{
+    validateMembers(members, n);
+    members_.assign(members, members + n);
+    built_ = false;
+}
+
+void Batch::validateMembers(Updater* const* members, uint32_t n) const
+{
+    if (n == 0) throw std::invalid_argument("[Batch] no systems");
+    for (uint32_t i = 0; i < n; ++i) {
+        Updater* u = members[i];
+        if (!u) throw std::invalid_argument("[Batch] null system");
+        if (!u->initialized()) throw std::runtime_error("[Batch] every system must be initialized");
+        if (u->gpu() != gpu_) throw std::invalid_argument("[Batch] every system must live on the batch GPU");
+        for (uint32_t j = 0; j < i; ++j)
+            if (members[j] == u) throw std::invalid_argument("[Batch] a system appears twice");
+    }
+}
+
 void Batch::rebuild()
 {
+    // the previous launches may still read the arena and the staging buffer
+    cuda_check(cudaStreamSynchronize(stream_), "batch");
+    cuda_check(cudaStreamSynchronize(stream2_), "batch");
     uint32_t const M = (uint32_t)members_.size();
     grid_.clear();
     resident_.clear();
@@ -100,9 +115,13 @@ void Batch::rebuild()
     size_t total = up256(sizeof(SysDev) * M) + up256(sizeof(StepEntry) * stepCap_ * M);
     for (auto const& g : grid_) total += up256(sizeof(TileRef) * g.tiles.size());
     for (auto const& g : resident_) total += up256(sizeof(uint32_t) * g.members.size());
-    cudaFree(arena_);
-    arena_ = nullptr;
-    cuda_check(cudaMalloc(&arena_, total), "cudaMalloc(batch)");
+    if (total > arenaBytes_) {   // grows only: membership changes reuse the arena
+        cudaFree(arena_);
+        arena_ = nullptr;
+        arenaBytes_ = 0;
+        cuda_check(cudaMalloc(&arena_, total), "cudaMalloc(batch)");
+        arenaBytes_ = total;
+    }
     char* p = static_cast<char*>(arena_);
     dSys_ = reinterpret_cast<SysDev*>(p);
     p += up256(sizeof(SysDev) * M);
@@ -123,9 +142,14 @@ void Batch::rebuild()
         cuda_check(cudaMemcpy(g.dList, g.members.data(), sizeof(uint32_t) * g.members.size(), cudaMemcpyHostToDevice),
                    "upload resident list");
     }
-    cudaFreeHost(hSteps_);
-    hSteps_ = nullptr;
-    cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * stepCap_ * M), "cudaMallocHost(batch steps)");
+    if (stepCap_ * M > hStepsCap_) {
+        cuda_check(cudaEventSynchronize(stepsFree_), "batch staging");
+        cudaFreeHost(hSteps_);
+        hSteps_ = nullptr;
+        hStepsCap_ = 0;
+        cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * stepCap_ * M * 2), "cudaMallocHost(batch steps)");
+        hStepsCap_ = stepCap_ * M * 2;
+    }
     if (graph_) {
         cudaGraphExecDestroy(graph_);
         graph_ = nullptr;
@@ -152,8 +176,16 @@ cudaError_t Batch::launchGrid(uint32_t t, uint32_t M)
 void Batch::run(int32_t nMcs)
 {
     if (nMcs <= 0) return;
-    cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
+    std::vector<int32_t> each(members_.size(), nMcs);
+    run(each.data());
+}
+
+void Batch::run(int32_t const* mcs)
+{
     uint32_t const M = (uint32_t)members_.size();
+    for (uint32_t m = 0; m < M; ++m)
+        if (mcs[m] < 0) throw std::invalid_argument("[Batch::run] negative MCS count");
+    cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
     // every member's own stream must be idle, and pending grid-path marks of members that will
     // run resident must be cleared first
     for (Updater* u : members_) u->synchronize();
@@ -166,7 +198,7 @@ void Batch::run(int32_t nMcs)
     std::vector<uint64_t> need(M);
     uint64_t T = 0;
     for (uint32_t m = 0; m < M; ++m) {
-        need[m] = (uint64_t)nMcs * members_[m]->nColors();
+        need[m] = (uint64_t)mcs[m] * members_[m]->nColors();
         T = std::max(T, need[m]);
     }
     for (uint64_t t0 = 0; t0 < T; t0 += stepCap_) {
@@ -221,7 +253,7 @@ void Batch::run(int32_t nMcs)
     }
     cuda_check(cudaEventRecord(done_, stream_), "event");
     for (uint32_t m = 0; m < M; ++m) {
-        members_[m]->noteExternalRun(need[m], (uint64_t)nMcs, !isResident_[m], members_[m]->lastColor());
+        members_[m]->noteExternalRun(need[m], (uint64_t)mcs[m], !isResident_[m], members_[m]->lastColor());
         members_[m]->streamWait(done_);
     }
 }

@@ -307,6 +307,13 @@ int bfm_server_result(bfm_server_handle s, uint64_t job, int32_t* xyz, uint32_t 
 {
     BFM_CALL(s, s->s.result(job, xyz, n, reinterpret_cast<long long*>(samples), cap, nSamples, latency));
 }
+int bfm_server_job_times(bfm_server_handle s, uint64_t job, double out[3])
+{
+    BFM_CALL(s, {
+        if (!out) throw std::invalid_argument("[bfm_server_job_times] null output");
+        s->s.jobTimes(job, out);
+    });
+}
 int bfm_server_stats(bfm_server_handle s, double out[8])
 {
     BFM_CALL(s, {
@@ -373,6 +380,14 @@ int bfm_batch_run(bfm_batch_handle b, int32_t n)
 {
     BFM_CALL(b, {
         b->b.run(n);
+        b->b.synchronize();
+    });
+}
+int bfm_batch_run_each(bfm_batch_handle b, const int32_t* mcs)
+{
+    BFM_CALL(b, {
+        if (!mcs) throw std::invalid_argument("[bfm_batch_run_each] null MCS array");
+        b->b.run(mcs);
         b->b.synchronize();
     });
 }

@@ -545,6 +545,14 @@ void Updater::enqueueObservables(long long* dOut, cudaStream_t s)
     ++launches_;
 }
 
+void Updater::observablesAsync(long long* hostPinned)
+{
+    enqueueObservables(dObsOut_, stream_);
+    cuda_check(cudaMemcpyAsync(hostPinned, dObsOut_, sizeof(long long) * obs_words(nMol_), cudaMemcpyDeviceToHost,
+                               stream_),
+               "download observables");
+}
+
 void Updater::observables(long long* out)
 {
     enqueueObservables(dObsOut_, stream_);

@@ -117,6 +117,7 @@ public:
     std::vector<uint32_t> moleculeSizes() const;
     void observables(long long* out);         // computes now, copies obs_words(nMol) int64
     void enqueueObservables(long long* dOut, cudaStream_t s);   // device buffer, no sync
+    void observablesAsync(long long* hostPinned);   // computes and copies on this system's stream, no sync
     void resetReference();                    // MSD reference := current positions
 
     // measurement
@@ -208,6 +209,9 @@ public:
     Batch(int gpu, Updater* const* members, uint32_t n);
     ~Batch();
     void run(int32_t nMcs);     // enqueue
+    void run(int32_t const* mcs);   // enqueue mcs[i] MCS of member i (0: the member idles)
+    // replaces the member list; streams, events and buffers are kept (buffers grow as needed)
+    void setMembers(Updater* const* members, uint32_t n);
     float runTimed(int32_t nMcs);   // run + CUDA-event time on the batch stream (ms)
     void synchronize();
     uint32_t size() const { return (uint32_t)members_.size(); }
@@ -236,6 +240,7 @@ private:
         size_t smem = 0;
     };
     void rebuild();
+    void validateMembers(Updater* const* members, uint32_t n) const;
     cudaError_t launchGrid(uint32_t t, uint32_t M);
     int gpu_;
     std::vector<Updater*> members_;
@@ -247,6 +252,7 @@ private:
     cudaStream_t stream_ = nullptr, stream2_ = nullptr;
     cudaEvent_t join_ = nullptr, fork_ = nullptr;
     void* arena_ = nullptr;                    // descriptors, tiles, lists, step entries
+    size_t arenaBytes_ = 0, hStepsCap_ = 0;
     SysDev* dSys_ = nullptr;                   // descriptors of all members
     StepEntry* dSteps_ = nullptr;              // [cap][members]
     StepEntry* hSteps_ = nullptr;

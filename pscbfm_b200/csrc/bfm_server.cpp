@@ -184,6 +184,16 @@ void Server::stats(double out[8])
     out[7] = std::chrono::duration<double>(Clock::now() - t0_).count();
 }
 
+void Server::jobTimes(uint64_t id, double out[3])
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    auto j = find(id);
+    auto since = [&](Clock::time_point t) { return std::chrono::duration<double>(t - t0_).count(); };
+    out[0] = since(j->arrival);
+    out[1] = j->state == kJobPending || j->start == Clock::time_point{} ? -1.0 : since(j->start);
+    out[2] = j->state >= kJobDone ? since(j->finish) : -1.0;
+}
+
 void Server::injectFault(int kind)
 {
     std::lock_guard<std::mutex> lk(mu_);
@@ -213,14 +223,22 @@ void Server::workerMain()
         std::vector<std::shared_ptr<Job>> active;
         std::unique_ptr<Batch> batch;
         bool changed = false;
+        long long* stage = nullptr;   // pinned staging of one chunk's observable samples
+        size_t stageWords = 0;
+        struct StageFree {
+            long long*& p;
+            ~StageFree() { cudaFreeHost(p); }
+        } stageFree{stage};
 
+        // jobs set up while a chunk runs; they join the batch at the next chunk boundary
+        std::vector<std::shared_ptr<Job>> incoming;
         auto admit = [&]() {
             // take pending jobs in arrival order while they fit; set them up outside the lock
             for (;;) {
                 std::shared_ptr<Job> j;
                 {
                     std::lock_guard<std::mutex> lk(mu_);
-                    if (pending_.empty() || active.size() >= maxJobs_) return;
+                    if (pending_.empty() || active.size() + incoming.size() >= maxJobs_) return;
                     auto const& head = pending_.front();
                     if (residentBytes_ + head->bytes > budget_) return;
                     j = head;
@@ -231,8 +249,7 @@ void Server::workerMain()
                 }
                 try {
                     j->u->initialize();
-                    active.push_back(j);
-                    changed = true;
+                    incoming.push_back(j);
                 } catch (std::exception const& e) {
                     std::lock_guard<std::mutex> lk(mu_);
                     j->state = kJobFailed;
@@ -255,31 +272,59 @@ void Server::workerMain()
                 if (stop_) break;
             }
             admit();
+            if (!incoming.empty()) {
+                active.insert(active.end(), incoming.begin(), incoming.end());
+                incoming.clear();
+                changed = true;
+            }
             if (active.empty()) continue;
             if (changed || !batch) {
                 std::vector<Updater*> members;
                 for (auto const& j : active) members.push_back(j->u.get());
-                batch.reset();
-                batch.reset(new Batch(gpu_, members.data(), (uint32_t)members.size()));
+                if (batch) batch->setMembers(members.data(), (uint32_t)members.size());
+                else batch.reset(new Batch(gpu_, members.data(), (uint32_t)members.size()));
                 changed = false;
             }
-            // chunks are also capped so that arrivals join and cancels take effect within a
-            // bounded amount of work
+            // The chunk ends at the nearest sample point of any running job, capped so that
+            // arrivals join and cancels take effect within a bounded amount of work. A job whose
+            // end falls inside the chunk runs only its remaining MCS and then idles, so job ends
+            // do not shorten the chunk for the others.
             int32_t chunk = kMaxChunkMcs;
-            for (auto const& j : active)
-                chunk = std::min(chunk, std::min(j->every - j->done % j->every, j->nMcs - j->done));
-            batch->run(chunk);
+            for (auto const& j : active) chunk = std::min(chunk, j->every - j->done % j->every);
+            std::vector<int32_t> mcs(active.size());
+            for (size_t i = 0; i < active.size(); ++i) mcs[i] = std::min(chunk, active[i]->nMcs - active[i]->done);
+            batch->run(mcs.data());
             admit();   // new jobs are set up on their own streams while the chunk runs
             batch->synchronize();
+            // observable samples: all computed and copied back before one wait per sampling job
+            std::vector<size_t> at(active.size(), SIZE_MAX);
+            size_t words = 0;
+            for (size_t i = 0; i < active.size(); ++i) {
+                auto const& j = active[i];
+                j->done += mcs[i];
+                if (mcs[i] > 0 && (j->done % j->every == 0 || j->done == j->nMcs)) {
+                    at[i] = words;
+                    words += obs_words(j->u->nMolecules());
+                }
+            }
+            if (words > stageWords) {
+                cudaFreeHost(stage);
+                stage = nullptr;
+                stageWords = 0;
+                cuda_check(cudaMallocHost(&stage, sizeof(long long) * words * 2), "cudaMallocHost(samples)");
+                stageWords = words * 2;
+            }
+            for (size_t i = 0; i < active.size(); ++i)
+                if (at[i] != SIZE_MAX) active[i]->u->observablesAsync(stage + at[i]);
+            for (size_t i = 0; i < active.size(); ++i)
+                if (at[i] != SIZE_MAX) {
+                    auto const& j = active[i];
+                    j->u->synchronize();
+                    size_t const w = obs_words(j->u->nMolecules());
+                    j->samples.insert(j->samples.end(), stage + at[i], stage + at[i] + w);
+                }
             std::vector<std::shared_ptr<Job>> keep;
             for (auto const& j : active) {
-                j->done += chunk;
-                if (j->done % j->every == 0 || j->done == j->nMcs) {
-                    size_t const w = obs_words(j->u->nMolecules());
-                    size_t const off = j->samples.size();
-                    j->samples.resize(off + w);
-                    j->u->observables(j->samples.data() + off);
-                }
                 bool cancelled;
                 {
                     std::lock_guard<std::mutex> lk(mu_);
@@ -291,15 +336,18 @@ void Server::workerMain()
                         xyz.resize(3ull * j->u->nMonomers());
                         j->u->getCoordinates(xyz.data(), j->u->nMonomers());
                     }
-                    batch.reset();   // the batch references this job's device state
-                    changed = true;
-                    std::lock_guard<std::mutex> lk(mu_);
-                    j->xyz.swap(xyz);
-                    j->state = cancelled ? kJobCancelled : kJobDone;
-                    j->finish = Clock::now();
-                    residentBytes_ -= j->bytes;
-                    j->u.reset();
-                    doneCv_.notify_all();
+                    changed = true;   // the batch gets its new member list before its next run
+                    std::unique_ptr<Updater> gone;
+                    {
+                        std::lock_guard<std::mutex> lk(mu_);
+                        j->xyz.swap(xyz);
+                        j->state = cancelled ? kJobCancelled : kJobDone;
+                        j->finish = Clock::now();
+                        residentBytes_ -= j->bytes;
+                        gone.swap(j->u);
+                        doneCv_.notify_all();
+                    }
+                    gone.reset();   // frees the job's device memory outside the lock
                 } else {
                     keep.push_back(j);
                 }
@@ -308,6 +356,7 @@ void Server::workerMain()
         }
         batch.reset();
         for (auto const& j : active) j->u.reset();
+        for (auto const& j : incoming) j->u.reset();
     } catch (std::exception const& e) {
         std::lock_guard<std::mutex> lk(mu_);
         dead_ = true;

@@ -302,6 +302,13 @@ class Batch:
     def run_async(self, n_mcs: int):
         self._call("bfm_batch_run_async", n_mcs)
 
+    def run_each(self, mcs):
+        """Member i advances mcs[i] MCS (0: it idles)."""
+        a = np.ascontiguousarray(mcs, dtype=np.int32)
+        if a.shape != (len(self.members),):
+            raise ValueError("one MCS count per member")
+        self._call("bfm_batch_run_each", a)
+
     def run_timed(self, n_mcs: int) -> float:
         ms = C.c_float()
         self._call("bfm_batch_run_timed", n_mcs, C.byref(ms))
@@ -396,6 +403,12 @@ class Server:
         self._call("bfm_server_stats", out)
         keys = ["completed", "failed", "moves", "p50_s", "p99_s", "mean_s", "resident_bytes", "elapsed_s"]
         return dict(zip(keys, out.tolist()))
+
+    def job_times(self, job: int) -> tuple:
+        """(arrival, admission, completion) in seconds since the server started; -1 = not yet."""
+        out = np.zeros(3, dtype=np.float64)
+        self._call("bfm_server_job_times", job, out)
+        return tuple(out.tolist())
 
     def inject_fault(self, kind: int = 1):
         self._call("bfm_server_inject_fault", kind)

@@ -169,6 +169,27 @@ def test_batch_equals_each_system_alone(resident):
         m.close()
 
 
+@pytest.mark.parametrize("resident", [True, False])
+def test_batch_uneven_mcs_per_member(resident):
+    """run_each: members advance different MCS counts (some idle) in one launch sequence, as the
+    server runs them; each trajectory stays its own."""
+    systems = S.ensemble(n_systems=8, base_seed=300) + [S.rings_and_free()]
+    members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
+    b = P.Batch(members, resident=resident)
+    plan = [[37, 0, 100, 1, 64, 65, 3, 0, 29], [5, 80, 0, 99, 1, 0, 70, 12, 29]]
+    for mcs in plan:
+        b.run_each(mcs)
+    totals = np.sum(plan, axis=0)
+    for s, m, t in zip(systems, members, totals):
+        ref, _ = O.run(s, int(t))
+        assert np.array_equal(m.get_coords(), ref), s.name
+        assert m.stats()["mcs"] == t
+        m.validate()
+    b.close()
+    for m in members:
+        m.close()
+
+
 def test_single_monomer_and_ragged_groups():
     # one free monomer, and a 33-monomer chain (groups of 17 and 16: ragged tiles)
     one = S.from_bonds((8, 8, 8), np.array([[1, 1, 1]]), np.zeros((0, 2)), seed=4)

@@ -41,10 +41,32 @@ def test_results_equal_alone_in_the_mix():
         assert np.array_equal(xyz, want_xyz), s.name
         assert np.array_equal(samples, want_samples), s.name
         assert lat > 0
+    times = [srv.job_times(j) for j in jobs]
+    assert any(s1 < f0 and s0 < f1 for (_, s0, f0) in times for (_, s1, f1) in times if f0 != f1)
     st = srv.stats()
     assert st["completed"] == len(jobs) and st["failed"] == 0
     assert st["p99_s"] >= st["p50_s"] > 0
     assert st["resident_bytes"] == 0
+    srv.close()
+
+
+def test_late_arrival_joins_running_batch():
+    import time
+    srv = P.Server(0, budget_bytes=8 << 30)
+    a = srv.submit(S.small_chains(), 20000, 1000)
+    while srv.status(a) == P.Server.PENDING:
+        time.sleep(0.001)
+    b = srv.submit(S.serpentine_chains(32, 16, 0.3, seed=9), 200, 100)
+    srv.wait(b, 120)
+    assert srv.status(a) == P.Server.RUNNING          # b was admitted and left while a ran
+    _, sa, _ = srv.job_times(a)
+    _, sb, fb = srv.job_times(b)
+    assert sa < sb < fb
+    srv.wait(a, 300)
+    fa = srv.job_times(a)[2]
+    assert fb < fa
+    want, _, _ = alone(S.serpentine_chains(32, 16, 0.3, seed=9), 200, 100)
+    assert np.array_equal(srv.result(b)[0], want)
     srv.close()
 
 
@@ -61,12 +83,15 @@ def test_budget_refusal_and_queueing():
     one = max(P.Server.estimate_bytes(s) for s in small)
     srv = P.Server(0, budget_bytes=one + one // 2)
     jobs = [srv.submit(s, 40, 10) for s in small]
-    lat = []
+    times = []
     for j in jobs:
         srv.wait(j, 120)
         assert srv.status(j) == P.Server.DONE
-        lat.append(srv.result(j)[2])
-    assert lat == sorted(lat)     # later arrivals waited for the earlier ones
+        times.append(srv.job_times(j))
+    for (a0, s0, f0), (a1, s1, f1) in zip(times, times[1:]):
+        assert a0 <= a1 and s1 >= f0    # in arrival order, each admitted after the previous left
+    for a, s, f in times:
+        assert a <= s <= f
     want, _, _ = alone(small[-1], 40, 10)
     assert np.array_equal(srv.result(jobs[-1])[0], want)
     srv.close()
