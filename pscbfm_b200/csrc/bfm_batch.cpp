@@ -2,11 +2,16 @@
 //
 // Systems whose lattices (and, in the bond-code representation, packed coordinates and bond
 // codes) fit one CTA's shared memory run in the resident kernel, one CTA per system, one launch
-// per chunk of sub-steps. The other systems share the grid-phase kernels: one check and one
-// perform launch per sub-step and representation cover the active colour group of every such
-// system at once, and a chunk of those launches is captured into a CUDA graph once and replayed.
-// The two paths run concurrently on two streams. Each system draws its own sub-steps from its own
-// stream exactly as it would alone, so its trajectory is unchanged by batching.
+// per run. The other systems share the grid-phase kernels: one check and one perform launch per
+// sub-step and representation cover the active colour group of every such system at once, and
+// chunks of those launches are captured into a CUDA graph once and replayed. Each system draws its
+// own sub-steps from its own stream exactly as it would alone, so its trajectory is unchanged by
+// batching.
+//
+// A run stages the step entries of all its sub-steps with one host-to-device copy; the resident
+// and the grid-phase launches then proceed on two streams without meeting until the run ends, and
+// the host returns as soon as the work is queued. Member streams are ordered before the run and
+// after it with events, never with host waits.
 
 #include <algorithm>
 #include <cstring>
@@ -17,7 +22,7 @@
 namespace bfm {
 
 namespace {
-constexpr uint32_t kBatchChunk = 64;      // sub-steps per staged chunk / per captured graph
+constexpr uint32_t kBatchChunk = 64;      // sub-steps per captured graph of the grid phase
 size_t up256(size_t v) { return (v + 255) & ~size_t(255); }
 }  // namespace
 
@@ -28,10 +33,8 @@ Batch::Batch(int gpu, Updater* const* members, uint32_t n) : gpu_(gpu)
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking), "cudaStreamCreate");
-    cuda_check(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "cudaEventCreate");
-    cuda_check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
-    cuda_check(cudaEventCreateWithFlags(&stepsFree_, cudaEventDisableTiming), "cudaEventCreate");
-    cuda_check(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "cudaEventCreate");
+    for (cudaEvent_t* e : {&join_, &fork_, &stepsFree_, &done_, &ready_})
+        cuda_check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
 }
 
 Batch::~Batch()
@@ -40,9 +43,11 @@ Batch::~Batch()
     if (stream_) cudaStreamSynchronize(stream_);
     if (stream2_) cudaStreamSynchronize(stream2_);
     if (graph_) cudaGraphExecDestroy(graph_);
-    cudaFree(arena_);
+    if (arena_) cudaFreeAsync(arena_, stream_);
+    if (dStepsAll_) cudaFreeAsync(dStepsAll_, stream_);
+    if (stream_) cudaStreamSynchronize(stream_);
     cudaFreeHost(hSteps_);
-    for (cudaEvent_t e : {join_, fork_, stepsFree_, done_})
+    for (cudaEvent_t e : {join_, fork_, stepsFree_, done_, ready_})
         if (e) cudaEventDestroy(e);
     if (stream_) cudaStreamDestroy(stream_);
     if (stream2_) cudaStreamDestroy(stream2_);
@@ -77,7 +82,7 @@ void Batch::validateMembers(Updater* const* members, uint32_t n) const
 
 void Batch::rebuild()
 {
-    // the previous launches may still read the arena and the staging buffer
+    // the previous launches may still read the arena
     cuda_check(cudaStreamSynchronize(stream_), "batch");
     cuda_check(cudaStreamSynchronize(stream2_), "batch");
     uint32_t const M = (uint32_t)members_.size();
@@ -116,40 +121,37 @@ void Batch::rebuild()
     for (auto const& g : grid_) total += up256(sizeof(TileRef) * g.tiles.size());
     for (auto const& g : resident_) total += up256(sizeof(uint32_t) * g.members.size());
     if (total > arenaBytes_) {   // grows only: membership changes reuse the arena
-        cudaFree(arena_);
+        if (arena_) cuda_check(cudaFreeAsync(arena_, stream_), "cudaFreeAsync(batch)");
         arena_ = nullptr;
         arenaBytes_ = 0;
-        cuda_check(cudaMalloc(&arena_, total), "cudaMalloc(batch)");
-        arenaBytes_ = total;
+        cuda_check(cudaMallocAsync(&arena_, total * 2, stream_), "cudaMallocAsync(batch)");
+        arenaBytes_ = total * 2;
     }
     char* p = static_cast<char*>(arena_);
     dSys_ = reinterpret_cast<SysDev*>(p);
     p += up256(sizeof(SysDev) * M);
-    dSteps_ = reinterpret_cast<StepEntry*>(p);
+    dWindow_ = reinterpret_cast<StepEntry*>(p);
     p += up256(sizeof(StepEntry) * stepCap_ * M);
     std::vector<SysDev> descs(M);
     for (uint32_t m = 0; m < M; ++m) descs[m] = members_[m]->desc();
-    cuda_check(cudaMemcpy(dSys_, descs.data(), sizeof(SysDev) * M, cudaMemcpyHostToDevice), "upload descriptors");
+    cuda_check(cudaMemcpyAsync(dSys_, descs.data(), sizeof(SysDev) * M, cudaMemcpyHostToDevice, stream_),
+               "upload descriptors");
     for (auto& g : grid_) {
         g.dTiles = reinterpret_cast<TileRef*>(p);
         p += up256(sizeof(TileRef) * g.tiles.size());
-        cuda_check(cudaMemcpy(g.dTiles, g.tiles.data(), sizeof(TileRef) * g.tiles.size(), cudaMemcpyHostToDevice),
+        cuda_check(cudaMemcpyAsync(g.dTiles, g.tiles.data(), sizeof(TileRef) * g.tiles.size(), cudaMemcpyHostToDevice,
+                                   stream_),
                    "upload tiles");
     }
     for (auto& g : resident_) {
         g.dList = reinterpret_cast<uint32_t*>(p);
         p += up256(sizeof(uint32_t) * g.members.size());
-        cuda_check(cudaMemcpy(g.dList, g.members.data(), sizeof(uint32_t) * g.members.size(), cudaMemcpyHostToDevice),
+        cuda_check(cudaMemcpyAsync(g.dList, g.members.data(), sizeof(uint32_t) * g.members.size(),
+                                   cudaMemcpyHostToDevice, stream_),
                    "upload resident list");
     }
-    if (stepCap_ * M > hStepsCap_) {
-        cuda_check(cudaEventSynchronize(stepsFree_), "batch staging");
-        cudaFreeHost(hSteps_);
-        hSteps_ = nullptr;
-        hStepsCap_ = 0;
-        cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * stepCap_ * M * 2), "cudaMallocHost(batch steps)");
-        hStepsCap_ = stepCap_ * M * 2;
-    }
+    // the host vectors above die with this call: finish their copies now
+    cuda_check(cudaStreamSynchronize(stream_), "batch uploads");
     if (graph_) {
         cudaGraphExecDestroy(graph_);
         graph_ = nullptr;
@@ -157,9 +159,8 @@ void Batch::rebuild()
     built_ = true;
 }
 
-cudaError_t Batch::launchGrid(uint32_t t, uint32_t M)
+cudaError_t Batch::launchGrid(StepEntry const* e)
 {
-    StepEntry const* e = dSteps_ + (size_t)t * M;
     SysDev const unused{};   // multi-system launches read each CTA's descriptor from dSys_
     for (auto const& g : grid_) {
         uint32_t const n = (uint32_t)g.tiles.size();
@@ -186,14 +187,15 @@ void Batch::run(int32_t const* mcs)
     for (uint32_t m = 0; m < M; ++m)
         if (mcs[m] < 0) throw std::invalid_argument("[Batch::run] negative MCS count");
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
-    // every member's own stream must be idle, and pending grid-path marks of members that will
-    // run resident must be cleared first
-    for (Updater* u : members_) u->synchronize();
     if (!built_) rebuild();
+    // pending grid-path marks of members that run resident are cleared on their own streams; then
+    // the batch waits for every member stream (uploads, scrubs, observables) on the device
     for (uint32_t m = 0; m < M; ++m)
         if (isResident_[m]) members_[m]->scrubPending(members_[m]->stream());
-    for (uint32_t m = 0; m < M; ++m)
-        if (isResident_[m]) members_[m]->synchronize();
+    for (Updater* u : members_) {
+        cuda_check(cudaEventRecord(ready_, u->stream()), "event");
+        cuda_check(cudaStreamWaitEvent(stream_, ready_, 0), "wait");
+    }
 
     std::vector<uint64_t> need(M);
     uint64_t T = 0;
@@ -201,50 +203,76 @@ void Batch::run(int32_t const* mcs)
         need[m] = (uint64_t)mcs[m] * members_[m]->nColors();
         T = std::max(T, need[m]);
     }
-    for (uint64_t t0 = 0; t0 < T; t0 += stepCap_) {
-        uint32_t const chunk = (uint32_t)std::min<uint64_t>(stepCap_, T - t0);
+    if (T > 0) {
+        size_t const entries = (size_t)T * M;
+        // the previous run's copy has read the host staging once stepsFree_ has passed
         cuda_check(cudaEventSynchronize(stepsFree_), "batch staging");
-        for (uint32_t t = 0; t < chunk; ++t)
+        if (entries > hStepsCap_) {
+            cudaFreeHost(hSteps_);
+            hSteps_ = nullptr;
+            hStepsCap_ = 0;
+            cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * entries * 2), "cudaMallocHost(batch steps)");
+            hStepsCap_ = entries * 2;
+        }
+        if (entries > dStepsCap_) {
+            if (dStepsAll_) cuda_check(cudaFreeAsync(dStepsAll_, stream_), "cudaFreeAsync(batch steps)");
+            dStepsAll_ = nullptr;
+            dStepsCap_ = 0;
+            cuda_check(cudaMallocAsync(&dStepsAll_, sizeof(StepEntry) * entries * 2, stream_),
+                       "cudaMallocAsync(batch steps)");
+            dStepsCap_ = entries * 2;
+        }
+        for (uint64_t t = 0; t < T; ++t)
             for (uint32_t m = 0; m < M; ++m) {
                 StepEntry& e = hSteps_[(size_t)t * M + m];
-                if (t0 + t < need[m]) e = members_[m]->nextStep();
+                if (t < need[m]) e = members_[m]->nextStep();
                 else e = StepEntry{kNoColor, 0u, 0u, kNoColor, 0u, 0u, 0u, 0u};
             }
-        cuda_check(cudaMemcpyAsync(dSteps_, hSteps_, sizeof(StepEntry) * chunk * M, cudaMemcpyHostToDevice, stream_),
+        cuda_check(cudaMemcpyAsync(dStepsAll_, hSteps_, sizeof(StepEntry) * entries, cudaMemcpyHostToDevice, stream_),
                    "batch steps H2D");
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         if (!resident_.empty()) {
+            // one launch per group for the whole run, on the second stream
             cuda_check(cudaEventRecord(fork_, stream_), "event");
             cuda_check(cudaStreamWaitEvent(stream2_, fork_, 0), "wait");
             for (auto const& g : resident_) {
                 cuda_check(g.codeMode == kCodeNone
-                               ? launch_resident(dSys_, g.dList, (uint32_t)g.members.size(), g.perThread, dSteps_, M,
-                                                 chunk, g.smem, stream2_)
-                               : launch_resident_bc(dSys_, g.dList, (uint32_t)g.members.size(), g.perThread, dSteps_,
-                                                    M, chunk, g.smem, g.codeMode, stream2_),
+                               ? launch_resident(dSys_, g.dList, (uint32_t)g.members.size(), g.perThread, dStepsAll_,
+                                                 M, (uint32_t)T, g.smem, stream2_)
+                               : launch_resident_bc(dSys_, g.dList, (uint32_t)g.members.size(), g.perThread,
+                                                    dStepsAll_, M, (uint32_t)T, g.smem, g.codeMode, stream2_),
                            "batch resident");
                 ++launches_;
             }
         }
         if (!grid_.empty()) {
-            if (chunk == stepCap_) {
-                if (!graph_) {
-                    cudaGraph_t g;
-                    cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
-                    cudaError_t err = cudaSuccess;
-                    for (uint32_t t = 0; t < stepCap_ && err == cudaSuccess; ++t) err = launchGrid(t, M);
-                    cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
-                    cuda_check(err, "capture batch launches");
-                    cuda_check(endErr, "end capture");
-                    cudaError_t const ie = cudaGraphInstantiate(&graph_, g, 0);
-                    cudaGraphDestroy(g);
-                    cuda_check(ie, "graph instantiate");
+            for (uint64_t t0 = 0; t0 < T; t0 += stepCap_) {
+                uint32_t const chunk = (uint32_t)std::min<uint64_t>(stepCap_, T - t0);
+                if (chunk == stepCap_) {
+                    // the captured graph reads its entries from the window
+                    cuda_check(cudaMemcpyAsync(dWindow_, dStepsAll_ + t0 * M, sizeof(StepEntry) * stepCap_ * M,
+                                               cudaMemcpyDeviceToDevice, stream_),
+                               "batch window");
+                    if (!graph_) {
+                        cudaGraph_t g;
+                        cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+                        cudaError_t err = cudaSuccess;
+                        for (uint32_t t = 0; t < stepCap_ && err == cudaSuccess; ++t)
+                            err = launchGrid(dWindow_ + (size_t)t * M);
+                        cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
+                        cuda_check(err, "capture batch launches");
+                        cuda_check(endErr, "end capture");
+                        cudaError_t const ie = cudaGraphInstantiate(&graph_, g, 0);
+                        cudaGraphDestroy(g);
+                        cuda_check(ie, "graph instantiate");
+                    }
+                    cuda_check(cudaGraphLaunch(graph_, stream_), "batch graph launch");
+                } else {
+                    for (uint32_t t = 0; t < chunk; ++t)
+                        cuda_check(launchGrid(dStepsAll_ + (t0 + t) * M), "batch grid launch");
                 }
-                cuda_check(cudaGraphLaunch(graph_, stream_), "batch graph launch");
-            } else {
-                for (uint32_t t = 0; t < chunk; ++t) cuda_check(launchGrid(t, M), "batch grid launch");
+                launches_ += 2ull * chunk * grid_.size();
             }
-            launches_ += 2ull * chunk * grid_.size();
         }
         if (!resident_.empty()) {
             cuda_check(cudaEventRecord(join_, stream2_), "event");

@@ -334,7 +334,8 @@ void Updater::initialize()
     size_t const oPlane = take(8ull * 768), oMoveOk = take(512);
     Device d;
     d.bytes = off;
-    cuda_check(cudaMalloc(&d.arena, off), "cudaMalloc(system arena)");
+    // stream-ordered: freeing it later does not wait for the whole device
+    cuda_check(cudaMallocAsync(&d.arena, off, stream_), "cudaMallocAsync(system arena)");
     char* base = static_cast<char*>(d.arena);
     dev_ = d;
     SysDev& h = dev_.h;
@@ -407,11 +408,8 @@ void Updater::initialize()
     cuda_check(cudaMemsetAsync(h.stats, 0, kStatBytes, s), "memset stats");
     cuda_check(cudaMemcpyAsync(dev_.dDesc, &h, sizeof(SysDev), cudaMemcpyHostToDevice, s), "upload descriptor");
     cuda_check(cudaMemsetAsync(dev_.dList, 0, 4, s), "memset list");
-    if (!hSteps_) {
-        cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * kStepCap), "cudaMallocHost(steps)");
-        hStepCap_ = kStepCap;
-    }
     if (!stepsFree_) cuda_check(cudaEventCreateWithFlags(&stepsFree_, cudaEventDisableTiming), "cudaEventCreate");
+    if (!batchOnly_) ensureStaging();
     cuda_check(cudaStreamSynchronize(s), "initialize");
     buildObservables();
     subStep_ = 0;
@@ -504,7 +502,7 @@ void Updater::buildObservables()
     };
     size_t const oMol = take(4ull * npad_), oEnds = take(8ull * nMol_), oR = take(12ull * npad_);
     size_t const oOut = take(sizeof(long long) * obs_words(nMol_));
-    cuda_check(cudaMalloc(&obsArena_, off), "cudaMalloc(observables)");
+    cuda_check(cudaMallocAsync(&obsArena_, off, stream_), "cudaMallocAsync(observables)");
     char* base = static_cast<char*>(obsArena_);
     obs_.molOfSlot = reinterpret_cast<uint32_t*>(base + oMol);
     obs_.ends = reinterpret_cast<uint32_t*>(base + oEnds);
@@ -673,9 +671,19 @@ void Updater::fillSteps(uint32_t nSteps, StepEntry* buf, bool)
     for (uint32_t t = 0; t < nSteps; ++t) buf[t] = nextStep();
 }
 
+void Updater::ensureStaging()
+{
+    // pinned staging of the step entries, allocated on the first run of this system's own paths
+    // (systems advanced only by a Batch never need it)
+    if (hSteps_) return;
+    cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * kStepCap), "cudaMallocHost(steps)");
+    hStepCap_ = kStepCap;
+}
+
 void Updater::scrubPending(cudaStream_t s)
 {
     if (lastColor_ == kNoColor) return;
+    ensureStaging();
     // a perform launch with no current colour only zeroes the previous sub-step's marks
     cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
     hSteps_[0] = StepEntry{kNoColor, 0u, (uint32_t)(subStep_ & 1u), lastColor_, 0u, 0u, grpOff_[lastColor_],
@@ -779,6 +787,7 @@ void Updater::timeKernels(int32_t nMcs, double out[4])
     // it runs on; sums per kernel
     requireInit("timeKernels");
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
+    ensureStaging();
     scrubPending(stream_);
     uint32_t const nSteps = (uint32_t)nMcs * (uint32_t)grpSize_.size();
     std::vector<cudaEvent_t> ev(3);
@@ -850,6 +859,7 @@ void Updater::run(int32_t nMcs)
     uint64_t const total = (uint64_t)nMcs * grpSize_.size();
     if (total > 0xFFFFFFFFull) throw std::invalid_argument("[runSimulationOnGPU] too many sub-steps in one call");
     uint32_t const nSteps = (uint32_t)total;
+    ensureStaging();
     int m = mode_;
     if (m == kModeAuto) m = residentEligible() ? kModeResident : kModeGraph;
     if (m == kModeResident && !residentEligible()) m = kModeGraph;
@@ -1040,15 +1050,17 @@ void Updater::validate()
 
 void Updater::freeDevice()
 {
+    if (!graphs_.empty() && stream_) cudaStreamSynchronize(stream_);   // no graph of ours in flight
     for (auto& g : graphs_) cudaGraphExecDestroy(g.second);
     graphs_.clear();
+    // stream-ordered frees: after this system's queued work (and whatever its stream waits on,
+    // such as the end of a Batch run), without waiting on the host or for other streams
     if (dev_.arena) {
         cudaSetDevice(gpu_);
-        if (stream_) cudaStreamSynchronize(stream_);
-        cudaFree(dev_.arena);
+        cudaFreeAsync(dev_.arena, stream_);
     }
     dev_ = Device{};
-    if (obsArena_) cudaFree(obsArena_);
+    if (obsArena_) cudaFreeAsync(obsArena_, stream_);
     obsArena_ = nullptr;
     obs_ = ObsDev{};
     dObsOut_ = nullptr;

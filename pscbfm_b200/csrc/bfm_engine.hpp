@@ -85,6 +85,9 @@ public:
     void setDrawCounter(uint64_t seed);
     void setDrawCallback(DrawFn fn, void* ctx);
     void setMode(int mode);
+    // a system that only a Batch advances skips the pinned staging of its own run paths
+    // (allocated on first use if it runs alone after all)
+    void setBatchOnly(bool on) { batchOnly_ = on; }
     int mode() const { return mode_; }
     void run(int32_t nMcs);                  // enqueue only
     void synchronize();
@@ -144,6 +147,7 @@ private:
     void enqueueResident(uint32_t nSteps);
     void fillSteps(uint32_t nSteps, StepEntry* hostBuf, bool residentParity);
     void freeDevice();
+    void ensureStaging();
 
     int gpu_ = 0;
     cudaStream_t stream_ = nullptr;
@@ -162,6 +166,7 @@ private:
     DrawFn drawFn_ = nullptr;
     void* drawCtx_ = nullptr;
     int mode_ = kModeAuto;
+    bool batchOnly_ = false;
 
     // after initialize
     std::vector<uint8_t> colour_;
@@ -241,7 +246,7 @@ private:
     };
     void rebuild();
     void validateMembers(Updater* const* members, uint32_t n) const;
-    cudaError_t launchGrid(uint32_t t, uint32_t M);
+    cudaError_t launchGrid(StepEntry const* e);   // one sub-step of every grid group, entries [members]
     int gpu_;
     std::vector<Updater*> members_;
     std::vector<char> isResident_;
@@ -250,12 +255,13 @@ private:
     bool residentOn_ = true;
     bool built_ = false;
     cudaStream_t stream_ = nullptr, stream2_ = nullptr;
-    cudaEvent_t join_ = nullptr, fork_ = nullptr;
-    void* arena_ = nullptr;                    // descriptors, tiles, lists, step entries
-    size_t arenaBytes_ = 0, hStepsCap_ = 0;
+    cudaEvent_t join_ = nullptr, fork_ = nullptr, ready_ = nullptr;
+    void* arena_ = nullptr;                    // descriptors, graph window, tiles, lists
+    size_t arenaBytes_ = 0, hStepsCap_ = 0, dStepsCap_ = 0;
     SysDev* dSys_ = nullptr;                   // descriptors of all members
-    StepEntry* dSteps_ = nullptr;              // [cap][members]
-    StepEntry* hSteps_ = nullptr;
+    StepEntry* dWindow_ = nullptr;             // [stepCap_][members]: entries the captured graph reads
+    StepEntry* dStepsAll_ = nullptr;           // [sub-steps of the run][members]
+    StepEntry* hSteps_ = nullptr;              // pinned staging of dStepsAll_
     size_t stepCap_ = 0;
     cudaEvent_t stepsFree_ = nullptr;
     cudaEvent_t done_ = nullptr;

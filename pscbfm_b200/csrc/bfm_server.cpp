@@ -2,12 +2,16 @@
 //
 // Jobs are submitted from any host thread (the system is described by a handle configured with
 // the setter API; the server copies that description). A worker thread admits pending jobs in
-// arrival order while their estimated device bytes fit the budget, initialises them (colouring,
-// upload) while the current chunk of the batch runs on the GPU, and advances every running job
-// with one Batch launch sequence per chunk. A chunk ends at the nearest sample point or job end
-// of any running job, so every job samples exactly at its multiples of k; finished and cancelled
-// jobs leave between chunks and their memory is freed. Each job keeps its own draw stream, so its
-// result equals running it alone.
+// arrival order while their estimated device bytes fit the budget and initialises them
+// (colouring, upload) while the GPU runs the others. Running jobs are grouped into lanes by how
+// they run: one lane for the systems on the grid-phase kernels and one per size class of the
+// systems that fit one CTA (resident kernel). Each lane is a Batch advanced in chunks on its own
+// streams; the lanes run concurrently and the worker services whichever lane finishes a chunk
+// first, so small jobs never wait for the chunks of large ones. A chunk ends at the nearest sample
+// point of the lane's jobs (capped at kMaxChunkMcs), so every job samples exactly at its
+// multiples of k; a job whose end falls inside a chunk runs only its remaining MCS. Finished and
+// cancelled jobs leave between chunks and their memory is freed in stream order. Each job keeps
+// its own draw stream, so its result equals running it alone.
 //
 // Failure handling stays on the host: a malformed job fails at submit, a job larger than the
 // budget is refused, a job whose set-up throws is marked failed, and a worker that dies marks
@@ -33,8 +37,10 @@ namespace bfm {
 
 using Clock = std::chrono::steady_clock;
 
-// longest stretch of MCS the running jobs advance between two admission points
+// longest stretch of MCS a lane advances between two admission points
 constexpr int32_t kMaxChunkMcs = 256;
+// lane of the systems on the grid-phase kernels; resident lanes are 0..4 (log2 monomers per thread)
+constexpr int kGridLane = 100;
 
 struct Server::Job {
     uint64_t id = 0;
@@ -65,6 +71,12 @@ Server::Server(int gpu, size_t budgetBytes, uint32_t maxJobs) : gpu_(gpu), budge
     if (budgetBytes == 0) throw std::invalid_argument("[Server] zero memory budget");
     if (maxJobs == 0) throw std::invalid_argument("[Server] zero job slots");
     cuda_check(cudaSetDevice(gpu), "cudaSetDevice");
+    // jobs allocate from the device's stream-ordered pool; keep up to the budget in the pool
+    // between jobs instead of returning it to the driver at every synchronisation (this process only)
+    cudaMemPool_t pool;
+    cuda_check(cudaDeviceGetDefaultMemPool(&pool, gpu), "cudaDeviceGetDefaultMemPool");
+    uint64_t keep = budgetBytes;
+    cuda_check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
     t0_ = Clock::now();
     worker_ = std::thread([this] { workerMain(); });
 }
@@ -93,6 +105,7 @@ uint64_t Server::submit(Updater const& setup, int32_t nMcs, int32_t every)
                           " device bytes, more than the whole budget of " + std::to_string(budget_));
     job->u.reset(new Updater(gpu_));
     job->u->copySetup(setup);
+    job->u->setBatchOnly(true);
     std::lock_guard<std::mutex> lk(mu_);
     if (dead_) throw std::runtime_error("[Server::submit] the server worker has stopped: " + deathReason_);
     if (stop_) throw std::runtime_error("[Server::submit] the server is shutting down");
@@ -216,13 +229,38 @@ std::shared_ptr<Server::Job> Server::find(uint64_t id)
 
 // ------------------------------------------------------------------------------------ worker
 
+namespace {
+
+// the lane a freshly initialised system runs in
+int lane_of(Updater const& u)
+{
+    if (!u.residentEligible()) return kGridLane;
+    int c = 0;
+    while ((kResidentBlock << c) < u.maxGroup()) ++c;
+    return c;
+}
+
+}  // namespace
+
+struct Server::Lane {
+    std::vector<std::shared_ptr<Job>> jobs;       // members of the batch, in batch order
+    std::vector<std::shared_ptr<Job>> incoming;   // initialised, join at the next chunk
+    std::unique_ptr<Batch> batch;
+    std::vector<int32_t> mcs;                     // MCS of each member in the chunk in flight
+    bool changed = false, inFlight = false;
+    cudaEvent_t done = nullptr;
+    ~Lane()
+    {
+        batch.reset();   // waits for its own streams
+        if (done) cudaEventDestroy(done);
+    }
+};
+
 void Server::workerMain()
 {
     try {
         cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
-        std::vector<std::shared_ptr<Job>> active;
-        std::unique_ptr<Batch> batch;
-        bool changed = false;
+        std::map<int, Lane> lanes;
         long long* stage = nullptr;   // pinned staging of one chunk's observable samples
         size_t stageWords = 0;
         struct StageFree {
@@ -230,17 +268,27 @@ void Server::workerMain()
             ~StageFree() { cudaFreeHost(p); }
         } stageFree{stage};
 
-        // jobs set up while a chunk runs; they join the batch at the next chunk boundary
-        std::vector<std::shared_ptr<Job>> incoming;
+        auto running = [&]() {
+            size_t n = 0;
+            for (auto const& kv : lanes) n += kv.second.jobs.size() + kv.second.incoming.size();
+            return n;
+        };
+        auto checkFault = [&]() {
+            std::lock_guard<std::mutex> lk(mu_);
+            if (fault_ == 1) throw std::runtime_error("injected worker fault");
+            return stop_;
+        };
+
+        // take pending jobs in arrival order while they fit; set them up outside the lock
         auto admit = [&]() {
-            // take pending jobs in arrival order while they fit; set them up outside the lock
+            bool any = false;
             for (;;) {
                 std::shared_ptr<Job> j;
                 {
                     std::lock_guard<std::mutex> lk(mu_);
-                    if (pending_.empty() || active.size() + incoming.size() >= maxJobs_) return;
+                    if (pending_.empty() || running() >= maxJobs_) return any;
                     auto const& head = pending_.front();
-                    if (residentBytes_ + head->bytes > budget_) return;
+                    if (residentBytes_ + head->bytes > budget_) return any;
                     j = head;
                     pending_.pop_front();
                     residentBytes_ += j->bytes;
@@ -249,7 +297,8 @@ void Server::workerMain()
                 }
                 try {
                     j->u->initialize();
-                    incoming.push_back(j);
+                    lanes[lane_of(*j->u)].incoming.push_back(j);
+                    any = true;
                 } catch (std::exception const& e) {
                     std::lock_guard<std::mutex> lk(mu_);
                     j->state = kJobFailed;
@@ -262,47 +311,39 @@ void Server::workerMain()
             }
         };
 
-        for (;;) {
-            {
-                std::unique_lock<std::mutex> lk(mu_);
-                if (fault_ == 1) throw std::runtime_error("injected worker fault");
-                if (stop_) break;
-                if (active.empty() && pending_.empty())
-                    cv_.wait_for(lk, std::chrono::milliseconds(5));
-                if (stop_) break;
+        auto launch = [&](Lane& L) {
+            if (!L.incoming.empty()) {
+                L.jobs.insert(L.jobs.end(), L.incoming.begin(), L.incoming.end());
+                L.incoming.clear();
+                L.changed = true;
             }
-            admit();
-            if (!incoming.empty()) {
-                active.insert(active.end(), incoming.begin(), incoming.end());
-                incoming.clear();
-                changed = true;
-            }
-            if (active.empty()) continue;
-            if (changed || !batch) {
+            if (L.jobs.empty()) return;
+            if (L.changed || !L.batch) {
                 std::vector<Updater*> members;
-                for (auto const& j : active) members.push_back(j->u.get());
-                if (batch) batch->setMembers(members.data(), (uint32_t)members.size());
-                else batch.reset(new Batch(gpu_, members.data(), (uint32_t)members.size()));
-                changed = false;
+                for (auto const& j : L.jobs) members.push_back(j->u.get());
+                if (L.batch) L.batch->setMembers(members.data(), (uint32_t)members.size());
+                else L.batch.reset(new Batch(gpu_, members.data(), (uint32_t)members.size()));
+                L.changed = false;
             }
-            // The chunk ends at the nearest sample point of any running job, capped so that
-            // arrivals join and cancels take effect within a bounded amount of work. A job whose
-            // end falls inside the chunk runs only its remaining MCS and then idles, so job ends
-            // do not shorten the chunk for the others.
+            if (!L.done) cuda_check(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming), "cudaEventCreate");
             int32_t chunk = kMaxChunkMcs;
-            for (auto const& j : active) chunk = std::min(chunk, j->every - j->done % j->every);
-            std::vector<int32_t> mcs(active.size());
-            for (size_t i = 0; i < active.size(); ++i) mcs[i] = std::min(chunk, active[i]->nMcs - active[i]->done);
-            batch->run(mcs.data());
-            admit();   // new jobs are set up on their own streams while the chunk runs
-            batch->synchronize();
+            for (auto const& j : L.jobs) chunk = std::min(chunk, j->every - j->done % j->every);
+            L.mcs.resize(L.jobs.size());
+            for (size_t i = 0; i < L.jobs.size(); ++i) L.mcs[i] = std::min(chunk, L.jobs[i]->nMcs - L.jobs[i]->done);
+            L.batch->run(L.mcs.data());
+            cuda_check(cudaEventRecord(L.done, L.batch->stream()), "event");
+            L.inFlight = true;
+        };
+
+        auto complete = [&](Lane& L) {
+            L.inFlight = false;
             // observable samples: all computed and copied back before one wait per sampling job
-            std::vector<size_t> at(active.size(), SIZE_MAX);
+            std::vector<size_t> at(L.jobs.size(), SIZE_MAX);
             size_t words = 0;
-            for (size_t i = 0; i < active.size(); ++i) {
-                auto const& j = active[i];
-                j->done += mcs[i];
-                if (mcs[i] > 0 && (j->done % j->every == 0 || j->done == j->nMcs)) {
+            for (size_t i = 0; i < L.jobs.size(); ++i) {
+                auto const& j = L.jobs[i];
+                j->done += L.mcs[i];
+                if (L.mcs[i] > 0 && (j->done % j->every == 0 || j->done == j->nMcs)) {
                     at[i] = words;
                     words += obs_words(j->u->nMolecules());
                 }
@@ -314,17 +355,17 @@ void Server::workerMain()
                 cuda_check(cudaMallocHost(&stage, sizeof(long long) * words * 2), "cudaMallocHost(samples)");
                 stageWords = words * 2;
             }
-            for (size_t i = 0; i < active.size(); ++i)
-                if (at[i] != SIZE_MAX) active[i]->u->observablesAsync(stage + at[i]);
-            for (size_t i = 0; i < active.size(); ++i)
+            for (size_t i = 0; i < L.jobs.size(); ++i)
+                if (at[i] != SIZE_MAX) L.jobs[i]->u->observablesAsync(stage + at[i]);
+            for (size_t i = 0; i < L.jobs.size(); ++i)
                 if (at[i] != SIZE_MAX) {
-                    auto const& j = active[i];
+                    auto const& j = L.jobs[i];
                     j->u->synchronize();
                     size_t const w = obs_words(j->u->nMolecules());
                     j->samples.insert(j->samples.end(), stage + at[i], stage + at[i] + w);
                 }
             std::vector<std::shared_ptr<Job>> keep;
-            for (auto const& j : active) {
+            for (auto const& j : L.jobs) {
                 bool cancelled;
                 {
                     std::lock_guard<std::mutex> lk(mu_);
@@ -336,7 +377,7 @@ void Server::workerMain()
                         xyz.resize(3ull * j->u->nMonomers());
                         j->u->getCoordinates(xyz.data(), j->u->nMonomers());
                     }
-                    changed = true;   // the batch gets its new member list before its next run
+                    L.changed = true;   // the batch gets its new member list before its next run
                     std::unique_ptr<Updater> gone;
                     {
                         std::lock_guard<std::mutex> lk(mu_);
@@ -347,16 +388,52 @@ void Server::workerMain()
                         gone.swap(j->u);
                         doneCv_.notify_all();
                     }
-                    gone.reset();   // frees the job's device memory outside the lock
+                    gone.reset();   // frees the job's device memory in stream order, outside the lock
                 } else {
                     keep.push_back(j);
                 }
             }
-            active.swap(keep);
+            L.jobs.swap(keep);
+        };
+
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                if (fault_ == 1) throw std::runtime_error("injected worker fault");
+                if (stop_) break;
+                if (running() == 0 && pending_.empty()) cv_.wait_for(lk, std::chrono::milliseconds(5));
+                if (stop_) break;
+            }
+            admit();
+            for (auto& kv : lanes)
+                if (!kv.second.inFlight) launch(kv.second);
+            // service the first lane that finishes; set arrivals up meanwhile
+            for (;;) {
+                bool progressed = false, busy = false;
+                for (auto& kv : lanes) {
+                    Lane& L = kv.second;
+                    if (!L.inFlight) continue;
+                    cudaError_t const q = cudaEventQuery(L.done);
+                    if (q == cudaSuccess) {
+                        complete(L);
+                        progressed = true;
+                    } else if (q == cudaErrorNotReady) {
+                        busy = true;
+                    } else {
+                        cuda_check(q, "lane");
+                    }
+                }
+                if (progressed || !busy) break;
+                if (checkFault()) break;
+                if (admit()) break;   // an idle lane may take the new job now
+                std::this_thread::sleep_for(std::chrono::microseconds(20));
+            }
         }
-        batch.reset();
-        for (auto const& j : active) j->u.reset();
-        for (auto const& j : incoming) j->u.reset();
+        for (auto& kv : lanes) {
+            kv.second.batch.reset();
+            for (auto const& j : kv.second.jobs) j->u.reset();
+            for (auto const& j : kv.second.incoming) j->u.reset();
+        }
     } catch (std::exception const& e) {
         std::lock_guard<std::mutex> lk(mu_);
         dead_ = true;

@@ -47,6 +47,7 @@ public:
 
 private:
     struct Job;
+    struct Lane;
     std::shared_ptr<Job> find(uint64_t id);
     void workerMain();
 
