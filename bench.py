@@ -41,6 +41,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["dense_melt", "small", "network", "ensemble"], default="dense_melt")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-cores", type=int, default=0, help="host processes of the CPU legs (0: all cores)")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched-vs-plain side measurement")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
@@ -251,9 +252,9 @@ def _cpu_worker(args):
     return attempted, t_total, s.n
 
 
-def cpu_replicas(kind, workload, steps, warmup):
+def cpu_replicas(kind, workload, steps, warmup, cores=0):
     import multiprocessing as mp
-    cores = os.cpu_count() or 1
+    cores = cores or os.cpu_count() or 1
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
         res = pool.map(_cpu_worker, [(kind, workload, steps, warmup)] * cores)
@@ -276,24 +277,31 @@ def dist_setup(args):
     return rank, world, local
 
 
-def reduce_max(x, world):
+def _all_reduce(x, world, op):
+    """One float across the ranks (CUDA tensor under NCCL, host tensor under gloo)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def reduce_max(x, world):
+    import torch.distributed as dist
+    return _all_reduce(x, world, dist.ReduceOp.MAX)
 
 
 def reduce_sum(x, world):
-    if world == 1:
-        return x
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _all_reduce(x, world, dist.ReduceOp.SUM)
+
+
+def aggregate_rate(units_per_rank, seconds_per_rank, world):
+    """Whole-job throughput of weak-scaled replicas: units of all ranks / the slowest rank's time."""
+    return reduce_sum(units_per_rank, world) / reduce_max(seconds_per_rank, world)
 
 
 def barrier(world):
@@ -352,7 +360,7 @@ def run_ours(args):
     accepted = sum(b["accepted"] - a["accepted"] for a, b in zip(stats0, stats1))
     t_max = reduce_max(ms / 1e3, world)
     moves = args.steps * n_total
-    value = world * moves / t_max
+    value = aggregate_rate(moves, ms / 1e3, world)
     p_chk, p_acc = tentative / max(attempted, 1), accepted / max(attempted, 1)
 
     # warm-L2 back-to-back number (no flush), for reference
@@ -427,7 +435,8 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, cores, _ = cpu_replicas("sequential", args.workload, steps=3 if n_total > 100000 else 40, warmup=1)
+        rate, cores, _ = cpu_replicas("sequential", args.workload, steps=3 if n_total > 100000 else 40, warmup=1,
+                                      cores=args.cpu_cores)
         cpu = {"value": rate, "unit": "attempted moves/s", "cores": cores, "kind": "port",
                "sample": ("random-sequential single-monomer BFM (LeMonADE serial-updater scheme), one replica of "
                           "the workload system per core, " + ("3" if n_total > 100000 else "40") + " MCS each")}
@@ -558,7 +567,8 @@ def run_reference(args):
     systems = build_workload(args.workload)
     config = workload_config(args.workload, systems)
     steps = min(args.steps, 5 if sum(s.n for s in systems) > 100000 else 50)
-    rate, cores, n = cpu_replicas("parallel", args.workload, steps=steps, warmup=min(args.warmup, 1))
+    rate, cores, n = cpu_replicas("parallel", args.workload, steps=steps, warmup=min(args.warmup, 1),
+                                  cores=args.cpu_cores)
     sample = (f"CPU restatement of the reference's colour-by-colour sweep (oracle/bfm_oracle.cpp), one "
               f"replica per core, {steps} MCS each after 1 warm-up MCS")
     line = {"impl": "reference", "metric": "attempted monomer moves/s", "value": rate, "unit": "attempted moves/s",

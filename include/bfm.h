@@ -92,6 +92,11 @@ int bfm_set_standard_bond_set(bfm_handle h);
 int bfm_populate_lattice(bfm_handle h);
 /* Draw stream (replaces the RandomNumberGenerators member, UpdaterGPUScBFM_AB_Type.h:131). */
 int bfm_set_seed(bfm_handle h, uint64_t seed);
+/* Position of the counter draw stream: the sub-steps drawn so far (0 after bfm_initialize). A run
+ * resumed from a checkpoint sets the saved position after bfm_initialize and continues bit-exactly.
+ * No counterpart in the reference, whose generator state is not saved. */
+int bfm_set_substep(bfm_handle h, uint64_t substep);
+int bfm_get_substep(bfm_handle h, uint64_t* substep);
 int bfm_set_draw_callback(bfm_handle h, bfm_draw_fn fn, void* ctx);
 /* Engine path, BFM_MODE_*. */
 int bfm_set_mode(bfm_handle h, int mode);

@@ -72,6 +72,8 @@ _SIGS = {
     "bfm_populate_lattice": [H],
     "bfm_set_seed": [H, C.c_uint64],
     "bfm_set_draw_callback": [H, DRAW_FN, C.c_void_p],
+    "bfm_set_substep": [H, C.c_uint64],
+    "bfm_get_substep": [H, C.POINTER(C.c_uint64)],
     "bfm_set_mode": [H, C.c_int],
     "bfm_set_representation": [H, C.c_int],
     "bfm_get_representation": [H, C.POINTER(C.c_int)],

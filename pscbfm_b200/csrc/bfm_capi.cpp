@@ -149,6 +149,14 @@ int bfm_set_standard_bond_set(bfm_handle h)
 }
 int bfm_populate_lattice(bfm_handle h) { BFM_CALL(h, h->u.populateLattice()); }
 int bfm_set_seed(bfm_handle h, uint64_t seed) { BFM_CALL(h, h->u.setDrawCounter(seed)); }
+int bfm_set_substep(bfm_handle h, uint64_t substep) { BFM_CALL(h, h->u.setSubStep(substep)); }
+int bfm_get_substep(bfm_handle h, uint64_t* substep)
+{
+    BFM_CALL(h, {
+        if (!substep) throw std::invalid_argument("[bfm_get_substep] null output");
+        *substep = h->u.subStep();
+    });
+}
 int bfm_set_draw_callback(bfm_handle h, bfm_draw_fn fn, void* ctx) { BFM_CALL(h, h->u.setDrawCallback(fn, ctx)); }
 int bfm_set_mode(bfm_handle h, int mode) { BFM_CALL(h, h->u.setMode(mode)); }
 int bfm_set_representation(bfm_handle h, int r) { BFM_CALL(h, h->u.setRepresentation(r)); }

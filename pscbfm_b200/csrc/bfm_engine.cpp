@@ -209,6 +209,15 @@ void Updater::setDrawCounter(uint64_t seed)
     drawCtx_ = nullptr;
 }
 
+void Updater::setSubStep(uint64_t t)
+{
+    requireInit("setSubStep");
+    if (drawKind_ != kDrawCounter) throw std::runtime_error("[setSubStep] only the counter draw stream has a position");
+    cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
+    scrubPending(stream_);   // pending marks are tied to the parity of the current position
+    subStep_ = t;
+}
+
 void Updater::setDrawCallback(DrawFn fn, void* ctx)
 {
     if (!fn) throw std::invalid_argument("[setDrawCallback] null callback");

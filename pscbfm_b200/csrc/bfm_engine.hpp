@@ -96,6 +96,8 @@ public:
     void stats(uint64_t out[4]);             // attempted, tentative, accepted, MCS done
     uint64_t substep() const { return subStep_; }
     uint64_t mcsDone() const { return mcsDone_; }
+    uint64_t subStep() const { return subStep_; }
+    void setSubStep(uint64_t t);   // position of the counter draw stream (after initialize)
     cudaStream_t stream() const { return stream_; }
     bool initialized() const { return dev_.arena != nullptr; }
     uint32_t nMonomers() const { return n_; }

@@ -146,6 +146,46 @@ class UpdaterGPUScBFM_AB_Type:
     # ---------------------------------------------------------------- engine extensions
     def set_seed(self, seed: int):
         self._call("bfm_set_seed", seed)
+        self._seed = int(seed)
+
+    def set_substep(self, substep: int):
+        """Position of the counter draw stream (after initialize), e.g. from a checkpoint."""
+        self._call("bfm_set_substep", substep)
+
+    def substep(self) -> int:
+        v = C.c_uint64()
+        self._call("bfm_get_substep", C.byref(v))
+        return v.value
+
+    def save_checkpoint(self, path: str, system):
+        """Writes the current positions of `system`'s monomers to a .bfm file whose header holds the
+        draw-stream position; load_checkpoint resumes from it bit-exactly."""
+        from .bfm_io import write_bfm
+        t = self.substep()
+        write_bfm(path, system, mcs=t // self.n_colors()[0], xyz=self.get_coords(), substep=t,
+                  seed=getattr(self, "_seed", 0))
+
+    @classmethod
+    def load_checkpoint(cls, path: str, system=None, gpu: int = 0, mode: int | None = None):
+        """A new initialised updater at the state save_checkpoint wrote. Returns (updater, system).
+
+        The colouring, like the reference's, depends on the order of each monomer's neighbour list,
+        and a .bfm file fixes that order only as its reader rebuilds it (explicit bonds first, then
+        the chain links). Pass the system the run started from to keep its order (positions come
+        from the file); without it the file's own order is used, which continues bit-exactly only
+        for systems that were themselves read from a .bfm file."""
+        import dataclasses
+        from .bfm_io import read_bfm
+        read, info = read_bfm(path)
+        if system is None:
+            system = read
+        else:
+            if system.n != read.n or tuple(system.box) != tuple(read.box):
+                raise ValueError("checkpoint does not match the given system (monomer count or box)")
+            system = dataclasses.replace(system, xyz=read.xyz.astype(np.int32), seed=info["seed"])
+        u = cls(gpu).load_system(system, seed=info["seed"], mode=mode)
+        u.set_substep(info["substep"])
+        return u, system
 
     def set_draw_callback(self, fn):
         """fn() -> int: an external host generator consumed twice per sub-step (colour, seed)."""
