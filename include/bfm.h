@@ -214,6 +214,8 @@ int bfm_server_wait(bfm_server_handle s, uint64_t job, double timeout_s);
  * BFM_ERR_BUSY if the job has not finished. */
 int bfm_server_result(bfm_server_handle s, uint64_t job, int32_t* xyz, uint32_t n, int64_t* samples,
                       uint64_t capacity_words, uint32_t* n_samples, double* latency_s);
+/* Total int64 words of a finished job's samples (n_samples x (5*n_mol+513)); BFM_ERR_BUSY before. */
+int bfm_server_sample_words(bfm_server_handle s, uint64_t job, uint64_t* words);
 /* out = {arrival, admission, completion} in seconds since bfm_server_create; a time not reached
  * yet is -1. */
 int bfm_server_job_times(bfm_server_handle s, uint64_t job, double out[3]);

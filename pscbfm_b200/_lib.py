@@ -115,6 +115,7 @@ _SIGS = {
                           C.POINTER(C.c_double)],
     "bfm_server_stats": [H, _f64p],
     "bfm_server_job_times": [H, C.c_uint64, _f64p],
+    "bfm_server_sample_words": [H, C.c_uint64, C.POINTER(C.c_uint64)],
     "bfm_server_inject_fault": [H, C.c_int],
     "bfm_color_graph": [C.c_uint32, _u32p, _u32p, C.c_uint32,
                         np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS"), C.POINTER(C.c_uint32)],

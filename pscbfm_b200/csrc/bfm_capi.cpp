@@ -315,6 +315,13 @@ int bfm_server_result(bfm_server_handle s, uint64_t job, int32_t* xyz, uint32_t 
 {
     BFM_CALL(s, s->s.result(job, xyz, n, reinterpret_cast<long long*>(samples), cap, nSamples, latency));
 }
+int bfm_server_sample_words(bfm_server_handle s, uint64_t job, uint64_t* words)
+{
+    BFM_CALL(s, {
+        if (!words) throw std::invalid_argument("[bfm_server_sample_words] null output");
+        *words = s->s.sampleWords(job);
+    });
+}
 int bfm_server_job_times(bfm_server_handle s, uint64_t job, double out[3])
 {
     BFM_CALL(s, {

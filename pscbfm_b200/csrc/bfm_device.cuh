@@ -9,10 +9,14 @@
 //                (word<<6 | bit, or kNoMark), used to scrub that bit one sub-step later
 //   lat          uint64 occupancy words, one bit per lattice cell (the monomer's corner cell)
 //   tmp          uint64 [2][nwords] ping-pong temporary lattices of tentative targets
-// A 64-bit word holds one 4x4x4 brick of cells in Z-curve order (bit = x0 y0 z0 x1 y1 z1);
-// bricks are numbered by per-axis contribution tables (brickTab), which the host fills with the
-// Z-curve of the brick coordinates. For a cubic box the bit of cell (x,y,z) is then exactly the
-// reference's Z-curve index (src/pscbfm/CRITICAL.cu:13-34 with USE_ZCURVE_FOR_LATTICE).
+// A 64-bit word holds one 4x4x4 brick of cells, bit (x&3) + 4 (y&3) + 16 (z&3), so the three
+// cells of a front-plane row along any axis are one bit run with a fixed stride; bricks are
+// numbered by the Z-curve (Morton order) of the brick coordinates, with the bits above the
+// smallest axis's brick count laid out linearly (non-cubic boxes), through per-axis contribution
+// tables (brickTab). The reference keeps one Z-curve index per cell (src/pscbfm/CRITICAL.cu:13-34);
+// only the occupancy of each cell matters to the sweep, so the bit order inside a word is free.
+// Bond-code representation (codeMode != kCodeNone) adds, per monomer, its packed masked
+// coordinates (pk) and a word of bond-table indices (code), see CodeWord below.
 #pragma once
 
 #include <cstdint>

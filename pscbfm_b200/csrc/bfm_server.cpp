@@ -207,6 +207,16 @@ void Server::jobTimes(uint64_t id, double out[3])
     out[2] = j->state >= kJobDone ? since(j->finish) : -1.0;
 }
 
+uint64_t Server::sampleWords(uint64_t id)
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    auto j = find(id);
+    if (j->state == kJobFailed) throw std::runtime_error("[Server::sampleWords] job failed: " + j->error);
+    if (j->state == kJobCancelled) throw std::runtime_error("[Server::sampleWords] job was cancelled");
+    if (j->state != kJobDone) throw BusyError("[Server::sampleWords] job not finished");
+    return j->samples.size();
+}
+
 void Server::injectFault(int kind)
 {
     std::lock_guard<std::mutex> lk(mu_);

@@ -40,7 +40,8 @@ public:
                 double* latencyS);
     // completed, failed, attempted moves of completed jobs, p50 s, p99 s, mean s, resident bytes, elapsed s
     void stats(double out[8]);
-    void jobTimes(uint64_t id, double out[3]);   // arrival, admission, completion (s since create; -1: not yet)
+    void jobTimes(uint64_t id, double out[3]);
+    uint64_t sampleWords(uint64_t id);            // int64 words of a finished job's samples   // arrival, admission, completion (s since create; -1: not yet)
     void injectFault(int kind);                // 1: the worker thread throws at its next loop
     bool dead();
     static size_t estimateBytes(Updater const& setup);

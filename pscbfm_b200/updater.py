@@ -426,17 +426,18 @@ class Server:
     def wait(self, job: int, timeout: float = 600.0):
         self._call("bfm_server_wait", job, timeout)
 
-    def result(self, job: int, n_mol: int | None = None):
+    def result(self, job: int):
+        """(final positions (n, 3), samples (n_samples, 5 n_mol + 513) int64, latency in s)."""
         n, n_mcs, every = self._sizes[job]
         xyz = np.zeros((n, 3), dtype=np.int32)
         ns = C.c_uint32()
         lat = C.c_double()
-        self._call("bfm_server_result", job, xyz.ctypes.data, n, None, 0, C.byref(ns), C.byref(lat))
-        samples = None
-        if n_mol is not None:
-            samples = np.zeros((ns.value, 5 * n_mol + 513), dtype=np.int64)
-            self._call("bfm_server_result", job, None, 0, samples.ctypes.data, samples.size, C.byref(ns), C.byref(lat))
-        return xyz, samples, lat.value
+        words = C.c_uint64()
+        self._call("bfm_server_sample_words", job, C.byref(words))
+        samples = np.zeros(words.value, dtype=np.int64)
+        self._call("bfm_server_result", job, xyz.ctypes.data, n, samples.ctypes.data, samples.size, C.byref(ns),
+                   C.byref(lat))
+        return xyz, samples.reshape(ns.value, -1), lat.value
 
     def stats(self) -> dict:
         out = np.zeros(8, dtype=np.float64)

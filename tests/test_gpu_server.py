@@ -37,7 +37,8 @@ def test_results_equal_alone_in_the_mix():
         assert srv.status(j) == P.Server.DONE
     for j, (s, n, k) in zip(jobs, plan):
         want_xyz, want_samples, n_mol = alone(s, n, k)
-        xyz, samples, lat = srv.result(j, n_mol=n_mol)
+        xyz, samples, lat = srv.result(j)
+        assert samples.shape[1] == 5 * n_mol + 513
         assert np.array_equal(xyz, want_xyz), s.name
         assert np.array_equal(samples, want_samples), s.name
         assert lat > 0
