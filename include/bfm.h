@@ -62,7 +62,10 @@ int bfm_set_gpu(bfm_handle h, int gpu);
 int bfm_cleanup(bfm_handle h);
 
 /* ------------------------------------------------------------------ setters */
-/* setPeriodicity (UpdaterGPUScBFM_AB_Type.cu:728-753): only fully periodic boxes. */
+/* setPeriodicity (UpdaterGPUScBFM_AB_Type.cu:728-753), before bfm_initialize. The reference's
+ * default build takes fully periodic boxes and its NONPERIODICITY build fully non-periodic ones;
+ * here each axis chooses. Along an axis without periodicity, corners must lie in [0, L-2] and a move
+ * that would leave that range is rejected (CRITICAL.cu:334-341). */
 int bfm_set_periodicity(bfm_handle h, int px, int py, int pz);
 /* setNrOfAllMonomers (UpdaterGPUScBFM_AB_Type.cu:699-726); runtime error if already set. */
 int bfm_set_n_monomers(bfm_handle h, uint32_t n);

@@ -58,7 +58,18 @@ struct System {
     std::vector<int32_t> x, y, z;                 // original monomer order
     std::vector<std::vector<uint32_t>> nbr;       // directed lists, in setConnectivity order
     bool forbidden[512];
+    uint32_t walls = 0;                           // bit a: axis a is not periodic
 };
+
+// CRITICAL.cu:334-341 (build with NONPERIODICITY): along an axis with walls the moved corner must
+// stay in [0, L-2] (the unsigned compare r1 < L-1 also rejects -1), so the whole cube stays inside.
+inline bool outside_walls(System const& s, int32_t x1, int32_t y1, int32_t z1)
+{
+    int32_t const c[3] = {x1, y1, z1};
+    for (int a = 0; a < 3; ++a)
+        if (((s.walls >> a) & 1u) && uint32_t(c[a]) >= s.box[a] - 1u) return true;
+    return false;
+}
 
 // CRITICAL.cu:243-261: bond vector -> 9-bit table index, each component masked to 3 bits.
 inline uint32_t bond_index(int32_t dx, int32_t dy, int32_t dz)
@@ -298,8 +309,9 @@ void sweep(System& s, Sorted const& g, Draws& draws, uint32_t nMcs, RunStats& st
                 int32_t dx, dy, dz;
                 dir_vec(dir, dx, dy, dz);
                 int32_t const x1 = px[k] + dx, y1 = py[k] + dy, z1 = pz[k] + dz;
-                bool bad = false;
+                bool bad = outside_walls(s, x1, y1, z1);
                 for (uint32_t j : nb[k]) {
+                    if (bad) break;
                     if (s.forbidden[bond_index(px[j] - x1, py[j] - y1, pz[j] - z1)]) { bad = true; break; }
                 }
                 uint8_t f = 0;
@@ -342,10 +354,11 @@ void set_err(char* err, int len, std::string const& msg)
 }
 
 System make_system(uint32_t n, int32_t const* xyz, uint32_t const* nbrCount, uint32_t const* nbrIds,
-                   uint32_t maxc, uint32_t const* box, uint8_t const* forbidden)
+                   uint32_t maxc, uint32_t const* box, uint32_t walls, uint8_t const* forbidden)
 {
     System s;
     s.n = n;
+    s.walls = walls & 7u;
     for (int a = 0; a < 3; ++a) s.box[a] = box[a];
     s.x.resize(n); s.y.resize(n); s.z.resize(n);
     s.nbr.resize(n);
@@ -360,6 +373,9 @@ System make_system(uint32_t n, int32_t const* xyz, uint32_t const* nbrCount, uin
     for (int i = 0; i < 512; ++i) s.forbidden[i] = forbidden[i] != 0;
     for (int a = 0; a < 3; ++a)
         if (box[a] == 0 || (box[a] & (box[a] - 1)) != 0) throw std::invalid_argument("box sides must be powers of two");
+    for (uint32_t i = 0; i < n; ++i)
+        if (outside_walls(s, s.x[i], s.y[i], s.z[i]))
+            throw std::invalid_argument("monomer " + std::to_string(i) + " lies outside the walls of the box");
     return s;
 }
 
@@ -401,9 +417,9 @@ void sequential_sweep(System& s, uint64_t seed, uint32_t nMcs, RunStats& st)
         int32_t dx, dy, dz;
         dir_vec(dir, dx, dy, dz);
         int32_t const x1 = s.x[k] + dx, y1 = s.y[k] + dy, z1 = s.z[k] + dz;
-        bool bad = false;
+        bool bad = outside_walls(s, x1, y1, z1);
         for (uint32_t j : s.nbr[k])
-            if (s.forbidden[bond_index(s.x[j] - x1, s.y[j] - y1, s.z[j] - z1)]) { bad = true; break; }
+            if (!bad && s.forbidden[bond_index(s.x[j] - x1, s.y[j] - y1, s.z[j] - z1)]) { bad = true; break; }
         ++st.attempted;
         if (bad || lat.front_occupied(s.x[k], s.y[k], s.z[k], dir)) continue;
         lat.cell[lat.at(s.x[k], s.y[k], s.z[k])] = 0;
@@ -463,13 +479,13 @@ int orc_color(uint32_t n, uint32_t const* nbrCount, uint32_t const* nbrIds, uint
 //   drawKind 1: explicit draws list (2 per sub-step), consumed from index 0
 // stats[0..2] += attempted, tentatively accepted, accepted.
 int orc_run(uint32_t n, int32_t const* xyzIn, uint32_t const* nbrCount, uint32_t const* nbrIds,
-            uint32_t maxc, uint32_t const* box, uint8_t const* forbidden, int drawKind, uint64_t seed,
+            uint32_t maxc, uint32_t const* box, uint32_t walls, uint8_t const* forbidden, int drawKind, uint64_t seed,
             uint64_t subStep0, uint32_t const* drawList, uint64_t drawLen, uint32_t nMcs,
             int32_t* xyzOut, uint64_t* stats, char* err, int errLen)
 {
     try {
         if (n == 0) throw std::invalid_argument("no monomers");
-        System s = make_system(n, xyzIn, nbrCount, nbrIds, maxc, box, forbidden);
+        System s = make_system(n, xyzIn, nbrCount, nbrIds, maxc, box, walls, forbidden);
         uint32_t nAllowed = 0;
         for (int i = 0; i < 512; ++i) nAllowed += s.forbidden[i] ? 0 : 1;
         if (nAllowed != 108)   // UpdaterGPUScBFM_AB_Type.cu:521-528
@@ -492,11 +508,11 @@ int orc_run(uint32_t n, int32_t const* xyzIn, uint32_t const* nbrCount, uint32_t
 
 // Random-sequential CPU baseline; stats[0..1] += attempted, accepted.
 int orc_seq_run(uint32_t n, int32_t const* xyzIn, uint32_t const* nbrCount, uint32_t const* nbrIds,
-                uint32_t maxc, uint32_t const* box, uint8_t const* forbidden, uint64_t seed, uint32_t nMcs,
+                uint32_t maxc, uint32_t const* box, uint32_t walls, uint8_t const* forbidden, uint64_t seed, uint32_t nMcs,
                 int32_t* xyzOut, uint64_t* stats, char* err, int errLen)
 {
     try {
-        System s = make_system(n, xyzIn, nbrCount, nbrIds, maxc, box, forbidden);
+        System s = make_system(n, xyzIn, nbrCount, nbrIds, maxc, box, walls, forbidden);
         RunStats st;
         sequential_sweep(s, seed, nMcs, st);
         for (uint32_t i = 0; i < n; ++i) {

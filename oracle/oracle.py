@@ -16,6 +16,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libpscbfm_ref.so")
+REF_LIB_NP = os.path.join(HERE, "_ref", "libpscbfm_ref_np.so")
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
@@ -23,7 +24,7 @@ _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 _u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
 
 _lib = None
-_ref = None
+_ref = {}
 
 
 def build():
@@ -46,11 +47,11 @@ def lib():
         L.orc_bond_index.restype = C.c_uint32
         L.orc_color.argtypes = [C.c_uint32, _u32p, _u32p, C.c_uint32, _u8p, C.c_char_p, C.c_int]
         L.orc_color.restype = C.c_int
-        L.orc_run.argtypes = [C.c_uint32, _i32p, _u32p, _u32p, C.c_uint32, _u32p, _u8p, C.c_int,
+        L.orc_run.argtypes = [C.c_uint32, _i32p, _u32p, _u32p, C.c_uint32, _u32p, C.c_uint32, _u8p, C.c_int,
                               C.c_uint64, C.c_uint64, _u32p, C.c_uint64, C.c_uint32, _i32p, _u64p,
                               C.c_char_p, C.c_int]
         L.orc_run.restype = C.c_int
-        L.orc_seq_run.argtypes = [C.c_uint32, _i32p, _u32p, _u32p, C.c_uint32, _u32p, _u8p, C.c_uint64,
+        L.orc_seq_run.argtypes = [C.c_uint32, _i32p, _u32p, _u32p, C.c_uint32, _u32p, C.c_uint32, _u8p, C.c_uint64,
                                   C.c_uint32, _i32p, _u64p, C.c_char_p, C.c_int]
         L.orc_seq_run.restype = C.c_int
         _lib = L
@@ -98,7 +99,7 @@ def run(sys, n_mcs: int, seed: int | None = None, substep0: int = 0, draws=None)
     else:
         kind, dl = 1, np.ascontiguousarray(draws, dtype=np.uint32)
         seed = 0
-    rc = lib().orc_run(sys.n, xyz, cnt, ids, sys.maxc, box, forb, kind, seed, substep0, dl,
+    rc = lib().orc_run(sys.n, xyz, cnt, ids, sys.maxc, box, sys.walls, forb, kind, seed, substep0, dl,
                        len(dl), n_mcs, out, stats, err, 512)
     if rc != 0:
         raise RuntimeError(err.value.decode())
@@ -110,7 +111,7 @@ def seq_run(sys, n_mcs: int, seed: int):
     out = np.zeros_like(xyz)
     stats = np.zeros(2, dtype=np.uint64)
     err = C.create_string_buffer(512)
-    rc = lib().orc_seq_run(sys.n, xyz, cnt, ids, sys.maxc, box, forb, seed, n_mcs, out, stats, err, 512)
+    rc = lib().orc_seq_run(sys.n, xyz, cnt, ids, sys.maxc, box, sys.walls, forb, seed, n_mcs, out, stats, err, 512)
     if rc != 0:
         raise RuntimeError(err.value.decode())
     return out.reshape(-1, 3), tuple(int(s) for s in stats)
@@ -118,32 +119,43 @@ def seq_run(sys, n_mcs: int, seed: int):
 
 # ------------------------------------------------------------------ reference updater (GPU box)
 
-def ref_available() -> bool:
-    return os.path.exists(REF_LIB)
+def _ref_path(walls: int) -> str:
+    """The default build for periodic boxes, the NONPERIODICITY build for boxes with walls on all
+    three axes (the reference has no build for mixed periodicity)."""
+    if walls == 0:
+        return REF_LIB
+    if walls == 7:
+        return REF_LIB_NP
+    raise ValueError("the reference updater supports fully periodic or fully non-periodic boxes only")
 
 
-def ref_lib():
-    global _ref
-    if _ref is None:
-        R = C.CDLL(REF_LIB)
+def ref_available(walls: int = 0) -> bool:
+    return os.path.exists(_ref_path(walls))
+
+
+def ref_lib(walls: int = 0):
+    path = _ref_path(walls)
+    if path not in _ref:
+        R = C.CDLL(path)
         R.bfmref_run.argtypes = [C.c_int, C.c_uint32, _i32p, _u32p, _u32p, C.c_uint32, _u32p, _u8p,
                                  _u32p, C.c_uint64, _u32p, C.c_uint32, _i32p, _u64p, C.c_char_p, C.c_int]
         R.bfmref_run.restype = C.c_int
-        _ref = R
-    return _ref
+        _ref[path] = R
+    return _ref[path]
 
 
 def ref_run(sys, draws, chunks, gpu: int = 0):
-    """Runs the reference updater (its own kernels) with the given draw list; chunks are the
-    nMCS of successive runSimulationOnGPU calls. Returns positions and the number of draws used."""
+    """Runs the reference updater (its own kernels; the NONPERIODICITY build for a box with walls)
+    with the given draw list; chunks are the nMCS of successive runSimulationOnGPU calls. Returns
+    positions and the number of draws used."""
     xyz, cnt, ids, box, forb = _arrs(sys)
     out = np.zeros_like(xyz)
     used = np.zeros(1, dtype=np.uint64)
     err = C.create_string_buffer(1024)
     d = np.ascontiguousarray(draws, dtype=np.uint32)
     ch = np.ascontiguousarray(chunks, dtype=np.uint32)
-    rc = ref_lib().bfmref_run(gpu, sys.n, xyz, cnt, ids, sys.maxc, box, forb, d, len(d), ch, len(ch),
-                              out, used, err, 1024)
+    rc = ref_lib(sys.walls).bfmref_run(gpu, sys.n, xyz, cnt, ids, sys.maxc, box, forb, d, len(d), ch, len(ch),
+                                       out, used, err, 1024)
     if rc != 0:
         raise RuntimeError(f"reference updater failed ({rc}): {err.value.decode()}")
     return out.reshape(-1, 3), int(used[0])

@@ -42,7 +42,11 @@ extern "C" int bfmref_run(int gpu, uint32_t n, int32_t const* xyz, uint32_t cons
             return -1;
         }
         UpdaterGPUScBFM_AB_Type u;
+#ifdef NONPERIODICITY
+        u.setPeriodicity(false, false, false);   // the only choice this build accepts
+#else
         u.setPeriodicity(true, true, true);
+#endif
         u.setNrOfAllMonomers(n);
         for (uint32_t i = 0; i < n; ++i) u.setMonomerCoordinates(i, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
         for (uint32_t i = 0; i < n; ++i) u.setAttribute(i, 1);

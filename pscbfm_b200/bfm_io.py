@@ -115,6 +115,7 @@ def read_bfm(path: str, seed: int = 0):
     s = from_bonds(tuple(box), xyz, extra + chain_bonds, attributes=attrs, name=path.rsplit("/", 1)[-1],
                    seed=info["seed"])
     s.forbidden = forbidden_table(allowed)
+    s.periodic = tuple(bool(p) for p in info["periodic"])
     info["bond_vectors"] = codes
     return s, info
 
@@ -125,10 +126,12 @@ def _default_codes():
 
 
 def write_bfm(path: str, system: BfmSystem, mcs: int = 0, xyz=None, substep: int | None = None,
-              seed: int | None = None, periodic=(True, True, True)):
+              seed: int | None = None, periodic=None):
     """Writes one frame. Chain lines follow bonds between consecutive ids whose vector has a code;
-    every other bond goes to !bonds."""
+    every other bond goes to !bonds. The periodicity is the system's unless given."""
     xyz = np.asarray(system.xyz if xyz is None else xyz, dtype=np.int64)
+    if periodic is None:
+        periodic = system.periodic
     n = system.n
     allowed = [tuple(int(c) for c in v) for v in standard_bond_vectors()]
     forb = system.forbidden

@@ -63,6 +63,7 @@ struct SysDev {
     unsigned long long const* planeTab;   // [3][4][4][4][4] front-plane masks (see plane_table_fill)
     uint8_t const* moveOk;           // [512] bit d: a bond with this index stays allowed after move d
     uint32_t codeMode;               // kCodeNone, kCode32, kCode64
+    uint32_t walls;                  // bit a: axis a is not periodic (corners stay in [0, L-2])
     uint32_t npad, nwords, maxc, nColors;
     uint32_t mask[3];                // box side - 1 (power-of-two box)
     uint32_t nb[3];                  // bricks per axis
@@ -121,6 +122,16 @@ __device__ __forceinline__ uint32_t move_dir(uint32_t iLocal, uint32_t seed)
 }
 
 // Position of value v (0..3) of axis a inside a brick word: bit = x + 4 y + 16 z.
+// CRITICAL.cu:334-341 (the reference's NONPERIODICITY build): along an axis with walls the moved
+// corner must stay in [0, L-2]; c is the current coordinate along the move's axis (in the box on
+// such an axis), and the unsigned compare rejects both -1 and L-1.
+__host__ __device__ __forceinline__ bool wall_blocks(uint32_t walls, uint32_t c, uint32_t dir, uint32_t const* mask)
+{
+    uint32_t const a = dir >> 1;
+    uint32_t const c1 = c + ((dir & 1u) ? 1u : 0xFFFFFFFFu);
+    return ((walls >> a) & 1u) && c1 >= mask[a];
+}
+
 __host__ __device__ __forceinline__ uint32_t brick_pos(uint32_t v, uint32_t a)
 {
     return v << (2u * a);

@@ -104,14 +104,10 @@ void Updater::requireInit(char const* who) const
 
 void Updater::setPeriodicity(bool px, bool py, bool pz)
 {
-    // UpdaterGPUScBFM_AB_Type.cu:728-753: the sweep is for fully periodic boxes only
-    if (!px || !py || !pz) {
-        std::ostringstream m;
-        m << "[UpdaterGPUScBFM_AB_Type::setPeriodicity] Simulation is intended to use completely periodic "
-             "boundary conditions, but setPeriodicity was called with ("
-          << px << "," << py << "," << pz << ")";
-        throw std::invalid_argument(m.str());
-    }
+    // UpdaterGPUScBFM_AB_Type.cu:728-753 accepts fully periodic boxes in its default build and
+    // fully non-periodic ones in its NONPERIODICITY build; here every axis chooses on its own.
+    if (initialized()) throw std::runtime_error("[setPeriodicity] call it before initialize");
+    walls_ = (px ? 0u : 1u) | (py ? 0u : 2u) | (pz ? 0u : 4u);
 }
 
 void Updater::setNrOfAllMonomers(uint32_t n)
@@ -242,16 +238,7 @@ void Updater::initialize()
         throw std::runtime_error(
             "[UpdaterGPUScBFM_AB_Type::initialize] Initialize was already called and may not be called again until "
             "cleanup was called!");
-    requireN("initialize");
-    if (n_ == 0) throw std::runtime_error("[initialize] the system has no monomers");
-    if (!box_[0]) throw std::runtime_error("[initialize] setLatticeSize has not been called");
-    uint32_t nAllowed = 0;
-    for (bool f : forbidden_) nAllowed += f ? 0 : 1;
-    if (nAllowed != 108) {
-        std::ostringstream m;
-        m << "[UpdaterGPUScBFM_AB_Type::initialize] Wrong bond-set! Expected 108 allowed bonds, but got " << nAllowed;
-        throw std::runtime_error(m.str());
-    }
+    checkSetup();
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
 
     // colouring and groups (UpdaterGPUScBFM_AB_Type.cu:549-608)
@@ -382,6 +369,7 @@ void Updater::initialize()
     h.planeTab = reinterpret_cast<unsigned long long*>(base + oPlane);
     h.moveOk = reinterpret_cast<uint8_t*>(base + oMoveOk);
     h.codeMode = codeMode_;
+    h.walls = walls_;
 
     cudaStream_t s = stream_;
     std::vector<unsigned long long> hplane(768);
@@ -580,6 +568,14 @@ void Updater::checkSetup() const
         m << "[UpdaterGPUScBFM_AB_Type::initialize] Wrong bond-set! Expected 108 allowed bonds, but got " << nAllowed;
         throw std::runtime_error(m.str());
     }
+    // along an axis with walls every corner must lie in [0, L-2] (the cube inside the box)
+    for (uint32_t i = 0; i < n_; ++i)
+        for (int a = 0; a < 3; ++a)
+            if (((walls_ >> a) & 1u) && uint32_t(xyz_[3ull * i + a]) >= box_[a] - 1u) {
+                std::ostringstream m;
+                m << "[initialize] monomer " << i << " lies outside the walls of the box along axis " << a;
+                throw std::runtime_error(m.str());
+            }
 }
 
 void Updater::copySetup(Updater const& o)
@@ -593,6 +589,7 @@ void Updater::copySetup(Updater const& o)
     nbrCnt_ = o.nbrCnt_;
     nbrIds_ = o.nbrIds_;
     for (int a = 0; a < 3; ++a) box_[a] = o.box_[a];
+    walls_ = o.walls_;
     std::copy(o.forbidden_, o.forbidden_ + 512, forbidden_);
     latticePopulated_ = o.latticePopulated_;
     drawKind_ = o.drawKind_;
@@ -934,6 +931,12 @@ void Updater::setCoordinates(int32_t const* xyz, uint32_t n)
 {
     requireN("setCoordinates");
     if (n != n_) throw std::invalid_argument("[setCoordinates] wrong monomer count");
+    if (initialized())
+        for (uint32_t i = 0; i < n_; ++i)
+            for (int a = 0; a < 3; ++a)
+                if (((walls_ >> a) & 1u) && uint32_t(xyz[3ull * i + a]) >= box_[a] - 1u)
+                    throw std::invalid_argument("[setCoordinates] monomer " + std::to_string(i) +
+                                                " lies outside the walls of the box");
     if (xyz != xyz_.data()) std::memcpy(xyz_.data(), xyz, sizeof(int32_t) * 3 * (size_t)n_);
     hostStale_ = false;
     if (!initialized()) return;
@@ -994,6 +997,10 @@ void Updater::validate()
     // every bond in the allowed set (looked up with the kernel's 3-bit component index).
     requireN("validate");
     pullPositions();
+    for (uint32_t i = 0; i < n_; ++i)
+        for (int a = 0; a < 3; ++a)
+            if (((walls_ >> a) & 1u) && uint32_t(xyz_[3ull * i + a]) >= box_[a] - 1u)
+                throw std::runtime_error("[validate] monomer " + std::to_string(i) + " crossed a wall");
     uint64_t const V = (uint64_t)box_[0] * box_[1] * box_[2];
     std::vector<uint8_t> cells(V, 0);
     uint64_t occupied = 0;

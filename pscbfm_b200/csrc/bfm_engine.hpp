@@ -160,6 +160,7 @@ private:
     std::vector<uint32_t> nbrCnt_;
     std::vector<uint32_t> nbrIds_;             // [n][kMaxConn]
     uint32_t box_[3] = {0, 0, 0};
+    uint32_t walls_ = 0;   // bit a: axis a is not periodic
     bool forbidden_[512];
     bool latticePopulated_ = false;
 

@@ -171,7 +171,8 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab,
     for (int q = 0; q < MPT; ++q) {
         uint32_t const i = start + tid + (uint32_t)q * B;
         dir[q] = move_dir(i, st.seed);
-        ok[q] = i < st.cnt && bonds_ok<W, false>(code[q], dir[q], S.moveOk);
+        ok[q] = i < st.cnt && !wall_blocks(S.walls, (pk[q] >> (10u * (dir[q] >> 1))) & 1023u, dir[q], S.mask) &&
+                bonds_ok<W, false>(code[q], dir[q], S.moveOk);
         front_plane<false>(pl[q], tab, S.planeTab, S, pk[q], dir[q]);
     }
     // stage 3: occupancy words
@@ -409,7 +410,8 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
             if (i < st.cnt) {
                 uint32_t const g = st.off + i;
                 uint32_t const dir = move_dir(i, st.seed);
-                if (bonds_ok<W, true>(code[g], dir, mok)) {
+                if (!wall_blocks(S.walls, (pk[g] >> (10u * (dir >> 1))) & 1023u, dir, S.mask) &&
+                    bonds_ok<W, true>(code[g], dir, mok)) {
                     Plane pl;
                     front_plane<true>(pl, tab, ptab, S, pk[g], dir);
                     unsigned long long hit = 0ull;

@@ -1,7 +1,8 @@
 """Synthetic BFM systems: the standard bond set and the straight-chain, network and ensemble
 layouts the sweep is measured on.
 
-A system is a periodic power-of-two box, int32 monomer corner positions (unfolded), directed
+A system is a power-of-two box (periodic, or with walls along chosen axes), int32 monomer corner
+positions (unfolded), directed
 neighbour lists in the order a LeMonADE-style caller would pass them to ``setConnectivity``
 (for every bond (a, b) in creation order: b is appended to a's list and a to b's list), integer
 attributes and the 512-entry forbidden-bond table indexed like
@@ -61,10 +62,16 @@ class BfmSystem:
     forbidden: np.ndarray = field(default_factory=forbidden_table)
     name: str = ""
     seed: int = 0
+    periodic: tuple = (True, True, True)   # an axis that is not periodic has walls at 0 and L-1
 
     @property
     def n(self) -> int:
         return int(self.xyz.shape[0])
+
+    @property
+    def walls(self) -> int:
+        """Bit a set: axis a is not periodic."""
+        return sum(1 << a for a in range(3) if not self.periodic[a])
 
     @property
     def maxc(self) -> int:
@@ -197,6 +204,17 @@ def serpentine_chains(L: int, chain_len: int, phi: float, name: str = "", seed: 
     ids = (np.arange(n_chains)[:, None] * chain_len + np.arange(chain_len - 1)[None, :]).reshape(-1)
     bonds = np.stack([ids, ids + 1], axis=1)
     return from_bonds((L, L, L), xyz, bonds, name=name or f"serp{L}_{n_chains}x{chain_len}", seed=seed)
+
+
+def walled(s: BfmSystem, walls: int = 7, name: str = "") -> BfmSystem:
+    """A copy of s with walls along the axes of the bit mask `walls` (bit a: axis a not periodic).
+    Every corner must already lie in [0, L-2] along those axes."""
+    import dataclasses
+    periodic = tuple(not (walls >> a) & 1 for a in range(3))
+    for a in range(3):
+        if (walls >> a) & 1 and (s.xyz[:, a].min() < 0 or s.xyz[:, a].max() > s.box[a] - 2):
+            raise ValueError(f"monomers outside the walls along axis {a}")
+    return dataclasses.replace(s, periodic=periodic, name=name or s.name + f"_walls{walls}")
 
 
 _RING3 = [(0, 0, 0), (2, 0, 0), (1, 2, 0)]

@@ -292,7 +292,7 @@ class UpdaterGPUScBFM_AB_Type:
         (src/pscbfm/GPUScBFM_AB_Type.h:83-130), then initializes."""
         if representation is not None:
             self.set_representation(representation)
-        self.setPeriodicity(True, True, True)
+        self.setPeriodicity(*[bool(p) for p in system.periodic])
         self.setNrOfAllMonomers(system.n)
         self.set_coords(system.xyz)
         attrs = np.ascontiguousarray(system.attributes, dtype=np.int32)

@@ -55,8 +55,18 @@ def fixture(key: str, seed: int = 17):
         fill[a] += 1
     return BfmSystem(tuple(int(v) for v in z[f"{key}_box"]), z[f"{key}_xyz"].astype(np.int32), cnt, ids,
                      z[f"{key}_attributes"].astype(np.int32), z[f"{key}_forbidden"].astype(np.uint8),
-                     name=key, seed=seed)
+                     name=key, seed=seed, periodic=tuple(bool(v) for v in z[f"{key}_periodic"]))
 
 
 CASES["fixture_linearchain128_200mcs"] = (lambda: fixture("linear_chains"), [200])
 FAST.append("fixture_linearchain128_200mcs")
+
+# Boxes with walls on all three axes, pinned against the reference's NONPERIODICITY build: the
+# reference's own non-periodic ring fixture (tests/Ring_N6_n6.bfm) and chains folded inside walls.
+WALL_CASES = {
+    "fixture_ring128_walls_3000mcs": (lambda: fixture("ring"), [3000]),
+    "serp32_lc16_walls_800mcs": (lambda: S.walled(S.serpentine_chains(32, 16, 0.3, seed=21)), [300, 500]),
+    "serp64_lc64_walls_300mcs": (lambda: S.walled(S.serpentine_chains(64, 64, 0.45, seed=23)), [300]),
+}
+CASES.update(WALL_CASES)
+FAST.extend(WALL_CASES)

@@ -18,9 +18,30 @@ def test_set_gpu_out_of_range():
         u.setGpu(999)
 
 
-def test_non_periodic_rejected():
-    with pytest.raises(ValueError, match="periodic"):
-        fresh().setPeriodicity(True, False, True)
+def test_monomer_outside_walls_rejected():
+    from pscbfm_b200 import systems as S
+    s = S.walled(S.serpentine_chains(32, 16, 0.3, seed=5), walls=2)
+    s.xyz = s.xyz.copy()
+    s.xyz[0, 1] = 31          # corner at L-1 along the walled axis: the cube would stick out
+    u = fresh()
+    with pytest.raises(RuntimeError, match="outside the walls"):
+        u.load_system(s)
+    u.close()
+    s.xyz[0, 1] = 30          # at L-2 it fits
+    v = fresh().load_system(s)
+    with pytest.raises(ValueError, match="outside the walls"):
+        bad = v.get_coords().copy()
+        bad[5, 1] = -1
+        v.set_coords(bad)
+    v.close()
+
+
+def test_periodicity_fixed_after_initialize():
+    from pscbfm_b200 import systems as S
+    u = fresh().load_system(S.small_chains())
+    with pytest.raises(RuntimeError, match="before initialize"):
+        u.setPeriodicity(False, False, False)
+    u.close()
 
 
 def test_monomer_count_set_twice():

@@ -85,6 +85,31 @@ def test_six_functional_network_vs_oracle(mode, repr_):
     assert (st["attempted"], st["tentative"], st["accepted"]) == ost
 
 
+@pytest.mark.parametrize("repr_", ["codes", "gather"])
+@pytest.mark.parametrize("mode", ["launch", "graph", "resident"])
+@pytest.mark.parametrize("walls", [1, 4, 6])
+def test_partial_walls_vs_oracle(walls, mode, repr_):
+    # the reference has builds for fully periodic and fully walled boxes only: mixed periodicity
+    # is pinned by the oracle
+    s = S.walled(S.serpentine_chains(32, 32, 0.35, seed=31), walls=walls)
+    ref, ost = O.run(s, 400)
+    xyz, st = run_engine(s, [150, 250], MODES[mode], repr_=REPRS[repr_])
+    assert np.array_equal(xyz, ref)
+    assert (st["attempted"], st["tentative"], st["accepted"]) == ost
+
+
+@pytest.mark.parametrize("mode", ["launch", "graph", "resident"])
+def test_hydrogel_fixture_with_walls_vs_oracle(mode):
+    # the reference's non-periodic hydrogel (tests/coloring-test-Hydrogel...bfm): up to 5 bonds per
+    # monomer, more than the reference build's MAX_CONNECTIVITY, so the oracle pins it
+    from cases import fixture
+    s = fixture("hydrogel")
+    ref, ost = O.run(s, 600)
+    xyz, st = run_engine(s, [600], MODES[mode])
+    assert np.array_equal(xyz, ref)
+    assert (st["attempted"], st["tentative"], st["accepted"]) == ost
+
+
 def test_dense_melt_full_config():
     """256^3 melt at phi = 0.5: the full 10^4 MCS of the config, split across calls and modes,
     equals one uninterrupted run; invariants hold; the first MCS match the oracle."""
@@ -152,6 +177,7 @@ def test_batch_equals_each_system_alone(resident):
     systems = S.ensemble(n_systems=20)
     systems.append(S.rings_and_free())         # three colours in the mix
     systems.append(S.crosslinked_network())    # 64-bit bond codes in the mix
+    systems.append(S.walled(S.serpentine_chains(64, 32, 0.3, seed=41)))   # walls in the mix
     members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
     # and two systems forced onto the gather representation
     for s in systems[:2]:

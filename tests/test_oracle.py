@@ -177,6 +177,30 @@ def test_sweep_keeps_invariants(build):
     assert not np.array_equal(xyz, s.xyz)
 
 
+@pytest.mark.parametrize("walls", [1, 2, 4, 7])
+def test_walls_keep_monomers_inside(walls):
+    s = S.walled(S.serpentine_chains(32, 16, 0.3, seed=5), walls=walls)
+    xyz, (att, tent, acc) = O.run(s, 300)
+    assert _ev_ok(xyz, s.box) and _bonds_ok(s, xyz)
+    for a in range(3):
+        if (walls >> a) & 1:
+            assert xyz[:, a].min() >= 0 and xyz[:, a].max() <= s.box[a] - 2
+            # the walls are reached: without them the chains would spread past them
+            assert xyz[:, a].min() == 0 or xyz[:, a].max() == s.box[a] - 2
+    assert 0 < acc <= tent <= att
+    # a periodic run of the same system differs once monomers meet the walls
+    free, _ = O.run(S.walled(s, walls=0), 300)
+    assert not np.array_equal(free, xyz)
+
+
+def test_monomer_outside_walls_rejected():
+    s = S.walled(S.serpentine_chains(32, 16, 0.3, seed=5), walls=1)
+    s.xyz = s.xyz.copy()
+    s.xyz[3, 0] = 31          # corner at L-1: the cube would stick out
+    with pytest.raises(RuntimeError, match="outside the walls"):
+        O.run(s, 1)
+
+
 def test_chunked_run_equals_single_run():
     s = S.rings_and_free()
     nc = int(O.color(s).max()) + 1
