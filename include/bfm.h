@@ -41,6 +41,8 @@ extern "C" {
 #define BFM_MODE_LAUNCH 1   /* check + perform launch per sub-step (the reference's structure) */
 #define BFM_MODE_GRAPH 2    /* the same launches captured into CUDA graphs */
 #define BFM_MODE_RESIDENT 3 /* one CTA per system, lattice in shared memory (box <= 64^3) */
+#define BFM_MODE_PERSISTENT 4 /* bond codes: one cooperative launch runs a whole chunk of sub-steps,
+                                 grid barriers between the phases (gather systems use GRAPH) */
 
 typedef struct bfm_updater* bfm_handle;
 typedef struct bfm_batch* bfm_batch_handle;

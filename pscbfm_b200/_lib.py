@@ -20,7 +20,7 @@ BFM_ERR_NULL_HANDLE = 5
 BFM_ERR_BUDGET = 6
 BFM_ERR_BUSY = 7
 
-MODE_AUTO, MODE_LAUNCH, MODE_GRAPH, MODE_RESIDENT = 0, 1, 2, 3
+MODE_AUTO, MODE_LAUNCH, MODE_GRAPH, MODE_RESIDENT, MODE_PERSISTENT = 0, 1, 2, 3, 4
 
 DRAW_FN = C.CFUNCTYPE(C.c_uint32, C.c_void_p)
 

@@ -71,6 +71,14 @@ struct SysDev {
     uint32_t forbid[16];             // bit i set <=> bond index i is forbidden
 };
 
+// Grid-wide barrier of the persistent sweep kernel; the host zeroes it before every launch.
+struct GridSync {
+    unsigned int count;   // CTAs arrived at the current barrier
+    unsigned int gen;     // barriers completed
+    unsigned int fault;   // set when a wait ran out; every CTA then leaves and the host reports it
+    unsigned int where;   // the barrier (generation) at which the first wait ran out
+};
+
 // Bond codes: field k (9 bits at 9k) of a monomer's code word is the bond index of
 // (neighbour k - monomer), i.e. the reference's table index (CRITICAL.cu:243-261) of that bond;
 // the count of fields sits above them. Valid only with symmetric neighbour lists, where the

@@ -8,6 +8,7 @@
 #include "bfm_engine.hpp"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <sstream>
 #include <string>
@@ -224,7 +225,7 @@ void Updater::setDrawCallback(DrawFn fn, void* ctx)
 
 void Updater::setMode(int mode)
 {
-    if (mode < kModeAuto || mode > kModeResident) throw std::invalid_argument("[setMode] unknown mode");
+    if (mode < kModeAuto || mode > kModePersistent) throw std::invalid_argument("[setMode] unknown mode");
     if (mode == kModeResident && initialized() && !residentEligible())
         throw std::invalid_argument("[setMode] this system does not fit the resident kernel");
     mode_ = mode;
@@ -326,6 +327,7 @@ void Updater::initialize()
     size_t const oMark = take(8ull * npad_), oLat = take(8ull * nwords), oTmp = take(16ull * nwords);
     size_t const oTab = take(4ull * tab.size()), oGrp = take(4ull * hgrp.size()), oStats = take(kStatBytes);
     size_t const oDesc = take(sizeof(SysDev)), oSteps = take(sizeof(StepEntry) * kStepCap), oList = take(4);
+    size_t const oGs = take(sizeof(GridSync));
     size_t const oPk = take(4ull * npad_), oCode = take(codeBytes * npad_), oNbrr = take(4ull * maxc_ * npad_);
     size_t const oPlane = take(8ull * 768), oMoveOk = take(512);
     Device d;
@@ -363,6 +365,7 @@ void Updater::initialize()
     dev_.dSteps = reinterpret_cast<StepEntry*>(base + oSteps);
     dev_.stepCap = kStepCap;
     dev_.dList = reinterpret_cast<uint32_t*>(base + oList);
+    dev_.gs = reinterpret_cast<GridSync*>(base + oGs);
     h.pk = reinterpret_cast<uint32_t*>(base + oPk);
     h.code = base + oCode;
     h.nbrr = reinterpret_cast<uint32_t*>(base + oNbrr);
@@ -405,6 +408,7 @@ void Updater::initialize()
     cuda_check(cudaMemsetAsync(h.stats, 0, kStatBytes, s), "memset stats");
     cuda_check(cudaMemcpyAsync(dev_.dDesc, &h, sizeof(SysDev), cudaMemcpyHostToDevice, s), "upload descriptor");
     cuda_check(cudaMemsetAsync(dev_.dList, 0, 4, s), "memset list");
+    cuda_check(cudaMemsetAsync(dev_.gs, 0, sizeof(GridSync), s), "memset grid barrier");
     if (!stepsFree_) cuda_check(cudaEventCreateWithFlags(&stepsFree_, cudaEventDisableTiming), "cudaEventCreate");
     if (!batchOnly_) ensureStaging();
     cuda_check(cudaStreamSynchronize(s), "initialize");
@@ -682,8 +686,12 @@ void Updater::ensureStaging()
     // pinned staging of the step entries, allocated on the first run of this system's own paths
     // (systems advanced only by a Batch never need it)
     if (hSteps_) return;
-    cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * kStepCap), "cudaMallocHost(steps)");
+    // one extra entry holds the copy of the persistent kernel's barrier state
+    static_assert(sizeof(GridSync) <= sizeof(StepEntry), "GridSync fits one staging entry");
+    cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * (kStepCap + 1)), "cudaMallocHost(steps)");
     hStepCap_ = kStepCap;
+    hGs_ = reinterpret_cast<GridSync*>(hSteps_ + kStepCap);
+    std::memset(hGs_, 0, sizeof(GridSync));
 }
 
 void Updater::scrubPending(cudaStream_t s)
@@ -869,11 +877,51 @@ void Updater::run(int32_t nMcs)
     int m = mode_;
     if (m == kModeAuto) m = residentEligible() ? kModeResident : kModeGraph;
     if (m == kModeResident && !residentEligible()) m = kModeGraph;
+    if (m == kModePersistent && codeMode_ == kCodeNone) m = kModeGraph;   // bond codes only
     if (m == kModeResident) enqueueResident(nSteps);
     else if (m == kModeGraph) enqueueGraph(nSteps);
+    else if (m == kModePersistent) enqueuePersistent(nSteps);
     else enqueueLaunch(nSteps);
     mcsDone_ += (uint64_t)nMcs;
     hostStale_ = true;
+}
+
+namespace {
+// monomers per thread and CTAs per SM of the persistent kernel (launch_sweep_bc); the environment
+// variable BFM_SWEEP_SHAPE overrides the default for tuning
+int sweep_shape()
+{
+    static int const shape = [] {
+        char const* e = std::getenv("BFM_SWEEP_SHAPE");
+        int const v = e ? std::atoi(e) : 1;
+        return (v >= 0 && v < kSweepShapes) ? v : 1;
+    }();
+    return shape;
+}
+}  // namespace
+
+void Updater::enqueuePersistent(uint32_t nSteps)
+{
+    scrubPending(stream_);   // marks of a previous grid-phase run, left for the next check
+    for (uint32_t done = 0; done < nSteps;) {
+        uint32_t const chunk = std::min(nSteps - done, hStepCap_);
+        cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
+        fillSteps(chunk, hSteps_, false);
+        cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
+                   "steps H2D");
+        cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
+        // count and generation restart at 0; the fault word stays set once a launch has failed
+        cuda_check(cudaMemsetAsync(dev_.gs, 0, 2 * sizeof(unsigned int), stream_), "clear grid barrier");
+        uint32_t grid = 0;
+        cuda_check(launch_sweep_bc(dev_.h, dev_.dSteps, chunk, maxGroup_, dev_.gs, codeMode_, sweep_shape(), stream_,
+                                   &grid),
+                   "persistent sweep");
+        ++launches_;
+        done += chunk;
+    }
+    // the fault word comes back with the next synchronisation
+    cuda_check(cudaMemcpyAsync(hGs_, dev_.gs, sizeof(GridSync), cudaMemcpyDeviceToHost, stream_), "grid status");
+    gsPending_ = true;
 }
 
 void Updater::runSimulationOnGPU(int32_t nMcs)
@@ -890,6 +938,15 @@ void Updater::streamWait(cudaEvent_t e)
 void Updater::synchronize()
 {
     if (stream_) cuda_check(cudaStreamSynchronize(stream_), "sweep");
+    if (gsPending_) {
+        gsPending_ = false;
+        if (hGs_->fault) {
+            std::ostringstream m;
+            m << "[runSimulationOnGPU] a grid barrier of the persistent sweep timed out (barrier " << hGs_->where
+              << "); the system's state is not usable";
+            throw CudaError(m.str());
+        }
+    }
 }
 
 // ============================================================================ read back
@@ -1085,6 +1142,8 @@ void Updater::freeDevice()
     if (hSteps_) {
         cudaFreeHost(hSteps_);
         hSteps_ = nullptr;
+        hGs_ = nullptr;
+        gsPending_ = false;
         hStepCap_ = 0;
     }
     if (stepsFree_) {

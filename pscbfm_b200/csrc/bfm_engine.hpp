@@ -51,6 +51,7 @@ enum Mode : int {
     kModeLaunch = 1,    // two kernel launches per sub-step, like the reference
     kModeGraph = 2,     // the same kernels captured into a CUDA graph per chunk of sub-steps
     kModeResident = 3,  // one CTA runs the whole chunk, lattice in shared memory
+    kModePersistent = 4,   // bond codes: one cooperative launch per chunk, grid barriers between phases
 };
 
 class Updater {
@@ -140,6 +141,7 @@ private:
         StepEntry* dSteps = nullptr;
         uint32_t stepCap = 0;
         uint32_t* dList = nullptr;     // resident kernel system list (one entry: 0)
+        GridSync* gs = nullptr;        // grid barrier of the persistent kernel
     };
     void requireN(char const* who) const;
     void requireInit(char const* who) const;
@@ -147,6 +149,7 @@ private:
     void enqueueLaunch(uint32_t nSteps);
     void enqueueGraph(uint32_t nSteps);
     void enqueueResident(uint32_t nSteps);
+    void enqueuePersistent(uint32_t nSteps);
     void fillSteps(uint32_t nSteps, StepEntry* hostBuf, bool residentParity);
     void freeDevice();
     void ensureStaging();
@@ -181,6 +184,8 @@ private:
     bool hostStale_ = false;
     Device dev_;
     StepEntry* hSteps_ = nullptr;              // pinned staging for step entries
+    GridSync* hGs_ = nullptr;                  // pinned copy of the persistent kernel's barrier state
+    bool gsPending_ = false;                   // hGs_ is being refreshed by the stream
     uint32_t hStepCap_ = 0;
     std::vector<std::pair<uint32_t, cudaGraphExec_t>> graphs_;   // captured chunk length -> graph
     cudaEvent_t stepsFree_ = nullptr;          // host staging may be rewritten after this event

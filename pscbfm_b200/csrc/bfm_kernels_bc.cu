@@ -19,7 +19,9 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 
 #include "bfm_device.cuh"
 #include "bfm_kernels.hpp"
@@ -122,9 +124,20 @@ __device__ __forceinline__ void cell_of(uint32_t pk, uint32_t const* tab, SysDev
     b = brick_bit(x, y, z);
 }
 
+// Loads of state the sweep changes (packed coordinates, codes, flags, lattices): through the
+// read-only data path where one launch only reads them (kNc), plain loads in the persistent
+// kernel, where other CTAs wrote them earlier in the same launch (the read-only path is not
+// coherent with those writes).
+template <bool kNc, typename T>
+__device__ __forceinline__ T ldm(T const* p)
+{
+    if constexpr (kNc) return __ldg(p);
+    else return *p;
+}
+
 // ---------------------------------------------------------------------------------- check
 
-template <typename W, int MPT>
+template <typename W, int MPT, bool kNc = true>
 __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab, StepEntry const& st, uint32_t start,
                                            uint32_t* tally)
 {
@@ -146,10 +159,10 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab,
         uint32_t const i = start + tid + (uint32_t)q * B;
         bool const a = active && i < st.cnt;
         bool const b = i < st.pcnt;   // pcnt is 0 when there is nothing to scrub
-        pk[q] = a ? __ldg(PK + st.off + i) : 0u;
-        code[q] = a ? __ldg(CODE + st.off + i) : W(0);
-        fb[q] = b ? __ldg(fprev + st.poff + i) : (uint8_t)0;
-        pkb[q] = b ? __ldg(PK + st.poff + i) : 0u;
+        pk[q] = a ? ldm<kNc>(PK + st.off + i) : 0u;
+        code[q] = a ? ldm<kNc>(CODE + st.off + i) : W(0);
+        fb[q] = b ? ldm<kNc>(fprev + st.poff + i) : (uint8_t)0;
+        pkb[q] = b ? ldm<kNc>(PK + st.poff + i) : 0u;
     }
     // scrub of the previous sub-step: every set bit of tmp[parity^1] belongs to one of its
     // tentative movers, so zeroing a whole marked word only clears bits that are due
@@ -182,7 +195,7 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab,
         hit[q] = 0ull;
 #pragma unroll
         for (int r = 0; r < 4; ++r)
-            if (ok[q] && pl[q].m[r]) hit[q] |= __ldg(S.lat + pl[q].w[r]) & pl[q].m[r];
+            if (ok[q] && pl[q].m[r]) hit[q] |= ldm<kNc>(S.lat + pl[q].w[r]) & pl[q].m[r];
     }
     // stage 4: decisions
 #pragma unroll
@@ -205,7 +218,7 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab,
 
 // ---------------------------------------------------------------------------------- perform
 
-template <typename W, int MPT>
+template <typename W, int MPT, bool kNc = true>
 __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* tab, StepEntry const& st,
                                              uint32_t start, uint32_t* tally)
 {
@@ -243,7 +256,7 @@ __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* ta
         hit[q] = 0ull;
 #pragma unroll
         for (int r = 0; r < 4; ++r)
-            if ((f[q] & 1u) && pl[q].m[r]) hit[q] |= __ldg(tcur + pl[q].w[r]) & pl[q].m[r];
+            if ((f[q] & 1u) && pl[q].m[r]) hit[q] |= ldm<kNc>(tcur + pl[q].w[r]) & pl[q].m[r];
     }
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
@@ -287,8 +300,8 @@ __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* ta
 
 // ---------------------------------------------------------------------------------- kernels
 
-template <typename W, int MPT, bool kMulti>
-__global__ void __launch_bounds__(kGridBlock) k_check_bc(const __grid_constant__ SysDev S1,
+template <typename W, int MPT, bool kMulti, int kMinBlocks = 1>
+__global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_check_bc(const __grid_constant__ SysDev S1,
                                                          SysDev const* __restrict__ sysv,
                                                          TileRef const* __restrict__ tiles,
                                                          StepEntry const* __restrict__ steps)
@@ -322,8 +335,8 @@ __global__ void __launch_bounds__(kGridBlock) k_check_bc(const __grid_constant__
     }
 }
 
-template <typename W, int MPT, bool kMulti>
-__global__ void __launch_bounds__(kGridBlock) k_perform_bc(const __grid_constant__ SysDev S1,
+template <typename W, int MPT, bool kMulti, int kMinBlocks = 1>
+__global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_perform_bc(const __grid_constant__ SysDev S1,
                                                            SysDev const* __restrict__ sysv,
                                                            TileRef const* __restrict__ tiles,
                                                            StepEntry const* __restrict__ steps)
@@ -351,6 +364,116 @@ __global__ void __launch_bounds__(kGridBlock) k_perform_bc(const __grid_constant
     perform_body<W, MPT>(S, tab, st, start, &tally);
     __syncthreads();
     if (threadIdx.x == 0) tally_flush(tally, S.stats, 2);
+}
+
+// ---------------------------------------------------------------------------------- persistent
+
+constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;   // a wait longer than 2 s is a fault
+
+__device__ __forceinline__ unsigned int ld_acquire_gpu(unsigned int const* p)
+{
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// All CTAs of the cooperative grid meet; every write before the barrier is visible to every
+// thread after it. Thread 0 of each CTA arrives on a counter; the last arrival resets it and opens
+// the next generation; the others wait on the generation with a time limit. Returns false on every
+// thread of the CTA if its wait ran out or another CTA's did (GridSync::fault): the kernel then
+// leaves, and the host reports the fault.
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned int& gen, unsigned int* okSm)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int ok = 1u;
+        unsigned int const g = gen;
+        __threadfence();
+        if (atomicAdd(&gs->count, 1u) == gridDim.x - 1u) {
+            atomicExch(&gs->count, 0u);
+            __threadfence();
+            atomicExch(&gs->gen, g + 1u);
+        } else {
+            unsigned long long const t0 = global_ns();
+            unsigned int polls = 0u;
+            while (ld_acquire_gpu(&gs->gen) == g) {
+                if (ld_acquire_gpu(&gs->fault) != 0u) {
+                    ok = 0u;
+                    break;
+                }
+                // a time limit, and a poll count as a second bound that does not trust the timer
+                if (global_ns() - t0 > kBarrierTimeoutNs || ++polls > (1u << 26)) {
+                    if (atomicExch(&gs->fault, 1u) == 0u) gs->where = g;
+                    ok = 0u;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        gen = g + 1u;
+        *okSm = ok;
+    }
+    __syncthreads();
+    return *okSm != 0u;
+}
+
+// One system, a whole run of sub-steps in one cooperative launch: per sub-step the check phase
+// over every tile, a grid barrier, the perform phase and (between sub-steps) another barrier. CTA b
+// takes tiles b, b + gridDim.x, ... of kGridBlock * MPT in-colour indices. Same bodies as
+// k_check_bc / k_perform_bc, with plain loads of the state other CTAs change during the launch;
+// the step entries are prefetched one sub-step ahead and the move counters flushed once.
+template <typename W, int MPT, int kMinBlocks>
+__global__ void __launch_bounds__(kGridBlock, kMinBlocks)
+    k_sweep_bc(const __grid_constant__ SysDev S, StepEntry const* __restrict__ steps, uint32_t nSteps,
+               uint32_t nTiles, GridSync* gs)
+{
+    __shared__ uint32_t tab[kMaxTab];
+    __shared__ uint32_t tallyT, tallyA, okSm;
+    if (ld_acquire_gpu(&gs->fault) != 0u) return;   // an earlier launch failed: the state is not usable
+    uint32_t const ntab = S.nb[0] + S.nb[1] + S.nb[2];
+    for (uint32_t w = threadIdx.x; w < ntab; w += blockDim.x) tab[w] = S.brickTab[w];
+    if (threadIdx.x == 0) {
+        tallyT = 0u;
+        tallyA = 0u;
+    }
+    __syncthreads();
+    constexpr uint32_t span = kGridBlock * MPT;
+    unsigned int gen = 0u;
+    unsigned long long att = 0ull;
+    StepEntry next = steps[0];
+    for (uint32_t t = 0; t < nSteps; ++t) {
+        StepEntry const st = next;
+        if (t + 1 < nSteps) next = steps[t + 1];
+        for (uint32_t k = blockIdx.x; k < nTiles; k += gridDim.x) {
+            uint32_t const start = k * span;
+            if (start >= st.cnt && start >= st.pcnt) break;
+            check_body<W, MPT, false>(S, tab, st, start, &tallyT);
+        }
+        if (st.color != kNoColor) att += st.cnt;
+        if (!grid_barrier(gs, gen, &okSm)) return;
+        if (st.color != kNoColor) {
+            for (uint32_t k = blockIdx.x; k < nTiles; k += gridDim.x) {
+                uint32_t const start = k * span;
+                if (start >= st.cnt) break;
+                perform_body<W, MPT, false>(S, tab, st, start, &tallyA);
+            }
+        }
+        if (t + 1 < nSteps && !grid_barrier(gs, gen, &okSm)) return;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        tally_flush(tallyT, S.stats, 1);
+        tally_flush(tallyA, S.stats, 2);
+        if (blockIdx.x == 0 && att) atomicAdd(S.stats, att);
+    }
 }
 
 // ---------------------------------------------------------------------------------- resident
@@ -498,17 +621,46 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
 
 namespace {
 
+// CTAs per SM the compiler must fit (register budget) for check / perform: shape 0 leaves the
+// registers free, 1 (the default: 40 / 48 registers, no spills, 1.15 / 1.38 waves on the 256^3
+// melt) asks 6 / 5, 2 asks 6 / 6. The environment variable BFM_GRID_SHAPE selects one for tuning.
+int grid_shape()
+{
+    static int const shape = [] {
+        char const* e = std::getenv("BFM_GRID_SHAPE");
+        int const v = e ? std::atoi(e) : 1;
+        return (v >= 0 && v <= 2) ? v : 1;
+    }();
+    return shape;
+}
+
+template <typename W, bool kMulti, int kMinCheck, int kMinPerform>
+void launch_grid_bc_k(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
+                      uint32_t nTiles, StepEntry const* dSteps, cudaStream_t s)
+{
+    if (check)
+        k_check_bc<W, kCheckMpt, kMulti, kMinCheck><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
+    else
+        k_perform_bc<W, kCheckMpt, kMulti, kMinPerform><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
+}
+
+template <typename W, bool kMulti>
+void launch_grid_bc_m(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
+                      uint32_t nTiles, StepEntry const* dSteps, cudaStream_t s)
+{
+    switch (grid_shape()) {
+    case 1: launch_grid_bc_k<W, kMulti, 6, 5>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
+    case 2: launch_grid_bc_k<W, kMulti, 6, 6>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
+    default: launch_grid_bc_k<W, kMulti, 1, 1>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
+    }
+}
+
 template <typename W>
 cudaError_t launch_grid_bc(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
                            uint32_t nTiles, StepEntry const* dSteps, cudaStream_t s)
 {
-    if (dTiles) {
-        if (check) k_check_bc<W, kCheckMpt, true><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
-        else k_perform_bc<W, kCheckMpt, true><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
-    } else {
-        if (check) k_check_bc<W, kCheckMpt, false><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
-        else k_perform_bc<W, kCheckMpt, false><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
-    }
+    if (dTiles) launch_grid_bc_m<W, true>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s);
+    else launch_grid_bc_m<W, false>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s);
     return cudaGetLastError();
 }
 
@@ -531,6 +683,61 @@ cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRe
     if (codeMode == kCode32) return launch_grid_bc<uint32_t>(false, hostDesc, dSys, dTiles, nTiles, dSteps, s);
     if (codeMode == kCode64)
         return launch_grid_bc<unsigned long long>(false, hostDesc, dSys, dTiles, nTiles, dSteps, s);
+    return cudaErrorInvalidValue;
+}
+
+namespace {
+
+template <typename W, int MPT, int kMinBlocks>
+cudaError_t launch_sweep_bc_k(SysDev const& S, StepEntry const* dSteps, uint32_t nSteps, uint32_t maxGroup,
+                              GridSync* gs, cudaStream_t s, uint32_t* gridOut)
+{
+    // co-resident CTAs per SM and SM count, once per device and instantiation
+    static thread_local int occ[64] = {}, nsm[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (!occ[dev & 63]) {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[dev & 63], k_sweep_bc<W, MPT, kMinBlocks>, kGridBlock, 0);
+        if (e != cudaSuccess) return e;
+        e = cudaDeviceGetAttribute(&nsm[dev & 63], cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        if (occ[dev & 63] < 1) return cudaErrorInvalidConfiguration;
+    }
+    uint32_t nTiles = (maxGroup + kGridBlock * MPT - 1) / (kGridBlock * MPT);
+    if (nTiles == 0) nTiles = 1;
+    uint32_t const grid = std::min<uint32_t>(nTiles, (uint32_t)(occ[dev & 63] * nsm[dev & 63]));
+    void* args[] = {const_cast<SysDev*>(&S), &dSteps, &nSteps, &nTiles, &gs};
+    e = cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(k_sweep_bc<W, MPT, kMinBlocks>), dim3(grid),
+                                    dim3(kGridBlock), args, 0, s);
+    if (gridOut) *gridOut = grid;
+    return e;
+}
+
+template <typename W>
+cudaError_t launch_sweep_bc_w(SysDev const& S, StepEntry const* dSteps, uint32_t nSteps, uint32_t maxGroup,
+                              GridSync* gs, int shape, cudaStream_t s, uint32_t* gridOut)
+{
+    switch (shape) {
+    case 0: return launch_sweep_bc_k<W, 2, 4>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
+    case 1: return launch_sweep_bc_k<W, 2, 5>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
+    case 2: return launch_sweep_bc_k<W, 1, 8>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
+    case 3: return launch_sweep_bc_k<W, 4, 3>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
+    case 4: return launch_sweep_bc_k<W, 1, 6>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_sweep_bc(SysDev const& hostDesc, StepEntry const* dSteps, uint32_t nSteps, uint32_t maxGroup,
+                            GridSync* gs, uint32_t codeMode, int shape, cudaStream_t s, uint32_t* gridOut)
+{
+    if (nSteps == 0) return cudaSuccess;
+    if (codeMode == kCode32)
+        return launch_sweep_bc_w<uint32_t>(hostDesc, dSteps, nSteps, maxGroup, gs, shape, s, gridOut);
+    if (codeMode == kCode64)
+        return launch_sweep_bc_w<unsigned long long>(hostDesc, dSteps, nSteps, maxGroup, gs, shape, s, gridOut);
     return cudaErrorInvalidValue;
 }
 

@@ -13,7 +13,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import MODE_AUTO, MODE_GRAPH, MODE_LAUNCH, MODE_RESIDENT  # noqa: F401
+from ._lib import MODE_AUTO, MODE_GRAPH, MODE_LAUNCH, MODE_PERSISTENT, MODE_RESIDENT  # noqa: F401
 
 REPR_AUTO, REPR_GATHER = 0, 1
 

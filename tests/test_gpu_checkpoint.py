@@ -9,7 +9,7 @@ from pscbfm_b200 import systems as S
 
 pytestmark = pytest.mark.gpu
 
-MODES = {"graph": P.MODE_GRAPH, "resident": P.MODE_RESIDENT, "launch": P.MODE_LAUNCH}
+MODES = {"graph": P.MODE_GRAPH, "resident": P.MODE_RESIDENT, "launch": P.MODE_LAUNCH, "persistent": P.MODE_PERSISTENT}
 
 
 @pytest.mark.parametrize("mode", list(MODES))

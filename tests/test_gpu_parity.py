@@ -12,7 +12,8 @@ from pscbfm_b200 import systems as S
 
 pytestmark = pytest.mark.gpu
 
-MODES = {"launch": P.MODE_LAUNCH, "graph": P.MODE_GRAPH, "resident": P.MODE_RESIDENT, "auto": P.MODE_AUTO}
+MODES = {"launch": P.MODE_LAUNCH, "graph": P.MODE_GRAPH, "resident": P.MODE_RESIDENT, "auto": P.MODE_AUTO,
+         "persistent": P.MODE_PERSISTENT}
 REPRS = {"codes": P.REPR_AUTO, "gather": P.REPR_GATHER}
 
 
@@ -35,7 +36,7 @@ def _resident_ok(s):
 
 
 @pytest.mark.parametrize("repr_", ["codes", "gather"])
-@pytest.mark.parametrize("mode", ["launch", "graph", "resident"])
+@pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent"])
 @pytest.mark.parametrize("name", list(CASES))
 def test_engine_reproduces_reference_updater(name, mode, repr_):
     g = json.load(open(GOLDEN_JSON))["cases"][name]
@@ -86,7 +87,7 @@ def test_six_functional_network_vs_oracle(mode, repr_):
 
 
 @pytest.mark.parametrize("repr_", ["codes", "gather"])
-@pytest.mark.parametrize("mode", ["launch", "graph", "resident"])
+@pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent"])
 @pytest.mark.parametrize("walls", [1, 4, 6])
 def test_partial_walls_vs_oracle(walls, mode, repr_):
     # the reference has builds for fully periodic and fully walled boxes only: mixed periodicity
@@ -98,7 +99,7 @@ def test_partial_walls_vs_oracle(walls, mode, repr_):
     assert (st["attempted"], st["tentative"], st["accepted"]) == ost
 
 
-@pytest.mark.parametrize("mode", ["launch", "graph", "resident"])
+@pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent"])
 def test_hydrogel_fixture_with_walls_vs_oracle(mode):
     # the reference's non-periodic hydrogel (tests/coloring-test-Hydrogel...bfm): up to 5 bonds per
     # monomer, more than the reference build's MAX_CONNECTIVITY, so the oracle pins it
@@ -132,13 +133,17 @@ def test_dense_melt_full_config():
 
 def test_mode_switches_mid_run():
     s = S.serpentine_chains(64, 32, 0.35, seed=21)
-    ref, _ = O.run(s, 90)
+    ref, _ = O.run(s, 150)
     u = P.UpdaterGPUScBFM_AB_Type(0)
     u.load_system(s, mode=P.MODE_LAUNCH)
     u.runSimulationOnGPU(30)
     u.set_mode(P.MODE_RESIDENT)
     u.runSimulationOnGPU(30)
     u.set_mode(P.MODE_GRAPH)
+    u.runSimulationOnGPU(30)
+    u.set_mode(P.MODE_PERSISTENT)
+    u.runSimulationOnGPU(30)
+    u.set_mode(P.MODE_LAUNCH)
     u.runSimulationOnGPU(30)
     assert np.array_equal(u.get_coords(), ref)
     u.close()
