@@ -62,6 +62,9 @@ struct SysDev {
     uint32_t const* nbrr;            // [maxc][npad] neighbour slot | reverse slot << 28
     unsigned long long const* planeTab;   // [3][4][4][4][4] front-plane masks (see plane_table_fill)
     uint8_t const* moveOk;           // [512] bit d: a bond with this index stays allowed after move d
+    uint32_t* mlist;                 // [2][listStride] tentative movers per tile segment, per parity
+    uint32_t* mcount;                // [2][countStride] entries of each segment
+    uint32_t listStride, countStride;
     uint32_t codeMode;               // kCodeNone, kCode32, kCode64
     uint32_t walls;                  // bit a: axis a is not periodic (corners stay in [0, L-2])
     uint32_t npad, nwords, maxc, nColors;

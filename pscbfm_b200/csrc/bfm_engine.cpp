@@ -297,7 +297,8 @@ void Updater::initialize()
     // m-th occurrence of j in i's list pairing with the m-th occurrence of i in j's) and <= 6
     // bonds per monomer
     codeMode_ = kCodeNone;
-    if (repr_ == kReprAuto && maxc_ <= 6) {
+    // (mover-list entries hold a slot in 27 bits)
+    if (repr_ == kReprAuto && maxc_ <= 6 && npad_ < (1u << 27)) {
         bool sym = true;
         for (uint32_t i = 0; i < n_ && sym; ++i)
             for (uint32_t k = 0; k < nbrCnt_[i] && sym; ++k) {
@@ -330,6 +331,9 @@ void Updater::initialize()
     size_t const oGs = take(sizeof(GridSync));
     size_t const oPk = take(4ull * npad_), oCode = take(codeBytes * npad_), oNbrr = take(4ull * maxc_ * npad_);
     size_t const oPlane = take(8ull * 768), oMoveOk = take(512);
+    // mover lists of the bond-code grid kernels: one segment of kBcTileSpan entries per tile
+    uint32_t const segs = codeMode_ == kCodeNone ? 0u : std::max((maxGroup_ + kBcTileSpan - 1) / kBcTileSpan, 1u);
+    size_t const oMlist = take(4ull * 2 * segs * kBcTileSpan), oMcount = take(4ull * 2 * segs);
     Device d;
     d.bytes = off;
     // stream-ordered: freeing it later does not wait for the whole device
@@ -371,6 +375,10 @@ void Updater::initialize()
     h.nbrr = reinterpret_cast<uint32_t*>(base + oNbrr);
     h.planeTab = reinterpret_cast<unsigned long long*>(base + oPlane);
     h.moveOk = reinterpret_cast<uint8_t*>(base + oMoveOk);
+    h.mlist = reinterpret_cast<uint32_t*>(base + oMlist);
+    h.mcount = reinterpret_cast<uint32_t*>(base + oMcount);
+    h.listStride = segs * kBcTileSpan;
+    h.countStride = segs;
     h.codeMode = codeMode_;
     h.walls = walls_;
 
@@ -409,6 +417,7 @@ void Updater::initialize()
     cuda_check(cudaMemcpyAsync(dev_.dDesc, &h, sizeof(SysDev), cudaMemcpyHostToDevice, s), "upload descriptor");
     cuda_check(cudaMemsetAsync(dev_.dList, 0, 4, s), "memset list");
     cuda_check(cudaMemsetAsync(dev_.gs, 0, sizeof(GridSync), s), "memset grid barrier");
+    if (segs) cuda_check(cudaMemsetAsync(h.mcount, 0, 4ull * 2 * segs, s), "memset mover counts");
     if (!stepsFree_) cuda_check(cudaEventCreateWithFlags(&stepsFree_, cudaEventDisableTiming), "cudaEventCreate");
     if (!batchOnly_) ensureStaging();
     cuda_check(cudaStreamSynchronize(s), "initialize");

@@ -49,8 +49,9 @@ cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRe
 // Persistent sweep (bond codes, one system): nSteps sub-steps of check, grid barrier, perform in
 // one cooperative launch of at most the co-resident CTA count. gs must be zeroed before the launch;
 // after it, gs->fault != 0 means a barrier wait ran out and the system's state is not usable.
-// shape selects monomers per thread and CTAs per SM: 0 (2, 4), 1 (2, 5), 2 (1, 8), 3 (4, 3), 4 (1, 6).
-constexpr int kSweepShapes = 5;
+// shape selects the CTAs per SM the register budget must fit: 0 -> 4, 1 -> 5, 2 -> 6 (two monomers
+// per thread, one mover-list segment per tile).
+constexpr int kSweepShapes = 3;
 cudaError_t launch_sweep_bc(SysDev const& hostDesc, StepEntry const* dSteps, uint32_t nSteps, uint32_t maxGroup,
                             GridSync* gs, uint32_t codeMode, int shape, cudaStream_t s, uint32_t* gridOut);
 size_t resident_bc_smem_bytes(uint32_t nwords, uint32_t ntab, uint32_t npad, uint32_t maxGroup, uint32_t codeMode);

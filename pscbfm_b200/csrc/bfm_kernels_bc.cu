@@ -135,41 +135,52 @@ __device__ __forceinline__ T ldm(T const* p)
     else return *p;
 }
 
+// Mover lists: the check of sub-step t appends each tentative mover of tile k (kBcTileSpan
+// in-colour indices) to segment k of list[parity] and stores the segment's length in
+// count[parity][k]; the perform walks only those entries and marks the applied ones; the check of
+// sub-step t+1 walks them again to zero the temporary-lattice words they marked. Entry: slot g
+// (bits 0-26), direction (27-29), applied (31).
+constexpr uint32_t kEntSlotMask = (1u << 27) - 1u;
+constexpr uint32_t kEntApplied = 1u << 31;
+
 // ---------------------------------------------------------------------------------- check
 
 template <typename W, int MPT, bool kNc = true>
 __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab, StepEntry const& st, uint32_t start,
-                                           uint32_t* tally)
+                                           uint32_t* segCount)
 {
     uint32_t const B = blockDim.x, tid = threadIdx.x;
     uint32_t const* const PK = S.pk;
     W const* const CODE = static_cast<W const*>(S.code);
-    uint8_t const* const fprev = S.flags + (size_t)(st.parity ^ 1u) * S.npad;
+    uint32_t const tile = start / kBcTileSpan;
     unsigned long long* const tprev = S.tmp + (size_t)(st.parity ^ 1u) * S.nwords;
-    uint8_t* const fcur = S.flags + (size_t)st.parity * S.npad;
     unsigned long long* const tcur = S.tmp + (size_t)st.parity * S.nwords;
+    uint32_t const* const lprev = S.mlist + (size_t)(st.parity ^ 1u) * S.listStride + (size_t)tile * kBcTileSpan;
+    uint32_t* const lcur = S.mlist + (size_t)st.parity * S.listStride + (size_t)tile * kBcTileSpan;
     bool const active = st.color != kNoColor;
 
-    // stage 1: every independent load of the pass
-    uint32_t pk[MPT], pkb[MPT];
+    // stage 1: every independent load of the pass (the previous sub-step's movers of this tile
+    // come from its list; pcnt is 0 when there is nothing to scrub)
+    uint32_t const nPrev = start < st.pcnt ? ldm<kNc>(S.mcount + (size_t)(st.parity ^ 1u) * S.countStride + tile) : 0u;
+    uint32_t pk[MPT], ent[MPT];
     W code[MPT];
-    uint8_t fb[MPT];
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
         uint32_t const i = start + tid + (uint32_t)q * B;
+        uint32_t const e = tid + (uint32_t)q * B;
         bool const a = active && i < st.cnt;
-        bool const b = i < st.pcnt;   // pcnt is 0 when there is nothing to scrub
         pk[q] = a ? ldm<kNc>(PK + st.off + i) : 0u;
         code[q] = a ? ldm<kNc>(CODE + st.off + i) : W(0);
-        fb[q] = b ? ldm<kNc>(fprev + st.poff + i) : (uint8_t)0;
-        pkb[q] = b ? ldm<kNc>(PK + st.poff + i) : 0u;
+        ent[q] = e < nPrev ? ldm<kNc>(lprev + e) : 0u;
     }
     // scrub of the previous sub-step: every set bit of tmp[parity^1] belongs to one of its
     // tentative movers, so zeroing a whole marked word only clears bits that are due
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
-        if (fb[q] & 1u) {
-            uint32_t const target = (fb[q] & 2u) ? pkb[q] : step_pk(pkb[q], (fb[q] >> 2) & 7u, S.mask);
+        uint32_t const e = tid + (uint32_t)q * B;
+        if (e < nPrev) {
+            uint32_t const pkb = ldm<kNc>(PK + (ent[q] & kEntSlotMask));
+            uint32_t const target = (ent[q] & kEntApplied) ? pkb : step_pk(pkb, (ent[q] >> 27) & 7u, S.mask);
             uint32_t w, b;
             cell_of(target, tab, S, w, b);
             tprev[w] = 0ull;
@@ -197,27 +208,30 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab,
         for (int r = 0; r < 4; ++r)
             if (ok[q] && pl[q].m[r]) hit[q] |= ldm<kNc>(S.lat + pl[q].w[r]) & pl[q].m[r];
     }
-    // stage 4: decisions
+    // stage 4: decisions; tentative movers go to this tile's list segment (one shared-memory
+    // atomic per warp reserves the warp's slots)
+    uint32_t const lane = tid & 31u;
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
         uint32_t const i = start + tid + (uint32_t)q * B;
         bool const go = ok[q] && hit[q] == 0ull;
-        if (i < st.cnt) {
-            uint8_t f = 0;
-            if (go) {
-                uint32_t w, b;
-                cell_of(step_pk(pk[q], dir[q], S.mask), tab, S, w, b);
-                atomicOr(tcur + w, 1ull << b);
-                f = (uint8_t)((dir[q] << 2) | 1u);
-            }
-            fcur[st.off + i] = f;
+        uint32_t const bal = __ballot_sync(0xffffffffu, go);
+        uint32_t base = 0;
+        if (lane == 0 && bal) base = atomicAdd(segCount, (uint32_t)__popc(bal));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (go) {
+            uint32_t w, b;
+            cell_of(step_pk(pk[q], dir[q], S.mask), tab, S, w, b);
+            atomicOr(tcur + w, 1ull << b);
+            lcur[base + __popc(bal & ((1u << lane) - 1u))] = (st.off + i) | (dir[q] << 27);
         }
-        tally_warp(go, tally);
     }
 }
 
 // ---------------------------------------------------------------------------------- perform
 
+// Walks the tentative movers the check listed for this tile (dense: no thread waits on a monomer
+// that did not move).
 template <typename W, int MPT, bool kNc = true>
 __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* tab, StepEntry const& st,
                                              uint32_t start, uint32_t* tally)
@@ -225,45 +239,53 @@ __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* ta
     uint32_t const B = blockDim.x, tid = threadIdx.x;
     uint32_t* const PK = S.pk;
     W* const CODE = static_cast<W*>(S.code);
-    uint8_t* const fcur = S.flags + (size_t)st.parity * S.npad;
+    uint32_t const tile = start / kBcTileSpan;
     unsigned long long const* const tcur = S.tmp + (size_t)st.parity * S.nwords;
+    uint32_t* const lcur = S.mlist + (size_t)st.parity * S.listStride + (size_t)tile * kBcTileSpan;
+    uint32_t const nCur = ldm<kNc>(S.mcount + (size_t)st.parity * S.countStride + tile);
+    if (tid >= nCur) return;
 
-    uint8_t f[MPT];
-    uint32_t pk[MPT];
+    uint32_t ent[MPT], pk[MPT];
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
-        uint32_t const i = start + tid + (uint32_t)q * B;
-        bool const a = i < st.cnt;
-        f[q] = a ? fcur[st.off + i] : (uint8_t)0;
-        pk[q] = a ? PK[st.off + i] : 0u;
+        uint32_t const e = tid + (uint32_t)q * B;
+        ent[q] = e < nCur ? ldm<kNc>(lcur + e) : 0u;
     }
     Plane pl[MPT];
     W code[MPT];
     uint32_t nbr[MPT][CodeWord<W>::kSlots];
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
-        uint32_t const g = st.off + start + tid + (uint32_t)q * B;
-        bool const t = f[q] & 1u;
-        front_plane<false>(pl[q], tab, S.planeTab, S, pk[q], (f[q] >> 2) & 7u);
+        uint32_t const e = tid + (uint32_t)q * B;
+        bool const t = e < nCur;
+        uint32_t const g = ent[q] & kEntSlotMask;
+        pk[q] = t ? PK[g] : 0u;
         code[q] = t ? CODE[g] : W(0);
 #pragma unroll
         for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k)
             nbr[q][k] = (t && k < S.maxc) ? __ldg(S.nbrr + (size_t)k * S.npad + g) : 0u;
     }
+#pragma unroll
+    for (int q = 0; q < MPT; ++q) front_plane<false>(pl[q], tab, S.planeTab, S, pk[q], (ent[q] >> 27) & 7u);
     unsigned long long hit[MPT];
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
+        uint32_t const e = tid + (uint32_t)q * B;
         hit[q] = 0ull;
 #pragma unroll
         for (int r = 0; r < 4; ++r)
-            if ((f[q] & 1u) && pl[q].m[r]) hit[q] |= ldm<kNc>(tcur + pl[q].w[r]) & pl[q].m[r];
+            if (e < nCur && pl[q].m[r]) hit[q] |= ldm<kNc>(tcur + pl[q].w[r]) & pl[q].m[r];
     }
+    uint32_t nAcc = 0;
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
-        uint32_t const g = st.off + start + tid + (uint32_t)q * B;
-        bool const go = (f[q] & 1u) && hit[q] == 0ull;
+        uint32_t const e = tid + (uint32_t)q * B;
+        uint32_t const g = ent[q] & kEntSlotMask;
+        bool const go = e < nCur && hit[q] == 0ull;
         if (go) {
-            uint32_t const dir = (f[q] >> 2) & 7u;
+            ++nAcc;
+            lcur[e] = ent[q] | kEntApplied;
+            uint32_t const dir = (ent[q] >> 27) & 7u;
             uint32_t const a = dir >> 1;
             int32_t const s = (dir & 1u) ? 1 : -1;
             uint32_t const pk1 = step_pk(pk[q], dir, S.mask);
@@ -278,22 +300,21 @@ __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* ta
             }
             PK[g] = pk1;
             atomicAdd((a == 0 ? S.x : (a == 1 ? S.y : S.z)) + g, s);
-            fcur[g] = (uint8_t)(f[q] | 2u);
             W const own = code[q];
             CODE[g] = code_shift(own, a, -s);
             uint32_t const n = uint32_t(own >> CodeWord<W>::kCountShift) & 7u;
 #pragma unroll
             for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k) {
                 if (k < n) {
-                    uint32_t const e = nbr[q][k];
+                    uint32_t const nb = nbr[q][k];
                     uint32_t const c = (0u - (uint32_t(own >> (9u * k + 3u * a)) & 7u)) & 7u;   // reverse field
                     uint32_t const nc = uint32_t(int32_t(c) + s) & 7u;
-                    atomicXor(CODE + (e & kSlotMask), W(c ^ nc) << (9u * (e >> kSlotShift) + 3u * a));
+                    atomicXor(CODE + (nb & kSlotMask), W(c ^ nc) << (9u * (nb >> kSlotShift) + 3u * a));
                 }
             }
         }
-        tally_warp(go, tally);
     }
+    if (nAcc) atomicAdd(tally, nAcc);   // threads past the list returned early: no warp-wide vote here
 }
 
 }  // namespace
@@ -322,16 +343,18 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_check_bc(const __gri
         __syncthreads();
     }
     SysDev const& S = kMulti ? Sm : S1;
-    __shared__ uint32_t tally;
+    static_assert(kGridBlock * MPT == kBcTileSpan, "a CTA covers one list segment");
+    __shared__ uint32_t segCount;
     uint32_t const ntab = S.nb[0] + S.nb[1] + S.nb[2];
     for (uint32_t w = threadIdx.x; w < ntab; w += blockDim.x) tab[w] = S.brickTab[w];
-    if (threadIdx.x == 0) tally = 0;
+    if (threadIdx.x == 0) segCount = 0;
     __syncthreads();
-    check_body<W, MPT>(S, tab, st, start, &tally);
+    check_body<W, MPT>(S, tab, st, start, &segCount);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        tally_flush(tally, S.stats, 1);
-        if (start == 0 && st.color != kNoColor) tally_flush(st.cnt, S.stats, 0);
+    if (threadIdx.x == 0 && st.color != kNoColor) {
+        S.mcount[(size_t)st.parity * S.countStride + start / kBcTileSpan] = segCount;
+        tally_flush(segCount, S.stats, 1);
+        if (start == 0) tally_flush(st.cnt, S.stats, 0);
     }
 }
 
@@ -435,8 +458,9 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
     k_sweep_bc(const __grid_constant__ SysDev S, StepEntry const* __restrict__ steps, uint32_t nSteps,
                uint32_t nTiles, GridSync* gs)
 {
+    static_assert(kGridBlock * MPT == kBcTileSpan, "a tile is one list segment");
     __shared__ uint32_t tab[kMaxTab];
-    __shared__ uint32_t tallyT, tallyA, okSm;
+    __shared__ uint32_t tallyT, tallyA, okSm, segCount;
     if (ld_acquire_gpu(&gs->fault) != 0u) return;   // an earlier launch failed: the state is not usable
     uint32_t const ntab = S.nb[0] + S.nb[1] + S.nb[2];
     for (uint32_t w = threadIdx.x; w < ntab; w += blockDim.x) tab[w] = S.brickTab[w];
@@ -455,7 +479,14 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
         for (uint32_t k = blockIdx.x; k < nTiles; k += gridDim.x) {
             uint32_t const start = k * span;
             if (start >= st.cnt && start >= st.pcnt) break;
-            check_body<W, MPT, false>(S, tab, st, start, &tallyT);
+            if (threadIdx.x == 0) segCount = 0u;
+            __syncthreads();
+            check_body<W, MPT, false>(S, tab, st, start, &segCount);
+            __syncthreads();
+            if (threadIdx.x == 0 && st.color != kNoColor) {
+                S.mcount[(size_t)st.parity * S.countStride + k] = segCount;
+                tallyT += segCount;
+            }
         }
         if (st.color != kNoColor) att += st.cnt;
         if (!grid_barrier(gs, gen, &okSm)) return;
@@ -719,11 +750,9 @@ cudaError_t launch_sweep_bc_w(SysDev const& S, StepEntry const* dSteps, uint32_t
                               GridSync* gs, int shape, cudaStream_t s, uint32_t* gridOut)
 {
     switch (shape) {
-    case 0: return launch_sweep_bc_k<W, 2, 4>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
-    case 1: return launch_sweep_bc_k<W, 2, 5>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
-    case 2: return launch_sweep_bc_k<W, 1, 8>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
-    case 3: return launch_sweep_bc_k<W, 4, 3>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
-    case 4: return launch_sweep_bc_k<W, 1, 6>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
+    case 0: return launch_sweep_bc_k<W, kCheckMpt, 4>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
+    case 1: return launch_sweep_bc_k<W, kCheckMpt, 5>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
+    case 2: return launch_sweep_bc_k<W, kCheckMpt, 6>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
     default: return cudaErrorInvalidValue;
     }
 }
