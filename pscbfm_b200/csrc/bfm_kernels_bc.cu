@@ -7,11 +7,14 @@
 // own fields change by -d and the reverse field of every neighbour by +d; the reverse field's old
 // value is the negation (mod 8) of the monomer's own field, so the update needs no extra load.
 //
-// Grid phase (k_check_bc, k_perform_bc): flags are double-buffered by sub-step parity, so the
-// check of sub-step t also zeroes the temporary-lattice words marked at t-1 (found from
-// flags[parity^1] and pk, both read-only during the check). Every independent load of a pass is
-// issued before any dependent one; a single-system launch takes the descriptor as a grid-constant
-// parameter.
+// Grid phase (k_check_bc, k_perform_bc): the check lists its tentative movers per tile (mover
+// lists, double-buffered by sub-step parity); the perform walks only those lists, and the check of
+// sub-step t also zeroes the temporary-lattice words marked at t-1 (found from list[parity^1] and
+// pk, both read-only during the check). Every independent load of a pass is issued before any
+// dependent one; a single-system launch takes the descriptor as a grid-constant parameter.
+//
+// Persistent (k_sweep_bc): the same bodies for a whole run of sub-steps in one cooperative launch,
+// with time-bounded grid barriers between the phases.
 //
 // Resident (k_resident_bc): one CTA owns a small system for a chunk of sub-steps; lattice, one
 // temporary lattice, pk and bond codes in shared memory; the check appends tentative movers to a
@@ -142,6 +145,9 @@ __device__ __forceinline__ T ldm(T const* p)
 // (bits 0-26), direction (27-29), applied (31).
 constexpr uint32_t kEntSlotMask = (1u << 27) - 1u;
 constexpr uint32_t kEntApplied = 1u << 31;
+// tiles whose movers one perform CTA of a single-system launch walks (about 17 % of a tile's
+// monomers are tentative, so one tile leaves most of a CTA idle)
+constexpr uint32_t kPerformTiles = 4;
 
 // ---------------------------------------------------------------------------------- check
 
@@ -230,91 +236,114 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab,
 
 // ---------------------------------------------------------------------------------- perform
 
-// Walks the tentative movers the check listed for this tile (dense: no thread waits on a monomer
-// that did not move).
-template <typename W, int MPT, bool kNc = true>
-__device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* tab, StepEntry const& st,
-                                             uint32_t start, uint32_t* tally)
+// Entries e, e + B, ... (MPT of them, those below total) of the concatenated mover lists of nT
+// tiles (pre: the lists' starting offsets, lbase: the first tile's segment): re-test the front
+// plane on the temporary lattice and apply the free moves. Returns the moves applied.
+template <typename W, int MPT, bool kNc>
+__device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t const* tab,
+                                                  unsigned long long const* tcur, uint32_t* lbase,
+                                                  uint32_t const* pre, uint32_t nT, uint32_t total, uint32_t e)
 {
-    uint32_t const B = blockDim.x, tid = threadIdx.x;
+    uint32_t const B = blockDim.x;
     uint32_t* const PK = S.pk;
     W* const CODE = static_cast<W*>(S.code);
-    uint32_t const tile = start / kBcTileSpan;
-    unsigned long long const* const tcur = S.tmp + (size_t)st.parity * S.nwords;
-    uint32_t* const lcur = S.mlist + (size_t)st.parity * S.listStride + (size_t)tile * kBcTileSpan;
-    uint32_t const nCur = ldm<kNc>(S.mcount + (size_t)st.parity * S.countStride + tile);
-    if (tid >= nCur) return;
-
-    uint32_t ent[MPT], pk[MPT];
+    uint32_t ent[MPT], pk[MPT], li[MPT];
+    bool live[MPT];
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
-        uint32_t const e = tid + (uint32_t)q * B;
-        ent[q] = e < nCur ? ldm<kNc>(lcur + e) : 0u;
+        uint32_t const eq = e + (uint32_t)q * B;
+        uint32_t j = 0;
+        while (j + 1 < nT && eq >= pre[j + 1]) ++j;
+        live[q] = eq < total;
+        li[q] = j * kBcTileSpan + (eq - pre[j]);
+        ent[q] = live[q] ? ldm<kNc>(lbase + li[q]) : 0u;
     }
     Plane pl[MPT];
     W code[MPT];
     uint32_t nbr[MPT][CodeWord<W>::kSlots];
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
-        uint32_t const e = tid + (uint32_t)q * B;
-        bool const t = e < nCur;
         uint32_t const g = ent[q] & kEntSlotMask;
-        pk[q] = t ? PK[g] : 0u;
-        code[q] = t ? CODE[g] : W(0);
+        pk[q] = live[q] ? PK[g] : 0u;
+        code[q] = live[q] ? CODE[g] : W(0);
 #pragma unroll
         for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k)
-            nbr[q][k] = (t && k < S.maxc) ? __ldg(S.nbrr + (size_t)k * S.npad + g) : 0u;
+            nbr[q][k] = (live[q] && k < S.maxc) ? __ldg(S.nbrr + (size_t)k * S.npad + g) : 0u;
     }
 #pragma unroll
     for (int q = 0; q < MPT; ++q) front_plane<false>(pl[q], tab, S.planeTab, S, pk[q], (ent[q] >> 27) & 7u);
     unsigned long long hit[MPT];
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
-        uint32_t const e = tid + (uint32_t)q * B;
         hit[q] = 0ull;
 #pragma unroll
         for (int r = 0; r < 4; ++r)
-            if (e < nCur && pl[q].m[r]) hit[q] |= ldm<kNc>(tcur + pl[q].w[r]) & pl[q].m[r];
+            if (live[q] && pl[q].m[r]) hit[q] |= ldm<kNc>(tcur + pl[q].w[r]) & pl[q].m[r];
     }
     uint32_t nAcc = 0;
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
-        uint32_t const e = tid + (uint32_t)q * B;
+        if (!live[q] || hit[q] != 0ull) continue;
+        ++nAcc;
         uint32_t const g = ent[q] & kEntSlotMask;
-        bool const go = e < nCur && hit[q] == 0ull;
-        if (go) {
-            ++nAcc;
-            lcur[e] = ent[q] | kEntApplied;
-            uint32_t const dir = (ent[q] >> 27) & 7u;
-            uint32_t const a = dir >> 1;
-            int32_t const s = (dir & 1u) ? 1 : -1;
-            uint32_t const pk1 = step_pk(pk[q], dir, S.mask);
-            uint32_t w0, b0, w1, b1;
-            cell_of(pk[q], tab, S, w0, b0);
-            cell_of(pk1, tab, S, w1, b1);
-            if (w0 == w1) {
-                atomicXor(S.lat + w0, (1ull << b0) | (1ull << b1));
-            } else {
-                atomicXor(S.lat + w0, 1ull << b0);
-                atomicXor(S.lat + w1, 1ull << b1);
-            }
-            PK[g] = pk1;
-            atomicAdd((a == 0 ? S.x : (a == 1 ? S.y : S.z)) + g, s);
-            W const own = code[q];
-            CODE[g] = code_shift(own, a, -s);
-            uint32_t const n = uint32_t(own >> CodeWord<W>::kCountShift) & 7u;
+        lbase[li[q]] = ent[q] | kEntApplied;
+        uint32_t const dir = (ent[q] >> 27) & 7u;
+        uint32_t const a = dir >> 1;
+        int32_t const s = (dir & 1u) ? 1 : -1;
+        uint32_t const pk1 = step_pk(pk[q], dir, S.mask);
+        uint32_t w0, b0, w1, b1;
+        cell_of(pk[q], tab, S, w0, b0);
+        cell_of(pk1, tab, S, w1, b1);
+        if (w0 == w1) {
+            atomicXor(S.lat + w0, (1ull << b0) | (1ull << b1));
+        } else {
+            atomicXor(S.lat + w0, 1ull << b0);
+            atomicXor(S.lat + w1, 1ull << b1);
+        }
+        PK[g] = pk1;
+        atomicAdd((a == 0 ? S.x : (a == 1 ? S.y : S.z)) + g, s);
+        W const own = code[q];
+        CODE[g] = code_shift(own, a, -s);
+        uint32_t const n = uint32_t(own >> CodeWord<W>::kCountShift) & 7u;
 #pragma unroll
-            for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k) {
-                if (k < n) {
-                    uint32_t const nb = nbr[q][k];
-                    uint32_t const c = (0u - (uint32_t(own >> (9u * k + 3u * a)) & 7u)) & 7u;   // reverse field
-                    uint32_t const nc = uint32_t(int32_t(c) + s) & 7u;
-                    atomicXor(CODE + (nb & kSlotMask), W(c ^ nc) << (9u * (nb >> kSlotShift) + 3u * a));
-                }
+        for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k) {
+            if (k < n) {
+                uint32_t const nb = nbr[q][k];
+                uint32_t const c = (0u - (uint32_t(own >> (9u * k + 3u * a)) & 7u)) & 7u;   // reverse field
+                uint32_t const nc = uint32_t(int32_t(c) + s) & 7u;
+                atomicXor(CODE + (nb & kSlotMask), W(c ^ nc) << (9u * (nb >> kSlotShift) + 3u * a));
             }
         }
     }
-    if (nAcc) atomicAdd(tally, nAcc);   // threads past the list returned early: no warp-wide vote here
+    return nAcc;
+}
+
+// Walks the tentative movers the check listed for tiles tile0 .. tile0+nT-1 (at most
+// kPerformTiles), as one dense range: no thread waits on a monomer that did not move. pre is
+// nT+1 words of shared memory; every thread of the CTA calls this.
+template <typename W, int MPT, bool kNc = true>
+__device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* tab, StepEntry const& st,
+                                             uint32_t tile0, uint32_t nT, uint32_t* tally, uint32_t* pre)
+{
+    uint32_t const B = blockDim.x, tid = threadIdx.x;
+    unsigned long long const* const tcur = S.tmp + (size_t)st.parity * S.nwords;
+    uint32_t* const lbase = S.mlist + (size_t)st.parity * S.listStride + (size_t)tile0 * kBcTileSpan;
+    uint32_t const* const cnt = S.mcount + (size_t)st.parity * S.countStride + tile0;
+    __syncthreads();   // pre of an earlier call has been read
+    if (tid == 0) {
+        uint32_t acc = 0;
+        for (uint32_t j = 0; j < nT; ++j) {
+            pre[j] = acc;
+            acc += ldm<kNc>(cnt + j);
+        }
+        pre[nT] = acc;
+    }
+    __syncthreads();
+    uint32_t const total = pre[nT];
+    uint32_t nAcc = 0;
+    for (uint32_t e0 = 0; e0 < total; e0 += B * MPT)
+        nAcc += perform_chunk<W, MPT, kNc>(S, tab, tcur, lbase, pre, nT, total, e0 + tid);
+    if (nAcc) atomicAdd(tally, nAcc);
 }
 
 }  // namespace
@@ -366,14 +395,20 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_perform_bc(const __g
 {
     __shared__ SysDev Sm;
     __shared__ uint32_t tab[kMaxTab];
-    uint32_t sys = 0, start = blockIdx.x * (kGridBlock * MPT);
+    __shared__ uint32_t pre[kPerformTiles + 1];
+    // one system: kPerformTiles consecutive tiles per CTA; a tile list: one tile per CTA
+    uint32_t sys = 0, tile0 = blockIdx.x * kPerformTiles, nT = kPerformTiles;
     if (kMulti) {
         TileRef const tr = tiles[blockIdx.x];
         sys = tr.sys;
-        start = tr.start;
+        tile0 = tr.start / kBcTileSpan;
+        nT = 1;
     }
     StepEntry const st = steps[sys];
-    if (st.color == kNoColor || start >= st.cnt) return;
+    if (st.color == kNoColor) return;
+    uint32_t const activeTiles = (st.cnt + kBcTileSpan - 1) / kBcTileSpan;
+    if (tile0 >= activeTiles) return;
+    nT = min(nT, activeTiles - tile0);
     if (kMulti) {
         copy_desc(Sm, sysv + sys);
         __syncthreads();
@@ -384,7 +419,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_perform_bc(const __g
     for (uint32_t w = threadIdx.x; w < ntab; w += blockDim.x) tab[w] = S.brickTab[w];
     if (threadIdx.x == 0) tally = 0;
     __syncthreads();
-    perform_body<W, MPT>(S, tab, st, start, &tally);
+    perform_body<W, MPT>(S, tab, st, tile0, nT, &tally, pre);
     __syncthreads();
     if (threadIdx.x == 0) tally_flush(tally, S.stats, 2);
 }
@@ -460,7 +495,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
 {
     static_assert(kGridBlock * MPT == kBcTileSpan, "a tile is one list segment");
     __shared__ uint32_t tab[kMaxTab];
-    __shared__ uint32_t tallyT, tallyA, okSm, segCount;
+    __shared__ uint32_t tallyT, tallyA, okSm, segCount, pre[2];
     if (ld_acquire_gpu(&gs->fault) != 0u) return;   // an earlier launch failed: the state is not usable
     uint32_t const ntab = S.nb[0] + S.nb[1] + S.nb[2];
     for (uint32_t w = threadIdx.x; w < ntab; w += blockDim.x) tab[w] = S.brickTab[w];
@@ -494,7 +529,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
             for (uint32_t k = blockIdx.x; k < nTiles; k += gridDim.x) {
                 uint32_t const start = k * span;
                 if (start >= st.cnt) break;
-                perform_body<W, MPT, false>(S, tab, st, start, &tallyA);
+                perform_body<W, MPT, false>(S, tab, st, k, 1u, &tallyA, pre);
             }
         }
         if (t + 1 < nSteps && !grid_barrier(gs, gen, &okSm)) return;
@@ -653,14 +688,16 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
 namespace {
 
 // CTAs per SM the compiler must fit (register budget) for check / perform: shape 0 leaves the
-// registers free, 1 (the default: 40 / 48 registers, no spills, 1.15 / 1.38 waves on the 256^3
-// melt) asks 6 / 5, 2 asks 6 / 6. The environment variable BFM_GRID_SHAPE selects one for tuning.
+// registers free (64 / 80), 1 asks 6 / 5 (40 / 48), 2 asks 6 / 6, 3 (the default) asks 7 / 5: the
+// check at 32 registers with a 20-byte spill runs the 1024 tiles of the 256^3 melt in one wave
+// (7 x 148 CTAs), 4-5 % faster than shape 1. The environment variable BFM_GRID_SHAPE selects a
+// shape for tuning.
 int grid_shape()
 {
     static int const shape = [] {
         char const* e = std::getenv("BFM_GRID_SHAPE");
-        int const v = e ? std::atoi(e) : 1;
-        return (v >= 0 && v <= 2) ? v : 1;
+        int const v = e ? std::atoi(e) : 3;
+        return (v >= 0 && v <= 3) ? v : 3;
     }();
     return shape;
 }
@@ -672,7 +709,9 @@ void launch_grid_bc_k(bool check, SysDev const& hostDesc, SysDev const* dSys, Ti
     if (check)
         k_check_bc<W, kCheckMpt, kMulti, kMinCheck><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
     else
-        k_perform_bc<W, kCheckMpt, kMulti, kMinPerform><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
+        k_perform_bc<W, kCheckMpt, kMulti, kMinPerform>
+            <<<kMulti ? nTiles : (nTiles + kPerformTiles - 1) / kPerformTiles, kGridBlock, 0, s>>>(hostDesc, dSys,
+                                                                                                   dTiles, dSteps);
 }
 
 template <typename W, bool kMulti>
@@ -682,6 +721,7 @@ void launch_grid_bc_m(bool check, SysDev const& hostDesc, SysDev const* dSys, Ti
     switch (grid_shape()) {
     case 1: launch_grid_bc_k<W, kMulti, 6, 5>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
     case 2: launch_grid_bc_k<W, kMulti, 6, 6>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
+    case 3: launch_grid_bc_k<W, kMulti, 7, 5>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
     default: launch_grid_bc_k<W, kMulti, 1, 1>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
     }
 }
