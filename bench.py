@@ -81,30 +81,30 @@ def check_bytes_per_move(systems, p_chk, code_mode):
 
     Gather representation (code_mode 0): own xyz 12 B, per neighbour 4 B id + 12 B xyz, neighbour
     count 1 B, flag write 1 B, 9 occupancy bits, one temporary bit per tentative move.
-    Bond codes (code_mode 1: 4 B words, 2: 8 B words): packed coordinate 4 B + code word, flag
-    write 1 B, the previous colour group's flag 1 B + packed coordinate 4 B (the scrub; the groups
-    are of equal size up to one monomer), 9 occupancy bits, one temporary bit set per tentative
-    move and one cleared per previous tentative move."""
+    Bond codes (code_mode 1: 4 B words, 2: 8 B words): packed coordinate 4 B + code word, 9
+    occupancy bits; per tentative move a 4 B mover-list entry and one temporary bit set; per
+    tentative move of the previous sub-step (the scrub, same rate) its list entry 4 B, its packed
+    coordinate 4 B and one temporary bit cleared."""
     n = sum(s.n for s in systems)
     kbar = sum(int(s.nbr_count.sum()) for s in systems) / n
     if code_mode == 0:
         return 12 + 16 * kbar + 1 + 1 + 9 / 8 + p_chk / 8, kbar
     w = 4 if code_mode == 1 else 8
-    return 4 + w + 1 + 5 + 9 / 8 + 2 * p_chk / 8, kbar
+    return 4 + w + 9 / 8 + p_chk * (4 + 1 / 8) + p_chk * (8 + 1 / 8), kbar
 
 
 def perform_bytes_per_move(kbar, p_chk, p_acc, code_mode):
-    """Algorithmic bytes of one attempted move in the perform kernel (bond codes): flag 1 B and
-    packed coordinate 4 B; per tentative move the code word, kbar neighbour references (4 B) and
-    9 temporary-lattice bits; per accepted move 2 lattice bits read and written, packed coordinate
-    4 B, one coordinate read+write 8 B, flag 1 B, own code word and kbar neighbour code words read
-    and written. Gather representation (code_mode 0): flag 1 B, per tentative move xyz 12 B and
-    9 temporary bits, per accepted move 2 lattice bits read and written, one coordinate 8 B, flag
-    1 B."""
+    """Algorithmic bytes of one attempted move in the perform kernel (bond codes), which walks only
+    the mover lists: per tentative move its list entry 4 B, packed coordinate 4 B, code word, kbar
+    neighbour references (4 B) and 9 temporary-lattice bits; per accepted move 2 lattice bits read
+    and written, packed coordinate 4 B, one coordinate read+write 8 B, the list entry 4 B, own code
+    word and kbar neighbour code words read and written. Gather representation (code_mode 0):
+    flag 1 B, per tentative move xyz 12 B and 9 temporary bits, per accepted move 2 lattice bits
+    read and written, one coordinate 8 B, flag 1 B."""
     if code_mode == 0:
         return 1 + p_chk * (12 + 9 / 8) + p_acc * (0.5 + 8 + 1)
     w = 4 if code_mode == 1 else 8
-    return 5 + p_chk * (w + 4 * kbar + 9 / 8) + p_acc * (0.5 + 4 + 8 + 1 + w + 2 * w * kbar)
+    return p_chk * (8 + w + 4 * kbar + 9 / 8) + p_acc * (0.5 + 4 + 8 + 4 + w + 2 * w * kbar)
 
 
 def measured_peaks():
@@ -115,13 +115,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(kernel_key):
-    """dram bytes per launch recorded from an ncu capture in profiles/<kernel_key>.md, if present."""
+def profiled_traffic(kernel_key, tag="dram_bytes_per_launch:"):
+    """A figure recorded from an ncu capture in profiles/<kernel_key>.md (the line starting with
+    tag: DRAM bytes per launch by default), if present."""
     p = os.path.join(ROOT, "profiles", kernel_key + ".md")
     if not os.path.exists(p):
         return None
     for ln in open(p):
-        if ln.strip().startswith("dram_bytes_per_launch:"):
+        if ln.strip().startswith(tag):
             try:
                 return float(ln.split(":", 1)[1].split()[0])
             except ValueError:
@@ -396,9 +397,12 @@ def run_ours(args):
                                 "bytes_per_attempted_move": round(b_perf, 3),
                                 "achieved": round(achieved_perf, 1), "frac": round(achieved_perf / hbm_peak, 4)},
                     "timing": "CUDA events around each launch on the engine stream, one sub-step at a time",
-                    "note": ("the state (about 36 B per monomer) stays in the 126 MB L2 between launches, so "
+                    "note": ("the state (about 40 B per monomer) stays in the 126 MB L2 between launches, so "
                              "the HBM fraction is low by construction; the kernels are bound by instruction "
                              "issue and dependent-load latency")}
+        l2pct = profiled_traffic(key, "lts_throughput_pct:")
+        roofline["l2"] = {"frac": None if l2pct is None else round(l2pct / 100, 4),
+                          "source": f"ncu lts__throughput.avg.pct_of_peak_sustained_elapsed, profiles/{key}.md"}
 
     # e2e through the C-ABI with host buffers: per step one bfm_run (host draws uploaded from
     # pinned memory) and a read of the step's counters; positions copied back at the end
