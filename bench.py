@@ -473,6 +473,7 @@ def batched_vs_plain(n_systems=256, mcs=100, plain_mcs=20):
     members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
     b = P.Batch(members)
     b.run(3)
+    tuned = b.autotune(5)          # the trials are warm-up MCS of the run
     batched_ms = b.run_timed(mcs)
     launches0 = b.launch_count()
     b.run_timed(1)
@@ -489,6 +490,8 @@ def batched_vs_plain(n_systems=256, mcs=100, plain_mcs=20):
     return {"workload": "ensemble_256_systems", "systems": n_systems, "monomers": n, "mcs": mcs,
             "batched": n * mcs / (batched_ms / 1e3), "plain": n * mcs / (plain_ms / 1e3),
             "ratio": plain_ms / batched_ms, "batched_launches_per_mcs": launches_per_mcs,
+            "autotuned": {"shape": tuned["shape"], "resident": tuned["resident"],
+                          "trials": [[t["shape"], t["resident"], round(t["ms_per_mcs"], 4)] for t in tuned["trials"]]},
             "plain_path": f"BFM_MODE_LAUNCH, one system at a time, {plain_mcs} MCS each scaled to {mcs}",
             "unit": "attempted moves/s"}
 

@@ -189,6 +189,15 @@ int bfm_batch_synchronize(bfm_batch_handle b);
 int bfm_batch_set_resident(bfm_batch_handle b, int on);
 /* Member i advances mcs[i] MCS (0 = it idles); one launch sequence for all, like bfm_batch_run. */
 int bfm_batch_run_each(bfm_batch_handle b, const int32_t* mcs);
+/* Register budget of the grid-phase kernels, 0..3, or -1 for the default; results do not change. */
+int bfm_batch_set_shape(bfm_batch_handle b, int shape);
+/* Autotuner: runs every configuration (kernel shape x resident path on / off) for 1 + mcs_per_trial
+ * MCS, keeps the fastest and reports it (shape, resident, ms per MCS). The trials are ordinary MCS
+ * of the run (results do not depend on the configuration): every member advances by n_trials x
+ * (1 + mcs_per_trial) MCS. trials (may be NULL) receives up to capacity triples (shape, resident,
+ * ms per MCS). */
+int bfm_batch_autotune(bfm_batch_handle b, int32_t mcs_per_trial, int* shape, int* resident, float* ms_per_mcs,
+                       float* trials, uint32_t capacity, uint32_t* n_trials);
 const char* bfm_batch_last_error(bfm_batch_handle b);
 
 /* ------------------------------------------------------------------ server (no reference counterpart) */

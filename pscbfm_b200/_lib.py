@@ -100,6 +100,10 @@ _SIGS = {
     "bfm_batch_run": [H, C.c_int32],
     "bfm_batch_run_async": [H, C.c_int32],
     "bfm_batch_run_each": [H, _i32p],
+    "bfm_batch_set_shape": [H, C.c_int],
+    "bfm_batch_autotune": [H, C.c_int32, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float),
+                           np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"), C.c_uint32,
+                           C.POINTER(C.c_uint32)],
     "bfm_batch_run_timed": [H, C.c_int32, C.POINTER(C.c_float)],
     "bfm_batch_synchronize": [H],
     "bfm_batch_set_resident": [H, C.c_int],

@@ -164,11 +164,12 @@ cudaError_t Batch::launchGrid(StepEntry const* e)
     SysDev const unused{};   // multi-system launches read each CTA's descriptor from dSys_
     for (auto const& g : grid_) {
         uint32_t const n = (uint32_t)g.tiles.size();
-        cudaError_t err = g.codeMode == kCodeNone ? launch_check(dSys_, g.dTiles, n, kGridBlock, e, stream_)
-                                                  : launch_check_bc(unused, dSys_, g.dTiles, n, e, g.codeMode, stream_);
+        cudaError_t err = g.codeMode == kCodeNone
+                              ? launch_check(dSys_, g.dTiles, n, kGridBlock, e, stream_)
+                              : launch_check_bc(unused, dSys_, g.dTiles, n, e, g.codeMode, stream_, shape_);
         if (err != cudaSuccess) return err;
         err = g.codeMode == kCodeNone ? launch_perform(dSys_, g.dTiles, n, kGridBlock, e, stream_)
-                                      : launch_perform_bc(unused, dSys_, g.dTiles, n, e, g.codeMode, stream_);
+                                      : launch_perform_bc(unused, dSys_, g.dTiles, n, e, g.codeMode, stream_, shape_);
         if (err != cudaSuccess) return err;
     }
     return cudaSuccess;
@@ -284,6 +285,42 @@ void Batch::run(int32_t const* mcs)
         members_[m]->noteExternalRun(need[m], (uint64_t)mcs[m], !isResident_[m], members_[m]->lastColor());
         members_[m]->streamWait(done_);
     }
+}
+
+void Batch::setShape(int shape)
+{
+    if (shape >= kGridShapes) throw std::invalid_argument("[Batch::setShape] unknown kernel shape");
+    if (shape != shape_) built_ = false;   // the captured graph holds the old kernels
+    shape_ = shape;
+}
+
+std::vector<Batch::Trial> Batch::autotune(int32_t mcsPerTrial)
+{
+    // Every configuration gives the same trajectories, so the trials are ordinary MCS of the run:
+    // each configuration runs 1 MCS (graph capture, warm-up) and then mcsPerTrial timed MCS.
+    if (mcsPerTrial <= 0) throw std::invalid_argument("[Batch::autotune] trials need at least one MCS");
+    cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
+    if (!built_) rebuild();
+    bool anyEligible = false;
+    for (Updater* u : members_) anyEligible = anyEligible || u->residentEligible();
+    std::vector<Trial> trials;
+    for (int resident = 1; resident >= 0; --resident) {
+        if (!resident && !anyEligible) break;   // the same configuration as resident on
+        setResidentEnabled(resident != 0);
+        rebuild();
+        int const nShapes = grid_.empty() ? 1 : kGridShapes;   // the shape only matters to grid groups
+        for (int s = 0; s < nShapes; ++s) {
+            setShape(grid_.empty() ? -1 : s);
+            runTimed(1);
+            trials.push_back(Trial{shape_, resident != 0, runTimed(mcsPerTrial) / (float)mcsPerTrial});
+        }
+    }
+    Trial best = trials.front();
+    for (Trial const& t : trials)
+        if (t.msPerMcs < best.msPerMcs) best = t;
+    setResidentEnabled(best.resident);
+    setShape(best.shape);
+    return trials;
 }
 
 float Batch::runTimed(int32_t nMcs)

@@ -2,6 +2,7 @@
 
 #include "../../include/bfm.h"
 
+#include <algorithm>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -396,6 +397,29 @@ int bfm_batch_run(bfm_batch_handle b, int32_t n)
     BFM_CALL(b, {
         b->b.run(n);
         b->b.synchronize();
+    });
+}
+int bfm_batch_set_shape(bfm_batch_handle b, int shape) { BFM_CALL(b, b->b.setShape(shape)); }
+int bfm_batch_autotune(bfm_batch_handle b, int32_t mcsPerTrial, int* shape, int* resident, float* msPerMcs,
+                       float* trials, uint32_t capacity, uint32_t* nTrials)
+{
+    BFM_CALL(b, {
+        auto const t = b->b.autotune(mcsPerTrial);
+        b->b.synchronize();
+        if (shape) *shape = b->b.shape();
+        if (resident) *resident = b->b.residentEnabled() ? 1 : 0;
+        if (msPerMcs) {
+            float best = t.front().msPerMcs;
+            for (auto const& x : t) best = std::min(best, x.msPerMcs);
+            *msPerMcs = best;
+        }
+        if (trials)
+            for (uint32_t i = 0; i < (uint32_t)t.size() && i < capacity; ++i) {
+                trials[3 * i] = (float)t[i].shape;
+                trials[3 * i + 1] = t[i].resident ? 1.f : 0.f;
+                trials[3 * i + 2] = t[i].msPerMcs;
+            }
+        if (nTrials) *nTrials = (uint32_t)t.size();
     });
 }
 int bfm_batch_run_each(bfm_batch_handle b, const int32_t* mcs)

@@ -225,6 +225,19 @@ public:
     void run(int32_t const* mcs);   // enqueue mcs[i] MCS of member i (0: the member idles)
     // replaces the member list; streams, events and buffers are kept (buffers grow as needed)
     void setMembers(Updater* const* members, uint32_t n);
+    // register budget of the grid-phase kernels (launch_check_bc), -1: the default
+    void setShape(int shape);
+    int shape() const { return shape_; }
+    bool residentEnabled() const { return residentOn_; }
+    // Runs the members under each configuration (kernel shape x resident path on / off) for
+    // 1 + mcsPerTrial MCS, keeps the fastest per MCS and returns every trial. The MCS count
+    // as ordinary steps of the run: the results do not depend on the configuration.
+    struct Trial {
+        int shape;
+        bool resident;
+        float msPerMcs;
+    };
+    std::vector<Trial> autotune(int32_t mcsPerTrial);
     float runTimed(int32_t nMcs);   // run + CUDA-event time on the batch stream (ms)
     void synchronize();
     uint32_t size() const { return (uint32_t)members_.size(); }
@@ -262,6 +275,7 @@ private:
     std::vector<ResidentGroup> resident_;
     bool residentOn_ = true;
     bool built_ = false;
+    int shape_ = -1;
     cudaStream_t stream_ = nullptr, stream2_ = nullptr;
     cudaEvent_t join_ = nullptr, fork_ = nullptr, ready_ = nullptr;
     void* arena_ = nullptr;                    // descriptors, graph window, tiles, lists

@@ -41,11 +41,14 @@ cudaError_t launch_resident(SysDev const* dSys, uint32_t const* dList, uint32_t 
 constexpr int kCheckMpt = 2;                                   // monomers per thread per pass
 constexpr uint32_t kBcTileSpan = kGridBlock * kCheckMpt;
 // dTiles == nullptr: single system, descriptor passed by value (hostDesc); otherwise the tile
-// list selects the system per CTA from dSys and hostDesc is unused.
+// list selects the system per CTA from dSys and hostDesc is unused. shape picks the register
+// budget (CTAs per SM) of the two kernels, 0 .. kGridShapes-1; negative: the default. Every shape
+// gives the same results.
+constexpr int kGridShapes = 4;
 cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
-                            StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s);
+                            StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1);
 cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
-                              StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s);
+                              StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1);
 // Persistent sweep (bond codes, one system): nSteps sub-steps of check, grid barrier, perform in
 // one cooperative launch of at most the co-resident CTA count. gs must be zeroed before the launch;
 // after it, gs->fault != 0 means a barrier wait ran out and the system's state is not usable.

@@ -690,14 +690,14 @@ namespace {
 // CTAs per SM the compiler must fit (register budget) for check / perform: shape 0 leaves the
 // registers free (64 / 80), 1 asks 6 / 5 (40 / 48), 2 asks 6 / 6, 3 (the default) asks 7 / 5: the
 // check at 32 registers with a 20-byte spill runs the 1024 tiles of the 256^3 melt in one wave
-// (7 x 148 CTAs), 4-5 % faster than shape 1. The environment variable BFM_GRID_SHAPE selects a
-// shape for tuning.
-int grid_shape()
+// (7 x 148 CTAs), 4-5 % faster than shape 1. A launch names its shape (Batch::autotune picks one);
+// a negative shape means the default, which the environment variable BFM_GRID_SHAPE can change.
+int default_grid_shape()
 {
     static int const shape = [] {
         char const* e = std::getenv("BFM_GRID_SHAPE");
         int const v = e ? std::atoi(e) : 3;
-        return (v >= 0 && v <= 3) ? v : 3;
+        return (v >= 0 && v < kGridShapes) ? v : 3;
     }();
     return shape;
 }
@@ -716,9 +716,9 @@ void launch_grid_bc_k(bool check, SysDev const& hostDesc, SysDev const* dSys, Ti
 
 template <typename W, bool kMulti>
 void launch_grid_bc_m(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
-                      uint32_t nTiles, StepEntry const* dSteps, cudaStream_t s)
+                      uint32_t nTiles, StepEntry const* dSteps, int shape, cudaStream_t s)
 {
-    switch (grid_shape()) {
+    switch (shape < 0 ? default_grid_shape() : shape) {
     case 1: launch_grid_bc_k<W, kMulti, 6, 5>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
     case 2: launch_grid_bc_k<W, kMulti, 6, 6>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
     case 3: launch_grid_bc_k<W, kMulti, 7, 5>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
@@ -728,32 +728,33 @@ void launch_grid_bc_m(bool check, SysDev const& hostDesc, SysDev const* dSys, Ti
 
 template <typename W>
 cudaError_t launch_grid_bc(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
-                           uint32_t nTiles, StepEntry const* dSteps, cudaStream_t s)
+                           uint32_t nTiles, StepEntry const* dSteps, int shape, cudaStream_t s)
 {
-    if (dTiles) launch_grid_bc_m<W, true>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s);
-    else launch_grid_bc_m<W, false>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s);
+    if (shape >= kGridShapes) return cudaErrorInvalidValue;
+    if (dTiles) launch_grid_bc_m<W, true>(check, hostDesc, dSys, dTiles, nTiles, dSteps, shape, s);
+    else launch_grid_bc_m<W, false>(check, hostDesc, dSys, dTiles, nTiles, dSteps, shape, s);
     return cudaGetLastError();
 }
 
 }  // namespace
 
 cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
-                            StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s)
+                            StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape)
 {
     if (nTiles == 0) return cudaSuccess;
-    if (codeMode == kCode32) return launch_grid_bc<uint32_t>(true, hostDesc, dSys, dTiles, nTiles, dSteps, s);
+    if (codeMode == kCode32) return launch_grid_bc<uint32_t>(true, hostDesc, dSys, dTiles, nTiles, dSteps, shape, s);
     if (codeMode == kCode64)
-        return launch_grid_bc<unsigned long long>(true, hostDesc, dSys, dTiles, nTiles, dSteps, s);
+        return launch_grid_bc<unsigned long long>(true, hostDesc, dSys, dTiles, nTiles, dSteps, shape, s);
     return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
-                              StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s)
+                              StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape)
 {
     if (nTiles == 0) return cudaSuccess;
-    if (codeMode == kCode32) return launch_grid_bc<uint32_t>(false, hostDesc, dSys, dTiles, nTiles, dSteps, s);
+    if (codeMode == kCode32) return launch_grid_bc<uint32_t>(false, hostDesc, dSys, dTiles, nTiles, dSteps, shape, s);
     if (codeMode == kCode64)
-        return launch_grid_bc<unsigned long long>(false, hostDesc, dSys, dTiles, nTiles, dSteps, s);
+        return launch_grid_bc<unsigned long long>(false, hostDesc, dSys, dTiles, nTiles, dSteps, shape, s);
     return cudaErrorInvalidValue;
 }
 

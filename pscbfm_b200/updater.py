@@ -342,6 +342,23 @@ class Batch:
     def run_async(self, n_mcs: int):
         self._call("bfm_batch_run_async", n_mcs)
 
+    def set_shape(self, shape: int):
+        """Register budget of the grid-phase kernels (0..3, -1 = default); results do not change."""
+        self._call("bfm_batch_set_shape", shape)
+
+    def autotune(self, mcs_per_trial: int = 10) -> dict:
+        """Tries every configuration (kernel shape x resident path on / off) for 1 + mcs_per_trial
+        MCS each and keeps the fastest. The trials advance every member (the results do not depend
+        on the configuration)."""
+        trials = np.zeros(3 * 16, dtype=np.float32)
+        shape, resident, best, n = C.c_int(), C.c_int(), C.c_float(), C.c_uint32()
+        self._call("bfm_batch_autotune", mcs_per_trial, C.byref(shape), C.byref(resident), C.byref(best), trials,
+                   16, C.byref(n))
+        rows = trials[:3 * min(n.value, 16)].reshape(-1, 3)
+        return {"shape": shape.value, "resident": bool(resident.value), "ms_per_mcs": best.value,
+                "mcs_spent": n.value * (1 + mcs_per_trial),
+                "trials": [{"shape": int(r[0]), "resident": bool(r[1]), "ms_per_mcs": float(r[2])} for r in rows]}
+
     def run_each(self, mcs):
         """Member i advances mcs[i] MCS (0: it idles)."""
         a = np.ascontiguousarray(mcs, dtype=np.int32)

@@ -200,6 +200,26 @@ def test_batch_equals_each_system_alone(resident):
         m.close()
 
 
+def test_batch_autotune_keeps_trajectories():
+    """The autotuner's trials are ordinary MCS under different kernel shapes and paths: every
+    member ends where the oracle puts it after the same number of MCS."""
+    systems = S.ensemble(n_systems=10, base_seed=700) + [S.crosslinked_network(), S.rings_and_free()]
+    members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
+    b = P.Batch(members)
+    rep = b.autotune(3)
+    assert len(rep["trials"]) == 8 and rep["mcs_spent"] == 8 * 4
+    assert {(t["shape"], t["resident"]) for t in rep["trials"]} == {(s, r) for s in range(4) for r in (True, False)}
+    assert rep["ms_per_mcs"] == min(t["ms_per_mcs"] for t in rep["trials"])
+    b.run(17)
+    for s, m in zip(systems, members):
+        ref, _ = O.run(s, rep["mcs_spent"] + 17)
+        assert np.array_equal(m.get_coords(), ref), s.name
+        m.validate()
+    b.close()
+    for m in members:
+        m.close()
+
+
 @pytest.mark.parametrize("resident", [True, False])
 def test_batch_uneven_mcs_per_member(resident):
     """run_each: members advance different MCS counts (some idle) in one launch sequence, as the
