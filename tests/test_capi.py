@@ -70,6 +70,21 @@ def test_colour_errors():
     assert L.bfm_color_graph(0, cnt, ids, 1, out, C.byref(nc)) == _lib.BFM_ERR_INVALID_ARGUMENT
 
 
+def test_lemonade_adapter_compiles(tmp_path):
+    """include/bfm_lemonade.hpp instantiated with an ingredients type that has the LeMonADE calls the
+    reference adapter makes (src/pscbfm/GPUScBFM_AB_Type.h:78-176) compiles and links (the updater
+    base class and VectorInt3 come from minimal stand-ins in tests/lemonade_stub)."""
+    import os
+    src = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lemonade_stub", "caller.cpp")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = tmp_path / "lemonade_caller"
+    r = subprocess.run(["g++", "-std=c++14", "-I", os.path.join(root, "include"),
+                        "-I", os.path.join(root, "tests", "lemonade_stub"), src, "-o", str(out),
+                        "-L", os.path.join(root, "pscbfm_b200"), "-lbfm",
+                        "-Wl,-rpath," + os.path.join(root, "pscbfm_b200")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 def test_cpp_wrapper_compiles_for_reference_style_callers(tmp_path):
     """A caller written like GPUScBFM_AB_Type::initialize/execute compiles and links against
     include/bfm_updater.hpp + libbfm.so."""

@@ -119,3 +119,29 @@ def test_reference_getters_and_colours():
     assert n == 3 and sizes.sum() == s.n
     assert u.execute() is True
     assert u.device_bytes() > 0
+
+
+def test_lemonade_adapter_runs_like_the_oracle(tmp_path):
+    """The LeMonADE-style program of tests/lemonade_stub/caller.cpp (two bonded monomers in a 32^3
+    box, the 108-vector set, 100 MCS of the counter stream with seed 7) ends where the oracle does,
+    and the adapter advances the molecules' age."""
+    import os
+    import subprocess
+    import numpy as np
+    from oracle import oracle as O
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    exe = tmp_path / "lemonade_caller"
+    r = subprocess.run(["g++", "-std=c++14", "-I", os.path.join(root, "include"),
+                        "-I", os.path.join(here, "lemonade_stub"), os.path.join(here, "lemonade_stub", "caller.cpp"),
+                        "-o", str(exe), "-L", os.path.join(root, "pscbfm_b200"), "-lbfm",
+                        "-Wl,-rpath," + os.path.join(root, "pscbfm_b200")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert run.returncode == 0, run.stdout + run.stderr
+    lines = run.stdout.split("\n")
+    got = np.array([[int(v) for v in ln.split()] for ln in lines[:2]])
+    assert lines[2] == "age 100"
+    s = S.from_bonds((32, 32, 32), np.array([[0, 0, 0], [2, 0, 0]]), [(0, 1)], seed=7)
+    ref, _ = O.run(s, 100)
+    assert np.array_equal(got, ref)
