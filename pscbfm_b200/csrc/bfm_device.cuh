@@ -63,6 +63,7 @@ struct SysDev {
     unsigned long long const* planeTab;   // [3][4][4][4][4] front-plane masks (see plane_table_fill)
     uint8_t const* moveOk;           // [512] bit d: a bond with this index stays allowed after move d
     uint32_t* mlist;                 // [2][listStride] tentative movers per tile segment, per parity
+    uint32_t* mword;                 // [2][listStride] the temporary-lattice word each listed mover marked
     uint32_t* mcount;                // [2][countStride] entries of each segment
     uint32_t listStride, countStride;
     uint32_t codeMode;               // kCodeNone, kCode32, kCode64

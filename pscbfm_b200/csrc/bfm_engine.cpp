@@ -333,7 +333,8 @@ void Updater::initialize()
     size_t const oPlane = take(8ull * 768), oMoveOk = take(512);
     // mover lists of the bond-code grid kernels: one segment of kBcTileSpan entries per tile
     uint32_t const segs = codeMode_ == kCodeNone ? 0u : std::max((maxGroup_ + kBcTileSpan - 1) / kBcTileSpan, 1u);
-    size_t const oMlist = take(4ull * 2 * segs * kBcTileSpan), oMcount = take(4ull * 2 * segs);
+    size_t const oMlist = take(4ull * 2 * segs * kBcTileSpan), oMword = take(4ull * 2 * segs * kBcTileSpan);
+    size_t const oMcount = take(4ull * 2 * segs);
     Device d;
     d.bytes = off;
     // stream-ordered: freeing it later does not wait for the whole device
@@ -376,6 +377,7 @@ void Updater::initialize()
     h.planeTab = reinterpret_cast<unsigned long long*>(base + oPlane);
     h.moveOk = reinterpret_cast<uint8_t*>(base + oMoveOk);
     h.mlist = reinterpret_cast<uint32_t*>(base + oMlist);
+    h.mword = reinterpret_cast<uint32_t*>(base + oMword);
     h.mcount = reinterpret_cast<uint32_t*>(base + oMcount);
     h.listStride = segs * kBcTileSpan;
     h.countStride = segs;
@@ -713,8 +715,8 @@ void Updater::scrubPending(cudaStream_t s)
                            grpSize_[lastColor_]};
     cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry), cudaMemcpyHostToDevice, s), "steps H2D");
     cuda_check(cudaEventRecord(stepsFree_, s), "event");
-    // gather kernels scrub in the perform, bond-code kernels in the check
-    cuda_check(codeMode_ == kCodeNone ? launchPerform(dev_.dSteps, s) : launchCheck(dev_.dSteps, s), "scrub");
+    // both representations scrub the previous sub-step's marks in the perform
+    cuda_check(launchPerform(dev_.dSteps, s), "scrub");
     ++launches_;
     lastColor_ = kNoColor;
 }

@@ -36,8 +36,8 @@ cudaError_t launch_resident(SysDev const* dSys, uint32_t const* dList, uint32_t 
                             StepEntry const* dSteps, uint32_t nSys, uint32_t nSteps, size_t smem, cudaStream_t s);
 
 // Bond-code kernels (SysDev::codeMode kCode32 / kCode64). Tiles span kBcTileSpan in-colour
-// indices. In this representation the check zeroes the previous sub-step's marks, so a
-// stand-alone scrub is a check launch whose entry has color == kNoColor.
+// indices. As in the gather representation, the perform zeroes the previous sub-step's marks, so a
+// stand-alone scrub is a perform launch whose entry has color == kNoColor.
 constexpr int kCheckMpt = 2;                                   // monomers per thread per pass
 constexpr uint32_t kBcTileSpan = kGridBlock * kCheckMpt;
 // dTiles == nullptr: single system, descriptor passed by value (hostDesc); otherwise the tile

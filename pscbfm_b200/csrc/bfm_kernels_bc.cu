@@ -7,11 +7,11 @@
 // own fields change by -d and the reverse field of every neighbour by +d; the reverse field's old
 // value is the negation (mod 8) of the monomer's own field, so the update needs no extra load.
 //
-// Grid phase (k_check_bc, k_perform_bc): the check lists its tentative movers per tile (mover
-// lists, double-buffered by sub-step parity); the perform walks only those lists, and the check of
-// sub-step t also zeroes the temporary-lattice words marked at t-1 (found from list[parity^1] and
-// pk, both read-only during the check). Every independent load of a pass is issued before any
-// dependent one; a single-system launch takes the descriptor as a grid-constant parameter.
+// Grid phase (k_check_bc, k_perform_bc): the check lists its tentative movers per tile, with the
+// temporary-lattice word each one marked (mover lists, double-buffered by sub-step parity); the
+// perform walks only those lists, and the perform of sub-step t also zeroes the words listed at
+// t-1. Every independent load of a pass is issued before any dependent one; a single-system
+// launch takes the descriptor as a grid-constant parameter.
 //
 // Persistent (k_sweep_bc): the same bodies for a whole run of sub-steps in one cooperative launch,
 // with time-bounded grid barriers between the phases.
@@ -139,12 +139,12 @@ __device__ __forceinline__ T ldm(T const* p)
 }
 
 // Mover lists: the check of sub-step t appends each tentative mover of tile k (kBcTileSpan
-// in-colour indices) to segment k of list[parity] and stores the segment's length in
-// count[parity][k]; the perform walks only those entries and marks the applied ones; the check of
-// sub-step t+1 walks them again to zero the temporary-lattice words they marked. Entry: slot g
-// (bits 0-26), direction (27-29), applied (31).
+// in-colour indices) to segment k of list[parity] (entry: slot g in bits 0-26, direction in
+// 27-29), the temporary-lattice word it marked to the same place of word[parity], and stores the
+// segment's length in count[parity][k]. The perform of sub-step t walks only the listed movers,
+// and zeroes the words listed at t-1 (nobody reads tmp[parity^1] during sub-step t, and the check
+// of t+1, which marks it again, comes after).
 constexpr uint32_t kEntSlotMask = (1u << 27) - 1u;
-constexpr uint32_t kEntApplied = 1u << 31;
 // tiles whose movers one perform CTA of a single-system launch walks (about 17 % of a tile's
 // monomers are tentative, so one tile leaves most of a CTA idle)
 constexpr uint32_t kPerformTiles = 4;
@@ -159,40 +159,21 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab,
     uint32_t const* const PK = S.pk;
     W const* const CODE = static_cast<W const*>(S.code);
     uint32_t const tile = start / kBcTileSpan;
-    unsigned long long* const tprev = S.tmp + (size_t)(st.parity ^ 1u) * S.nwords;
     unsigned long long* const tcur = S.tmp + (size_t)st.parity * S.nwords;
-    uint32_t const* const lprev = S.mlist + (size_t)(st.parity ^ 1u) * S.listStride + (size_t)tile * kBcTileSpan;
-    uint32_t* const lcur = S.mlist + (size_t)st.parity * S.listStride + (size_t)tile * kBcTileSpan;
-    bool const active = st.color != kNoColor;
+    size_t const seg = (size_t)st.parity * S.listStride + (size_t)tile * kBcTileSpan;
+    uint32_t* const lcur = S.mlist + seg;
+    uint32_t* const wcur = S.mword + seg;
 
-    // stage 1: every independent load of the pass (the previous sub-step's movers of this tile
-    // come from its list; pcnt is 0 when there is nothing to scrub)
-    uint32_t const nPrev = start < st.pcnt ? ldm<kNc>(S.mcount + (size_t)(st.parity ^ 1u) * S.countStride + tile) : 0u;
-    uint32_t pk[MPT], ent[MPT];
+    // stage 1: every independent load of the pass
+    uint32_t pk[MPT];
     W code[MPT];
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
         uint32_t const i = start + tid + (uint32_t)q * B;
-        uint32_t const e = tid + (uint32_t)q * B;
-        bool const a = active && i < st.cnt;
+        bool const a = i < st.cnt;
         pk[q] = a ? ldm<kNc>(PK + st.off + i) : 0u;
         code[q] = a ? ldm<kNc>(CODE + st.off + i) : W(0);
-        ent[q] = e < nPrev ? ldm<kNc>(lprev + e) : 0u;
     }
-    // scrub of the previous sub-step: every set bit of tmp[parity^1] belongs to one of its
-    // tentative movers, so zeroing a whole marked word only clears bits that are due
-#pragma unroll
-    for (int q = 0; q < MPT; ++q) {
-        uint32_t const e = tid + (uint32_t)q * B;
-        if (e < nPrev) {
-            uint32_t const pkb = ldm<kNc>(PK + (ent[q] & kEntSlotMask));
-            uint32_t const target = (ent[q] & kEntApplied) ? pkb : step_pk(pkb, (ent[q] >> 27) & 7u, S.mask);
-            uint32_t w, b;
-            cell_of(target, tab, S, w, b);
-            tprev[w] = 0ull;
-        }
-    }
-    if (!active) return;
     // stage 2: direction, bonds, front-plane words
     uint32_t dir[MPT];
     bool ok[MPT];
@@ -229,7 +210,9 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab,
             uint32_t w, b;
             cell_of(step_pk(pk[q], dir[q], S.mask), tab, S, w, b);
             atomicOr(tcur + w, 1ull << b);
-            lcur[base + __popc(bal & ((1u << lane) - 1u))] = (st.off + i) | (dir[q] << 27);
+            uint32_t const slot = base + __popc(bal & ((1u << lane) - 1u));
+            lcur[slot] = (st.off + i) | (dir[q] << 27);
+            wcur[slot] = w;
         }
     }
 }
@@ -286,7 +269,6 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
         if (!live[q] || hit[q] != 0ull) continue;
         ++nAcc;
         uint32_t const g = ent[q] & kEntSlotMask;
-        lbase[li[q]] = ent[q] | kEntApplied;
         uint32_t const dir = (ent[q] >> 27) & 7u;
         uint32_t const a = dir >> 1;
         int32_t const s = (dir & 1u) ? 1 : -1;
@@ -318,31 +300,55 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
     return nAcc;
 }
 
-// Walks the tentative movers the check listed for tiles tile0 .. tile0+nT-1 (at most
-// kPerformTiles), as one dense range: no thread waits on a monomer that did not move. pre is
-// nT+1 words of shared memory; every thread of the CTA calls this.
+// For tiles tile0 .. tile0+nT-1 (at most kPerformTiles): zeroes the temporary-lattice words the
+// previous sub-step's movers marked, then walks this sub-step's tentative movers as one dense range
+// (no thread waits on a monomer that did not move). pre is 2 (nT+1) words of shared memory: the
+// starting offsets of the current and of the previous lists. A tile's list counts only if the
+// tile lies inside that sub-step's colour group (older lengths may remain in count[]). Every thread
+// of the CTA calls this; st.color == kNoColor only scrubs.
 template <typename W, int MPT, bool kNc = true>
 __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* tab, StepEntry const& st,
                                              uint32_t tile0, uint32_t nT, uint32_t* tally, uint32_t* pre)
 {
     uint32_t const B = blockDim.x, tid = threadIdx.x;
     unsigned long long const* const tcur = S.tmp + (size_t)st.parity * S.nwords;
+    unsigned long long* const tprev = S.tmp + (size_t)(st.parity ^ 1u) * S.nwords;
     uint32_t* const lbase = S.mlist + (size_t)st.parity * S.listStride + (size_t)tile0 * kBcTileSpan;
+    uint32_t const* const wprev = S.mword + (size_t)(st.parity ^ 1u) * S.listStride + (size_t)tile0 * kBcTileSpan;
     uint32_t const* const cnt = S.mcount + (size_t)st.parity * S.countStride + tile0;
+    uint32_t const* const cntPrev = S.mcount + (size_t)(st.parity ^ 1u) * S.countStride + tile0;
+    uint32_t* const preP = pre + nT + 1;
+    bool const active = st.color != kNoColor;
     __syncthreads();   // pre of an earlier call has been read
     if (tid == 0) {
-        uint32_t acc = 0;
+        uint32_t acc = 0, accP = 0;
         for (uint32_t j = 0; j < nT; ++j) {
+            uint32_t const start = (tile0 + j) * kBcTileSpan;
             pre[j] = acc;
-            acc += ldm<kNc>(cnt + j);
+            preP[j] = accP;
+            acc += (active && start < st.cnt) ? ldm<kNc>(cnt + j) : 0u;
+            accP += start < st.pcnt ? ldm<kNc>(cntPrev + j) : 0u;
         }
         pre[nT] = acc;
+        preP[nT] = accP;
     }
     __syncthreads();
+    // scrub of the previous sub-step: every set bit of tmp[parity^1] belongs to one of its
+    // tentative movers, so zeroing a whole marked word only clears bits that are due. The first
+    // words are loaded before the movers' chain starts and zeroed after it, so the two overlap.
+    uint32_t const totalP = preP[nT];
+    auto scrubWord = [&](uint32_t e) {
+        uint32_t j = 0;
+        while (j + 1 < nT && e >= preP[j + 1]) ++j;
+        return ldm<kNc>(wprev + j * kBcTileSpan + (e - preP[j]));
+    };
+    uint32_t const w0 = tid < totalP ? scrubWord(tid) : 0u;
     uint32_t const total = pre[nT];
     uint32_t nAcc = 0;
     for (uint32_t e0 = 0; e0 < total; e0 += B * MPT)
         nAcc += perform_chunk<W, MPT, kNc>(S, tab, tcur, lbase, pre, nT, total, e0 + tid);
+    if (tid < totalP) tprev[w0] = 0ull;
+    for (uint32_t e = tid + B; e < totalP; e += B) tprev[scrubWord(e)] = 0ull;
     if (nAcc) atomicAdd(tally, nAcc);
 }
 
@@ -365,8 +371,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_check_bc(const __gri
         start = tr.start;
     }
     StepEntry const st = steps[sys];
-    if (st.color == kNoColor && st.prevColor == kNoColor) return;
-    if (start >= st.cnt && start >= st.pcnt) return;
+    if (st.color == kNoColor || start >= st.cnt) return;
     if (kMulti) {
         copy_desc(Sm, sysv + sys);
         __syncthreads();
@@ -391,13 +396,14 @@ template <typename W, int MPT, bool kMulti, int kMinBlocks = 1>
 __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_perform_bc(const __grid_constant__ SysDev S1,
                                                            SysDev const* __restrict__ sysv,
                                                            TileRef const* __restrict__ tiles,
-                                                           StepEntry const* __restrict__ steps)
+                                                           StepEntry const* __restrict__ steps,
+                                                           uint32_t tilesPerCta)
 {
     __shared__ SysDev Sm;
     __shared__ uint32_t tab[kMaxTab];
-    __shared__ uint32_t pre[kPerformTiles + 1];
-    // one system: kPerformTiles consecutive tiles per CTA; a tile list: one tile per CTA
-    uint32_t sys = 0, tile0 = blockIdx.x * kPerformTiles, nT = kPerformTiles;
+    __shared__ uint32_t pre[2 * (kPerformTiles + 1)];
+    // one system: tilesPerCta (<= kPerformTiles) consecutive tiles per CTA; a tile list: one tile
+    uint32_t sys = 0, tile0 = blockIdx.x * tilesPerCta, nT = tilesPerCta;
     if (kMulti) {
         TileRef const tr = tiles[blockIdx.x];
         sys = tr.sys;
@@ -405,8 +411,9 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_perform_bc(const __g
         nT = 1;
     }
     StepEntry const st = steps[sys];
-    if (st.color == kNoColor) return;
-    uint32_t const activeTiles = (st.cnt + kBcTileSpan - 1) / kBcTileSpan;
+    // tiles holding this sub-step's movers or the previous sub-step's marks
+    uint32_t const reach = max(st.color != kNoColor ? st.cnt : 0u, st.pcnt);
+    uint32_t const activeTiles = (reach + kBcTileSpan - 1) / kBcTileSpan;
     if (tile0 >= activeTiles) return;
     nT = min(nT, activeTiles - tile0);
     if (kMulti) {
@@ -495,7 +502,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
 {
     static_assert(kGridBlock * MPT == kBcTileSpan, "a tile is one list segment");
     __shared__ uint32_t tab[kMaxTab];
-    __shared__ uint32_t tallyT, tallyA, okSm, segCount, pre[2];
+    __shared__ uint32_t tallyT, tallyA, okSm, segCount, pre[4];
     if (ld_acquire_gpu(&gs->fault) != 0u) return;   // an earlier launch failed: the state is not usable
     uint32_t const ntab = S.nb[0] + S.nb[1] + S.nb[2];
     for (uint32_t w = threadIdx.x; w < ntab; w += blockDim.x) tab[w] = S.brickTab[w];
@@ -511,26 +518,25 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
     for (uint32_t t = 0; t < nSteps; ++t) {
         StepEntry const st = next;
         if (t + 1 < nSteps) next = steps[t + 1];
+        bool const active = st.color != kNoColor;
         for (uint32_t k = blockIdx.x; k < nTiles; k += gridDim.x) {
             uint32_t const start = k * span;
-            if (start >= st.cnt && start >= st.pcnt) break;
+            if (!active || start >= st.cnt) break;
             if (threadIdx.x == 0) segCount = 0u;
             __syncthreads();
             check_body<W, MPT, false>(S, tab, st, start, &segCount);
             __syncthreads();
-            if (threadIdx.x == 0 && st.color != kNoColor) {
+            if (threadIdx.x == 0) {
                 S.mcount[(size_t)st.parity * S.countStride + k] = segCount;
                 tallyT += segCount;
             }
         }
-        if (st.color != kNoColor) att += st.cnt;
+        if (active) att += st.cnt;
         if (!grid_barrier(gs, gen, &okSm)) return;
-        if (st.color != kNoColor) {
-            for (uint32_t k = blockIdx.x; k < nTiles; k += gridDim.x) {
-                uint32_t const start = k * span;
-                if (start >= st.cnt) break;
-                perform_body<W, MPT, false>(S, tab, st, k, 1u, &tallyA, pre);
-            }
+        uint32_t const reach = max(active ? st.cnt : 0u, st.pcnt);   // movers now, marks of t-1
+        for (uint32_t k = blockIdx.x; k < nTiles; k += gridDim.x) {
+            if (k * span >= reach) break;
+            perform_body<W, MPT, false>(S, tab, st, k, 1u, &tallyA, pre);
         }
         if (t + 1 < nSteps && !grid_barrier(gs, gen, &okSm)) return;
     }
@@ -702,16 +708,30 @@ int default_grid_shape()
     return shape;
 }
 
+// SMs of the current device (cached per device)
+int sm_count()
+{
+    static thread_local int count[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    int& c = count[dev & 63];
+    if (!c && cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) c = 148;
+    return c;
+}
+
 template <typename W, bool kMulti, int kMinCheck, int kMinPerform>
 void launch_grid_bc_k(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
                       uint32_t nTiles, StepEntry const* dSteps, cudaStream_t s)
 {
-    if (check)
+    if (check) {
         k_check_bc<W, kCheckMpt, kMulti, kMinCheck><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
-    else
-        k_perform_bc<W, kCheckMpt, kMulti, kMinPerform>
-            <<<kMulti ? nTiles : (nTiles + kPerformTiles - 1) / kPerformTiles, kGridBlock, 0, s>>>(hostDesc, dSys,
-                                                                                                   dTiles, dSteps);
+        return;
+    }
+    // one system: several tiles per perform CTA only while that still leaves every SM a CTA, since
+    // a small system's perform is bound by the length of its dependency chain, not by its warps
+    uint32_t const g = (!kMulti && nTiles >= kPerformTiles * (uint32_t)sm_count()) ? kPerformTiles : 1u;
+    k_perform_bc<W, kCheckMpt, kMulti, kMinPerform>
+        <<<kMulti ? nTiles : (nTiles + g - 1) / g, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps, g);
 }
 
 template <typename W, bool kMulti>
