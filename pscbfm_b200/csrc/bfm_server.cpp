@@ -39,8 +39,10 @@ using Clock = std::chrono::steady_clock;
 
 // longest stretch of MCS a lane advances between two admission points
 constexpr int32_t kMaxChunkMcs = 256;
-// lane of the systems on the grid-phase kernels; resident lanes are 0..4 (log2 monomers per thread)
+// lanes of the systems on the grid-phase kernels (kGridLane .. kGridLane + kGridLanes - 1);
+// resident lanes are 0..4 (log2 monomers per thread)
 constexpr int kGridLane = 100;
+constexpr int kGridLanes = 4;
 
 struct Server::Job {
     uint64_t id = 0;
@@ -241,10 +243,10 @@ std::shared_ptr<Server::Job> Server::find(uint64_t id)
 
 namespace {
 
-// the lane a freshly initialised system runs in
-int lane_of(Updater const& u)
+// the resident lane of a freshly initialised system that fits one CTA, or -1
+int resident_lane_of(Updater const& u)
 {
-    if (!u.residentEligible()) return kGridLane;
+    if (!u.residentEligible()) return -1;
     int c = 0;
     while ((kResidentBlock << c) < u.maxGroup()) ++c;
     return c;
@@ -289,6 +291,30 @@ void Server::workerMain()
             return stop_;
         };
 
+        // Systems that fit one CTA go to the resident lane of their size class. The others go to
+        // the grid lane with the least work left (monomers x remaining MCS): each grid lane is
+        // bound by the latency of its launches, so spreading long jobs over several lanes that run
+        // concurrently keeps each near its own speed.
+        auto lane_for = [&](Job const& j) {
+            int const r = resident_lane_of(*j.u);
+            if (r >= 0) return r;
+            int best = kGridLane;
+            double bestLoad = -1.0;
+            for (int k = 0; k < kGridLanes; ++k) {
+                double load = 0.0;
+                auto it = lanes.find(kGridLane + k);
+                if (it != lanes.end()) {
+                    for (auto const& q : it->second.jobs) load += (double)q->u->nMonomers() * (q->nMcs - q->done);
+                    for (auto const& q : it->second.incoming) load += (double)q->u->nMonomers() * (q->nMcs - q->done);
+                }
+                if (bestLoad < 0.0 || load < bestLoad) {
+                    bestLoad = load;
+                    best = kGridLane + k;
+                }
+            }
+            return best;
+        };
+
         // take pending jobs in arrival order while they fit; set them up outside the lock
         auto admit = [&]() {
             bool any = false;
@@ -307,7 +333,7 @@ void Server::workerMain()
                 }
                 try {
                     j->u->initialize();
-                    lanes[lane_of(*j->u)].incoming.push_back(j);
+                    lanes[lane_for(*j)].incoming.push_back(j);
                     any = true;
                 } catch (std::exception const& e) {
                     std::lock_guard<std::mutex> lk(mu_);
