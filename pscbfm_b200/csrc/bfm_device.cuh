@@ -4,9 +4,9 @@
 //   x, y, z      int32 structure-of-arrays, unfolded corner positions, npad entries
 //   nbr          uint32 [maxc][npad] neighbour slots (sorted ids), slot k of monomer g at k*npad+g
 //   nnb          uint8  [npad] neighbour count
-//   flags        uint8  [npad] tentative-move flag of the last check: dir<<2 | 1
+//   flags        uint8  [npad] tentative-move flag of the last check: dir<<2 | 1 (gather kernels)
 //   tmark        uint32 [2][npad] temporary-lattice bit set by the last check of each parity
-//                (word<<6 | bit, or kNoMark), used to scrub that bit one sub-step later
+//                (word<<6 | bit, or kNoMark), used to scrub that bit one sub-step later (gather)
 //   lat          uint64 occupancy words, one bit per lattice cell (the monomer's corner cell)
 //   tmp          uint64 [2][nwords] ping-pong temporary lattices of tentative targets
 // A 64-bit word holds one 4x4x4 brick of cells, bit (x&3) + 4 (y&3) + 16 (z&3), so the three
@@ -16,7 +16,8 @@
 // tables (brickTab). The reference keeps one Z-curve index per cell (src/pscbfm/CRITICAL.cu:13-34);
 // only the occupancy of each cell matters to the sweep, so the bit order inside a word is free.
 // Bond-code representation (codeMode != kCodeNone) adds, per monomer, its packed masked
-// coordinates (pk) and a word of bond-table indices (code), see CodeWord below.
+// coordinates (pk) and a word of bond-table indices (code), see CodeWord below, and per parity
+// the mover lists of the grid kernels (mlist, mword, mcount) in place of flags and tmark.
 #pragma once
 
 #include <cstdint>
@@ -49,7 +50,7 @@ struct SysDev {
     int32_t* z;
     uint32_t const* nbr;
     uint8_t const* nnb;
-    uint8_t* flags;                  // [2][npad]; the gather kernels use the first npad
+    uint8_t* flags;                  // [2][npad]; the gather kernels use the first npad (unused by bond codes)
     uint32_t* tmark;                 // [2][npad] (gather kernels)
     unsigned long long* lat;
     unsigned long long* tmp;         // [2][nwords]

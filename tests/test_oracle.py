@@ -259,3 +259,33 @@ def test_oracle_observables_basics():
     assert raw[5 * m:5 * m + 512].sum() == s.nbr_count.sum()
     # straight chains of 32 with bond (2,0,0): Ree^2 = 62^2
     assert (raw[4 * m:5 * m] == 62 ** 2).all()
+
+
+def _chain_statistics(s, run, n_blocks=40, block=100, skip=10):
+    """Block means of <Ree^2>, <Rg^2> and <b^2> over the chains of s (consecutive ids) after the
+    first `skip` blocks."""
+    import dataclasses
+    mol = O.molecules(s)
+    m = int(mol.max()) + 1
+    cur, ree, rg, b2 = s, [], [], []
+    for b in range(n_blocks):
+        xyz = run(cur, block, b)
+        cur = dataclasses.replace(cur, xyz=xyz.astype(np.int32))
+        c = xyz.astype(np.float64).reshape(m, s.n // m, 3)
+        ree.append(((c[:, -1] - c[:, 0]) ** 2).sum(1).mean())
+        rg.append(((c - c.mean(1, keepdims=True)) ** 2).sum(2).mean())
+        b2.append((np.diff(c, axis=1) ** 2).sum(2).mean())
+    return [float(np.mean(v[skip:])) for v in (ree, rg, b2)]
+
+
+def test_parallel_sweep_samples_like_the_serial_updater():
+    """The colour-by-colour parallel sweep and the random-sequential serial updater (the CPU
+    baseline) are different Markov chains with the same equilibrium: their chain statistics agree
+    within statistical error (not bit for bit)."""
+    s = S.serpentine_chains(32, 16, 0.3, seed=5)
+    par = _chain_statistics(s, lambda cur, k, b: O.run(cur, k, seed=1000 + b)[0])
+    seq = _chain_statistics(s, lambda cur, k, b: O.seq_run(cur, k, seed=2000 + b)[0])
+    for name, p, q, tol in zip(("Ree2", "Rg2", "b2"), par, seq, (0.08, 0.08, 0.01)):
+        assert abs(p - q) <= tol * q, (name, p, q)
+    # and far from the straight initial chains (Ree^2 = (2 (16-1))^2 = 900)
+    assert par[0] < 400
