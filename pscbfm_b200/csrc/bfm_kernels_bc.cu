@@ -637,6 +637,12 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
         for (uint32_t e = tid; e < nList; e += B) {
             uint32_t const g = list[e] & kSlotMask, dir = list[e] >> kSlotShift;
             uint32_t const p = pk[g];
+            // the neighbour references live in global memory: ask for them before the test, so
+            // their latency overlaps it
+            uint32_t nb[CodeWord<W>::kSlots];
+#pragma unroll
+            for (uint32_t q = 0; q < CodeWord<W>::kSlots; ++q)
+                nb[q] = q < S.maxc ? __ldg(S.nbrr + (size_t)q * np + g) : 0u;
             Plane pl;
             front_plane<true>(pl, tab, ptab, S, p, dir);
             unsigned long long hit = 0ull;
@@ -661,11 +667,14 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
             W const own = code[g];
             code[g] = code_shift(own, a, -s);
             uint32_t const n = uint32_t(own >> CodeWord<W>::kCountShift) & 7u;
-            for (uint32_t q = 0; q < n; ++q) {
-                uint32_t const ent = __ldg(S.nbrr + (size_t)q * np + g);
-                uint32_t const c = (0u - (uint32_t(own >> (9u * q + 3u * a)) & 7u)) & 7u;
-                uint32_t const nc = uint32_t(int32_t(c) + s) & 7u;
-                atomicXor(code + (ent & kSlotMask), W(c ^ nc) << (9u * (ent >> kSlotShift) + 3u * a));
+#pragma unroll
+            for (uint32_t q = 0; q < CodeWord<W>::kSlots; ++q) {
+                if (q < n) {
+                    uint32_t const ent = nb[q];
+                    uint32_t const c = (0u - (uint32_t(own >> (9u * q + 3u * a)) & 7u)) & 7u;
+                    uint32_t const nc = uint32_t(int32_t(c) + s) & 7u;
+                    atomicXor(code + (ent & kSlotMask), W(c ^ nc) << (9u * (ent >> kSlotShift) + 3u * a));
+                }
             }
             ++nAcc;
         }
