@@ -15,9 +15,10 @@
 // smallest axis's brick count laid out linearly (non-cubic boxes), through per-axis contribution
 // tables (brickTab). The reference keeps one Z-curve index per cell (src/pscbfm/CRITICAL.cu:13-34);
 // only the occupancy of each cell matters to the sweep, so the bit order inside a word is free.
-// Bond-code representation (codeMode != kCodeNone) adds, per monomer, its packed masked
-// coordinates (pk) and a word of bond-table indices (code), see CodeWord below, and per parity
-// the mover lists of the grid kernels (mlist, mword, mcount) in place of flags and tmark.
+// Bond-code representation (codeMode != kCodeNone) adds, per monomer, the lattice address of its
+// corner (pk = brick word << 6 | bit in the brick, see lattice_address) and a word of bond-table
+// indices (code), see CodeWord below, and per parity the mover lists of the grid kernels (mlist,
+// mword, mcount) in place of flags and tmark.
 #pragma once
 
 #include <cstdint>
@@ -61,8 +62,9 @@ struct SysDev {
     uint32_t* pk;                    // [npad] packed lattice coordinates x | y << 10 | z << 20 (masked)
     void* code;                      // [npad] uint32 (3 slots) or uint64 (6 slots) bond codes
     uint32_t const* nbrr;            // [maxc][npad] neighbour slot | reverse slot << 28
-    unsigned long long const* planeTab;   // [3][4][4][4][4] front-plane masks (see plane_table_fill)
+    unsigned long long const* planeTab;   // [3][64][4] front-plane masks (see plane_table_fill)
     uint8_t const* moveOk;           // [512] bit d: a bond with this index stays allowed after move d
+    uint32_t const* dirTab;          // [6][kDirWords] lattice-address parameters per direction (dir_table_fill)
     uint32_t* mlist;                 // [2][listStride] tentative movers per tile segment, per parity
     uint32_t* mword;                 // [2][listStride] the temporary-lattice word each listed mover marked
     uint32_t* mcount;                // [2][countStride] entries of each segment
@@ -213,10 +215,11 @@ inline void brick_tables_fill(uint32_t const nb[3], uint32_t* tab)
 }
 
 // Host: masks of the front plane inside the (at most 2x2) bricks it touches. Entry
-// ((((a*4 + fo)*4 + lu)*4 + lv)*4 + k) for a move along axis a: fo = in-brick coordinate of the
-// plane along a, lu / lv = in-brick coordinate of the first of the three cells along the two other
-// axes u < v; k = 2*i + j selects the brick (i: u-brick 0 or 1, j: v-brick 0 or 1). A run that
-// starts at 2 or 3 spills into the next brick; a zero mask means that brick is not touched.
+// ((a*64 + lo)*4 + k) for a move along axis a, lo = the low six bits of the lattice address of the
+// plane's first cell (its in-brick position: x&3 | (y&3)<<2 | (z&3)<<4): the plane lies at that
+// cell's coordinate along a and spans three cells from it along the two other axes u < v;
+// k = 2*i + j selects the brick (i: u-brick 0 or 1, j: v-brick 0 or 1). A run that starts at 2 or
+// 3 spills into the next brick; a zero mask means that brick is not touched.
 inline void plane_table_fill(unsigned long long* t)
 {
     auto run = [](uint32_t ax, uint32_t lo, uint32_t hi) {
@@ -226,21 +229,132 @@ inline void plane_table_fill(unsigned long long* t)
     };
     for (uint32_t a = 0; a < 3; ++a) {
         uint32_t const u = a == 0 ? 1u : 0u, v = a == 2 ? 1u : 2u;
-        for (uint32_t fo = 0; fo < 4; ++fo)
-            for (uint32_t lu = 0; lu < 4; ++lu)
-                for (uint32_t lv = 0; lv < 4; ++lv) {
-                    unsigned long long const mu0 = lu <= 1 ? run(u, lu, lu + 2) : run(u, lu, 3);
-                    unsigned long long const mu1 = lu <= 1 ? 0ull : run(u, 0, lu - 2);
-                    unsigned long long const mv0 = lv <= 1 ? run(v, lv, lv + 2) : run(v, lv, 3);
-                    unsigned long long const mv1 = lv <= 1 ? 0ull : run(v, 0, lv - 2);
-                    uint32_t const sh = brick_pos(fo, a);
-                    unsigned long long* e = t + ((((a * 4 + fo) * 4 + lu) * 4 + lv) * 4);
-                    e[0] = (mu0 * mv0) << sh;
-                    e[1] = (mu0 * mv1) << sh;
-                    e[2] = (mu1 * mv0) << sh;
-                    e[3] = (mu1 * mv1) << sh;
-                }
+        for (uint32_t lo = 0; lo < 64; ++lo) {
+            uint32_t const fo = (lo >> (2 * a)) & 3u, lu = (lo >> (2 * u)) & 3u, lv = (lo >> (2 * v)) & 3u;
+            unsigned long long const mu0 = lu <= 1 ? run(u, lu, lu + 2) : run(u, lu, 3);
+            unsigned long long const mu1 = lu <= 1 ? 0ull : run(u, 0, lu - 2);
+            unsigned long long const mv0 = lv <= 1 ? run(v, lv, lv + 2) : run(v, lv, 3);
+            unsigned long long const mv1 = lv <= 1 ? 0ull : run(v, 0, lv - 2);
+            uint32_t const sh = brick_pos(fo, a);
+            unsigned long long* e = t + (a * 64 + lo) * 4;
+            e[0] = (mu0 * mv0) << sh;
+            e[1] = (mu0 * mv1) << sh;
+            e[2] = (mu1 * mv0) << sh;
+            e[3] = (mu1 * mv1) << sh;
+        }
     }
+}
+
+// Lattice address of the corner cell (x, y, z) (coordinates inside the box): its brick word << 6
+// | its bit in the brick. The brick index scatters the bits of each axis's brick coordinate to
+// fixed positions, so every axis owns a fixed set of address bits (axis_address_mask) and a step
+// along one axis is an add confined to those bits: with M the axis's mask and D a step scattered
+// into M (one cell: the lowest bit of M; minus one cell: M itself), the stepped address is
+// (((p | ~M) + D) & M) | (p & ~M) — the set bits outside M carry across them, and the carry out of
+// the top of M is dropped, which wraps the axis periodically.
+inline uint32_t lattice_address(uint32_t x, uint32_t y, uint32_t z, uint32_t const nb[3], uint32_t const* tab)
+{
+    uint32_t const w = tab[x >> 2] + tab[nb[0] + (y >> 2)] + tab[nb[0] + nb[1] + (z >> 2)];
+    return (w << 6) | brick_bit(x, y, z);
+}
+
+inline uint32_t axis_address_mask(uint32_t a, uint32_t const nb[3], uint32_t const* tab)
+{
+    uint32_t const off = a == 0 ? 0u : (a == 1 ? nb[0] : nb[0] + nb[1]);
+    return (tab[off + nb[a] - 1u] << 6) | (3u << (2u * a));
+}
+
+// Per-direction parameters of the lattice-address arithmetic, kDirWords words per direction d
+// (axis a = d >> 1, the two other axes u < v):
+//   [0] Ma                     address mask of the move's axis
+//   [1] step                   the move, scattered into Ma (+1 or -1 along a)
+//   [2] Mu  [3] Mv             address masks of the two other axes
+//   [4] front                  the front plane's offset along a, scattered into Ma (+2 or -2)
+//   [5] Mu >> 6  [6] Mv >> 6   the masks of u and v in a brick index
+//   [7] wall                   address bits (in Ma) of the corner that may not move along d on a
+//                              walled axis (coordinate L-2 for +, 0 for -); 1 << 31 (never equal to
+//                              an address's bits in Ma) when the axis is periodic
+constexpr uint32_t kDirWords = 8;
+constexpr uint32_t kNoWall = 1u << 31;
+
+inline void dir_table_fill(uint32_t const nb[3], uint32_t const* tab, uint32_t const mask[3], uint32_t walls,
+                           uint32_t* out)
+{
+    uint32_t M[3];
+    for (uint32_t a = 0; a < 3; ++a) M[a] = axis_address_mask(a, nb, tab);
+    for (uint32_t d = 0; d < 6; ++d) {
+        uint32_t const a = d >> 1, u = a == 0 ? 1u : 0u, v = a == 2 ? 1u : 2u;
+        bool const up = (d & 1u) != 0;
+        uint32_t* e = out + d * kDirWords;
+        e[0] = M[a];
+        e[1] = up ? (1u << (2u * a)) : M[a];
+        e[2] = M[u];
+        e[3] = M[v];
+        e[4] = up ? (2u << (2u * a)) : (M[a] & ~(1u << (2u * a)));   // -2: every bit of Ma but the lowest
+        e[5] = M[u] >> 6;
+        e[6] = M[v] >> 6;
+        uint32_t c[3] = {0u, 0u, 0u};
+        c[a] = up ? mask[a] - 1u : 0u;
+        e[7] = ((walls >> a) & 1u) ? lattice_address(c[0], c[1], c[2], nb, tab) : kNoWall;
+    }
+}
+
+struct Plane {
+    uint32_t w[4];
+    unsigned long long m[4];
+};
+
+// Per-direction parameters of the lattice-address arithmetic (dir_table_fill); the kernels read
+// them from the CTA's shared copy of the table.
+struct DirParams {
+    uint32_t ma, step, mu, mv, front, bu, bv, wall;   // the order of dir_table_fill
+};
+
+__host__ __device__ __forceinline__ DirParams dir_params(uint32_t const* dtab, uint32_t dir)
+{
+    uint4 const a = *reinterpret_cast<uint4 const*>(dtab + dir * kDirWords);
+    uint4 const b = *reinterpret_cast<uint4 const*>(dtab + dir * kDirWords + 4u);
+    return {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+}
+
+// The lattice address p stepped by d, scattered into the axis mask m (see lattice_address).
+__host__ __device__ __forceinline__ uint32_t addr_add(uint32_t p, uint32_t m, uint32_t d)
+{
+    return (((p | ~m) + d) & m) | (p & ~m);
+}
+
+// The <= 2x2 brick words of the front plane of the move from p along dir and their masks. The
+// plane's first cell is p + 2 d along the move's axis and -1 along the two other axes; the low
+// six bits of its address select the masks (ptab: global memory through L1, or shared memory)
+// and the neighbouring bricks along u and v are one step of the brick index along those axes.
+template <bool kSharedTables>
+__host__ __device__ __forceinline__ void front_plane(Plane& pl, unsigned long long const* ptab, DirParams const& D,
+                                            uint32_t p, uint32_t dir)
+{
+    uint32_t const f = ((((p | ~D.ma) + D.front) & D.ma) | (((p | ~D.mu) + D.mu) & D.mu)) |
+                       (((p | ~D.mv) + D.mv) & D.mv);
+    uint32_t const ti = ((dir >> 1) * 64u + (f & 63u)) * 4u;
+    ulonglong2 m01, m23;
+#ifdef __CUDA_ARCH__
+    if (!kSharedTables) {
+        m01 = __ldg(reinterpret_cast<ulonglong2 const*>(ptab + ti));
+        m23 = __ldg(reinterpret_cast<ulonglong2 const*>(ptab + ti + 2));
+    } else
+#endif
+    {
+        m01 = *reinterpret_cast<ulonglong2 const*>(ptab + ti);
+        m23 = *reinterpret_cast<ulonglong2 const*>(ptab + ti + 2);
+    }
+    uint32_t const w00 = f >> 6;
+    uint32_t const w10 = addr_add(w00, D.bu, 1u);
+    pl.w[0] = w00;
+    pl.m[0] = m01.x;
+    pl.w[1] = addr_add(w00, D.bv, 1u);
+    pl.m[1] = m01.y;
+    pl.w[2] = w10;
+    pl.m[2] = m23.x;
+    pl.w[3] = addr_add(w10, D.bv, 1u);
+    pl.m[3] = m23.y;
 }
 
 // Host: bit d of ok[idx] is set when the bond with table index idx (neighbour - monomer, every

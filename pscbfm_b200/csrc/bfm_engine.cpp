@@ -330,7 +330,7 @@ void Updater::initialize()
     size_t const oDesc = take(sizeof(SysDev)), oSteps = take(sizeof(StepEntry) * kStepCap), oList = take(4);
     size_t const oGs = take(sizeof(GridSync));
     size_t const oPk = take(4ull * npad_), oCode = take(codeBytes * npad_), oNbrr = take(4ull * maxc_ * npad_);
-    size_t const oPlane = take(8ull * 768), oMoveOk = take(512);
+    size_t const oPlane = take(8ull * 768), oMoveOk = take(512), oDir = take(4ull * 6 * kDirWords);
     // mover lists of the bond-code grid kernels: one segment of kBcTileSpan entries per tile
     uint32_t const segs = codeMode_ == kCodeNone ? 0u : std::max((maxGroup_ + kBcTileSpan - 1) / kBcTileSpan, 1u);
     size_t const oMlist = take(4ull * 2 * segs * kBcTileSpan), oMword = take(4ull * 2 * segs * kBcTileSpan);
@@ -376,6 +376,7 @@ void Updater::initialize()
     h.nbrr = reinterpret_cast<uint32_t*>(base + oNbrr);
     h.planeTab = reinterpret_cast<unsigned long long*>(base + oPlane);
     h.moveOk = reinterpret_cast<uint8_t*>(base + oMoveOk);
+    h.dirTab = reinterpret_cast<uint32_t*>(base + oDir);
     h.mlist = reinterpret_cast<uint32_t*>(base + oMlist);
     h.mword = reinterpret_cast<uint32_t*>(base + oMword);
     h.mcount = reinterpret_cast<uint32_t*>(base + oMcount);
@@ -389,10 +390,17 @@ void Updater::initialize()
     plane_table_fill(hplane.data());
     std::vector<uint8_t> hmove(512);
     move_ok_fill(forbidden_, hmove.data());
+    // index 0 (the zero vector) is never a bond of a valid state: its entry allows every direction,
+    // so the unused (zero) fields of a code word drop out of the AND over all fields
+    hmove[0] = 0x3F;
+    std::vector<uint32_t> hdir(6 * kDirWords);
+    dir_table_fill(nb, tab.data(), h.mask, walls_, hdir.data());
     cuda_check(cudaMemcpyAsync(const_cast<unsigned long long*>(h.planeTab), hplane.data(), 8ull * 768,
                                cudaMemcpyHostToDevice, s), "upload plane table");
     cuda_check(cudaMemcpyAsync(const_cast<uint8_t*>(h.moveOk), hmove.data(), 512, cudaMemcpyHostToDevice, s),
                "upload move table");
+    cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(h.dirTab), hdir.data(), 4ull * hdir.size(),
+                               cudaMemcpyHostToDevice, s), "upload direction table");
     if (codeMode_ != kCodeNone) {
         hostCodes(hpk, hcode, hnbrr);
         cuda_check(cudaMemcpyAsync(h.pk, hpk.data(), 4ull * npad_, cudaMemcpyHostToDevice, s), "upload pk");
@@ -432,8 +440,10 @@ void Updater::initialize()
 
 void Updater::hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, std::vector<uint32_t>& nbrr) const
 {
-    // packed lattice coordinates, bond-code words and neighbour slots with their reverse slot,
-    // all in sorted order, from the host positions
+    // lattice addresses, bond-code words and neighbour slots with their reverse slot, all in
+    // sorted order, from the host positions
+    uint32_t const nb[3] = {box_[0] / 4, box_[1] / 4, box_[2] / 4};
+    std::vector<uint32_t> const tab = brick_tables(nb);
     pk.assign(npad_, 0u);
     size_t const w = codeMode_ == kCode64 ? 8 : 4;
     uint32_t const countShift = codeMode_ == kCode64 ? 54 : 27;
@@ -442,8 +452,8 @@ void Updater::hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, s
     for (uint32_t i = 0; i < n_; ++i) {
         uint32_t const s = oldToNew_[i];
         int32_t const* p = &xyz_[3 * (size_t)i];
-        pk[s] = (uint32_t(p[0]) & (box_[0] - 1)) | ((uint32_t(p[1]) & (box_[1] - 1)) << 10) |
-                ((uint32_t(p[2]) & (box_[2] - 1)) << 20);
+        pk[s] = lattice_address(uint32_t(p[0]) & (box_[0] - 1), uint32_t(p[1]) & (box_[1] - 1),
+                                uint32_t(p[2]) & (box_[2] - 1), nb, tab.data());
         uint64_t c = (uint64_t)nbrCnt_[i] << countShift;
         for (uint32_t k = 0; k < nbrCnt_[i]; ++k) {
             uint32_t const j = nbrIds_[(size_t)i * kMaxConn + k];
@@ -651,7 +661,7 @@ size_t Updater::residentSmem() const
 {
     uint32_t const ntab = dev_.h.nb[0] + dev_.h.nb[1] + dev_.h.nb[2];
     return codeMode_ == kCodeNone ? resident_smem_bytes(dev_.h.nwords, ntab)
-                                  : resident_bc_smem_bytes(dev_.h.nwords, ntab, npad_, maxGroup_, codeMode_);
+                                  : resident_bc_smem_bytes(dev_.h.nwords, npad_, maxGroup_, codeMode_);
 }
 
 bool Updater::residentEligible() const

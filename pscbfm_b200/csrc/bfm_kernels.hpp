@@ -57,7 +57,7 @@ cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRe
 constexpr int kSweepShapes = 3;
 cudaError_t launch_sweep_bc(SysDev const& hostDesc, StepEntry const* dSteps, uint32_t nSteps, uint32_t maxGroup,
                             GridSync* gs, uint32_t codeMode, int shape, cudaStream_t s, uint32_t* gridOut);
-size_t resident_bc_smem_bytes(uint32_t nwords, uint32_t ntab, uint32_t npad, uint32_t maxGroup, uint32_t codeMode);
+size_t resident_bc_smem_bytes(uint32_t nwords, uint32_t npad, uint32_t maxGroup, uint32_t codeMode);
 cudaError_t launch_resident_bc(SysDev const* dSys, uint32_t const* dList, uint32_t nCta, uint32_t perThread,
                                StepEntry const* dSteps, uint32_t nSys, uint32_t nSteps, size_t smem, uint32_t codeMode,
                                cudaStream_t s);

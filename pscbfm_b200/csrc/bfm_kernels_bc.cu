@@ -33,7 +33,7 @@ namespace bfm {
 
 namespace {
 
-constexpr uint32_t kMaxTab = 768;   // brick-table entries for boxes up to 1024 per side
+constexpr uint32_t kDirTab = 6 * kDirWords;   // words of the per-direction address table
 
 __device__ __forceinline__ void copy_desc(SysDev& dst, SysDev const* src)
 {
@@ -43,88 +43,18 @@ __device__ __forceinline__ void copy_desc(SysDev& dst, SysDev const* src)
     for (uint32_t w = threadIdx.x; w < sizeof(SysDev) / 4; w += blockDim.x) d[w] = s[w];
 }
 
-struct Plane {
-    uint32_t w[4];
-    unsigned long long m[4];
-};
-
-// The <= 2x2 brick words of the front plane at pk + 2 d (perpendicular +-1) and their masks; the
-// masks come from the plane table (ptab: global memory through L1, or shared memory).
-template <bool kSharedTables>
-__device__ __forceinline__ void front_plane(Plane& p, uint32_t const* tab, unsigned long long const* ptab,
-                                            SysDev const& S, uint32_t pk, uint32_t dir)
-{
-    uint32_t const c0 = pk & 1023u, c1 = (pk >> 10) & 1023u, c2 = pk >> 20;
-    uint32_t const a = dir >> 1;
-    // coordinate, box mask, brick count and table offset of the move axis a and of the two
-    // perpendicular axes u < v
-    uint32_t const ca = a == 0 ? c0 : (a == 1 ? c1 : c2);
-    uint32_t const cu = a == 0 ? c1 : c0;
-    uint32_t const cv = a == 2 ? c1 : c2;
-    uint32_t const ma = a == 0 ? S.mask[0] : (a == 1 ? S.mask[1] : S.mask[2]);
-    uint32_t const mu = a == 0 ? S.mask[1] : S.mask[0];
-    uint32_t const mv = a == 2 ? S.mask[1] : S.mask[2];
-    uint32_t const nbu = a == 0 ? S.nb[1] : S.nb[0];
-    uint32_t const nbv = a == 2 ? S.nb[1] : S.nb[2];
-    uint32_t const oa = a == 0 ? 0u : (a == 1 ? S.nb[0] : S.nb[0] + S.nb[1]);
-    uint32_t const ou = a == 0 ? S.nb[0] : 0u;
-    uint32_t const ov = a == 2 ? S.nb[0] : S.nb[0] + S.nb[1];
-    uint32_t const f = (ca + ((dir & 1u) ? 2u : 0xFFFFFFFEu)) & ma;
-    uint32_t const pu = (cu - 1u) & mu, pv = (cv - 1u) & mv;
-    uint32_t const ti = ((((a * 4u + (f & 3u)) * 4u + (pu & 3u)) * 4u + (pv & 3u)) * 4u);
-    ulonglong2 m01, m23;
-    if (kSharedTables) {
-        m01 = *reinterpret_cast<ulonglong2 const*>(ptab + ti);
-        m23 = *reinterpret_cast<ulonglong2 const*>(ptab + ti + 2);
-    } else {
-        m01 = __ldg(reinterpret_cast<ulonglong2 const*>(ptab + ti));
-        m23 = __ldg(reinterpret_cast<ulonglong2 const*>(ptab + ti + 2));
-    }
-    uint32_t const bu0 = pu >> 2, bv0 = pv >> 2;
-    uint32_t const wa = tab[oa + (f >> 2)];
-    uint32_t const wu0 = tab[ou + bu0], wu1 = tab[ou + ((bu0 + 1u) & (nbu - 1u))];
-    uint32_t const wv0 = tab[ov + bv0], wv1 = tab[ov + ((bv0 + 1u) & (nbv - 1u))];
-    p.w[0] = wa + wu0 + wv0;
-    p.m[0] = m01.x;
-    p.w[1] = wa + wu0 + wv1;
-    p.m[1] = m01.y;
-    p.w[2] = wa + wu1 + wv0;
-    p.m[2] = m23.x;
-    p.w[3] = wa + wu1 + wv1;
-    p.m[3] = m23.y;
-}
-
-// True if every bond of the code word stays allowed after the move along dir (move table).
+// True if every bond of the code word stays allowed after the move along dir: the AND of the move
+// table's entries over all fields (an unused field is index 0, whose entry allows every move).
 template <typename W, bool kSharedTables>
 __device__ __forceinline__ bool bonds_ok(W code, uint32_t dir, uint8_t const* ok)
 {
-    uint32_t const n = uint32_t(code >> CodeWord<W>::kCountShift) & 7u;
-    bool r = true;
+    uint32_t m = 0xFFu;
 #pragma unroll
     for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k) {
-        if (k < n) {
-            uint32_t const idx = uint32_t(code >> (9u * k)) & 511u;
-            uint32_t const m = kSharedTables ? ok[idx] : __ldg(ok + idx);
-            r = r && ((m >> dir) & 1u);
-        }
+        uint32_t const idx = uint32_t(code >> (9u * k)) & 511u;
+        m &= kSharedTables ? ok[idx] : __ldg(ok + idx);
     }
-    return r;
-}
-
-__device__ __forceinline__ uint32_t step_pk(uint32_t pk, uint32_t dir, uint32_t const* mask)
-{
-    uint32_t const a = dir >> 1;
-    uint32_t const sh = 10u * a;
-    uint32_t const c = (pk >> sh) & 1023u;
-    uint32_t const nc = (c + ((dir & 1u) ? 1u : 0xFFFFFFFFu)) & mask[a];
-    return (pk & ~(1023u << sh)) | (nc << sh);
-}
-
-__device__ __forceinline__ void cell_of(uint32_t pk, uint32_t const* tab, SysDev const& S, uint32_t& w, uint32_t& b)
-{
-    uint32_t const x = pk & 1023u, y = (pk >> 10) & 1023u, z = pk >> 20;
-    w = tab[x >> 2] + tab[S.nb[0] + (y >> 2)] + tab[S.nb[0] + S.nb[1] + (z >> 2)];
-    b = brick_bit(x, y, z);
+    return (m >> dir) & 1u;
 }
 
 // Loads of state the sweep changes (packed coordinates, codes, flags, lattices): through the
@@ -152,7 +82,7 @@ constexpr uint32_t kPerformTiles = 4;
 // ---------------------------------------------------------------------------------- check
 
 template <typename W, int MPT, bool kNc = true>
-__device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab, StepEntry const& st, uint32_t start,
+__device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab, StepEntry const& st, uint32_t start,
                                            uint32_t* segCount)
 {
     uint32_t const B = blockDim.x, tid = threadIdx.x;
@@ -174,7 +104,8 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab,
         pk[q] = a ? ldm<kNc>(PK + st.off + i) : 0u;
         code[q] = a ? ldm<kNc>(CODE + st.off + i) : W(0);
     }
-    // stage 2: direction, bonds, front-plane words
+    // stage 2: direction, walls, bonds, front-plane words; the target's address replaces the
+    // monomer's
     uint32_t dir[MPT];
     bool ok[MPT];
     Plane pl[MPT];
@@ -182,9 +113,10 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab,
     for (int q = 0; q < MPT; ++q) {
         uint32_t const i = start + tid + (uint32_t)q * B;
         dir[q] = move_dir(i, st.seed);
-        ok[q] = i < st.cnt && !wall_blocks(S.walls, (pk[q] >> (10u * (dir[q] >> 1))) & 1023u, dir[q], S.mask) &&
-                bonds_ok<W, false>(code[q], dir[q], S.moveOk);
-        front_plane<false>(pl[q], tab, S.planeTab, S, pk[q], dir[q]);
+        DirParams const D = dir_params(dtab, dir[q]);
+        ok[q] = i < st.cnt && (pk[q] & D.ma) != D.wall && bonds_ok<W, false>(code[q], dir[q], S.moveOk);
+        front_plane<false>(pl[q], S.planeTab, D, pk[q], dir[q]);
+        pk[q] = addr_add(pk[q], D.ma, D.step);
     }
     // stage 3: occupancy words
     unsigned long long hit[MPT];
@@ -207,9 +139,8 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab,
         if (lane == 0 && bal) base = atomicAdd(segCount, (uint32_t)__popc(bal));
         base = __shfl_sync(0xffffffffu, base, 0);
         if (go) {
-            uint32_t w, b;
-            cell_of(step_pk(pk[q], dir[q], S.mask), tab, S, w, b);
-            atomicOr(tcur + w, 1ull << b);
+            uint32_t const w = pk[q] >> 6;
+            atomicOr(tcur + w, 1ull << (pk[q] & 63u));
             uint32_t const slot = base + __popc(bal & ((1u << lane) - 1u));
             lcur[slot] = (st.off + i) | (dir[q] << 27);
             wcur[slot] = w;
@@ -223,7 +154,7 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* tab,
 // tiles (pre: the lists' starting offsets, lbase: the first tile's segment): re-test the front
 // plane on the temporary lattice and apply the free moves. Returns the moves applied.
 template <typename W, int MPT, bool kNc>
-__device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t const* tab,
+__device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t const* dtab,
                                                   unsigned long long const* tcur, uint32_t* lbase,
                                                   uint32_t const* pre, uint32_t nT, uint32_t total, uint32_t e)
 {
@@ -254,7 +185,10 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
             nbr[q][k] = (live[q] && k < S.maxc) ? __ldg(S.nbrr + (size_t)k * S.npad + g) : 0u;
     }
 #pragma unroll
-    for (int q = 0; q < MPT; ++q) front_plane<false>(pl[q], tab, S.planeTab, S, pk[q], (ent[q] >> 27) & 7u);
+    for (int q = 0; q < MPT; ++q) {
+        uint32_t const d = (ent[q] >> 27) & 7u;
+        front_plane<false>(pl[q], S.planeTab, dir_params(dtab, d), pk[q], d);
+    }
     unsigned long long hit[MPT];
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
@@ -272,15 +206,14 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
         uint32_t const dir = (ent[q] >> 27) & 7u;
         uint32_t const a = dir >> 1;
         int32_t const s = (dir & 1u) ? 1 : -1;
-        uint32_t const pk1 = step_pk(pk[q], dir, S.mask);
-        uint32_t w0, b0, w1, b1;
-        cell_of(pk[q], tab, S, w0, b0);
-        cell_of(pk1, tab, S, w1, b1);
+        uint2 const ms = *reinterpret_cast<uint2 const*>(dtab + dir * kDirWords);   // words 0, 1: Ma, step
+        uint32_t const pk1 = addr_add(pk[q], ms.x, ms.y);
+        uint32_t const w0 = pk[q] >> 6, w1 = pk1 >> 6;
         if (w0 == w1) {
-            atomicXor(S.lat + w0, (1ull << b0) | (1ull << b1));
+            atomicXor(S.lat + w0, (1ull << (pk[q] & 63u)) | (1ull << (pk1 & 63u)));
         } else {
-            atomicXor(S.lat + w0, 1ull << b0);
-            atomicXor(S.lat + w1, 1ull << b1);
+            atomicXor(S.lat + w0, 1ull << (pk[q] & 63u));
+            atomicXor(S.lat + w1, 1ull << (pk1 & 63u));
         }
         PK[g] = pk1;
         atomicAdd((a == 0 ? S.x : (a == 1 ? S.y : S.z)) + g, s);
@@ -307,7 +240,7 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
 // tile lies inside that sub-step's colour group (older lengths may remain in count[]). Every thread
 // of the CTA calls this; st.color == kNoColor only scrubs.
 template <typename W, int MPT, bool kNc = true>
-__device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* tab, StepEntry const& st,
+__device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* dtab, StepEntry const& st,
                                              uint32_t tile0, uint32_t nT, uint32_t* tally, uint32_t* pre)
 {
     uint32_t const B = blockDim.x, tid = threadIdx.x;
@@ -346,7 +279,7 @@ __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* ta
     uint32_t const total = pre[nT];
     uint32_t nAcc = 0;
     for (uint32_t e0 = 0; e0 < total; e0 += B * MPT)
-        nAcc += perform_chunk<W, MPT, kNc>(S, tab, tcur, lbase, pre, nT, total, e0 + tid);
+        nAcc += perform_chunk<W, MPT, kNc>(S, dtab, tcur, lbase, pre, nT, total, e0 + tid);
     if (tid < totalP) tprev[w0] = 0ull;
     for (uint32_t e = tid + B; e < totalP; e += B) tprev[scrubWord(e)] = 0ull;
     if (nAcc) atomicAdd(tally, nAcc);
@@ -363,7 +296,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_check_bc(const __gri
                                                          StepEntry const* __restrict__ steps)
 {
     __shared__ SysDev Sm;
-    __shared__ uint32_t tab[kMaxTab];
+    __shared__ __align__(16) uint32_t dtab[kDirTab];
     uint32_t sys = 0, start = blockIdx.x * (kGridBlock * MPT);
     if (kMulti) {
         TileRef const tr = tiles[blockIdx.x];
@@ -379,11 +312,10 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_check_bc(const __gri
     SysDev const& S = kMulti ? Sm : S1;
     static_assert(kGridBlock * MPT == kBcTileSpan, "a CTA covers one list segment");
     __shared__ uint32_t segCount;
-    uint32_t const ntab = S.nb[0] + S.nb[1] + S.nb[2];
-    for (uint32_t w = threadIdx.x; w < ntab; w += blockDim.x) tab[w] = S.brickTab[w];
+    if (threadIdx.x < kDirTab) dtab[threadIdx.x] = S.dirTab[threadIdx.x];
     if (threadIdx.x == 0) segCount = 0;
     __syncthreads();
-    check_body<W, MPT>(S, tab, st, start, &segCount);
+    check_body<W, MPT>(S, dtab, st, start, &segCount);
     __syncthreads();
     if (threadIdx.x == 0 && st.color != kNoColor) {
         S.mcount[(size_t)st.parity * S.countStride + start / kBcTileSpan] = segCount;
@@ -400,7 +332,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_perform_bc(const __g
                                                            uint32_t tilesPerCta)
 {
     __shared__ SysDev Sm;
-    __shared__ uint32_t tab[kMaxTab];
+    __shared__ __align__(16) uint32_t dtab[kDirTab];
     __shared__ uint32_t pre[2 * (kPerformTiles + 1)];
     // one system: tilesPerCta (<= kPerformTiles) consecutive tiles per CTA; a tile list: one tile
     uint32_t sys = 0, tile0 = blockIdx.x * tilesPerCta, nT = tilesPerCta;
@@ -422,11 +354,10 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_perform_bc(const __g
     }
     SysDev const& S = kMulti ? Sm : S1;
     __shared__ uint32_t tally;
-    uint32_t const ntab = S.nb[0] + S.nb[1] + S.nb[2];
-    for (uint32_t w = threadIdx.x; w < ntab; w += blockDim.x) tab[w] = S.brickTab[w];
+    if (threadIdx.x < kDirTab) dtab[threadIdx.x] = S.dirTab[threadIdx.x];
     if (threadIdx.x == 0) tally = 0;
     __syncthreads();
-    perform_body<W, MPT>(S, tab, st, tile0, nT, &tally, pre);
+    perform_body<W, MPT>(S, dtab, st, tile0, nT, &tally, pre);
     __syncthreads();
     if (threadIdx.x == 0) tally_flush(tally, S.stats, 2);
 }
@@ -501,11 +432,10 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
                uint32_t nTiles, GridSync* gs)
 {
     static_assert(kGridBlock * MPT == kBcTileSpan, "a tile is one list segment");
-    __shared__ uint32_t tab[kMaxTab];
+    __shared__ __align__(16) uint32_t dtab[kDirTab];
     __shared__ uint32_t tallyT, tallyA, okSm, segCount, pre[4];
     if (ld_acquire_gpu(&gs->fault) != 0u) return;   // an earlier launch failed: the state is not usable
-    uint32_t const ntab = S.nb[0] + S.nb[1] + S.nb[2];
-    for (uint32_t w = threadIdx.x; w < ntab; w += blockDim.x) tab[w] = S.brickTab[w];
+    if (threadIdx.x < kDirTab) dtab[threadIdx.x] = S.dirTab[threadIdx.x];
     if (threadIdx.x == 0) {
         tallyT = 0u;
         tallyA = 0u;
@@ -524,7 +454,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
             if (!active || start >= st.cnt) break;
             if (threadIdx.x == 0) segCount = 0u;
             __syncthreads();
-            check_body<W, MPT, false>(S, tab, st, start, &segCount);
+            check_body<W, MPT, false>(S, dtab, st, start, &segCount);
             __syncthreads();
             if (threadIdx.x == 0) {
                 S.mcount[(size_t)st.parity * S.countStride + k] = segCount;
@@ -536,7 +466,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
         uint32_t const reach = max(active ? st.cnt : 0u, st.pcnt);   // movers now, marks of t-1
         for (uint32_t k = blockIdx.x; k < nTiles; k += gridDim.x) {
             if (k * span >= reach) break;
-            perform_body<W, MPT, false>(S, tab, st, k, 1u, &tallyA, pre);
+            perform_body<W, MPT, false>(S, dtab, st, k, 1u, &tallyA, pre);
         }
         if (t + 1 < nSteps && !grid_barrier(gs, gen, &okSm)) return;
     }
@@ -565,16 +495,16 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
     uint32_t const nw = S.nwords, np = S.npad;
     uint32_t const B = blockDim.x, tid = threadIdx.x, lane = tid & 31u;
     unsigned long long* const ptab = smem;                  // 768 plane masks
-    unsigned long long* const lat = smem + 768;
+    uint32_t* const dtab = reinterpret_cast<uint32_t*>(smem + 768);   // kDirTab words (16-byte aligned)
+    unsigned long long* const lat = smem + 768 + kDirTab / 2;
     unsigned long long* const tmp = lat + nw;
     W* const code = reinterpret_cast<W*>(tmp + nw);
     uint32_t* const pk = reinterpret_cast<uint32_t*>(code + np);
-    uint32_t* const tab = pk + np;
-    uint32_t const ntab = S.nb[0] + S.nb[1] + S.nb[2];
-    uint8_t* const mok = reinterpret_cast<uint8_t*>(tab + ((ntab + 3u) & ~3u));   // 512 move-table bytes
+    uint8_t* const mok = reinterpret_cast<uint8_t*>(pk + np);   // 512 move-table bytes
     uint32_t* const list = reinterpret_cast<uint32_t*>(mok + 512);
     W const* const gcode = static_cast<W const*>(S.code);
     for (uint32_t w = tid; w < 768; w += B) ptab[w] = S.planeTab[w];
+    if (tid < kDirTab) dtab[tid] = S.dirTab[tid];
     for (uint32_t w = tid; w < 512; w += B) mok[w] = S.moveOk[w];
     for (uint32_t w = tid; w < nw; w += B) {
         lat[w] = S.lat[w];
@@ -584,7 +514,6 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
         code[g] = gcode[g];
         pk[g] = S.pk[g];
     }
-    for (uint32_t w = tid; w < ntab; w += B) tab[w] = S.brickTab[w];
     if (tid == 0) listCount = 0;
     uint32_t nTent = 0, nAcc = 0;
     unsigned long long nAtt = 0;
@@ -605,18 +534,18 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
             if (i < st.cnt) {
                 uint32_t const g = st.off + i;
                 uint32_t const dir = move_dir(i, st.seed);
-                if (!wall_blocks(S.walls, (pk[g] >> (10u * (dir >> 1))) & 1023u, dir, S.mask) &&
-                    bonds_ok<W, true>(code[g], dir, mok)) {
+                uint32_t const p = pk[g];
+                DirParams const D = dir_params(dtab, dir);
+                if ((p & D.ma) != D.wall && bonds_ok<W, true>(code[g], dir, mok)) {
                     Plane pl;
-                    front_plane<true>(pl, tab, ptab, S, pk[g], dir);
+                    front_plane<true>(pl, ptab, D, p, dir);
                     unsigned long long hit = 0ull;
 #pragma unroll
                     for (int r = 0; r < 4; ++r)
                         if (pl.m[r]) hit |= lat[pl.w[r]] & pl.m[r];
                     if (hit == 0ull) {
-                        uint32_t w, b;
-                        cell_of(step_pk(pk[g], dir, S.mask), tab, S, w, b);
-                        atomicOr(tmp + w, 1ull << b);
+                        uint32_t const to = addr_add(p, D.ma, D.step);
+                        atomicOr(tmp + (to >> 6), 1ull << (to & 63u));
                         go = true;
                         entry = g | (dir << kSlotShift);
                     }
@@ -644,7 +573,8 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
             for (uint32_t q = 0; q < CodeWord<W>::kSlots; ++q)
                 nb[q] = q < S.maxc ? __ldg(S.nbrr + (size_t)q * np + g) : 0u;
             Plane pl;
-            front_plane<true>(pl, tab, ptab, S, p, dir);
+            DirParams const D = dir_params(dtab, dir);
+            front_plane<true>(pl, ptab, D, p, dir);
             unsigned long long hit = 0ull;
 #pragma unroll
             for (int r = 0; r < 4; ++r)
@@ -652,15 +582,13 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
             if (hit != 0ull) continue;
             uint32_t const a = dir >> 1;
             int32_t const s = (dir & 1u) ? 1 : -1;
-            uint32_t const p1 = step_pk(p, dir, S.mask);
-            uint32_t w0, b0, w1, b1;
-            cell_of(p, tab, S, w0, b0);
-            cell_of(p1, tab, S, w1, b1);
+            uint32_t const p1 = addr_add(p, D.ma, D.step);
+            uint32_t const w0 = p >> 6, w1 = p1 >> 6;
             if (w0 == w1) {
-                atomicXor(lat + w0, (1ull << b0) | (1ull << b1));
+                atomicXor(lat + w0, (1ull << (p & 63u)) | (1ull << (p1 & 63u)));
             } else {
-                atomicXor(lat + w0, 1ull << b0);
-                atomicXor(lat + w1, 1ull << b1);
+                atomicXor(lat + w0, 1ull << (p & 63u));
+                atomicXor(lat + w1, 1ull << (p1 & 63u));
             }
             pk[g] = p1;
             atomicAdd((a == 0 ? S.x : (a == 1 ? S.y : S.z)) + g, s);
@@ -840,11 +768,10 @@ cudaError_t launch_sweep_bc(SysDev const& hostDesc, StepEntry const* dSteps, uin
     return cudaErrorInvalidValue;
 }
 
-size_t resident_bc_smem_bytes(uint32_t nwords, uint32_t ntab, uint32_t npad, uint32_t maxGroup, uint32_t codeMode)
+size_t resident_bc_smem_bytes(uint32_t nwords, uint32_t npad, uint32_t maxGroup, uint32_t codeMode)
 {
     size_t const w = codeMode == kCode64 ? 8 : 4;
-    return 768 * 8 + (size_t)nwords * 2 * 8 + (size_t)npad * (w + 4) + (size_t)((ntab + 3u) & ~3u) * 4 + 512 +
-           (size_t)maxGroup * 4;
+    return 768 * 8 + kDirTab * 4 + (size_t)nwords * 2 * 8 + (size_t)npad * (w + 4) + 512 + (size_t)maxGroup * 4;
 }
 
 namespace {

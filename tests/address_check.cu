@@ -1,0 +1,128 @@
+// Host check (no GPU) of the lattice-address arithmetic the bond-code kernels use
+// (pscbfm_b200/csrc/bfm_device.cuh). For several box shapes, every corner position and every
+// direction d (axis a, sign s):
+//   1. the step lands on the address of the cell one move away (periodic wrap included);
+//   2. the front plane's words and masks name exactly the nine cells p + 2 s e_a + i e_u + j e_v,
+//      i, j in {-1, 0, 1}: the cells whose corners the moved cube would newly overlap;
+//   3. on a walled axis the wall entry blocks exactly the moves that leave [0, L-2], and on a
+//      periodic axis it blocks none.
+// Prints "ok" and exits 0, or prints the first disagreement and exits 1.
+#include <cstdio>
+#include <set>
+#include <utility>
+#include <vector>
+
+#include "bfm_device.cuh"
+
+using namespace bfm;
+
+namespace {
+
+uint32_t address(uint32_t const c[3], uint32_t const nb[3], std::vector<uint32_t> const& tab)
+{
+    return lattice_address(c[0], c[1], c[2], nb, tab.data());
+}
+
+int check_box(uint32_t const box[3])
+{
+    uint32_t const nb[3] = {box[0] / 4, box[1] / 4, box[2] / 4};
+    uint32_t const mask[3] = {box[0] - 1, box[1] - 1, box[2] - 1};
+    std::vector<uint32_t> tab(nb[0] + nb[1] + nb[2]);
+    brick_tables_fill(nb, tab.data());
+    std::vector<unsigned long long> ptab(768);
+    plane_table_fill(ptab.data());
+    alignas(16) uint32_t dirP[6 * kDirWords], dirW[6 * kDirWords];
+    dir_table_fill(nb, tab.data(), mask, 0u, dirP);
+    dir_table_fill(nb, tab.data(), mask, 7u, dirW);
+    for (uint32_t z = 0; z < box[2]; ++z)
+        for (uint32_t y = 0; y < box[1]; ++y)
+            for (uint32_t x = 0; x < box[0]; ++x) {
+                uint32_t const c0[3] = {x, y, z};
+                uint32_t const p = address(c0, nb, tab);
+                for (uint32_t d = 0; d < 6; ++d) {
+                    uint32_t const a = d >> 1, u = a == 0 ? 1u : 0u, v = a == 2 ? 1u : 2u;
+                    int32_t const s = (d & 1u) ? 1 : -1;
+                    DirParams const D = dir_params(dirP, d);
+                    // the perform kernel loads words 0 and 1 of an entry as (Ma, step)
+                    if (dirP[d * kDirWords] != D.ma || dirP[d * kDirWords + 1] != D.step) {
+                        std::printf("direction table order\n");
+                        return 1;
+                    }
+                    // 1. the step
+                    uint32_t c1[3] = {x, y, z};
+                    c1[a] = uint32_t(int32_t(c1[a]) + s) & mask[a];
+                    if (addr_add(p, D.ma, D.step) != address(c1, nb, tab)) {
+                        std::printf("step: box %u %u %u at %u %u %u dir %u\n", box[0], box[1], box[2], x, y, z, d);
+                        return 1;
+                    }
+                    // 2. the front plane
+                    Plane pl;
+                    front_plane<true>(pl, ptab.data(), D, p, d);
+                    std::set<std::pair<uint32_t, uint32_t>> got, want;
+                    for (int r = 0; r < 4; ++r)
+                        for (uint32_t b = 0; b < 64; ++b)
+                            if ((pl.m[r] >> b) & 1ull) got.insert({pl.w[r], b});
+                    for (int i = -1; i <= 1; ++i)
+                        for (int j = -1; j <= 1; ++j) {
+                            uint32_t c[3] = {x, y, z};
+                            c[a] = uint32_t(int32_t(c[a]) + 2 * s) & mask[a];
+                            c[u] = uint32_t(int32_t(c[u]) + i) & mask[u];
+                            c[v] = uint32_t(int32_t(c[v]) + j) & mask[v];
+                            uint32_t const q = address(c, nb, tab);
+                            want.insert({q >> 6, q & 63u});
+                        }
+                    if (got != want) {
+                        std::printf("plane: box %u %u %u at %u %u %u dir %u (%zu cells, want %zu)\n", box[0], box[1],
+                                    box[2], x, y, z, d, got.size(), want.size());
+                        return 1;
+                    }
+                    // 3. walls: corners of a walled axis lie in [0, L-2]
+                    if ((p & D.ma) == D.wall) {
+                        std::printf("periodic axis blocked: box %u %u %u dir %u\n", box[0], box[1], box[2], d);
+                        return 1;
+                    }
+                    if (c0[a] <= mask[a] - 1u) {
+                        DirParams const W = dir_params(dirW, d);
+                        int32_t const t = int32_t(c0[a]) + s;
+                        bool const leaves = t < 0 || t > int32_t(mask[a]) - 1;
+                        if (((p & W.ma) == W.wall) != leaves) {
+                            std::printf("wall: box %u %u %u at %u %u %u dir %u\n", box[0], box[1], box[2], x, y, z, d);
+                            return 1;
+                        }
+                    }
+                }
+            }
+    return 0;
+}
+
+}  // namespace
+
+int main()
+{
+    uint32_t const boxes[][3] = {{4, 4, 4},    {8, 8, 8},    {32, 32, 32}, {16, 32, 64},
+                                 {64, 8, 4},   {128, 16, 32}, {4, 64, 8},  {8, 4, 256}};
+    for (auto const& b : boxes)
+        if (check_box(b)) return 1;
+    // the largest box: the address uses 30 bits, and the top corner steps and wraps correctly
+    uint32_t const nb[3] = {256, 256, 256};
+    std::vector<uint32_t> tab(768);
+    brick_tables_fill(nb, tab.data());
+    uint32_t const mask[3] = {1023, 1023, 1023};
+    alignas(16) uint32_t dir[6 * kDirWords];
+    dir_table_fill(nb, tab.data(), mask, 0u, dir);
+    uint32_t const top[3] = {1023, 1023, 1023}, zero[3] = {0, 0, 0};
+    uint32_t const pt = address(top, nb, tab);
+    if (pt >= (1u << 30)) return std::printf("address of the top corner exceeds 30 bits\n"), 1;
+    for (uint32_t d = 1; d < 6; d += 2) {
+        DirParams const D = dir_params(dir, d);
+        uint32_t c[3] = {1023, 1023, 1023};
+        c[d >> 1] = 0;
+        if (addr_add(pt, D.ma, D.step) != address(c, nb, tab)) return std::printf("wrap at 1024\n"), 1;
+        DirParams const M = dir_params(dir, d - 1);
+        uint32_t e[3] = {0, 0, 0};
+        e[d >> 1] = 1023;
+        if (addr_add(address(zero, nb, tab), M.ma, M.step) != address(e, nb, tab)) return std::printf("wrap at 0\n"), 1;
+    }
+    std::printf("ok\n");
+    return 0;
+}
