@@ -175,6 +175,54 @@ cudaError_t Batch::launchGrid(StepEntry const* e)
     return cudaSuccess;
 }
 
+void Batch::reserveSteps(size_t entries)
+{
+    // the previous run's copy has read the host staging once stepsFree_ has passed
+    cuda_check(cudaEventSynchronize(stepsFree_), "batch staging");
+    if (entries > hStepsCap_) {
+        cudaFreeHost(hSteps_);
+        hSteps_ = nullptr;
+        hStepsCap_ = 0;
+        cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * entries * 2), "cudaMallocHost(batch steps)");
+        hStepsCap_ = entries * 2;
+    }
+    if (entries > dStepsCap_) {
+        if (dStepsAll_) cuda_check(cudaFreeAsync(dStepsAll_, stream_), "cudaFreeAsync(batch steps)");
+        dStepsAll_ = nullptr;
+        dStepsCap_ = 0;
+        cuda_check(cudaMallocAsync(&dStepsAll_, sizeof(StepEntry) * entries * 2, stream_),
+                   "cudaMallocAsync(batch steps)");
+        dStepsCap_ = entries * 2;
+    }
+}
+
+void Batch::ensureGraph()
+{
+    if (graph_) return;
+    uint32_t const M = (uint32_t)members_.size();
+    cudaGraph_t g;
+    cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t err = cudaSuccess;
+    for (uint32_t t = 0; t < stepCap_ && err == cudaSuccess; ++t) err = launchGrid(dWindow_ + (size_t)t * M);
+    cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
+    cuda_check(err, "capture batch launches");
+    cuda_check(endErr, "end capture");
+    cudaError_t const ie = cudaGraphInstantiate(&graph_, g, 0);
+    cudaGraphDestroy(g);
+    cuda_check(ie, "graph instantiate");
+}
+
+void Batch::prepare(int32_t const* mcs)
+{
+    // one-time host work of a run (staging growth, graph capture), done ahead of a timed run
+    uint32_t const M = (uint32_t)members_.size();
+    uint64_t T = 0;
+    for (uint32_t m = 0; m < M; ++m) T = std::max(T, (uint64_t)std::max(mcs[m], 0) * members_[m]->nColors());
+    if (T == 0) return;
+    reserveSteps((size_t)T * M);
+    if (!grid_.empty() && T >= stepCap_) ensureGraph();
+}
+
 void Batch::run(int32_t nMcs)
 {
     if (nMcs <= 0) return;
@@ -206,23 +254,7 @@ void Batch::run(int32_t const* mcs)
     }
     if (T > 0) {
         size_t const entries = (size_t)T * M;
-        // the previous run's copy has read the host staging once stepsFree_ has passed
-        cuda_check(cudaEventSynchronize(stepsFree_), "batch staging");
-        if (entries > hStepsCap_) {
-            cudaFreeHost(hSteps_);
-            hSteps_ = nullptr;
-            hStepsCap_ = 0;
-            cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * entries * 2), "cudaMallocHost(batch steps)");
-            hStepsCap_ = entries * 2;
-        }
-        if (entries > dStepsCap_) {
-            if (dStepsAll_) cuda_check(cudaFreeAsync(dStepsAll_, stream_), "cudaFreeAsync(batch steps)");
-            dStepsAll_ = nullptr;
-            dStepsCap_ = 0;
-            cuda_check(cudaMallocAsync(&dStepsAll_, sizeof(StepEntry) * entries * 2, stream_),
-                       "cudaMallocAsync(batch steps)");
-            dStepsCap_ = entries * 2;
-        }
+        reserveSteps(entries);
         for (uint64_t t = 0; t < T; ++t)
             for (uint32_t m = 0; m < M; ++m) {
                 StepEntry& e = hSteps_[(size_t)t * M + m];
@@ -254,19 +286,7 @@ void Batch::run(int32_t const* mcs)
                     cuda_check(cudaMemcpyAsync(dWindow_, dStepsAll_ + t0 * M, sizeof(StepEntry) * stepCap_ * M,
                                                cudaMemcpyDeviceToDevice, stream_),
                                "batch window");
-                    if (!graph_) {
-                        cudaGraph_t g;
-                        cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
-                        cudaError_t err = cudaSuccess;
-                        for (uint32_t t = 0; t < stepCap_ && err == cudaSuccess; ++t)
-                            err = launchGrid(dWindow_ + (size_t)t * M);
-                        cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
-                        cuda_check(err, "capture batch launches");
-                        cuda_check(endErr, "end capture");
-                        cudaError_t const ie = cudaGraphInstantiate(&graph_, g, 0);
-                        cudaGraphDestroy(g);
-                        cuda_check(ie, "graph instantiate");
-                    }
+                    ensureGraph();
                     cuda_check(cudaGraphLaunch(graph_, stream_), "batch graph launch");
                 } else {
                     for (uint32_t t = 0; t < chunk; ++t)
@@ -328,6 +348,10 @@ float Batch::runTimed(int32_t nMcs)
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
     for (Updater* u : members_) u->synchronize();
     if (!built_) rebuild();
+    if (nMcs > 0) {
+        std::vector<int32_t> each(members_.size(), nMcs);
+        prepare(each.data());
+    }
     cudaEvent_t a, b;
     cuda_check(cudaEventCreate(&a), "cudaEventCreate");
     cuda_check(cudaEventCreate(&b), "cudaEventCreate");

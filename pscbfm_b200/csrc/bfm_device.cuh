@@ -66,7 +66,7 @@ struct SysDev {
     uint8_t const* moveOk;           // [512] bit d: a bond with this index stays allowed after move d
     uint32_t const* dirTab;          // [6][kDirWords] lattice-address parameters per direction (dir_table_fill)
     uint32_t* mlist;                 // [2][listStride] tentative movers per tile segment, per parity
-    uint32_t* mword;                 // [2][listStride] the temporary-lattice word each listed mover marked
+    uint32_t* mword;                 // [2][listStride] each listed mover's target address (the cell it marked)
     uint32_t* mcount;                // [2][countStride] entries of each segment
     uint32_t listStride, countStride;
     uint32_t codeMode;               // kCodeNone, kCode32, kCode64
@@ -323,16 +323,24 @@ __host__ __device__ __forceinline__ uint32_t addr_add(uint32_t p, uint32_t m, ui
     return (((p | ~m) + d) & m) | (p & ~m);
 }
 
-// The <= 2x2 brick words of the front plane of the move from p along dir and their masks. The
-// plane's first cell is p + 2 d along the move's axis and -1 along the two other axes; the low
+// The scattered step opposite to step along the axis with mask ma: -1 (ma) for a positive move,
+// +1 (the lowest bit of ma) for a negative one.
+__host__ __device__ __forceinline__ uint32_t addr_back(uint32_t ma, uint32_t step)
+{
+    return step ^ ma ^ (ma & (0u - ma));
+}
+
+// The <= 2x2 brick words of the front plane of a move along dir and their masks. The plane's
+// first cell is base + da along the move's axis (da scattered into Ma) and -1 along the two other
+// axes: da = D.front (+2 d) from the monomer's address, D.step (+d) from its target's; the low
 // six bits of its address select the masks (ptab: global memory through L1, or shared memory)
 // and the neighbouring bricks along u and v are one step of the brick index along those axes.
 template <bool kSharedTables>
 __host__ __device__ __forceinline__ void front_plane(Plane& pl, unsigned long long const* ptab, DirParams const& D,
-                                            uint32_t p, uint32_t dir)
+                                                     uint32_t base, uint32_t da, uint32_t dir)
 {
-    uint32_t const f = ((((p | ~D.ma) + D.front) & D.ma) | (((p | ~D.mu) + D.mu) & D.mu)) |
-                       (((p | ~D.mv) + D.mv) & D.mv);
+    uint32_t const f = ((((base | ~D.ma) + da) & D.ma) | (((base | ~D.mu) + D.mu) & D.mu)) |
+                       (((base | ~D.mv) + D.mv) & D.mv);
     uint32_t const ti = ((dir >> 1) * 64u + (f & 63u)) * 4u;
     ulonglong2 m01, m23;
 #ifdef __CUDA_ARCH__

@@ -28,6 +28,20 @@ void cuda_check(cudaError_t e, char const* what);
 
 std::vector<uint8_t> colour_bond_graph(uint32_t n, uint32_t const* cnt, uint32_t const* ids, uint32_t stride);
 
+// Offsets of a system's device arrays in its arena (each array on a 256-byte boundary) and the
+// arena's size. Updater::initialize lays its arena out with it; Server::estimateBytes bounds a
+// job's device bytes with it before the job is coloured.
+struct ArenaLayout {
+    size_t x, y, z, nbr, nnb, flags, mark, lat, tmp, tab, grp, stats, desc, steps, list, gs;
+    size_t pk, code, nbrr, plane, moveOk, dir, mlist, mword, mcount;
+    uint32_t segs;   // mover-list segments (tiles) per parity
+    size_t bytes;
+};
+ArenaLayout arena_layout(uint32_t npad, uint32_t maxc, uint32_t nwords, uint32_t ntab, uint32_t nColors,
+                         uint32_t maxGroup, uint32_t codeMode);
+// Bytes of the observables arena of a system (Updater::buildObservables).
+size_t observables_bytes(uint32_t npad, uint32_t nMol);
+
 // Host draw stream: per sub-step one draw for the colour (draw % nColors) and one for the seed,
 // in that order (src/pscbfm/CRITICAL.cu:509-510).
 enum DrawKind : int { kDrawCounter = 0, kDrawCallback = 1 };
@@ -81,6 +95,9 @@ public:
     void copySetup(Updater const& other);    // setter state of another (uninitialised) updater
     uint32_t maxNeighbours() const;
     uint64_t boxVolume() const { return (uint64_t)box_[0] * box_[1] * box_[2]; }
+    uint32_t boxSide(int a) const { return box_[a]; }
+    // molecules (connected components of the bond graph) of the current set-up, on the host
+    uint32_t countMolecules() const;
     void setCoordinates(int32_t const* xyz, uint32_t n);
     void getCoordinates(int32_t* xyz, uint32_t n);
     void setDrawCounter(uint64_t seed);
@@ -198,7 +215,10 @@ private:
     ObsDev obs_{};
     long long* dObsOut_ = nullptr;
     void buildObservables();
+    std::vector<uint32_t> moleculeRoots() const;   // lowest monomer id of each monomer's molecule
     cudaGraphExec_t graphFor(uint32_t nSteps);
+    int effectiveMode() const;                // the path run() takes (mode_ with AUTO resolved)
+    void prepareGraphs(uint32_t nSteps);      // capture the graphs a graph-path run of nSteps replays
     void hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, std::vector<uint32_t>& nbrr) const;
 
 public:
@@ -268,6 +288,9 @@ private:
     void rebuild();
     void validateMembers(Updater* const* members, uint32_t n) const;
     cudaError_t launchGrid(StepEntry const* e);   // one sub-step of every grid group, entries [members]
+    void reserveSteps(size_t entries);           // host staging and device entries for a run
+    void ensureGraph();                          // capture the graph of stepCap_ sub-steps
+    void prepare(int32_t const* mcs);            // both, for a run of mcs[i] MCS per member
     int gpu_;
     std::vector<Updater*> members_;
     std::vector<char> isResident_;

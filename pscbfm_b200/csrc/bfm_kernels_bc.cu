@@ -70,10 +70,11 @@ __device__ __forceinline__ T ldm(T const* p)
 
 // Mover lists: the check of sub-step t appends each tentative mover of tile k (kBcTileSpan
 // in-colour indices) to segment k of list[parity] (entry: slot g in bits 0-26, direction in
-// 27-29), the temporary-lattice word it marked to the same place of word[parity], and stores the
-// segment's length in count[parity][k]. The perform of sub-step t walks only the listed movers,
-// and zeroes the words listed at t-1 (nobody reads tmp[parity^1] during sub-step t, and the check
-// of t+1, which marks it again, comes after).
+// 27-29), the lattice address of its target (the temporary-lattice cell it marked) to the same
+// place of word[parity], and stores the segment's length in count[parity][k]. The perform of
+// sub-step t walks only the listed movers, and zeroes the words of the targets listed at t-1
+// (nobody reads tmp[parity^1] during sub-step t, and the check of t+1, which marks it again,
+// comes after).
 constexpr uint32_t kEntSlotMask = (1u << 27) - 1u;
 // tiles whose movers one perform CTA of a single-system launch walks (about 17 % of a tile's
 // monomers are tentative, so one tile leaves most of a CTA idle)
@@ -94,7 +95,8 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
     uint32_t* const lcur = S.mlist + seg;
     uint32_t* const wcur = S.mword + seg;
 
-    // stage 1: every independent load of the pass
+    // stage 1: every independent load of the pass; they stay in flight across the barrier that
+    // publishes the caller's shared writes (the direction table, the segment count)
     uint32_t pk[MPT];
     W code[MPT];
 #pragma unroll
@@ -104,6 +106,7 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
         pk[q] = a ? ldm<kNc>(PK + st.off + i) : 0u;
         code[q] = a ? ldm<kNc>(CODE + st.off + i) : W(0);
     }
+    __syncthreads();
     // stage 2: direction, walls, bonds, front-plane words; the target's address replaces the
     // monomer's
     uint32_t dir[MPT];
@@ -115,7 +118,7 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
         dir[q] = move_dir(i, st.seed);
         DirParams const D = dir_params(dtab, dir[q]);
         ok[q] = i < st.cnt && (pk[q] & D.ma) != D.wall && bonds_ok<W, false>(code[q], dir[q], S.moveOk);
-        front_plane<false>(pl[q], S.planeTab, D, pk[q], dir[q]);
+        front_plane<false>(pl[q], S.planeTab, D, pk[q], D.front, dir[q]);
         pk[q] = addr_add(pk[q], D.ma, D.step);
     }
     // stage 3: occupancy words
@@ -143,7 +146,7 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
             atomicOr(tcur + w, 1ull << (pk[q] & 63u));
             uint32_t const slot = base + __popc(bal & ((1u << lane) - 1u));
             lcur[slot] = (st.off + i) | (dir[q] << 27);
-            wcur[slot] = w;
+            wcur[slot] = pk[q];
         }
     }
 }
@@ -151,17 +154,20 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
 // ---------------------------------------------------------------------------------- perform
 
 // Entries e, e + B, ... (MPT of them, those below total) of the concatenated mover lists of nT
-// tiles (pre: the lists' starting offsets, lbase: the first tile's segment): re-test the front
-// plane on the temporary lattice and apply the free moves. Returns the moves applied.
+// tiles (pre: the lists' starting offsets, lbase / tbase: the first tile's segment of the entries
+// and of the target addresses): re-test the front plane on the temporary lattice and apply the
+// free moves. The plane and the old position follow from the target's address, so the monomer's
+// own address is not loaded. Returns the moves applied.
 template <typename W, int MPT, bool kNc>
 __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t const* dtab,
-                                                  unsigned long long const* tcur, uint32_t* lbase,
-                                                  uint32_t const* pre, uint32_t nT, uint32_t total, uint32_t e)
+                                                  unsigned long long const* tcur, uint32_t const* lbase,
+                                                  uint32_t const* tbase, uint32_t const* pre, uint32_t nT,
+                                                  uint32_t total, uint32_t e)
 {
     uint32_t const B = blockDim.x;
     uint32_t* const PK = S.pk;
     W* const CODE = static_cast<W*>(S.code);
-    uint32_t ent[MPT], pk[MPT], li[MPT];
+    uint32_t ent[MPT], to[MPT];
     bool live[MPT];
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
@@ -169,8 +175,9 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
         uint32_t j = 0;
         while (j + 1 < nT && eq >= pre[j + 1]) ++j;
         live[q] = eq < total;
-        li[q] = j * kBcTileSpan + (eq - pre[j]);
-        ent[q] = live[q] ? ldm<kNc>(lbase + li[q]) : 0u;
+        uint32_t const li = j * kBcTileSpan + (eq - pre[j]);
+        ent[q] = live[q] ? ldm<kNc>(lbase + li) : 0u;
+        to[q] = live[q] ? ldm<kNc>(tbase + li) : 0u;
     }
     Plane pl[MPT];
     W code[MPT];
@@ -178,7 +185,6 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
         uint32_t const g = ent[q] & kEntSlotMask;
-        pk[q] = live[q] ? PK[g] : 0u;
         code[q] = live[q] ? CODE[g] : W(0);
 #pragma unroll
         for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k)
@@ -187,7 +193,8 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
         uint32_t const d = (ent[q] >> 27) & 7u;
-        front_plane<false>(pl[q], S.planeTab, dir_params(dtab, d), pk[q], d);
+        DirParams const D = dir_params(dtab, d);
+        front_plane<false>(pl[q], S.planeTab, D, to[q], D.step, d);
     }
     unsigned long long hit[MPT];
 #pragma unroll
@@ -207,12 +214,13 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
         uint32_t const a = dir >> 1;
         int32_t const s = (dir & 1u) ? 1 : -1;
         uint2 const ms = *reinterpret_cast<uint2 const*>(dtab + dir * kDirWords);   // words 0, 1: Ma, step
-        uint32_t const pk1 = addr_add(pk[q], ms.x, ms.y);
-        uint32_t const w0 = pk[q] >> 6, w1 = pk1 >> 6;
+        uint32_t const pk1 = to[q];
+        uint32_t const pk0 = addr_add(pk1, ms.x, addr_back(ms.x, ms.y));
+        uint32_t const w0 = pk0 >> 6, w1 = pk1 >> 6;
         if (w0 == w1) {
-            atomicXor(S.lat + w0, (1ull << (pk[q] & 63u)) | (1ull << (pk1 & 63u)));
+            atomicXor(S.lat + w0, (1ull << (pk0 & 63u)) | (1ull << (pk1 & 63u)));
         } else {
-            atomicXor(S.lat + w0, 1ull << (pk[q] & 63u));
+            atomicXor(S.lat + w0, 1ull << (pk0 & 63u));
             atomicXor(S.lat + w1, 1ull << (pk1 & 63u));
         }
         PK[g] = pk1;
@@ -246,24 +254,32 @@ __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* dt
     uint32_t const B = blockDim.x, tid = threadIdx.x;
     unsigned long long const* const tcur = S.tmp + (size_t)st.parity * S.nwords;
     unsigned long long* const tprev = S.tmp + (size_t)(st.parity ^ 1u) * S.nwords;
-    uint32_t* const lbase = S.mlist + (size_t)st.parity * S.listStride + (size_t)tile0 * kBcTileSpan;
+    uint32_t const* const lbase = S.mlist + (size_t)st.parity * S.listStride + (size_t)tile0 * kBcTileSpan;
+    uint32_t const* const tbase = S.mword + (size_t)st.parity * S.listStride + (size_t)tile0 * kBcTileSpan;
     uint32_t const* const wprev = S.mword + (size_t)(st.parity ^ 1u) * S.listStride + (size_t)tile0 * kBcTileSpan;
     uint32_t const* const cnt = S.mcount + (size_t)st.parity * S.countStride + tile0;
     uint32_t const* const cntPrev = S.mcount + (size_t)(st.parity ^ 1u) * S.countStride + tile0;
     uint32_t* const preP = pre + nT + 1;
     bool const active = st.color != kNoColor;
-    __syncthreads();   // pre of an earlier call has been read
-    if (tid == 0) {
-        uint32_t acc = 0, accP = 0;
-        for (uint32_t j = 0; j < nT; ++j) {
-            uint32_t const start = (tile0 + j) * kBcTileSpan;
-            pre[j] = acc;
-            preP[j] = accP;
-            acc += (active && start < st.cnt) ? ldm<kNc>(cnt + j) : 0u;
-            accP += start < st.pcnt ? ldm<kNc>(cntPrev + j) : 0u;
+    // the list lengths, this sub-step's in lanes 0..nT-1 and the previous sub-step's in lanes
+    // 16..16+nT-1, loaded by one warp before the barrier and scanned after it
+    uint32_t const j = tid & 15u;
+    uint32_t c = 0;
+    if (tid < 32 && j < nT) {
+        uint32_t const start = (tile0 + j) * kBcTileSpan;
+        if (tid < 16) c = (active && start < st.cnt) ? ldm<kNc>(cnt + j) : 0u;
+        else c = start < st.pcnt ? ldm<kNc>(cntPrev + j) : 0u;
+    }
+    __syncthreads();   // pre of an earlier call has been read; the caller's shared writes are visible
+    if (tid < 32) {
+#pragma unroll
+        for (uint32_t o = 1; o < 16; o <<= 1) {
+            uint32_t const v = __shfl_up_sync(0xffffffffu, c, o, 16);
+            if (j >= o) c += v;
         }
-        pre[nT] = acc;
-        preP[nT] = accP;
+        uint32_t* const dst = tid < 16 ? pre : preP;
+        if (j < nT) dst[j + 1] = c;
+        if (j == 0) dst[0] = 0u;
     }
     __syncthreads();
     // scrub of the previous sub-step: every set bit of tmp[parity^1] belongs to one of its
@@ -273,13 +289,13 @@ __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* dt
     auto scrubWord = [&](uint32_t e) {
         uint32_t j = 0;
         while (j + 1 < nT && e >= preP[j + 1]) ++j;
-        return ldm<kNc>(wprev + j * kBcTileSpan + (e - preP[j]));
+        return ldm<kNc>(wprev + j * kBcTileSpan + (e - preP[j])) >> 6;
     };
     uint32_t const w0 = tid < totalP ? scrubWord(tid) : 0u;
     uint32_t const total = pre[nT];
     uint32_t nAcc = 0;
     for (uint32_t e0 = 0; e0 < total; e0 += B * MPT)
-        nAcc += perform_chunk<W, MPT, kNc>(S, dtab, tcur, lbase, pre, nT, total, e0 + tid);
+        nAcc += perform_chunk<W, MPT, kNc>(S, dtab, tcur, lbase, tbase, pre, nT, total, e0 + tid);
     if (tid < totalP) tprev[w0] = 0ull;
     for (uint32_t e = tid + B; e < totalP; e += B) tprev[scrubWord(e)] = 0ull;
     if (nAcc) atomicAdd(tally, nAcc);
@@ -298,6 +314,8 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_check_bc(const __gri
     __shared__ SysDev Sm;
     __shared__ __align__(16) uint32_t dtab[kDirTab];
     uint32_t sys = 0, start = blockIdx.x * (kGridBlock * MPT);
+    // one system: the direction table's load goes out with the step entry's
+    uint32_t dv = (!kMulti && threadIdx.x < kDirTab) ? S1.dirTab[threadIdx.x] : 0u;
     if (kMulti) {
         TileRef const tr = tiles[blockIdx.x];
         sys = tr.sys;
@@ -308,14 +326,14 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_check_bc(const __gri
     if (kMulti) {
         copy_desc(Sm, sysv + sys);
         __syncthreads();
+        if (threadIdx.x < kDirTab) dv = Sm.dirTab[threadIdx.x];
     }
     SysDev const& S = kMulti ? Sm : S1;
     static_assert(kGridBlock * MPT == kBcTileSpan, "a CTA covers one list segment");
     __shared__ uint32_t segCount;
-    if (threadIdx.x < kDirTab) dtab[threadIdx.x] = S.dirTab[threadIdx.x];
+    if (threadIdx.x < kDirTab) dtab[threadIdx.x] = dv;
     if (threadIdx.x == 0) segCount = 0;
-    __syncthreads();
-    check_body<W, MPT>(S, dtab, st, start, &segCount);
+    check_body<W, MPT>(S, dtab, st, start, &segCount);   // publishes both with its first barrier
     __syncthreads();
     if (threadIdx.x == 0 && st.color != kNoColor) {
         S.mcount[(size_t)st.parity * S.countStride + start / kBcTileSpan] = segCount;
@@ -336,6 +354,8 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_perform_bc(const __g
     __shared__ uint32_t pre[2 * (kPerformTiles + 1)];
     // one system: tilesPerCta (<= kPerformTiles) consecutive tiles per CTA; a tile list: one tile
     uint32_t sys = 0, tile0 = blockIdx.x * tilesPerCta, nT = tilesPerCta;
+    // one system: the direction table's load goes out with the step entry's
+    uint32_t dv = (!kMulti && threadIdx.x < kDirTab) ? S1.dirTab[threadIdx.x] : 0u;
     if (kMulti) {
         TileRef const tr = tiles[blockIdx.x];
         sys = tr.sys;
@@ -351,13 +371,13 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_perform_bc(const __g
     if (kMulti) {
         copy_desc(Sm, sysv + sys);
         __syncthreads();
+        if (threadIdx.x < kDirTab) dv = Sm.dirTab[threadIdx.x];
     }
     SysDev const& S = kMulti ? Sm : S1;
     __shared__ uint32_t tally;
-    if (threadIdx.x < kDirTab) dtab[threadIdx.x] = S.dirTab[threadIdx.x];
+    if (threadIdx.x < kDirTab) dtab[threadIdx.x] = dv;
     if (threadIdx.x == 0) tally = 0;
-    __syncthreads();
-    perform_body<W, MPT>(S, dtab, st, tile0, nT, &tally, pre);
+    perform_body<W, MPT>(S, dtab, st, tile0, nT, &tally, pre);   // publishes both with its first barrier
     __syncthreads();
     if (threadIdx.x == 0) tally_flush(tally, S.stats, 2);
 }
@@ -452,8 +472,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
         for (uint32_t k = blockIdx.x; k < nTiles; k += gridDim.x) {
             uint32_t const start = k * span;
             if (!active || start >= st.cnt) break;
-            if (threadIdx.x == 0) segCount = 0u;
-            __syncthreads();
+            if (threadIdx.x == 0) segCount = 0u;   // published by check_body's first barrier
             check_body<W, MPT, false>(S, dtab, st, start, &segCount);
             __syncthreads();
             if (threadIdx.x == 0) {
@@ -538,7 +557,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
                 DirParams const D = dir_params(dtab, dir);
                 if ((p & D.ma) != D.wall && bonds_ok<W, true>(code[g], dir, mok)) {
                     Plane pl;
-                    front_plane<true>(pl, ptab, D, p, dir);
+                    front_plane<true>(pl, ptab, D, p, D.front, dir);
                     unsigned long long hit = 0ull;
 #pragma unroll
                     for (int r = 0; r < 4; ++r)
@@ -574,7 +593,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
                 nb[q] = q < S.maxc ? __ldg(S.nbrr + (size_t)q * np + g) : 0u;
             Plane pl;
             DirParams const D = dir_params(dtab, dir);
-            front_plane<true>(pl, ptab, D, p, dir);
+            front_plane<true>(pl, ptab, D, p, D.front, dir);
             unsigned long long hit = 0ull;
 #pragma unroll
             for (int r = 0; r < 4; ++r)

@@ -59,13 +59,21 @@ struct Server::Job {
 
 size_t Server::estimateBytes(Updater const& setup)
 {
-    // mirrors the arena of Updater::initialize (with colour-group padding slack) plus the
-    // observables arena and the step staging
-    uint64_t const n = setup.nMonomers() + 32ull * 8;
-    uint64_t const maxc = std::max<uint64_t>(setup.maxNeighbours(), 1);
-    uint64_t const V = setup.boxVolume();
-    uint64_t const perMonomer = 12 + 4 * maxc + 1 + 2 + 8 + 4 + 8 + 4 * maxc + 4 + 12;
-    return (size_t)(n * perMonomer + 3 * V / 8 + 64 * 1024 + 16 * 1024);
+    // An upper bound of what the job holds on the device, before it is coloured: the arena of
+    // Updater::initialize with the largest values colouring can give (greedy colouring uses at
+    // most maxc + 1 colours; each colour group is padded to 32 slots; one group may hold every
+    // monomer; 64-bit bond codes), the observables arena, and the job's share of its lane's step
+    // entries (a chunk of at most kMaxChunkMcs MCS, buffers grown to twice the need).
+    uint32_t const n = setup.nMonomers();
+    uint32_t const maxc = std::max(setup.maxNeighbours(), 1u);
+    uint32_t const nC = maxc + 1;
+    uint32_t const npad = std::max(n + 32u * nC, 32u);
+    uint32_t const nwords = (uint32_t)(setup.boxVolume() / 64);
+    uint32_t const ntab = (setup.boxSide(0) + setup.boxSide(1) + setup.boxSide(2)) / 4;
+    size_t const arena = arena_layout(npad, maxc, nwords, ntab, nC, std::max(n, 1u), kCode64).bytes;
+    size_t const obs = observables_bytes(npad, setup.countMolecules());
+    size_t const steps = 2ull * sizeof(StepEntry) * kMaxChunkMcs * nC;
+    return arena + obs + steps;
 }
 
 Server::Server(int gpu, size_t budgetBytes, uint32_t maxJobs) : gpu_(gpu), budget_(budgetBytes), maxJobs_(maxJobs)

@@ -57,7 +57,22 @@ int check_box(uint32_t const box[3])
                     }
                     // 2. the front plane
                     Plane pl;
-                    front_plane<true>(pl, ptab.data(), D, p, d);
+                    front_plane<true>(pl, ptab.data(), D, p, D.front, d);
+                    // the same plane from the target's address (the grid perform's form), and the
+                    // step back from the target
+                    uint32_t const to = addr_add(p, D.ma, D.step);
+                    Plane pt;
+                    front_plane<true>(pt, ptab.data(), D, to, D.step, d);
+                    for (int r = 0; r < 4; ++r)
+                        if (pt.m[r] != pl.m[r] || (pl.m[r] && pt.w[r] != pl.w[r])) {
+                            std::printf("plane from the target: box %u %u %u at %u %u %u dir %u\n", box[0], box[1],
+                                        box[2], x, y, z, d);
+                            return 1;
+                        }
+                    if (addr_add(to, D.ma, addr_back(D.ma, D.step)) != p) {
+                        std::printf("step back: box %u %u %u at %u %u %u dir %u\n", box[0], box[1], box[2], x, y, z, d);
+                        return 1;
+                    }
                     std::set<std::pair<uint32_t, uint32_t>> got, want;
                     for (int r = 0; r < 4; ++r)
                         for (uint32_t b = 0; b < 64; ++b)

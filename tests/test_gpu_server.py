@@ -98,6 +98,16 @@ def test_budget_refusal_and_queueing():
     srv.close()
 
 
+@pytest.mark.parametrize("build", [S.small_chains, S.crosslinked_network, S.rings_and_free, S.dense_melt,
+                                   lambda: S.serpentine_chains(64, 64, 0.4, seed=13)])
+def test_estimate_covers_the_arena(build):
+    """Admission charges at least what the system's arena takes on the device."""
+    s = build()
+    u = P.UpdaterGPUScBFM_AB_Type(0).load_system(s)
+    assert P.Server.estimate_bytes(s) >= u.device_bytes()
+    u.close()
+
+
 def test_cancel_pending_and_running():
     srv = P.Server(0, budget_bytes=8 << 30, max_jobs=1)
     a = srv.submit(S.small_chains(), 200000, 100000)   # long: occupies the only slot
