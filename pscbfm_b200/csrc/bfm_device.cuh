@@ -64,7 +64,7 @@ struct SysDev {
     uint32_t const* nbrr;            // [maxc][npad] neighbour slot | reverse slot << 28
     unsigned long long const* planeTab;   // [3][64][4] front-plane masks (see plane_table_fill)
     uint8_t const* moveOk;           // [512] bit d: a bond with this index stays allowed after move d
-    uint32_t const* dirTab;          // [6][kDirWords] lattice-address parameters per direction (dir_table_fill)
+    uint32_t const* dirTab;          // [kDirTab] lattice-address parameters per direction (dir_table_fill)
     uint32_t* mlist;                 // [2][listStride] tentative movers per tile segment, per parity
     uint32_t* mword;                 // [2][listStride] each listed mover's target address (the cell it marked)
     uint32_t* mcount;                // [2][countStride] entries of each segment
@@ -265,7 +265,9 @@ inline uint32_t axis_address_mask(uint32_t a, uint32_t const nb[3], uint32_t con
 }
 
 // Per-direction parameters of the lattice-address arithmetic, kDirWords words per direction d
-// (axis a = d >> 1, the two other axes u < v):
+// (axis a = d >> 1, the two other axes u < v), stored as two arrays of 16-byte halves: words 0-3
+// of direction d at 4 d, words 4-7 at kDirHalf + 4 d (kDirTab words in all). A warp's 16-byte
+// loads of the six directions then fall in distinct shared-memory banks.
 //   [0] Ma                     address mask of the move's axis
 //   [1] step                   the move, scattered into Ma (+1 or -1 along a)
 //   [2] Mu  [3] Mv             address masks of the two other axes
@@ -275,6 +277,8 @@ inline uint32_t axis_address_mask(uint32_t a, uint32_t const nb[3], uint32_t con
 //                              walled axis (coordinate L-2 for +, 0 for -); 1 << 31 (never equal to
 //                              an address's bits in Ma) when the axis is periodic
 constexpr uint32_t kDirWords = 8;
+constexpr uint32_t kDirHalf = 6 * 4;
+constexpr uint32_t kDirTab = 6 * kDirWords;
 constexpr uint32_t kNoWall = 1u << 31;
 
 inline void dir_table_fill(uint32_t const nb[3], uint32_t const* tab, uint32_t const mask[3], uint32_t walls,
@@ -285,17 +289,18 @@ inline void dir_table_fill(uint32_t const nb[3], uint32_t const* tab, uint32_t c
     for (uint32_t d = 0; d < 6; ++d) {
         uint32_t const a = d >> 1, u = a == 0 ? 1u : 0u, v = a == 2 ? 1u : 2u;
         bool const up = (d & 1u) != 0;
-        uint32_t* e = out + d * kDirWords;
+        uint32_t* e = out + d * 4;
+        uint32_t* f = out + kDirHalf + d * 4;
         e[0] = M[a];
         e[1] = up ? (1u << (2u * a)) : M[a];
         e[2] = M[u];
         e[3] = M[v];
-        e[4] = up ? (2u << (2u * a)) : (M[a] & ~(1u << (2u * a)));   // -2: every bit of Ma but the lowest
-        e[5] = M[u] >> 6;
-        e[6] = M[v] >> 6;
+        f[0] = up ? (2u << (2u * a)) : (M[a] & ~(1u << (2u * a)));   // -2: every bit of Ma but the lowest
+        f[1] = M[u] >> 6;
+        f[2] = M[v] >> 6;
         uint32_t c[3] = {0u, 0u, 0u};
         c[a] = up ? mask[a] - 1u : 0u;
-        e[7] = ((walls >> a) & 1u) ? lattice_address(c[0], c[1], c[2], nb, tab) : kNoWall;
+        f[3] = ((walls >> a) & 1u) ? lattice_address(c[0], c[1], c[2], nb, tab) : kNoWall;
     }
 }
 
@@ -312,8 +317,8 @@ struct DirParams {
 
 __host__ __device__ __forceinline__ DirParams dir_params(uint32_t const* dtab, uint32_t dir)
 {
-    uint4 const a = *reinterpret_cast<uint4 const*>(dtab + dir * kDirWords);
-    uint4 const b = *reinterpret_cast<uint4 const*>(dtab + dir * kDirWords + 4u);
+    uint4 const a = *reinterpret_cast<uint4 const*>(dtab + dir * 4u);
+    uint4 const b = *reinterpret_cast<uint4 const*>(dtab + kDirHalf + dir * 4u);
     return {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 }
 

@@ -86,7 +86,7 @@ ArenaLayout arena_layout(uint32_t npad, uint32_t maxc, uint32_t nwords, uint32_t
     L.nbrr = take(4ull * maxc * npad);
     L.plane = take(8ull * 768);
     L.moveOk = take(512);
-    L.dir = take(4ull * 6 * kDirWords);
+    L.dir = take(4ull * kDirTab);
     // mover lists of the bond-code grid kernels: one segment of kBcTileSpan entries per tile
     L.segs = codeMode == kCodeNone ? 0u : std::max((maxGroup + kBcTileSpan - 1) / kBcTileSpan, 1u);
     L.mlist = take(4ull * 2 * L.segs * kBcTileSpan);
@@ -424,7 +424,7 @@ void Updater::initialize()
     // index 0 (the zero vector) is never a bond of a valid state: its entry allows every direction,
     // so the unused (zero) fields of a code word drop out of the AND over all fields
     hmove[0] = 0x3F;
-    std::vector<uint32_t> hdir(6 * kDirWords);
+    std::vector<uint32_t> hdir(kDirTab);
     dir_table_fill(nb, tab.data(), h.mask, walls_, hdir.data());
     cuda_check(cudaMemcpyAsync(const_cast<unsigned long long*>(h.planeTab), hplane.data(), 8ull * 768,
                                cudaMemcpyHostToDevice, s), "upload plane table");

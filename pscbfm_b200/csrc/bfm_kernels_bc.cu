@@ -33,7 +33,6 @@ namespace bfm {
 
 namespace {
 
-constexpr uint32_t kDirTab = 6 * kDirWords;   // words of the per-direction address table
 
 __device__ __forceinline__ void copy_desc(SysDev& dst, SysDev const* src)
 {
@@ -213,7 +212,7 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
         uint32_t const dir = (ent[q] >> 27) & 7u;
         uint32_t const a = dir >> 1;
         int32_t const s = (dir & 1u) ? 1 : -1;
-        uint2 const ms = *reinterpret_cast<uint2 const*>(dtab + dir * kDirWords);   // words 0, 1: Ma, step
+        uint2 const ms = *reinterpret_cast<uint2 const*>(dtab + dir * 4u);   // words 0, 1: Ma, step
         uint32_t const pk1 = to[q];
         uint32_t const pk0 = addr_add(pk1, ms.x, addr_back(ms.x, ms.y));
         uint32_t const w0 = pk0 >> 6, w1 = pk1 >> 6;

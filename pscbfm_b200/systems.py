@@ -177,33 +177,36 @@ def crosslinked_network() -> BfmSystem:
     return from_bonds((L, L, L), xyz, bonds, attributes=attrs, maxc=8, name="network128_512x6", seed=3)
 
 
-def serpentine_chains(L: int, chain_len: int, phi: float, name: str = "", seed: int = 0) -> BfmSystem:
-    """Periodic L^3 box with floor(phi L^3 / (8 chain_len)) linear chains (at least one).
+def serpentine_chains(L, chain_len: int, phi: float, name: str = "", seed: int = 0) -> BfmSystem:
+    """Periodic box (L^3 for an int L, Lx x Ly x Lz for a 3-tuple) with floor(phi V / (8 chain_len))
+    linear chains (at least one), V the box volume.
 
     Monomer slots are the points of the lattice 2Z^3 inside the box, visited by a boustrophedon
     path (x fastest, rows reversing, layers reversing) whose consecutive slots are one axis bond
     of length 2 apart. Chain c occupies chain_len consecutive slots starting at slot
-    floor(c P / n_chains), P = (L/2)^3, so chains longer than the box fold instead of
+    floor(c P / n_chains), P the number of slots, so chains longer than the box fold instead of
     overlapping themselves."""
-    h = L // 2
-    P = h ** 3
-    n_chains = max(1, int(np.floor(phi * L ** 3 / (8 * chain_len))))
+    box = (L, L, L) if np.isscalar(L) else tuple(int(v) for v in L)
+    hx, hy, hz = (v // 2 for v in box)
+    P = hx * hy * hz
+    n_chains = max(1, int(np.floor(phi * box[0] * box[1] * box[2] / (8 * chain_len))))
     if n_chains * chain_len > P:
         raise ValueError("system does not fit")
     s = np.arange(P, dtype=np.int64)
-    zc, rem = s // (h * h), s % (h * h)
-    yr = rem // h
-    yc = np.where(zc % 2 == 0, yr, h - 1 - yr)
-    xr = rem % h
-    row = zc * h + yr                      # running row count keeps the x direction alternating
-    xc = np.where(row % 2 == 0, xr, h - 1 - xr)
+    zc, rem = s // (hx * hy), s % (hx * hy)
+    yr = rem // hx
+    yc = np.where(zc % 2 == 0, yr, hy - 1 - yr)
+    xr = rem % hx
+    row = zc * hy + yr                     # running row count keeps the x direction alternating
+    xc = np.where(row % 2 == 0, xr, hx - 1 - xr)
     path = np.stack([2 * xc, 2 * yc, 2 * zc], axis=1)
     starts = (np.arange(n_chains, dtype=np.int64) * P) // n_chains
     slots = (starts[:, None] + np.arange(chain_len)[None, :]).reshape(-1)
     xyz = path[slots].astype(np.int32)
     ids = (np.arange(n_chains)[:, None] * chain_len + np.arange(chain_len - 1)[None, :]).reshape(-1)
     bonds = np.stack([ids, ids + 1], axis=1)
-    return from_bonds((L, L, L), xyz, bonds, name=name or f"serp{L}_{n_chains}x{chain_len}", seed=seed)
+    tag = f"{box[0]}" if box[0] == box[1] == box[2] else "x".join(str(v) for v in box)
+    return from_bonds(box, xyz, bonds, name=name or f"serp{tag}_{n_chains}x{chain_len}", seed=seed)
 
 
 def walled(s: BfmSystem, walls: int = 7, name: str = "") -> BfmSystem:

@@ -31,7 +31,7 @@ int check_box(uint32_t const box[3])
     brick_tables_fill(nb, tab.data());
     std::vector<unsigned long long> ptab(768);
     plane_table_fill(ptab.data());
-    alignas(16) uint32_t dirP[6 * kDirWords], dirW[6 * kDirWords];
+    alignas(16) uint32_t dirP[kDirTab], dirW[kDirTab];
     dir_table_fill(nb, tab.data(), mask, 0u, dirP);
     dir_table_fill(nb, tab.data(), mask, 7u, dirW);
     for (uint32_t z = 0; z < box[2]; ++z)
@@ -44,7 +44,7 @@ int check_box(uint32_t const box[3])
                     int32_t const s = (d & 1u) ? 1 : -1;
                     DirParams const D = dir_params(dirP, d);
                     // the perform kernel loads words 0 and 1 of an entry as (Ma, step)
-                    if (dirP[d * kDirWords] != D.ma || dirP[d * kDirWords + 1] != D.step) {
+                    if (dirP[d * 4] != D.ma || dirP[d * 4 + 1] != D.step) {
                         std::printf("direction table order\n");
                         return 1;
                     }
@@ -123,7 +123,7 @@ int main()
     std::vector<uint32_t> tab(768);
     brick_tables_fill(nb, tab.data());
     uint32_t const mask[3] = {1023, 1023, 1023};
-    alignas(16) uint32_t dir[6 * kDirWords];
+    alignas(16) uint32_t dir[kDirTab];
     dir_table_fill(nb, tab.data(), mask, 0u, dir);
     uint32_t const top[3] = {1023, 1023, 1023}, zero[3] = {0, 0, 0};
     uint32_t const pt = address(top, nb, tab);

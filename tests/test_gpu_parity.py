@@ -49,6 +49,32 @@ def test_engine_reproduces_reference_updater(name, mode, repr_):
     assert st["mcs"] == sum(chunks)
 
 
+NON_CUBIC = {
+    "serp64x32x128_lc32": (lambda: S.serpentine_chains((64, 32, 128), 32, 0.4, seed=31), [150, 50]),
+    "serp16x64x32_lc16_walls_xz": (lambda: S.walled(S.serpentine_chains((16, 64, 32), 16, 0.35, seed=33), walls=5),
+                                   [200]),
+    "serp128x8x16_lc8": (lambda: S.serpentine_chains((128, 8, 16), 8, 0.3, seed=35), [300]),
+    "serp8x8x256_lc32": (lambda: S.serpentine_chains((8, 8, 256), 32, 0.3, seed=37), [120, 180]),
+}
+
+
+@pytest.mark.parametrize("repr_", ["codes", "gather"])
+@pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent"])
+@pytest.mark.parametrize("name", list(NON_CUBIC))
+def test_non_cubic_boxes_vs_oracle(name, mode, repr_):
+    """Boxes with unequal power-of-two sides: the brick index interleaves the axes' low bits and
+    appends the longer axes' high bits. The reference updater always indexes its lattice by an
+    interleaved Z-curve, which runs past its lattice array when the sides differ, so the oracle
+    (a linear lattice) alone pins these. The resident mode falls back to the graph path where a
+    system does not fit one CTA."""
+    build, chunks = NON_CUBIC[name]
+    s = build()
+    want, _ = O.run(s, sum(chunks))
+    xyz, st = run_engine(s, chunks, MODES[mode], repr_=REPRS[repr_])
+    assert np.array_equal(xyz, want)
+    assert st["mcs"] == sum(chunks)
+
+
 def test_asymmetric_lists_fall_back_to_gather():
     # a bond listed in one direction only: the reference checks it from one side only
     xyz = np.array([[2 * j, 0, 0] for j in range(16)])
