@@ -81,30 +81,31 @@ def check_bytes_per_move(systems, p_chk, code_mode):
 
     Gather representation (code_mode 0): own xyz 12 B, per neighbour 4 B id + 12 B xyz, neighbour
     count 1 B, flag write 1 B, 9 occupancy bits, one temporary bit per tentative move.
-    Bond codes (code_mode 1: 4 B words, 2: 8 B words): packed coordinate 4 B + code word, 9
-    occupancy bits; per tentative move a 4 B mover-list entry and one temporary bit set; per
-    tentative move of the previous sub-step (the scrub, same rate) its list entry 4 B, its packed
-    coordinate 4 B and one temporary bit cleared."""
+    Bond codes (code_mode 1: 4 B words, 2: 8 B words): lattice address 4 B + code word, 9
+    occupancy bits; per tentative move a 4 B mover-list entry, its 4 B target address and one
+    temporary bit set."""
     n = sum(s.n for s in systems)
     kbar = sum(int(s.nbr_count.sum()) for s in systems) / n
     if code_mode == 0:
         return 12 + 16 * kbar + 1 + 1 + 9 / 8 + p_chk / 8, kbar
     w = 4 if code_mode == 1 else 8
-    return 4 + w + 9 / 8 + p_chk * (4 + 1 / 8) + p_chk * (8 + 1 / 8), kbar
+    return 4 + w + 9 / 8 + p_chk * (8 + 1 / 8), kbar
 
 
 def perform_bytes_per_move(kbar, p_chk, p_acc, code_mode):
     """Algorithmic bytes of one attempted move in the perform kernel (bond codes), which walks only
-    the mover lists: per tentative move its list entry 4 B, packed coordinate 4 B, code word, kbar
-    neighbour references (4 B) and 9 temporary-lattice bits; per accepted move 2 lattice bits read
-    and written, packed coordinate 4 B, one coordinate read+write 8 B, the list entry 4 B, own code
-    word and kbar neighbour code words read and written. Gather representation (code_mode 0):
-    flag 1 B, per tentative move xyz 12 B and 9 temporary bits, per accepted move 2 lattice bits
-    read and written, one coordinate 8 B, flag 1 B."""
+    the mover lists: per tentative move its list entry 4 B, its target address 4 B, its code word,
+    kbar neighbour references (4 B) and 9 temporary-lattice bits; per tentative move of the
+    previous sub-step (the scrub, same rate) its target address 4 B and one temporary bit
+    cleared; per accepted move 2 lattice bits read and written, the new lattice address 4 B, one
+    coordinate read+write 8 B, the own code word written and kbar neighbour code words read and
+    written. Gather representation (code_mode 0): flag 1 B, per tentative move xyz 12 B and 9
+    temporary bits, per accepted move 2 lattice bits read and written, one coordinate 8 B, flag
+    1 B."""
     if code_mode == 0:
         return 1 + p_chk * (12 + 9 / 8) + p_acc * (0.5 + 8 + 1)
     w = 4 if code_mode == 1 else 8
-    return p_chk * (8 + w + 4 * kbar + 9 / 8) + p_acc * (0.5 + 4 + 8 + 4 + w + 2 * w * kbar)
+    return p_chk * (8 + w + 4 * kbar + 9 / 8) + p_chk * (4 + 1 / 8) + p_acc * (0.5 + 4 + 8 + w + 2 * w * kbar)
 
 
 def measured_peaks():
