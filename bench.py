@@ -76,6 +76,10 @@ def workload_config(name, systems):
 
 # ------------------------------------------------------------------ algorithmic bytes (roofline)
 
+STEP_ENTRY_BYTES = 32          # one sub-step's draw entry (colour, seed, group), bfm_device.cuh StepEntry
+STATS_BYTES = 3 * 64 * 8       # the move counters: attempted / tentative / accepted in 64 slots each
+
+
 def check_bytes_per_move(systems, p_chk, code_mode):
     """Algorithmic bytes of one attempted move in the check kernel.
 
@@ -405,26 +409,26 @@ def run_ours(args):
         roofline["l2"] = {"frac": None if l2pct is None else round(l2pct / 100, 4),
                           "source": f"ncu lts__throughput.avg.pct_of_peak_sustained_elapsed, profiles/{key}.md"}
 
-    # e2e through the C-ABI with host buffers: per step one bfm_run (host draws uploaded from
-    # pinned memory) and a read of the step's counters; positions copied back at the end
-    import numpy as np
-    host_xyz = np.empty((systems[0].n, 3), dtype=np.int32)
+    # e2e through the C-ABI with host buffers: per step one run of 1 MCS (its sub-steps' draw
+    # entries uploaded from pinned memory) and a read of the move counters, which waits for the
+    # step; the positions, in the caller's order, copied back into a pinned host array at the end
+    host_xyz = torch.empty((systems[0].n, 3), dtype=torch.int32, pin_memory=True).numpy()
     torch.cuda.synchronize()
     t = time.perf_counter()
     for _ in range(args.steps):
         if batch is None:
-            u0.runSimulationOnGPU(1)
+            u0.run_async(1)
         else:
             batch.run(1)
         u0.stats()
     u0.get_coords(host_xyz)
     e2e_s = time.perf_counter() - t
-    nC0 = u0.n_colors()[0]
     e2e_value = world * moves / reduce_max(e2e_s, world)
     e2e = {"value": e2e_value, "unit": "attempted moves/s",
-           "h2d_bytes_per_step": 16 * sum(m.n_colors()[0] for m in members),
-           "d2h_bytes_per_step": 32 * (1 if batch is None else 1) + round(12 * systems[0].n / args.steps),
-           "calls": "bfm_run(1) + bfm_get_stats per step, bfm_get_coords_bulk once"}
+           "h2d_bytes_per_step": STEP_ENTRY_BYTES * sum(m.n_colors()[0] for m in members),
+           "d2h_bytes_per_step": STATS_BYTES + round(12 * systems[0].n / args.steps),
+           "calls": "bfm_run_async(1) + bfm_get_stats per step (the counter read waits for the step), "
+                    "bfm_get_coords_bulk once into pinned memory"}
 
     for m in members:
         m.validate()   # excluded volume, bonds and the device lattice after the timed run

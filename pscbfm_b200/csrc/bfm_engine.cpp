@@ -54,8 +54,8 @@ inline uint32_t host_brick_pos(uint32_t v, uint32_t a) { return brick_pos(v, a);
 
 }  // namespace
 
-ArenaLayout arena_layout(uint32_t npad, uint32_t maxc, uint32_t nwords, uint32_t ntab, uint32_t nColors,
-                         uint32_t maxGroup, uint32_t codeMode)
+ArenaLayout arena_layout(uint32_t n, uint32_t npad, uint32_t maxc, uint32_t nwords, uint32_t ntab,
+                         uint32_t nColors, uint32_t maxGroup, uint32_t codeMode)
 {
     ArenaLayout L{};
     size_t off = 0;
@@ -92,6 +92,9 @@ ArenaLayout arena_layout(uint32_t npad, uint32_t maxc, uint32_t nwords, uint32_t
     L.mlist = take(4ull * 2 * L.segs * kBcTileSpan);
     L.mword = take(4ull * 2 * L.segs * kBcTileSpan);
     L.mcount = take(4ull * 2 * L.segs);
+    // position read-back in the caller's order
+    L.slotOf = take(4ull * n);
+    L.xyzOut = take(12ull * n);
     L.bytes = off;
     return L;
 }
@@ -364,7 +367,7 @@ void Updater::initialize()
     std::vector<uint32_t> hnbrr;
 
     // one arena for every device array of this system
-    ArenaLayout const L = arena_layout(npad_, maxc_, nwords, (uint32_t)tab.size(), nC, maxGroup_, codeMode_);
+    ArenaLayout const L = arena_layout(n_, npad_, maxc_, nwords, (uint32_t)tab.size(), nC, maxGroup_, codeMode_);
     uint32_t const segs = L.segs;
     Device d;
     d.bytes = L.bytes;
@@ -402,6 +405,8 @@ void Updater::initialize()
     dev_.stepCap = kStepCap;
     dev_.dList = reinterpret_cast<uint32_t*>(base + L.list);
     dev_.gs = reinterpret_cast<GridSync*>(base + L.gs);
+    dev_.slotOf = reinterpret_cast<uint32_t*>(base + L.slotOf);
+    dev_.xyzOut = reinterpret_cast<int32_t*>(base + L.xyzOut);
     h.pk = reinterpret_cast<uint32_t*>(base + L.pk);
     h.code = base + L.code;
     h.nbrr = reinterpret_cast<uint32_t*>(base + L.nbrr);
@@ -454,6 +459,8 @@ void Updater::initialize()
                                cudaMemcpyHostToDevice, s), "upload brick table");
     cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(h.grp), hgrp.data(), 4ull * hgrp.size(),
                                cudaMemcpyHostToDevice, s), "upload groups");
+    if (n_) cuda_check(cudaMemcpyAsync(dev_.slotOf, oldToNew_.data(), 4ull * n_, cudaMemcpyHostToDevice, s),
+                       "upload slot order");
     cuda_check(cudaMemsetAsync(h.stats, 0, kStatBytes, s), "memset stats");
     cuda_check(cudaMemcpyAsync(dev_.dDesc, &h, sizeof(SysDev), cudaMemcpyHostToDevice, s), "upload descriptor");
     cuda_check(cudaMemsetAsync(dev_.dList, 0, 4, s), "memset list");
@@ -754,12 +761,14 @@ void Updater::ensureStaging()
     // pinned staging of the step entries, allocated on the first run of this system's own paths
     // (systems advanced only by a Batch never need it)
     if (hSteps_) return;
-    // one extra entry holds the copy of the persistent kernel's barrier state
+    // one extra entry holds the copy of the persistent kernel's barrier state, and after it the
+    // copy of the move counters
     static_assert(sizeof(GridSync) <= sizeof(StepEntry), "GridSync fits one staging entry");
-    cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * (kStepCap + 1)), "cudaMallocHost(steps)");
+    cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * (kStepCap + 1) + kStatBytes), "cudaMallocHost(steps)");
     hStepCap_ = kStepCap;
     hGs_ = reinterpret_cast<GridSync*>(hSteps_ + kStepCap);
     std::memset(hGs_, 0, sizeof(GridSync));
+    hStats_ = reinterpret_cast<unsigned long long*>(hSteps_ + kStepCap + 1);
 }
 
 void Updater::scrubPending(cudaStream_t s)
@@ -1039,20 +1048,19 @@ void Updater::synchronize()
 
 // ============================================================================ read back
 
+void Updater::downloadPositions(int32_t* out)
+{
+    // the device puts the positions into the caller's order; one copy brings them over
+    cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
+    cuda_check(launch_gather_positions(dev_.h, dev_.slotOf, n_, dev_.xyzOut, stream_), "gather positions");
+    cuda_check(cudaMemcpyAsync(out, dev_.xyzOut, 12ull * n_, cudaMemcpyDeviceToHost, stream_), "download positions");
+    synchronize();
+}
+
 void Updater::pullPositions()
 {
     if (!hostStale_ || !initialized()) return;
-    std::vector<int32_t> hx(npad_), hy(npad_), hz(npad_);
-    cuda_check(cudaMemcpyAsync(hx.data(), dev_.h.x, 4ull * npad_, cudaMemcpyDeviceToHost, stream_), "download x");
-    cuda_check(cudaMemcpyAsync(hy.data(), dev_.h.y, 4ull * npad_, cudaMemcpyDeviceToHost, stream_), "download y");
-    cuda_check(cudaMemcpyAsync(hz.data(), dev_.h.z, 4ull * npad_, cudaMemcpyDeviceToHost, stream_), "download z");
-    cuda_check(cudaStreamSynchronize(stream_), "download positions");
-    for (uint32_t i = 0; i < n_; ++i) {
-        uint32_t const s = oldToNew_[i];
-        xyz_[3 * (size_t)i] = hx[s];
-        xyz_[3 * (size_t)i + 1] = hy[s];
-        xyz_[3 * (size_t)i + 2] = hz[s];
-    }
+    if (n_) downloadPositions(xyz_.data());
     hostStale_ = false;
 }
 
@@ -1068,7 +1076,11 @@ void Updater::getCoordinates(int32_t* xyz, uint32_t n)
 {
     requireN("getCoordinates");
     if (n != n_) throw std::invalid_argument("[getCoordinates] wrong monomer count");
-    pullPositions();
+    if (hostStale_ && initialized()) {
+        // straight into the caller's buffer; the host copy stays stale until a getter needs it
+        if (n_) downloadPositions(xyz);
+        return;
+    }
     std::memcpy(xyz, xyz_.data(), sizeof(int32_t) * 3 * (size_t)n_);
 }
 
@@ -1126,7 +1138,10 @@ std::vector<uint32_t> Updater::groupSizes() const
 void Updater::stats(uint64_t out[4])
 {
     requireInit("stats");
-    unsigned long long slots[3 * kStatSlots];
+    // into the pinned staging where this system has it (a copy to pageable memory is staged by
+    // the driver and costs more per call)
+    unsigned long long local[3 * kStatSlots];
+    unsigned long long* const slots = hStats_ ? hStats_ : local;
     cuda_check(cudaMemcpyAsync(slots, dev_.h.stats, kStatBytes, cudaMemcpyDeviceToHost, stream_), "stats");
     cuda_check(cudaStreamSynchronize(stream_), "stats");
     for (uint32_t c = 0; c < 3; ++c) {
@@ -1231,6 +1246,7 @@ void Updater::freeDevice()
         cudaFreeHost(hSteps_);
         hSteps_ = nullptr;
         hGs_ = nullptr;
+        hStats_ = nullptr;
         gsPending_ = false;
         hStepCap_ = 0;
     }

@@ -33,12 +33,12 @@ std::vector<uint8_t> colour_bond_graph(uint32_t n, uint32_t const* cnt, uint32_t
 // job's device bytes with it before the job is coloured.
 struct ArenaLayout {
     size_t x, y, z, nbr, nnb, flags, mark, lat, tmp, tab, grp, stats, desc, steps, list, gs;
-    size_t pk, code, nbrr, plane, moveOk, dir, mlist, mword, mcount;
+    size_t pk, code, nbrr, plane, moveOk, dir, mlist, mword, mcount, slotOf, xyzOut;
     uint32_t segs;   // mover-list segments (tiles) per parity
     size_t bytes;
 };
-ArenaLayout arena_layout(uint32_t npad, uint32_t maxc, uint32_t nwords, uint32_t ntab, uint32_t nColors,
-                         uint32_t maxGroup, uint32_t codeMode);
+ArenaLayout arena_layout(uint32_t n, uint32_t npad, uint32_t maxc, uint32_t nwords, uint32_t ntab,
+                         uint32_t nColors, uint32_t maxGroup, uint32_t codeMode);
 // Bytes of the observables arena of a system (Updater::buildObservables).
 size_t observables_bytes(uint32_t npad, uint32_t nMol);
 
@@ -159,10 +159,13 @@ private:
         uint32_t stepCap = 0;
         uint32_t* dList = nullptr;     // resident kernel system list (one entry: 0)
         GridSync* gs = nullptr;        // grid barrier of the persistent kernel
+        uint32_t* slotOf = nullptr;    // [n] sorted slot of each monomer (caller's order)
+        int32_t* xyzOut = nullptr;     // [3 n] positions in the caller's order, for read-back
     };
     void requireN(char const* who) const;
     void requireInit(char const* who) const;
     void pullPositions();
+    void downloadPositions(int32_t* out);   // positions in the caller's order, x y z interleaved
     void enqueueLaunch(uint32_t nSteps);
     void enqueueGraph(uint32_t nSteps);
     void enqueueResident(uint32_t nSteps);
@@ -202,6 +205,7 @@ private:
     Device dev_;
     StepEntry* hSteps_ = nullptr;              // pinned staging for step entries
     GridSync* hGs_ = nullptr;                  // pinned copy of the persistent kernel's barrier state
+    unsigned long long* hStats_ = nullptr;     // pinned copy of the move counters (stats)
     bool gsPending_ = false;                   // hGs_ is being refreshed by the stream
     uint32_t hStepCap_ = 0;
     std::vector<std::pair<uint32_t, cudaGraphExec_t>> graphs_;   // captured chunk length -> graph

@@ -18,6 +18,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <cstdint>
 
 #include "bfm_device.cuh"
@@ -312,6 +314,22 @@ __global__ void k_build_lattice(SysDev const* __restrict__ sysv, uint32_t n)
     }
 }
 
+// ------------------------------------------------------------------------ position read-back
+
+// Positions in the caller's monomer order, x y z interleaved: out[3 i + a] is coordinate a of the
+// monomer in sorted slot slotOf[i]. One copy of out then gives the caller's array.
+__global__ void k_gather_positions(int32_t const* __restrict__ x, int32_t const* __restrict__ y,
+                                   int32_t const* __restrict__ z, uint32_t const* __restrict__ slotOf, uint32_t n,
+                                   int32_t* __restrict__ out)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t const g = slotOf[i];
+        out[3ull * i] = x[g];
+        out[3ull * i + 1] = y[g];
+        out[3ull * i + 2] = z[g];
+    }
+}
+
 // ------------------------------------------------------------------------ launchers
 
 cudaError_t launch_check(SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles, uint32_t tileSpan,
@@ -367,6 +385,16 @@ cudaError_t launch_resident(SysDev const* dSys, uint32_t const* dList, uint32_t 
     case 16: return launch_resident_k<16>(dSys, dList, nCta, dSteps, nSys, nSteps, smem, s);
     default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_gather_positions(SysDev const& h, uint32_t const* slotOf, uint32_t n, int32_t* out,
+                                    cudaStream_t s)
+{
+    uint32_t const block = 256;
+    uint32_t const grid = std::min((n + block - 1) / block, 148u * 8u);
+    if (grid == 0) return cudaSuccess;
+    k_gather_positions<<<grid, block, 0, s>>>(h.x, h.y, h.z, slotOf, n, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_build_lattice(SysDev const* dSys, uint32_t npad, cudaStream_t s)

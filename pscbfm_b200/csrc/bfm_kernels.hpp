@@ -77,5 +77,8 @@ cudaError_t launch_observables(SysDev const* dSys, ObsDev const& o, long long* d
 
 // Sets the occupancy bit of every non-padding slot of system dSys[0] (lat must be zeroed).
 cudaError_t launch_build_lattice(SysDev const* dSys, uint32_t npad, cudaStream_t s);
+// Positions in the caller's order, x y z interleaved (out[3 i + a] from sorted slot slotOf[i]).
+cudaError_t launch_gather_positions(SysDev const& h, uint32_t const* slotOf, uint32_t n, int32_t* out,
+                                    cudaStream_t s);
 
 }  // namespace bfm

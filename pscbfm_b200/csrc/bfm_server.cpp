@@ -70,7 +70,7 @@ size_t Server::estimateBytes(Updater const& setup)
     uint32_t const npad = std::max(n + 32u * nC, 32u);
     uint32_t const nwords = (uint32_t)(setup.boxVolume() / 64);
     uint32_t const ntab = (setup.boxSide(0) + setup.boxSide(1) + setup.boxSide(2)) / 4;
-    size_t const arena = arena_layout(npad, maxc, nwords, ntab, nC, std::max(n, 1u), kCode64).bytes;
+    size_t const arena = arena_layout(n, npad, maxc, nwords, ntab, nC, std::max(n, 1u), kCode64).bytes;
     size_t const obs = observables_bytes(npad, setup.countMolecules());
     size_t const steps = 2ull * sizeof(StepEntry) * kMaxChunkMcs * nC;
     return arena + obs + steps;
