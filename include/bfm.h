@@ -37,7 +37,9 @@ extern "C" {
 #define BFM_ERR_BUSY 7             /* server: result not ready yet */
 
 /* engine paths (bfm_set_mode) */
-#define BFM_MODE_AUTO 0     /* resident if the system fits one CTA, else graph */
+#define BFM_MODE_AUTO 0     /* resident for small systems (largest colour group <= 4096 and fits one CTA),
+                               persistent up to about three 512-monomer tiles per SM (bond codes),
+                               else graph */
 #define BFM_MODE_LAUNCH 1   /* check + perform launch per sub-step (the reference's structure) */
 #define BFM_MODE_GRAPH 2    /* the same launches captured into CUDA graphs */
 #define BFM_MODE_RESIDENT 3 /* one CTA per system, lattice in shared memory (box <= 64^3) */
@@ -105,6 +107,14 @@ int bfm_get_substep(bfm_handle h, uint64_t* substep);
 int bfm_set_draw_callback(bfm_handle h, bfm_draw_fn fn, void* ctx);
 /* Engine path, BFM_MODE_*. */
 int bfm_set_mode(bfm_handle h, int mode);
+/* The path the next run takes (after bfm_initialize): the mode set by bfm_set_mode with
+ * BFM_MODE_AUTO resolved, and a mode the system cannot use replaced by BFM_MODE_GRAPH. */
+int bfm_get_path(bfm_handle h, int* mode);
+/* Fault injection for tests (no counterpart in the reference): the next BFM_MODE_PERSISTENT launch
+ * of this handle starts its grid-barrier arrival count where no barrier can complete, so every
+ * CTA's wait runs out at its time limit (2 s) and the run reports the timeout (BFM_ERR_CUDA).
+ * Nothing faults on the GPU and the device stays usable; this system's state is not. */
+int bfm_inject_barrier_stall(bfm_handle h);
 /* Device representation of the bonds, chosen before bfm_initialize: BFM_REPR_AUTO (bond codes —
  * each monomer keeps the table indices of its bonds, updated exactly when it or a neighbour moves
  * — when every bond is listed in both directions and no monomer has more than 6; otherwise the

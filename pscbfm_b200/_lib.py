@@ -82,6 +82,8 @@ _SIGS = {
     "bfm_run": [H, C.c_int32],
     "bfm_run_async": [H, C.c_int32],
     "bfm_synchronize": [H],
+    "bfm_inject_barrier_stall": [H],
+    "bfm_get_path": [H, C.POINTER(C.c_int)],
     "bfm_get_coord": [H, C.c_uint32, C.c_int, C.POINTER(C.c_int32)],
     "bfm_get_coords_bulk": [H, _i32p, C.c_uint32],
     "bfm_n_colors": [H, C.POINTER(C.c_uint32), C.c_void_p, C.c_uint32],

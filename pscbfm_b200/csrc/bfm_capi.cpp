@@ -171,6 +171,14 @@ int bfm_get_representation(bfm_handle h, int* out)
 int bfm_initialize(bfm_handle h) { BFM_CALL(h, h->u.initialize()); }
 int bfm_run(bfm_handle h, int32_t n) { BFM_CALL(h, h->u.runSimulationOnGPU(n)); }
 int bfm_run_async(bfm_handle h, int32_t n) { BFM_CALL(h, h->u.run(n)); }
+int bfm_inject_barrier_stall(bfm_handle h) { BFM_CALL(h, h->u.injectBarrierStall()); }
+int bfm_get_path(bfm_handle h, int* mode)
+{
+    BFM_CALL(h, {
+        if (!mode) throw std::invalid_argument("[bfm_get_path] null output");
+        *mode = h->u.path();
+    });
+}
 int bfm_synchronize(bfm_handle h) { BFM_CALL(h, h->u.synchronize()); }
 int bfm_get_coord(bfm_handle h, uint32_t i, int axis, int32_t* out)
 {

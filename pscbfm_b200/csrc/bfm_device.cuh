@@ -78,12 +78,13 @@ struct SysDev {
     uint32_t forbid[16];             // bit i set <=> bond index i is forbidden
 };
 
-// Grid-wide barrier of the persistent sweep kernel; the host zeroes it before every launch.
+// Grid-wide barrier of the persistent sweep kernel: a count of arrivals that only grows during a
+// launch (the host zeroes it before every launch); barrier k of a launch completes when the count
+// reaches k x the grid size.
 struct GridSync {
-    unsigned int count;   // CTAs arrived at the current barrier
-    unsigned int gen;     // barriers completed
+    unsigned int count;   // arrivals so far in this launch
     unsigned int fault;   // set when a wait ran out; every CTA then leaves and the host reports it
-    unsigned int where;   // the barrier (generation) at which the first wait ran out
+    unsigned int where;   // the barrier (1, 2, ... within the launch) at which the first wait ran out
 };
 
 // Bond codes: field k (9 bits at 9k) of a monomer's code word is the bond index of

@@ -139,6 +139,9 @@ void Updater::setGpu(int gpu)
         stream_ = nullptr;
     }
     gpu_ = gpu;
+    int sms = 0;
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, gpu), "cudaDeviceGetAttribute");
+    smCount_ = (uint32_t)sms;
     if (!stream_) cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
 }
 
@@ -956,10 +959,31 @@ void Updater::enqueueResident(uint32_t nSteps)
     lastColor_ = kNoColor;   // the resident kernel leaves no marks in the global temporary lattices
 }
 
+int Updater::path() const
+{
+    requireInit("path");
+    return effectiveMode();
+}
+
+int Updater::autoMode() const
+{
+    // One system on a B200, per MCS: the resident kernel (one SM) is fastest while the largest
+    // colour group is at most 4 x 1024 monomers (8K-monomer chains: 13.7 us, persistent 15.5,
+    // graph 17.3); from there the persistent sweep, whose barriers cost less than the graph's
+    // launch gaps, while its tiles fit about three per SM (13K-262K monomers: 17-19 us against
+    // 19-22); beyond, the graph of separate launches (1M monomers: 30 us against 36).
+    if (residentEligible() && maxGroup_ <= 4u * kResidentBlock) return kModeResident;
+    if (codeMode_ != kCodeNone) {
+        uint32_t const tiles = (maxGroup_ + kBcTileSpan - 1) / kBcTileSpan;
+        if (tiles <= 3u * smCount_) return kModePersistent;
+    }
+    return kModeGraph;
+}
+
 int Updater::effectiveMode() const
 {
     int m = mode_;
-    if (m == kModeAuto) m = residentEligible() ? kModeResident : kModeGraph;
+    if (m == kModeAuto) m = autoMode();
     if (m == kModeResident && !residentEligible()) m = kModeGraph;
     if (m == kModePersistent && codeMode_ == kCodeNone) m = kModeGraph;   // bond codes only
     return m;
@@ -984,14 +1008,15 @@ void Updater::run(int32_t nMcs)
 }
 
 namespace {
-// monomers per thread and CTAs per SM of the persistent kernel (launch_sweep_bc); the environment
-// variable BFM_SWEEP_SHAPE overrides the default for tuning
+// CTAs per SM of the persistent kernel (launch_sweep_bc: 4, 5 or 6); 4, the default, is as fast
+// as the others up to a few hundred thousand monomers and faster above. The environment variable
+// BFM_SWEEP_SHAPE overrides it for tuning
 int sweep_shape()
 {
     static int const shape = [] {
         char const* e = std::getenv("BFM_SWEEP_SHAPE");
-        int const v = e ? std::atoi(e) : 1;
-        return (v >= 0 && v < kSweepShapes) ? v : 1;
+        int const v = e ? std::atoi(e) : 0;
+        return (v >= 0 && v < kSweepShapes) ? v : 0;
     }();
     return shape;
 }
@@ -1007,8 +1032,11 @@ void Updater::enqueuePersistent(uint32_t nSteps)
         cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
                    "steps H2D");
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
-        // count and generation restart at 0; the fault word stays set once a launch has failed
-        cuda_check(cudaMemsetAsync(dev_.gs, 0, 2 * sizeof(unsigned int), stream_), "clear grid barrier");
+        // the arrival count restarts at 0 (an injected stall starts it at 0x80808080, from where no
+        // barrier's target is reached); the fault word stays set once a launch has failed
+        cuda_check(cudaMemsetAsync(&dev_.gs->count, stallNext_ ? 0x80 : 0, sizeof(unsigned int), stream_),
+                   "clear grid barrier");
+        stallNext_ = false;
         uint32_t grid = 0;
         cuda_check(launch_sweep_bc(dev_.h, dev_.dSteps, chunk, maxGroup_, dev_.gs, codeMode_, sweep_shape(), stream_,
                                    &grid),

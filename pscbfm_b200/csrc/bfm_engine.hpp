@@ -145,6 +145,9 @@ public:
 
     // measurement
     float runTimed(int32_t nMcs);            // run + CUDA-event time on the handle's stream (ms)
+    // the next persistent launch starts its barrier count where no barrier completes (tests)
+    void injectBarrierStall() { stallNext_ = true; }
+    int path() const;                        // the path the next run takes (BFM_MODE_*)
     void timeKernels(int32_t nMcs, double out[4]);   // check ms, perform ms, launches of each
     uint64_t launches() const { return launches_; }  // kernels launched by this handle so far
     void addLaunches(uint64_t n) { launches_ += n; }
@@ -207,6 +210,8 @@ private:
     GridSync* hGs_ = nullptr;                  // pinned copy of the persistent kernel's barrier state
     unsigned long long* hStats_ = nullptr;     // pinned copy of the move counters (stats)
     bool gsPending_ = false;                   // hGs_ is being refreshed by the stream
+    bool stallNext_ = false;                   // injectBarrierStall
+    uint32_t smCount_ = 148;                   // SMs of the device (setGpu)
     uint32_t hStepCap_ = 0;
     std::vector<std::pair<uint32_t, cudaGraphExec_t>> graphs_;   // captured chunk length -> graph
     cudaEvent_t stepsFree_ = nullptr;          // host staging may be rewritten after this event
@@ -222,6 +227,7 @@ private:
     std::vector<uint32_t> moleculeRoots() const;   // lowest monomer id of each monomer's molecule
     cudaGraphExec_t graphFor(uint32_t nSteps);
     int effectiveMode() const;                // the path run() takes (mode_ with AUTO resolved)
+    int autoMode() const;                     // the path BFM_MODE_AUTO takes for this system
     void prepareGraphs(uint32_t nSteps);      // capture the graphs a graph-path run of nSteps replays
     void hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, std::vector<uint32_t>& nbrr) const;
 

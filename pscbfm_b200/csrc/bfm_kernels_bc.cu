@@ -399,41 +399,45 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 
+__device__ __forceinline__ void red_release_gpu_add(unsigned int* p, unsigned int v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // All CTAs of the cooperative grid meet; every write before the barrier is visible to every
-// thread after it. Thread 0 of each CTA arrives on a counter; the last arrival resets it and opens
-// the next generation; the others wait on the generation with a time limit. Returns false on every
-// thread of the CTA if its wait ran out or another CTA's did (GridSync::fault): the kernel then
-// leaves, and the host reports the fault.
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned int& gen, unsigned int* okSm)
+// thread after it. After the CTA barrier, thread 0 adds the CTA's arrival to a count that only
+// grows (a release add, which orders the whole CTA's earlier writes before it) and waits with
+// acquire loads until the count reaches this barrier's target, gridDim.x above the previous one.
+// Nothing is reset between barriers, and the signed difference keeps the comparison right
+// across a wrap of the count. The wait is bounded by time and by a poll count; on every thread
+// of the CTA it returns false if it ran out or another CTA's did (GridSync::fault): the kernel
+// then leaves, and the host reports the fault.
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned int& target, unsigned int* okSm)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned int ok = 1u;
-        unsigned int const g = gen;
-        __threadfence();
-        if (atomicAdd(&gs->count, 1u) == gridDim.x - 1u) {
-            atomicExch(&gs->count, 0u);
-            __threadfence();
-            atomicExch(&gs->gen, g + 1u);
-        } else {
+        target += gridDim.x;
+        red_release_gpu_add(&gs->count, 1u);
+        if (int(ld_acquire_gpu(&gs->count) - target) < 0) {
             unsigned long long const t0 = global_ns();
             unsigned int polls = 0u;
-            while (ld_acquire_gpu(&gs->gen) == g) {
-                if (ld_acquire_gpu(&gs->fault) != 0u) {
-                    ok = 0u;
-                    break;
-                }
+            while (int(ld_acquire_gpu(&gs->count) - target) < 0) {
                 // a time limit, and a poll count as a second bound that does not trust the timer
-                if (global_ns() - t0 > kBarrierTimeoutNs || ++polls > (1u << 26)) {
-                    if (atomicExch(&gs->fault, 1u) == 0u) gs->where = g;
-                    ok = 0u;
-                    break;
+                if ((++polls & 255u) == 0u) {
+                    if (ld_acquire_gpu(&gs->fault) != 0u) {
+                        ok = 0u;
+                        break;
+                    }
+                    if (global_ns() - t0 > kBarrierTimeoutNs || polls > (1u << 24)) {
+                        if (atomicExch(&gs->fault, 1u) == 0u) gs->where = target / gridDim.x;
+                        ok = 0u;
+                        break;
+                    }
                 }
-                __nanosleep(32);
+                __nanosleep(20);
             }
         }
-        __threadfence();
-        gen = g + 1u;
         *okSm = ok;
     }
     __syncthreads();
@@ -461,7 +465,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
     }
     __syncthreads();
     constexpr uint32_t span = kGridBlock * MPT;
-    unsigned int gen = 0u;
+    unsigned int target = 0u;   // this CTA's count target of the next barrier
     unsigned long long att = 0ull;
     StepEntry next = steps[0];
     for (uint32_t t = 0; t < nSteps; ++t) {
@@ -480,13 +484,13 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
             }
         }
         if (active) att += st.cnt;
-        if (!grid_barrier(gs, gen, &okSm)) return;
+        if (!grid_barrier(gs, target, &okSm)) return;
         uint32_t const reach = max(active ? st.cnt : 0u, st.pcnt);   // movers now, marks of t-1
         for (uint32_t k = blockIdx.x; k < nTiles; k += gridDim.x) {
             if (k * span >= reach) break;
             perform_body<W, MPT, false>(S, dtab, st, k, 1u, &tallyA, pre);
         }
-        if (t + 1 < nSteps && !grid_barrier(gs, gen, &okSm)) return;
+        if (t + 1 < nSteps && !grid_barrier(gs, target, &okSm)) return;
     }
     __syncthreads();
     if (threadIdx.x == 0) {

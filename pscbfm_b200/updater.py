@@ -216,6 +216,17 @@ class UpdaterGPUScBFM_AB_Type:
     def synchronize(self):
         self._call("bfm_synchronize")
 
+    def path(self) -> int:
+        """The engine path the next run takes (MODE_*): the set mode with MODE_AUTO resolved."""
+        v = C.c_int()
+        self._call("bfm_get_path", C.byref(v))
+        return v.value
+
+    def inject_barrier_stall(self):
+        """Tests: the next persistent launch's grid barrier cannot complete; the run reports the
+        timeout of its bounded wait (BfmCudaError) and the device stays usable."""
+        self._call("bfm_inject_barrier_stall")
+
     def n_colors(self):
         n = C.c_uint32()
         self._call("bfm_n_colors", C.byref(n), None, 0)

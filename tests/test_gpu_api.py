@@ -145,3 +145,52 @@ def test_lemonade_adapter_runs_like_the_oracle(tmp_path):
     s = S.from_bonds((32, 32, 32), np.array([[0, 0, 0], [2, 0, 0]]), [(0, 1)], seed=7)
     ref, _ = O.run(s, 100)
     assert np.array_equal(got, ref)
+
+
+def test_persistent_barrier_timeout_is_reported():
+    """A persistent launch whose grid barrier cannot complete (injected on the host: the arrival
+    count starts where no barrier's target is reached) ends at the barrier's time limit, the run
+    reports the timeout, and the device stays usable for the next system."""
+    import time
+    import numpy as np
+    from oracle import oracle as O
+    s = S.small_chains()
+    u = fresh()
+    u.load_system(s, mode=P.MODE_PERSISTENT)
+    u.inject_barrier_stall()
+    t = time.perf_counter()
+    with pytest.raises(P.BfmCudaError, match="timed out"):
+        u.runSimulationOnGPU(3)
+    assert time.perf_counter() - t < 60
+    u.close()
+    v = fresh()
+    v.load_system(s, mode=P.MODE_PERSISTENT)
+    v.runSimulationOnGPU(20)
+    want, _ = O.run(s, 20)
+    assert np.array_equal(v.get_coords(), want)
+    v.close()
+
+
+def test_auto_mode_picks_the_path_by_size():
+    """AUTO: resident for a small system that fits one CTA, the persistent sweep for mid-size
+    bond-code systems, the graph of launches for the 1M-monomer melt and for systems without bond
+    codes."""
+    import numpy as np
+    cases = [(S.small_chains(), P.MODE_RESIDENT), (S.crosslinked_network(), P.MODE_PERSISTENT),
+             (S.serpentine_chains(128, 64, 0.3, seed=3), P.MODE_PERSISTENT), (S.dense_melt(), P.MODE_GRAPH)]
+    for s, want in cases:
+        u = fresh()
+        u.load_system(s)
+        assert u.path() == want, s.name
+        u.close()
+    # a bond listed in one direction only: no bond codes, so no persistent sweep
+    xyz = np.array([[2 * j, 0, 0] for j in range(16)])
+    s = S.from_bonds((128, 128, 128), xyz, [(j, j + 1) for j in range(15)], seed=8)
+    s.nbr_count = s.nbr_count.copy()
+    s.nbr_count[5] = 1
+    u = fresh()
+    u.load_system(s)
+    assert u.representation() == 0 and u.path() == P.MODE_GRAPH
+    u.set_mode(P.MODE_PERSISTENT)
+    assert u.path() == P.MODE_GRAPH      # a mode the system cannot use falls back to the graph
+    u.close()
