@@ -92,7 +92,7 @@ void Batch::rebuild()
     auto gridGroup = [&](uint32_t mode) -> GridGroup& {
         for (auto& g : grid_)
             if (g.codeMode == mode) return g;
-        grid_.push_back(GridGroup{mode, {}, nullptr});
+        grid_.push_back(GridGroup{mode, {}, nullptr, {}});
         return grid_.back();
     };
     auto resGroup = [&](uint32_t mode) -> ResidentGroup& {
@@ -114,6 +114,7 @@ void Batch::rebuild()
             uint32_t const span = u->codeMode() == kCodeNone ? kGridBlock : kBcTileSpan;
             uint32_t const t = u->gridTiles();
             for (uint32_t k = 0; k < t; ++k) g.tiles.push_back(TileRef{m, k * span});
+            g.members.push_back(m);
         }
     }
     stepCap_ = kBatchChunk;
@@ -164,6 +165,22 @@ cudaError_t Batch::launchGrid(StepEntry const* e)
     SysDev const unused{};   // multi-system launches read each CTA's descriptor from dSys_
     for (auto const& g : grid_) {
         uint32_t const n = (uint32_t)g.tiles.size();
+        if (g.members.size() == 1) {
+            // a lone system runs the single-system kernels, as it would alone (descriptor as a launch
+            // parameter, several tiles per perform CTA): a long job left alone in a server lane
+            // then runs at its own speed
+            uint32_t const m = g.members[0];
+            Updater const& u = *members_[m];
+            cudaError_t err = g.codeMode == kCodeNone
+                                  ? launch_check(u.deviceDesc(), nullptr, n, kGridBlock, e + m, stream_)
+                                  : launch_check_bc(u.desc(), u.deviceDesc(), nullptr, n, e + m, g.codeMode, stream_, shape_);
+            if (err != cudaSuccess) return err;
+            err = g.codeMode == kCodeNone
+                      ? launch_perform(u.deviceDesc(), nullptr, n, kGridBlock, e + m, stream_)
+                      : launch_perform_bc(u.desc(), u.deviceDesc(), nullptr, n, e + m, g.codeMode, stream_, shape_);
+            if (err != cudaSuccess) return err;
+            continue;
+        }
         cudaError_t err = g.codeMode == kCodeNone
                               ? launch_check(dSys_, g.dTiles, n, kGridBlock, e, stream_)
                               : launch_check_bc(unused, dSys_, g.dTiles, n, e, g.codeMode, stream_, shape_);

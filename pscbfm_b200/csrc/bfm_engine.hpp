@@ -287,6 +287,7 @@ private:
         uint32_t codeMode;
         std::vector<TileRef> tiles;
         TileRef* dTiles = nullptr;
+        std::vector<uint32_t> members;   // batch indices of the group's systems
     };
     struct ResidentGroup {
         uint32_t codeMode;

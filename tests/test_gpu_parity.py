@@ -277,3 +277,26 @@ def test_single_monomer_and_ragged_groups():
             ref, _ = O.run(s, 120)
             got, _ = run_engine(s, [120], MODES[mode])
             assert np.array_equal(got, ref), (s.name, mode)
+
+
+def test_batch_lone_grid_members_vs_oracle():
+    """A grid group with a single system runs the single-system kernels inside the batch: the
+    network (bond codes) and an asymmetric chain (gather representation), each alone in its group
+    beside resident systems, for enough sub-steps that the batch's captured graph runs too; every
+    member equals the oracle."""
+    net = S.crosslinked_network()
+    xyz = np.array([[2 * j, 0, 0] for j in range(16)])
+    asym = S.from_bonds((128, 128, 128), xyz, [(j, j + 1) for j in range(15)], seed=8)
+    asym.nbr_count = asym.nbr_count.copy()
+    asym.nbr_count[5] = 1
+    small = [S.serpentine_chains(32, 16, 0.3, seed=40 + i) for i in range(3)]
+    systems = [net, asym] + small
+    members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
+    b = P.Batch(members)
+    b.run(70)
+    for s, m in zip(systems, members):
+        want, _ = O.run(s, 70)
+        assert np.array_equal(m.get_coords(), want), s.name
+        m.validate()
+    for m in members:
+        m.close()
