@@ -92,7 +92,7 @@ void Batch::rebuild()
     auto gridGroup = [&](uint32_t mode) -> GridGroup& {
         for (auto& g : grid_)
             if (g.codeMode == mode) return g;
-        grid_.push_back(GridGroup{mode, {}, nullptr, {}});
+        grid_.push_back(GridGroup{mode, {}, nullptr, {}, nullptr, {}});
         return grid_.back();
     };
     auto resGroup = [&](uint32_t mode) -> ResidentGroup& {
@@ -117,9 +117,10 @@ void Batch::rebuild()
             g.members.push_back(m);
         }
     }
+    for (auto& g : grid_) g.ptiles = g.codeMode == kCodeNone ? g.tiles : perform_tile_list(g.tiles);
     stepCap_ = kBatchChunk;
     size_t total = up256(sizeof(SysDev) * M) + up256(sizeof(StepEntry) * stepCap_ * M);
-    for (auto const& g : grid_) total += up256(sizeof(TileRef) * g.tiles.size());
+    for (auto const& g : grid_) total += up256(sizeof(TileRef) * g.tiles.size()) + up256(sizeof(TileRef) * g.ptiles.size());
     for (auto const& g : resident_) total += up256(sizeof(uint32_t) * g.members.size());
     if (total > arenaBytes_) {   // grows only: membership changes reuse the arena
         if (arena_) cuda_check(cudaFreeAsync(arena_, stream_), "cudaFreeAsync(batch)");
@@ -143,6 +144,11 @@ void Batch::rebuild()
         cuda_check(cudaMemcpyAsync(g.dTiles, g.tiles.data(), sizeof(TileRef) * g.tiles.size(), cudaMemcpyHostToDevice,
                                    stream_),
                    "upload tiles");
+        g.dPTiles = reinterpret_cast<TileRef*>(p);
+        p += up256(sizeof(TileRef) * g.ptiles.size());
+        cuda_check(cudaMemcpyAsync(g.dPTiles, g.ptiles.data(), sizeof(TileRef) * g.ptiles.size(),
+                                   cudaMemcpyHostToDevice, stream_),
+                   "upload perform tiles");
     }
     for (auto& g : resident_) {
         g.dList = reinterpret_cast<uint32_t*>(p);
@@ -185,8 +191,9 @@ cudaError_t Batch::launchGrid(StepEntry const* e)
                               ? launch_check(dSys_, g.dTiles, n, kGridBlock, e, stream_)
                               : launch_check_bc(unused, dSys_, g.dTiles, n, e, g.codeMode, stream_, shape_);
         if (err != cudaSuccess) return err;
-        err = g.codeMode == kCodeNone ? launch_perform(dSys_, g.dTiles, n, kGridBlock, e, stream_)
-                                      : launch_perform_bc(unused, dSys_, g.dTiles, n, e, g.codeMode, stream_, shape_);
+        err = g.codeMode == kCodeNone
+                  ? launch_perform(dSys_, g.dTiles, n, kGridBlock, e, stream_)
+                  : launch_perform_bc(unused, dSys_, g.dPTiles, (uint32_t)g.ptiles.size(), e, g.codeMode, stream_, shape_);
         if (err != cudaSuccess) return err;
     }
     return cudaSuccess;

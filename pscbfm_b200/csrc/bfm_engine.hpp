@@ -287,6 +287,8 @@ private:
         uint32_t codeMode;
         std::vector<TileRef> tiles;
         TileRef* dTiles = nullptr;
+        std::vector<TileRef> ptiles;     // the perform's list (bond codes: tiles grouped, perform_tile_list)
+        TileRef* dPTiles = nullptr;
         std::vector<uint32_t> members;   // batch indices of the group's systems
     };
     struct ResidentGroup {

@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include "bfm_device.cuh"
 
@@ -21,6 +22,7 @@ constexpr int32_t kPadCoord = INT32_MIN;      // x of an unused (padding) slot
 struct TileRef {
     uint32_t sys;
     uint32_t start;
+    uint32_t count = 1;   // consecutive tiles from start (bond-code perform lists group up to 4)
 };
 
 // dTiles == nullptr: single system 0, CTA b covers [b*tileSpan, (b+1)*tileSpan).
@@ -45,6 +47,9 @@ constexpr uint32_t kBcTileSpan = kGridBlock * kCheckMpt;
 // budget (CTAs per SM) of the two kernels, 0 .. kGridShapes-1; negative: the default. Every shape
 // gives the same results.
 constexpr int kGridShapes = 4;
+// The perform launch's tile list for a check tile list of bond-code systems: consecutive tiles of one
+// system grouped four to an entry when the list holds at least four tiles per SM.
+std::vector<TileRef> perform_tile_list(std::vector<TileRef> const& tiles);
 cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
                             StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1);
 cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,

@@ -351,7 +351,8 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_perform_bc(const __g
     __shared__ SysDev Sm;
     __shared__ __align__(16) uint32_t dtab[kDirTab];
     __shared__ uint32_t pre[2 * (kPerformTiles + 1)];
-    // one system: tilesPerCta (<= kPerformTiles) consecutive tiles per CTA; a tile list: one tile
+    // one system: tilesPerCta (<= kPerformTiles) consecutive tiles per CTA; a tile list: the
+    // entry's count (<= kPerformTiles) of one system's consecutive tiles
     uint32_t sys = 0, tile0 = blockIdx.x * tilesPerCta, nT = tilesPerCta;
     // one system: the direction table's load goes out with the step entry's
     uint32_t dv = (!kMulti && threadIdx.x < kDirTab) ? S1.dirTab[threadIdx.x] : 0u;
@@ -359,7 +360,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_perform_bc(const __g
         TileRef const tr = tiles[blockIdx.x];
         sys = tr.sys;
         tile0 = tr.start / kBcTileSpan;
-        nT = 1;
+        nT = min(tr.count, kPerformTiles);
     }
     StepEntry const st = steps[sys];
     // tiles holding this sub-step's movers or the previous sub-step's marks
@@ -716,6 +717,27 @@ cudaError_t launch_grid_bc(bool check, SysDev const& hostDesc, SysDev const* dSy
 }
 
 }  // namespace
+
+std::vector<TileRef> perform_tile_list(std::vector<TileRef> const& tiles)
+{
+    // the same rule as one system's launch: four consecutive tiles of a system per CTA when the
+    // launch has at least four tiles per SM
+    uint32_t const g = tiles.size() >= (size_t)kPerformTiles * (uint32_t)sm_count() ? kPerformTiles : 1u;
+    std::vector<TileRef> out;
+    for (size_t i = 0; i < tiles.size();) {
+        TileRef t = tiles[i];
+        t.count = 1;
+        size_t k = i + 1;
+        while (k < tiles.size() && t.count < g && tiles[k].sys == t.sys &&
+               tiles[k].start == t.start + t.count * kBcTileSpan) {
+            ++t.count;
+            ++k;
+        }
+        out.push_back(t);
+        i = k;
+    }
+    return out;
+}
 
 cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
                             StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape)
