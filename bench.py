@@ -268,6 +268,10 @@ def cpu_replicas(kind, workload, steps, warmup, cores=0):
     return rate, cores, res[0][2]
 
 
+def cpu_per_core(rate, cores):
+    return rate / max(cores, 1)
+
+
 # ------------------------------------------------------------------ main arm
 
 def dist_setup(args):
@@ -335,6 +339,8 @@ def run_ours(args):
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
     members = [P.UpdaterGPUScBFM_AB_Type(local).load_system(s) for s in systems]
+    colours = [m.n_colors()[0] for m in members]
+    config = dict(config, colours=colours[0] if len(colours) == 1 else f"{min(colours)}-{max(colours)} per system")
     batch = P.Batch(members, gpu=local) if len(members) > 1 else None
     u0 = members[0]
 
@@ -425,7 +431,7 @@ def run_ours(args):
     e2e_s = time.perf_counter() - t
     e2e_value = world * moves / reduce_max(e2e_s, world)
     e2e = {"value": e2e_value, "unit": "attempted moves/s",
-           "h2d_bytes_per_step": STEP_ENTRY_BYTES * sum(m.n_colors()[0] for m in members),
+           "h2d_bytes_per_step": STEP_ENTRY_BYTES * sum(colours),
            "d2h_bytes_per_step": STATS_BYTES + round(12 * systems[0].n / args.steps),
            "calls": "bfm_run_async(1) + bfm_get_stats per step (the counter read waits for the step), "
                     "bfm_get_coords_bulk once into pinned memory"}
@@ -446,7 +452,8 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, _ = cpu_replicas("sequential", args.workload, steps=3 if n_total > 100000 else 40, warmup=1,
                                       cores=args.cpu_cores)
-        cpu = {"value": rate, "unit": "attempted moves/s", "cores": cores, "kind": "port",
+        cpu = {"value": rate, "unit": "attempted moves/s", "cores": cores, "per_core": cpu_per_core(rate, cores),
+               "kind": "port",
                "sample": ("random-sequential single-monomer BFM (LeMonADE serial-updater scheme), one replica of "
                           "the workload system per core, " + ("3" if n_total > 100000 else "40") + " MCS each")}
     launches_total = reduce_sum(float(launches), world)
@@ -458,6 +465,9 @@ def run_ours(args):
                 "config": dict(config, l2="flushed (256 MiB write) before every timed step",
                                path="auto" if batch is None else "batch", parallelism=f"replicas x{world}"),
                 "value_warm_l2": value_warm, "p_chk": p_chk, "p_acc": p_acc,
+                "moves_timed": {"attempted": attempted, "tentative": tentative, "accepted": accepted,
+                                "sub_steps": args.steps * sum(colours)},
+                "l2_cache_bytes": torch.cuda.get_device_properties(local).L2_cache_size,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches_total),
                 "clocks": clocks}
         line.update(extras)
@@ -586,8 +596,8 @@ def run_reference(args):
     line = {"impl": "reference", "metric": "attempted monomer moves/s", "value": rate, "unit": "attempted moves/s",
             "n_gpus": args.gpus, "steps": steps, "warmup": 1, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic", "config": config,
-            "cpu_baseline": {"value": rate, "unit": "attempted moves/s", "cores": cores, "kind": "port",
-                             "sample": sample},
+            "cpu_baseline": {"value": rate, "unit": "attempted moves/s", "cores": cores,
+                             "per_core": cpu_per_core(rate, cores), "kind": "port", "sample": sample},
             "e2e": {"value": rate, "unit": "attempted moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
