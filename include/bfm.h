@@ -111,7 +111,8 @@ int bfm_set_mode(bfm_handle h, int mode);
  * BFM_MODE_AUTO resolved, and a mode the system cannot use replaced by BFM_MODE_GRAPH. */
 int bfm_get_path(bfm_handle h, int* mode);
 /* Fault injection for tests (no counterpart in the reference): the next BFM_MODE_PERSISTENT launch
- * of this handle starts its grid-barrier arrival count where no barrier can complete, so every
+ * of this handle runs as a cooperative grid (never as one cluster, whose barriers are in hardware)
+ * and starts its grid-barrier arrival count where no barrier can complete, so every
  * CTA's wait runs out at its time limit (2 s) and the run reports the timeout (BFM_ERR_CUDA).
  * Nothing faults on the GPU and the device stays usable; this system's state is not. */
 int bfm_inject_barrier_stall(bfm_handle h);

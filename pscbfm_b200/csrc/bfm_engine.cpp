@@ -1036,10 +1036,12 @@ void Updater::enqueuePersistent(uint32_t nSteps)
         // barrier's target is reached); the fault word stays set once a launch has failed
         cuda_check(cudaMemsetAsync(&dev_.gs->count, stallNext_ ? 0x80 : 0, sizeof(unsigned int), stream_),
                    "clear grid barrier");
+        // an injected stall tests the grid barrier in global memory, so that launch is cooperative
+        bool const allowCluster = !stallNext_;
         stallNext_ = false;
         uint32_t grid = 0;
-        cuda_check(launch_sweep_bc(dev_.h, dev_.dSteps, chunk, maxGroup_, dev_.gs, codeMode_, sweep_shape(), stream_,
-                                   &grid),
+        cuda_check(launch_sweep_bc(dev_.h, dev_.dSteps, chunk, maxGroup_, dev_.gs, codeMode_, sweep_shape(),
+                                   allowCluster, stream_, &grid),
                    "persistent sweep");
         ++launches_;
         done += chunk;

@@ -54,14 +54,17 @@ cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef 
                             StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1);
 cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
                               StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1);
-// Persistent sweep (bond codes, one system): nSteps sub-steps of check, grid barrier, perform in
-// one cooperative launch of at most the co-resident CTA count. gs must be zeroed before the launch;
-// after it, gs->fault != 0 means a barrier wait ran out and the system's state is not usable.
-// shape selects the CTAs per SM the register budget must fit: 0 -> 4, 1 -> 5, 2 -> 6 (two monomers
-// per thread, one mover-list segment per tile).
+// Persistent sweep (bond codes, one system): nSteps sub-steps of check, barrier, perform in one
+// launch of at most the co-resident CTA count: a grid of at most 16 CTAs as one thread-block
+// cluster (hardware barriers) where allowCluster and the device can run it, otherwise a
+// cooperative launch with grid barriers in global memory. gs->count must be zeroed before the
+// launch; after it, gs->fault != 0 means a grid-barrier wait ran out and the system's state is not
+// usable. shape selects the CTAs per SM the register budget must fit: 0 -> 4, 1 -> 5, 2 -> 6 (two
+// monomers per thread, one mover-list segment per tile).
 constexpr int kSweepShapes = 3;
 cudaError_t launch_sweep_bc(SysDev const& hostDesc, StepEntry const* dSteps, uint32_t nSteps, uint32_t maxGroup,
-                            GridSync* gs, uint32_t codeMode, int shape, cudaStream_t s, uint32_t* gridOut);
+                            GridSync* gs, uint32_t codeMode, int shape, bool allowCluster, cudaStream_t s,
+                            uint32_t* gridOut);
 size_t resident_bc_smem_bytes(uint32_t nwords, uint32_t npad, uint32_t maxGroup, uint32_t codeMode);
 cudaError_t launch_resident_bc(SysDev const* dSys, uint32_t const* dList, uint32_t nCta, uint32_t perThread,
                                StepEntry const* dSteps, uint32_t nSys, uint32_t nSteps, size_t smem, uint32_t codeMode,

@@ -1,20 +1,22 @@
 // Bond-code kernels of the BFM sweep (sm_100a).
 //
 // The same sub-step as the gather kernels (check: CRITICAL.cu:298-374, perform + apply:
-// CRITICAL.cu:376-411, clear: :561-573), on a different state: each monomer keeps its packed
-// lattice coordinates (pk) and a bond-code word whose 9-bit fields are the reference's bond-table
+// CRITICAL.cu:376-411, clear: :561-573), on a different state: each monomer keeps the lattice
+// address of its corner (pk: brick word << 6 | bit; moves and front planes are adds confined to one
+// axis's address bits) and a bond-code word whose 9-bit fields are the reference's bond-table
 // indices of its bonds, so the check needs no neighbour positions. When a monomer moves by d, its
 // own fields change by -d and the reverse field of every neighbour by +d; the reverse field's old
 // value is the negation (mod 8) of the monomer's own field, so the update needs no extra load.
 //
 // Grid phase (k_check_bc, k_perform_bc): the check lists its tentative movers per tile, with the
-// temporary-lattice word each one marked (mover lists, double-buffered by sub-step parity); the
-// perform walks only those lists, and the perform of sub-step t also zeroes the words listed at
-// t-1. Every independent load of a pass is issued before any dependent one; a single-system
+// address of the temporary-lattice cell each one marked (mover lists, double-buffered by sub-step
+// parity); the perform walks only those lists, and the perform of sub-step t also zeroes the words
+// listed at t-1. Every independent load of a pass is issued before any dependent one; a single-system
 // launch takes the descriptor as a grid-constant parameter.
 //
-// Persistent (k_sweep_bc): the same bodies for a whole run of sub-steps in one cooperative launch,
-// with time-bounded grid barriers between the phases.
+// Persistent (k_sweep_bc): the same bodies for a whole run of sub-steps in one launch: a grid of
+// at most 16 CTAs as one thread-block cluster with hardware barriers between the phases, a larger
+// one as a cooperative launch with time-bounded grid barriers.
 //
 // Resident (k_resident_bc): one CTA owns a small system for a chunk of sub-steps; lattice, one
 // temporary lattice, pk and bond codes in shared memory; the check appends tentative movers to a
@@ -445,12 +447,20 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned int& target,
     return *okSm != 0u;
 }
 
+// The whole grid as one thread-block cluster: the hardware cluster barrier, with release and
+// acquire semantics at cluster scope, orders every thread's earlier global writes before any
+// thread's later reads. Every CTA of the sweep reaches the same sequence of barriers.
+__device__ __forceinline__ void cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 // One system, a whole run of sub-steps in one cooperative launch: per sub-step the check phase
 // over every tile, a grid barrier, the perform phase and (between sub-steps) another barrier. CTA b
 // takes tiles b, b + gridDim.x, ... of kGridBlock * MPT in-colour indices. Same bodies as
 // k_check_bc / k_perform_bc, with plain loads of the state other CTAs change during the launch;
 // the step entries are prefetched one sub-step ahead and the move counters flushed once.
-template <typename W, int MPT, int kMinBlocks>
+template <typename W, int MPT, int kMinBlocks, bool kCluster>
 __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
     k_sweep_bc(const __grid_constant__ SysDev S, StepEntry const* __restrict__ steps, uint32_t nSteps,
                uint32_t nTiles, GridSync* gs)
@@ -485,13 +495,17 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
             }
         }
         if (active) att += st.cnt;
-        if (!grid_barrier(gs, target, &okSm)) return;
+        if constexpr (kCluster) cluster_barrier();
+        else if (!grid_barrier(gs, target, &okSm)) return;
         uint32_t const reach = max(active ? st.cnt : 0u, st.pcnt);   // movers now, marks of t-1
         for (uint32_t k = blockIdx.x; k < nTiles; k += gridDim.x) {
             if (k * span >= reach) break;
             perform_body<W, MPT, false>(S, dtab, st, k, 1u, &tallyA, pre);
         }
-        if (t + 1 < nSteps && !grid_barrier(gs, target, &okSm)) return;
+        if (t + 1 < nSteps) {
+            if constexpr (kCluster) cluster_barrier();
+            else if (!grid_barrier(gs, target, &okSm)) return;
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -761,17 +775,23 @@ cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRe
 
 namespace {
 
+// A sweep grid of at most this many CTAs runs as one cluster (a non-portable size above 8)
+constexpr uint32_t kMaxSweepCluster = 16;
+
 template <typename W, int MPT, int kMinBlocks>
 cudaError_t launch_sweep_bc_k(SysDev const& S, StepEntry const* dSteps, uint32_t nSteps, uint32_t maxGroup,
-                              GridSync* gs, cudaStream_t s, uint32_t* gridOut)
+                              GridSync* gs, bool allowCluster, cudaStream_t s, uint32_t* gridOut)
 {
-    // co-resident CTAs per SM and SM count, once per device and instantiation
+    // co-resident CTAs per SM and SM count, once per device and instantiation; which cluster sizes
+    // can run, once per device, instantiation and size
     static thread_local int occ[64] = {}, nsm[64] = {};
+    static thread_local signed char clusterOk[64][kMaxSweepCluster + 1] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (!occ[dev & 63]) {
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[dev & 63], k_sweep_bc<W, MPT, kMinBlocks>, kGridBlock, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[dev & 63], k_sweep_bc<W, MPT, kMinBlocks, false>,
+                                                          kGridBlock, 0);
         if (e != cudaSuccess) return e;
         e = cudaDeviceGetAttribute(&nsm[dev & 63], cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
@@ -780,21 +800,46 @@ cudaError_t launch_sweep_bc_k(SysDev const& S, StepEntry const* dSteps, uint32_t
     uint32_t nTiles = (maxGroup + kGridBlock * MPT - 1) / (kGridBlock * MPT);
     if (nTiles == 0) nTiles = 1;
     uint32_t const grid = std::min<uint32_t>(nTiles, (uint32_t)(occ[dev & 63] * nsm[dev & 63]));
-    void* args[] = {const_cast<SysDev*>(&S), &dSteps, &nSteps, &nTiles, &gs};
-    e = cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(k_sweep_bc<W, MPT, kMinBlocks>), dim3(grid),
-                                    dim3(kGridBlock), args, 0, s);
     if (gridOut) *gridOut = grid;
-    return e;
+    void* args[] = {const_cast<SysDev*>(&S), &dSteps, &nSteps, &nTiles, &gs};
+    if (allowCluster && grid <= kMaxSweepCluster) {
+        // the whole grid as one cluster, its barriers in hardware, where the device can run it
+        auto kernel = k_sweep_bc<W, MPT, kMinBlocks, true>;
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = grid;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(kGridBlock);
+        cfg.stream = s;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        signed char& ok = clusterOk[dev & 63][grid];
+        if (ok == 0) {
+            ok = -1;
+            if (grid <= 8 || cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+                                 cudaSuccess) {
+                int clusters = 0;
+                if (cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg) == cudaSuccess && clusters >= 1) ok = 1;
+            }
+            cudaGetLastError();   // a size the device refuses is not an error of this call
+        }
+        if (ok == 1) return cudaLaunchKernelExC(&cfg, reinterpret_cast<void const*>(kernel), args);
+    }
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(k_sweep_bc<W, MPT, kMinBlocks, false>),
+                                       dim3(grid), dim3(kGridBlock), args, 0, s);
 }
 
 template <typename W>
 cudaError_t launch_sweep_bc_w(SysDev const& S, StepEntry const* dSteps, uint32_t nSteps, uint32_t maxGroup,
-                              GridSync* gs, int shape, cudaStream_t s, uint32_t* gridOut)
+                              GridSync* gs, bool allowCluster, int shape, cudaStream_t s, uint32_t* gridOut)
 {
     switch (shape) {
-    case 0: return launch_sweep_bc_k<W, kCheckMpt, 4>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
-    case 1: return launch_sweep_bc_k<W, kCheckMpt, 5>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
-    case 2: return launch_sweep_bc_k<W, kCheckMpt, 6>(S, dSteps, nSteps, maxGroup, gs, s, gridOut);
+    case 0: return launch_sweep_bc_k<W, kCheckMpt, 4>(S, dSteps, nSteps, maxGroup, gs, allowCluster, s, gridOut);
+    case 1: return launch_sweep_bc_k<W, kCheckMpt, 5>(S, dSteps, nSteps, maxGroup, gs, allowCluster, s, gridOut);
+    case 2: return launch_sweep_bc_k<W, kCheckMpt, 6>(S, dSteps, nSteps, maxGroup, gs, allowCluster, s, gridOut);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -802,13 +847,15 @@ cudaError_t launch_sweep_bc_w(SysDev const& S, StepEntry const* dSteps, uint32_t
 }  // namespace
 
 cudaError_t launch_sweep_bc(SysDev const& hostDesc, StepEntry const* dSteps, uint32_t nSteps, uint32_t maxGroup,
-                            GridSync* gs, uint32_t codeMode, int shape, cudaStream_t s, uint32_t* gridOut)
+                            GridSync* gs, uint32_t codeMode, int shape, bool allowCluster, cudaStream_t s,
+                            uint32_t* gridOut)
 {
     if (nSteps == 0) return cudaSuccess;
     if (codeMode == kCode32)
-        return launch_sweep_bc_w<uint32_t>(hostDesc, dSteps, nSteps, maxGroup, gs, shape, s, gridOut);
+        return launch_sweep_bc_w<uint32_t>(hostDesc, dSteps, nSteps, maxGroup, gs, allowCluster, shape, s, gridOut);
     if (codeMode == kCode64)
-        return launch_sweep_bc_w<unsigned long long>(hostDesc, dSteps, nSteps, maxGroup, gs, shape, s, gridOut);
+        return launch_sweep_bc_w<unsigned long long>(hostDesc, dSteps, nSteps, maxGroup, gs, allowCluster, shape, s,
+                                                     gridOut);
     return cudaErrorInvalidValue;
 }
 
