@@ -57,9 +57,9 @@ struct SysDev {
     unsigned long long* tmp;         // [2][nwords]
     uint32_t const* brickTab;        // [nb0 + nb1 + nb2]
     uint32_t const* grp;             // [2 * nColors]: offset, size
-    unsigned long long* stats;       // [4]: attempted, tentative, accepted, spare
+    unsigned long long* stats;       // [3][kStatSlots]: attempted, tentative, accepted (striped)
     // bond-code representation (codeMode != kCodeNone)
-    uint32_t* pk;                    // [npad] packed lattice coordinates x | y << 10 | z << 20 (masked)
+    uint32_t* pk;                    // [npad] lattice address of the corner: brick word << 6 | bit (lattice_address)
     void* code;                      // [npad] uint32 (3 slots) or uint64 (6 slots) bond codes
     uint32_t const* nbrr;            // [maxc][npad] neighbour slot | reverse slot << 28
     unsigned long long const* planeTab;   // [3][64][4] front-plane masks (see plane_table_fill)
@@ -308,6 +308,7 @@ inline void dir_table_fill(uint32_t const nb[3], uint32_t const* tab, uint32_t c
 struct Plane {
     uint32_t w[4];
     unsigned long long m[4];
+    uint32_t touch;   // bit k set <=> brick k is touched (m[k] != 0), from the address alone
 };
 
 // Per-direction parameters of the lattice-address arithmetic (dir_table_fill); the kernels read
@@ -369,6 +370,11 @@ __host__ __device__ __forceinline__ void front_plane(Plane& pl, unsigned long lo
     pl.m[2] = m23.x;
     pl.w[3] = addr_add(w10, D.bv, 1u);
     pl.m[3] = m23.y;
+    // the run of three cells along u (v) spills into the next brick when it starts at in-brick
+    // coordinate 2 or 3, i.e. when the high in-brick bit of that axis (one of bits 1, 3, 5) is set;
+    // loads predicated on this need not wait for the masks
+    uint32_t const tu = (f & D.mu & 0x2Au) != 0u, tv = (f & D.mv & 0x2Au) != 0u;
+    pl.touch = 1u | (tv << 1) | (tu << 2) | ((tu & tv) << 3);
 }
 
 // Host: bit d of ok[idx] is set when the bond with table index idx (neighbour - monomer, every

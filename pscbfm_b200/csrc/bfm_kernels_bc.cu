@@ -129,7 +129,7 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
         hit[q] = 0ull;
 #pragma unroll
         for (int r = 0; r < 4; ++r)
-            if (ok[q] && pl[q].m[r]) hit[q] |= ldm<kNc>(S.lat + pl[q].w[r]) & pl[q].m[r];
+            if (ok[q] && ((pl[q].touch >> r) & 1u)) hit[q] |= ldm<kNc>(S.lat + pl[q].w[r]) & pl[q].m[r];
     }
     // stage 4: decisions; tentative movers go to this tile's list segment (one shared-memory
     // atomic per warp reserves the warp's slots)
@@ -203,7 +203,7 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
         hit[q] = 0ull;
 #pragma unroll
         for (int r = 0; r < 4; ++r)
-            if (live[q] && pl[q].m[r]) hit[q] |= ldm<kNc>(tcur + pl[q].w[r]) & pl[q].m[r];
+            if (live[q] && ((pl[q].touch >> r) & 1u)) hit[q] |= ldm<kNc>(tcur + pl[q].w[r]) & pl[q].m[r];
     }
     uint32_t nAcc = 0;
 #pragma unroll
@@ -579,7 +579,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
                     unsigned long long hit = 0ull;
 #pragma unroll
                     for (int r = 0; r < 4; ++r)
-                        if (pl.m[r]) hit |= lat[pl.w[r]] & pl.m[r];
+                        if (pl.m[r]) hit |= lat[pl.w[r]] & pl.m[r];   // masks from shared memory
                     if (hit == 0ull) {
                         uint32_t const to = addr_add(p, D.ma, D.step);
                         atomicOr(tmp + (to >> 6), 1ull << (to & 63u));

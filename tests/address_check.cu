@@ -73,6 +73,13 @@ int check_box(uint32_t const box[3])
                         std::printf("step back: box %u %u %u at %u %u %u dir %u\n", box[0], box[1], box[2], x, y, z, d);
                         return 1;
                     }
+                    for (int r = 0; r < 4; ++r)
+                        if (((pl.touch >> r) & 1u) != (pl.m[r] != 0ull ? 1u : 0u) ||
+                            ((pt.touch >> r) & 1u) != (pt.m[r] != 0ull ? 1u : 0u)) {
+                            std::printf("touched bricks: box %u %u %u at %u %u %u dir %u\n", box[0], box[1], box[2], x,
+                                        y, z, d);
+                            return 1;
+                        }
                     std::set<std::pair<uint32_t, uint32_t>> got, want;
                     for (int r = 0; r < 4; ++r)
                         for (uint32_t b = 0; b < 64; ++b)
