@@ -38,13 +38,17 @@ extern "C" {
 
 /* engine paths (bfm_set_mode) */
 #define BFM_MODE_AUTO 0     /* resident for small systems (largest colour group <= 4096 and fits one CTA),
-                               persistent up to about three 512-monomer tiles per SM (bond codes),
-                               else graph */
+                               cluster where a cluster's shared memory holds the system at <= 2
+                               chunks of 32 slots per warp, persistent up to about three 512-monomer
+                               tiles per SM (bond codes), else graph */
 #define BFM_MODE_LAUNCH 1   /* check + perform launch per sub-step (the reference's structure) */
 #define BFM_MODE_GRAPH 2    /* the same launches captured into CUDA graphs */
 #define BFM_MODE_RESIDENT 3 /* one CTA per system, lattice in shared memory (box <= 64^3) */
 #define BFM_MODE_PERSISTENT 4 /* bond codes: one cooperative launch runs a whole chunk of sub-steps,
                                  grid barriers between the phases (gather systems use GRAPH) */
+#define BFM_MODE_CLUSTER 5    /* bond codes: one thread-block cluster (2-16 CTAs) holds the system's
+                                 lattice and state in its shared memory for a whole chunk of
+                                 sub-steps (systems too large for one CTA, up to about 200 KB x 16) */
 
 typedef struct bfm_updater* bfm_handle;
 typedef struct bfm_batch* bfm_batch_handle;

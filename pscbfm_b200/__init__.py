@@ -6,6 +6,6 @@ its Python host binding (updater.py), the synthetic systems it is measured on (s
 the build script (build.py).
 """
 from .updater import UpdaterGPUScBFM_AB_Type, Batch, MODE_AUTO, MODE_LAUNCH, MODE_GRAPH, MODE_RESIDENT  # noqa: F401
-from .updater import MODE_PERSISTENT  # noqa: F401
+from .updater import MODE_PERSISTENT, MODE_CLUSTER  # noqa: F401
 from .updater import REPR_AUTO, REPR_GATHER, Server  # noqa: F401
 from ._lib import BfmCudaError, BfmBudgetError, BfmBusy  # noqa: F401

@@ -20,7 +20,7 @@ BFM_ERR_NULL_HANDLE = 5
 BFM_ERR_BUDGET = 6
 BFM_ERR_BUSY = 7
 
-MODE_AUTO, MODE_LAUNCH, MODE_GRAPH, MODE_RESIDENT, MODE_PERSISTENT = 0, 1, 2, 3, 4
+MODE_AUTO, MODE_LAUNCH, MODE_GRAPH, MODE_RESIDENT, MODE_PERSISTENT, MODE_CLUSTER = 0, 1, 2, 3, 4, 5
 
 DRAW_FN = C.CFUNCTYPE(C.c_uint32, C.c_void_p)
 
@@ -87,7 +87,7 @@ _SIGS = {
     "bfm_get_coord": [H, C.c_uint32, C.c_int, C.POINTER(C.c_int32)],
     "bfm_get_coords_bulk": [H, _i32p, C.c_uint32],
     "bfm_n_colors": [H, C.POINTER(C.c_uint32), C.c_void_p, C.c_uint32],
-    "bfm_get_stats": [H, _u64p],
+    "bfm_get_stats": [H, C.POINTER(C.c_uint64)],   # a ctypes buffer: read once per step by callers
     "bfm_validate": [H],
     "bfm_device_bytes": [H, C.POINTER(C.c_uint64)],
     "bfm_run_timed": [H, C.c_int32, C.POINTER(C.c_float)],

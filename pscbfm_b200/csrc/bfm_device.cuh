@@ -311,6 +311,36 @@ struct Plane {
     uint32_t touch;   // bit k set <=> brick k is touched (m[k] != 0), from the address alone
 };
 
+// Cluster-resident layout (k_cluster_bc): a system held in the shared memory of a cluster of
+// 2^logC CTAs. Lattice word w (occupancy and temporary) lives in CTA w mod 2^logC at local word
+// w >> logC. Slots are dealt out in chunks of 32 (a colour group starts at a multiple of 32): slot
+// g lives in CTA (g / 32) mod 2^logC, at local index (g / (32 * 2^logC)) * 32 + g mod 32, so every
+// colour group spreads evenly over the CTAs and a CTA checks exactly the slots it holds.
+__host__ __device__ __forceinline__ uint32_t cluster_word_rank(uint32_t w, uint32_t logC)
+{
+    return w & ((1u << logC) - 1u);
+}
+__host__ __device__ __forceinline__ uint32_t cluster_word_local(uint32_t w, uint32_t logC) { return w >> logC; }
+__host__ __device__ __forceinline__ uint32_t cluster_slot_rank(uint32_t g, uint32_t logC)
+{
+    return (g >> 5) & ((1u << logC) - 1u);
+}
+__host__ __device__ __forceinline__ uint32_t cluster_slot_local(uint32_t g, uint32_t logC)
+{
+    return ((g >> (5u + logC)) << 5) | (g & 31u);
+}
+// the slot held at local index l of CTA r (inverse of the two above)
+__host__ __device__ __forceinline__ uint32_t cluster_slot_of(uint32_t l, uint32_t r, uint32_t logC)
+{
+    return ((((l >> 5) << logC) | r) << 5) | (l & 31u);
+}
+// local slot capacity of each CTA for npad slots (npad a multiple of 32)
+__host__ __device__ __forceinline__ uint32_t cluster_slots_per_cta(uint32_t npad, uint32_t logC)
+{
+    uint32_t const chunks = npad >> 5;
+    return ((chunks + (1u << logC) - 1u) >> logC) << 5;
+}
+
 // Per-direction parameters of the lattice-address arithmetic (dir_table_fill); the kernels read
 // them from the CTA's shared copy of the table.
 struct DirParams {

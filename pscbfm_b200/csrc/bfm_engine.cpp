@@ -279,7 +279,7 @@ void Updater::setDrawCallback(DrawFn fn, void* ctx)
 
 void Updater::setMode(int mode)
 {
-    if (mode < kModeAuto || mode > kModePersistent) throw std::invalid_argument("[setMode] unknown mode");
+    if (mode < kModeAuto || mode > kModeCluster) throw std::invalid_argument("[setMode] unknown mode");
     if (mode == kModeResident && initialized() && !residentEligible())
         throw std::invalid_argument("[setMode] this system does not fit the resident kernel");
     mode_ = mode;
@@ -473,6 +473,7 @@ void Updater::initialize()
     if (!batchOnly_) ensureStaging();
     cuda_check(cudaStreamSynchronize(s), "initialize");
     buildObservables();
+    planCluster();
     subStep_ = 0;
     mcsDone_ = 0;
     lastColor_ = kNoColor;
@@ -959,6 +960,52 @@ void Updater::enqueueResident(uint32_t nSteps)
     lastColor_ = kNoColor;   // the resident kernel leaves no marks in the global temporary lattices
 }
 
+void Updater::planCluster()
+{
+    // the smallest cluster (2..16 CTAs) whose shared memory holds the system with at most 2 chunks
+    // of 32 slots per warp and colour (each chunk a warp walks waits on remote shared memory), else
+    // the smallest with at most 8; only configurations the device can run
+    clusterLogC_ = 0;
+    clusterPer_ = 0;
+    clusterSmem_ = 0;
+    if (codeMode_ == kCodeNone) return;
+    uint32_t const chunks = (maxGroup_ + 31u) / 32u;
+    for (uint32_t maxPer : {2u, 8u})
+        for (uint32_t logC = 1; logC <= 4; ++logC) {
+            uint32_t const C = 1u << logC;
+            if (dev_.h.nwords < C) continue;
+            uint32_t const perCta = (chunks + C - 1u) / C, perWarp = (perCta + 31u) / 32u;
+            uint32_t per = 1;
+            while (per < perWarp) per *= 2;
+            if (per > maxPer) continue;
+            size_t const smem = cluster_bc_smem_bytes(dev_.h.nwords, npad_, logC, per, codeMode_);
+            if (smem > kResidentMaxSmem || !cluster_bc_runnable(logC, per, smem, codeMode_)) continue;
+            clusterLogC_ = logC;
+            clusterPer_ = per;
+            clusterSmem_ = smem;
+            return;
+        }
+}
+
+void Updater::enqueueCluster(uint32_t nSteps)
+{
+    scrubPending(stream_);
+    for (uint32_t done = 0; done < nSteps;) {
+        uint32_t const chunk = std::min(nSteps - done, hStepCap_);
+        cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
+        fillSteps(chunk, hSteps_, true);
+        cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
+                   "steps H2D");
+        cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
+        cuda_check(launch_cluster_bc(dev_.dDesc, dev_.dList, 1, clusterLogC_, clusterPer_, dev_.dSteps, chunk,
+                                     clusterSmem_, codeMode_, stream_),
+                   "cluster");
+        ++launches_;
+        done += chunk;
+    }
+    lastColor_ = kNoColor;   // the cluster keeps its temporary lattice in shared memory
+}
+
 int Updater::path() const
 {
     requireInit("path");
@@ -967,12 +1014,15 @@ int Updater::path() const
 
 int Updater::autoMode() const
 {
-    // One system on a B200, per MCS: the resident kernel (one SM) is fastest while the largest
-    // colour group is at most 4 x 1024 monomers (8K-monomer chains: 13.7 us, persistent 15.5,
-    // graph 17.3); from there the persistent sweep, whose barriers cost less than the graph's
-    // launch gaps, while its tiles fit about three per SM (13K-262K monomers: 17-19 us against
-    // 19-22); beyond, the graph of separate launches (1M monomers: 30 us against 36).
+    // One system on a B200, per MCS: the resident kernel (one SM) while the largest colour group is
+    // at most 4 x 1024 monomers (1.2K-monomer chains 4.2 us, against 6.4 on a cluster and 11.9
+    // persistent; 8K: 13.7, 13.1, 13.1); then a cluster of CTAs holding the system in distributed
+    // shared memory where it takes at most two chunks of 32 slots per warp and colour (11K-39K
+    // monomers: 12.4-14.0 us against 13.1-16.0 persistent); then the persistent sweep while its
+    // tiles fit about three per SM (to 262K monomers: 16-19 us against 19-22 graph); beyond, the
+    // graph of separate launches (1M monomers: 30 us against 36).
     if (residentEligible() && maxGroup_ <= 4u * kResidentBlock) return kModeResident;
+    if (clusterEligible() && clusterPer_ <= 2u) return kModeCluster;
     if (codeMode_ != kCodeNone) {
         uint32_t const tiles = (maxGroup_ + kBcTileSpan - 1) / kBcTileSpan;
         if (tiles <= 3u * smCount_) return kModePersistent;
@@ -986,6 +1036,7 @@ int Updater::effectiveMode() const
     if (m == kModeAuto) m = autoMode();
     if (m == kModeResident && !residentEligible()) m = kModeGraph;
     if (m == kModePersistent && codeMode_ == kCodeNone) m = kModeGraph;   // bond codes only
+    if (m == kModeCluster && !clusterEligible()) m = kModeGraph;
     return m;
 }
 
@@ -1002,6 +1053,7 @@ void Updater::run(int32_t nMcs)
     if (m == kModeResident) enqueueResident(nSteps);
     else if (m == kModeGraph) enqueueGraph(nSteps);
     else if (m == kModePersistent) enqueuePersistent(nSteps);
+    else if (m == kModeCluster) enqueueCluster(nSteps);
     else enqueueLaunch(nSteps);
     mcsDone_ += (uint64_t)nMcs;
     hostStale_ = true;

@@ -61,11 +61,12 @@ inline uint32_t counter_draw(uint64_t seed, uint64_t k)
 
 // Engine path of one updater's run().
 enum Mode : int {
-    kModeAuto = 0,      // resident if the system fits one CTA, else graph
+    kModeAuto = 0,      // by size: resident, cluster, persistent or graph (autoMode)
     kModeLaunch = 1,    // two kernel launches per sub-step, like the reference
     kModeGraph = 2,     // the same kernels captured into a CUDA graph per chunk of sub-steps
     kModeResident = 3,  // one CTA runs the whole chunk, lattice in shared memory
     kModePersistent = 4,   // bond codes: one cooperative launch per chunk, grid barriers between phases
+    kModeCluster = 5,      // bond codes: one cluster of CTAs holds the system in shared memory
 };
 
 class Updater {
@@ -122,6 +123,7 @@ public:
     size_t deviceBytes() const { return dev_.bytes; }
     uint32_t maxGroup() const { return maxGroup_; }
     bool residentEligible() const;
+    bool clusterEligible() const { return clusterLogC_ != 0; }
     int gpu() const { return gpu_; }
     void validate();                         // host-side EV and bond-set check (checkSystem)
 
@@ -172,6 +174,8 @@ private:
     void enqueueLaunch(uint32_t nSteps);
     void enqueueGraph(uint32_t nSteps);
     void enqueueResident(uint32_t nSteps);
+    void enqueueCluster(uint32_t nSteps);
+    void planCluster();   // the cluster size and chunks per warp of the cluster-resident kernel
     void enqueuePersistent(uint32_t nSteps);
     void fillSteps(uint32_t nSteps, StepEntry* hostBuf, bool residentParity);
     void freeDevice();
@@ -212,6 +216,9 @@ private:
     bool gsPending_ = false;                   // hGs_ is being refreshed by the stream
     bool stallNext_ = false;                   // injectBarrierStall
     uint32_t smCount_ = 148;                   // SMs of the device (setGpu)
+    uint32_t clusterLogC_ = 0;                 // cluster of 2^logC CTAs holds the system (0: does not fit)
+    uint32_t clusterPer_ = 0;                  // chunks of 32 slots per warp and colour
+    size_t clusterSmem_ = 0;                   // dynamic shared memory per CTA
     uint32_t hStepCap_ = 0;
     std::vector<std::pair<uint32_t, cudaGraphExec_t>> graphs_;   // captured chunk length -> graph
     cudaEvent_t stepsFree_ = nullptr;          // host staging may be rewritten after this event

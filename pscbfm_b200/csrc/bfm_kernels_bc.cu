@@ -22,6 +22,7 @@
 // temporary lattice, pk and bond codes in shared memory; the check appends tentative movers to a
 // shared list (warp ballot + one atomic per warp), so the perform runs with full warps.
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -663,6 +664,201 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
     if (tid == 0 && nAtt) atomicAdd(S.stats + (blockIdx.x % kStatSlots), nAtt);
 }
 
+// ---------------------------------------------------------------------------------- cluster-resident
+
+// A 64-bit OR / XOR into distributed shared memory as 32-bit atomics on the two halves (the bits
+// are independent, so the result is the same). Measured on B200: 64-bit bitwise atomics on
+// another CTA's shared memory (through map_shared_rank, or atom.shared::cluster.*.b64) lose updates
+// when several CTAs hit the same word, while 32-bit ones do not.
+__device__ __forceinline__ void dsmem_or64(unsigned long long* p, unsigned long long v)
+{
+    unsigned int* const h = reinterpret_cast<unsigned int*>(p);
+    if ((unsigned int)v) atomicOr(h, (unsigned int)v);
+    if ((unsigned int)(v >> 32)) atomicOr(h + 1, (unsigned int)(v >> 32));
+}
+__device__ __forceinline__ void dsmem_xor64(unsigned long long* p, unsigned long long v)
+{
+    unsigned int* const h = reinterpret_cast<unsigned int*>(p);
+    if ((unsigned int)v) atomicXor(h, (unsigned int)v);
+    if ((unsigned int)(v >> 32)) atomicXor(h + 1, (unsigned int)(v >> 32));
+}
+__device__ __forceinline__ void dsmem_xor(unsigned int* p, unsigned int v) { atomicXor(p, v); }
+__device__ __forceinline__ void dsmem_xor(unsigned long long* p, unsigned long long v) { dsmem_xor64(p, v); }
+
+// One thread-block cluster of 2^logC CTAs (1024 threads each) owns a system whose lattice,
+// temporary lattice, addresses and codes fit their shared memory together, for a whole run of
+// sub-steps (layout: cluster_word_rank, cluster_slot_rank). Each CTA checks the slots it holds,
+// lists its own tentative movers and performs them; lattice and temporary words and neighbours'
+// codes held by another CTA are reached through distributed shared memory. Three cluster barriers
+// per sub-step (after the check, after the perform, after the temporary lattice is cleared) take
+// the place of the resident kernel's CTA barriers; every CTA of a cluster runs the same system and
+// so reaches the same barriers. A CTA leaves only after the last barrier, when no other CTA
+// accesses its shared memory any more. Grid: one cluster per system of sysList.
+template <typename W, int K>
+__global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* __restrict__ sysv,
+                                                                   uint32_t const* __restrict__ sysList,
+                                                                   StepEntry const* __restrict__ steps,
+                                                                   uint32_t nSys, uint32_t nSteps)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    uint32_t const C = cluster.num_blocks(), rank = cluster.block_rank();
+    uint32_t logC = 0;
+    while ((1u << logC) < C) ++logC;   // a power of two (launch_cluster_bc)
+    __shared__ SysDev S;
+    __shared__ uint32_t listCount;
+    extern __shared__ unsigned long long smem[];
+    uint32_t const sysId = sysList[blockIdx.x >> logC];
+    copy_desc(S, sysv + sysId);
+    __syncthreads();
+    uint32_t const np = S.npad, nwC = S.nwords >> logC, cap = cluster_slots_per_cta(np, logC);
+    uint32_t const B = blockDim.x, tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    unsigned long long* const ptab = smem;                                   // 768 plane masks
+    uint32_t* const dtab = reinterpret_cast<uint32_t*>(smem + 768);          // kDirTab words
+    unsigned long long* const lat = smem + 768 + kDirTab / 2;                // nwC words
+    unsigned long long* const tmp = lat + nwC;                               // nwC words
+    W* const code = reinterpret_cast<W*>(tmp + nwC);                         // cap slots
+    uint32_t* const pk = reinterpret_cast<uint32_t*>(code + cap);            // cap slots
+    uint8_t* const mok = reinterpret_cast<uint8_t*>(pk + cap);               // 512 move-table bytes
+    uint32_t* const list = reinterpret_cast<uint32_t*>(mok + 512);           // K x 1024 entries
+    W const* const gcode = static_cast<W const*>(S.code);
+    for (uint32_t w = tid; w < 768; w += B) ptab[w] = S.planeTab[w];
+    if (tid < kDirTab) dtab[tid] = S.dirTab[tid];
+    for (uint32_t w = tid; w < 512; w += B) mok[w] = S.moveOk[w];
+    for (uint32_t l = tid; l < nwC; l += B) {
+        lat[l] = S.lat[(l << logC) | rank];
+        tmp[l] = 0ull;
+    }
+    for (uint32_t l = tid; l < cap; l += B) {
+        uint32_t const g = cluster_slot_of(l, rank, logC);
+        bool const in = g < np;
+        code[l] = in ? gcode[g] : W(0);
+        pk[l] = in ? S.pk[g] : 0u;
+    }
+    if (tid == 0) listCount = 0;
+    cluster.sync();   // every CTA's part of the state is in place before any remote access
+
+    auto latAt = [&](uint32_t w) { return cluster.map_shared_rank(lat + (w >> logC), w & (C - 1u)); };
+    auto tmpAt = [&](uint32_t w) { return cluster.map_shared_rank(tmp + (w >> logC), w & (C - 1u)); };
+    auto codeAt = [&](uint32_t g) {
+        return cluster.map_shared_rank(code + cluster_slot_local(g, logC), cluster_slot_rank(g, logC));
+    };
+
+    uint32_t nTent = 0, nAcc = 0;
+    unsigned long long nAtt = 0;
+    StepEntry next = nSteps ? steps[sysId] : StepEntry{};
+    for (uint32_t t = 0; t < nSteps; ++t) {
+        StepEntry const st = next;
+        if (t + 1 < nSteps) next = steps[(size_t)(t + 1) * nSys + sysId];   // prefetch
+        if (st.color == kNoColor) continue;
+        if (rank == 0) nAtt += st.cnt;
+        // check: this CTA's chunks of 32 slots of the colour group (the group starts at a chunk)
+        uint32_t const end = st.off + st.cnt, c0 = st.off >> 5, cEnd = (end + 31u) >> 5;
+        uint32_t const cFirst = c0 + ((rank - c0) & (C - 1u));
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            uint32_t const c = cFirst + (warp + (uint32_t)k * 32u) * C;
+            uint32_t const g = c * 32u + lane;
+            bool go = false;
+            uint32_t entry = 0;
+            if (c < cEnd && g < end) {
+                uint32_t const l = cluster_slot_local(g, logC);
+                uint32_t const dir = move_dir(g - st.off, st.seed);
+                uint32_t const p = pk[l];
+                DirParams const D = dir_params(dtab, dir);
+                if ((p & D.ma) != D.wall && bonds_ok<W, true>(code[l], dir, mok)) {
+                    Plane pl;
+                    front_plane<true>(pl, ptab, D, p, D.front, dir);
+                    unsigned long long hit = 0ull;
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+                        if (pl.m[r]) hit |= *latAt(pl.w[r]) & pl.m[r];
+                    if (hit == 0ull) {
+                        uint32_t const to = addr_add(p, D.ma, D.step);
+                        dsmem_or64(tmpAt(to >> 6), 1ull << (to & 63u));
+                        go = true;
+                        entry = l | (dir << kSlotShift);
+                    }
+                }
+            }
+            uint32_t const bal = __ballot_sync(0xffffffffu, go);
+            if (bal) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(&listCount, (uint32_t)__popc(bal));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (go) list[base + __popc(bal & ((1u << lane) - 1u))] = entry;
+                nTent += lane == 0 ? (uint32_t)__popc(bal) : 0u;
+            }
+        }
+        cluster.sync();   // every CTA's marks are in place
+        // perform over this CTA's list
+        uint32_t const nList = listCount;
+        for (uint32_t e = tid; e < nList; e += B) {
+            uint32_t const l = list[e] & kSlotMask, dir = list[e] >> kSlotShift;
+            uint32_t const g = cluster_slot_of(l, rank, logC);
+            uint32_t const p = pk[l];
+            uint32_t nb[CodeWord<W>::kSlots];
+#pragma unroll
+            for (uint32_t q = 0; q < CodeWord<W>::kSlots; ++q)
+                nb[q] = q < S.maxc ? __ldg(S.nbrr + (size_t)q * np + g) : 0u;
+            Plane pl;
+            DirParams const D = dir_params(dtab, dir);
+            front_plane<true>(pl, ptab, D, p, D.front, dir);
+            unsigned long long hit = 0ull;
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (pl.m[r]) hit |= *tmpAt(pl.w[r]) & pl.m[r];
+            if (hit != 0ull) continue;
+            uint32_t const a = dir >> 1;
+            int32_t const s = (dir & 1u) ? 1 : -1;
+            uint32_t const p1 = addr_add(p, D.ma, D.step);
+            uint32_t const w0 = p >> 6, w1 = p1 >> 6;
+            if (w0 == w1) {
+                dsmem_xor64(latAt(w0), (1ull << (p & 63u)) | (1ull << (p1 & 63u)));
+            } else {
+                dsmem_xor64(latAt(w0), 1ull << (p & 63u));
+                dsmem_xor64(latAt(w1), 1ull << (p1 & 63u));
+            }
+            pk[l] = p1;
+            atomicAdd((a == 0 ? S.x : (a == 1 ? S.y : S.z)) + g, s);
+            W const own = code[l];
+            code[l] = code_shift(own, a, -s);
+            uint32_t const n = uint32_t(own >> CodeWord<W>::kCountShift) & 7u;
+#pragma unroll
+            for (uint32_t q = 0; q < CodeWord<W>::kSlots; ++q) {
+                if (q < n) {
+                    uint32_t const ent = nb[q];
+                    uint32_t const cr = (0u - (uint32_t(own >> (9u * q + 3u * a)) & 7u)) & 7u;
+                    uint32_t const nc = uint32_t(int32_t(cr) + s) & 7u;
+                    dsmem_xor(codeAt(ent & kSlotMask), W(cr ^ nc) << (9u * (ent >> kSlotShift) + 3u * a));
+                }
+            }
+            ++nAcc;
+        }
+        cluster.sync();   // every perform has read the temporary lattice
+        for (uint32_t l = tid; l < nwC; l += B) tmp[l] = 0ull;
+        if (tid == 0) listCount = 0;
+        cluster.sync();
+    }
+    // after the last cluster barrier no CTA reaches into another's shared memory
+    W* const gcodeOut = static_cast<W*>(S.code);
+    for (uint32_t l = tid; l < nwC; l += B) S.lat[(l << logC) | rank] = lat[l];
+    for (uint32_t l = tid; l < cap; l += B) {
+        uint32_t const g = cluster_slot_of(l, rank, logC);
+        if (g < np) {
+            gcodeOut[g] = code[l];
+            S.pk[g] = pk[l];
+        }
+    }
+    uint32_t const tsum = __reduce_add_sync(0xffffffffu, nTent);
+    uint32_t const asum = __reduce_add_sync(0xffffffffu, nAcc);
+    if (lane == 0) {
+        tally_flush(tsum, S.stats, 1);
+        tally_flush(asum, S.stats, 2);
+    }
+    if (tid == 0 && nAtt) atomicAdd(S.stats + (blockIdx.x % kStatSlots), nAtt);
+}
+
 // ---------------------------------------------------------------------------------- launchers
 
 namespace {
@@ -911,6 +1107,113 @@ cudaError_t launch_resident_bc(SysDev const* dSys, uint32_t const* dList, uint32
         return launch_resident_bc_w<uint32_t>(dSys, dList, nCta, perThread, dSteps, nSys, nSteps, smem, s);
     if (codeMode == kCode64)
         return launch_resident_bc_w<unsigned long long>(dSys, dList, nCta, perThread, dSteps, nSys, nSteps, smem, s);
+    return cudaErrorInvalidValue;
+}
+
+size_t cluster_bc_smem_bytes(uint32_t nwords, uint32_t npad, uint32_t logC, uint32_t perThread, uint32_t codeMode)
+{
+    size_t const w = codeMode == kCode64 ? 8 : 4;
+    size_t const cap = cluster_slots_per_cta(npad, logC);
+    return 768 * 8 + kDirTab * 4 + (size_t)(nwords >> logC) * 2 * 8 + cap * (w + 4) + 512 +
+           (size_t)perThread * kResidentBlock * 4;
+}
+
+namespace {
+
+template <typename W, int K>
+cudaError_t cluster_bc_config(uint32_t logC, size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribute* attr,
+                              uint32_t nSys, cudaStream_t s, bool& runnable)
+{
+    auto kernel = k_cluster_bc<W, K>;
+    uint32_t const C = 1u << logC;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (C > 8) {
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg = {};
+    cfg.gridDim = dim3(nSys * C);
+    cfg.blockDim = dim3(kResidentBlock);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    e = cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg);
+    runnable = e == cudaSuccess && clusters >= 1;
+    return e;
+}
+
+template <typename W, int K>
+cudaError_t launch_cluster_bc_k(SysDev const* dSys, uint32_t const* dList, uint32_t nSys, uint32_t logC,
+                                StepEntry const* dSteps, uint32_t nSteps, size_t smem, cudaStream_t s)
+{
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute attr[1];
+    bool runnable = false;
+    cudaError_t e = cluster_bc_config<W, K>(logC, smem, cfg, attr, nSys, s, runnable);
+    if (e != cudaSuccess) return e;
+    if (!runnable) return cudaErrorInvalidConfiguration;
+    return cudaLaunchKernelEx(&cfg, k_cluster_bc<W, K>, dSys, dList, dSteps, nSys, nSteps);
+}
+
+template <typename W>
+cudaError_t launch_cluster_bc_w(SysDev const* dSys, uint32_t const* dList, uint32_t nSys, uint32_t logC,
+                                uint32_t perThread, StepEntry const* dSteps, uint32_t nSteps, size_t smem,
+                                cudaStream_t s)
+{
+    switch (perThread) {
+    case 1: return launch_cluster_bc_k<W, 1>(dSys, dList, nSys, logC, dSteps, nSteps, smem, s);
+    case 2: return launch_cluster_bc_k<W, 2>(dSys, dList, nSys, logC, dSteps, nSteps, smem, s);
+    case 4: return launch_cluster_bc_k<W, 4>(dSys, dList, nSys, logC, dSteps, nSteps, smem, s);
+    case 8: return launch_cluster_bc_k<W, 8>(dSys, dList, nSys, logC, dSteps, nSteps, smem, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename W>
+bool cluster_bc_runnable_w(uint32_t logC, uint32_t perThread, size_t smem)
+{
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute attr[1];
+    bool runnable = false;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (perThread) {
+    case 1: e = cluster_bc_config<W, 1>(logC, smem, cfg, attr, 1, nullptr, runnable); break;
+    case 2: e = cluster_bc_config<W, 2>(logC, smem, cfg, attr, 1, nullptr, runnable); break;
+    case 4: e = cluster_bc_config<W, 4>(logC, smem, cfg, attr, 1, nullptr, runnable); break;
+    case 8: e = cluster_bc_config<W, 8>(logC, smem, cfg, attr, 1, nullptr, runnable); break;
+    default: break;
+    }
+    if (e != cudaSuccess) cudaGetLastError();   // a configuration the device refuses is an answer, not an error
+    return e == cudaSuccess && runnable;
+}
+
+}  // namespace
+
+bool cluster_bc_runnable(uint32_t logC, uint32_t perThread, size_t smem, uint32_t codeMode)
+{
+    if (logC < 1 || logC > 4 || smem > kResidentMaxSmem) return false;
+    if (codeMode == kCode32) return cluster_bc_runnable_w<uint32_t>(logC, perThread, smem);
+    if (codeMode == kCode64) return cluster_bc_runnable_w<unsigned long long>(logC, perThread, smem);
+    return false;
+}
+
+cudaError_t launch_cluster_bc(SysDev const* dSys, uint32_t const* dList, uint32_t nSys, uint32_t logC,
+                              uint32_t perThread, StepEntry const* dSteps, uint32_t nSteps, size_t smem,
+                              uint32_t codeMode, cudaStream_t s)
+{
+    if (nSys == 0 || nSteps == 0) return cudaSuccess;
+    if (logC < 1 || logC > 4 || smem > kResidentMaxSmem) return cudaErrorInvalidValue;
+    if (codeMode == kCode32)
+        return launch_cluster_bc_w<uint32_t>(dSys, dList, nSys, logC, perThread, dSteps, nSteps, smem, s);
+    if (codeMode == kCode64)
+        return launch_cluster_bc_w<unsigned long long>(dSys, dList, nSys, logC, perThread, dSteps, nSteps, smem, s);
     return cudaErrorInvalidValue;
 }
 

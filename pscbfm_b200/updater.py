@@ -13,7 +13,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import MODE_AUTO, MODE_GRAPH, MODE_LAUNCH, MODE_PERSISTENT, MODE_RESIDENT  # noqa: F401
+from ._lib import MODE_AUTO, MODE_GRAPH, MODE_LAUNCH, MODE_PERSISTENT, MODE_RESIDENT, MODE_CLUSTER  # noqa: F401
 
 REPR_AUTO, REPR_GATHER = 0, 1
 
@@ -235,9 +235,12 @@ class UpdaterGPUScBFM_AB_Type:
         return n.value, sizes
 
     def stats(self):
-        out = np.zeros(4, dtype=np.uint64)
+        """Move counters (waits for the handle's queued work): attempted, tentative, accepted, MCS."""
+        out = self.__dict__.get("_stats_buf")
+        if out is None:
+            out = self._stats_buf = (C.c_uint64 * 4)()
         self._call("bfm_get_stats", out)
-        return {"attempted": int(out[0]), "tentative": int(out[1]), "accepted": int(out[2]), "mcs": int(out[3])}
+        return {"attempted": out[0], "tentative": out[1], "accepted": out[2], "mcs": out[3]}
 
     def validate(self):
         self._call("bfm_validate")

@@ -145,6 +145,31 @@ int main()
         e[d >> 1] = 1023;
         if (addr_add(address(zero, nb, tab), M.ma, M.step) != address(e, nb, tab)) return std::printf("wrap at 0\n"), 1;
     }
+    // the cluster-resident layout: every slot and every lattice word has one owner and one local
+    // index inside that owner's capacity, and the inverse maps back
+    for (uint32_t logC = 1; logC <= 4; ++logC) {
+        uint32_t const C = 1u << logC;
+        for (uint32_t npad : {32u, 64u, 96u, 480u, 4096u, 11264u + 32u, 131072u}) {
+            uint32_t const cap = cluster_slots_per_cta(npad, logC);
+            std::vector<char> seen((size_t)C * cap, 0);
+            for (uint32_t g = 0; g < npad; ++g) {
+                uint32_t const r = cluster_slot_rank(g, logC), l = cluster_slot_local(g, logC);
+                if (r >= C || l >= cap || seen[(size_t)r * cap + l] || cluster_slot_of(l, r, logC) != g)
+                    return std::printf("cluster slot layout: C %u npad %u slot %u\n", C, npad, g), 1;
+                seen[(size_t)r * cap + l] = 1;
+            }
+        }
+        for (uint32_t nw : {2u, 16u, 64u, 512u, 4096u, 32768u}) {
+            if (nw < C) continue;
+            std::vector<char> seen(nw, 0);
+            for (uint32_t w = 0; w < nw; ++w) {
+                uint32_t const r = cluster_word_rank(w, logC), l = cluster_word_local(w, logC);
+                if (r >= C || l >= nw / C || seen[(size_t)r * (nw / C) + l])
+                    return std::printf("cluster word layout: C %u nw %u word %u\n", C, nw, w), 1;
+                seen[(size_t)r * (nw / C) + l] = 1;
+            }
+        }
+    }
     std::printf("ok\n");
     return 0;
 }

@@ -9,7 +9,8 @@ from pscbfm_b200 import systems as S
 
 pytestmark = pytest.mark.gpu
 
-MODES = {"graph": P.MODE_GRAPH, "resident": P.MODE_RESIDENT, "launch": P.MODE_LAUNCH, "persistent": P.MODE_PERSISTENT}
+MODES = {"graph": P.MODE_GRAPH, "resident": P.MODE_RESIDENT, "launch": P.MODE_LAUNCH, "persistent": P.MODE_PERSISTENT,
+         "cluster": P.MODE_CLUSTER}
 
 
 @pytest.mark.parametrize("mode", list(MODES))

@@ -13,7 +13,7 @@ from pscbfm_b200 import systems as S
 pytestmark = pytest.mark.gpu
 
 MODES = {"launch": P.MODE_LAUNCH, "graph": P.MODE_GRAPH, "resident": P.MODE_RESIDENT, "auto": P.MODE_AUTO,
-         "persistent": P.MODE_PERSISTENT}
+         "persistent": P.MODE_PERSISTENT, "cluster": P.MODE_CLUSTER}
 REPRS = {"codes": P.REPR_AUTO, "gather": P.REPR_GATHER}
 
 
@@ -36,7 +36,7 @@ def _resident_ok(s):
 
 
 @pytest.mark.parametrize("repr_", ["codes", "gather"])
-@pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent"])
+@pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent", "cluster"])
 @pytest.mark.parametrize("name", list(CASES))
 def test_engine_reproduces_reference_updater(name, mode, repr_):
     g = json.load(open(GOLDEN_JSON))["cases"][name]
@@ -59,7 +59,7 @@ NON_CUBIC = {
 
 
 @pytest.mark.parametrize("repr_", ["codes", "gather"])
-@pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent"])
+@pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent", "cluster"])
 @pytest.mark.parametrize("name", list(NON_CUBIC))
 def test_non_cubic_boxes_vs_oracle(name, mode, repr_):
     """Boxes with unequal power-of-two sides: the brick index interleaves the axes' low bits and
@@ -73,6 +73,28 @@ def test_non_cubic_boxes_vs_oracle(name, mode, repr_):
     xyz, st = run_engine(s, chunks, MODES[mode], repr_=REPRS[repr_])
     assert np.array_equal(xyz, want)
     assert st["mcs"] == sum(chunks)
+
+
+@pytest.mark.parametrize("build", [S.crosslinked_network, lambda: S.serpentine_chains(128, 64, 0.3, seed=3),
+                                   lambda: S.serpentine_chains(64, 64, 0.8, seed=13),
+                                   lambda: S.walled(S.serpentine_chains((128, 32, 64), 16, 0.35, seed=41), walls=6)])
+def test_cluster_kernel_vs_oracle(build):
+    """Systems too large for one CTA's shared memory, held by a cluster of CTAs: the cluster path
+    runs (bfm_get_path) and every chunk of the run equals the oracle."""
+    s = build()
+    u = P.UpdaterGPUScBFM_AB_Type(0)
+    u.load_system(s, mode=P.MODE_CLUSTER)
+    assert u.path() == P.MODE_CLUSTER, s.name
+    done = 0
+    for chunk in (1, 9, 40):
+        u.runSimulationOnGPU(chunk)
+        done += chunk
+        want, ost = O.run(s, done)
+        assert np.array_equal(u.get_coords(), want), (s.name, done)
+    u.validate()
+    st = u.stats()
+    assert st["mcs"] == done and (st["attempted"], st["tentative"], st["accepted"]) == ost
+    u.close()
 
 
 def test_asymmetric_lists_fall_back_to_gather():
@@ -113,7 +135,7 @@ def test_six_functional_network_vs_oracle(mode, repr_):
 
 
 @pytest.mark.parametrize("repr_", ["codes", "gather"])
-@pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent"])
+@pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent", "cluster"])
 @pytest.mark.parametrize("walls", [1, 4, 6])
 def test_partial_walls_vs_oracle(walls, mode, repr_):
     # the reference has builds for fully periodic and fully walled boxes only: mixed periodicity
@@ -125,7 +147,7 @@ def test_partial_walls_vs_oracle(walls, mode, repr_):
     assert (st["attempted"], st["tentative"], st["accepted"]) == ost
 
 
-@pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent"])
+@pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent", "cluster"])
 def test_hydrogel_fixture_with_walls_vs_oracle(mode):
     # the reference's non-periodic hydrogel (tests/coloring-test-Hydrogel...bfm): up to 5 bonds per
     # monomer, more than the reference build's MAX_CONNECTIVITY, so the oracle pins it
