@@ -505,8 +505,9 @@ def batched_vs_plain(n_systems=256, mcs=100, plain_mcs=20):
     return {"workload": "ensemble_256_systems", "systems": n_systems, "monomers": n, "mcs": mcs,
             "batched": n * mcs / (batched_ms / 1e3), "plain": n * mcs / (plain_ms / 1e3),
             "ratio": plain_ms / batched_ms, "batched_launches_per_mcs": launches_per_mcs,
-            "autotuned": {"shape": tuned["shape"], "resident": tuned["resident"],
-                          "trials": [[t["shape"], t["resident"], round(t["ms_per_mcs"], 4)] for t in tuned["trials"]]},
+            "autotuned": {"shape": tuned["shape"], "resident": tuned["resident"], "cluster": tuned["cluster"],
+                          "trials": [[t["shape"], t["resident"], t["cluster"], round(t["ms_per_mcs"], 4)]
+                                     for t in tuned["trials"]]},
             "plain_path": f"BFM_MODE_LAUNCH, one system at a time, {plain_mcs} MCS each scaled to {mcs}",
             "unit": "attempted moves/s"}
 

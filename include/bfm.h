@@ -38,9 +38,9 @@ extern "C" {
 
 /* engine paths (bfm_set_mode) */
 #define BFM_MODE_AUTO 0     /* resident for small systems (largest colour group <= 4096 and fits one CTA),
-                               cluster where a cluster's shared memory holds the system at <= 2
-                               chunks of 32 slots per warp, persistent up to about three 512-monomer
-                               tiles per SM (bond codes), else graph */
+                               cluster where a cluster's shared memory holds the system with at
+                               most 48 chunks of 32 slots per CTA and colour, persistent up to about
+                               three 512-monomer tiles per SM (bond codes), else graph */
 #define BFM_MODE_LAUNCH 1   /* check + perform launch per sub-step (the reference's structure) */
 #define BFM_MODE_GRAPH 2    /* the same launches captured into CUDA graphs */
 #define BFM_MODE_RESIDENT 3 /* one CTA per system, lattice in shared memory (box <= 64^3) */
@@ -202,16 +202,22 @@ int bfm_batch_launch_count(bfm_batch_handle b, uint64_t* out);
 int bfm_batch_synchronize(bfm_batch_handle b);
 /* 0: every system on the grid path; 1 (default): small systems on the resident kernel. */
 int bfm_batch_set_resident(bfm_batch_handle b, int on);
+/* 1 (default): systems too large for one CTA that a cluster of CTAs holds with at most two chunks
+ * of 32 monomers per warp and colour (bond codes; there the cluster-resident kernel of
+ * BFM_MODE_CLUSTER beats the grid-phase kernels) run in that kernel while the batch's clusters take
+ * at most half of the SMs; 0: they share the grid-phase kernels. */
+int bfm_batch_set_cluster(bfm_batch_handle b, int on);
 /* Member i advances mcs[i] MCS (0 = it idles); one launch sequence for all, like bfm_batch_run. */
 int bfm_batch_run_each(bfm_batch_handle b, const int32_t* mcs);
 /* Register budget of the grid-phase kernels, 0..3, or -1 for the default; results do not change. */
 int bfm_batch_set_shape(bfm_batch_handle b, int shape);
-/* Autotuner: runs every configuration (kernel shape x resident path on / off) for 1 + mcs_per_trial
- * MCS, keeps the fastest and reports it (shape, resident, ms per MCS). The trials are ordinary MCS
- * of the run (results do not depend on the configuration): every member advances by n_trials x
- * (1 + mcs_per_trial) MCS. trials (may be NULL) receives up to capacity triples (shape, resident,
+/* Autotuner: runs every configuration (kernel shape x resident path on / off x cluster path on /
+ * off) for 1 + mcs_per_trial MCS, keeps the fastest and reports it (shape, paths, ms per MCS;
+ * paths: bit 0 the resident path, bit 1 the cluster path). The trials are ordinary MCS of the run
+ * (results do not depend on the configuration): every member advances by n_trials x
+ * (1 + mcs_per_trial) MCS. trials (may be NULL) receives up to capacity triples (shape, paths,
  * ms per MCS). */
-int bfm_batch_autotune(bfm_batch_handle b, int32_t mcs_per_trial, int* shape, int* resident, float* ms_per_mcs,
+int bfm_batch_autotune(bfm_batch_handle b, int32_t mcs_per_trial, int* shape, int* paths, float* ms_per_mcs,
                        float* trials, uint32_t capacity, uint32_t* n_trials);
 const char* bfm_batch_last_error(bfm_batch_handle b);
 

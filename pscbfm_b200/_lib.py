@@ -109,6 +109,7 @@ _SIGS = {
     "bfm_batch_run_timed": [H, C.c_int32, C.POINTER(C.c_float)],
     "bfm_batch_synchronize": [H],
     "bfm_batch_set_resident": [H, C.c_int],
+    "bfm_batch_set_cluster": [H, C.c_int],
     "bfm_sweep_noalloc": [C.c_void_p, C.c_int32, C.c_uint64, C.c_uint64, C.c_void_p, C.c_char_p, C.c_size_t],
     "bfm_server_create": [C.POINTER(C.c_void_p), C.c_int, C.c_uint64, C.c_uint32],
     "bfm_server_destroy": [H],

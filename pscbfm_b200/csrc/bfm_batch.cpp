@@ -2,7 +2,11 @@
 //
 // Systems whose lattices (and, in the bond-code representation, packed coordinates and bond
 // codes) fit one CTA's shared memory run in the resident kernel, one CTA per system, one launch
-// per run. The other systems share the grid-phase kernels: one check and one perform launch per
+// per run. Systems of the bond-code representation that a cluster of 2-16 CTAs holds in its
+// distributed shared memory with at most two chunks of 32 slots per warp and colour (where that
+// kernel beats the grid-phase kernels) run in the cluster-resident kernel, one cluster per system and one
+// launch per run and cluster size, while the batch's clusters take at most half of the SMs. The
+// other systems share the grid-phase kernels: one check and one perform launch per
 // sub-step and representation cover the active colour group of every such system at once, and
 // chunks of those launches are captured into a CUDA graph once and replayed. Each system draws its
 // own sub-steps from its own stream exactly as it would alone, so its trajectory is unchanged by
@@ -10,7 +14,7 @@
 //
 // A run stages the step entries of all its sub-steps with one host-to-device copy; the resident
 // and the grid-phase launches then proceed on two streams without meeting until the run ends, and
-// the host returns as soon as the work is queued. Member streams are ordered before the run and
+// the host returns as soon as the work is queued. Each cluster group runs on a stream of its own. Member streams are ordered before the run and
 // after it with events, never with host waits.
 
 #include <algorithm>
@@ -35,6 +39,9 @@ Batch::Batch(int gpu, Updater* const* members, uint32_t n) : gpu_(gpu)
     cuda_check(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking), "cudaStreamCreate");
     for (cudaEvent_t* e : {&join_, &fork_, &stepsFree_, &done_, &ready_})
         cuda_check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, gpu_) == cudaSuccess && sms > 0)
+        smCount_ = (uint32_t)sms;
 }
 
 Batch::~Batch()
@@ -42,6 +49,7 @@ Batch::~Batch()
     cudaSetDevice(gpu_);
     if (stream_) cudaStreamSynchronize(stream_);
     if (stream2_) cudaStreamSynchronize(stream2_);
+    for (cudaStream_t q : side_) cudaStreamSynchronize(q);
     if (graph_) cudaGraphExecDestroy(graph_);
     if (arena_) cudaFreeAsync(arena_, stream_);
     if (dStepsAll_) cudaFreeAsync(dStepsAll_, stream_);
@@ -49,6 +57,8 @@ Batch::~Batch()
     cudaFreeHost(hSteps_);
     for (cudaEvent_t e : {join_, fork_, stepsFree_, done_, ready_})
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : sideJoin_) cudaEventDestroy(e);
+    for (cudaStream_t q : side_) cudaStreamDestroy(q);
     if (stream_) cudaStreamDestroy(stream_);
     if (stream2_) cudaStreamDestroy(stream2_);
 }
@@ -57,6 +67,13 @@ uint32_t Batch::residentCount() const
 {
     uint32_t n = 0;
     for (auto const& g : resident_) n += (uint32_t)g.members.size();
+    return n;
+}
+
+uint32_t Batch::clusterCount() const
+{
+    uint32_t n = 0;
+    for (auto const& g : cluster_) n += (uint32_t)g.members.size();
     return n;
 }
 
@@ -85,10 +102,12 @@ void Batch::rebuild()
     // the previous launches may still read the arena
     cuda_check(cudaStreamSynchronize(stream_), "batch");
     cuda_check(cudaStreamSynchronize(stream2_), "batch");
+    for (cudaStream_t q : side_) cuda_check(cudaStreamSynchronize(q), "batch");
     uint32_t const M = (uint32_t)members_.size();
     grid_.clear();
     resident_.clear();
-    isResident_.assign(M, 0);
+    cluster_.clear();
+    wholeRun_.assign(M, 0);
     auto gridGroup = [&](uint32_t mode) -> GridGroup& {
         for (auto& g : grid_)
             if (g.codeMode == mode) return g;
@@ -101,14 +120,29 @@ void Batch::rebuild()
         resident_.push_back(ResidentGroup{mode, {}, nullptr, 1, 0});
         return resident_.back();
     };
+    auto clusterGroup = [&](uint32_t mode, uint32_t logC) -> ClusterGroup& {
+        for (auto& g : cluster_)
+            if (g.codeMode == mode && g.logC == logC) return g;
+        cluster_.push_back(ClusterGroup{mode, logC, {}, nullptr, 1, 0, cluster_.size()});
+        return cluster_.back();
+    };
+    uint32_t clusterCtas = 0;
     for (uint32_t m = 0; m < M; ++m) {
         Updater* u = members_[m];
+        uint32_t const C = 1u << u->clusterLogC();
         if (residentOn_ && u->residentEligible()) {
             ResidentGroup& g = resGroup(u->codeMode());
             g.members.push_back(m);
             g.smem = std::max(g.smem, u->residentSmem());
             while (g.perThread * kResidentBlock < u->maxGroup()) g.perThread *= 2;
-            isResident_[m] = 1;
+            wholeRun_[m] = 1;
+        } else if (clusterOn_ && u->clusterEligible() && u->clusterForBatch() && clusterCtas + C <= smCount_ / 2u) {
+            ClusterGroup& g = clusterGroup(u->codeMode(), u->clusterLogC());
+            g.members.push_back(m);
+            g.smem = std::max(g.smem, u->clusterSmem());
+            g.perThread = std::max(g.perThread, u->clusterPer());
+            clusterCtas += C;
+            wholeRun_[m] = 1;
         } else {
             GridGroup& g = gridGroup(u->codeMode());
             uint32_t const span = u->codeMode() == kCodeNone ? kGridBlock : kBcTileSpan;
@@ -122,6 +156,28 @@ void Batch::rebuild()
     size_t total = up256(sizeof(SysDev) * M) + up256(sizeof(StepEntry) * stepCap_ * M);
     for (auto const& g : grid_) total += up256(sizeof(TileRef) * g.tiles.size()) + up256(sizeof(TileRef) * g.ptiles.size());
     for (auto const& g : resident_) total += up256(sizeof(uint32_t) * g.members.size());
+    for (auto const& g : cluster_) total += up256(sizeof(uint32_t) * g.members.size());
+    while (side_.size() < cluster_.size()) {
+        cudaStream_t q = nullptr;
+        cudaEvent_t e = nullptr;
+        cuda_check(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking), "cudaStreamCreate");
+        side_.push_back(q);
+        cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        sideJoin_.push_back(e);
+    }
+    for (auto& g : cluster_) {
+        // one launch runs every cluster of the group at one size; a member planned with fewer
+        // chunks per warp runs as well with more (the kernel walks only its own chunks)
+        size_t smem = 0;
+        for (uint32_t m : g.members) {
+            Updater const* u = members_[m];
+            smem = std::max(smem, cluster_bc_smem_bytes(u->desc().nwords, u->desc().npad, g.logC, g.perThread,
+                                                        g.codeMode));
+        }
+        g.smem = smem;
+        if (!cluster_bc_runnable(g.logC, g.perThread, g.smem, g.codeMode))
+            throw std::runtime_error("[Batch] a cluster group's configuration does not run on this device");
+    }
     if (total > arenaBytes_) {   // grows only: membership changes reuse the arena
         if (arena_) cuda_check(cudaFreeAsync(arena_, stream_), "cudaFreeAsync(batch)");
         arena_ = nullptr;
@@ -156,6 +212,13 @@ void Batch::rebuild()
         cuda_check(cudaMemcpyAsync(g.dList, g.members.data(), sizeof(uint32_t) * g.members.size(),
                                    cudaMemcpyHostToDevice, stream_),
                    "upload resident list");
+    }
+    for (auto& g : cluster_) {
+        g.dList = reinterpret_cast<uint32_t*>(p);
+        p += up256(sizeof(uint32_t) * g.members.size());
+        cuda_check(cudaMemcpyAsync(g.dList, g.members.data(), sizeof(uint32_t) * g.members.size(),
+                                   cudaMemcpyHostToDevice, stream_),
+                   "upload cluster list");
     }
     // the host vectors above die with this call: finish their copies now
     cuda_check(cudaStreamSynchronize(stream_), "batch uploads");
@@ -261,10 +324,11 @@ void Batch::run(int32_t const* mcs)
         if (mcs[m] < 0) throw std::invalid_argument("[Batch::run] negative MCS count");
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
     if (!built_) rebuild();
-    // pending grid-path marks of members that run resident are cleared on their own streams; then
-    // the batch waits for every member stream (uploads, scrubs, observables) on the device
+    // pending grid-path marks of members that run in a resident or cluster kernel are cleared on
+    // their own streams; then the batch waits for every member stream (uploads, scrubs,
+    // observables) on the device
     for (uint32_t m = 0; m < M; ++m)
-        if (isResident_[m]) members_[m]->scrubPending(members_[m]->stream());
+        if (wholeRun_[m]) members_[m]->scrubPending(members_[m]->stream());
     for (Updater* u : members_) {
         cuda_check(cudaEventRecord(ready_, u->stream()), "event");
         cuda_check(cudaStreamWaitEvent(stream_, ready_, 0), "wait");
@@ -288,9 +352,19 @@ void Batch::run(int32_t const* mcs)
         cuda_check(cudaMemcpyAsync(dStepsAll_, hSteps_, sizeof(StepEntry) * entries, cudaMemcpyHostToDevice, stream_),
                    "batch steps H2D");
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
+        if (!resident_.empty() || !cluster_.empty()) cuda_check(cudaEventRecord(fork_, stream_), "event");
+        for (auto const& g : cluster_) {
+            // one launch per cluster size for the whole run, each on a stream of its own
+            cudaStream_t const q = side_[g.side];
+            cuda_check(cudaStreamWaitEvent(q, fork_, 0), "wait");
+            cuda_check(launch_cluster_bc(dSys_, g.dList, (uint32_t)g.members.size(), g.logC, g.perThread, dStepsAll_,
+                                         M, (uint32_t)T, g.smem, g.codeMode, q),
+                       "batch cluster");
+            cuda_check(cudaEventRecord(sideJoin_[g.side], q), "event");
+            ++launches_;
+        }
         if (!resident_.empty()) {
             // one launch per group for the whole run, on the second stream
-            cuda_check(cudaEventRecord(fork_, stream_), "event");
             cuda_check(cudaStreamWaitEvent(stream2_, fork_, 0), "wait");
             for (auto const& g : resident_) {
                 cuda_check(g.codeMode == kCodeNone
@@ -323,10 +397,11 @@ void Batch::run(int32_t const* mcs)
             cuda_check(cudaEventRecord(join_, stream2_), "event");
             cuda_check(cudaStreamWaitEvent(stream_, join_, 0), "wait");
         }
+        for (auto const& g : cluster_) cuda_check(cudaStreamWaitEvent(stream_, sideJoin_[g.side], 0), "wait");
     }
     cuda_check(cudaEventRecord(done_, stream_), "event");
     for (uint32_t m = 0; m < M; ++m) {
-        members_[m]->noteExternalRun(need[m], (uint64_t)mcs[m], !isResident_[m], members_[m]->lastColor());
+        members_[m]->noteExternalRun(need[m], (uint64_t)mcs[m], !wholeRun_[m], members_[m]->lastColor());
         members_[m]->streamWait(done_);
     }
 }
@@ -345,24 +420,36 @@ std::vector<Batch::Trial> Batch::autotune(int32_t mcsPerTrial)
     if (mcsPerTrial <= 0) throw std::invalid_argument("[Batch::autotune] trials need at least one MCS");
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
     if (!built_) rebuild();
-    bool anyEligible = false;
-    for (Updater* u : members_) anyEligible = anyEligible || u->residentEligible();
+    // cluster on and off differ only where a member that does not run resident could run in a
+    // cluster
+    bool anyResident = false, anyCluster[2] = {false, false};
+    for (Updater* u : members_) {
+        anyResident = anyResident || u->residentEligible();
+        bool const cl = u->clusterEligible() && u->clusterForBatch();
+        anyCluster[0] = anyCluster[0] || cl;
+        anyCluster[1] = anyCluster[1] || (cl && !u->residentEligible());
+    }
     std::vector<Trial> trials;
     for (int resident = 1; resident >= 0; --resident) {
-        if (!resident && !anyEligible) break;   // the same configuration as resident on
-        setResidentEnabled(resident != 0);
-        rebuild();
-        int const nShapes = grid_.empty() ? 1 : kGridShapes;   // the shape only matters to grid groups
-        for (int s = 0; s < nShapes; ++s) {
-            setShape(grid_.empty() ? -1 : s);
-            runTimed(1);
-            trials.push_back(Trial{shape_, resident != 0, runTimed(mcsPerTrial) / (float)mcsPerTrial});
+        if (!resident && !anyResident) break;   // the same configuration as resident on
+        for (int cl = 1; cl >= 0; --cl) {
+            if (!cl && !anyCluster[resident]) break;   // the same configuration as cluster on
+            setResidentEnabled(resident != 0);
+            setClusterEnabled(cl != 0);
+            rebuild();
+            int const nShapes = grid_.empty() ? 1 : kGridShapes;   // the shape only matters to grid groups
+            for (int s = 0; s < nShapes; ++s) {
+                setShape(grid_.empty() ? -1 : s);
+                runTimed(1);
+                trials.push_back(Trial{shape_, resident != 0, cl != 0, runTimed(mcsPerTrial) / (float)mcsPerTrial});
+            }
         }
     }
     Trial best = trials.front();
     for (Trial const& t : trials)
         if (t.msPerMcs < best.msPerMcs) best = t;
     setResidentEnabled(best.resident);
+    setClusterEnabled(best.cluster);
     setShape(best.shape);
     return trials;
 }

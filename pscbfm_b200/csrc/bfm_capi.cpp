@@ -408,14 +408,14 @@ int bfm_batch_run(bfm_batch_handle b, int32_t n)
     });
 }
 int bfm_batch_set_shape(bfm_batch_handle b, int shape) { BFM_CALL(b, b->b.setShape(shape)); }
-int bfm_batch_autotune(bfm_batch_handle b, int32_t mcsPerTrial, int* shape, int* resident, float* msPerMcs,
+int bfm_batch_autotune(bfm_batch_handle b, int32_t mcsPerTrial, int* shape, int* paths, float* msPerMcs,
                        float* trials, uint32_t capacity, uint32_t* nTrials)
 {
     BFM_CALL(b, {
         auto const t = b->b.autotune(mcsPerTrial);
         b->b.synchronize();
         if (shape) *shape = b->b.shape();
-        if (resident) *resident = b->b.residentEnabled() ? 1 : 0;
+        if (paths) *paths = (b->b.residentEnabled() ? 1 : 0) | (b->b.clusterEnabled() ? 2 : 0);
         if (msPerMcs) {
             float best = t.front().msPerMcs;
             for (auto const& x : t) best = std::min(best, x.msPerMcs);
@@ -424,7 +424,7 @@ int bfm_batch_autotune(bfm_batch_handle b, int32_t mcsPerTrial, int* shape, int*
         if (trials)
             for (uint32_t i = 0; i < (uint32_t)t.size() && i < capacity; ++i) {
                 trials[3 * i] = (float)t[i].shape;
-                trials[3 * i + 1] = t[i].resident ? 1.f : 0.f;
+                trials[3 * i + 1] = (float)((t[i].resident ? 1 : 0) | (t[i].cluster ? 2 : 0));
                 trials[3 * i + 2] = t[i].msPerMcs;
             }
         if (nTrials) *nTrials = (uint32_t)t.size();
@@ -455,5 +455,6 @@ int bfm_batch_launch_count(bfm_batch_handle b, uint64_t* out)
     });
 }
 int bfm_batch_set_resident(bfm_batch_handle b, int on) { BFM_CALL(b, b->b.setResidentEnabled(on != 0)); }
+int bfm_batch_set_cluster(bfm_batch_handle b, int on) { BFM_CALL(b, b->b.setClusterEnabled(on != 0)); }
 
 }  // extern "C"

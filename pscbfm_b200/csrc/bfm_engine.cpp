@@ -962,27 +962,36 @@ void Updater::enqueueResident(uint32_t nSteps)
 
 void Updater::planCluster()
 {
-    // the smallest cluster (2..16 CTAs) whose shared memory holds the system with at most 2 chunks
-    // of 32 slots per warp and colour (each chunk a warp walks waits on remote shared memory), else
-    // the smallest with at most 8; only configurations the device can run
+    // Three tiers, each the smallest cluster (2..16 CTAs) the device can run whose CTAs walk at
+    // most so many chunks of 32 slots per colour: 48 (1.5 per warp; the plan BFM_MODE_AUTO takes),
+    // 64 (2 per warp; the plan a Batch takes) and 256 (8 per warp; BFM_MODE_CLUSTER only). Each
+    // chunk a warp walks waits on remote shared memory, so the kernel's time per sub-step grows
+    // with the chunks per CTA. Alone on a B200 (chains in 64^3 and 128^3 boxes, 11K-60K monomers)
+    // it beats the persistent sweep up to about 48 chunks per CTA (9.1-15.2 us per MCS against
+    // 12.9-16.0) and loses from about 51-59 (16.2-17.5 against 15.8-16.1), while up to 64 it still
+    // beats the graph of launches (17.5 against 18.0), the path a Batch runs such a system on
+    // otherwise; at 8 chunks per warp it takes 25-30 us.
+    constexpr uint32_t kLimits[3] = {48u, 64u, 256u};
     clusterLogC_ = 0;
     clusterPer_ = 0;
     clusterSmem_ = 0;
+    clusterTier_ = 0;
     if (codeMode_ == kCodeNone) return;
     uint32_t const chunks = (maxGroup_ + 31u) / 32u;
-    for (uint32_t maxPer : {2u, 8u})
+    for (uint32_t tier = 0; tier < 3; ++tier)
         for (uint32_t logC = 1; logC <= 4; ++logC) {
             uint32_t const C = 1u << logC;
             if (dev_.h.nwords < C) continue;
             uint32_t const perCta = (chunks + C - 1u) / C, perWarp = (perCta + 31u) / 32u;
+            if (perCta > kLimits[tier]) continue;
             uint32_t per = 1;
             while (per < perWarp) per *= 2;
-            if (per > maxPer) continue;
             size_t const smem = cluster_bc_smem_bytes(dev_.h.nwords, npad_, logC, per, codeMode_);
             if (smem > kResidentMaxSmem || !cluster_bc_runnable(logC, per, smem, codeMode_)) continue;
             clusterLogC_ = logC;
             clusterPer_ = per;
             clusterSmem_ = smem;
+            clusterTier_ = 3 - tier;
             return;
         }
 }
@@ -997,7 +1006,7 @@ void Updater::enqueueCluster(uint32_t nSteps)
         cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
                    "steps H2D");
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
-        cuda_check(launch_cluster_bc(dev_.dDesc, dev_.dList, 1, clusterLogC_, clusterPer_, dev_.dSteps, chunk,
+        cuda_check(launch_cluster_bc(dev_.dDesc, dev_.dList, 1, clusterLogC_, clusterPer_, dev_.dSteps, 1, chunk,
                                      clusterSmem_, codeMode_, stream_),
                    "cluster");
         ++launches_;
@@ -1017,12 +1026,12 @@ int Updater::autoMode() const
     // One system on a B200, per MCS: the resident kernel (one SM) while the largest colour group is
     // at most 4 x 1024 monomers (1.2K-monomer chains 4.2 us, against 6.4 on a cluster and 11.9
     // persistent; 8K: 13.7, 13.1, 13.1); then a cluster of CTAs holding the system in distributed
-    // shared memory where it takes at most two chunks of 32 slots per warp and colour (11K-39K
-    // monomers: 12.4-14.0 us against 13.1-16.0 persistent); then the persistent sweep while its
-    // tiles fit about three per SM (to 262K monomers: 16-19 us against 19-22 graph); beyond, the
-    // graph of separate launches (1M monomers: 30 us against 36).
+    // shared memory where each CTA walks at most 48 chunks of 32 slots per colour (planCluster;
+    // 11K-52K monomers: 11.6-15.3 us against 12.9-16.0 persistent); then the persistent sweep
+    // while its tiles fit about three per SM (to 262K monomers: 16-19 us against 18-22 graph);
+    // beyond, the graph of separate launches (1M monomers: 30 us against 36).
     if (residentEligible() && maxGroup_ <= 4u * kResidentBlock) return kModeResident;
-    if (clusterEligible() && clusterPer_ <= 2u) return kModeCluster;
+    if (clusterEligible() && clusterTier_ >= 3) return kModeCluster;
     if (codeMode_ != kCodeNone) {
         uint32_t const tiles = (maxGroup_ + kBcTileSpan - 1) / kBcTileSpan;
         if (tiles <= 3u * smCount_) return kModePersistent;

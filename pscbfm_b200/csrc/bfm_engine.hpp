@@ -124,6 +124,13 @@ public:
     uint32_t maxGroup() const { return maxGroup_; }
     bool residentEligible() const;
     bool clusterEligible() const { return clusterLogC_ != 0; }
+    // the cluster-resident kernel's plan: log2 CTAs per cluster, chunks per warp, shared memory,
+    // and whether BFM_MODE_AUTO (clusterFast) or a Batch (clusterForBatch) takes it (planCluster)
+    uint32_t clusterLogC() const { return clusterLogC_; }
+    uint32_t clusterPer() const { return clusterPer_; }
+    size_t clusterSmem() const { return clusterSmem_; }
+    bool clusterFast() const { return clusterTier_ >= 3; }
+    bool clusterForBatch() const { return clusterTier_ >= 2; }
     int gpu() const { return gpu_; }
     void validate();                         // host-side EV and bond-set check (checkSystem)
 
@@ -219,6 +226,7 @@ private:
     uint32_t clusterLogC_ = 0;                 // cluster of 2^logC CTAs holds the system (0: does not fit)
     uint32_t clusterPer_ = 0;                  // chunks of 32 slots per warp and colour
     size_t clusterSmem_ = 0;                   // dynamic shared memory per CTA
+    uint32_t clusterTier_ = 0;                 // 3: AUTO takes the plan, 2: a Batch does, 1: forced only
     uint32_t hStepCap_ = 0;
     std::vector<std::pair<uint32_t, cudaGraphExec_t>> graphs_;   // captured chunk length -> graph
     cudaEvent_t stepsFree_ = nullptr;          // host staging may be rewritten after this event
@@ -251,8 +259,9 @@ public:
 };
 
 // A set of initialised updaters on one GPU advanced together: systems that fit one CTA run in the
-// resident kernel (one launch per chunk), the others share one grid-phase launch per phase and
-// sub-step, captured into a CUDA graph. Every system keeps its own draw stream, so its
+// resident kernel and systems that fit a cluster of CTAs in the cluster-resident kernel (one
+// launch per run and group), the others share one grid-phase launch per phase and sub-step,
+// captured into a CUDA graph. Every system keeps its own draw stream, so its
 // trajectory is identical to running it alone.
 class Batch {
 public:
@@ -266,12 +275,14 @@ public:
     void setShape(int shape);
     int shape() const { return shape_; }
     bool residentEnabled() const { return residentOn_; }
-    // Runs the members under each configuration (kernel shape x resident path on / off) for
-    // 1 + mcsPerTrial MCS, keeps the fastest per MCS and returns every trial. The MCS count
-    // as ordinary steps of the run: the results do not depend on the configuration.
+    bool clusterEnabled() const { return clusterOn_; }
+    // Runs the members under each configuration (kernel shape x resident path on / off x cluster
+    // path on / off) for 1 + mcsPerTrial MCS, keeps the fastest per MCS and returns every trial.
+    // The MCS count as ordinary steps of the run: the results do not depend on the configuration.
     struct Trial {
         int shape;
         bool resident;
+        bool cluster;
         float msPerMcs;
     };
     std::vector<Trial> autotune(int32_t mcsPerTrial);
@@ -284,8 +295,18 @@ public:
         if (on != residentOn_) built_ = false;
         residentOn_ = on;
     }
+    // members too large for one CTA whose cluster plan beats the grid-phase kernels
+    // (Updater::clusterForBatch: at most two chunks of 32 slots per warp and colour) run in the
+    // cluster-resident kernel, while the batch's clusters take at most half of the SMs (the rest
+    // stay with the grid-phase kernels)
+    void setClusterEnabled(bool on)
+    {
+        if (on != clusterOn_) built_ = false;
+        clusterOn_ = on;
+    }
     cudaStream_t stream() const { return stream_; }
     uint32_t residentCount() const;
+    uint32_t clusterCount() const;
     uint64_t launches() const { return launches_; }
 
 private:
@@ -305,6 +326,17 @@ private:
         uint32_t perThread = 1;
         size_t smem = 0;
     };
+    // members of one representation with the same cluster size, one launch per run on a stream
+    // of their own (side_[side])
+    struct ClusterGroup {
+        uint32_t codeMode;
+        uint32_t logC;
+        std::vector<uint32_t> members;
+        uint32_t* dList = nullptr;
+        uint32_t perThread = 1;
+        size_t smem = 0;
+        size_t side = 0;
+    };
     void rebuild();
     void validateMembers(Updater* const* members, uint32_t n) const;
     cudaError_t launchGrid(StepEntry const* e);   // one sub-step of every grid group, entries [members]
@@ -313,10 +345,15 @@ private:
     void prepare(int32_t const* mcs);            // both, for a run of mcs[i] MCS per member
     int gpu_;
     std::vector<Updater*> members_;
-    std::vector<char> isResident_;
+    std::vector<char> wholeRun_;               // member runs in a resident or cluster kernel
     std::vector<GridGroup> grid_;
     std::vector<ResidentGroup> resident_;
+    std::vector<ClusterGroup> cluster_;
+    std::vector<cudaStream_t> side_;           // streams of the cluster groups (grown, never shrunk)
+    std::vector<cudaEvent_t> sideJoin_;
+    uint32_t smCount_ = 148;
     bool residentOn_ = true;
+    bool clusterOn_ = true;
     bool built_ = false;
     int shape_ = -1;
     cudaStream_t stream_ = nullptr, stream2_ = nullptr;

@@ -67,14 +67,15 @@ cudaError_t launch_sweep_bc(SysDev const& hostDesc, StepEntry const* dSteps, uin
                             uint32_t* gridOut);
 size_t resident_bc_smem_bytes(uint32_t nwords, uint32_t npad, uint32_t maxGroup, uint32_t codeMode);
 // Cluster-resident sweep (bond codes): one cluster of 2^logC CTAs of kResidentBlock threads per
-// system of dList (logC 1..4), state in the cluster's shared memory for nSteps sub-steps; perThread
-// (1, 2, 4, 8) chunks of 32 slots per warp and colour. cluster_bc_runnable: whether the device can
-// run that configuration (kernel attributes set, cudaOccupancyMaxActiveClusters >= 1).
+// system of dList[0..nClusters) (logC 1..4), state in the cluster's shared memory for nSteps
+// sub-steps whose entries are dSteps[t * stride + system]; perThread (1, 2, 4, 8) chunks of 32
+// slots per warp and colour. cluster_bc_runnable: whether the device can run that configuration
+// (kernel attributes set, cudaOccupancyMaxActiveClusters >= 1).
 size_t cluster_bc_smem_bytes(uint32_t nwords, uint32_t npad, uint32_t logC, uint32_t perThread, uint32_t codeMode);
 bool cluster_bc_runnable(uint32_t logC, uint32_t perThread, size_t smem, uint32_t codeMode);
-cudaError_t launch_cluster_bc(SysDev const* dSys, uint32_t const* dList, uint32_t nSys, uint32_t logC,
-                              uint32_t perThread, StepEntry const* dSteps, uint32_t nSteps, size_t smem,
-                              uint32_t codeMode, cudaStream_t s);
+cudaError_t launch_cluster_bc(SysDev const* dSys, uint32_t const* dList, uint32_t nClusters, uint32_t logC,
+                              uint32_t perThread, StepEntry const* dSteps, uint32_t stride, uint32_t nSteps,
+                              size_t smem, uint32_t codeMode, cudaStream_t s);
 cudaError_t launch_resident_bc(SysDev const* dSys, uint32_t const* dList, uint32_t nCta, uint32_t perThread,
                                StepEntry const* dSteps, uint32_t nSys, uint32_t nSteps, size_t smem, uint32_t codeMode,
                                cudaStream_t s);

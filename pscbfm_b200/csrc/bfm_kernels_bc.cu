@@ -693,12 +693,13 @@ __device__ __forceinline__ void dsmem_xor(unsigned long long* p, unsigned long l
 // per sub-step (after the check, after the perform, after the temporary lattice is cleared) take
 // the place of the resident kernel's CTA barriers; every CTA of a cluster runs the same system and
 // so reaches the same barriers. A CTA leaves only after the last barrier, when no other CTA
-// accesses its shared memory any more. Grid: one cluster per system of sysList.
+// accesses its shared memory any more. Grid: one cluster per system of sysList; the entries of
+// sub-step t are steps[t * stride + system].
 template <typename W, int K>
 __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* __restrict__ sysv,
                                                                    uint32_t const* __restrict__ sysList,
                                                                    StepEntry const* __restrict__ steps,
-                                                                   uint32_t nSys, uint32_t nSteps)
+                                                                   uint32_t stride, uint32_t nSteps)
 {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
@@ -749,7 +750,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
     StepEntry next = nSteps ? steps[sysId] : StepEntry{};
     for (uint32_t t = 0; t < nSteps; ++t) {
         StepEntry const st = next;
-        if (t + 1 < nSteps) next = steps[(size_t)(t + 1) * nSys + sysId];   // prefetch
+        if (t + 1 < nSteps) next = steps[(size_t)(t + 1) * stride + sysId];   // prefetch
         if (st.color == kNoColor) continue;
         if (rank == 0) nAtt += st.cnt;
         // check: this CTA's chunks of 32 slots of the colour group (the group starts at a chunk)
@@ -1122,7 +1123,7 @@ namespace {
 
 template <typename W, int K>
 cudaError_t cluster_bc_config(uint32_t logC, size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribute* attr,
-                              uint32_t nSys, cudaStream_t s, bool& runnable)
+                              uint32_t nClusters, cudaStream_t s, bool& runnable)
 {
     auto kernel = k_cluster_bc<W, K>;
     uint32_t const C = 1u << logC;
@@ -1137,7 +1138,7 @@ cudaError_t cluster_bc_config(uint32_t logC, size_t smem, cudaLaunchConfig_t& cf
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg = {};
-    cfg.gridDim = dim3(nSys * C);
+    cfg.gridDim = dim3(nClusters * C);
     cfg.blockDim = dim3(kResidentBlock);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
@@ -1150,28 +1151,29 @@ cudaError_t cluster_bc_config(uint32_t logC, size_t smem, cudaLaunchConfig_t& cf
 }
 
 template <typename W, int K>
-cudaError_t launch_cluster_bc_k(SysDev const* dSys, uint32_t const* dList, uint32_t nSys, uint32_t logC,
-                                StepEntry const* dSteps, uint32_t nSteps, size_t smem, cudaStream_t s)
+cudaError_t launch_cluster_bc_k(SysDev const* dSys, uint32_t const* dList, uint32_t nClusters, uint32_t logC,
+                                StepEntry const* dSteps, uint32_t stride, uint32_t nSteps, size_t smem,
+                                cudaStream_t s)
 {
     cudaLaunchConfig_t cfg;
     cudaLaunchAttribute attr[1];
     bool runnable = false;
-    cudaError_t e = cluster_bc_config<W, K>(logC, smem, cfg, attr, nSys, s, runnable);
+    cudaError_t e = cluster_bc_config<W, K>(logC, smem, cfg, attr, nClusters, s, runnable);
     if (e != cudaSuccess) return e;
     if (!runnable) return cudaErrorInvalidConfiguration;
-    return cudaLaunchKernelEx(&cfg, k_cluster_bc<W, K>, dSys, dList, dSteps, nSys, nSteps);
+    return cudaLaunchKernelEx(&cfg, k_cluster_bc<W, K>, dSys, dList, dSteps, stride, nSteps);
 }
 
 template <typename W>
-cudaError_t launch_cluster_bc_w(SysDev const* dSys, uint32_t const* dList, uint32_t nSys, uint32_t logC,
-                                uint32_t perThread, StepEntry const* dSteps, uint32_t nSteps, size_t smem,
-                                cudaStream_t s)
+cudaError_t launch_cluster_bc_w(SysDev const* dSys, uint32_t const* dList, uint32_t nClusters, uint32_t logC,
+                                uint32_t perThread, StepEntry const* dSteps, uint32_t stride, uint32_t nSteps,
+                                size_t smem, cudaStream_t s)
 {
     switch (perThread) {
-    case 1: return launch_cluster_bc_k<W, 1>(dSys, dList, nSys, logC, dSteps, nSteps, smem, s);
-    case 2: return launch_cluster_bc_k<W, 2>(dSys, dList, nSys, logC, dSteps, nSteps, smem, s);
-    case 4: return launch_cluster_bc_k<W, 4>(dSys, dList, nSys, logC, dSteps, nSteps, smem, s);
-    case 8: return launch_cluster_bc_k<W, 8>(dSys, dList, nSys, logC, dSteps, nSteps, smem, s);
+    case 1: return launch_cluster_bc_k<W, 1>(dSys, dList, nClusters, logC, dSteps, stride, nSteps, smem, s);
+    case 2: return launch_cluster_bc_k<W, 2>(dSys, dList, nClusters, logC, dSteps, stride, nSteps, smem, s);
+    case 4: return launch_cluster_bc_k<W, 4>(dSys, dList, nClusters, logC, dSteps, stride, nSteps, smem, s);
+    case 8: return launch_cluster_bc_k<W, 8>(dSys, dList, nClusters, logC, dSteps, stride, nSteps, smem, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1204,16 +1206,17 @@ bool cluster_bc_runnable(uint32_t logC, uint32_t perThread, size_t smem, uint32_
     return false;
 }
 
-cudaError_t launch_cluster_bc(SysDev const* dSys, uint32_t const* dList, uint32_t nSys, uint32_t logC,
-                              uint32_t perThread, StepEntry const* dSteps, uint32_t nSteps, size_t smem,
-                              uint32_t codeMode, cudaStream_t s)
+cudaError_t launch_cluster_bc(SysDev const* dSys, uint32_t const* dList, uint32_t nClusters, uint32_t logC,
+                              uint32_t perThread, StepEntry const* dSteps, uint32_t stride, uint32_t nSteps,
+                              size_t smem, uint32_t codeMode, cudaStream_t s)
 {
-    if (nSys == 0 || nSteps == 0) return cudaSuccess;
+    if (nClusters == 0 || nSteps == 0) return cudaSuccess;
     if (logC < 1 || logC > 4 || smem > kResidentMaxSmem) return cudaErrorInvalidValue;
     if (codeMode == kCode32)
-        return launch_cluster_bc_w<uint32_t>(dSys, dList, nSys, logC, perThread, dSteps, nSteps, smem, s);
+        return launch_cluster_bc_w<uint32_t>(dSys, dList, nClusters, logC, perThread, dSteps, stride, nSteps, smem, s);
     if (codeMode == kCode64)
-        return launch_cluster_bc_w<unsigned long long>(dSys, dList, nSys, logC, perThread, dSteps, nSteps, smem, s);
+        return launch_cluster_bc_w<unsigned long long>(dSys, dList, nClusters, logC, perThread, dSteps, stride, nSteps,
+                                                       smem, s);
     return cudaErrorInvalidValue;
 }
 

@@ -333,7 +333,7 @@ class UpdaterGPUScBFM_AB_Type:
 class Batch:
     """Many initialised updaters on one GPU advanced together (include/bfm.h, bfm_batch_*)."""
 
-    def __init__(self, members, gpu: int = 0, resident: bool = True):
+    def __init__(self, members, gpu: int = 0, resident: bool = True, cluster: bool = True):
         self._L = _lib.load()
         self.members = list(members)
         arr = (C.c_void_p * len(self.members))(*[m.handle for m in self.members])
@@ -344,6 +344,8 @@ class Batch:
         self._h = h
         if not resident:
             self._call("bfm_batch_set_resident", 0)
+        if not cluster:
+            self._call("bfm_batch_set_cluster", 0)
 
     def _call(self, name, *args):
         st = getattr(self._L, name)(self._h, *args)
@@ -361,17 +363,23 @@ class Batch:
         self._call("bfm_batch_set_shape", shape)
 
     def autotune(self, mcs_per_trial: int = 10) -> dict:
-        """Tries every configuration (kernel shape x resident path on / off) for 1 + mcs_per_trial
-        MCS each and keeps the fastest. The trials advance every member (the results do not depend
-        on the configuration)."""
+        """Tries every configuration (kernel shape x resident path on / off x cluster path on / off)
+        for 1 + mcs_per_trial MCS each and keeps the fastest. The trials advance every member (the
+        results do not depend on the configuration)."""
         trials = np.zeros(3 * 16, dtype=np.float32)
-        shape, resident, best, n = C.c_int(), C.c_int(), C.c_float(), C.c_uint32()
-        self._call("bfm_batch_autotune", mcs_per_trial, C.byref(shape), C.byref(resident), C.byref(best), trials,
+        shape, paths, best, n = C.c_int(), C.c_int(), C.c_float(), C.c_uint32()
+        self._call("bfm_batch_autotune", mcs_per_trial, C.byref(shape), C.byref(paths), C.byref(best), trials,
                    16, C.byref(n))
         rows = trials[:3 * min(n.value, 16)].reshape(-1, 3)
-        return {"shape": shape.value, "resident": bool(resident.value), "ms_per_mcs": best.value,
-                "mcs_spent": n.value * (1 + mcs_per_trial),
-                "trials": [{"shape": int(r[0]), "resident": bool(r[1]), "ms_per_mcs": float(r[2])} for r in rows]}
+        return {"shape": shape.value, "resident": bool(paths.value & 1), "cluster": bool(paths.value & 2),
+                "ms_per_mcs": best.value, "mcs_spent": n.value * (1 + mcs_per_trial),
+                "trials": [{"shape": int(r[0]), "resident": bool(int(r[1]) & 1), "cluster": bool(int(r[1]) & 2),
+                            "ms_per_mcs": float(r[2])} for r in rows]}
+
+    def set_cluster(self, on: bool):
+        """Members too large for one CTA that a cluster of CTAs holds run in the cluster-resident
+        kernel (default on); off: they share the grid-phase kernels. Results do not change."""
+        self._call("bfm_batch_set_cluster", 1 if on else 0)
 
     def run_each(self, mcs):
         """Member i advances mcs[i] MCS (0: it idles)."""

@@ -225,8 +225,8 @@ def test_set_coords_after_initialize():
     assert np.array_equal(got, ref)
 
 
-@pytest.mark.parametrize("resident", [True, False])
-def test_batch_equals_each_system_alone(resident):
+@pytest.mark.parametrize("resident,cluster", [(True, True), (False, True), (True, False)])
+def test_batch_equals_each_system_alone(resident, cluster):
     systems = S.ensemble(n_systems=20)
     systems.append(S.rings_and_free())         # three colours in the mix
     systems.append(S.crosslinked_network())    # 64-bit bond codes in the mix
@@ -236,7 +236,7 @@ def test_batch_equals_each_system_alone(resident):
     for s in systems[:2]:
         members.append(P.UpdaterGPUScBFM_AB_Type(0).load_system(s, representation=P.REPR_GATHER))
     systems = systems + systems[:2]
-    b = P.Batch(members, resident=resident)
+    b = P.Batch(members, resident=resident, cluster=cluster)
     b.run(60)
     b.run(40)
     for s, m in zip(systems, members):
@@ -255,8 +255,10 @@ def test_batch_autotune_keeps_trajectories():
     members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
     b = P.Batch(members)
     rep = b.autotune(3)
-    assert len(rep["trials"]) == 8 and rep["mcs_spent"] == 8 * 4
-    assert {(t["shape"], t["resident"]) for t in rep["trials"]} == {(s, r) for s in range(4) for r in (True, False)}
+    # the network runs in a cluster of CTAs alone, so the cluster path is a dimension of the trials
+    assert len(rep["trials"]) == 16 and rep["mcs_spent"] == 16 * 4
+    assert {(t["shape"], t["resident"], t["cluster"]) for t in rep["trials"]} == \
+        {(s, r, c) for s in range(4) for r in (True, False) for c in (True, False)}
     assert rep["ms_per_mcs"] == min(t["ms_per_mcs"] for t in rep["trials"])
     b.run(17)
     for s, m in zip(systems, members):
@@ -264,6 +266,43 @@ def test_batch_autotune_keeps_trajectories():
         assert np.array_equal(m.get_coords(), ref), s.name
         m.validate()
     b.close()
+    for m in members:
+        m.close()
+
+
+@pytest.mark.parametrize("cluster", [True, False])
+def test_batch_cluster_members_vs_oracle(cluster):
+    """Members too large for one CTA that a cluster of CTAs holds run in the cluster-resident kernel
+    inside a batch (one launch per run and cluster size, entries strided by the member count),
+    beside resident and grid-phase members, with uneven MCS per member: every trajectory equals the
+    oracle's."""
+    systems = [S.crosslinked_network(), S.serpentine_chains(64, 64, 0.8, seed=13), S.small_chains(),
+               S.serpentine_chains(128, 64, 0.3, seed=3), S.serpentine_chains(128, 32, 0.1, seed=17)]
+    members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
+    b = P.Batch(members, cluster=cluster)
+    plan = [[40, 7, 25, 3, 0], [0, 33, 25, 12, 41]]
+    for mcs in plan:
+        b.run_each(mcs)
+    totals = np.sum(plan, axis=0)
+    for s, m, t in zip(systems, members, totals):
+        ref, _ = O.run(s, int(t))
+        assert np.array_equal(m.get_coords(), ref), s.name
+        assert m.stats()["mcs"] == t
+        m.validate()
+    b.close()
+    # the two cluster members alone: one launch per cluster size and run, not two per sub-step
+    pair = P.Batch(members[:2], cluster=cluster)
+    n0 = pair.launch_count()
+    pair.run(5)
+    launched = pair.launch_count() - n0
+    if cluster:
+        assert launched <= 2
+    else:
+        assert launched >= 2 * 5 * 2   # a check and a perform per sub-step, two colours or more
+    pair.close()
+    for s, m, t in zip(systems[:2], members[:2], totals[:2]):
+        ref, _ = O.run(s, int(t) + 5)
+        assert np.array_equal(m.get_coords(), ref), s.name
     for m in members:
         m.close()
 
