@@ -416,25 +416,32 @@ def run_ours(args):
                           "source": f"ncu lts__throughput.avg.pct_of_peak_sustained_elapsed, profiles/{key}.md"}
 
     # e2e through the C-ABI with host buffers: per step one run of 1 MCS (its sub-steps' draw
-    # entries uploaded from pinned memory) and a read of the move counters, which waits for the
-    # step; the positions, in the caller's order, copied back into a pinned host array at the end
+    # entries uploaded from pinned memory) and a read of that step's move counters, which waits
+    # for the step; the host queues step t + 1 before it waits for step t's counters, so one step
+    # is in flight while it reads; the positions, in the caller's order, copied back into a pinned
+    # host array at the end
     host_xyz = torch.empty((systems[0].n, 3), dtype=torch.int32, pin_memory=True).numpy()
     torch.cuda.synchronize()
     t = time.perf_counter()
+    prev = None
     for _ in range(args.steps):
         if batch is None:
             u0.run_async(1)
         else:
-            batch.run(1)
-        u0.stats()
+            batch.run_async(1)
+        ticket = u0.stats_async()
+        if prev is not None:
+            u0.stats_wait(prev)
+        prev = ticket
+    u0.stats_wait(prev)
     u0.get_coords(host_xyz)
     e2e_s = time.perf_counter() - t
     e2e_value = world * moves / reduce_max(e2e_s, world)
     e2e = {"value": e2e_value, "unit": "attempted moves/s",
            "h2d_bytes_per_step": STEP_ENTRY_BYTES * sum(colours),
            "d2h_bytes_per_step": STATS_BYTES + round(12 * systems[0].n / args.steps),
-           "calls": "bfm_run_async(1) + bfm_get_stats per step (the counter read waits for the step), "
-                    "bfm_get_coords_bulk once into pinned memory"}
+           "calls": "bfm_run_async(1) + bfm_stats_enqueue per step, bfm_stats_wait on the previous step's "
+                    "ticket (one step in flight), bfm_get_coords_bulk once into pinned memory"}
 
     for m in members:
         m.validate()   # excluded volume, bonds and the device lattice after the timed run

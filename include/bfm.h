@@ -152,6 +152,13 @@ int bfm_n_colors(bfm_handle h, uint32_t* n_colors, uint32_t* sizes, uint32_t cap
 /* Counters since initialize: attempted moves, tentatively accepted (check passed), accepted,
  * MCS done. */
 int bfm_get_stats(bfm_handle h, uint64_t out[4]);
+/* The same counters without waiting for later work (no reference counterpart): bfm_stats_enqueue
+ * queues their copy after the work queued so far on the handle's stream and returns a ticket;
+ * bfm_stats_wait waits for that copy only, while work queued after it keeps running, and writes the
+ * counters as they stood then. The last 8 tickets of a handle stay valid; an older or unknown
+ * ticket is BFM_ERR_INVALID_ARGUMENT. */
+int bfm_stats_enqueue(bfm_handle h, uint64_t* ticket);
+int bfm_stats_wait(bfm_handle h, uint64_t ticket, uint64_t out[4]);
 /* checkSystem (UpdaterGPUScBFM_AB_Type.cu:882-986): excluded volume and bond set on the host. */
 int bfm_validate(bfm_handle h);
 /* Device bytes held by the handle. */

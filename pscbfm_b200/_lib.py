@@ -88,6 +88,8 @@ _SIGS = {
     "bfm_get_coords_bulk": [H, _i32p, C.c_uint32],
     "bfm_n_colors": [H, C.POINTER(C.c_uint32), C.c_void_p, C.c_uint32],
     "bfm_get_stats": [H, C.POINTER(C.c_uint64)],   # a ctypes buffer: read once per step by callers
+    "bfm_stats_enqueue": [H, C.POINTER(C.c_uint64)],
+    "bfm_stats_wait": [H, C.c_uint64, C.POINTER(C.c_uint64)],
     "bfm_validate": [H],
     "bfm_device_bytes": [H, C.POINTER(C.c_uint64)],
     "bfm_run_timed": [H, C.c_int32, C.POINTER(C.c_float)],

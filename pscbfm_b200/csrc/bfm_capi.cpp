@@ -210,6 +210,20 @@ int bfm_get_stats(bfm_handle h, uint64_t out[4])
         h->u.stats(out);
     });
 }
+int bfm_stats_enqueue(bfm_handle h, uint64_t* ticket)
+{
+    BFM_CALL(h, {
+        if (!ticket) throw std::invalid_argument("[bfm_stats_enqueue] null output");
+        *ticket = h->u.statsEnqueue();
+    });
+}
+int bfm_stats_wait(bfm_handle h, uint64_t ticket, uint64_t out[4])
+{
+    BFM_CALL(h, {
+        if (!out) throw std::invalid_argument("[bfm_stats_wait] null output");
+        h->u.statsWait(ticket, out);
+    });
+}
 int bfm_validate(bfm_handle h) { BFM_CALL(h, h->u.validate()); }
 int bfm_device_bytes(bfm_handle h, uint64_t* out)
 {

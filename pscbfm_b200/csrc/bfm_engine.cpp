@@ -8,6 +8,7 @@
 #include "bfm_engine.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <sstream>
@@ -768,11 +769,17 @@ void Updater::ensureStaging()
     // one extra entry holds the copy of the persistent kernel's barrier state, and after it the
     // copy of the move counters
     static_assert(sizeof(GridSync) <= sizeof(StepEntry), "GridSync fits one staging entry");
-    cuda_check(cudaMallocHost(&hSteps_, sizeof(StepEntry) * (kStepCap + 1) + kStatBytes), "cudaMallocHost(steps)");
+    void* p = nullptr;
+    cuda_check(cudaHostAlloc(&p, sizeof(StepEntry) * (kStepCap + 1) + kStatBytes, cudaHostAllocMapped),
+               "cudaHostAlloc(steps)");
+    hSteps_ = static_cast<StepEntry*>(p);
     hStepCap_ = kStepCap;
     hGs_ = reinterpret_cast<GridSync*>(hSteps_ + kStepCap);
     std::memset(hGs_, 0, sizeof(GridSync));
     hStats_ = reinterpret_cast<unsigned long long*>(hSteps_ + kStepCap + 1);
+    void* d = nullptr;
+    cuda_check(cudaHostGetDevicePointer(&d, hStats_, 0), "stats staging device address");
+    dStats_ = static_cast<unsigned long long*>(d);
 }
 
 void Updater::scrubPending(cudaStream_t s)
@@ -1229,17 +1236,51 @@ std::vector<uint32_t> Updater::groupSizes() const
 void Updater::stats(uint64_t out[4])
 {
     requireInit("stats");
-    // into the pinned staging where this system has it (a copy to pageable memory is staged by
-    // the driver and costs more per call)
-    unsigned long long local[3 * kStatSlots];
-    unsigned long long* const slots = hStats_ ? hStats_ : local;
-    cuda_check(cudaMemcpyAsync(slots, dev_.h.stats, kStatBytes, cudaMemcpyDeviceToHost, stream_), "stats");
+    // the sums written into the mapped pinned staging by a kernel on the stream
+    ensureStaging();
+    cuda_check(launch_publish_stats(dev_.h.stats, dStats_, stream_), "stats");
     cuda_check(cudaStreamSynchronize(stream_), "stats");
-    for (uint32_t c = 0; c < 3; ++c) {
-        out[c] = 0;
-        for (uint32_t s = 0; s < kStatSlots; ++s) out[c] += slots[c * kStatSlots + s];
-    }
+    std::atomic_thread_fence(std::memory_order_acquire);
+    unsigned long long const volatile* const sums = hStats_;
+    for (uint32_t c = 0; c < 3; ++c) out[c] = sums[c];
     out[3] = mcsDone_;
+}
+
+uint64_t Updater::statsEnqueue()
+{
+    requireInit("stats");
+    if (!hStatRing_) {
+        void* p = nullptr;
+        cuda_check(cudaHostAlloc(&p, 4 * sizeof(unsigned long long) * kStatRing, cudaHostAllocMapped),
+                   "cudaHostAlloc(stats ring)");
+        hStatRing_ = static_cast<unsigned long long*>(p);
+        void* d = nullptr;
+        cuda_check(cudaHostGetDevicePointer(&d, p, 0), "stats ring device address");
+        dStatRing_ = static_cast<unsigned long long*>(d);
+        for (cudaEvent_t& e : statEv_) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    // a slot's previous write precedes this one on the stream, so the slot is reused in order; the
+    // sums are written into host memory by a kernel (no copy-engine transfer between the kernels)
+    uint64_t const t = ++statNext_;
+    uint32_t const k = (uint32_t)(t % kStatRing);
+    cuda_check(launch_publish_stats(dev_.h.stats, dStatRing_ + 4ull * k, stream_), "stats");
+    cuda_check(cudaEventRecord(statEv_[k], stream_), "event");
+    statTicket_[k] = t;
+    statMcs_[k] = mcsDone_;
+    return t;
+}
+
+void Updater::statsWait(uint64_t ticket, uint64_t out[4])
+{
+    requireInit("stats");
+    uint32_t const k = (uint32_t)(ticket % kStatRing);
+    if (ticket == 0 || !hStatRing_ || statTicket_[k] != ticket)
+        throw std::invalid_argument("[stats] unknown ticket, or one older than the last 8 of this system");
+    cuda_check(cudaEventSynchronize(statEv_[k]), "stats");
+    std::atomic_thread_fence(std::memory_order_acquire);
+    unsigned long long const volatile* const slot = hStatRing_ + 4ull * k;
+    for (uint32_t c = 0; c < 3; ++c) out[c] = slot[c];
+    out[3] = statMcs_[k];
 }
 
 void Updater::validate()
@@ -1338,12 +1379,24 @@ void Updater::freeDevice()
         hSteps_ = nullptr;
         hGs_ = nullptr;
         hStats_ = nullptr;
+        dStats_ = nullptr;
         gsPending_ = false;
         hStepCap_ = 0;
     }
     if (stepsFree_) {
         cudaEventDestroy(stepsFree_);
         stepsFree_ = nullptr;
+    }
+    if (hStatRing_) {
+        for (cudaEvent_t& e : statEv_) {
+            if (e) cudaEventSynchronize(e);
+            if (e) cudaEventDestroy(e);
+            e = nullptr;
+        }
+        cudaFreeHost(hStatRing_);
+        hStatRing_ = nullptr;
+        dStatRing_ = nullptr;
+        for (uint32_t k = 0; k < kStatRing; ++k) statTicket_[k] = 0;
     }
 }
 

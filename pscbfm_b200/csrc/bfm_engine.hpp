@@ -113,6 +113,12 @@ public:
     uint32_t nColors() const;
     std::vector<uint32_t> groupSizes() const;
     void stats(uint64_t out[4]);             // attempted, tentative, accepted, MCS done
+    // the counters read without waiting for later work: statsEnqueue queues their copy after the
+    // work queued so far and returns a ticket, statsWait waits for that copy only (the last
+    // kStatRing tickets stay valid)
+    static constexpr uint32_t kStatRing = 8;
+    uint64_t statsEnqueue();
+    void statsWait(uint64_t ticket, uint64_t out[4]);
     uint64_t substep() const { return subStep_; }
     uint64_t mcsDone() const { return mcsDone_; }
     uint64_t subStep() const { return subStep_; }
@@ -220,6 +226,11 @@ private:
     StepEntry* hSteps_ = nullptr;              // pinned staging for step entries
     GridSync* hGs_ = nullptr;                  // pinned copy of the persistent kernel's barrier state
     unsigned long long* hStats_ = nullptr;     // pinned copy of the move counters (stats)
+    unsigned long long* hStatRing_ = nullptr;  // kStatRing mapped pinned slots (statsEnqueue)
+    unsigned long long* dStatRing_ = nullptr;  // the same, as the device addresses them
+    unsigned long long* dStats_ = nullptr;     // hStats_ as the device addresses it
+    cudaEvent_t statEv_[kStatRing] = {};
+    uint64_t statTicket_[kStatRing] = {}, statMcs_[kStatRing] = {}, statNext_ = 0;
     bool gsPending_ = false;                   // hGs_ is being refreshed by the stream
     bool stallNext_ = false;                   // injectBarrierStall
     uint32_t smCount_ = 148;                   // SMs of the device (setGpu)

@@ -330,6 +330,19 @@ __global__ void k_gather_positions(int32_t const* __restrict__ x, int32_t const*
     }
 }
 
+// One warp: each counter's slots summed with a warp reduction, written to host memory. The host
+// reads them only after an event behind this kernel has completed, so no fence is needed here.
+__global__ void k_publish_stats(unsigned long long const* __restrict__ stats, unsigned long long* __restrict__ out)
+{
+    uint32_t const lane = threadIdx.x;
+    for (uint32_t c = 0; c < 3; ++c) {
+        unsigned long long v = 0;
+        for (uint32_t k = lane; k < kStatSlots; k += 32) v += stats[c * kStatSlots + k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) out[c] = v;
+    }
+}
+
 // ------------------------------------------------------------------------ launchers
 
 cudaError_t launch_check(SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles, uint32_t tileSpan,
@@ -394,6 +407,12 @@ cudaError_t launch_gather_positions(SysDev const& h, uint32_t const* slotOf, uin
     uint32_t const grid = std::min((n + block - 1) / block, 148u * 8u);
     if (grid == 0) return cudaSuccess;
     k_gather_positions<<<grid, block, 0, s>>>(h.x, h.y, h.z, slotOf, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_publish_stats(unsigned long long const* stats, unsigned long long* out, cudaStream_t s)
+{
+    k_publish_stats<<<1, 32, 0, s>>>(stats, out);
     return cudaGetLastError();
 }
 

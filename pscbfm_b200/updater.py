@@ -242,6 +242,23 @@ class UpdaterGPUScBFM_AB_Type:
         self._call("bfm_get_stats", out)
         return {"attempted": out[0], "tentative": out[1], "accepted": out[2], "mcs": out[3]}
 
+    def stats_async(self) -> int:
+        """Queues a copy of the move counters after the work queued so far; returns a ticket for
+        stats_wait (the last 8 tickets stay valid)."""
+        t = self.__dict__.get("_ticket_buf")
+        if t is None:
+            t = self._ticket_buf = C.c_uint64()
+        self._call("bfm_stats_enqueue", C.byref(t))
+        return t.value
+
+    def stats_wait(self, ticket: int) -> dict:
+        """The counters as they stood when the ticket was queued; waits for that copy only."""
+        out = self.__dict__.get("_wait_buf")
+        if out is None:
+            out = self._wait_buf = (C.c_uint64 * 4)()
+        self._call("bfm_stats_wait", ticket, out)
+        return {"attempted": out[0], "tentative": out[1], "accepted": out[2], "mcs": out[3]}
+
     def validate(self):
         self._call("bfm_validate")
 

@@ -196,3 +196,36 @@ def test_auto_mode_picks_the_path_by_size():
     u.set_mode(P.MODE_PERSISTENT)
     assert u.path() == P.MODE_GRAPH      # a mode the system cannot use falls back to the graph
     u.close()
+
+
+def test_stats_read_without_waiting_for_later_work():
+    """bfm_stats_enqueue / bfm_stats_wait: each ticket gives the counters as they stood when it was
+    queued, while later runs stay queued; the counters equal a synchronous read after the same MCS
+    on an identical system; tickets older than the last 8 are refused."""
+    s = S.small_chains()
+    a = fresh()
+    a.load_system(s, mode=P.MODE_GRAPH)
+    b = fresh()
+    b.load_system(s, mode=P.MODE_GRAPH)
+    tickets = []
+    for _ in range(3):
+        a.run_async(4)
+        tickets.append(a.stats_async())
+    a.run_async(50)   # queued behind the third copy
+    seen = []
+    for t in tickets:
+        seen.append(a.stats_wait(t))
+    for k, got in enumerate(seen):
+        b.runSimulationOnGPU(4)
+        want = b.stats()
+        assert got == want and got["mcs"] == 4 * (k + 1)
+    a.synchronize()
+    assert a.stats()["mcs"] == 62
+    for _ in range(8):
+        a.stats_async()
+    with pytest.raises(ValueError):
+        a.stats_wait(tickets[0])
+    with pytest.raises(ValueError):
+        a.stats_wait(0)
+    a.close()
+    b.close()
