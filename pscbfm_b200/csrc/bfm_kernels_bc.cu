@@ -689,10 +689,11 @@ __device__ __forceinline__ void dsmem_xor(unsigned long long* p, unsigned long l
 // temporary lattice, addresses and codes fit their shared memory together, for a whole run of
 // sub-steps (layout: cluster_word_rank, cluster_slot_rank). Each CTA checks the slots it holds,
 // lists its own tentative movers and performs them; lattice and temporary words and neighbours'
-// codes held by another CTA are reached through distributed shared memory. Three cluster barriers
-// per sub-step (after the check, after the perform, after the temporary lattice is cleared) take
-// the place of the resident kernel's CTA barriers; every CTA of a cluster runs the same system and
-// so reaches the same barriers. A CTA leaves only after the last barrier, when no other CTA
+// codes held by another CTA are reached through distributed shared memory. Two cluster barriers
+// per sub-step (after the check, after the perform) take the place of the resident kernel's CTA
+// barriers; the temporary lattice has one copy per sub-step parity, each CTA clearing its words of
+// the previous one while it checks. Every CTA of a cluster runs the same system and so reaches
+// the same barriers. A CTA leaves only after the last barrier, when no other CTA
 // accesses its shared memory any more. Grid: one cluster per system of sysList; the entries of
 // sub-step t are steps[t * stride + system].
 template <typename W, int K>
@@ -707,7 +708,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
     uint32_t logC = 0;
     while ((1u << logC) < C) ++logC;   // a power of two (launch_cluster_bc)
     __shared__ SysDev S;
-    __shared__ uint32_t listCount;
+    __shared__ uint32_t listCount[2];   // per sub-step parity
     extern __shared__ unsigned long long smem[];
     uint32_t const sysId = sysList[blockIdx.x >> logC];
     copy_desc(S, sysv + sysId);
@@ -717,8 +718,8 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
     unsigned long long* const ptab = smem;                                   // 768 plane masks
     uint32_t* const dtab = reinterpret_cast<uint32_t*>(smem + 768);          // kDirTab words
     unsigned long long* const lat = smem + 768 + kDirTab / 2;                // nwC words
-    unsigned long long* const tmp = lat + nwC;                               // nwC words
-    W* const code = reinterpret_cast<W*>(tmp + nwC);                         // cap slots
+    unsigned long long* const tmp = lat + nwC;                               // 2 x nwC words
+    W* const code = reinterpret_cast<W*>(tmp + 2u * nwC);                    // cap slots
     uint32_t* const pk = reinterpret_cast<uint32_t*>(code + cap);            // cap slots
     uint8_t* const mok = reinterpret_cast<uint8_t*>(pk + cap);               // 512 move-table bytes
     uint32_t* const list = reinterpret_cast<uint32_t*>(mok + 512);           // K x 1024 entries
@@ -729,6 +730,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
     for (uint32_t l = tid; l < nwC; l += B) {
         lat[l] = S.lat[(l << logC) | rank];
         tmp[l] = 0ull;
+        tmp[nwC + l] = 0ull;
     }
     for (uint32_t l = tid; l < cap; l += B) {
         uint32_t const g = cluster_slot_of(l, rank, logC);
@@ -736,11 +738,16 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
         code[l] = in ? gcode[g] : W(0);
         pk[l] = in ? S.pk[g] : 0u;
     }
-    if (tid == 0) listCount = 0;
+    if (tid < 2) listCount[tid] = 0;
     cluster.sync();   // every CTA's part of the state is in place before any remote access
 
     auto latAt = [&](uint32_t w) { return cluster.map_shared_rank(lat + (w >> logC), w & (C - 1u)); };
-    auto tmpAt = [&](uint32_t w) { return cluster.map_shared_rank(tmp + (w >> logC), w & (C - 1u)); };
+    // the temporary lattice and the list count alternate with the parity of the sub-steps run, so
+    // each CTA clears the previous sub-step's words while it checks: two cluster barriers per
+    // sub-step (after the check, after the perform)
+    auto tmpAt = [&](uint32_t par, uint32_t w) {
+        return cluster.map_shared_rank(tmp + par * nwC + (w >> logC), w & (C - 1u));
+    };
     auto codeAt = [&](uint32_t g) {
         return cluster.map_shared_rank(code + cluster_slot_local(g, logC), cluster_slot_rank(g, logC));
     };
@@ -748,11 +755,16 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
     uint32_t nTent = 0, nAcc = 0;
     unsigned long long nAtt = 0;
     StepEntry next = nSteps ? steps[sysId] : StepEntry{};
+    uint32_t par = 0;
     for (uint32_t t = 0; t < nSteps; ++t) {
         StepEntry const st = next;
         if (t + 1 < nSteps) next = steps[(size_t)(t + 1) * stride + sysId];   // prefetch
         if (st.color == kNoColor) continue;
         if (rank == 0) nAtt += st.cnt;
+        // the previous sub-step's marks and list count: no CTA reads them after the barrier that
+        // ended that sub-step, and none writes them before the barrier that ends this one
+        for (uint32_t l = tid; l < nwC; l += B) tmp[(par ^ 1u) * nwC + l] = 0ull;
+        if (tid == 0) listCount[par ^ 1u] = 0;
         // check: this CTA's chunks of 32 slots of the colour group (the group starts at a chunk)
         uint32_t const end = st.off + st.cnt, c0 = st.off >> 5, cEnd = (end + 31u) >> 5;
         uint32_t const cFirst = c0 + ((rank - c0) & (C - 1u));
@@ -776,7 +788,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
                         if (pl.m[r]) hit |= *latAt(pl.w[r]) & pl.m[r];
                     if (hit == 0ull) {
                         uint32_t const to = addr_add(p, D.ma, D.step);
-                        dsmem_or64(tmpAt(to >> 6), 1ull << (to & 63u));
+                        dsmem_or64(tmpAt(par, to >> 6), 1ull << (to & 63u));
                         go = true;
                         entry = l | (dir << kSlotShift);
                     }
@@ -785,7 +797,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
             uint32_t const bal = __ballot_sync(0xffffffffu, go);
             if (bal) {
                 uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(&listCount, (uint32_t)__popc(bal));
+                if (lane == 0) base = atomicAdd(&listCount[par], (uint32_t)__popc(bal));
                 base = __shfl_sync(0xffffffffu, base, 0);
                 if (go) list[base + __popc(bal & ((1u << lane) - 1u))] = entry;
                 nTent += lane == 0 ? (uint32_t)__popc(bal) : 0u;
@@ -793,7 +805,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
         }
         cluster.sync();   // every CTA's marks are in place
         // perform over this CTA's list
-        uint32_t const nList = listCount;
+        uint32_t const nList = listCount[par];
         for (uint32_t e = tid; e < nList; e += B) {
             uint32_t const l = list[e] & kSlotMask, dir = list[e] >> kSlotShift;
             uint32_t const g = cluster_slot_of(l, rank, logC);
@@ -808,7 +820,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
             unsigned long long hit = 0ull;
 #pragma unroll
             for (int r = 0; r < 4; ++r)
-                if (pl.m[r]) hit |= *tmpAt(pl.w[r]) & pl.m[r];
+                if (pl.m[r]) hit |= *tmpAt(par, pl.w[r]) & pl.m[r];
             if (hit != 0ull) continue;
             uint32_t const a = dir >> 1;
             int32_t const s = (dir & 1u) ? 1 : -1;
@@ -836,10 +848,8 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
             }
             ++nAcc;
         }
-        cluster.sync();   // every perform has read the temporary lattice
-        for (uint32_t l = tid; l < nwC; l += B) tmp[l] = 0ull;
-        if (tid == 0) listCount = 0;
-        cluster.sync();
+        cluster.sync();   // every perform is done: the lattice is settled for the next check
+        par ^= 1u;
     }
     // after the last cluster barrier no CTA reaches into another's shared memory
     W* const gcodeOut = static_cast<W*>(S.code);
@@ -1115,7 +1125,7 @@ size_t cluster_bc_smem_bytes(uint32_t nwords, uint32_t npad, uint32_t logC, uint
 {
     size_t const w = codeMode == kCode64 ? 8 : 4;
     size_t const cap = cluster_slots_per_cta(npad, logC);
-    return 768 * 8 + kDirTab * 4 + (size_t)(nwords >> logC) * 2 * 8 + cap * (w + 4) + 512 +
+    return 768 * 8 + kDirTab * 4 + (size_t)(nwords >> logC) * 3 * 8 + cap * (w + 4) + 512 +
            (size_t)perThread * kResidentBlock * 4;
 }
 
