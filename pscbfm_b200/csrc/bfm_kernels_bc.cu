@@ -518,6 +518,10 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
 
 // ---------------------------------------------------------------------------------- resident
 
+// The whole system in one CTA's shared memory for nSteps sub-steps: lattice, one temporary
+// lattice per sub-step parity (the previous one cleared while the next check runs), packed
+// coordinates, bond codes and the mover list; one CTA per system of sysList, entries of sub-step t
+// at steps[t * nSys + system]. Two CTA barriers per sub-step (after the check, after the perform).
 template <typename W, int K>
 __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const* __restrict__ sysv,
                                                                     uint32_t const* __restrict__ sysList,
@@ -525,7 +529,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
                                                                     uint32_t nSys, uint32_t nSteps)
 {
     __shared__ SysDev S;
-    __shared__ uint32_t listCount;
+    __shared__ uint32_t listCount[2];   // per sub-step parity
     extern __shared__ unsigned long long smem[];
     uint32_t const sysId = sysList[blockIdx.x];
     copy_desc(S, sysv + sysId);
@@ -535,8 +539,8 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
     unsigned long long* const ptab = smem;                  // 768 plane masks
     uint32_t* const dtab = reinterpret_cast<uint32_t*>(smem + 768);   // kDirTab words (16-byte aligned)
     unsigned long long* const lat = smem + 768 + kDirTab / 2;
-    unsigned long long* const tmp = lat + nw;
-    W* const code = reinterpret_cast<W*>(tmp + nw);
+    unsigned long long* const tmp = lat + nw;               // 2 x nw words (per sub-step parity)
+    W* const code = reinterpret_cast<W*>(tmp + 2u * nw);
     uint32_t* const pk = reinterpret_cast<uint32_t*>(code + np);
     uint8_t* const mok = reinterpret_cast<uint8_t*>(pk + np);   // 512 move-table bytes
     uint32_t* const list = reinterpret_cast<uint32_t*>(mok + 512);
@@ -547,22 +551,29 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
     for (uint32_t w = tid; w < nw; w += B) {
         lat[w] = S.lat[w];
         tmp[w] = 0ull;
+        tmp[nw + w] = 0ull;
     }
     for (uint32_t g = tid; g < np; g += B) {
         code[g] = gcode[g];
         pk[g] = S.pk[g];
     }
-    if (tid == 0) listCount = 0;
+    if (tid < 2) listCount[tid] = 0;
     uint32_t nTent = 0, nAcc = 0;
     unsigned long long nAtt = 0;
     StepEntry next = nSteps ? steps[sysId] : StepEntry{};
     __syncthreads();
 
+    uint32_t par = 0;
     for (uint32_t t = 0; t < nSteps; ++t) {
         StepEntry const st = next;
         if (t + 1 < nSteps) next = steps[(size_t)(t + 1) * nSys + sysId];   // prefetch
         if (st.color == kNoColor) continue;
         nAtt += st.cnt;
+        unsigned long long* const tmpCur = tmp + par * nw;
+        // the previous sub-step's marks and list count: read by no thread after the barrier that
+        // ended that sub-step, written by none before the barrier that ends this one
+        for (uint32_t w = tid; w < nw; w += B) tmp[(par ^ 1u) * nw + w] = 0ull;
+        if (tid == 0) listCount[par ^ 1u] = 0;
         // check: tentative movers -> tmp bit + shared list (one atomic per warp)
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -583,7 +594,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
                         if (pl.m[r]) hit |= lat[pl.w[r]] & pl.m[r];   // masks from shared memory
                     if (hit == 0ull) {
                         uint32_t const to = addr_add(p, D.ma, D.step);
-                        atomicOr(tmp + (to >> 6), 1ull << (to & 63u));
+                        atomicOr(tmpCur + (to >> 6), 1ull << (to & 63u));
                         go = true;
                         entry = g | (dir << kSlotShift);
                     }
@@ -592,7 +603,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
             uint32_t const bal = __ballot_sync(0xffffffffu, go);
             if (bal) {
                 uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(&listCount, (uint32_t)__popc(bal));
+                if (lane == 0) base = atomicAdd(&listCount[par], (uint32_t)__popc(bal));
                 base = __shfl_sync(0xffffffffu, base, 0);
                 if (go) list[base + __popc(bal & ((1u << lane) - 1u))] = entry;
                 nTent += lane == 0 ? (uint32_t)__popc(bal) : 0u;
@@ -600,7 +611,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
         }
         __syncthreads();
         // perform over the compact list
-        uint32_t const nList = listCount;
+        uint32_t const nList = listCount[par];
         for (uint32_t e = tid; e < nList; e += B) {
             uint32_t const g = list[e] & kSlotMask, dir = list[e] >> kSlotShift;
             uint32_t const p = pk[g];
@@ -616,7 +627,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
             unsigned long long hit = 0ull;
 #pragma unroll
             for (int r = 0; r < 4; ++r)
-                if (pl.m[r]) hit |= tmp[pl.w[r]] & pl.m[r];
+                if (pl.m[r]) hit |= tmpCur[pl.w[r]] & pl.m[r];
             if (hit != 0ull) continue;
             uint32_t const a = dir >> 1;
             int32_t const s = (dir & 1u) ? 1 : -1;
@@ -644,10 +655,8 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
             }
             ++nAcc;
         }
-        __syncthreads();
-        for (uint32_t w = tid; w < nw; w += B) tmp[w] = 0ull;
-        if (tid == 0) listCount = 0;
-        __syncthreads();
+        __syncthreads();   // every perform is done: the lattice is settled for the next check
+        par ^= 1u;
     }
     W* const gcodeOut = static_cast<W*>(S.code);
     for (uint32_t w = tid; w < nw; w += B) S.lat[w] = lat[w];
@@ -1069,7 +1078,7 @@ cudaError_t launch_sweep_bc(SysDev const& hostDesc, StepEntry const* dSteps, uin
 size_t resident_bc_smem_bytes(uint32_t nwords, uint32_t npad, uint32_t maxGroup, uint32_t codeMode)
 {
     size_t const w = codeMode == kCode64 ? 8 : 4;
-    return 768 * 8 + kDirTab * 4 + (size_t)nwords * 2 * 8 + (size_t)npad * (w + 4) + 512 + (size_t)maxGroup * 4;
+    return 768 * 8 + kDirTab * 4 + (size_t)nwords * 3 * 8 + (size_t)npad * (w + 4) + 512 + (size_t)maxGroup * 4;
 }
 
 namespace {
