@@ -37,7 +37,7 @@ extern "C" {
 #define BFM_ERR_BUSY 7             /* server: result not ready yet */
 
 /* engine paths (bfm_set_mode) */
-#define BFM_MODE_AUTO 0     /* resident for small systems (largest colour group <= 4096 and fits one CTA),
+#define BFM_MODE_AUTO 0     /* resident for small systems (largest colour group <= 2048 and fits one CTA),
                                cluster where a cluster's shared memory holds the system with at
                                most 48 chunks of 32 slots per CTA and colour, persistent up to about
                                three 512-monomer tiles per SM (bond codes), else graph */

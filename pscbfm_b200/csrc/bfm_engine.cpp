@@ -1031,13 +1031,13 @@ int Updater::path() const
 int Updater::autoMode() const
 {
     // One system on a B200, per MCS: the resident kernel (one SM) while the largest colour group is
-    // at most 4 x 1024 monomers (1.2K-monomer chains 4.2 us, against 6.4 on a cluster and 11.9
-    // persistent; 8K: 13.7, 13.1, 13.1); then a cluster of CTAs holding the system in distributed
-    // shared memory where each CTA walks at most 48 chunks of 32 slots per colour (planCluster;
-    // 11K-52K monomers: 11.6-15.3 us against 12.9-16.0 persistent); then the persistent sweep
-    // while its tiles fit about three per SM (to 262K monomers: 16-19 us against 18-22 graph);
-    // beyond, the graph of separate launches (1M monomers: 30 us against 36).
-    if (residentEligible() && maxGroup_ <= 4u * kResidentBlock) return kModeResident;
+    // at most 2 x 1024 monomers (1.2K-3.3K-monomer chains 3.8-6.6 us, against 5.5-7.8 on a
+    // cluster; 6.5K-8K: 11.4-13.2 against 8.3-8.8); then a cluster of CTAs holding the system in
+    // distributed shared memory where each CTA walks at most 48 chunks of 32 slots per colour
+    // (planCluster; 8K-47K monomers: 8.3-14.7 us against 12.8-16.0 persistent); then the
+    // persistent sweep while its tiles fit about three per SM (to 262K monomers: 16-19 us against
+    // 18-22 graph); beyond, the graph of separate launches (1M monomers: 30 us against 36).
+    if (residentEligible() && maxGroup_ <= 2u * kResidentBlock) return kModeResident;
     if (clusterEligible() && clusterTier_ >= 3) return kModeCluster;
     if (codeMode_ != kCodeNone) {
         uint32_t const tiles = (maxGroup_ + kBcTileSpan - 1) / kBcTileSpan;

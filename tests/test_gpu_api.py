@@ -172,11 +172,13 @@ def test_persistent_barrier_timeout_is_reported():
 
 
 def test_auto_mode_picks_the_path_by_size():
-    """AUTO: resident for a small system that fits one CTA, a cluster of CTAs for systems its shared
-    memory holds at 48 chunks of 32 per CTA, the persistent sweep for larger bond-code systems, the
-    graph of launches for the 1M-monomer melt and for systems without bond codes."""
+    """AUTO: resident for a system whose largest colour group is at most 2048, a cluster of CTAs for
+    systems its shared memory holds at 48 chunks of 32 per CTA, the persistent sweep for larger
+    bond-code systems, the graph of launches for the 1M-monomer melt and for systems without bond
+    codes."""
     import numpy as np
-    cases = [(S.small_chains(), P.MODE_RESIDENT), (S.crosslinked_network(), P.MODE_CLUSTER),
+    cases = [(S.serpentine_chains(32, 32, 0.3, seed=3), P.MODE_RESIDENT), (S.small_chains(), P.MODE_CLUSTER),
+             (S.crosslinked_network(), P.MODE_CLUSTER),
              (S.serpentine_chains(64, 64, 0.8, seed=13), P.MODE_CLUSTER),
              (S.serpentine_chains(128, 64, 0.23, seed=5), P.MODE_PERSISTENT),   # 59 chunks per CTA of 16
              (S.serpentine_chains(128, 64, 0.3, seed=3), P.MODE_PERSISTENT), (S.dense_melt(), P.MODE_GRAPH)]
