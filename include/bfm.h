@@ -39,7 +39,8 @@ extern "C" {
 /* engine paths (bfm_set_mode) */
 #define BFM_MODE_AUTO 0     /* resident for small systems (largest colour group <= 2048 and fits one CTA),
                                cluster where a cluster's shared memory holds the system with at
-                               most 48 chunks of 32 slots per CTA and colour, persistent up to about
+                               most 48 chunks of 32 slots per CTA and colour (one per warp where a
+                               cluster of up to 16 CTAs allows), persistent up to about
                                three 512-monomer tiles per SM (bond codes), else graph */
 #define BFM_MODE_LAUNCH 1   /* check + perform launch per sub-step (the reference's structure) */
 #define BFM_MODE_GRAPH 2    /* the same launches captured into CUDA graphs */

@@ -969,23 +969,25 @@ void Updater::enqueueResident(uint32_t nSteps)
 
 void Updater::planCluster()
 {
-    // Three tiers, each the smallest cluster (2..16 CTAs) the device can run whose CTAs walk at
-    // most so many chunks of 32 slots per colour: 48 (1.5 per warp; the plan BFM_MODE_AUTO takes),
-    // 64 (2 per warp; the plan a Batch takes) and 256 (8 per warp; BFM_MODE_CLUSTER only). Each
-    // chunk a warp walks waits on remote shared memory, so the kernel's time per sub-step grows
-    // with the chunks per CTA. Alone on a B200 (chains in 64^3 and 128^3 boxes, 11K-60K monomers)
-    // it beats the persistent sweep up to about 48 chunks per CTA (9.1-15.2 us per MCS against
-    // 12.9-16.0) and loses from about 51-59 (16.2-17.5 against 15.8-16.1), while up to 64 it still
-    // beats the graph of launches (17.5 against 18.0), the path a Batch runs such a system on
-    // otherwise; at 8 chunks per warp it takes 25-30 us.
-    constexpr uint32_t kLimits[3] = {48u, 64u, 256u};
+    // Tiers, each the smallest cluster (2..16 CTAs) the device can run whose CTAs walk at most so
+    // many chunks of 32 slots per colour: 32 (one per warp) and then 48 (1.5 per warp), the plans
+    // BFM_MODE_AUTO takes; 64 (2 per warp), the plan a Batch takes; 256 (8 per warp),
+    // BFM_MODE_CLUSTER only. Each chunk a warp walks waits on remote shared memory, so the
+    // kernel's time per sub-step grows with the chunks per warp more than with the cluster size.
+    // Alone on a B200 (chains in 64^3 and 128^3 boxes, 11K-60K monomers, two barriers per
+    // sub-step): one chunk per warp 8.9-11.3 us per MCS, up to 48 chunks per CTA 11.6-14.7, both
+    // ahead of the persistent sweep (12.8-16.0); at 51-59 about even with it (15.3-16.9 against
+    // 15.8) while still ahead of the graph of launches (17.9-18.1), the path a Batch runs such a
+    // system on otherwise; at 8 chunks per warp 25-32.
+    constexpr uint32_t kLimits[4] = {32u, 48u, 64u, 256u};
+    constexpr uint32_t kTier[4] = {3u, 3u, 2u, 1u};
     clusterLogC_ = 0;
     clusterPer_ = 0;
     clusterSmem_ = 0;
     clusterTier_ = 0;
     if (codeMode_ == kCodeNone) return;
     uint32_t const chunks = (maxGroup_ + 31u) / 32u;
-    for (uint32_t tier = 0; tier < 3; ++tier)
+    for (uint32_t tier = 0; tier < 4; ++tier)
         for (uint32_t logC = 1; logC <= 4; ++logC) {
             uint32_t const C = 1u << logC;
             if (dev_.h.nwords < C) continue;
@@ -998,7 +1000,7 @@ void Updater::planCluster()
             clusterLogC_ = logC;
             clusterPer_ = per;
             clusterSmem_ = smem;
-            clusterTier_ = 3 - tier;
+            clusterTier_ = kTier[tier];
             return;
         }
 }
@@ -1033,8 +1035,9 @@ int Updater::autoMode() const
     // One system on a B200, per MCS: the resident kernel (one SM) while the largest colour group is
     // at most 2 x 1024 monomers (1.2K-3.3K-monomer chains 3.8-6.6 us, against 5.5-7.8 on a
     // cluster; 6.5K-8K: 11.4-13.2 against 8.3-8.8); then a cluster of CTAs holding the system in
-    // distributed shared memory where each CTA walks at most 48 chunks of 32 slots per colour
-    // (planCluster; 8K-47K monomers: 8.3-14.7 us against 12.8-16.0 persistent); then the
+    // distributed shared memory where each CTA walks at most 48 chunks of 32 slots per colour,
+    // one per warp where a cluster of up to 16 CTAs allows (planCluster; 8K-47K monomers: 8.3-14.7
+    // us against 12.8-16.0 persistent); then the
     // persistent sweep while its tiles fit about three per SM (to 262K monomers: 16-19 us against
     // 18-22 graph); beyond, the graph of separate launches (1M monomers: 30 us against 36).
     if (residentEligible() && maxGroup_ <= 2u * kResidentBlock) return kModeResident;
