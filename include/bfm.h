@@ -92,7 +92,10 @@ int bfm_set_coords_bulk(bfm_handle h, const int32_t* xyz, uint32_t n);
 int bfm_add_bond(bfm_handle h, uint32_t a, uint32_t b);
 /* Bulk form: pairs[2*k] -> pairs[2*k+1] for k < n_pairs, in order (same as n_pairs calls). */
 int bfm_add_bonds_bulk(bfm_handle h, const uint32_t* pairs, uint32_t n_pairs);
-/* setLatticeSize (UpdaterGPUScBFM_AB_Type.cu:797-848): powers of two, 4..1024 per side. */
+/* setLatticeSize (UpdaterGPUScBFM_AB_Type.cu:797-848): 4..1024 per side, a power of two along a
+ * periodic axis (the reference's rule for every axis); along an axis without periodicity any side
+ * (the lattice there is the next power of two; nothing wraps). A non-power-of-two side on an axis
+ * that is periodic when this or bfm_set_periodicity is called is BFM_ERR_RUNTIME. */
 int bfm_set_box(bfm_handle h, uint32_t bx, uint32_t by, uint32_t bz);
 /* copyBondSet (UpdaterGPUScBFM_AB_Type.cu:693-697): entry (dx&7)|(dy&7)<<3|(dz&7)<<6 of the
  * 512-entry table; everything starts forbidden. */

@@ -59,6 +59,7 @@ struct System {
     std::vector<std::vector<uint32_t>> nbr;       // directed lists, in setConnectivity order
     bool forbidden[512];
     uint32_t walls = 0;                           // bit a: axis a is not periodic
+    uint32_t lattice[3] = {0, 0, 0};              // cells per axis (see make_system)
 };
 
 // CRITICAL.cu:334-341 (build with NONPERIODICITY): along an axis with walls the moved corner must
@@ -291,7 +292,7 @@ void sweep(System& s, Sorted const& g, Draws& draws, uint32_t nMcs, RunStats& st
         auto& dst = nb[g.oldToNew[i]];
         for (uint32_t j : s.nbr[i]) dst.push_back(g.oldToNew[j]);
     }
-    Lattice lat(s.box), tmp(s.box);
+    Lattice lat(s.lattice), tmp(s.lattice);
     for (uint32_t k = 0; k < n; ++k) lat.cell[lat.at(px[k], py[k], pz[k])] = 1;
 
     std::vector<uint8_t> flag(n, 0);
@@ -371,8 +372,19 @@ System make_system(uint32_t n, int32_t const* xyz, uint32_t const* nbrCount, uin
         }
     }
     for (int i = 0; i < 512; ++i) s.forbidden[i] = forbidden[i] != 0;
-    for (int a = 0; a < 3; ++a)
-        if (box[a] == 0 || (box[a] & (box[a] - 1)) != 0) throw std::invalid_argument("box sides must be powers of two");
+    // The reference's lattice index needs power-of-two sides (UpdaterGPUScBFM_AB_Type.cu:797-848).
+    // Generalised here to walled axes of any side >= 4: corners stay in [0, L-2] there, so the
+    // axis never wraps and the box can sit in the lowest cells of a power-of-two side (the +-1
+    // cells of a front plane at a wall then land on cells no corner occupies, as in the
+    // reference's walled power-of-two boxes). Periodic axes still need a power of two.
+    for (int a = 0; a < 3; ++a) {
+        bool const p2 = box[a] != 0 && (box[a] & (box[a] - 1)) == 0;
+        if (box[a] < 4 || (!((s.walls >> a) & 1u) && !p2))
+            throw std::invalid_argument("box sides must be powers of two (any side >= 4 along a walled axis)");
+        uint32_t P = 4;
+        while (P < box[a]) P *= 2;
+        s.lattice[a] = P;
+    }
     for (uint32_t i = 0; i < n; ++i)
         if (outside_walls(s, s.x[i], s.y[i], s.z[i]))
             throw std::invalid_argument("monomer " + std::to_string(i) + " lies outside the walls of the box");
@@ -406,7 +418,7 @@ struct Xoshiro128 {
 
 void sequential_sweep(System& s, uint64_t seed, uint32_t nMcs, RunStats& st)
 {
-    Lattice lat(s.box);
+    Lattice lat(s.lattice);
     for (uint32_t k = 0; k < s.n; ++k) lat.cell[lat.at(s.x[k], s.y[k], s.z[k])] = 1;
     Xoshiro128 rng(seed);
     uint64_t const attempts = (uint64_t)nMcs * s.n;

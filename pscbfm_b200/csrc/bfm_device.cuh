@@ -72,7 +72,9 @@ struct SysDev {
     uint32_t codeMode;               // kCodeNone, kCode32, kCode64
     uint32_t walls;                  // bit a: axis a is not periodic (corners stay in [0, L-2])
     uint32_t npad, nwords, maxc, nColors;
-    uint32_t mask[3];                // box side - 1 (power-of-two box)
+    uint32_t mask[3];                // lattice side - 1 (a power of two; the box side but along a
+                                     // walled axis whose side is not one)
+    uint32_t lim[3];                 // box side - 1: on a walled axis a moved corner stays below it
     uint32_t nb[3];                  // bricks per axis
     uint32_t mb, hx, hy;             // brick_index parameters
     uint32_t forbid[16];             // bit i set <=> bond index i is forbidden
@@ -140,12 +142,12 @@ __device__ __forceinline__ uint32_t move_dir(uint32_t iLocal, uint32_t seed)
 // Position of value v (0..3) of axis a inside a brick word: bit = x + 4 y + 16 z.
 // CRITICAL.cu:334-341 (the reference's NONPERIODICITY build): along an axis with walls the moved
 // corner must stay in [0, L-2]; c is the current coordinate along the move's axis (in the box on
-// such an axis), and the unsigned compare rejects both -1 and L-1.
-__host__ __device__ __forceinline__ bool wall_blocks(uint32_t walls, uint32_t c, uint32_t dir, uint32_t const* mask)
+// such an axis), and the unsigned compare against lim = L - 1 rejects both -1 and L-1.
+__host__ __device__ __forceinline__ bool wall_blocks(uint32_t walls, uint32_t c, uint32_t dir, uint32_t const* lim)
 {
     uint32_t const a = dir >> 1;
     uint32_t const c1 = c + ((dir & 1u) ? 1u : 0xFFFFFFFFu);
-    return ((walls >> a) & 1u) && c1 >= mask[a];
+    return ((walls >> a) & 1u) && c1 >= lim[a];
 }
 
 __host__ __device__ __forceinline__ uint32_t brick_pos(uint32_t v, uint32_t a)
@@ -282,7 +284,9 @@ constexpr uint32_t kDirHalf = 6 * 4;
 constexpr uint32_t kDirTab = 6 * kDirWords;
 constexpr uint32_t kNoWall = 1u << 31;
 
-inline void dir_table_fill(uint32_t const nb[3], uint32_t const* tab, uint32_t const mask[3], uint32_t walls,
+// hi[a]: the highest corner coordinate a walled axis a allows (its box side - 2); the wall word of a
+// move along a walled axis is the address of the corner that may not move further that way.
+inline void dir_table_fill(uint32_t const nb[3], uint32_t const* tab, uint32_t const hi[3], uint32_t walls,
                            uint32_t* out)
 {
     uint32_t M[3];
@@ -300,7 +304,7 @@ inline void dir_table_fill(uint32_t const nb[3], uint32_t const* tab, uint32_t c
         f[1] = M[u] >> 6;
         f[2] = M[v] >> 6;
         uint32_t c[3] = {0u, 0u, 0u};
-        c[a] = up ? mask[a] - 1u : 0u;
+        c[a] = up ? hi[a] : 0u;
         f[3] = ((walls >> a) & 1u) ? lattice_address(c[0], c[1], c[2], nb, tab) : kNoWall;
     }
 }

@@ -32,6 +32,16 @@ constexpr uint32_t kSlotAlign = 32;
 
 bool pow2(uint32_t v) { return v && !(v & (v - 1)); }
 
+// UpdaterGPUScBFM_AB_Type.cu:797-848 (the reference's message for a side its bit shifts cannot take)
+std::string not_pow2_message(uint32_t bx, uint32_t by, uint32_t bz)
+{
+    std::ostringstream m;
+    m << "[UpdaterGPUScBFM_AB_Type::setLatticeSize] Could not determine value for bit shift. Check whether "
+         "the box size is a power of 2 (and at least 4)! ( box="
+      << bx << "," << by << "," << bz << " )";
+    return m.str();
+}
+
 uint32_t ilog2(uint32_t v)
 {
     uint32_t l = 0;
@@ -163,7 +173,24 @@ void Updater::setPeriodicity(bool px, bool py, bool pz)
     // UpdaterGPUScBFM_AB_Type.cu:728-753 accepts fully periodic boxes in its default build and
     // fully non-periodic ones in its NONPERIODICITY build; here every axis chooses on its own.
     if (initialized()) throw std::runtime_error("[setPeriodicity] call it before initialize");
-    walls_ = (px ? 0u : 1u) | (py ? 0u : 2u) | (pz ? 0u : 4u);
+    uint32_t const walls = (px ? 0u : 1u) | (py ? 0u : 2u) | (pz ? 0u : 4u);
+    for (int a = 0; a < 3; ++a)
+        if (!((walls >> a) & 1u) && box_[a] && !pow2(box_[a]))
+            throw std::runtime_error(not_pow2_message(box_[0], box_[1], box_[2]) +
+                                     " A periodic axis needs a power-of-two side.");
+    walls_ = walls;
+}
+
+uint32_t Updater::latticeSide(int a) const
+{
+    // a periodic axis wraps with the lattice's mask, so its side is the box side (a power of two);
+    // a walled axis never wraps (corners stay in [0, L-2]), so its box sits in the lowest cells of
+    // a power-of-two lattice side and the walls stay at the box side
+    uint32_t const L = box_[a];
+    if (!((walls_ >> a) & 1u) || pow2(L)) return L;
+    uint32_t P = 4;
+    while (P < L) P *= 2;
+    return P;
 }
 
 void Updater::setNrOfAllMonomers(uint32_t n)
@@ -225,13 +252,12 @@ void Updater::setLatticeSize(uint32_t bx, uint32_t by, uint32_t bz)
           << ") is larger than supported (<= 1024 per side)";
         throw std::invalid_argument(m.str());
     }
-    if (!pow2(bx) || !pow2(by) || !pow2(bz) || bx < 4 || by < 4 || bz < 4) {
-        std::ostringstream m;
-        m << "[UpdaterGPUScBFM_AB_Type::setLatticeSize] Could not determine value for bit shift. Check whether "
-             "the box size is a power of 2 (and at least 4)! ( box="
-          << bx << "," << by << "," << bz << " )";
-        throw std::runtime_error(m.str());
-    }
+    // the reference needs powers of two on every axis; here only periodic axes do (setPeriodicity
+    // comes first in the reference's call order, and checks the sides again if it comes later)
+    uint32_t const b[3] = {bx, by, bz};
+    for (int a = 0; a < 3; ++a)
+        if (b[a] < 4 || (!((walls_ >> a) & 1u) && !pow2(b[a])))
+            throw std::runtime_error(not_pow2_message(bx, by, bz));
     box_[0] = bx;
     box_[1] = by;
     box_[2] = bz;
@@ -321,7 +347,8 @@ void Updater::initialize()
     for (uint32_t i = 0; i < n_; ++i) maxc_ = std::max(maxc_, nbrCnt_[i]);
 
     // host images
-    uint32_t nb[3] = {box_[0] / 4, box_[1] / 4, box_[2] / 4};
+    uint32_t const P[3] = {latticeSide(0), latticeSide(1), latticeSide(2)};
+    uint32_t nb[3] = {P[0] / 4, P[1] / 4, P[2] / 4};
     uint32_t const nwords = nb[0] * nb[1] * nb[2];
     std::vector<uint32_t> tab = brick_tables(nb);
     std::vector<int32_t> hx(npad_, kPadCoord), hy(npad_, 0), hz(npad_, 0);
@@ -337,8 +364,7 @@ void Updater::initialize()
         hnnb[s] = (uint8_t)nbrCnt_[i];
         for (uint32_t k = 0; k < nbrCnt_[i]; ++k)
             hnbr[(size_t)k * npad_ + s] = oldToNew_[nbrIds_[(size_t)i * kMaxConn + k]];
-        uint32_t const mx = uint32_t(x) & (box_[0] - 1), my = uint32_t(y) & (box_[1] - 1),
-                       mz = uint32_t(z) & (box_[2] - 1);
+        uint32_t const mx = uint32_t(x) & (P[0] - 1), my = uint32_t(y) & (P[1] - 1), mz = uint32_t(z) & (P[2] - 1);
         uint32_t const w = tab[mx >> 2] + tab[nb[0] + (my >> 2)] + tab[nb[0] + nb[1] + (mz >> 2)];
         uint32_t const b = host_brick_pos(mx & 3, 0) | host_brick_pos(my & 3, 1) | host_brick_pos(mz & 3, 2);
         hlat[w] |= 1ull << b;
@@ -397,7 +423,8 @@ void Updater::initialize()
     h.maxc = maxc_;
     h.nColors = nC;
     for (int a = 0; a < 3; ++a) {
-        h.mask[a] = box_[a] - 1;
+        h.mask[a] = P[a] - 1;
+        h.lim[a] = box_[a] - 1;
         h.nb[a] = nb[a];
     }
     brick_params(nb, h.mb, h.hx, h.hy);
@@ -434,7 +461,8 @@ void Updater::initialize()
     // so the unused (zero) fields of a code word drop out of the AND over all fields
     hmove[0] = 0x3F;
     std::vector<uint32_t> hdir(kDirTab);
-    dir_table_fill(nb, tab.data(), h.mask, walls_, hdir.data());
+    uint32_t const hi[3] = {box_[0] - 2, box_[1] - 2, box_[2] - 2};   // walls at the box sides
+    dir_table_fill(nb, tab.data(), hi, walls_, hdir.data());
     cuda_check(cudaMemcpyAsync(const_cast<unsigned long long*>(h.planeTab), hplane.data(), 8ull * 768,
                                cudaMemcpyHostToDevice, s), "upload plane table");
     cuda_check(cudaMemcpyAsync(const_cast<uint8_t*>(h.moveOk), hmove.data(), 512, cudaMemcpyHostToDevice, s),
@@ -485,7 +513,8 @@ void Updater::hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, s
 {
     // lattice addresses, bond-code words and neighbour slots with their reverse slot, all in
     // sorted order, from the host positions
-    uint32_t const nb[3] = {box_[0] / 4, box_[1] / 4, box_[2] / 4};
+    uint32_t const P[3] = {latticeSide(0), latticeSide(1), latticeSide(2)};
+    uint32_t const nb[3] = {P[0] / 4, P[1] / 4, P[2] / 4};
     std::vector<uint32_t> const tab = brick_tables(nb);
     pk.assign(npad_, 0u);
     size_t const w = codeMode_ == kCode64 ? 8 : 4;
@@ -495,8 +524,8 @@ void Updater::hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, s
     for (uint32_t i = 0; i < n_; ++i) {
         uint32_t const s = oldToNew_[i];
         int32_t const* p = &xyz_[3 * (size_t)i];
-        pk[s] = lattice_address(uint32_t(p[0]) & (box_[0] - 1), uint32_t(p[1]) & (box_[1] - 1),
-                                uint32_t(p[2]) & (box_[2] - 1), nb, tab.data());
+        pk[s] = lattice_address(uint32_t(p[0]) & (P[0] - 1), uint32_t(p[1]) & (P[1] - 1), uint32_t(p[2]) & (P[2] - 1),
+                                nb, tab.data());
         uint64_t c = (uint64_t)nbrCnt_[i] << countShift;
         for (uint32_t k = 0; k < nbrCnt_[i]; ++k) {
             uint32_t const j = nbrIds_[(size_t)i * kMaxConn + k];
@@ -645,6 +674,9 @@ void Updater::checkSetup() const
     requireN("initialize");
     if (n_ == 0) throw std::runtime_error("[initialize] the system has no monomers");
     if (!box_[0]) throw std::runtime_error("[initialize] setLatticeSize has not been called");
+    for (int a = 0; a < 3; ++a)
+        if (!((walls_ >> a) & 1u) && !pow2(box_[a]))
+            throw std::runtime_error(not_pow2_message(box_[0], box_[1], box_[2]));
     uint32_t nAllowed = 0;
     for (bool f : forbidden_) nAllowed += f ? 0 : 1;
     if (nAllowed != 108) {
@@ -1296,15 +1328,18 @@ void Updater::validate()
         for (int a = 0; a < 3; ++a)
             if (((walls_ >> a) & 1u) && uint32_t(xyz_[3ull * i + a]) >= box_[a] - 1u)
                 throw std::runtime_error("[validate] monomer " + std::to_string(i) + " crossed a wall");
-    uint64_t const V = (uint64_t)box_[0] * box_[1] * box_[2];
+    // cells on the lattice (a walled axis of any side sits in a power-of-two lattice side and never
+    // wraps; a periodic axis wraps with its mask)
+    uint32_t const P[3] = {latticeSide(0), latticeSide(1), latticeSide(2)};
+    uint64_t const V = (uint64_t)P[0] * P[1] * P[2];
     std::vector<uint8_t> cells(V, 0);
     uint64_t occupied = 0;
     for (uint32_t i = 0; i < n_; ++i)
         for (int c = 0; c < 8; ++c) {
-            uint32_t const x = uint32_t(xyz_[3 * (size_t)i] + (c & 1)) & (box_[0] - 1);
-            uint32_t const y = uint32_t(xyz_[3 * (size_t)i + 1] + ((c >> 1) & 1)) & (box_[1] - 1);
-            uint32_t const z = uint32_t(xyz_[3 * (size_t)i + 2] + ((c >> 2) & 1)) & (box_[2] - 1);
-            uint8_t& cell = cells[x + (uint64_t)box_[0] * (y + (uint64_t)box_[1] * z)];
+            uint32_t const x = uint32_t(xyz_[3 * (size_t)i] + (c & 1)) & (P[0] - 1);
+            uint32_t const y = uint32_t(xyz_[3 * (size_t)i + 1] + ((c >> 1) & 1)) & (P[1] - 1);
+            uint32_t const z = uint32_t(xyz_[3 * (size_t)i + 2] + ((c >> 2) & 1)) & (P[2] - 1);
+            uint8_t& cell = cells[x + (uint64_t)P[0] * (y + (uint64_t)P[1] * z)];
             occupied += cell ? 0 : 1;
             cell = 1;
         }
@@ -1337,9 +1372,9 @@ void Updater::validate()
         std::vector<uint32_t> tab = brick_tables(dev_.h.nb);
         std::vector<unsigned long long> want(dev_.h.nwords, 0ull);
         for (uint32_t i = 0; i < n_; ++i) {
-            uint32_t const mx = uint32_t(xyz_[3 * (size_t)i]) & (box_[0] - 1);
-            uint32_t const my = uint32_t(xyz_[3 * (size_t)i + 1]) & (box_[1] - 1);
-            uint32_t const mz = uint32_t(xyz_[3 * (size_t)i + 2]) & (box_[2] - 1);
+            uint32_t const mx = uint32_t(xyz_[3 * (size_t)i]) & dev_.h.mask[0];
+            uint32_t const my = uint32_t(xyz_[3 * (size_t)i + 1]) & dev_.h.mask[1];
+            uint32_t const mz = uint32_t(xyz_[3 * (size_t)i + 2]) & dev_.h.mask[2];
             uint32_t const w = tab[mx >> 2] + tab[dev_.h.nb[0] + (my >> 2)] + tab[dev_.h.nb[0] + dev_.h.nb[1] + (mz >> 2)];
             want[w] |= 1ull << (host_brick_pos(mx & 3, 0) | host_brick_pos(my & 3, 1) | host_brick_pos(mz & 3, 2));
         }

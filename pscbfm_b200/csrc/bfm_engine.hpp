@@ -97,6 +97,10 @@ public:
     uint32_t maxNeighbours() const;
     uint64_t boxVolume() const { return (uint64_t)box_[0] * box_[1] * box_[2]; }
     uint32_t boxSide(int a) const { return box_[a]; }
+    // side of the occupancy lattice along axis a: the box side, or for a walled axis whose side is
+    // not a power of two the next power of two (the box sits in its lowest cells)
+    uint32_t latticeSide(int a) const;
+    uint64_t latticeVolume() const { return (uint64_t)latticeSide(0) * latticeSide(1) * latticeSide(2); }
     // molecules (connected components of the bond graph) of the current set-up, on the host
     uint32_t countMolecules() const;
     void setCoordinates(int32_t const* xyz, uint32_t n);

@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(kGridBlock) k_check(SysDev const* __restrict__
             int32_t const x1 = x0 + dx, y1 = y0 + dy, z1 = z0 + dz;
             uint32_t const nn = __ldg(S.nnb + g);
             uint32_t const ca = (dir >> 1) == 0 ? uint32_t(x0) : ((dir >> 1) == 1 ? uint32_t(y0) : uint32_t(z0));
-            ok = !wall_blocks(S.walls, ca, dir, S.mask);
+            ok = !wall_blocks(S.walls, ca, dir, S.lim);
             for (uint32_t k = 0; k < nn; ++k) {
                 uint32_t const j = __ldg(S.nbr + (size_t)k * S.npad + g);
                 uint32_t const idx = bond_index(__ldg(S.x + j) - x1, __ldg(S.y + j) - y1, __ldg(S.z + j) - z1);
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident(SysDev const* __
                 int32_t const x1 = x0 + dx, y1 = y0 + dy, z1 = z0 + dz;
                 uint32_t const nn = S.nnb[g];
                 uint32_t const ca = (dir >> 1) == 0 ? uint32_t(x0) : ((dir >> 1) == 1 ? uint32_t(y0) : uint32_t(z0));
-                bool ok = !wall_blocks(S.walls, ca, dir, S.mask);
+                bool ok = !wall_blocks(S.walls, ca, dir, S.lim);
                 for (uint32_t q = 0; q < nn; ++q) {
                     uint32_t const j = S.nbr[(size_t)q * S.npad + g];
                     if (forbidden(S.forbid, bond_index(X[j] - x1, Y[j] - y1, Z[j] - z1))) ok = false;

@@ -147,6 +147,7 @@ extern "C" int bfm_sweep_noalloc(const bfm_noalloc_system* s, int32_t n_mcs, uin
     d.nColors = nC;
     for (int a = 0; a < 3; ++a) {
         d.mask[a] = s->box[a] - 1;
+        d.lim[a] = s->box[a] - 1;
         d.nb[a] = nb[a];
     }
     for (uint32_t i = 0; i < 512; ++i)

@@ -68,8 +68,8 @@ size_t Server::estimateBytes(Updater const& setup)
     uint32_t const maxc = std::max(setup.maxNeighbours(), 1u);
     uint32_t const nC = maxc + 1;
     uint32_t const npad = std::max(n + 32u * nC, 32u);
-    uint32_t const nwords = (uint32_t)(setup.boxVolume() / 64);
-    uint32_t const ntab = (setup.boxSide(0) + setup.boxSide(1) + setup.boxSide(2)) / 4;
+    uint32_t const nwords = (uint32_t)(setup.latticeVolume() / 64);
+    uint32_t const ntab = (setup.latticeSide(0) + setup.latticeSide(1) + setup.latticeSide(2)) / 4;
     size_t const arena = arena_layout(n, npad, maxc, nwords, ntab, nC, std::max(n, 1u), kCode64).bytes;
     size_t const obs = observables_bytes(npad, setup.countMolecules());
     size_t const steps = 2ull * sizeof(StepEntry) * kMaxChunkMcs * nC;

@@ -1,11 +1,10 @@
 """Synthetic BFM systems: the standard bond set and the straight-chain, network and ensemble
 layouts the sweep is measured on.
 
-A system is a power-of-two box (periodic, or with walls along chosen axes), int32 monomer corner
-positions (unfolded), directed
-neighbour lists in the order a LeMonADE-style caller would pass them to ``setConnectivity``
-(for every bond (a, b) in creation order: b is appended to a's list and a to b's list), integer
-attributes and the 512-entry forbidden-bond table indexed like
+A system is a box (periodic axes of power-of-two side, or walls along chosen axes of any side),
+int32 monomer corner positions (unfolded), directed neighbour lists in the order a
+LeMonADE-style caller would pass them to ``setConnectivity`` (for every bond (a, b) in creation
+order: b is appended to a's list and a to b's list), integer attributes and the 512-entry forbidden-bond table indexed like
 ``linearizeBondVectorIndex`` (src/pscbfm/CRITICAL.cu:243-261).
 
 No public dataset is involved: every layout is generated deterministically from its sizes.

@@ -27,13 +27,14 @@ int check_box(uint32_t const box[3])
 {
     uint32_t const nb[3] = {box[0] / 4, box[1] / 4, box[2] / 4};
     uint32_t const mask[3] = {box[0] - 1, box[1] - 1, box[2] - 1};
+    uint32_t const hi[3] = {box[0] - 2, box[1] - 2, box[2] - 2};
     std::vector<uint32_t> tab(nb[0] + nb[1] + nb[2]);
     brick_tables_fill(nb, tab.data());
     std::vector<unsigned long long> ptab(768);
     plane_table_fill(ptab.data());
     alignas(16) uint32_t dirP[kDirTab], dirW[kDirTab];
-    dir_table_fill(nb, tab.data(), mask, 0u, dirP);
-    dir_table_fill(nb, tab.data(), mask, 7u, dirW);
+    dir_table_fill(nb, tab.data(), hi, 0u, dirP);
+    dir_table_fill(nb, tab.data(), hi, 7u, dirW);
     for (uint32_t z = 0; z < box[2]; ++z)
         for (uint32_t y = 0; y < box[1]; ++y)
             for (uint32_t x = 0; x < box[0]; ++x) {
@@ -129,9 +130,9 @@ int main()
     uint32_t const nb[3] = {256, 256, 256};
     std::vector<uint32_t> tab(768);
     brick_tables_fill(nb, tab.data());
-    uint32_t const mask[3] = {1023, 1023, 1023};
+    uint32_t const hi[3] = {1022, 1022, 1022};
     alignas(16) uint32_t dir[kDirTab];
-    dir_table_fill(nb, tab.data(), mask, 0u, dir);
+    dir_table_fill(nb, tab.data(), hi, 0u, dir);
     uint32_t const top[3] = {1023, 1023, 1023}, zero[3] = {0, 0, 0};
     uint32_t const pt = address(top, nb, tab);
     if (pt >= (1u << 30)) return std::printf("address of the top corner exceeds 30 bits\n"), 1;

@@ -58,6 +58,23 @@ def test_box_must_be_power_of_two():
         fresh().setLatticeSize(2048, 64, 64)
 
 
+def test_walled_axis_of_any_side():
+    """A walled axis takes any side >= 4; a periodic one needs a power of two, whichever of
+    setPeriodicity and setLatticeSize comes first."""
+    u = fresh()
+    u.setPeriodicity(False, True, True)
+    u.setLatticeSize(48, 64, 64)
+    with pytest.raises(RuntimeError, match="power of 2"):
+        u.setPeriodicity(True, True, True)
+    v = fresh()
+    v.setPeriodicity(False, False, True)
+    with pytest.raises(RuntimeError, match="power of 2"):
+        v.setLatticeSize(48, 40, 24)
+    v.setLatticeSize(48, 40, 32)
+    with pytest.raises(RuntimeError, match="power of 2"):
+        v.setLatticeSize(48, 40, 3)
+
+
 def test_too_many_bonds():
     u = fresh()
     u.setNrOfAllMonomers(20)

@@ -55,6 +55,13 @@ NON_CUBIC = {
                                    [200]),
     "serp128x8x16_lc8": (lambda: S.serpentine_chains((128, 8, 16), 8, 0.3, seed=35), [300]),
     "serp8x8x256_lc32": (lambda: S.serpentine_chains((8, 8, 256), 32, 0.3, seed=37), [120, 180]),
+    # walled axes whose sides are not powers of two (the lattice side is the next power of two)
+    "serp48x40x24_lc16_walls_xyz": (lambda: S.walled(S.serpentine_chains((48, 40, 24), 16, 0.35, seed=43), walls=7),
+                                    [200]),
+    "serp36x64x32_lc16_walls_x": (lambda: S.walled(S.serpentine_chains((36, 64, 32), 16, 0.35, seed=45), walls=1),
+                                  [150, 50]),
+    "serp64x32x100_lc32_walls_z": (lambda: S.walled(S.serpentine_chains((64, 32, 100), 32, 0.3, seed=47), walls=4),
+                                   [120]),
 }
 
 
@@ -62,8 +69,8 @@ NON_CUBIC = {
 @pytest.mark.parametrize("mode", ["launch", "graph", "resident", "persistent", "cluster"])
 @pytest.mark.parametrize("name", list(NON_CUBIC))
 def test_non_cubic_boxes_vs_oracle(name, mode, repr_):
-    """Boxes with unequal power-of-two sides: the brick index interleaves the axes' low bits and
-    appends the longer axes' high bits. The reference updater always indexes its lattice by an
+    """Boxes with unequal sides (powers of two, or any side >= 4 along a walled axis): the brick
+    index interleaves the axes' low bits and appends the longer axes' high bits. The reference updater always indexes its lattice by an
     interleaved Z-curve, which runs past its lattice array when the sides differ, so the oracle
     (a linear lattice) alone pins these. The resident mode falls back to the graph path where a
     system does not fit one CTA."""

@@ -193,6 +193,27 @@ def test_walls_keep_monomers_inside(walls):
     assert not np.array_equal(free, xyz)
 
 
+@pytest.mark.parametrize("box,walls", [((48, 40, 24), 7), ((36, 64, 32), 1), ((32, 44, 64), 2), ((64, 32, 20), 4)])
+def test_walled_axes_of_any_side(box, walls):
+    """Walled axes take any side >= 4 (the box sits in the lowest cells of a power-of-two lattice
+    side; nothing wraps there): excluded volume, the bond set and the walls hold, and the walls are
+    reached."""
+    s = S.walled(S.serpentine_chains(box, 16, 0.3, seed=9), walls=walls)
+    xyz, (att, tent, acc) = O.run(s, 300)
+    assert _ev_ok(xyz, s.box) and _bonds_ok(s, xyz)
+    for a in range(3):
+        if (walls >> a) & 1:
+            assert xyz[:, a].min() >= 0 and xyz[:, a].max() <= s.box[a] - 2
+            assert xyz[:, a].min() == 0 or xyz[:, a].max() == s.box[a] - 2
+    assert 0 < acc <= tent <= att
+
+
+def test_periodic_axis_needs_a_power_of_two():
+    s = S.walled(S.serpentine_chains((48, 32, 32), 16, 0.3, seed=9), walls=2)   # x periodic, 48
+    with pytest.raises(RuntimeError, match="powers of two"):
+        O.run(s, 1)
+
+
 def test_monomer_outside_walls_rejected():
     s = S.walled(S.serpentine_chains(32, 16, 0.3, seed=5), walls=1)
     s.xyz = s.xyz.copy()
