@@ -26,6 +26,8 @@ SYSTEMS = {
     "network": S.crosslinked_network,
     "rings_and_free": S.rings_and_free,
     "serpentine": lambda: S.serpentine_chains(32, 64, 0.4, seed=5),
+    # walled axes of sides that are not powers of two
+    "walled_48x40x24": lambda: S.walled(S.serpentine_chains((48, 40, 24), 16, 0.3, seed=7), walls=7),
 }
 
 
@@ -37,6 +39,7 @@ def test_round_trip(key, tmp_path):
     r, info = bfm_io.read_bfm(p)
     assert info["mcs"] == 123
     assert tuple(r.box) == tuple(s.box)
+    assert tuple(r.periodic) == tuple(s.periodic)
     assert np.array_equal(r.xyz, s.xyz)
     assert _pairs(r) == _pairs(s)
     assert _nbr_sets(r) == _nbr_sets(s)
