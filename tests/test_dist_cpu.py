@@ -1,6 +1,8 @@
-"""Multi-process paths on the CPU (gloo, world size 2): the bench's reductions over ranks and the
-reference arm under torchrun. The sweep does not shard (one system is one replica), so N GPUs
-run N independent replicas and the only cross-rank steps are these reductions."""
+"""Multi-process paths on the CPU (gloo, world size 2): the bench's reductions over ranks, the
+reference arm under torchrun, and sets of systems sharded over ranks with their results gathered
+to rank 0. One system does not shard (one system is one replica), so N GPUs run N independent
+replicas or N disjoint subsets of systems, and the only cross-rank steps are reductions and the
+gather after the runs."""
 import json
 import os
 import socket
@@ -49,6 +51,74 @@ def test_reductions_over_two_gloo_ranks():
     for rank, mx, sm, rate in got:
         assert mx == 2.5 and sm == 6.0
         assert rate == pytest.approx(300.0)
+
+
+def _shard_main(rank, world, port, q):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                           timeout=datetime.timedelta(seconds=60))
+    from oracle import oracle as O
+    from pscbfm_b200 import sharding
+    systems, mcs = _shard_case()
+    seen = []
+
+    def run_local(ss, ms):
+        seen.extend(s.name for s in ss)
+        return [O.run(s, m)[0] for s, m in zip(ss, ms)]
+
+    res = sharding.run_sharded(systems, mcs, run_local, rank=rank, world=world)
+    q.put((rank, seen, None if res is None else [r.tolist() for r in res]))
+    dist.destroy_process_group()
+
+
+def _shard_case():
+    from pscbfm_b200 import systems as S
+    systems = [S.serpentine_chains(32, 16, 0.2 + 0.05 * k, name=f"shard{k}", seed=70 + k) for k in range(5)]
+    systems.append(S.walled(S.serpentine_chains((24, 32, 20), 8, 0.3, seed=79), walls=5, name="shard5"))
+    return systems, [40, 10, 25, 5, 30, 20]
+
+
+def test_shard_systems_is_balanced_and_deterministic():
+    sys.path.insert(0, ROOT)
+    from pscbfm_b200.sharding import shard_systems
+    costs = [5, 1, 4, 3, 3, 2, 8]
+    a = shard_systems(costs, 3)
+    assert a == shard_systems(costs, 3)
+    assert sorted(i for part in a for i in part) == list(range(len(costs)))
+    loads = [sum(costs[i] for i in part) for part in a]
+    assert max(loads) - min(loads) <= max(costs)
+    # in decreasing cost 8, 5, 4, 3, 3, 2, 1, each to the least-loaded rank (ties: the lower rank)
+    assert a == [[1, 6], [0, 4], [2, 3, 5]]          # 8 + 1 | 5 + 3 | 4 + 3 + 2
+    assert shard_systems([1.0, 1.0], 4) == [[0], [1], [], []]
+
+
+def test_sharded_runs_over_two_gloo_ranks_gather_to_rank0():
+    """Two ranks split six systems by monomers x MCS, each runs its own (the oracle stands in for
+    a rank's GPU), and rank 0 receives every system's final positions in the original order,
+    equal to running each system alone."""
+    import multiprocessing as mp
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = sorted((q.get(timeout=300) for _ in procs), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    systems, mcs = _shard_case()
+    (_, seen0, res0), (_, seen1, res1) = got
+    assert res1 is None and len(res0) == len(systems)
+    assert seen0 and seen1 and sorted(seen0 + seen1) == sorted(s.name for s in systems)
+    for s, m, r in zip(systems, mcs, res0):
+        want, _ = O.run(s, m)
+        assert np.array_equal(np.asarray(r), want), s.name
 
 
 def test_reference_arm_under_torchrun_prints_one_line():

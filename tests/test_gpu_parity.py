@@ -314,6 +314,20 @@ def test_batch_cluster_members_vs_oracle(cluster):
         m.close()
 
 
+def test_sharded_batch_runner_on_one_gpu():
+    """run_sharded on one rank with the Batch runner: each system's positions and MCS count equal
+    running it alone (the multi-rank assignment and gather are tested over gloo on the CPU)."""
+    from pscbfm_b200 import sharding
+    systems = [S.serpentine_chains(32, 16, 0.3, seed=81), S.crosslinked_network(),
+               S.walled(S.serpentine_chains((48, 40, 24), 16, 0.35, seed=43), walls=7)]
+    mcs = [30, 12, 20]
+    res = sharding.run_sharded(systems, mcs, sharding.batch_runner(0))
+    for s, m, (xyz, st) in zip(systems, mcs, res):
+        want, _ = O.run(s, m)
+        assert np.array_equal(xyz, want), s.name
+        assert st["mcs"] == m
+
+
 @pytest.mark.parametrize("resident", [True, False])
 def test_batch_uneven_mcs_per_member(resident):
     """run_each: members advance different MCS counts (some idle) in one launch sequence, as the
