@@ -117,7 +117,7 @@ def seq_run(sys, n_mcs: int, seed: int):
     return out.reshape(-1, 3), tuple(int(s) for s in stats)
 
 
-# ------------------------------------------------------------------ reference updater (GPU box)
+# ------------------------------------------------------------------ reference updater (on a GPU)
 
 def _ref_path(walls: int) -> str:
     """The default build for periodic boxes, the NONPERIODICITY build for boxes with walls on all

@@ -3,7 +3,7 @@
 // Drives pscbfm's own GPU updater, compiled for sm_100a from the reference sources by
 // oracle/Makefile (target `ref`, output oracle/_ref/libpscbfm_ref.so), through its setter API in
 // the order GPUScBFM_AB_Type::initialize/execute use (src/pscbfm/GPUScBFM_AB_Type.h:78-163).
-// The tests call it on the GPU box to pin the CPU oracle (oracle/bfm_oracle.cpp) against the
+// The GPU tests call it to pin the CPU oracle (oracle/bfm_oracle.cpp) against the
 // reference kernels on identical inputs and an identical host draw stream.
 
 #include <cstdint>

@@ -82,7 +82,8 @@ Server::Server(int gpu, size_t budgetBytes, uint32_t maxJobs) : gpu_(gpu), budge
     if (maxJobs == 0) throw std::invalid_argument("[Server] zero job slots");
     cuda_check(cudaSetDevice(gpu), "cudaSetDevice");
     // jobs allocate from the device's stream-ordered pool; keep up to the budget in the pool
-    // between jobs instead of returning it to the driver at every synchronisation (this process only)
+    // between jobs instead of returning it to the CUDA driver at every synchronisation (this
+    // process only)
     cudaMemPool_t pool;
     cuda_check(cudaDeviceGetDefaultMemPool(&pool, gpu), "cudaDeviceGetDefaultMemPool");
     uint64_t keep = budgetBytes;
