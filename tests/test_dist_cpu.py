@@ -94,6 +94,25 @@ def test_shard_systems_is_balanced_and_deterministic():
     assert shard_systems([1.0, 1.0], 4) == [[0], [1], [], []]
 
 
+def test_run_sharded_on_one_rank_needs_no_process_group():
+    sys.path.insert(0, ROOT)
+    from pscbfm_b200 import sharding
+    systems, mcs = _shard_case()
+    calls = []
+
+    def run_local(ss, ms):
+        calls.append(len(ss))
+        return [(s.name, m) for s, m in zip(ss, ms)]
+
+    out = sharding.run_sharded(systems, mcs, run_local)
+    assert calls == [len(systems)]
+    assert out == [(s.name, m) for s, m in zip(systems, mcs)]
+    with pytest.raises(ValueError):
+        sharding.run_sharded(systems, mcs[:-1], run_local)
+    with pytest.raises(RuntimeError):
+        sharding.run_sharded(systems, mcs, lambda ss, ms: [])
+
+
 def test_sharded_runs_over_two_gloo_ranks_gather_to_rank0():
     """Two ranks split six systems by monomers x MCS, each runs its own (the oracle stands in for
     a rank's GPU), and rank 0 receives every system's final positions in the original order,
