@@ -2,8 +2,8 @@
 
 ctypes bindings of the CPU restatement of the reference sweep (oracle/bfm_oracle.cpp, built as
 oracle/liboracle.so) and of the reference updater compiled for sm_100a
-(oracle/_ref/libpscbfm_ref.so, GPU only). Only tests/, the smoke entry and the CPU-baseline leg of
-bench.py import this module; the engine in pscbfm_b200/ never does.
+(oracle/_ref/libpscbfm_ref*.so, GPU only). Only tests/, the smoke entry and the baseline legs of
+bench.py (CPU baseline, reference arm) import this module; the engine in pscbfm_b200/ never does.
 """
 from __future__ import annotations
 
@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libpscbfm_ref.so")
 REF_LIB_NP = os.path.join(HERE, "_ref", "libpscbfm_ref_np.so")
+REF_LIB_C8 = os.path.join(HERE, "_ref", "libpscbfm_ref_c8.so")
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
@@ -119,46 +120,81 @@ def seq_run(sys, n_mcs: int, seed: int):
 
 # ------------------------------------------------------------------ reference updater (on a GPU)
 
-def _ref_path(walls: int) -> str:
+def _ref_path(walls: int, conn: int = 0) -> str:
     """The default build for periodic boxes, the NONPERIODICITY build for boxes with walls on all
-    three axes (the reference has no build for mixed periodicity)."""
+    three axes (the reference has no build for mixed periodicity), the MAX_CONNECTIVITY 8 build for
+    periodic systems with more than 4 bonds on some monomer (the reference has no build with both)."""
+    if conn > 8:
+        raise ValueError("the reference updater accepts at most 8 bonds per monomer")
     if walls == 0:
-        return REF_LIB
-    if walls == 7:
+        return REF_LIB if conn <= 4 else REF_LIB_C8
+    if walls == 7 and conn <= 4:
         return REF_LIB_NP
-    raise ValueError("the reference updater supports fully periodic or fully non-periodic boxes only")
+    raise ValueError("the reference updater supports fully periodic boxes, or fully non-periodic ones with at "
+                     "most 4 bonds per monomer")
 
 
-def ref_available(walls: int = 0) -> bool:
-    return os.path.exists(_ref_path(walls))
+def _conn(sys) -> int:
+    return int(np.max(sys.nbr_count)) if sys.n else 0
 
 
-def ref_lib(walls: int = 0):
-    path = _ref_path(walls)
+def ref_available(walls: int = 0, conn: int = 0) -> bool:
+    return os.path.exists(_ref_path(walls, conn))
+
+
+def ref_lib(walls: int = 0, conn: int = 0):
+    path = _ref_path(walls, conn)
     if path not in _ref:
         R = C.CDLL(path)
         R.bfmref_run.argtypes = [C.c_int, C.c_uint32, _i32p, _u32p, _u32p, C.c_uint32, _u32p, _u8p,
                                  _u32p, C.c_uint64, _u32p, C.c_uint32, _i32p, _u64p, C.c_char_p, C.c_int]
         R.bfmref_run.restype = C.c_int
+        R.bfmref_time.argtypes = [C.c_int, C.c_uint32, _i32p, _u32p, _u32p, C.c_uint32, _u32p, _u8p,
+                                  _u32p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
+                                  C.POINTER(C.c_float), C.POINTER(C.c_double), _i32p, C.c_char_p, C.c_int]
+        R.bfmref_time.restype = C.c_int
+        R.bfmref_max_connectivity.argtypes = []
+        R.bfmref_max_connectivity.restype = C.c_int
         _ref[path] = R
     return _ref[path]
 
 
 def ref_run(sys, draws, chunks, gpu: int = 0):
-    """Runs the reference updater (its own kernels; the NONPERIODICITY build for a box with walls)
-    with the given draw list; chunks are the nMCS of successive runSimulationOnGPU calls. Returns
-    positions and the number of draws used."""
+    """Runs the reference updater (its own kernels; the NONPERIODICITY build for a box with walls,
+    the MAX_CONNECTIVITY 8 build for more than 4 bonds per monomer) with the given draw list; chunks
+    are the nMCS of successive runSimulationOnGPU calls. Returns positions and the number of draws
+    used."""
     xyz, cnt, ids, box, forb = _arrs(sys)
     out = np.zeros_like(xyz)
     used = np.zeros(1, dtype=np.uint64)
     err = C.create_string_buffer(1024)
     d = np.ascontiguousarray(draws, dtype=np.uint32)
     ch = np.ascontiguousarray(chunks, dtype=np.uint32)
-    rc = ref_lib(sys.walls).bfmref_run(gpu, sys.n, xyz, cnt, ids, sys.maxc, box, forb, d, len(d), ch, len(ch),
-                                       out, used, err, 1024)
+    rc = ref_lib(sys.walls, _conn(sys)).bfmref_run(gpu, sys.n, xyz, cnt, ids, sys.maxc, box, forb, d, len(d), ch,
+                                                   len(ch), out, used, err, 1024)
     if rc != 0:
         raise RuntimeError(f"reference updater failed ({rc}): {err.value.decode()}")
     return out.reshape(-1, 3), int(used[0])
+
+
+def ref_time(sys, warm_mcs: int, timed_mcs: int, reps: int = 1, gpu: int = 0):
+    """Times the reference updater on the system with the counter draw stream of its seed: one
+    untimed runSimulationOnGPU(warm_mcs), then `reps` timed calls of timed_mcs MCS. Returns
+    (device ms, host seconds, final positions), sums over the timed calls; every call includes the
+    reference's own copy-back of the positions."""
+    xyz, cnt, ids, box, forb = _arrs(sys)
+    n_colors = int(color(sys).max()) + 1 if sys.n else 1
+    draws = counter_draws(sys.seed, 0, 2 * n_colors * (warm_mcs + reps * timed_mcs))
+    out = np.zeros_like(xyz)
+    ms = C.c_float(0.0)
+    wall = C.c_double(0.0)
+    err = C.create_string_buffer(1024)
+    rc = ref_lib(sys.walls, _conn(sys)).bfmref_time(gpu, sys.n, xyz, cnt, ids, sys.maxc, box, forb, draws,
+                                                    len(draws), warm_mcs, timed_mcs, reps, C.byref(ms),
+                                                    C.byref(wall), out, err, 1024)
+    if rc != 0:
+        raise RuntimeError(f"reference updater failed ({rc}): {err.value.decode()}")
+    return float(ms.value), float(wall.value), out.reshape(-1, 3)
 
 
 # ------------------------------------------------------------------ observables (int64 recomputation)

@@ -2,6 +2,7 @@
 reference updater itself (src/pscbfm/UpdaterGPUScBFM_AB_Type.cu + CRITICAL.cu, compiled for sm_100a
 by oracle/Makefile) fed the engine's counter draw stream; see make_golden.py. Every case respects
 the reference's limits: at most 4 bonds per monomer and int16 coordinates."""
+import functools
 import hashlib
 import os
 import sys
@@ -70,3 +71,31 @@ WALL_CASES = {
 }
 CASES.update(WALL_CASES)
 FAST.extend(WALL_CASES)
+
+
+# The configs at their stated run lengths, pinned against the reference updater: the 256^3 melt for
+# 10^4 MCS (seed 7), the 128^3 six-functional network for 10^5 MCS (seed 3; the reference's
+# MAX_CONNECTIVITY 8 build) and every one of the 256 ensemble systems for 10^4 MCS alone (seeds
+# 1000 + i). Generated by make_golden.py --long into reference_long.json.
+LONG_JSON = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_long.json")
+ENSEMBLE_MCS = 10000
+LONG_CASES = {
+    "melt256_16384x64_10000mcs": (S.dense_melt, [10000]),
+    "network128_512x6_100000mcs": (S.crosslinked_network, [100000]),
+}
+
+
+@functools.lru_cache(maxsize=1)
+def _ensemble():
+    return tuple(S.ensemble())
+
+
+def ensemble_case(i: int):
+    """Member i of the 256-system ensemble (box, chain length and volume fraction drawn from the
+    ensemble's generator seed; seed 1000 + i)."""
+    return _ensemble()[i]
+
+
+def ensemble_cases():
+    return {f"ensemble256_{i:03d}_{ENSEMBLE_MCS}mcs": (lambda i=i: ensemble_case(i), [ENSEMBLE_MCS])
+            for i in range(256)}

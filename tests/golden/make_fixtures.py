@@ -3,7 +3,7 @@ with pscbfm_b200.bfm_io.read_bfm, so that the tests need neither the reference t
 files. Positions are stored as int16 (the reference's coordinate type), neighbour lists as the
 directed (owner, target) pairs in list order, plus the box, periodicity and forbidden-bond table.
 
-    python tests/golden/make_fixtures.py [/path/to/pscbfm/tests]
+    python tests/golden/make_fixtures.py [/path/to/pscbfm/tests]   (default: $PSCBFM_REFERENCE/tests)
 """
 import os
 import sys
@@ -36,4 +36,5 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/tests")
+    tree = os.environ.get("PSCBFM_REFERENCE", "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(tree, "tests"))
