@@ -189,6 +189,17 @@ int bfm_run_timed(bfm_handle h, int32_t n_mcs, float* ms);
 int bfm_time_kernels(bfm_handle h, int32_t n_mcs, double out[4]);
 /* Kernels this handle has launched so far (graph replays counted per kernel). */
 int bfm_launch_count(bfm_handle h, uint64_t* out);
+/* Bytes the run and read-back calls of this handle have copied so far: out[0] host -> device (step
+ * entries; with the counter draw stream on the graph path only the first entry of a chain, the
+ * device makes the rest), out[1] device -> host (positions, move counters). Set-up uploads are not
+ * counted. */
+int bfm_transfer_bytes(bfm_handle h, uint64_t out[2]);
+/* Device probes for the sweep's latency model, on GPU gpu: out = {L2 hit latency in ns (dependent
+ * loads of a random cycle through 8 MB, one per 128-byte line), L2 read bandwidth in GB/s (32 MB
+ * read 20 times by every SM), period in us of back-to-back empty kernels of 1024 x 256 threads in a
+ * captured graph, SM count}. Allocates and frees about 40 MB; synchronises the device's work on
+ * its own stream only. */
+int bfm_probe_device(int gpu, double out[4]);
 
 /* ------------------------------------------------------------------ host-only helpers (no GPU needed) */
 /* The colouring step of initialize (graphColoring.tpp:77-293 with uniform rebalancing,
@@ -278,7 +289,8 @@ const char* bfm_server_last_error(bfm_server_handle s);
  * loops where cudaMalloc/cudaFree would synchronise the device. The caller owns every input and
  * output buffer; the engine's scratch is one fixed 32 MiB device array inside the library, held by
  * every GPU that loads it until the process exits. Systems needing more scratch than that
- * (roughly npad * 9 B + box volume / 4 B) are rejected with BFM_ERR_INVALID_ARGUMENT. The first
+ * (npad * 9 B + 3/8 B per box site + about 140 KB of tables and sub-step entries) are rejected
+ * with BFM_ERR_INVALID_ARGUMENT. Boxes are periodic along all three axes. The first
  * call on a device performs a one-time set-up (the scratch's device address) and should come
  * before any stream capture. All calls share the scratch: calls that overlap on the GPU race. */
 typedef struct bfm_noalloc_system {

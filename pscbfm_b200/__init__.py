@@ -7,6 +7,6 @@ the build script (build.py).
 """
 from .updater import UpdaterGPUScBFM_AB_Type, Batch, MODE_AUTO, MODE_LAUNCH, MODE_GRAPH, MODE_RESIDENT  # noqa: F401
 from .updater import MODE_PERSISTENT, MODE_CLUSTER  # noqa: F401
-from .updater import REPR_AUTO, REPR_GATHER, Server  # noqa: F401
+from .updater import REPR_AUTO, REPR_GATHER, Server, probe_device  # noqa: F401
 from ._lib import BfmCudaError, BfmBudgetError, BfmBusy  # noqa: F401
 from .sharding import shard_systems, run_sharded, batch_runner  # noqa: F401

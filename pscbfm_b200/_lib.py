@@ -99,6 +99,8 @@ _SIGS = {
     "bfm_reset_msd_reference": [H],
     "bfm_time_kernels": [H, C.c_int32, _f64p],
     "bfm_launch_count": [H, C.POINTER(C.c_uint64)],
+    "bfm_transfer_bytes": [H, C.POINTER(C.c_uint64)],
+    "bfm_probe_device": [C.c_int, _f64p],
     "bfm_batch_create": [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p), C.c_uint32],
     "bfm_batch_destroy": [H],
     "bfm_batch_run": [H, C.c_int32],

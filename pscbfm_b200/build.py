@@ -22,7 +22,7 @@ COMMON = ["-std=c++17", "-O3", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", INCLUDE]
 CU_FLAGS = ARCH + ["-lineinfo", "--expt-relaxed-constexpr"]
 
 SOURCES = ["bfm_kernels.cu", "bfm_kernels_bc.cu", "bfm_observables.cu", "bfm_engine.cpp", "bfm_batch.cpp",
-           "bfm_color.cpp", "bfm_capi.cpp", "bfm_server.cpp", "bfm_noalloc.cu"]
+           "bfm_color.cpp", "bfm_capi.cpp", "bfm_server.cpp", "bfm_noalloc.cu", "bfm_probe.cu"]
 
 
 def _headers():

@@ -282,6 +282,14 @@ int bfm_launch_count(bfm_handle h, uint64_t* out)
         *out = h->u.launches();
     });
 }
+int bfm_transfer_bytes(bfm_handle h, uint64_t out[2])
+{
+    BFM_CALL(h, {
+        if (!out) throw std::invalid_argument("[bfm_transfer_bytes] null output");
+        out[0] = h->u.h2dBytes();
+        out[1] = h->u.d2hBytes();
+    });
+}
 
 // ---------------------------------------------------------------- server
 

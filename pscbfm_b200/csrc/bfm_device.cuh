@@ -72,6 +72,7 @@ struct SysDev {
     uint32_t codeMode;               // kCodeNone, kCode32, kCode64
     uint32_t walls;                  // bit a: axis a is not periodic (corners stay in [0, L-2])
     uint32_t npad, nwords, maxc, nColors;
+    struct StepGen* gen;             // device-side producer of the counter stream's sub-step entries
     uint32_t mask[3];                // lattice side - 1 (a power of two; the box side but along a
                                      // walled axis whose side is not one)
     uint32_t lim[3];                 // box side - 1: on a walled axis a moved corner stays below it
@@ -118,6 +119,55 @@ struct StepEntry {
     uint32_t prevColor;
     uint32_t off, cnt, poff, pcnt;
 };
+
+// Counter draw stream: draw k of seed s is the upper 32 bits of SplitMix64(SplitMix64(s) +
+// (k + 1) * golden gamma) (Steele, Lea & Flood 2014); sub-step t consumes draws 2t (its colour,
+// draw % nColors) and 2t + 1 (its seed), the reference's order (CRITICAL.cu:509-510).
+__host__ __device__ __forceinline__ uint64_t sm64_mix(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__host__ __device__ __forceinline__ uint32_t counter_draw(uint64_t seed, uint64_t k)
+{
+    return (uint32_t)(sm64_mix(sm64_mix(seed) + (k + 1) * 0x9E3779B97F4A7C15ull) >> 32);
+}
+
+// Device-side producer of sub-step entries for the counter stream (one per system, in its arena).
+// A perform launch given a `next` slot writes the entry of sub-step `next` there (on != 0): its
+// colour and seed from the counter stream of `seed`, its previous colour = the colour of sub-step
+// next - 1, the one the launch performs; then it advances `next`. Consecutive launches of a
+// captured graph so hand each other their entries without a host copy.
+struct StepGen {
+    unsigned long long seed;
+    unsigned long long next;   // sub-step index of the next entry to write
+    uint32_t on;               // 0: the host supplies the entries (another draw stream)
+    uint32_t nColors;
+    uint32_t pad[2];
+};
+static_assert(sizeof(StepGen) == sizeof(StepEntry), "StepGen takes one entry slot before the entries");
+
+// Written by one thread: the entry of sub-step g->next into *out (see StepGen).
+__device__ __forceinline__ void write_next_step(StepGen* g, uint32_t const* grp, StepEntry* out)
+{
+    StepGen const s = *g;
+    if (!s.on) return;
+    uint64_t const t = s.next;
+    uint32_t const c = counter_draw(s.seed, 2 * t) % s.nColors;
+    uint32_t const pc = counter_draw(s.seed, 2 * (t - 1)) % s.nColors;
+    StepEntry e;
+    e.color = c;
+    e.seed = counter_draw(s.seed, 2 * t + 1);
+    e.parity = (uint32_t)(t & 1u);
+    e.prevColor = pc;
+    e.off = grp[2 * c];
+    e.cnt = grp[2 * c + 1];
+    e.poff = grp[2 * pc];
+    e.pcnt = grp[2 * pc + 1];
+    *out = e;
+    g->next = t + 1;
+}
 
 // Move-direction hash, src/pscbfm/CRITICAL.cu:2-11 (Jenkins' 6-shift 32-bit integer hash).
 // The constants and shifts must stay as they are: they define the trajectory.

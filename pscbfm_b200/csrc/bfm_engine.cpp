@@ -89,7 +89,7 @@ ArenaLayout arena_layout(uint32_t n, uint32_t npad, uint32_t maxc, uint32_t nwor
     L.grp = take(4ull * 2 * nColors);
     L.stats = take(kStatBytes);
     L.desc = take(sizeof(SysDev));
-    L.steps = take(sizeof(StepEntry) * kStepCap);
+    L.steps = take(sizeof(StepEntry) * (kStepCap + 1));   // the StepGen, then the entries
     L.list = take(4);
     L.gs = take(sizeof(GridSync));
     L.pk = take(4ull * npad);
@@ -432,7 +432,8 @@ void Updater::initialize()
     for (uint32_t i = 0; i < 512; ++i)
         if (forbidden_[i]) h.forbid[i >> 5] |= 1u << (i & 31);
     dev_.dDesc = reinterpret_cast<SysDev*>(base + L.desc);
-    dev_.dSteps = reinterpret_cast<StepEntry*>(base + L.steps);
+    h.gen = reinterpret_cast<StepGen*>(base + L.steps);
+    dev_.dSteps = reinterpret_cast<StepEntry*>(base + L.steps) + 1;
     dev_.stepCap = kStepCap;
     dev_.dList = reinterpret_cast<uint32_t*>(base + L.list);
     dev_.gs = reinterpret_cast<GridSync*>(base + L.gs);
@@ -497,6 +498,7 @@ void Updater::initialize()
     cuda_check(cudaMemcpyAsync(dev_.dDesc, &h, sizeof(SysDev), cudaMemcpyHostToDevice, s), "upload descriptor");
     cuda_check(cudaMemsetAsync(dev_.dList, 0, 4, s), "memset list");
     cuda_check(cudaMemsetAsync(dev_.gs, 0, sizeof(GridSync), s), "memset grid barrier");
+    cuda_check(cudaMemsetAsync(h.gen, 0, sizeof(StepGen), s), "memset step producer");   // off
     if (segs) cuda_check(cudaMemsetAsync(h.mcount, 0, 4ull * 2 * segs, s), "memset mover counts");
     if (!stepsFree_) cuda_check(cudaEventCreateWithFlags(&stepsFree_, cudaEventDisableTiming), "cudaEventCreate");
     if (!batchOnly_) ensureStaging();
@@ -507,6 +509,8 @@ void Updater::initialize()
     mcsDone_ = 0;
     lastColor_ = kNoColor;
     hostStale_ = false;
+    chainValid_ = false;
+    genOn_ = 0;
 }
 
 void Updater::hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, std::vector<uint32_t>& nbrr) const
@@ -742,10 +746,19 @@ cudaError_t Updater::launchCheck(StepEntry const* e, cudaStream_t s) const
     return launch_check_bc(dev_.h, dev_.dDesc, nullptr, gridTiles(), e, codeMode_, s);
 }
 
-cudaError_t Updater::launchPerform(StepEntry const* e, cudaStream_t s) const
+cudaError_t Updater::launchPerform(StepEntry const* e, cudaStream_t s, PerformArgs const& pa) const
 {
-    if (codeMode_ == kCodeNone) return launch_perform(dev_.dDesc, nullptr, gridTiles(), kGridBlock, e, s);
-    return launch_perform_bc(dev_.h, dev_.dDesc, nullptr, gridTiles(), e, codeMode_, s);
+    if (codeMode_ == kCodeNone) return launch_perform(dev_.dDesc, nullptr, gridTiles(), kGridBlock, e, s, pa.next);
+    return launch_perform_bc(dev_.h, dev_.dDesc, nullptr, gridTiles(), e, codeMode_, s, -1, pa);
+}
+
+PerformArgs Updater::performArgs(StepEntry const& e)
+{
+    // what the host knows of the sub-step: its parity, and whether the previous sub-step left marks
+    PerformArgs pa;
+    pa.parity = e.parity;
+    pa.scope = (e.color != kNoColor ? kPerfCur : 0u) | (e.prevColor != kNoColor ? kPerfPrev : 0u);
+    return pa;
 }
 
 size_t Updater::residentSmem() const
@@ -791,6 +804,7 @@ StepEntry Updater::nextStep()
 void Updater::fillSteps(uint32_t nSteps, StepEntry* buf, bool)
 {
     for (uint32_t t = 0; t < nSteps; ++t) buf[t] = nextStep();
+    chainValid_ = false;   // the host's entries go to the device's entry slots
 }
 
 void Updater::ensureStaging()
@@ -801,14 +815,18 @@ void Updater::ensureStaging()
     // one extra entry holds the copy of the persistent kernel's barrier state, and after it the
     // copy of the move counters
     static_assert(sizeof(GridSync) <= sizeof(StepEntry), "GridSync fits one staging entry");
+    // (entry kStepCap), then the producer's state and the first entry of a chain (kStepCap + 1,
+    // kStepCap + 2, copied together to the producer's slot and the first entry slot)
     void* p = nullptr;
-    cuda_check(cudaHostAlloc(&p, sizeof(StepEntry) * (kStepCap + 1) + kStatBytes, cudaHostAllocMapped),
+    cuda_check(cudaHostAlloc(&p, sizeof(StepEntry) * (kStepCap + 3) + kStatBytes, cudaHostAllocMapped),
                "cudaHostAlloc(steps)");
     hSteps_ = static_cast<StepEntry*>(p);
     hStepCap_ = kStepCap;
     hGs_ = reinterpret_cast<GridSync*>(hSteps_ + kStepCap);
     std::memset(hGs_, 0, sizeof(GridSync));
-    hStats_ = reinterpret_cast<unsigned long long*>(hSteps_ + kStepCap + 1);
+    hGen_ = reinterpret_cast<StepGen*>(hSteps_ + kStepCap + 1);
+    hStats_ = reinterpret_cast<unsigned long long*>(hSteps_ + kStepCap + 3);
+    if (!genFree_) cuda_check(cudaEventCreateWithFlags(&genFree_, cudaEventDisableTiming), "cudaEventCreate");
     void* d = nullptr;
     cuda_check(cudaHostGetDevicePointer(&d, hStats_, 0), "stats staging device address");
     dStats_ = static_cast<unsigned long long*>(d);
@@ -823,9 +841,11 @@ void Updater::scrubPending(cudaStream_t s)
     hSteps_[0] = StepEntry{kNoColor, 0u, (uint32_t)(subStep_ & 1u), lastColor_, 0u, 0u, grpOff_[lastColor_],
                            grpSize_[lastColor_]};
     cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry), cudaMemcpyHostToDevice, s), "steps H2D");
+    h2dBytes_ += sizeof(StepEntry);
     cuda_check(cudaEventRecord(stepsFree_, s), "event");
+    chainValid_ = false;
     // both representations scrub the previous sub-step's marks in the perform
-    cuda_check(launchPerform(dev_.dSteps, s), "scrub");
+    cuda_check(launchPerform(dev_.dSteps, s, performArgs(hSteps_[0])), "scrub");
     ++launches_;
     lastColor_ = kNoColor;
 }
@@ -846,26 +866,35 @@ void Updater::enqueueLaunch(uint32_t nSteps)
         fillSteps(chunk, hSteps_, false);
         cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
                    "steps H2D");
+        h2dBytes_ += sizeof(StepEntry) * chunk;
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         for (uint32_t t = 0; t < chunk; ++t) {
             cuda_check(launchCheck(dev_.dSteps + t, stream_), "check");
-            cuda_check(launchPerform(dev_.dSteps + t, stream_), "perform");
+            cuda_check(launchPerform(dev_.dSteps + t, stream_, performArgs(hSteps_[t])), "perform");
         }
         launches_ += 2ull * chunk;
         done += chunk;
     }
 }
 
-cudaGraphExec_t Updater::graphFor(uint32_t nSteps)
+cudaGraphExec_t Updater::graphFor(uint32_t nSteps, uint32_t parity0)
 {
     for (auto const& g : graphs_)
-        if (g.first == nSteps) return g.second;
+        if (g.nSteps == nSteps && g.parity0 == parity0) return g.exec;
+    // node t performs the sub-step whose entry sits in slot t and, in a graph of two or more
+    // sub-steps, writes the entry of the next one into slot t + 1 (the last node into slot 0,
+    // where the next replay starts) when the device producer is on; the perform's parity is a
+    // launch parameter, so a graph is captured per length and parity of its first sub-step
     cudaGraph_t g;
     cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t err = cudaSuccess;
     for (uint32_t t = 0; t < nSteps && err == cudaSuccess; ++t) {
         err = launchCheck(dev_.dSteps + t, stream_);
-        if (err == cudaSuccess) err = launchPerform(dev_.dSteps + t, stream_);
+        PerformArgs pa;
+        pa.parity = (parity0 + t) & 1u;
+        pa.scope = kPerfCur | kPerfPrev;   // a scrub with no marks pending only zeroes zero words
+        pa.next = nSteps >= 2 ? dev_.dSteps + (t + 1) % nSteps : nullptr;
+        if (err == cudaSuccess) err = launchPerform(dev_.dSteps + t, stream_, pa);
     }
     cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
     cuda_check(err, "capture launches");
@@ -874,31 +903,77 @@ cudaGraphExec_t Updater::graphFor(uint32_t nSteps)
     cudaError_t const instErr = cudaGraphInstantiate(&exec, g, 0);
     cudaGraphDestroy(g);
     cuda_check(instErr, "graph instantiate");
-    graphs_.emplace_back(nSteps, exec);
+    graphs_.push_back({nSteps, parity0, exec});
     return exec;
 }
 
 void Updater::prepareGraphs(uint32_t nSteps)
 {
+    // the (length, first parity) of every chunk a graph-path run of nSteps from here replays: the
+    // full chunks start at no more than two parities, then the tail
     uint32_t const G = std::min(kGraphMcs * (uint32_t)grpSize_.size(), hStepCap_);
-    if (nSteps >= G) graphFor(G);
-    if (nSteps % G) graphFor(nSteps % G);
+    uint32_t const full = nSteps / G, rest = nSteps % G;
+    for (uint32_t k = 0; k < full && k < 2; ++k) graphFor(G, (uint32_t)((subStep_ + (uint64_t)k * G) & 1u));
+    if (rest) graphFor(rest, (uint32_t)((subStep_ + (uint64_t)full * G) & 1u));
+}
+
+void Updater::seedChain(cudaStream_t s)
+{
+    // the first entry of a chain from the host, with the producer's state: one copy
+    cuda_check(cudaEventSynchronize(genFree_), "producer staging");
+    StepEntry const e0 = nextStep();
+    hGen_[0] = StepGen{drawSeed_, subStep_, 1u, (uint32_t)grpSize_.size(), {0u, 0u}};
+    std::memcpy(reinterpret_cast<StepEntry*>(hGen_) + 1, &e0, sizeof(StepEntry));
+    cuda_check(cudaMemcpyAsync(dev_.h.gen, hGen_, 2 * sizeof(StepEntry), cudaMemcpyHostToDevice, s), "chain H2D");
+    h2dBytes_ += 2 * sizeof(StepEntry);
+    cuda_check(cudaEventRecord(genFree_, s), "event");
+    genOn_ = 1;
+}
+
+void Updater::producerOff(cudaStream_t s)
+{
+    // host-made entries in the slots a captured graph reads: its nodes must not overwrite them
+    if (genOn_ == 0) return;
+    cuda_check(cudaEventSynchronize(genFree_), "producer staging");
+    hGen_[0] = StepGen{0ull, 0ull, 0u, 0u, {0u, 0u}};
+    cuda_check(cudaMemcpyAsync(dev_.h.gen, hGen_, sizeof(StepGen), cudaMemcpyHostToDevice, s), "producer off");
+    h2dBytes_ += sizeof(StepGen);
+    cuda_check(cudaEventRecord(genFree_, s), "event");
+    genOn_ = 0;
 }
 
 void Updater::enqueueGraph(uint32_t nSteps)
 {
     // full chunks of kGraphMcs MCS replay one graph; a shorter tail (or a short run) replays a
-    // graph of its own length, captured once and kept
+    // graph of its own length, captured once and kept. With the counter stream the device makes
+    // the entries: the host copies only the first entry of a chain (and the producer's state)
+    // when the device's chain does not continue from the host's position, otherwise nothing.
     uint32_t const nC = (uint32_t)grpSize_.size();
     uint32_t const G = std::min(kGraphMcs * nC, hStepCap_);
     for (uint32_t done = 0; done < nSteps;) {
         uint32_t const chunk = std::min(G, nSteps - done);
-        cudaGraphExec_t const exec = graphFor(chunk);
-        cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
-        fillSteps(chunk, hSteps_, false);
-        cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
-                   "steps H2D");
-        cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
+        cudaGraphExec_t const exec = graphFor(chunk, (uint32_t)(subStep_ & 1u));
+        if (drawKind_ == kDrawCounter && chunk >= 2) {
+            uint32_t todo = chunk;
+            if (!(chainValid_ && chainSub_ == subStep_ && chainPrev_ == lastColor_ && chainSeed_ == drawSeed_)) {
+                seedChain(stream_);   // consumes the chunk's first sub-step
+                --todo;
+            }
+            for (uint32_t t = 0; t < todo; ++t) nextStep();   // the host's copy of the position
+            chainValid_ = true;
+            chainSub_ = subStep_;
+            chainPrev_ = lastColor_;
+            chainSeed_ = drawSeed_;
+        } else {
+            producerOff(stream_);
+            cuda_check(cudaEventSynchronize(stepsFree_), "steps staging");
+            fillSteps(chunk, hSteps_, false);
+            cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice,
+                                       stream_),
+                       "steps H2D");
+            h2dBytes_ += sizeof(StepEntry) * chunk;
+            cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
+        }
         cuda_check(cudaGraphLaunch(exec, stream_), "graph launch");
         launches_ += 2ull * chunk;
         done += chunk;
@@ -948,12 +1023,13 @@ void Updater::timeKernels(int32_t nMcs, double out[4])
         fillSteps(chunk, hSteps_, false);
         cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
                    "steps H2D");
+        h2dBytes_ += sizeof(StepEntry) * chunk;
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         for (uint32_t t = 0; t < chunk; ++t) {
             cuda_check(cudaEventRecord(ev[0], stream_), "event");
             cuda_check(launchCheck(dev_.dSteps + t, stream_), "check");
             cuda_check(cudaEventRecord(ev[1], stream_), "event");
-            cuda_check(launchPerform(dev_.dSteps + t, stream_), "perform");
+            cuda_check(launchPerform(dev_.dSteps + t, stream_, performArgs(hSteps_[t])), "perform");
             cuda_check(cudaEventRecord(ev[2], stream_), "event");
             cuda_check(cudaEventSynchronize(ev[2]), "timed kernels");
             float a = 0, b = 0;
@@ -987,6 +1063,7 @@ void Updater::enqueueResident(uint32_t nSteps)
         fillSteps(chunk, hSteps_, true);
         cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
                    "steps H2D");
+        h2dBytes_ += sizeof(StepEntry) * chunk;
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         cuda_check(codeMode_ == kCodeNone
                        ? launch_resident(dev_.dDesc, dev_.dList, 1, per, dev_.dSteps, 1, chunk, smem, stream_)
@@ -1046,6 +1123,7 @@ void Updater::enqueueCluster(uint32_t nSteps)
         fillSteps(chunk, hSteps_, true);
         cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
                    "steps H2D");
+        h2dBytes_ += sizeof(StepEntry) * chunk;
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         cuda_check(launch_cluster_bc(dev_.dDesc, dev_.dList, 1, clusterLogC_, clusterPer_, dev_.dSteps, 1, chunk,
                                      clusterSmem_, codeMode_, stream_),
@@ -1134,6 +1212,7 @@ void Updater::enqueuePersistent(uint32_t nSteps)
         fillSteps(chunk, hSteps_, false);
         cuda_check(cudaMemcpyAsync(dev_.dSteps, hSteps_, sizeof(StepEntry) * chunk, cudaMemcpyHostToDevice, stream_),
                    "steps H2D");
+        h2dBytes_ += sizeof(StepEntry) * chunk;
         cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         // the arrival count restarts at 0 (an injected stall starts it at 0x80808080, from where no
         // barrier's target is reached); the fault word stays set once a launch has failed
@@ -1151,6 +1230,7 @@ void Updater::enqueuePersistent(uint32_t nSteps)
     }
     // the fault word comes back with the next synchronisation
     cuda_check(cudaMemcpyAsync(hGs_, dev_.gs, sizeof(GridSync), cudaMemcpyDeviceToHost, stream_), "grid status");
+    d2hBytes_ += sizeof(GridSync);
     gsPending_ = true;
 }
 
@@ -1187,6 +1267,7 @@ void Updater::downloadPositions(int32_t* out)
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
     cuda_check(launch_gather_positions(dev_.h, dev_.slotOf, n_, dev_.xyzOut, stream_), "gather positions");
     cuda_check(cudaMemcpyAsync(out, dev_.xyzOut, 12ull * n_, cudaMemcpyDeviceToHost, stream_), "download positions");
+    d2hBytes_ += 12ull * n_;
     synchronize();
 }
 
@@ -1274,6 +1355,7 @@ void Updater::stats(uint64_t out[4])
     // the sums written into the mapped pinned staging by a kernel on the stream
     ensureStaging();
     cuda_check(launch_publish_stats(dev_.h.stats, dStats_, stream_), "stats");
+    d2hBytes_ += 3 * sizeof(unsigned long long);   // written into mapped host memory
     cuda_check(cudaStreamSynchronize(stream_), "stats");
     std::atomic_thread_fence(std::memory_order_acquire);
     unsigned long long const volatile* const sums = hStats_;
@@ -1299,6 +1381,7 @@ uint64_t Updater::statsEnqueue()
     uint64_t const t = ++statNext_;
     uint32_t const k = (uint32_t)(t % kStatRing);
     cuda_check(launch_publish_stats(dev_.h.stats, dStatRing_ + 4ull * k, stream_), "stats");
+    d2hBytes_ += 3 * sizeof(unsigned long long);   // written into mapped host memory
     cuda_check(cudaEventRecord(statEv_[k], stream_), "event");
     statTicket_[k] = t;
     statMcs_[k] = mcsDone_;
@@ -1397,7 +1480,7 @@ void Updater::validate()
 void Updater::freeDevice()
 {
     if (!graphs_.empty() && stream_) cudaStreamSynchronize(stream_);   // no graph of ours in flight
-    for (auto& g : graphs_) cudaGraphExecDestroy(g.second);
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
     graphs_.clear();
     // stream-ordered frees: after this system's queued work (and whatever its stream waits on,
     // such as the end of a Batch run), without waiting on the host or for other streams
@@ -1412,10 +1495,18 @@ void Updater::freeDevice()
     dObsOut_ = nullptr;
     nMol_ = 0;
     molSize_.clear();
+    if (genFree_) {
+        cudaEventSynchronize(genFree_);
+        cudaEventDestroy(genFree_);
+        genFree_ = nullptr;
+    }
+    chainValid_ = false;
+    genOn_ = 0;
     if (hSteps_) {
         cudaFreeHost(hSteps_);
         hSteps_ = nullptr;
         hGs_ = nullptr;
+        hGen_ = nullptr;
         hStats_ = nullptr;
         dStats_ = nullptr;
         gsPending_ = false;

@@ -47,17 +47,7 @@ size_t observables_bytes(uint32_t npad, uint32_t nMol);
 enum DrawKind : int { kDrawCounter = 0, kDrawCallback = 1 };
 using DrawFn = uint32_t (*)(void*);
 
-// SplitMix64 finaliser (Steele, Lea & Flood 2014), keyed counter stream.
-inline uint64_t sm64_mix(uint64_t z)
-{
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-}
-inline uint32_t counter_draw(uint64_t seed, uint64_t k)
-{
-    return (uint32_t)(sm64_mix(sm64_mix(seed) + (k + 1) * 0x9E3779B97F4A7C15ull) >> 32);
-}
+// The counter stream's draws: counter_draw (bfm_device.cuh).
 
 // Engine path of one updater's run().
 enum Mode : int {
@@ -169,6 +159,10 @@ public:
     int path() const;                        // the path the next run takes (BFM_MODE_*)
     void timeKernels(int32_t nMcs, double out[4]);   // check ms, perform ms, launches of each
     uint64_t launches() const { return launches_; }  // kernels launched by this handle so far
+    // bytes the run and read-back calls have moved host -> device and device -> host so far
+    // (step entries, chain starts, positions, move counters; not the set-up's uploads)
+    uint64_t h2dBytes() const { return h2dBytes_; }
+    uint64_t d2hBytes() const { return d2hBytes_; }
     void addLaunches(uint64_t n) { launches_ += n; }
 
 private:
@@ -228,6 +222,14 @@ private:
     bool hostStale_ = false;
     Device dev_;
     StepEntry* hSteps_ = nullptr;              // pinned staging for step entries
+    StepGen* hGen_ = nullptr;                  // pinned staging of a chain's start: producer + first entry
+    cudaEvent_t genFree_ = nullptr;            // hGen_ may be rewritten after this event
+    // the device's entry chain (graph path, counter stream): slot 0 holds the entry of sub-step
+    // chainSub_ with previous colour chainPrev_ of the stream of chainSeed_ while chainValid_
+    bool chainValid_ = false;
+    uint64_t chainSub_ = 0, chainSeed_ = 0;
+    uint32_t chainPrev_ = kNoColor;
+    uint32_t genOn_ = 0;                       // the device producer's `on`, as last written
     GridSync* hGs_ = nullptr;                  // pinned copy of the persistent kernel's barrier state
     unsigned long long* hStats_ = nullptr;     // pinned copy of the move counters (stats)
     unsigned long long* hStatRing_ = nullptr;  // kStatRing mapped pinned slots (statsEnqueue)
@@ -243,9 +245,14 @@ private:
     size_t clusterSmem_ = 0;                   // dynamic shared memory per CTA
     uint32_t clusterTier_ = 0;                 // 3: AUTO takes the plan, 2: a Batch does, 1: forced only
     uint32_t hStepCap_ = 0;
-    std::vector<std::pair<uint32_t, cudaGraphExec_t>> graphs_;   // captured chunk length -> graph
+    struct GraphExec {
+        uint32_t nSteps, parity0;               // chunk length, parity of its first sub-step
+        cudaGraphExec_t exec;
+    };
+    std::vector<GraphExec> graphs_;
     cudaEvent_t stepsFree_ = nullptr;          // host staging may be rewritten after this event
     uint64_t launches_ = 0;
+    uint64_t h2dBytes_ = 0, d2hBytes_ = 0;
     int repr_ = 0;
     uint32_t codeMode_ = kCodeNone;
     uint32_t nMol_ = 0;
@@ -255,7 +262,9 @@ private:
     long long* dObsOut_ = nullptr;
     void buildObservables();
     std::vector<uint32_t> moleculeRoots() const;   // lowest monomer id of each monomer's molecule
-    cudaGraphExec_t graphFor(uint32_t nSteps);
+    cudaGraphExec_t graphFor(uint32_t nSteps, uint32_t parity0);
+    void seedChain(cudaStream_t s);           // the device chain restarts at the host's position
+    void producerOff(cudaStream_t s);         // the device producer stops writing entries
     int effectiveMode() const;                // the path run() takes (mode_ with AUTO resolved)
     int autoMode() const;                     // the path BFM_MODE_AUTO takes for this system
     void prepareGraphs(uint32_t nSteps);      // capture the graphs a graph-path run of nSteps replays
@@ -269,7 +278,8 @@ public:
     uint32_t codeMode() const { return codeMode_; }
     uint32_t gridTiles() const;                               // CTAs of one grid-phase launch
     cudaError_t launchCheck(StepEntry const* e, cudaStream_t s) const;
-    cudaError_t launchPerform(StepEntry const* e, cudaStream_t s) const;
+    cudaError_t launchPerform(StepEntry const* e, cudaStream_t s, PerformArgs const& pa) const;
+    static PerformArgs performArgs(StepEntry const& e);   // parity and scope of a host-made entry
     size_t residentSmem() const;
 };
 

@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(kGridBlock) k_check(SysDev const* __restrict__
 
 __global__ void __launch_bounds__(kGridBlock) k_perform(SysDev const* __restrict__ sysv,
                                                         TileRef const* __restrict__ tiles, uint32_t tileSpan,
-                                                        StepEntry const* __restrict__ steps)
+                                                        StepEntry const* __restrict__ steps, StepEntry* next)
 {
     __shared__ SysDev S;
     __shared__ uint32_t tally;
@@ -125,6 +125,8 @@ __global__ void __launch_bounds__(kGridBlock) k_perform(SysDev const* __restrict
     load_sys(S, sysv + tr.sys);
     if (threadIdx.x == 0) tally = 0;
     __syncthreads();
+    // one system in a captured graph: hand the next launch its entry (write_next_step)
+    if (next != nullptr && blockIdx.x == 0 && threadIdx.x == 0) write_next_step(S.gen, S.grp, next);
 
     // scrub the marks of the previous sub-step of this system (other parity)
     if (st.prevColor != kNoColor) {
@@ -354,10 +356,10 @@ cudaError_t launch_check(SysDev const* dSys, TileRef const* dTiles, uint32_t nTi
 }
 
 cudaError_t launch_perform(SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles, uint32_t tileSpan,
-                           StepEntry const* dSteps, cudaStream_t s)
+                           StepEntry const* dSteps, cudaStream_t s, StepEntry* next)
 {
     if (nTiles == 0) return cudaSuccess;
-    k_perform<<<nTiles, kGridBlock, 0, s>>>(dSys, dTiles, tileSpan, dSteps);
+    k_perform<<<nTiles, kGridBlock, 0, s>>>(dSys, dTiles, tileSpan, dSteps, next);
     return cudaGetLastError();
 }
 

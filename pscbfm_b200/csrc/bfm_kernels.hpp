@@ -28,8 +28,9 @@ struct TileRef {
 // dTiles == nullptr: single system 0, CTA b covers [b*tileSpan, (b+1)*tileSpan).
 cudaError_t launch_check(SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles, uint32_t tileSpan,
                          StepEntry const* dSteps, cudaStream_t s);
+// next != nullptr (one system): CTA 0 writes the following sub-step's entry there (write_next_step)
 cudaError_t launch_perform(SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles, uint32_t tileSpan,
-                           StepEntry const* dSteps, cudaStream_t s);
+                           StepEntry const* dSteps, cudaStream_t s, StepEntry* next = nullptr);
 
 // Resident kernel: CTA b runs system dList[b] through sub-steps 0..nSteps-1 of dSteps
 // ([nSteps][nSys] entries). perThread = ceil(largest colour group / kResidentBlock), in {1,2,4,8,16}.
@@ -47,13 +48,25 @@ constexpr uint32_t kBcTileSpan = kGridBlock * kCheckMpt;
 // budget (CTAs per SM) of the two kernels, 0 .. kGridShapes-1; negative: the default. Every shape
 // gives the same results.
 constexpr int kGridShapes = 4;
-// The perform launch's tile list for a check tile list of bond-code systems: consecutive tiles of one
-// system grouped four to an entry when the list holds at least four tiles per SM.
+// The perform launch's tile list for a check tile list of bond-code systems: one tile per entry.
 std::vector<TileRef> perform_tile_list(std::vector<TileRef> const& tiles);
 cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
                             StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1);
+// The perform takes one warp per tile. A single-system launch may carry the sub-step's parity and
+// scope (kPerfCur: walk its tentative movers, kPerfPrev: zero the previous sub-step's marks), so
+// it reads no step entry; parity == kParityFromEntry reads both from dSteps[0]. next != nullptr
+// (one system): CTA 0 writes the following sub-step's entry there (write_next_step). Tile lists
+// (several systems) always read each system's entry; parity, scope and next are ignored.
+constexpr uint32_t kParityFromEntry = 0xFFFFFFFFu;
+constexpr uint32_t kPerfCur = 1u, kPerfPrev = 2u;
+struct PerformArgs {
+    uint32_t parity = kParityFromEntry;
+    uint32_t scope = kPerfCur | kPerfPrev;
+    StepEntry* next = nullptr;
+};
 cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
-                              StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1);
+                              StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1,
+                              PerformArgs const& pa = PerformArgs{});
 // Persistent sweep (bond codes, one system): nSteps sub-steps of check, barrier, perform in one
 // launch of at most the co-resident CTA count: a grid of at most 16 CTAs as one thread-block
 // cluster (hardware barriers) where allowCluster and the device can run it, otherwise a

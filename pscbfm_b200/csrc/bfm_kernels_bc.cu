@@ -78,9 +78,10 @@ __device__ __forceinline__ T ldm(T const* p)
 // (nobody reads tmp[parity^1] during sub-step t, and the check of t+1, which marks it again,
 // comes after).
 constexpr uint32_t kEntSlotMask = (1u << 27) - 1u;
-// tiles whose movers one perform CTA of a single-system launch walks (about 17 % of a tile's
-// monomers are tentative, so one tile leaves most of a CTA idle)
-constexpr uint32_t kPerformTiles = 4;
+// Tentative movers a lane of the grid perform takes per pass over its tile's list: 32 x kPerfQ
+// entries, loaded together with the list's length (about a sixth of a dense tile's 512 monomers
+// move tentatively, so one pass covers a tile of a dense system; longer lists take more passes).
+constexpr int kPerfQ = 4;
 
 // ---------------------------------------------------------------------------------- check
 
@@ -155,37 +156,22 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
 
 // ---------------------------------------------------------------------------------- perform
 
-// Entries e, e + B, ... (MPT of them, those below total) of the concatenated mover lists of nT
-// tiles (pre: the lists' starting offsets, lbase / tbase: the first tile's segment of the entries
-// and of the target addresses): re-test the front plane on the temporary lattice and apply the
-// free moves. The plane and the old position follow from the target's address, so the monomer's
-// own address is not loaded. Returns the moves applied.
-template <typename W, int MPT, bool kNc>
-__device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t const* dtab,
-                                                  unsigned long long const* tcur, uint32_t const* lbase,
-                                                  uint32_t const* tbase, uint32_t const* pre, uint32_t nT,
-                                                  uint32_t total, uint32_t e)
+// Movers ent[q] (list entries: slot | direction << 27) with targets to[q], for the q with
+// live[q]: re-test the front plane on the temporary lattice and apply the free moves. The plane
+// and the old position follow from the target's address, so the monomer's own address is not
+// loaded. Returns the moves applied.
+template <typename W, int N, bool kNc>
+__device__ __forceinline__ uint32_t perform_movers(SysDev const& S, uint32_t const* dtab,
+                                                   unsigned long long const* tcur, uint32_t const (&ent)[N],
+                                                   uint32_t const (&to)[N], bool const (&live)[N])
 {
-    uint32_t const B = blockDim.x;
     uint32_t* const PK = S.pk;
     W* const CODE = static_cast<W*>(S.code);
-    uint32_t ent[MPT], to[MPT];
-    bool live[MPT];
+    Plane pl[N];
+    W code[N];
+    uint32_t nbr[N][CodeWord<W>::kSlots];
 #pragma unroll
-    for (int q = 0; q < MPT; ++q) {
-        uint32_t const eq = e + (uint32_t)q * B;
-        uint32_t j = 0;
-        while (j + 1 < nT && eq >= pre[j + 1]) ++j;
-        live[q] = eq < total;
-        uint32_t const li = j * kBcTileSpan + (eq - pre[j]);
-        ent[q] = live[q] ? ldm<kNc>(lbase + li) : 0u;
-        to[q] = live[q] ? ldm<kNc>(tbase + li) : 0u;
-    }
-    Plane pl[MPT];
-    W code[MPT];
-    uint32_t nbr[MPT][CodeWord<W>::kSlots];
-#pragma unroll
-    for (int q = 0; q < MPT; ++q) {
+    for (int q = 0; q < N; ++q) {
         uint32_t const g = ent[q] & kEntSlotMask;
         code[q] = live[q] ? CODE[g] : W(0);
 #pragma unroll
@@ -193,14 +179,14 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
             nbr[q][k] = (live[q] && k < S.maxc) ? __ldg(S.nbrr + (size_t)k * S.npad + g) : 0u;
     }
 #pragma unroll
-    for (int q = 0; q < MPT; ++q) {
+    for (int q = 0; q < N; ++q) {
         uint32_t const d = (ent[q] >> 27) & 7u;
         DirParams const D = dir_params(dtab, d);
         front_plane<false>(pl[q], S.planeTab, D, to[q], D.step, d);
     }
-    unsigned long long hit[MPT];
+    unsigned long long hit[N];
 #pragma unroll
-    for (int q = 0; q < MPT; ++q) {
+    for (int q = 0; q < N; ++q) {
         hit[q] = 0ull;
 #pragma unroll
         for (int r = 0; r < 4; ++r)
@@ -208,7 +194,7 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
     }
     uint32_t nAcc = 0;
 #pragma unroll
-    for (int q = 0; q < MPT; ++q) {
+    for (int q = 0; q < N; ++q) {
         if (!live[q] || hit[q] != 0ull) continue;
         ++nAcc;
         uint32_t const g = ent[q] & kEntSlotMask;
@@ -243,8 +229,34 @@ __device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t cons
     return nAcc;
 }
 
-// For tiles tile0 .. tile0+nT-1 (at most kPerformTiles): zeroes the temporary-lattice words the
-// previous sub-step's movers marked, then walks this sub-step's tentative movers as one dense range
+// Entries e, e + B, ... (MPT of them, those below total) of the concatenated mover lists of nT
+// tiles (pre: the lists' starting offsets, lbase / tbase: the first tile's segment of the entries
+// and of the target addresses), through perform_movers. Returns the moves applied.
+template <typename W, int MPT, bool kNc>
+__device__ __forceinline__ uint32_t perform_chunk(SysDev const& S, uint32_t const* dtab,
+                                                  unsigned long long const* tcur, uint32_t const* lbase,
+                                                  uint32_t const* tbase, uint32_t const* pre, uint32_t nT,
+                                                  uint32_t total, uint32_t e)
+{
+    uint32_t const B = blockDim.x;
+    uint32_t ent[MPT], to[MPT];
+    bool live[MPT];
+#pragma unroll
+    for (int q = 0; q < MPT; ++q) {
+        uint32_t const eq = e + (uint32_t)q * B;
+        uint32_t j = 0;
+        while (j + 1 < nT && eq >= pre[j + 1]) ++j;
+        live[q] = eq < total;
+        uint32_t const li = j * kBcTileSpan + (eq - pre[j]);
+        ent[q] = live[q] ? ldm<kNc>(lbase + li) : 0u;
+        to[q] = live[q] ? ldm<kNc>(tbase + li) : 0u;
+    }
+    return perform_movers<W, MPT, kNc>(S, dtab, tcur, ent, to, live);
+}
+
+// The persistent sweep's perform. For tiles tile0 .. tile0+nT-1 (at most 16): zeroes the
+// temporary-lattice words the previous sub-step's movers marked, then walks this sub-step's
+// tentative movers as one dense range
 // (no thread waits on a monomer that did not move). pre is 2 (nT+1) words of shared memory: the
 // starting offsets of the current and of the previous lists. A tile's list counts only if the
 // tile lies inside that sub-step's colour group (older lengths may remain in count[]). Every thread
@@ -303,6 +315,63 @@ __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* dt
     if (nAcc) atomicAdd(tally, nAcc);
 }
 
+// Grid-phase perform: one warp per tile. The warp walks list segment `tile` of this sub-step
+// (parity p: its tentative movers) and of the previous one (parity p ^ 1: it zeroes the
+// temporary-lattice words those movers marked). Every load of the first pass is independent of
+// the others: both list lengths and the first 32 kPerfQ entries and target addresses of both lists
+// come in one round trip, so no length scan or barrier precedes the movers' own loads; entries
+// past a list's end lie inside the tile's segment and are ignored. The lengths are exact for every
+// tile of the launch: a check CTA whose tile lies beyond its colour group stores a zero length.
+// Longer lists take further passes. Returns the moves applied.
+template <typename W, bool kNc>
+__device__ __forceinline__ uint32_t perform_tile(SysDev const& S, uint32_t const* dtab, uint32_t p, uint32_t tile,
+                                                 bool doCur, bool doPrev)
+{
+    uint32_t const lane = threadIdx.x & 31u;
+    size_t const seg = (size_t)tile * kBcTileSpan;
+    uint32_t const* const lc = S.mlist + (size_t)p * S.listStride + seg;
+    uint32_t const* const wc = S.mword + (size_t)p * S.listStride + seg;
+    uint32_t const* const wp = S.mword + (size_t)(p ^ 1u) * S.listStride + seg;
+    unsigned long long const* const tcur = S.tmp + (size_t)p * S.nwords;
+    unsigned long long* const tprev = S.tmp + (size_t)(p ^ 1u) * S.nwords;
+    uint32_t const cnt = doCur ? ldm<kNc>(S.mcount + (size_t)p * S.countStride + tile) : 0u;
+    uint32_t const pcnt = doPrev ? ldm<kNc>(S.mcount + (size_t)(p ^ 1u) * S.countStride + tile) : 0u;
+    uint32_t ent[kPerfQ], to[kPerfQ], pw[kPerfQ];
+    bool live[kPerfQ];
+#pragma unroll
+    for (int q = 0; q < kPerfQ; ++q) {
+        uint32_t const e = lane + 32u * (uint32_t)q;
+        ent[q] = doCur ? ldm<kNc>(lc + e) : 0u;
+        to[q] = doCur ? ldm<kNc>(wc + e) : 0u;
+        pw[q] = doPrev ? ldm<kNc>(wp + e) : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < kPerfQ; ++q) live[q] = lane + 32u * (uint32_t)q < cnt;
+    uint32_t nAcc = perform_movers<W, kPerfQ, kNc>(S, dtab, tcur, ent, to, live);
+#pragma unroll
+    for (int q = 0; q < kPerfQ; ++q)
+        if (lane + 32u * (uint32_t)q < pcnt) tprev[pw[q] >> 6] = 0ull;
+    constexpr uint32_t kPass = 32u * kPerfQ;
+    for (uint32_t b = kPass; b < cnt; b += kPass) {
+#pragma unroll
+        for (int q = 0; q < kPerfQ; ++q) {
+            uint32_t const e = b + lane + 32u * (uint32_t)q;
+            live[q] = e < cnt;
+            ent[q] = live[q] ? ldm<kNc>(lc + e) : 0u;
+            to[q] = live[q] ? ldm<kNc>(wc + e) : 0u;
+        }
+        nAcc += perform_movers<W, kPerfQ, kNc>(S, dtab, tcur, ent, to, live);
+    }
+    for (uint32_t b = kPass; b < pcnt; b += kPass) {
+#pragma unroll
+        for (int q = 0; q < kPerfQ; ++q) {
+            uint32_t const e = b + lane + 32u * (uint32_t)q;
+            if (e < pcnt) tprev[ldm<kNc>(wp + e) >> 6] = 0ull;
+        }
+    }
+    return nAcc;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------------- kernels
@@ -324,7 +393,13 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_check_bc(const __gri
         start = tr.start;
     }
     StepEntry const st = steps[sys];
-    if (st.color == kNoColor || start >= st.cnt) return;
+    if (st.color == kNoColor) return;
+    if (start >= st.cnt) {
+        // one system: the tile lies beyond this colour group; its list length becomes 0, so every
+        // length the perform reads is this sub-step's (it does not read the step entry)
+        if (!kMulti && threadIdx.x == 0) S1.mcount[(size_t)st.parity * S1.countStride + start / kBcTileSpan] = 0u;
+        return;
+    }
     if (kMulti) {
         copy_desc(Sm, sysv + sys);
         __syncthreads();
@@ -344,45 +419,54 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_check_bc(const __gri
     }
 }
 
-template <typename W, int MPT, bool kMulti, int kMinBlocks = 1>
-__global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_perform_bc(const __grid_constant__ SysDev S1,
-                                                           SysDev const* __restrict__ sysv,
-                                                           TileRef const* __restrict__ tiles,
-                                                           StepEntry const* __restrict__ steps,
-                                                           uint32_t tilesPerCta)
+// Grid-phase perform, one warp (CTA) per tile of kBcTileSpan in-colour indices (perform_tile).
+// One system: `parity` and `scope` (kPerfCur: walk this sub-step's movers, kPerfPrev: scrub the
+// previous sub-step's marks) come with the launch, so no load precedes the lists'; with parity ==
+// kParityFromEntry they come from the step entry (a launch captured once and replayed on other
+// entries). `next` != nullptr: CTA 0 also writes the following sub-step's entry there
+// (write_next_step). A tile list (kMulti): warp b takes tile tiles[b] of system tiles[b].sys, whose
+// step entry says what to do.
+template <typename W, bool kMulti>
+__global__ void __launch_bounds__(32) k_perform_bc(const __grid_constant__ SysDev S1, SysDev const* __restrict__ sysv,
+                                                   TileRef const* __restrict__ tiles,
+                                                   StepEntry const* __restrict__ steps, uint32_t parity,
+                                                   uint32_t scope, StepEntry* next)
 {
     __shared__ SysDev Sm;
     __shared__ __align__(16) uint32_t dtab[kDirTab];
-    __shared__ uint32_t pre[2 * (kPerformTiles + 1)];
-    // one system: tilesPerCta (<= kPerformTiles) consecutive tiles per CTA; a tile list: the
-    // entry's count (<= kPerformTiles) of one system's consecutive tiles
-    uint32_t sys = 0, tile0 = blockIdx.x * tilesPerCta, nT = tilesPerCta;
-    // one system: the direction table's load goes out with the step entry's
-    uint32_t dv = (!kMulti && threadIdx.x < kDirTab) ? S1.dirTab[threadIdx.x] : 0u;
-    if (kMulti) {
+    uint32_t const lane = threadIdx.x;
+    uint32_t p = parity, tile = blockIdx.x;
+    bool cur = (scope & kPerfCur) != 0u, prev = (scope & kPerfPrev) != 0u;
+    if (!kMulti) {
+        if (next != nullptr && blockIdx.x == 0 && lane == 0) write_next_step(S1.gen, S1.grp, next);
+        uint32_t const d0 = S1.dirTab[lane];
+        uint32_t const d1 = lane + 32u < kDirTab ? S1.dirTab[lane + 32u] : 0u;
+        if (parity == kParityFromEntry) {
+            StepEntry const st = steps[0];
+            uint32_t const start = tile * kBcTileSpan;
+            p = st.parity;
+            cur = st.color != kNoColor && start < st.cnt;
+            prev = st.prevColor != kNoColor && start < st.pcnt;
+        }
+        dtab[lane] = d0;
+        if (lane + 32u < kDirTab) dtab[lane + 32u] = d1;
+    } else {
         TileRef const tr = tiles[blockIdx.x];
-        sys = tr.sys;
-        tile0 = tr.start / kBcTileSpan;
-        nT = min(tr.count, kPerformTiles);
+        copy_desc(Sm, sysv + tr.sys);
+        StepEntry const st = steps[tr.sys];
+        p = st.parity;
+        tile = tr.start / kBcTileSpan;
+        cur = st.color != kNoColor && tr.start < st.cnt;
+        prev = st.prevColor != kNoColor && tr.start < st.pcnt;
+        __syncwarp();
+        dtab[lane] = Sm.dirTab[lane];
+        if (lane + 32u < kDirTab) dtab[lane + 32u] = Sm.dirTab[lane + 32u];
     }
-    StepEntry const st = steps[sys];
-    // tiles holding this sub-step's movers or the previous sub-step's marks
-    uint32_t const reach = max(st.color != kNoColor ? st.cnt : 0u, st.pcnt);
-    uint32_t const activeTiles = (reach + kBcTileSpan - 1) / kBcTileSpan;
-    if (tile0 >= activeTiles) return;
-    nT = min(nT, activeTiles - tile0);
-    if (kMulti) {
-        copy_desc(Sm, sysv + sys);
-        __syncthreads();
-        if (threadIdx.x < kDirTab) dv = Sm.dirTab[threadIdx.x];
-    }
+    __syncwarp();
+    if (!cur && !prev) return;
     SysDev const& S = kMulti ? Sm : S1;
-    __shared__ uint32_t tally;
-    if (threadIdx.x < kDirTab) dtab[threadIdx.x] = dv;
-    if (threadIdx.x == 0) tally = 0;
-    perform_body<W, MPT>(S, dtab, st, tile0, nT, &tally, pre);   // publishes both with its first barrier
-    __syncthreads();
-    if (threadIdx.x == 0) tally_flush(tally, S.stats, 2);
+    uint32_t const nAcc = __reduce_add_sync(0xffffffffu, perform_tile<W, true>(S, dtab, p, tile, cur, prev));
+    if (lane == 0) tally_flush(nAcc, S.stats, 2);
 }
 
 // ---------------------------------------------------------------------------------- persistent
@@ -909,40 +993,38 @@ int sm_count()
     return c;
 }
 
-template <typename W, bool kMulti, int kMinCheck, int kMinPerform>
+template <typename W, bool kMulti, int kMinCheck>
 void launch_grid_bc_k(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
-                      uint32_t nTiles, StepEntry const* dSteps, cudaStream_t s)
+                      uint32_t nTiles, StepEntry const* dSteps, PerformArgs const& pa, cudaStream_t s)
 {
     if (check) {
         k_check_bc<W, kCheckMpt, kMulti, kMinCheck><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
         return;
     }
-    // one system: several tiles per perform CTA only while that still leaves every SM a CTA, since
-    // a small system's perform is bound by the length of its dependency chain, not by its warps
-    uint32_t const g = (!kMulti && nTiles >= kPerformTiles * (uint32_t)sm_count()) ? kPerformTiles : 1u;
-    k_perform_bc<W, kCheckMpt, kMulti, kMinPerform>
-        <<<kMulti ? nTiles : (nTiles + g - 1) / g, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps, g);
+    k_perform_bc<W, kMulti><<<nTiles, 32, 0, s>>>(hostDesc, dSys, dTiles, dSteps, pa.parity, pa.scope, pa.next);
 }
 
+// shape: the check's register budget, 0: the compiler's choice, 1: 6 CTAs per SM, 2: 5, 3: 7 (the
+// default; BFM_GRID_SHAPE overrides it); the perform (one warp per tile) has a single form
 template <typename W, bool kMulti>
 void launch_grid_bc_m(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
-                      uint32_t nTiles, StepEntry const* dSteps, int shape, cudaStream_t s)
+                      uint32_t nTiles, StepEntry const* dSteps, PerformArgs const& pa, int shape, cudaStream_t s)
 {
     switch (shape < 0 ? default_grid_shape() : shape) {
-    case 1: launch_grid_bc_k<W, kMulti, 6, 5>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
-    case 2: launch_grid_bc_k<W, kMulti, 6, 6>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
-    case 3: launch_grid_bc_k<W, kMulti, 7, 5>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
-    default: launch_grid_bc_k<W, kMulti, 1, 1>(check, hostDesc, dSys, dTiles, nTiles, dSteps, s); break;
+    case 1: launch_grid_bc_k<W, kMulti, 6>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
+    case 2: launch_grid_bc_k<W, kMulti, 5>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
+    case 3: launch_grid_bc_k<W, kMulti, 7>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
+    default: launch_grid_bc_k<W, kMulti, 1>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
     }
 }
 
 template <typename W>
 cudaError_t launch_grid_bc(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
-                           uint32_t nTiles, StepEntry const* dSteps, int shape, cudaStream_t s)
+                           uint32_t nTiles, StepEntry const* dSteps, PerformArgs const& pa, int shape, cudaStream_t s)
 {
     if (shape >= kGridShapes) return cudaErrorInvalidValue;
-    if (dTiles) launch_grid_bc_m<W, true>(check, hostDesc, dSys, dTiles, nTiles, dSteps, shape, s);
-    else launch_grid_bc_m<W, false>(check, hostDesc, dSys, dTiles, nTiles, dSteps, shape, s);
+    if (dTiles) launch_grid_bc_m<W, true>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, s);
+    else launch_grid_bc_m<W, false>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, s);
     return cudaGetLastError();
 }
 
@@ -950,22 +1032,9 @@ cudaError_t launch_grid_bc(bool check, SysDev const& hostDesc, SysDev const* dSy
 
 std::vector<TileRef> perform_tile_list(std::vector<TileRef> const& tiles)
 {
-    // the same rule as one system's launch: four consecutive tiles of a system per CTA when the
-    // launch has at least four tiles per SM
-    uint32_t const g = tiles.size() >= (size_t)kPerformTiles * (uint32_t)sm_count() ? kPerformTiles : 1u;
-    std::vector<TileRef> out;
-    for (size_t i = 0; i < tiles.size();) {
-        TileRef t = tiles[i];
-        t.count = 1;
-        size_t k = i + 1;
-        while (k < tiles.size() && t.count < g && tiles[k].sys == t.sys &&
-               tiles[k].start == t.start + t.count * kBcTileSpan) {
-            ++t.count;
-            ++k;
-        }
-        out.push_back(t);
-        i = k;
-    }
+    // the perform takes one tile per warp, like the check's list
+    std::vector<TileRef> out(tiles);
+    for (auto& t : out) t.count = 1;
     return out;
 }
 
@@ -973,19 +1042,23 @@ cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef 
                             StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape)
 {
     if (nTiles == 0) return cudaSuccess;
-    if (codeMode == kCode32) return launch_grid_bc<uint32_t>(true, hostDesc, dSys, dTiles, nTiles, dSteps, shape, s);
+    PerformArgs const none{};
+    if (codeMode == kCode32)
+        return launch_grid_bc<uint32_t>(true, hostDesc, dSys, dTiles, nTiles, dSteps, none, shape, s);
     if (codeMode == kCode64)
-        return launch_grid_bc<unsigned long long>(true, hostDesc, dSys, dTiles, nTiles, dSteps, shape, s);
+        return launch_grid_bc<unsigned long long>(true, hostDesc, dSys, dTiles, nTiles, dSteps, none, shape, s);
     return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
-                              StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape)
+                              StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape,
+                              PerformArgs const& pa)
 {
     if (nTiles == 0) return cudaSuccess;
-    if (codeMode == kCode32) return launch_grid_bc<uint32_t>(false, hostDesc, dSys, dTiles, nTiles, dSteps, shape, s);
+    if (codeMode == kCode32)
+        return launch_grid_bc<uint32_t>(false, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, s);
     if (codeMode == kCode64)
-        return launch_grid_bc<unsigned long long>(false, hostDesc, dSys, dTiles, nTiles, dSteps, shape, s);
+        return launch_grid_bc<unsigned long long>(false, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, s);
     return cudaErrorInvalidValue;
 }
 

@@ -126,7 +126,7 @@ extern "C" int bfm_sweep_noalloc(const bfm_noalloc_system* s, int32_t n_mcs, uin
     char* const B = static_cast<char*>(base);
     cudaStream_t const st = static_cast<cudaStream_t>(stream_ptr);
 
-    // descriptor (host stack copy), group table, brick tables
+    // descriptor (host stack copy), group table, brick tables; every axis is periodic (walls = 0)
     SysDev d;
     std::memset(&d, 0, sizeof(d));
     d.x = s->x;
@@ -189,11 +189,10 @@ extern "C" int bfm_sweep_noalloc(const bfm_noalloc_system* s, int32_t n_mcs, uin
     uint32_t ring = 0;
     for (uint64_t t = 0; t < total;) {
         uint32_t const m = (uint32_t)((total - t) < kHostChunk ? (total - t) : kHostChunk);
-        if (ring + m > kStepRing) {
-            // the ring is reused only after the kernels that read it have finished
-            NOALLOC_CHECK(cudaStreamSynchronize(st), "ring wrap");
-            ring = 0;
-        }
+        // Reusing the ring from its start needs no wait: the copy below is queued on the same
+        // stream as the kernels that read the old entries, so it runs after them, and the host
+        // chunk is staged before cudaMemcpyAsync returns.
+        if (ring + m > kStepRing) ring = 0;
         for (uint32_t i = 0; i < m; ++i) {
             uint64_t const sub = substep0 + t + i;
             StepEntry& q = chunk[i];

@@ -62,13 +62,18 @@ def batch_runner(gpu: int):
     ``gpu`` (each its own MCS count); returns per system its positions and move counters."""
     def run(systems, mcs):
         from .updater import Batch, UpdaterGPUScBFM_AB_Type
-        members = [UpdaterGPUScBFM_AB_Type(gpu).load_system(s) for s in systems]
-        b = Batch(members, gpu=gpu)
+        members, b = [], None
         try:
+            for s in systems:
+                u = UpdaterGPUScBFM_AB_Type(gpu)
+                members.append(u)           # closed below even if load_system raises
+                u.load_system(s)
+            b = Batch(members, gpu=gpu)
             b.run_each(list(mcs))
             return [(m.get_coords(), m.stats()) for m in members]
         finally:
-            b.close()
+            if b is not None:
+                b.close()
             for m in members:
                 m.close()
     return run

@@ -31,6 +31,17 @@ def color_graph(system) -> np.ndarray:
     return out
 
 
+def probe_device(gpu: int = 0) -> dict:
+    """bfm_probe_device: L2 hit latency, L2 read bandwidth and the period of back-to-back kernels of
+    the grid-phase shape in a captured graph, measured on the GPU."""
+    out = np.zeros(4, dtype=np.float64)
+    st = _lib.load().bfm_probe_device(gpu, out)
+    if st != _lib.BFM_OK:
+        _lib.raise_for(st, "bfm_probe_device failed")
+    return {"l2_latency_ns": float(out[0]), "l2_read_gbs": float(out[1]), "kernel_period_us": float(out[2]),
+            "sms": int(out[3])}
+
+
 def counter_draw(seed: int, k: int) -> int:
     return int(_lib.load().bfm_counter_draw(seed, k))
 
@@ -300,6 +311,12 @@ class UpdaterGPUScBFM_AB_Type:
         self._call("bfm_time_kernels", n_mcs, out)
         return {"check_ms": out[0], "perform_ms": out[1], "check_launches": int(out[2]),
                 "perform_launches": int(out[3])}
+
+    def transfer_bytes(self) -> tuple:
+        """(host -> device, device -> host) bytes of the run and read-back calls so far."""
+        v = (C.c_uint64 * 2)()
+        self._call("bfm_transfer_bytes", v)
+        return int(v[0]), int(v[1])
 
     def launch_count(self) -> int:
         v = C.c_uint64()

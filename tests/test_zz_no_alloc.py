@@ -48,40 +48,52 @@ def sorted_layout(s):
     return nC, sizes, offs, npad, slot, xyz, nbr, nnb
 
 
-def test_noalloc_matches_bfm_run_on_two_calls():
+def _two_calls_match_bfm_run(s, mcs):
+    """Two bfm_sweep_noalloc calls of `mcs` MCS each on caller-owned buffers, each compared with
+    bfm_run after the same number of MCS."""
     torch = pytest.importorskip("torch")
     L = _lib.load()
+    nC, sizes, offs, npad, slot, xyz, nbr, nnb = sorted_layout(s)
+    # existing entry point
+    u = P.UpdaterGPUScBFM_AB_Type(0)
+    u.load_system(s, mode=P.MODE_LAUNCH)
+    u.runSimulationOnGPU(mcs)
+    want1 = u.get_coords().copy()
+    u.runSimulationOnGPU(mcs)
+    want2 = u.get_coords().copy()
+    u.close()
+    # caller-owned device buffers
+    dx, dy, dz = (torch.from_numpy(xyz[a].copy()).cuda() for a in range(3))
+    dnbr = torch.from_numpy(nbr.reshape(-1).view(np.int32).copy()).cuda()
+    dnnb = torch.from_numpy(nnb.copy()).cuda()
+    forb = np.ascontiguousarray(s.forbidden, dtype=np.uint8)
+    sysd = _lib.NoallocSystem()
+    sysd.x, sysd.y, sysd.z = dx.data_ptr(), dy.data_ptr(), dz.data_ptr()
+    sysd.nbr, sysd.nnb = dnbr.data_ptr(), dnnb.data_ptr()
+    sysd.npad, sysd.maxc, sysd.n_colors = npad, s.maxc, nC
+    sysd.box = (C.c_uint32 * 3)(*s.box)
+    sysd.group_offset = offs.ctypes.data
+    sysd.group_size = sizes.ctypes.data
+    sysd.forbidden = forb.ctypes.data
+    err = C.create_string_buffer(256)
+    stream = torch.cuda.current_stream().cuda_stream
+    for call, want in enumerate((want1, want2)):
+        st = L.bfm_sweep_noalloc(C.byref(sysd), mcs, s.seed, call * mcs * nC, stream, err, 256)
+        assert st == _lib.BFM_OK, err.value.decode()
+        torch.cuda.synchronize()
+        got = np.stack([dx.cpu().numpy(), dy.cpu().numpy(), dz.cpu().numpy()], axis=1)[slot]
+        assert np.array_equal(got, want), (s.name, call)
+
+
+def test_noalloc_matches_bfm_run_on_two_calls():
     for s in (S.small_chains(), S.rings_and_free()):
-        nC, sizes, offs, npad, slot, xyz, nbr, nnb = sorted_layout(s)
-        # existing entry point
-        u = P.UpdaterGPUScBFM_AB_Type(0)
-        u.load_system(s, mode=P.MODE_LAUNCH)
-        u.runSimulationOnGPU(40)
-        want1 = u.get_coords().copy()
-        u.runSimulationOnGPU(40)
-        want2 = u.get_coords().copy()
-        u.close()
-        # caller-owned device buffers
-        dx, dy, dz = (torch.from_numpy(xyz[a].copy()).cuda() for a in range(3))
-        dnbr = torch.from_numpy(nbr.reshape(-1).view(np.int32).copy()).cuda()
-        dnnb = torch.from_numpy(nnb.copy()).cuda()
-        forb = np.ascontiguousarray(s.forbidden, dtype=np.uint8)
-        sysd = _lib.NoallocSystem()
-        sysd.x, sysd.y, sysd.z = dx.data_ptr(), dy.data_ptr(), dz.data_ptr()
-        sysd.nbr, sysd.nnb = dnbr.data_ptr(), dnnb.data_ptr()
-        sysd.npad, sysd.maxc, sysd.n_colors = npad, s.maxc, nC
-        sysd.box = (C.c_uint32 * 3)(*s.box)
-        sysd.group_offset = offs.ctypes.data
-        sysd.group_size = sizes.ctypes.data
-        sysd.forbidden = forb.ctypes.data
-        err = C.create_string_buffer(256)
-        stream = torch.cuda.current_stream().cuda_stream
-        for call, want in enumerate((want1, want2)):
-            st = L.bfm_sweep_noalloc(C.byref(sysd), 40, s.seed, call * 40 * nC, stream, err, 256)
-            assert st == _lib.BFM_OK, err.value.decode()
-            torch.cuda.synchronize()
-            got = np.stack([dx.cpu().numpy(), dy.cpu().numpy(), dz.cpu().numpy()], axis=1)[slot]
-            assert np.array_equal(got, want), (s.name, call)
+        _two_calls_match_bfm_run(s, 40)
+
+
+def test_noalloc_long_calls_reuse_the_step_ring():
+    """3 colours x 2000 MCS = 6000 sub-steps per call, more than the 4096 entries of the staged
+    sub-step ring, which is then reused from its start in stream order (no host wait)."""
+    _two_calls_match_bfm_run(S.rings_and_free(), 2000)
 
 
 def test_noalloc_rejects_oversized_system():
