@@ -14,7 +14,10 @@ stream, with the L2 flushed (a 256 MiB write) before every step; max over ranks.
 GPU under torchrun; a single system does not shard, so N GPUs run N replicas (weak scaling).
 
 --impl reference times the reference's algorithm on the host cores: the CPU restatement of the
-reference sweep (oracle/), one replica per core, same metric and workload.
+reference sweep (oracle/), one replica per core, same metric and workload; beside it
+(`reference_gpu`) the reference's own GPU updater, compiled from its sources into oracle/_ref, on
+the same workload and GPU. The main arm carries the same reference-updater leg for the three
+single-system workloads as a baseline beside its own numbers (never as the measured path).
 """
 from __future__ import annotations
 
@@ -76,8 +79,9 @@ def workload_config(name, systems):
 
 # ------------------------------------------------------------------ algorithmic bytes (roofline)
 
-STEP_ENTRY_BYTES = 32          # one sub-step's draw entry (colour, seed, group), bfm_device.cuh StepEntry
-STATS_BYTES = 3 * 64 * 8       # the move counters: attempted / tentative / accepted in 64 slots each
+# dependent L2 round trips of one sub-step on the grid path (the latency model of the roofline)
+CHECK_ROUND_TRIPS = 3          # step entry -> lattice address and bond code -> occupancy words
+PERFORM_ROUND_TRIPS = 2        # list lengths, entries and targets -> code, neighbour refs, temporary words
 
 
 def check_bytes_per_move(systems, p_chk, code_mode):
@@ -411,9 +415,25 @@ def run_ours(args):
                     "note": ("the state (about 40 B per monomer) stays in the 126 MB L2 between launches, so "
                              "the HBM fraction is low by construction; the kernels are bound by instruction "
                              "issue and dependent-load latency")}
-        l2pct = profiled_traffic(key, "lts_throughput_pct:")
-        roofline["l2"] = {"frac": None if l2pct is None else round(l2pct / 100, 4),
-                          "source": f"ncu lts__throughput.avg.pct_of_peak_sustained_elapsed, profiles/{key}.md"}
+        # measured in this run on this GPU: the L2's read bandwidth, its hit latency and the period of
+        # back-to-back kernels of the grid-phase shape in a graph (bfm_probe_device)
+        probe = P.probe_device(local)
+        roofline["l2"] = {"achieved": round(achieved, 1), "peak": round(probe["l2_read_gbs"], 1), "unit": "GB/s",
+                          "frac": round(achieved / probe["l2_read_gbs"], 4),
+                          "peak_source": "bfm_probe_device: 32 MB read 20 times by every SM, this run"}
+        # latency bound of one MCS: per sub-step the check's dependent L2 round trips (step entry ->
+        # lattice address and code -> occupancy words) and the perform's (list lengths, entries and
+        # targets -> code words, neighbour references and temporary-lattice words), each one L2 hit
+        # latency, plus two kernel periods
+        rt = CHECK_ROUND_TRIPS + PERFORM_ROUND_TRIPS
+        bound_us = nC * (rt * probe["l2_latency_ns"] / 1e3 + 2 * probe["kernel_period_us"])
+        warm_us = warm_ms * 1e3 / args.steps
+        roofline["latency"] = {"bound_us_per_mcs": round(bound_us, 2), "measured_us_per_mcs": round(warm_us, 2),
+                               "frac": round(bound_us / warm_us, 4), "l2_latency_ns": round(probe["l2_latency_ns"], 1),
+                               "kernel_period_us": round(probe["kernel_period_us"], 3),
+                               "round_trips_per_sub_step": rt, "sub_steps_per_mcs": nC,
+                               "model": "sub-steps x (dependent L2 round trips x L2 hit latency + 2 kernel periods), "
+                                        "against the warm-L2 device time per MCS"}
 
     # e2e through the C-ABI with host buffers: per step one run of 1 MCS (its sub-steps' draw
     # entries uploaded from pinned memory) and a read of that step's move counters, which waits
@@ -421,6 +441,7 @@ def run_ours(args):
     # is in flight while it reads; the positions, in the caller's order, copied back into a pinned
     # host array at the end
     host_xyz = torch.empty((systems[0].n, 3), dtype=torch.int32, pin_memory=True).numpy()
+    xfer0 = [m.transfer_bytes() for m in members]
     torch.cuda.synchronize()
     t = time.perf_counter()
     prev = None
@@ -436,12 +457,18 @@ def run_ours(args):
     u0.stats_wait(prev)
     u0.get_coords(host_xyz)
     e2e_s = time.perf_counter() - t
+    xfer1 = [m.transfer_bytes() for m in members]
+    h2d = sum(b[0] - a[0] for a, b in zip(xfer0, xfer1))
+    d2h = sum(b[1] - a[1] for a, b in zip(xfer0, xfer1))
     e2e_value = world * moves / reduce_max(e2e_s, world)
     e2e = {"value": e2e_value, "unit": "attempted moves/s",
-           "h2d_bytes_per_step": STEP_ENTRY_BYTES * sum(colours),
-           "d2h_bytes_per_step": STATS_BYTES + round(12 * systems[0].n / args.steps),
-           "calls": "bfm_run_async(1) + bfm_stats_enqueue per step, bfm_stats_wait on the previous step's "
-                    "ticket (one step in flight), bfm_get_coords_bulk once into pinned memory"}
+           "h2d_bytes_per_step": round(h2d / args.steps, 1), "d2h_bytes_per_step": round(d2h / args.steps, 1),
+           "h2d_bytes": h2d, "d2h_bytes": d2h,
+           "calls": "bfm_run_async(1) + bfm_stats_enqueue per step (the three move counters written into "
+                    "mapped host memory), bfm_stats_wait on the previous step's ticket (one step in flight), "
+                    "bfm_get_coords_bulk once into pinned memory; byte counts from bfm_transfer_bytes (the "
+                    "step entries of the counter stream are made on the device, so after a chain's first "
+                    "entry no host-to-device copy is needed)"}
 
     for m in members:
         m.validate()   # excluded volume, bonds and the device lattice after the timed run
@@ -452,6 +479,15 @@ def run_ours(args):
         for m in members:
             m.close()
         members, batch = [], None
+        extras["reference_gpu"] = reference_gpu(gpu=local)
+        r = extras["reference_gpu"]["workloads"].get(args.workload, {})
+        if "reference_device" in r:
+            # the engine's numbers of this line against the reference updater's on this GPU
+            extras["vs_reference_gpu"] = {"value": value / r["reference_device"],
+                                          "value_warm_l2": value_warm / r["reference_device"],
+                                          "e2e": e2e_value / r["reference_host_clock"],
+                                          "note": "value and value_warm_l2 over the reference's device time (warm "
+                                                  "L2, its own call shape); e2e over its host-clock rate"}
         extras["batched"] = batched_vs_plain()
         extras["served"] = served(local)
 
@@ -484,38 +520,100 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def batched_vs_plain(n_systems=256, mcs=100, plain_mcs=20):
-    """The batched ensemble (256 systems, own seeds): the batch (one launch sequence per chunk for
-    all systems) against the plain path (each system alone through the per-sub-step launch path).
-    Both timed with CUDA events; the plain time is per system over plain_mcs MCS, scaled to mcs."""
+ENSEMBLE_MCS = 10000
+REFERENCE_LONG = os.path.join(ROOT, "tests", "golden", "reference_long.json")
+
+
+def positions_sha256(xyz):
+    import hashlib
+    import numpy as np
+    return hashlib.sha256(np.ascontiguousarray(np.asarray(xyz, dtype="<i4").reshape(-1, 3)).tobytes()).hexdigest()
+
+
+def plain_rates(systems, sample_mcs, gpu=0, every=None, mcs_cap=None):
+    """Each system alone, one after another, on the plain paths: BFM_MODE_LAUNCH (two launches per
+    sub-step, the reference's structure) and BFM_MODE_AUTO (the engine's own choice for one system:
+    resident, cluster, persistent or graph). Per system 3 untimed MCS, then min(sample_mcs, its MCS)
+    timed (CUDA events; with `every`, observables read back every `every` MCS as the server does, on
+    the host clock). Returns per mode the attempted moves and seconds of the timed samples."""
+    import pscbfm_b200 as P
+    out = {}
+    for name, mode in (("launch", P.MODE_LAUNCH), ("auto", P.MODE_AUTO)):
+        moves, secs = 0, 0.0
+        for i, sy in enumerate(systems):
+            k = sample_mcs if mcs_cap is None else min(sample_mcs, mcs_cap[i])
+            u = P.UpdaterGPUScBFM_AB_Type(gpu).load_system(sy, mode=mode)
+            u.runSimulationOnGPU(3)
+            if every is None:
+                secs += u.run_timed(k) / 1e3
+            else:
+                u.synchronize()
+                t = time.perf_counter()
+                done = 0
+                while done < k:
+                    step = min(every - done % every, k - done)
+                    u.runSimulationOnGPU(step)
+                    done += step
+                    if done % every == 0:
+                        u.observables_raw()
+                secs += time.perf_counter() - t
+            moves += sy.n * k
+            u.close()
+        out[name] = (moves, secs)
+    return out
+
+
+def batched_vs_plain(mcs=ENSEMBLE_MCS, sample_mcs=200):
+    """The 256-system ensemble (own seeds 1000 + i) in one Batch for its full 10^4 MCS: the run's first
+    MCS are the autotuner's trials, then a timed sample of sample_mcs MCS, then the rest of the run
+    timed; every member's final positions are compared with the reference updater's run of that
+    system alone (tests/golden/reference_long.json). Beside it the same systems one at a time on the
+    two plain paths over a timed sample of sample_mcs MCS each (plain_rates). Rates are measured, not
+    extrapolated: attempted moves / device seconds of each timed region."""
+    import json
     import pscbfm_b200 as P
     from pscbfm_b200 import systems as S
-    systems = S.ensemble(n_systems=n_systems)
+    systems = S.ensemble(n_systems=256)
     n = sum(s.n for s in systems)
     members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
     b = P.Batch(members)
     b.run(3)
-    tuned = b.autotune(5)          # the trials are warm-up MCS of the run
-    batched_ms = b.run_timed(mcs)
+    tuned = b.autotune(2)          # the trials are MCS of the run
+    done = 3 + tuned["mcs_spent"]
+    sample_ms = b.run_timed(sample_mcs)
     launches0 = b.launch_count()
-    b.run_timed(1)
-    launches_per_mcs = b.launch_count() - launches0
-    b.close()
-    plain_ms = 0.0
-    for m in members:
-        m.set_mode(P.MODE_LAUNCH)
-        m.run_timed(1)
-        plain_ms += m.run_timed(plain_mcs) * (mcs / plain_mcs)
+    rest = mcs - done - sample_mcs
+    rest_ms = b.run_timed(rest)
+    launches_per_mcs = (b.launch_count() - launches0) / rest
+    b.synchronize()
+    parity = {"checked": False}
+    if os.path.exists(REFERENCE_LONG):
+        gold = json.load(open(REFERENCE_LONG))["cases"]
+        same = sum(positions_sha256(m.get_coords()) == gold[f"ensemble256_{i:03d}_{mcs}mcs"]["sha256"]
+                   for i, m in enumerate(members))
+        parity = {"checked": True, "members_equal_reference": int(same), "members": len(members),
+                  "mcs": mcs, "against": "reference updater run on each system alone (reference_long.json)"}
     for m in members:
         m.validate()
+    b.close()
+    for m in members:
         m.close()
-    return {"workload": "ensemble_256_systems", "systems": n_systems, "monomers": n, "mcs": mcs,
-            "batched": n * mcs / (batched_ms / 1e3), "plain": n * mcs / (plain_ms / 1e3),
-            "ratio": plain_ms / batched_ms, "batched_launches_per_mcs": launches_per_mcs,
+    plain = plain_rates(systems, sample_mcs)
+    batched_sample = n * sample_mcs / (sample_ms / 1e3)
+    batched_long = n * rest / (rest_ms / 1e3)
+    rate = {k: v[0] / v[1] for k, v in plain.items()}
+    return {"workload": "ensemble_256_systems", "systems": len(systems), "monomers": n, "mcs": mcs,
+            "batched": batched_long, "batched_sample": batched_sample,
+            "plain_launch": rate["launch"], "plain_auto": rate["auto"],
+            "ratio_vs_plain_launch": batched_sample / rate["launch"],
+            "ratio_vs_plain_auto": batched_sample / rate["auto"],
+            "batched_launches_per_mcs": launches_per_mcs, "parity": parity,
             "autotuned": {"shape": tuned["shape"], "resident": tuned["resident"], "cluster": tuned["cluster"],
                           "trials": [[t["shape"], t["resident"], t["cluster"], round(t["ms_per_mcs"], 4)]
                                      for t in tuned["trials"]]},
-            "plain_path": f"BFM_MODE_LAUNCH, one system at a time, {plain_mcs} MCS each scaled to {mcs}",
+            "timing": (f"batched: CUDA events over MCS {done}-{done + sample_mcs} (batched_sample, compared with "
+                       f"the plain samples) and {done + sample_mcs}-{mcs} (batched); plain: each system alone, "
+                       f"CUDA events over its MCS 3-{3 + sample_mcs}"),
             "unit": "attempted moves/s"}
 
 
@@ -533,32 +631,19 @@ def served_jobs(n_jobs, seed=777):
     return systems, [int(m) for m in mcs]
 
 
-def served(gpu=0, n_jobs=32, rates=SERVED_RATES, budget=150 << 30, every=100, plain_mcs=300):
-    """Poisson arrivals at each rate lambda into the job server (HBM budget 150 GB, observables every
-    100 MCS); latency = submit to completion on the host clock. The plain reference point runs the
-    same jobs one at a time through the per-sub-step launch path with the same observable sampling
-    (each job timed over min(MCS, plain_mcs) MCS and scaled to its MCS)."""
+def served(gpu=0, n_jobs=200, rates=SERVED_RATES, budget=150 << 30, every=100, sample_mcs=300):
+    """Poisson arrivals at each rate lambda of n_jobs jobs into the job server (HBM budget 150 GB,
+    observables every 100 MCS); latency = submit to completion on the host clock. Beside it the
+    same jobs one at a time on the two plain paths (plain_rates: min(MCS, sample_mcs) MCS of each
+    job timed with the same observable sampling); the ratios compare measured rates."""
     import numpy as np
     import pscbfm_b200 as P
     systems, mcs = served_jobs(n_jobs)
     work = sum(s.n * m for s, m in zip(systems, mcs))
+    longest = int(np.argmax([s.n * m for s, m in zip(systems, mcs)]))
     setups = [P.UpdaterGPUScBFM_AB_Type(gpu).load_system(s, initialize=False) for s in systems]
-    # plain: one job at a time
-    plain_s = 0.0
-    for s, m in zip(systems, mcs):
-        u = P.UpdaterGPUScBFM_AB_Type(gpu).load_system(s, mode=P.MODE_LAUNCH)
-        u.runSimulationOnGPU(1)
-        k = min(m, plain_mcs)
-        t = time.perf_counter()
-        done = 0
-        while done < k:
-            step = min(every - done % every, k - done)
-            u.runSimulationOnGPU(step)
-            done += step
-            if done % every == 0:
-                u.observables_raw()
-        plain_s += (time.perf_counter() - t) * m / k
-        u.close()
+    plain = plain_rates(systems, sample_mcs, gpu=gpu, every=every, mcs_cap=mcs)
+    rate = {k: v[0] / v[1] for k, v in plain.items()}
     rows = []
     for lam in rates:
         rng = np.random.Generator(np.random.PCG64(int(lam)))
@@ -575,19 +660,75 @@ def served(gpu=0, n_jobs=32, rates=SERVED_RATES, budget=150 << 30, every=100, pl
             srv.wait(j, 900)
         makespan = time.perf_counter() - t0
         st = srv.stats()
+        lat_longest = srv.job_times(jobs[longest])
         srv.close()
         if st["completed"] != n_jobs:
             raise RuntimeError(f"served: {st['completed']} of {n_jobs} jobs completed")
+        moves_per_s = work / makespan
         rows.append({"lambda_jobs_per_s": lam, "p50_s": round(st["p50_s"], 4), "p99_s": round(st["p99_s"], 4),
-                     "mean_s": round(st["mean_s"], 4), "makespan_s": round(makespan, 3),
-                     "moves_per_s": work / makespan, "ratio_vs_plain": plain_s / makespan})
+                     "mean_s": round(st["mean_s"], 4), "makespan_s": round(makespan, 3), "moves_per_s": moves_per_s,
+                     "ratio_vs_plain_launch": moves_per_s / rate["launch"],
+                     "ratio_vs_plain_auto": moves_per_s / rate["auto"],
+                     "longest_job_share_of_makespan": round((lat_longest[2] - lat_longest[0]) / makespan, 4)})
     for u in setups:
         u.close()
     return {"jobs_per_rate": n_jobs, "monomers_x_mcs": work, "every": every, "budget_bytes": budget,
-            "plain_one_at_a_time_s": plain_s, "plain_moves_per_s": work / plain_s, "rates": rows,
+            "plain_launch": rate["launch"], "plain_auto": rate["auto"], "rates": rows,
+            "longest_job": {"monomers": systems[longest].n, "mcs": mcs[longest], "box": list(systems[longest].box)},
             "unit": "attempted moves/s", "clock": "host wall clock, submit to completion",
-            "plain_path": f"BFM_MODE_LAUNCH one job at a time with observables every {every} MCS, "
-                          f"min(MCS, {plain_mcs}) MCS timed per job and scaled to its MCS"}
+            "plain": (f"each job alone on BFM_MODE_LAUNCH and on BFM_MODE_AUTO with observables every {every} MCS; "
+                      f"min(MCS, {sample_mcs}) MCS of each timed; rates = attempted moves / seconds of the samples")}
+
+
+REFERENCE_GPU_RUNS = {"dense_melt": (10, 200), "small": (100, 1000), "network": (100, 1000)}
+
+
+def reference_gpu(workloads=("dense_melt", "small", "network"), gpu=0, with_engine=True):
+    """Baseline leg: the reference's own GPU updater (src/pscbfm, compiled for sm_100a from its
+    sources into oracle/_ref by oracle/Makefile), timed on this GPU like its own tGpuLoop figure
+    (CUDA events on the legacy default stream it runs on, around runSimulationOnGPU(n), after an
+    untimed warm-up call), with the host clock of the same call beside it (the reference's MCS*N/t).
+    Beside each, the engine through the same call shape: one runSimulationOnGPU(n) plus the read-back
+    of the positions, host clock (with_engine; the reference arm runs the reference alone). Never the
+    engine's measured path: a baseline, like cpu_baseline."""
+    import numpy as np
+    from oracle import oracle as O
+    out = {}
+    for w in workloads:
+        s = build_workload(w)[0]
+        warm, timed = REFERENCE_GPU_RUNS[w]
+        conn = int(s.nbr_count.max())
+        if not O.ref_available(s.walls, conn):
+            out[w] = {"unavailable": "oracle/_ref not built (needs the reference sources at build time)"}
+            continue
+        ms, wall, ref_xyz = O.ref_time(s, warm, timed, reps=1, gpu=gpu)
+        moves = s.n * timed
+        row = {"monomers": s.n, "warmup_mcs": warm, "timed_mcs": timed,
+               "reference_device": moves / (ms / 1e3), "reference_ms_per_mcs": ms / timed,
+               "reference_host_clock": moves / wall,
+               "reference_build": "MAX_CONNECTIVITY 8" if conn > 4 else "MAX_CONNECTIVITY 4"}
+        out[w] = row
+        if not with_engine:
+            continue
+        import pscbfm_b200 as P
+        u = P.UpdaterGPUScBFM_AB_Type(gpu).load_system(s)
+        u.runSimulationOnGPU(warm)
+        t0 = time.perf_counter()
+        u.runSimulationOnGPU(timed)
+        ours_xyz = u.get_coords().copy()
+        t_ours = time.perf_counter() - t0
+        ours_dev_ms = u.run_timed(timed)
+        u.close()
+        row.update({"engine_same_call_host_clock": moves / t_ours, "engine_device": moves / (ours_dev_ms / 1e3),
+                    "ratio_device": (moves / (ours_dev_ms / 1e3)) / row["reference_device"],
+                    "ratio_host_clock": (moves / t_ours) / row["reference_host_clock"],
+                    "same_positions": bool(np.array_equal(ref_xyz, ours_xyz))})
+    return {"unit": "attempted moves/s", "workloads": out,
+            "how": ("reference: bfmref_time (oracle/ref_harness.cu), CUDA events on stream 0 around "
+                    "runSimulationOnGPU(timed_mcs) after runSimulationOnGPU(warmup_mcs), block size 128 and "
+                    "cudaMemset clearing (its stock settings); both include its copy-back of the positions. "
+                    "engine: the same two calls through the C-ABI plus bfm_get_coords_bulk (host clock), and a "
+                    "second run of timed_mcs timed by CUDA events (device); warm L2 on both sides")}
 
 
 def run_reference(args):
@@ -601,12 +742,19 @@ def run_reference(args):
                                   cores=args.cpu_cores)
     sample = (f"CPU restatement of the reference's colour-by-colour sweep (oracle/bfm_oracle.cpp), one "
               f"replica per core, {steps} MCS each after 1 warm-up MCS")
+    ref_gpu = None
+    if args.workload in REFERENCE_GPU_RUNS:
+        try:
+            ref_gpu = reference_gpu(workloads=(args.workload,), with_engine=False)
+        except Exception as e:   # no GPU or no reference build: the CPU arm stands alone
+            ref_gpu = {"unavailable": str(e).splitlines()[0][:200]}
     line = {"impl": "reference", "metric": "attempted monomer moves/s", "value": rate, "unit": "attempted moves/s",
             "n_gpus": args.gpus, "steps": steps, "warmup": 1, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic", "config": config,
             "cpu_baseline": {"value": rate, "unit": "attempted moves/s", "cores": cores,
                              "per_core": cpu_per_core(rate, cores), "kind": "port", "sample": sample},
-            "e2e": {"value": rate, "unit": "attempted moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": rate, "unit": "attempted moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_gpu": ref_gpu}
     print(json.dumps(line), flush=True)
 
 
