@@ -4,6 +4,7 @@
 // compile unchanged. Non-zero status codes become the reference's exception types.
 #pragma once
 
+#include <chrono>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -34,11 +35,19 @@ public:
     void setConnectivity(uint32_t a, uint32_t b) { check(bfm_add_bond(h_, a, b)); }
     void setLatticeSize(uint32_t bx, uint32_t by, uint32_t bz) { check(bfm_set_box(h_, bx, by, bz)); }
     void populateLattice() { check(bfm_populate_lattice(h_)); }
-    void runSimulationOnGPU(int32_t nMcs) { check(bfm_run(h_, nMcs)); }
+    void runSimulationOnGPU(int32_t nMcs)
+    {
+        check(bfm_run(h_, nMcs));
+        mtCopyBack0 = std::chrono::high_resolution_clock::now();
+    }
     int32_t getMonomerPositionInX(uint32_t i) { return coord(i, 0); }
     int32_t getMonomerPositionInY(uint32_t i) { return coord(i, 1); }
     int32_t getMonomerPositionInZ(uint32_t i) { return coord(i, 2); }
     void setPeriodicity(bool px, bool py, bool pz) { check(bfm_set_periodicity(h_, px, py, pz)); }
+
+    // when the last runSimulationOnGPU finished its sweep, before the positions are read back
+    // (the reference's public member, CRITICAL.cu:656, which its adapter reads)
+    std::chrono::time_point<std::chrono::high_resolution_clock> mtCopyBack0;
 
     // engine extensions
     void setSeed(uint64_t seed) { check(bfm_set_seed(h_, seed)); }

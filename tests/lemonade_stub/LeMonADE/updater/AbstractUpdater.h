@@ -1,5 +1,6 @@
 // Test stand-in for LeMonADE's updater base class (LeMonADE is not installed here): only what
-// include/bfm_lemonade.hpp uses, so that the adapter's code is compiled by the test suite.
+// include/bfm_lemonade.hpp and the reference's adapter (src/pscbfm/GPUScBFM_AB_Type.h) use, so that
+// both adapters' code is compiled by the test suite.
 #pragma once
 
 class AbstractUpdater

@@ -1,6 +1,7 @@
 """The C-ABI library: it loads, exports every symbol include/bfm.h declares, the Python binding
 declares a signature for each, and without a GPU it fails loudly (no CPU fallback)."""
 import ctypes as C
+import os
 import subprocess
 
 import numpy as np
@@ -122,3 +123,18 @@ int main() {
                         "-L", os.path.join(root, "pscbfm_b200"), "-lbfm",
                         "-Wl,-rpath," + os.path.join(root, "pscbfm_b200")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_reference_adapter_compiles_unchanged():
+    """The reference's LeMonADE adapter (src/pscbfm/GPUScBFM_AB_Type.h) and its logger header,
+    copied unchanged, compile and link over include/bfm_updater.hpp (oracle/Makefile target
+    `adapter`); the GPU suite runs the result against the oracle. Needs the reference tree
+    ($PSCBFM_REFERENCE, by default where this build's reference lies)."""
+    tree = os.environ.get("PSCBFM_REFERENCE", "/root/reference")
+    if not os.path.exists(os.path.join(tree, "src", "pscbfm", "GPUScBFM_AB_Type.h")):
+        pytest.skip("reference tree not present")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run(["make", "-s", "-B", "-C", os.path.join(root, "oracle"), "adapter", f"REF={tree}"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert os.path.exists(os.path.join(root, "oracle", "_ref", "ref_adapter"))

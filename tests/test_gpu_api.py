@@ -164,6 +164,41 @@ def test_lemonade_adapter_runs_like_the_oracle(tmp_path):
     assert np.array_equal(got, ref)
 
 
+def _adapter_input(s, steps, calls):
+    lines = [f"box {s.box[0]} {s.box[1]} {s.box[2]}", "periodic " + " ".join(str(int(p)) for p in s.periodic),
+             f"monomers {s.n}"]
+    lines += [f"{x} {y} {z} {a}" for (x, y, z), a in zip(s.xyz.tolist(), s.attributes.tolist())]
+    for i in range(s.n):
+        k = int(s.nbr_count[i])
+        lines.append(" ".join([str(k)] + [str(int(v)) for v in s.nbr_ids[i, :k]]))
+    lines.append(f"run {steps} {calls}")
+    return "\n".join(lines) + "\n"
+
+
+@pytest.mark.parametrize("build,steps,calls", [(S.small_chains, 50, 3), (S.square_network, 200, 2)])
+def test_reference_adapter_over_engine_vs_oracle(build, steps, calls):
+    """The reference's own LeMonADE adapter (src/pscbfm/GPUScBFM_AB_Type.h, compiled unchanged over
+    include/bfm_updater.hpp into oracle/_ref/ref_adapter) drives the engine through its
+    initialize/execute/cleanup: after `calls` execute() calls of `steps` MCS the positions equal the
+    oracle's after steps x calls MCS of the engine's default counter stream (seed 0), and the
+    molecules' age is steps x calls."""
+    import os
+    import subprocess
+    import numpy as np
+    from oracle import oracle as O
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "ref_adapter")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/ref_adapter is built only where the reference sources are present")
+    s = build()
+    run = subprocess.run([exe], input=_adapter_input(s, steps, calls), capture_output=True, text=True, timeout=300)
+    assert run.returncode == 0, run.stdout[-2000:] + run.stderr[-2000:]
+    lines = run.stdout.strip().split("\n")
+    got = np.array([[int(v) for v in ln.split()] for ln in lines[:s.n]])
+    assert lines[s.n] == f"age {steps * calls}"
+    want, _ = O.run(s, steps * calls, seed=0)
+    assert np.array_equal(got, want)
+
+
 def test_persistent_barrier_timeout_is_reported():
     """A persistent launch whose grid barrier cannot complete (injected on the host: the arrival
     count starts where no barrier's target is reached) ends at the barrier's time limit, the run
