@@ -115,6 +115,11 @@ int bfm_get_substep(bfm_handle h, uint64_t* substep);
 int bfm_set_draw_callback(bfm_handle h, bfm_draw_fn fn, void* ctx);
 /* Engine path, BFM_MODE_*. */
 int bfm_set_mode(bfm_handle h, int mode);
+/* CTA size of the check on this handle's grid paths (bond codes): 128, 256 or 512 threads over the
+ * same 512-monomer tile (0: the default, 256); results do not change. No reference counterpart:
+ * the reference's runSimulationOnGPU times block sizes itself when built with
+ * AUTO_CONFIGURE_BEST_SETTINGS_FOR_PSCBFM_ALGORITHM (CRITICAL.cu:445-487). */
+int bfm_set_grid_block(bfm_handle h, int block);
 /* The path the next run takes (after bfm_initialize): the mode set by bfm_set_mode with
  * BFM_MODE_AUTO resolved, and a mode the system cannot use replaced by BFM_MODE_GRAPH. */
 int bfm_get_path(bfm_handle h, int* mode);
@@ -233,12 +238,17 @@ int bfm_batch_set_cluster(bfm_batch_handle b, int on);
 int bfm_batch_run_each(bfm_batch_handle b, const int32_t* mcs);
 /* Register budget of the grid-phase kernels, 0..3, or -1 for the default; results do not change. */
 int bfm_batch_set_shape(bfm_batch_handle b, int shape);
+/* CTA size of the grid groups' check: 128, 256 or 512 threads over the same 512-monomer tile (0:
+ * the default, 256); results do not change. */
+int bfm_batch_set_block(bfm_batch_handle b, int block);
 /* Autotuner: runs every configuration (kernel shape x resident path on / off x cluster path on /
  * off) for 1 + mcs_per_trial MCS, keeps the fastest and reports it (shape, paths, ms per MCS;
  * paths: bit 0 the resident path, bit 1 the cluster path). The trials are ordinary MCS of the run
  * (results do not depend on the configuration): every member advances by n_trials x
- * (1 + mcs_per_trial) MCS. trials (may be NULL) receives up to capacity triples (shape, paths,
- * ms per MCS). */
+ * (1 + mcs_per_trial) MCS. Two stages: the paths (resident / cluster kernels on or off) with the
+ * grid kernels' defaults, then for the best paths the grid check's register budget (shape) x CTA
+ * size (128, 256, 512 threads; the reference sweeps its block size, CRITICAL.cu:445-487). trials
+ * (may be NULL) receives up to capacity quadruples (shape, paths, block, ms per MCS). */
 int bfm_batch_autotune(bfm_batch_handle b, int32_t mcs_per_trial, int* shape, int* paths, float* ms_per_mcs,
                        float* trials, uint32_t capacity, uint32_t* n_trials);
 const char* bfm_batch_last_error(bfm_batch_handle b);

@@ -107,6 +107,8 @@ _SIGS = {
     "bfm_batch_run_async": [H, C.c_int32],
     "bfm_batch_run_each": [H, _i32p],
     "bfm_batch_set_shape": [H, C.c_int],
+    "bfm_batch_set_block": [H, C.c_int],
+    "bfm_set_grid_block": [H, C.c_int],
     "bfm_batch_autotune": [H, C.c_int32, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float),
                            np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"), C.c_uint32,
                            C.POINTER(C.c_uint32)],

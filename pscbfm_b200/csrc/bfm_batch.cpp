@@ -242,7 +242,7 @@ cudaError_t Batch::launchGrid(StepEntry const* e)
             Updater const& u = *members_[m];
             cudaError_t err = g.codeMode == kCodeNone
                                   ? launch_check(u.deviceDesc(), nullptr, n, kGridBlock, e + m, stream_)
-                                  : launch_check_bc(u.desc(), u.deviceDesc(), nullptr, n, e + m, g.codeMode, stream_, shape_);
+                                  : launch_check_bc(u.desc(), u.deviceDesc(), nullptr, n, e + m, g.codeMode, stream_, shape_, block_);
             if (err != cudaSuccess) return err;
             err = g.codeMode == kCodeNone
                       ? launch_perform(u.deviceDesc(), nullptr, n, kGridBlock, e + m, stream_)
@@ -252,7 +252,7 @@ cudaError_t Batch::launchGrid(StepEntry const* e)
         }
         cudaError_t err = g.codeMode == kCodeNone
                               ? launch_check(dSys_, g.dTiles, n, kGridBlock, e, stream_)
-                              : launch_check_bc(unused, dSys_, g.dTiles, n, e, g.codeMode, stream_, shape_);
+                              : launch_check_bc(unused, dSys_, g.dTiles, n, e, g.codeMode, stream_, shape_, block_);
         if (err != cudaSuccess) return err;
         err = g.codeMode == kCodeNone
                   ? launch_perform(dSys_, g.dTiles, n, kGridBlock, e, stream_)
@@ -413,6 +413,14 @@ void Batch::setShape(int shape)
     shape_ = shape;
 }
 
+void Batch::setBlock(int block)
+{
+    if (block != 0 && !check_block_ok(block))
+        throw std::invalid_argument("[Batch::setBlock] the check's CTA size must be 128, 256 or 512 threads");
+    if (block != block_) built_ = false;   // the captured graph holds the old kernels
+    block_ = block;
+}
+
 std::vector<Batch::Trial> Batch::autotune(int32_t mcsPerTrial)
 {
     // Every configuration gives the same trajectories, so the trials are ordinary MCS of the run:
@@ -429,28 +437,47 @@ std::vector<Batch::Trial> Batch::autotune(int32_t mcsPerTrial)
         anyCluster[0] = anyCluster[0] || cl;
         anyCluster[1] = anyCluster[1] || (cl && !u->residentEligible());
     }
+    // Two stages, each configuration timed over the same kind of MCS: first the paths (resident
+    // kernel on / off x cluster kernel on / off, where either can matter) with the grid kernels'
+    // defaults; then, for the best paths and if some member runs on the grid-phase kernels, the
+    // check's register budget (kGridShapes) x its CTA size (128, 256, 512 threads), as the
+    // reference sweeps its block size (CRITICAL.cu:445-487).
     std::vector<Trial> trials;
+    auto time_it = [&](bool resident, bool cl, int shape, int block) {
+        setResidentEnabled(resident);
+        setClusterEnabled(cl);
+        setShape(shape);
+        setBlock(block);
+        rebuild();
+        runTimed(1);
+        trials.push_back(Trial{shape_, resident, cl, block_, runTimed(mcsPerTrial) / (float)mcsPerTrial});
+        return trials.back();
+    };
+    Trial best{};
+    bool first = true;
     for (int resident = 1; resident >= 0; --resident) {
         if (!resident && !anyResident) break;   // the same configuration as resident on
         for (int cl = 1; cl >= 0; --cl) {
             if (!cl && !anyCluster[resident]) break;   // the same configuration as cluster on
-            setResidentEnabled(resident != 0);
-            setClusterEnabled(cl != 0);
-            rebuild();
-            int const nShapes = grid_.empty() ? 1 : kGridShapes;   // the shape only matters to grid groups
-            for (int s = 0; s < nShapes; ++s) {
-                setShape(grid_.empty() ? -1 : s);
-                runTimed(1);
-                trials.push_back(Trial{shape_, resident != 0, cl != 0, runTimed(mcsPerTrial) / (float)mcsPerTrial});
-            }
+            Trial const t = time_it(resident != 0, cl != 0, -1, 0);
+            if (first || t.msPerMcs < best.msPerMcs) best = t;
+            first = false;
         }
     }
-    Trial best = trials.front();
-    for (Trial const& t : trials)
-        if (t.msPerMcs < best.msPerMcs) best = t;
+    setResidentEnabled(best.resident);
+    setClusterEnabled(best.cluster);
+    rebuild();
+    if (!grid_.empty()) {
+        for (int block : {128, 256, 512})
+            for (int sh = 0; sh < kGridShapes; ++sh) {
+                Trial const t = time_it(best.resident, best.cluster, sh, block);
+                if (t.msPerMcs < best.msPerMcs) best = t;
+            }
+    }
     setResidentEnabled(best.resident);
     setClusterEnabled(best.cluster);
     setShape(best.shape);
+    setBlock(best.block);
     return trials;
 }
 

@@ -168,6 +168,7 @@ int bfm_get_representation(bfm_handle h, int* out)
         *out = (int)h->u.codeMode();
     });
 }
+int bfm_set_grid_block(bfm_handle h, int block) { BFM_CALL(h, h->u.setGridBlock(block)); }
 int bfm_initialize(bfm_handle h) { BFM_CALL(h, h->u.initialize()); }
 int bfm_run(bfm_handle h, int32_t n) { BFM_CALL(h, h->u.runSimulationOnGPU(n)); }
 int bfm_run_async(bfm_handle h, int32_t n) { BFM_CALL(h, h->u.run(n)); }
@@ -430,6 +431,7 @@ int bfm_batch_run(bfm_batch_handle b, int32_t n)
     });
 }
 int bfm_batch_set_shape(bfm_batch_handle b, int shape) { BFM_CALL(b, b->b.setShape(shape)); }
+int bfm_batch_set_block(bfm_batch_handle b, int block) { BFM_CALL(b, b->b.setBlock(block)); }
 int bfm_batch_autotune(bfm_batch_handle b, int32_t mcsPerTrial, int* shape, int* paths, float* msPerMcs,
                        float* trials, uint32_t capacity, uint32_t* nTrials)
 {
@@ -445,9 +447,10 @@ int bfm_batch_autotune(bfm_batch_handle b, int32_t mcsPerTrial, int* shape, int*
         }
         if (trials)
             for (uint32_t i = 0; i < (uint32_t)t.size() && i < capacity; ++i) {
-                trials[3 * i] = (float)t[i].shape;
-                trials[3 * i + 1] = (float)((t[i].resident ? 1 : 0) | (t[i].cluster ? 2 : 0));
-                trials[3 * i + 2] = t[i].msPerMcs;
+                trials[4 * i] = (float)t[i].shape;
+                trials[4 * i + 1] = (float)((t[i].resident ? 1 : 0) | (t[i].cluster ? 2 : 0));
+                trials[4 * i + 2] = (float)t[i].block;
+                trials[4 * i + 3] = t[i].msPerMcs;
             }
         if (nTrials) *nTrials = (uint32_t)t.size();
     });

@@ -304,6 +304,20 @@ void Updater::setDrawCallback(DrawFn fn, void* ctx)
     drawCtx_ = ctx;
 }
 
+void Updater::setGridBlock(int block)
+{
+    // CTA size of the bond-code check (0: the default); the captured graphs hold the old launches
+    if (block != 0 && !check_block_ok(block))
+        throw std::invalid_argument("[setGridBlock] the check's CTA size must be 128, 256 or 512 threads");
+    if (block == gridBlock_) return;
+    if (!graphs_.empty()) {
+        if (stream_) cuda_check(cudaStreamSynchronize(stream_), "setGridBlock");
+        for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
+        graphs_.clear();
+    }
+    gridBlock_ = block;
+}
+
 void Updater::setMode(int mode)
 {
     if (mode < kModeAuto || mode > kModeCluster) throw std::invalid_argument("[setMode] unknown mode");
@@ -743,7 +757,7 @@ uint32_t Updater::gridTiles() const
 cudaError_t Updater::launchCheck(StepEntry const* e, cudaStream_t s) const
 {
     if (codeMode_ == kCodeNone) return launch_check(dev_.dDesc, nullptr, gridTiles(), kGridBlock, e, s);
-    return launch_check_bc(dev_.h, dev_.dDesc, nullptr, gridTiles(), e, codeMode_, s);
+    return launch_check_bc(dev_.h, dev_.dDesc, nullptr, gridTiles(), e, codeMode_, s, -1, gridBlock_);
 }
 
 cudaError_t Updater::launchPerform(StepEntry const* e, cudaStream_t s, PerformArgs const& pa) const

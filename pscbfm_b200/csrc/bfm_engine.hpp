@@ -98,6 +98,9 @@ public:
     void setDrawCounter(uint64_t seed);
     void setDrawCallback(DrawFn fn, void* ctx);
     void setMode(int mode);
+    // CTA size of the bond-code check on the grid paths (128, 256, 512; 0: the default 256)
+    void setGridBlock(int block);
+    int gridBlock() const { return gridBlock_; }
     // a system that only a Batch advances skips the pinned staging of its own run paths
     // (allocated on first use if it runs alone after all)
     void setBatchOnly(bool on) { batchOnly_ = on; }
@@ -253,6 +256,7 @@ private:
     cudaEvent_t stepsFree_ = nullptr;          // host staging may be rewritten after this event
     uint64_t launches_ = 0;
     uint64_t h2dBytes_ = 0, d2hBytes_ = 0;
+    int gridBlock_ = 0;
     int repr_ = 0;
     uint32_t codeMode_ = kCodeNone;
     uint32_t nMol_ = 0;
@@ -299,6 +303,9 @@ public:
     // register budget of the grid-phase kernels (launch_check_bc), -1: the default
     void setShape(int shape);
     int shape() const { return shape_; }
+    // CTA size of the grid groups' check (128, 256, 512; 0: the default)
+    void setBlock(int block);
+    int block() const { return block_; }
     bool residentEnabled() const { return residentOn_; }
     bool clusterEnabled() const { return clusterOn_; }
     // Runs the members under each configuration (kernel shape x resident path on / off x cluster
@@ -308,6 +315,7 @@ public:
         int shape;
         bool resident;
         bool cluster;
+        int block;
         float msPerMcs;
     };
     std::vector<Trial> autotune(int32_t mcsPerTrial);
@@ -381,6 +389,7 @@ private:
     bool clusterOn_ = true;
     bool built_ = false;
     int shape_ = -1;
+    int block_ = 0;
     cudaStream_t stream_ = nullptr, stream2_ = nullptr;
     cudaEvent_t join_ = nullptr, fork_ = nullptr, ready_ = nullptr;
     void* arena_ = nullptr;                    // descriptors, graph window, tiles, lists

@@ -41,17 +41,22 @@ cudaError_t launch_resident(SysDev const* dSys, uint32_t const* dList, uint32_t 
 // Bond-code kernels (SysDev::codeMode kCode32 / kCode64). Tiles span kBcTileSpan in-colour
 // indices. As in the gather representation, the perform zeroes the previous sub-step's marks, so a
 // stand-alone scrub is a perform launch whose entry has color == kNoColor.
-constexpr int kCheckMpt = 2;                                   // monomers per thread per pass
-constexpr uint32_t kBcTileSpan = kGridBlock * kCheckMpt;
+constexpr int kCheckMpt = 2;                                   // monomers per thread (256-thread CTAs)
+constexpr uint32_t kBcTileSpan = kGridBlock * kCheckMpt;       // 512 in-colour indices per tile
+// CTA sizes of the bond-code check: 128, 256 or 512 threads over the same tile (4, 2 or 1
+// monomers per thread); every size gives the same results
+constexpr uint32_t kCheckBlockDefault = 256;
+inline bool check_block_ok(int block) { return block == 128 || block == 256 || block == 512; }
 // dTiles == nullptr: single system, descriptor passed by value (hostDesc); otherwise the tile
-// list selects the system per CTA from dSys and hostDesc is unused. shape picks the register
-// budget (CTAs per SM) of the two kernels, 0 .. kGridShapes-1; negative: the default. Every shape
-// gives the same results.
+// list selects the system per CTA from dSys and hostDesc is unused. shape picks the check's register
+// budget (resident threads per SM), 0 .. kGridShapes-1, and block its CTA size (check_block_ok);
+// negative / 0: the defaults. Every shape and block gives the same results.
 constexpr int kGridShapes = 4;
 // The perform launch's tile list for a check tile list of bond-code systems: one tile per entry.
 std::vector<TileRef> perform_tile_list(std::vector<TileRef> const& tiles);
 cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
-                            StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1);
+                            StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1,
+                            int block = 0);
 // The perform takes one warp per tile. A single-system launch may carry the sub-step's parity and
 // scope (kPerfCur: walk its tentative movers, kPerfPrev: zero the previous sub-step's marks), so
 // it reads no step entry; parity == kParityFromEntry reads both from dSteps[0]. next != nullptr

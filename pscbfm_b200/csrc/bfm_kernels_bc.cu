@@ -376,15 +376,19 @@ __device__ __forceinline__ uint32_t perform_tile(SysDev const& S, uint32_t const
 
 // ---------------------------------------------------------------------------------- kernels
 
-template <typename W, int MPT, bool kMulti, int kMinBlocks = 1>
-__global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_check_bc(const __grid_constant__ SysDev S1,
+// Grid-phase check: CTA b of B threads covers tile b (kBcTileSpan in-colour indices, kBcTileSpan / B
+// per thread); a tile list (kMulti) gives each CTA its system and tile.
+template <typename W, int B, bool kMulti, int kMinBlocks = 1>
+__global__ void __launch_bounds__(B, kMinBlocks) k_check_bc(const __grid_constant__ SysDev S1,
                                                          SysDev const* __restrict__ sysv,
                                                          TileRef const* __restrict__ tiles,
                                                          StepEntry const* __restrict__ steps)
 {
     __shared__ SysDev Sm;
     __shared__ __align__(16) uint32_t dtab[kDirTab];
-    uint32_t sys = 0, start = blockIdx.x * (kGridBlock * MPT);
+    constexpr int MPT = (int)kBcTileSpan / B;
+    static_assert(B * MPT == (int)kBcTileSpan, "a CTA covers one list segment");
+    uint32_t sys = 0, start = blockIdx.x * kBcTileSpan;
     // one system: the direction table's load goes out with the step entry's
     uint32_t dv = (!kMulti && threadIdx.x < kDirTab) ? S1.dirTab[threadIdx.x] : 0u;
     if (kMulti) {
@@ -406,7 +410,6 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks) k_check_bc(const __gri
         if (threadIdx.x < kDirTab) dv = Sm.dirTab[threadIdx.x];
     }
     SysDev const& S = kMulti ? Sm : S1;
-    static_assert(kGridBlock * MPT == kBcTileSpan, "a CTA covers one list segment");
     __shared__ uint32_t segCount;
     if (threadIdx.x < kDirTab) dtab[threadIdx.x] = dv;
     if (threadIdx.x == 0) segCount = 0;
@@ -993,38 +996,54 @@ int sm_count()
     return c;
 }
 
-template <typename W, bool kMulti, int kMinCheck>
+template <typename W, bool kMulti, int B, int kMinCheck>
 void launch_grid_bc_k(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
                       uint32_t nTiles, StepEntry const* dSteps, PerformArgs const& pa, cudaStream_t s)
 {
     if (check) {
-        k_check_bc<W, kCheckMpt, kMulti, kMinCheck><<<nTiles, kGridBlock, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
+        k_check_bc<W, B, kMulti, kMinCheck><<<nTiles, B, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
         return;
     }
     k_perform_bc<W, kMulti><<<nTiles, 32, 0, s>>>(hostDesc, dSys, dTiles, dSteps, pa.parity, pa.scope, pa.next);
 }
 
-// shape: the check's register budget, 0: the compiler's choice, 1: 6 CTAs per SM, 2: 5, 3: 7 (the
-// default; BFM_GRID_SHAPE overrides it); the perform (one warp per tile) has a single form
-template <typename W, bool kMulti>
-void launch_grid_bc_m(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
+// shape: the check's register budget in resident threads per SM, 0: the compiler's choice, 1: 1536,
+// 2: 1280, 3: 1792 (the default; BFM_GRID_SHAPE overrides it); block: the check's CTA size (128, 256
+// or 512 threads over the same 512-monomer tile). The perform (one warp per tile) has one form.
+template <typename W, bool kMulti, int B>
+void launch_grid_bc_b(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
                       uint32_t nTiles, StepEntry const* dSteps, PerformArgs const& pa, int shape, cudaStream_t s)
 {
     switch (shape < 0 ? default_grid_shape() : shape) {
-    case 1: launch_grid_bc_k<W, kMulti, 6>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
-    case 2: launch_grid_bc_k<W, kMulti, 5>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
-    case 3: launch_grid_bc_k<W, kMulti, 7>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
-    default: launch_grid_bc_k<W, kMulti, 1>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
+    case 1: launch_grid_bc_k<W, kMulti, B, 1536 / B>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
+    case 2: launch_grid_bc_k<W, kMulti, B, 1280 / B>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
+    case 3: launch_grid_bc_k<W, kMulti, B, 1792 / B>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
+    default: launch_grid_bc_k<W, kMulti, B, 1>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
     }
+}
+
+template <typename W, bool kMulti>
+void launch_grid_bc_m(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
+                      uint32_t nTiles, StepEntry const* dSteps, PerformArgs const& pa, int shape, int block,
+                      cudaStream_t s)
+{
+    if (!check) {   // the perform's form does not depend on shape or block
+        launch_grid_bc_k<W, kMulti, 256, 1>(false, hostDesc, dSys, dTiles, nTiles, dSteps, pa, s);
+        return;
+    }
+    if (block == 128) launch_grid_bc_b<W, kMulti, 128>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, s);
+    else if (block == 512) launch_grid_bc_b<W, kMulti, 512>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, s);
+    else launch_grid_bc_b<W, kMulti, 256>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, s);
 }
 
 template <typename W>
 cudaError_t launch_grid_bc(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
-                           uint32_t nTiles, StepEntry const* dSteps, PerformArgs const& pa, int shape, cudaStream_t s)
+                           uint32_t nTiles, StepEntry const* dSteps, PerformArgs const& pa, int shape, int block,
+                           cudaStream_t s)
 {
-    if (shape >= kGridShapes) return cudaErrorInvalidValue;
-    if (dTiles) launch_grid_bc_m<W, true>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, s);
-    else launch_grid_bc_m<W, false>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, s);
+    if (shape >= kGridShapes || !check_block_ok(block)) return cudaErrorInvalidValue;
+    if (dTiles) launch_grid_bc_m<W, true>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, block, s);
+    else launch_grid_bc_m<W, false>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, block, s);
     return cudaGetLastError();
 }
 
@@ -1039,14 +1058,15 @@ std::vector<TileRef> perform_tile_list(std::vector<TileRef> const& tiles)
 }
 
 cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
-                            StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape)
+                            StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape, int block)
 {
     if (nTiles == 0) return cudaSuccess;
     PerformArgs const none{};
+    if (block <= 0) block = (int)kCheckBlockDefault;
     if (codeMode == kCode32)
-        return launch_grid_bc<uint32_t>(true, hostDesc, dSys, dTiles, nTiles, dSteps, none, shape, s);
+        return launch_grid_bc<uint32_t>(true, hostDesc, dSys, dTiles, nTiles, dSteps, none, shape, block, s);
     if (codeMode == kCode64)
-        return launch_grid_bc<unsigned long long>(true, hostDesc, dSys, dTiles, nTiles, dSteps, none, shape, s);
+        return launch_grid_bc<unsigned long long>(true, hostDesc, dSys, dTiles, nTiles, dSteps, none, shape, block, s);
     return cudaErrorInvalidValue;
 }
 
@@ -1056,9 +1076,11 @@ cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRe
 {
     if (nTiles == 0) return cudaSuccess;
     if (codeMode == kCode32)
-        return launch_grid_bc<uint32_t>(false, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, s);
+        return launch_grid_bc<uint32_t>(false, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape,
+                                        (int)kCheckBlockDefault, s);
     if (codeMode == kCode64)
-        return launch_grid_bc<unsigned long long>(false, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, s);
+        return launch_grid_bc<unsigned long long>(false, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape,
+                                                  (int)kCheckBlockDefault, s);
     return cudaErrorInvalidValue;
 }
 

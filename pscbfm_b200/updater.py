@@ -204,6 +204,10 @@ class UpdaterGPUScBFM_AB_Type:
         self._draw_cb = cb
         self._call("bfm_set_draw_callback", cb, None)
 
+    def set_grid_block(self, block: int):
+        """CTA size of the bond-code check on the grid paths (128, 256, 512; 0 = default 256)."""
+        self._call("bfm_set_grid_block", block)
+
     def set_mode(self, mode: int):
         self._call("bfm_set_mode", mode)
 
@@ -396,19 +400,27 @@ class Batch:
         """Register budget of the grid-phase kernels (0..3, -1 = default); results do not change."""
         self._call("bfm_batch_set_shape", shape)
 
+    def set_block(self, block: int):
+        """CTA size of the grid groups' check (128, 256, 512; 0 = default); results do not change."""
+        self._call("bfm_batch_set_block", block)
+
     def autotune(self, mcs_per_trial: int = 10) -> dict:
-        """Tries every configuration (kernel shape x resident path on / off x cluster path on / off)
-        for 1 + mcs_per_trial MCS each and keeps the fastest. The trials advance every member (the
-        results do not depend on the configuration)."""
-        trials = np.zeros(3 * 16, dtype=np.float32)
+        """Times the configurations in two stages (the resident / cluster paths on or off, then the
+        grid check's register budget x CTA size for the best paths), 1 + mcs_per_trial MCS each,
+        and keeps the fastest. The trials advance every member (the results do not depend on the
+        configuration)."""
+        cap = 64
+        trials = np.zeros(4 * cap, dtype=np.float32)
         shape, paths, best, n = C.c_int(), C.c_int(), C.c_float(), C.c_uint32()
         self._call("bfm_batch_autotune", mcs_per_trial, C.byref(shape), C.byref(paths), C.byref(best), trials,
-                   16, C.byref(n))
-        rows = trials[:3 * min(n.value, 16)].reshape(-1, 3)
+                   cap, C.byref(n))
+        rows = trials[:4 * min(n.value, cap)].reshape(-1, 4)
+        t = [{"shape": int(r[0]), "resident": bool(int(r[1]) & 1), "cluster": bool(int(r[1]) & 2),
+              "block": int(r[2]), "ms_per_mcs": float(r[3])} for r in rows]
+        bt = min(t, key=lambda q: q["ms_per_mcs"])
         return {"shape": shape.value, "resident": bool(paths.value & 1), "cluster": bool(paths.value & 2),
-                "ms_per_mcs": best.value, "mcs_spent": n.value * (1 + mcs_per_trial),
-                "trials": [{"shape": int(r[0]), "resident": bool(int(r[1]) & 1), "cluster": bool(int(r[1]) & 2),
-                            "ms_per_mcs": float(r[2])} for r in rows]}
+                "block": bt["block"], "ms_per_mcs": best.value, "mcs_spent": n.value * (1 + mcs_per_trial),
+                "trials": t}
 
     def set_cluster(self, on: bool):
         """Members too large for one CTA that a cluster of CTAs holds run in the cluster-resident

@@ -256,16 +256,19 @@ def test_batch_equals_each_system_alone(resident, cluster):
 
 
 def test_batch_autotune_keeps_trajectories():
-    """The autotuner's trials are ordinary MCS under different kernel shapes and paths: every
-    member ends where the oracle puts it after the same number of MCS."""
+    """The autotuner's trials are ordinary MCS under different paths, kernel shapes and CTA sizes:
+    every member ends where the oracle puts it after the same number of MCS."""
     systems = S.ensemble(n_systems=10, base_seed=700) + [S.crosslinked_network(), S.rings_and_free()]
     members = [P.UpdaterGPUScBFM_AB_Type(0).load_system(s) for s in systems]
     b = P.Batch(members)
     rep = b.autotune(3)
-    # the network runs in a cluster of CTAs alone, so the cluster path is a dimension of the trials
+    # stage 1: the paths (the network runs in a cluster of CTAs alone, so the cluster path is a
+    # dimension); stage 2: the grid check's register budget x CTA size for the best paths (the
+    # 128^3 members run on the grid-phase kernels under every path choice)
+    paths, grid = rep["trials"][:4], rep["trials"][4:]
+    assert {(t["resident"], t["cluster"]) for t in paths} == {(r, c) for r in (True, False) for c in (True, False)}
+    assert {(t["shape"], t["block"]) for t in grid} == {(s, bl) for s in range(4) for bl in (128, 256, 512)}
     assert len(rep["trials"]) == 16 and rep["mcs_spent"] == 16 * 4
-    assert {(t["shape"], t["resident"], t["cluster"]) for t in rep["trials"]} == \
-        {(s, r, c) for s in range(4) for r in (True, False) for c in (True, False)}
     assert rep["ms_per_mcs"] == min(t["ms_per_mcs"] for t in rep["trials"])
     b.run(17)
     for s, m in zip(systems, members):
@@ -382,3 +385,28 @@ def test_batch_lone_grid_members_vs_oracle():
         m.validate()
     for m in members:
         m.close()
+
+
+@pytest.mark.parametrize("block", [128, 256, 512])
+@pytest.mark.parametrize("name", ["melt256_16384x64_20mcs", "serp64_lc128_300mcs", "chains64_256x32_chunked"])
+def test_check_block_sizes_vs_reference(name, block):
+    """The bond-code check with 128, 256 or 512 threads over the same 512-monomer tile (4, 2 or 1
+    monomers per thread), on the graph path and one launch at a time: identical to the reference."""
+    g = json.load(open(GOLDEN_JSON))["cases"][name]
+    build, chunks = CASES[name]
+    s = build()
+    for mode in (P.MODE_GRAPH, P.MODE_LAUNCH):
+        u = P.UpdaterGPUScBFM_AB_Type(0)
+        u.load_system(s, mode=mode)
+        u.set_grid_block(block)
+        for c in chunks:
+            u.runSimulationOnGPU(c)
+        assert positions_digest(u.get_coords()) == g["sha256"], (name, block, mode)
+        u.close()
+
+
+def test_check_block_size_rejects_other_sizes():
+    u = P.UpdaterGPUScBFM_AB_Type(0)
+    with pytest.raises(ValueError, match="128, 256 or 512"):
+        u.set_grid_block(64)
+    u.close()
