@@ -310,3 +310,20 @@ def test_parallel_sweep_samples_like_the_serial_updater():
         assert abs(p - q) <= tol * q, (name, p, q)
     # and far from the straight initial chains (Ree^2 = (2 (16-1))^2 = 900)
     assert par[0] < 400
+
+
+def test_oracle_reproduces_reference_at_full_ensemble_length():
+    """The smallest ensemble systems after their full 10^4 MCS: the oracle ends where the reference
+    updater does (tests/golden/reference_long.json, make_golden.py --long)."""
+    from cases import LONG_JSON, ENSEMBLE_MCS, ensemble_case, ensemble_cases
+    if not os.path.exists(LONG_JSON):
+        pytest.fail("tests/golden/reference_long.json is missing (make_golden.py --long)")
+    gold = json.load(open(LONG_JSON))["cases"]
+    names = list(ensemble_cases())
+    sizes = sorted(range(len(names)), key=lambda i: gold[names[i]]["n"])
+    for i in sizes[:4]:
+        s = ensemble_case(i)
+        g = gold[names[i]]
+        assert s.n == g["n"] and s.seed == g["seed"]
+        xyz, _ = O.run(s, ENSEMBLE_MCS)
+        assert positions_digest(xyz) == g["sha256"], names[i]
