@@ -87,7 +87,8 @@ constexpr int kPerfQ = 4;
 
 template <typename W, int MPT, bool kNc = true>
 __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab, StepEntry const& st, uint32_t start,
-                                           uint32_t* segCount)
+                                           uint32_t* segCount, uint32_t const* pkPre = nullptr,
+                                           W const* codePre = nullptr)
 {
     uint32_t const B = blockDim.x, tid = threadIdx.x;
     uint32_t const* const PK = S.pk;
@@ -106,8 +107,13 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
     for (int q = 0; q < MPT; ++q) {
         uint32_t const i = start + tid + (uint32_t)q * B;
         bool const a = i < st.cnt;
-        pk[q] = a ? ldm<kNc>(PK + st.off + i) : 0u;
-        code[q] = a ? ldm<kNc>(CODE + st.off + i) : W(0);
+        if (pkPre != nullptr) {   // loaded by the caller before the step entry arrived
+            pk[q] = a ? pkPre[q] : 0u;
+            code[q] = a ? codePre[q] : W(0);
+        } else {
+            pk[q] = a ? ldm<kNc>(PK + st.off + i) : 0u;
+            code[q] = a ? ldm<kNc>(CODE + st.off + i) : W(0);
+        }
     }
     __syncthreads();
     // stage 2: direction, walls, bonds, front-plane words; the target's address replaces the
@@ -172,7 +178,7 @@ __device__ __forceinline__ uint32_t perform_movers(SysDev const& S, uint32_t con
     uint32_t nbr[N][CodeWord<W>::kSlots];
 #pragma unroll
     for (int q = 0; q < N; ++q) {
-        uint32_t const g = ent[q] & kEntSlotMask;
+        uint32_t const g = live[q] ? ent[q] & kEntSlotMask : 0u;
         code[q] = live[q] ? CODE[g] : W(0);
 #pragma unroll
         for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k)
@@ -180,7 +186,9 @@ __device__ __forceinline__ uint32_t perform_movers(SysDev const& S, uint32_t con
     }
 #pragma unroll
     for (int q = 0; q < N; ++q) {
-        uint32_t const d = (ent[q] >> 27) & 7u;
+        // a lane past its list's end may hold any stale word: direction 0 keeps its table reads in
+        // range (the direction table has six entries, the plane table three axes)
+        uint32_t const d = live[q] ? (ent[q] >> 27) & 7u : 0u;
         DirParams const D = dir_params(dtab, d);
         front_plane<false>(pl[q], S.planeTab, D, to[q], D.step, d);
     }
@@ -396,6 +404,22 @@ __global__ void __launch_bounds__(B, kMinBlocks) k_check_bc(const __grid_constan
         sys = tr.sys;
         start = tr.start;
     }
+    // one system of two colour groups (S1.spec2): the addresses and codes of both groups' slots of
+    // this tile are loaded together with the step entry, which then picks one, so the entry's load
+    // does not delay theirs
+    uint32_t pre2[2][MPT];
+    W code2[2][MPT];
+    if (!kMulti && S1.spec2) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int q = 0; q < MPT; ++q) {
+                uint32_t const i = start + threadIdx.x + (uint32_t)q * B;
+                bool const a = i < S1.grp2[2 * c + 1];
+                pre2[c][q] = a ? __ldg(S1.pk + S1.grp2[2 * c] + i) : 0u;
+                code2[c][q] = a ? __ldg(static_cast<W const*>(S1.code) + S1.grp2[2 * c] + i) : W(0);
+            }
+    }
     StepEntry const st = steps[sys];
     if (st.color == kNoColor) return;
     if (start >= st.cnt) {
@@ -413,7 +437,19 @@ __global__ void __launch_bounds__(B, kMinBlocks) k_check_bc(const __grid_constan
     __shared__ uint32_t segCount;
     if (threadIdx.x < kDirTab) dtab[threadIdx.x] = dv;
     if (threadIdx.x == 0) segCount = 0;
-    check_body<W, MPT>(S, dtab, st, start, &segCount);   // publishes both with its first barrier
+    if (!kMulti && S1.spec2) {
+        bool const second = st.color != 0u;
+        uint32_t pkSel[MPT];
+        W codeSel[MPT];
+#pragma unroll
+        for (int q = 0; q < MPT; ++q) {
+            pkSel[q] = second ? pre2[1][q] : pre2[0][q];
+            codeSel[q] = second ? code2[1][q] : code2[0][q];
+        }
+        check_body<W, MPT>(S, dtab, st, start, &segCount, pkSel, codeSel);   // publishes both with its first barrier
+    } else {
+        check_body<W, MPT>(S, dtab, st, start, &segCount);
+    }
     __syncthreads();
     if (threadIdx.x == 0 && st.color != kNoColor) {
         S.mcount[(size_t)st.parity * S.countStride + start / kBcTileSpan] = segCount;
