@@ -79,6 +79,8 @@ def workload_config(name, systems):
 
 # ------------------------------------------------------------------ algorithmic bytes (roofline)
 
+E2E_IN_FLIGHT = 2               # steps queued ahead of the one whose counters the e2e loop reads
+
 # dependent L2 round trips of one sub-step on the grid path (the latency model of the roofline)
 CHECK_ROUND_TRIPS = 3          # step entry -> lattice address and bond code -> occupancy words
 PERFORM_ROUND_TRIPS = 2        # list lengths, entries and targets -> code, neighbour refs, temporary words
@@ -435,26 +437,25 @@ def run_ours(args):
                                "model": "sub-steps x (dependent L2 round trips x L2 hit latency + 2 kernel periods), "
                                         "against the warm-L2 device time per MCS"}
 
-    # e2e through the C-ABI with host buffers: per step one run of 1 MCS (its sub-steps' draw
-    # entries uploaded from pinned memory) and a read of that step's move counters, which waits
-    # for the step; the host queues step t + 1 before it waits for step t's counters, so one step
-    # is in flight while it reads; the positions, in the caller's order, copied back into a pinned
-    # host array at the end
+    # e2e through the C-ABI with host buffers: per step one run of 1 MCS and a read of that step's
+    # move counters into host memory; the host queues steps t + 1 and t + 2 before it waits for
+    # step t's counters, so two steps are in flight while it reads; the positions, in the caller's
+    # order, copied back into a pinned host array at the end
     host_xyz = torch.empty((systems[0].n, 3), dtype=torch.int32, pin_memory=True).numpy()
     xfer0 = [m.transfer_bytes() for m in members]
     torch.cuda.synchronize()
     t = time.perf_counter()
-    prev = None
+    pending = []
     for _ in range(args.steps):
         if batch is None:
             u0.run_async(1)
         else:
             batch.run_async(1)
-        ticket = u0.stats_async()
-        if prev is not None:
-            u0.stats_wait(prev)
-        prev = ticket
-    u0.stats_wait(prev)
+        pending.append(u0.stats_async())
+        if len(pending) > E2E_IN_FLIGHT:
+            u0.stats_wait(pending.pop(0))
+    for ticket in pending:
+        u0.stats_wait(ticket)
     u0.get_coords(host_xyz)
     e2e_s = time.perf_counter() - t
     xfer1 = [m.transfer_bytes() for m in members]
@@ -465,7 +466,8 @@ def run_ours(args):
            "h2d_bytes_per_step": round(h2d / args.steps, 1), "d2h_bytes_per_step": round(d2h / args.steps, 1),
            "h2d_bytes": h2d, "d2h_bytes": d2h,
            "calls": "bfm_run_async(1) + bfm_stats_enqueue per step (the three move counters written into "
-                    "mapped host memory), bfm_stats_wait on the previous step's ticket (one step in flight), "
+                    "mapped host memory), bfm_stats_wait on the ticket of the step before the previous one "
+                    "(two steps in flight), "
                     "bfm_get_coords_bulk once into pinned memory; byte counts from bfm_transfer_bytes (the "
                     "step entries of the counter stream are made on the device, so after a chain's first "
                     "entry no host-to-device copy is needed)"}
@@ -703,9 +705,11 @@ def reference_gpu(workloads=("dense_melt", "small", "network"), gpu=0, with_engi
         if not O.ref_available(s.walls, conn):
             out[w] = {"unavailable": "oracle/_ref not built (needs the reference sources at build time)"}
             continue
-        ms, wall, ref_xyz = O.ref_time(s, warm, timed, reps=1, gpu=gpu)
+        # the reference's warm-up call is warm + timed MCS, so that after it both sides have run the
+        # same sub-steps (the engine's warm-up is `warm` plus one timed run of `timed` MCS)
+        ms, wall, ref_xyz = O.ref_time(s, warm + timed, timed, reps=1, gpu=gpu)
         moves = s.n * timed
-        row = {"monomers": s.n, "warmup_mcs": warm, "timed_mcs": timed,
+        row = {"monomers": s.n, "warmup_mcs": warm + timed, "timed_mcs": timed,
                "reference_device": moves / (ms / 1e3), "reference_ms_per_mcs": ms / timed,
                "reference_host_clock": moves / wall,
                "reference_build": "MAX_CONNECTIVITY 8" if conn > 4 else "MAX_CONNECTIVITY 4"}
@@ -713,13 +717,16 @@ def reference_gpu(workloads=("dense_melt", "small", "network"), gpu=0, with_engi
         if not with_engine:
             continue
         import pscbfm_b200 as P
+        import torch
         u = P.UpdaterGPUScBFM_AB_Type(gpu).load_system(s)
         u.runSimulationOnGPU(warm)
+        host = torch.empty((s.n, 3), dtype=torch.int32, pin_memory=True).numpy()
+        ours_dev_ms = u.run_timed(timed)   # also captures the graphs a call of timed MCS replays
         t0 = time.perf_counter()
         u.runSimulationOnGPU(timed)
-        ours_xyz = u.get_coords().copy()
+        u.get_coords(host)
         t_ours = time.perf_counter() - t0
-        ours_dev_ms = u.run_timed(timed)
+        ours_xyz = host.copy()
         u.close()
         row.update({"engine_same_call_host_clock": moves / t_ours, "engine_device": moves / (ours_dev_ms / 1e3),
                     "ratio_device": (moves / (ours_dev_ms / 1e3)) / row["reference_device"],
@@ -729,8 +736,10 @@ def reference_gpu(workloads=("dense_melt", "small", "network"), gpu=0, with_engi
             "how": ("reference: bfmref_time (oracle/ref_harness.cu), CUDA events on stream 0 around "
                     "runSimulationOnGPU(timed_mcs) after runSimulationOnGPU(warmup_mcs), block size 128 and "
                     "cudaMemset clearing (its stock settings); both include its copy-back of the positions. "
-                    "engine: the same two calls through the C-ABI plus bfm_get_coords_bulk (host clock), and a "
-                    "second run of timed_mcs timed by CUDA events (device); warm L2 on both sides")}
+                    "engine: after the same warm-up MCS (the last timed_mcs of them timed by CUDA events: "
+                    "engine_device), one runSimulationOnGPU(timed_mcs) plus bfm_get_coords_bulk into pinned "
+                    "memory on the host clock (engine_same_call_host_clock); warm L2 on both sides; "
+                    "same_positions compares the two after the same MCS")}
 
 
 def run_reference(args):

@@ -73,8 +73,6 @@ struct SysDev {
     uint32_t walls;                  // bit a: axis a is not periodic (corners stay in [0, L-2])
     uint32_t npad, nwords, maxc, nColors;
     struct StepGen* gen;             // device-side producer of the counter stream's sub-step entries
-    uint32_t spec2;                  // 1: two colour groups, grp2 holds them (the grid check loads both
-    uint32_t grp2[4];                //    groups' slots with its step entry): offset, size of each
     uint32_t mask[3];                // lattice side - 1 (a power of two; the box side but along a
                                      // walled axis whose side is not one)
     uint32_t lim[3];                 // box side - 1: on a walled axis a moved corner stays below it

@@ -65,15 +65,6 @@ inline uint32_t host_brick_pos(uint32_t v, uint32_t a) { return brick_pos(v, a);
 
 }  // namespace
 
-static bool check_spec_enabled()
-{
-    static bool const on = [] {
-        char const* e = std::getenv("BFM_CHECK_SPEC");
-        return e != nullptr && std::atoi(e) != 0;
-    }();
-    return on;
-}
-
 ArenaLayout arena_layout(uint32_t n, uint32_t npad, uint32_t maxc, uint32_t nwords, uint32_t ntab,
                          uint32_t nColors, uint32_t maxGroup, uint32_t codeMode)
 {
@@ -445,13 +436,6 @@ void Updater::initialize()
     h.nwords = nwords;
     h.maxc = maxc_;
     h.nColors = nC;
-    // two colour groups: the grid check may load both groups' slots with its step entry
-    // (BFM_CHECK_SPEC=1 turns that on)
-    h.spec2 = (nC == 2 && check_spec_enabled()) ? 1u : 0u;
-    for (uint32_t c = 0; c < 2; ++c) {
-        h.grp2[2 * c] = c < nC ? grpOff_[c] : 0u;
-        h.grp2[2 * c + 1] = c < nC ? grpSize_[c] : 0u;
-    }
     for (int a = 0; a < 3; ++a) {
         h.mask[a] = P[a] - 1;
         h.lim[a] = box_[a] - 1;

@@ -77,9 +77,10 @@ cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRe
 // cluster (hardware barriers) where allowCluster and the device can run it, otherwise a
 // cooperative launch with grid barriers in global memory. gs->count must be zeroed before the
 // launch; after it, gs->fault != 0 means a grid-barrier wait ran out and the system's state is not
-// usable. shape selects the CTAs per SM the register budget must fit: 0 -> 4, 1 -> 5, 2 -> 6 (two
-// monomers per thread, one mover-list segment per tile).
-constexpr int kSweepShapes = 3;
+// usable. shape selects the CTAs per SM the register budget must fit: 0 -> 4, 1 -> 5, 2 -> 6 (256
+// threads, two monomers per thread), 3 -> 7 (128 threads, four monomers per thread); one
+// mover-list segment of 512 monomers per tile in every shape.
+constexpr int kSweepShapes = 4;
 cudaError_t launch_sweep_bc(SysDev const& hostDesc, StepEntry const* dSteps, uint32_t nSteps, uint32_t maxGroup,
                             GridSync* gs, uint32_t codeMode, int shape, bool allowCluster, cudaStream_t s,
                             uint32_t* gridOut);

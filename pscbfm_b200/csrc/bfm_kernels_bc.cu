@@ -87,8 +87,7 @@ constexpr int kPerfQ = 4;
 
 template <typename W, int MPT, bool kNc = true>
 __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab, StepEntry const& st, uint32_t start,
-                                           uint32_t* segCount, uint32_t const* pkPre = nullptr,
-                                           W const* codePre = nullptr)
+                                           uint32_t* segCount)
 {
     uint32_t const B = blockDim.x, tid = threadIdx.x;
     uint32_t const* const PK = S.pk;
@@ -107,13 +106,8 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
     for (int q = 0; q < MPT; ++q) {
         uint32_t const i = start + tid + (uint32_t)q * B;
         bool const a = i < st.cnt;
-        if (pkPre != nullptr) {   // loaded by the caller before the step entry arrived
-            pk[q] = a ? pkPre[q] : 0u;
-            code[q] = a ? codePre[q] : W(0);
-        } else {
-            pk[q] = a ? ldm<kNc>(PK + st.off + i) : 0u;
-            code[q] = a ? ldm<kNc>(CODE + st.off + i) : W(0);
-        }
+        pk[q] = a ? ldm<kNc>(PK + st.off + i) : 0u;
+        code[q] = a ? ldm<kNc>(CODE + st.off + i) : W(0);
     }
     __syncthreads();
     // stage 2: direction, walls, bonds, front-plane words; the target's address replaces the
@@ -404,22 +398,6 @@ __global__ void __launch_bounds__(B, kMinBlocks) k_check_bc(const __grid_constan
         sys = tr.sys;
         start = tr.start;
     }
-    // one system of two colour groups (S1.spec2): the addresses and codes of both groups' slots of
-    // this tile are loaded together with the step entry, which then picks one, so the entry's load
-    // does not delay theirs
-    uint32_t pre2[2][MPT];
-    W code2[2][MPT];
-    if (!kMulti && S1.spec2) {
-#pragma unroll
-        for (int c = 0; c < 2; ++c)
-#pragma unroll
-            for (int q = 0; q < MPT; ++q) {
-                uint32_t const i = start + threadIdx.x + (uint32_t)q * B;
-                bool const a = i < S1.grp2[2 * c + 1];
-                pre2[c][q] = a ? __ldg(S1.pk + S1.grp2[2 * c] + i) : 0u;
-                code2[c][q] = a ? __ldg(static_cast<W const*>(S1.code) + S1.grp2[2 * c] + i) : W(0);
-            }
-    }
     StepEntry const st = steps[sys];
     if (st.color == kNoColor) return;
     if (start >= st.cnt) {
@@ -437,19 +415,7 @@ __global__ void __launch_bounds__(B, kMinBlocks) k_check_bc(const __grid_constan
     __shared__ uint32_t segCount;
     if (threadIdx.x < kDirTab) dtab[threadIdx.x] = dv;
     if (threadIdx.x == 0) segCount = 0;
-    if (!kMulti && S1.spec2) {
-        bool const second = st.color != 0u;
-        uint32_t pkSel[MPT];
-        W codeSel[MPT];
-#pragma unroll
-        for (int q = 0; q < MPT; ++q) {
-            pkSel[q] = second ? pre2[1][q] : pre2[0][q];
-            codeSel[q] = second ? code2[1][q] : code2[0][q];
-        }
-        check_body<W, MPT>(S, dtab, st, start, &segCount, pkSel, codeSel);   // publishes both with its first barrier
-    } else {
-        check_body<W, MPT>(S, dtab, st, start, &segCount);
-    }
+    check_body<W, MPT>(S, dtab, st, start, &segCount);   // publishes both with its first barrier
     __syncthreads();
     if (threadIdx.x == 0 && st.color != kNoColor) {
         S.mcount[(size_t)st.parity * S.countStride + start / kBcTileSpan] = segCount;
@@ -584,12 +550,12 @@ __device__ __forceinline__ void cluster_barrier()
 // takes tiles b, b + gridDim.x, ... of kGridBlock * MPT in-colour indices. Same bodies as
 // k_check_bc / k_perform_bc, with plain loads of the state other CTAs change during the launch;
 // the step entries are prefetched one sub-step ahead and the move counters flushed once.
-template <typename W, int MPT, int kMinBlocks, bool kCluster>
-__global__ void __launch_bounds__(kGridBlock, kMinBlocks)
+template <typename W, int MPT, int kMinBlocks, bool kCluster, int B = (int)kGridBlock>
+__global__ void __launch_bounds__(B, kMinBlocks)
     k_sweep_bc(const __grid_constant__ SysDev S, StepEntry const* __restrict__ steps, uint32_t nSteps,
                uint32_t nTiles, GridSync* gs)
 {
-    static_assert(kGridBlock * MPT == kBcTileSpan, "a tile is one list segment");
+    static_assert(B * MPT == (int)kBcTileSpan, "a tile is one list segment");
     __shared__ __align__(16) uint32_t dtab[kDirTab];
     __shared__ uint32_t tallyT, tallyA, okSm, segCount, pre[4];
     if (ld_acquire_gpu(&gs->fault) != 0u) return;   // an earlier launch failed: the state is not usable
@@ -599,7 +565,7 @@ __global__ void __launch_bounds__(kGridBlock, kMinBlocks)
         tallyA = 0u;
     }
     __syncthreads();
-    constexpr uint32_t span = kGridBlock * MPT;
+    constexpr uint32_t span = kBcTileSpan;
     unsigned int target = 0u;   // this CTA's count target of the next barrier
     unsigned long long att = 0ull;
     StepEntry next = steps[0];
@@ -1125,7 +1091,7 @@ namespace {
 // A sweep grid of at most this many CTAs runs as one cluster (a non-portable size above 8)
 constexpr uint32_t kMaxSweepCluster = 16;
 
-template <typename W, int MPT, int kMinBlocks>
+template <typename W, int MPT, int kMinBlocks, int B = (int)kGridBlock>
 cudaError_t launch_sweep_bc_k(SysDev const& S, StepEntry const* dSteps, uint32_t nSteps, uint32_t maxGroup,
                               GridSync* gs, bool allowCluster, cudaStream_t s, uint32_t* gridOut)
 {
@@ -1137,21 +1103,21 @@ cudaError_t launch_sweep_bc_k(SysDev const& S, StepEntry const* dSteps, uint32_t
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (!occ[dev & 63]) {
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[dev & 63], k_sweep_bc<W, MPT, kMinBlocks, false>,
-                                                          kGridBlock, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[dev & 63], k_sweep_bc<W, MPT, kMinBlocks, false, B>,
+                                                          B, 0);
         if (e != cudaSuccess) return e;
         e = cudaDeviceGetAttribute(&nsm[dev & 63], cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
         if (occ[dev & 63] < 1) return cudaErrorInvalidConfiguration;
     }
-    uint32_t nTiles = (maxGroup + kGridBlock * MPT - 1) / (kGridBlock * MPT);
+    uint32_t nTiles = (maxGroup + kBcTileSpan - 1) / kBcTileSpan;
     if (nTiles == 0) nTiles = 1;
     uint32_t const grid = std::min<uint32_t>(nTiles, (uint32_t)(occ[dev & 63] * nsm[dev & 63]));
     if (gridOut) *gridOut = grid;
     void* args[] = {const_cast<SysDev*>(&S), &dSteps, &nSteps, &nTiles, &gs};
     if (allowCluster && grid <= kMaxSweepCluster) {
         // the whole grid as one cluster, its barriers in hardware, where the device can run it
-        auto kernel = k_sweep_bc<W, MPT, kMinBlocks, true>;
+        auto kernel = k_sweep_bc<W, MPT, kMinBlocks, true, B>;
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1159,7 +1125,7 @@ cudaError_t launch_sweep_bc_k(SysDev const& S, StepEntry const* dSteps, uint32_t
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
         cfg.gridDim = dim3(grid);
-        cfg.blockDim = dim3(kGridBlock);
+        cfg.blockDim = dim3(B);
         cfg.stream = s;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
@@ -1175,8 +1141,8 @@ cudaError_t launch_sweep_bc_k(SysDev const& S, StepEntry const* dSteps, uint32_t
         }
         if (ok == 1) return cudaLaunchKernelExC(&cfg, reinterpret_cast<void const*>(kernel), args);
     }
-    return cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(k_sweep_bc<W, MPT, kMinBlocks, false>),
-                                       dim3(grid), dim3(kGridBlock), args, 0, s);
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(k_sweep_bc<W, MPT, kMinBlocks, false, B>),
+                                       dim3(grid), dim3(B), args, 0, s);
 }
 
 template <typename W>
@@ -1187,6 +1153,9 @@ cudaError_t launch_sweep_bc_w(SysDev const& S, StepEntry const* dSteps, uint32_t
     case 0: return launch_sweep_bc_k<W, kCheckMpt, 4>(S, dSteps, nSteps, maxGroup, gs, allowCluster, s, gridOut);
     case 1: return launch_sweep_bc_k<W, kCheckMpt, 5>(S, dSteps, nSteps, maxGroup, gs, allowCluster, s, gridOut);
     case 2: return launch_sweep_bc_k<W, kCheckMpt, 6>(S, dSteps, nSteps, maxGroup, gs, allowCluster, s, gridOut);
+    // 128-thread CTAs, four monomers per thread, seven CTAs per SM: up to 7 x SMs tiles of 512
+    // monomers (a million-monomer colour group) each take a CTA of their own
+    case 3: return launch_sweep_bc_k<W, 4, 7, 128>(S, dSteps, nSteps, maxGroup, gs, allowCluster, s, gridOut);
     default: return cudaErrorInvalidValue;
     }
 }
