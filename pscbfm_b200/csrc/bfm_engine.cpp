@@ -106,6 +106,7 @@ ArenaLayout arena_layout(uint32_t n, uint32_t npad, uint32_t maxc, uint32_t nwor
     // position read-back in the caller's order
     L.slotOf = take(4ull * n);
     L.xyzOut = take(12ull * n);
+    L.snap = take(8ull * (4 * kSnapRing + 1));   // counter snapshots of graph replays, then their count
     L.bytes = off;
     return L;
 }
@@ -453,6 +454,8 @@ void Updater::initialize()
     dev_.gs = reinterpret_cast<GridSync*>(base + L.gs);
     dev_.slotOf = reinterpret_cast<uint32_t*>(base + L.slotOf);
     dev_.xyzOut = reinterpret_cast<int32_t*>(base + L.xyzOut);
+    dev_.snap = reinterpret_cast<unsigned long long*>(base + L.snap);
+    dev_.snapSeq = dev_.snap + 4 * kSnapRing;
     h.pk = reinterpret_cast<uint32_t*>(base + L.pk);
     h.code = base + L.code;
     h.nbrr = reinterpret_cast<uint32_t*>(base + L.nbrr);
@@ -513,6 +516,7 @@ void Updater::initialize()
     cuda_check(cudaMemsetAsync(dev_.dList, 0, 4, s), "memset list");
     cuda_check(cudaMemsetAsync(dev_.gs, 0, sizeof(GridSync), s), "memset grid barrier");
     cuda_check(cudaMemsetAsync(h.gen, 0, sizeof(StepGen), s), "memset step producer");   // off
+    cuda_check(cudaMemsetAsync(dev_.snap, 0, 8ull * (4 * kSnapRing + 1), s), "memset snapshots");
     if (segs) {
         cuda_check(cudaMemsetAsync(h.mcount, 0, 4ull * 2 * segs, s), "memset mover counts");
         // the grid perform loads list slots past a list's end and ignores them: they start as zeros
@@ -530,6 +534,8 @@ void Updater::initialize()
     hostStale_ = false;
     chainValid_ = false;
     genOn_ = 0;
+    snapIssued_ = 0;
+    lastRunSnap_ = false;
 }
 
 void Updater::hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, std::vector<uint32_t>& nbrr) const
@@ -863,6 +869,7 @@ void Updater::scrubPending(cudaStream_t s)
     h2dBytes_ += sizeof(StepEntry);
     cuda_check(cudaEventRecord(stepsFree_, s), "event");
     chainValid_ = false;
+    lastRunSnap_ = false;
     // both representations scrub the previous sub-step's marks in the perform
     cuda_check(launchPerform(dev_.dSteps, s, performArgs(hSteps_[0])), "scrub");
     ++launches_;
@@ -872,6 +879,7 @@ void Updater::scrubPending(cudaStream_t s)
 void Updater::noteExternalRun(uint64_t subSteps, uint64_t mcs, bool pendingMarks, uint32_t lastColor)
 {
     (void)subSteps;
+    lastRunSnap_ = false;
     mcsDone_ += mcs;
     hostStale_ = true;
     lastColor_ = pendingMarks ? lastColor : kNoColor;
@@ -915,6 +923,7 @@ cudaGraphExec_t Updater::graphFor(uint32_t nSteps, uint32_t parity0)
         pa.next = nSteps >= 2 ? dev_.dSteps + (t + 1) % nSteps : nullptr;
         if (err == cudaSuccess) err = launchPerform(dev_.dSteps + t, stream_, pa);
     }
+    if (err == cudaSuccess) err = launch_snapshot_stats(dev_.h.stats, dev_.snap, dev_.snapSeq, stream_);
     cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
     cuda_check(err, "capture launches");
     cuda_check(endErr, "end capture");
@@ -994,9 +1003,11 @@ void Updater::enqueueGraph(uint32_t nSteps)
             cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         }
         cuda_check(cudaGraphLaunch(exec, stream_), "graph launch");
-        launches_ += 2ull * chunk;
+        launches_ += 2ull * chunk + 1;
+        ++snapIssued_;
         done += chunk;
     }
+    lastRunSnap_ = true;
 }
 
 float Updater::runTimed(int32_t nMcs)
@@ -1029,6 +1040,7 @@ void Updater::timeKernels(int32_t nMcs, double out[4])
     // it runs on; sums per kernel
     requireInit("timeKernels");
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
+    lastRunSnap_ = false;
     ensureStaging();
     scrubPending(stream_);
     uint32_t const nSteps = (uint32_t)nMcs * (uint32_t)grpSize_.size();
@@ -1197,6 +1209,7 @@ void Updater::run(int32_t nMcs)
     if (total > 0xFFFFFFFFull) throw std::invalid_argument("[runSimulationOnGPU] too many sub-steps in one call");
     uint32_t const nSteps = (uint32_t)total;
     ensureStaging();
+    lastRunSnap_ = false;   // enqueueGraph sets it again
     int const m = effectiveMode();
     if (m == kModeResident) enqueueResident(nSteps);
     else if (m == kModeGraph) enqueueGraph(nSteps);
@@ -1395,13 +1408,31 @@ uint64_t Updater::statsEnqueue()
         dStatRing_ = static_cast<unsigned long long*>(d);
         for (cudaEvent_t& e : statEv_) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
     }
-    // a slot's previous write precedes this one on the stream, so the slot is reused in order; the
-    // sums are written into host memory by a kernel (no copy-engine transfer between the kernels)
+    // the sums are written into host memory by a kernel (no copy-engine transfer between the
+    // kernels); a slot's new write waits for its previous one, whichever stream made it
     uint64_t const t = ++statNext_;
     uint32_t const k = (uint32_t)(t % kStatRing);
-    cuda_check(launch_publish_stats(dev_.h.stats, dStatRing_ + 4ull * k, stream_), "stats");
+    if (lastRunSnap_) {
+        // the last graph replay left its counters in snapshot slot (snapIssued_ - 1): copy that into
+        // host memory on the publishing stream, so the sweep's stream goes on at once
+        if (!pubStream_) {
+            cuda_check(cudaStreamCreateWithFlags(&pubStream_, cudaStreamNonBlocking), "cudaStreamCreate");
+            cuda_check(cudaEventCreateWithFlags(&pubEv_, cudaEventDisableTiming), "cudaEventCreate");
+        }
+        cuda_check(cudaEventRecord(pubEv_, stream_), "event");
+        cuda_check(cudaStreamWaitEvent(pubStream_, pubEv_, 0), "wait");
+        cuda_check(cudaStreamWaitEvent(pubStream_, statEv_[k], 0), "wait");
+        uint64_t const slot = (snapIssued_ - 1) % kSnapRing;
+        cuda_check(launch_publish_snap(dev_.snap + 4 * slot, dStatRing_ + 4ull * k, pubStream_), "stats");
+        cuda_check(cudaEventRecord(statEv_[k], pubStream_), "event");
+        statSeq_[k] = snapIssued_;
+    } else {
+        cuda_check(cudaStreamWaitEvent(stream_, statEv_[k], 0), "wait");
+        cuda_check(launch_publish_stats(dev_.h.stats, dStatRing_ + 4ull * k, stream_), "stats");
+        cuda_check(cudaEventRecord(statEv_[k], stream_), "event");
+        statSeq_[k] = 0;
+    }
     d2hBytes_ += 3 * sizeof(unsigned long long);   // written into mapped host memory
-    cuda_check(cudaEventRecord(statEv_[k], stream_), "event");
     statTicket_[k] = t;
     statMcs_[k] = mcsDone_;
     return t;
@@ -1416,6 +1447,9 @@ void Updater::statsWait(uint64_t ticket, uint64_t out[4])
     cuda_check(cudaEventSynchronize(statEv_[k]), "stats");
     std::atomic_thread_fence(std::memory_order_acquire);
     unsigned long long const volatile* const slot = hStatRing_ + 4ull * k;
+    if (statSeq_[k] != 0 && slot[3] != statSeq_[k])
+        throw CudaError("[stats] the counters' snapshot was replaced before it was copied (more than 64 graph "
+                        "replays ahead of the read)");
     for (uint32_t c = 0; c < 3; ++c) out[c] = slot[c];
     out[3] = statMcs_[k];
 }
@@ -1498,6 +1532,16 @@ void Updater::validate()
 
 void Updater::freeDevice()
 {
+    // the publishing stream reads the arena's snapshots and writes the host ring: done first
+    if (pubStream_) {
+        cudaStreamSynchronize(pubStream_);
+        cudaStreamDestroy(pubStream_);
+        pubStream_ = nullptr;
+    }
+    if (pubEv_) {
+        cudaEventDestroy(pubEv_);
+        pubEv_ = nullptr;
+    }
     if (!graphs_.empty() && stream_) cudaStreamSynchronize(stream_);   // no graph of ours in flight
     for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
     graphs_.clear();
@@ -1546,6 +1590,7 @@ void Updater::freeDevice()
         dStatRing_ = nullptr;
         for (uint32_t k = 0; k < kStatRing; ++k) statTicket_[k] = 0;
     }
+
 }
 
 void Updater::cleanup()

@@ -33,7 +33,7 @@ std::vector<uint8_t> colour_bond_graph(uint32_t n, uint32_t const* cnt, uint32_t
 // job's device bytes with it before the job is coloured.
 struct ArenaLayout {
     size_t x, y, z, nbr, nnb, flags, mark, lat, tmp, tab, grp, stats, desc, steps, list, gs;
-    size_t pk, code, nbrr, plane, moveOk, dir, mlist, mword, mcount, slotOf, xyzOut;
+    size_t pk, code, nbrr, plane, moveOk, dir, mlist, mword, mcount, slotOf, xyzOut, snap;
     uint32_t segs;   // mover-list segments (tiles) per parity
     size_t bytes;
 };
@@ -180,6 +180,8 @@ private:
         GridSync* gs = nullptr;        // grid barrier of the persistent kernel
         uint32_t* slotOf = nullptr;    // [n] sorted slot of each monomer (caller's order)
         int32_t* xyzOut = nullptr;     // [3 n] positions in the caller's order, for read-back
+        unsigned long long* snap = nullptr;      // [kSnapRing][4] counter snapshots of graph replays
+        unsigned long long* snapSeq = nullptr;   // snapshots taken so far
     };
     void requireN(char const* who) const;
     void requireInit(char const* who) const;
@@ -240,6 +242,13 @@ private:
     unsigned long long* dStats_ = nullptr;     // hStats_ as the device addresses it
     cudaEvent_t statEv_[kStatRing] = {};
     uint64_t statTicket_[kStatRing] = {}, statMcs_[kStatRing] = {}, statNext_ = 0;
+    // every graph replay ends with a counter snapshot (k_snapshot_stats); a ticket taken right after
+    // a graph-path run copies that snapshot into host memory on pubStream_, off the sweep's stream
+    uint64_t statSeq_[kStatRing] = {};   // expected snapshot sequence of a ticket (0: direct read)
+    uint64_t snapIssued_ = 0;            // graph replays enqueued (= the device's snapshot count)
+    bool lastRunSnap_ = false;           // the last work changing the counters was a graph replay
+    cudaStream_t pubStream_ = nullptr;
+    cudaEvent_t pubEv_ = nullptr;
     bool gsPending_ = false;                   // hGs_ is being refreshed by the stream
     bool stallNext_ = false;                   // injectBarrierStall
     uint32_t smCount_ = 148;                   // SMs of the device (setGpu)

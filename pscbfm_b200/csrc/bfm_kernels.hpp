@@ -63,6 +63,8 @@ cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef 
 // (one system): CTA 0 writes the following sub-step's entry there (write_next_step). Tile lists
 // (several systems) always read each system's entry; parity, scope and next are ignored.
 constexpr uint32_t kParityFromEntry = 0xFFFFFFFFu;
+constexpr uint32_t kPerformWarpsDefault = 4;   // warps per CTA of the perform
+constexpr uint32_t kPerformGroupDefault = 4;   // warps per tile of the perform
 constexpr uint32_t kPerfCur = 1u, kPerfPrev = 2u;
 struct PerformArgs {
     uint32_t parity = kParityFromEntry;
@@ -77,10 +79,9 @@ cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRe
 // cluster (hardware barriers) where allowCluster and the device can run it, otherwise a
 // cooperative launch with grid barriers in global memory. gs->count must be zeroed before the
 // launch; after it, gs->fault != 0 means a grid-barrier wait ran out and the system's state is not
-// usable. shape selects the CTAs per SM the register budget must fit: 0 -> 4, 1 -> 5, 2 -> 6 (256
-// threads, two monomers per thread), 3 -> 7 (128 threads, four monomers per thread); one
-// mover-list segment of 512 monomers per tile in every shape.
-constexpr int kSweepShapes = 4;
+// usable. shape selects the CTAs per SM the register budget must fit: 0 -> 4, 1 -> 5, 2 -> 6 (two
+// monomers per thread, one mover-list segment per tile).
+constexpr int kSweepShapes = 3;
 cudaError_t launch_sweep_bc(SysDev const& hostDesc, StepEntry const* dSteps, uint32_t nSteps, uint32_t maxGroup,
                             GridSync* gs, uint32_t codeMode, int shape, bool allowCluster, cudaStream_t s,
                             uint32_t* gridOut);
@@ -120,5 +121,12 @@ cudaError_t launch_gather_positions(SysDev const& h, uint32_t const* slotOf, uin
 // Writes the sums over the kStatSlots slots of the three move counters (attempted, tentative,
 // accepted) into out[0..3), mapped pinned host memory.
 cudaError_t launch_publish_stats(unsigned long long const* stats, unsigned long long* out, cudaStream_t s);
+// The sweep graph's last node: the counters' sums into a device ring of kSnapRing slots of four
+// words ({attempted, tentative, accepted, sequence}), slot *seq % kSnapRing, and ++*seq. Then
+// k_publish_snap copies one slot into host memory on another stream.
+constexpr uint32_t kSnapRing = 64;
+cudaError_t launch_snapshot_stats(unsigned long long const* stats, unsigned long long* snap, unsigned long long* seq,
+                                  cudaStream_t s);
+cudaError_t launch_publish_snap(unsigned long long const* slot, unsigned long long* out, cudaStream_t s);
 
 }  // namespace bfm

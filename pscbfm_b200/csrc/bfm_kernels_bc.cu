@@ -317,17 +317,18 @@ __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* dt
     if (nAcc) atomicAdd(tally, nAcc);
 }
 
-// Grid-phase perform: one warp per tile. The warp walks list segment `tile` of this sub-step
-// (parity p: its tentative movers) and of the previous one (parity p ^ 1: it zeroes the
-// temporary-lattice words those movers marked). Every load of the first pass is independent of
-// the others: both list lengths and the first 32 kPerfQ entries and target addresses of both lists
-// come in one round trip, so no length scan or barrier precedes the movers' own loads; entries
-// past a list's end lie inside the tile's segment and are ignored. The lengths are exact for every
-// tile of the launch: a check CTA whose tile lies beyond its colour group stores a zero length.
-// Longer lists take further passes. Returns the moves applied.
-template <typename W, bool kNc>
+// Grid-phase perform of one tile by a group of G warps (`sub` = this warp's index in the group):
+// the group walks list segment `tile` of this sub-step (parity p: its tentative movers) and of the
+// previous one (parity p ^ 1: it zeroes the temporary-lattice words those movers marked), warp
+// `sub` taking entries sub * 32 + lane + 32 G q. Every load of the first pass is independent of the
+// others: both list lengths and Q entries, target addresses and previous targets per lane come in
+// one round trip, so no length scan or barrier precedes the movers' own loads; entries past a
+// list's end lie inside the tile's segment and are ignored. The lengths are exact for every tile of
+// the launch: a check CTA whose tile lies beyond its colour group stores a zero length. Longer lists
+// take further passes. Returns the moves this warp applied.
+template <typename W, bool kNc, int Q>
 __device__ __forceinline__ uint32_t perform_tile(SysDev const& S, uint32_t const* dtab, uint32_t p, uint32_t tile,
-                                                 bool doCur, bool doPrev)
+                                                 bool doCur, bool doPrev, uint32_t sub, uint32_t G)
 {
     uint32_t const lane = threadIdx.x & 31u;
     size_t const seg = (size_t)tile * kBcTileSpan;
@@ -338,36 +339,37 @@ __device__ __forceinline__ uint32_t perform_tile(SysDev const& S, uint32_t const
     unsigned long long* const tprev = S.tmp + (size_t)(p ^ 1u) * S.nwords;
     uint32_t const cnt = doCur ? ldm<kNc>(S.mcount + (size_t)p * S.countStride + tile) : 0u;
     uint32_t const pcnt = doPrev ? ldm<kNc>(S.mcount + (size_t)(p ^ 1u) * S.countStride + tile) : 0u;
-    uint32_t ent[kPerfQ], to[kPerfQ], pw[kPerfQ];
-    bool live[kPerfQ];
+    uint32_t const first = sub * 32u + lane, stride = 32u * G;
+    uint32_t ent[Q], to[Q], pw[Q];
+    bool live[Q];
 #pragma unroll
-    for (int q = 0; q < kPerfQ; ++q) {
-        uint32_t const e = lane + 32u * (uint32_t)q;
+    for (int q = 0; q < Q; ++q) {
+        uint32_t const e = first + stride * (uint32_t)q;   // < 32 G Q <= kBcTileSpan
         ent[q] = doCur ? ldm<kNc>(lc + e) : 0u;
         to[q] = doCur ? ldm<kNc>(wc + e) : 0u;
         pw[q] = doPrev ? ldm<kNc>(wp + e) : 0u;
     }
 #pragma unroll
-    for (int q = 0; q < kPerfQ; ++q) live[q] = lane + 32u * (uint32_t)q < cnt;
-    uint32_t nAcc = perform_movers<W, kPerfQ, kNc>(S, dtab, tcur, ent, to, live);
+    for (int q = 0; q < Q; ++q) live[q] = first + stride * (uint32_t)q < cnt;
+    uint32_t nAcc = perform_movers<W, Q, kNc>(S, dtab, tcur, ent, to, live);
 #pragma unroll
-    for (int q = 0; q < kPerfQ; ++q)
-        if (lane + 32u * (uint32_t)q < pcnt) tprev[pw[q] >> 6] = 0ull;
-    constexpr uint32_t kPass = 32u * kPerfQ;
-    for (uint32_t b = kPass; b < cnt; b += kPass) {
+    for (int q = 0; q < Q; ++q)
+        if (first + stride * (uint32_t)q < pcnt) tprev[pw[q] >> 6] = 0ull;
+    uint32_t const pass = stride * (uint32_t)Q;
+    for (uint32_t b = pass; b < cnt; b += pass) {
 #pragma unroll
-        for (int q = 0; q < kPerfQ; ++q) {
-            uint32_t const e = b + lane + 32u * (uint32_t)q;
+        for (int q = 0; q < Q; ++q) {
+            uint32_t const e = b + first + stride * (uint32_t)q;
             live[q] = e < cnt;
             ent[q] = live[q] ? ldm<kNc>(lc + e) : 0u;
             to[q] = live[q] ? ldm<kNc>(wc + e) : 0u;
         }
-        nAcc += perform_movers<W, kPerfQ, kNc>(S, dtab, tcur, ent, to, live);
+        nAcc += perform_movers<W, Q, kNc>(S, dtab, tcur, ent, to, live);
     }
-    for (uint32_t b = kPass; b < pcnt; b += kPass) {
+    for (uint32_t b = pass; b < pcnt; b += pass) {
 #pragma unroll
-        for (int q = 0; q < kPerfQ; ++q) {
-            uint32_t const e = b + lane + 32u * (uint32_t)q;
+        for (int q = 0; q < Q; ++q) {
+            uint32_t const e = b + first + stride * (uint32_t)q;
             if (e < pcnt) tprev[ldm<kNc>(wp + e) >> 6] = 0ull;
         }
     }
@@ -424,26 +426,34 @@ __global__ void __launch_bounds__(B, kMinBlocks) k_check_bc(const __grid_constan
     }
 }
 
-// Grid-phase perform, one warp (CTA) per tile of kBcTileSpan in-colour indices (perform_tile).
+// Grid-phase perform: groups of G warps per tile of kBcTileSpan in-colour indices (perform_tile),
+// PW warps per CTA (PW / G tiles); the groups of a CTA share nothing and never wait for each other.
 // One system: `parity` and `scope` (kPerfCur: walk this sub-step's movers, kPerfPrev: scrub the
 // previous sub-step's marks) come with the launch, so no load precedes the lists'; with parity ==
 // kParityFromEntry they come from the step entry (a launch captured once and replayed on other
-// entries). `next` != nullptr: CTA 0 also writes the following sub-step's entry there
-// (write_next_step). A tile list (kMulti): warp b takes tile tiles[b] of system tiles[b].sys, whose
-// step entry says what to do.
-template <typename W, bool kMulti>
-__global__ void __launch_bounds__(32) k_perform_bc(const __grid_constant__ SysDev S1, SysDev const* __restrict__ sysv,
-                                                   TileRef const* __restrict__ tiles,
-                                                   StepEntry const* __restrict__ steps, uint32_t parity,
-                                                   uint32_t scope, StepEntry* next)
+// entries). `next` != nullptr: the first warp of tile 0 also writes the following sub-step's entry
+// there (write_next_step). A tile list (kMulti): group b takes tile tiles[b] of system
+// tiles[b].sys, whose step entry says what to do. nTiles: tiles of the launch (groups past it leave
+// at once). Every warp of a group has 32 x (4 / G) list slots per pass.
+template <typename W, bool kMulti, int PW, int G>
+__global__ void __launch_bounds__(32 * PW) k_perform_bc(const __grid_constant__ SysDev S1, SysDev const* __restrict__ sysv,
+                                                        TileRef const* __restrict__ tiles,
+                                                        StepEntry const* __restrict__ steps, uint32_t parity,
+                                                        uint32_t scope, StepEntry* next, uint32_t nTiles)
 {
-    __shared__ SysDev Sm;
-    __shared__ __align__(16) uint32_t dtab[kDirTab];
-    uint32_t const lane = threadIdx.x;
-    uint32_t p = parity, tile = blockIdx.x;
+    static_assert(PW % G == 0 && kPerfQ % G == 0, "whole groups, whole slots per lane");
+    constexpr int Q = kPerfQ / G;
+    __shared__ SysDev Sm[kMulti ? PW : 1];
+    __shared__ __align__(16) uint32_t dtabs[PW][kDirTab];
+    uint32_t const lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    uint32_t const wt = (blockIdx.x * PW + wid) / G;   // this group's tile (single) or tile-list entry
+    uint32_t const sub = wid % G;
+    if (wt >= nTiles) return;
+    uint32_t* const dtab = dtabs[wid];
+    uint32_t p = parity, tile = wt;
     bool cur = (scope & kPerfCur) != 0u, prev = (scope & kPerfPrev) != 0u;
     if (!kMulti) {
-        if (next != nullptr && blockIdx.x == 0 && lane == 0) write_next_step(S1.gen, S1.grp, next);
+        if (next != nullptr && wt == 0 && sub == 0 && lane == 0) write_next_step(S1.gen, S1.grp, next);
         uint32_t const d0 = S1.dirTab[lane];
         uint32_t const d1 = lane + 32u < kDirTab ? S1.dirTab[lane + 32u] : 0u;
         if (parity == kParityFromEntry) {
@@ -456,22 +466,30 @@ __global__ void __launch_bounds__(32) k_perform_bc(const __grid_constant__ SysDe
         dtab[lane] = d0;
         if (lane + 32u < kDirTab) dtab[lane + 32u] = d1;
     } else {
-        TileRef const tr = tiles[blockIdx.x];
-        copy_desc(Sm, sysv + tr.sys);
+        TileRef const tr = tiles[wt];
+        SysDev& D = Sm[kMulti ? wid : 0];
+        {   // the warp copies its system's descriptor
+            static_assert(sizeof(SysDev) % 4 == 0, "SysDev is copied word by word");
+            uint32_t const* src = reinterpret_cast<uint32_t const*>(sysv + tr.sys);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&D);
+            for (uint32_t w = lane; w < sizeof(SysDev) / 4; w += 32u) dst[w] = src[w];
+        }
         StepEntry const st = steps[tr.sys];
         p = st.parity;
         tile = tr.start / kBcTileSpan;
         cur = st.color != kNoColor && tr.start < st.cnt;
         prev = st.prevColor != kNoColor && tr.start < st.pcnt;
         __syncwarp();
-        dtab[lane] = Sm.dirTab[lane];
-        if (lane + 32u < kDirTab) dtab[lane + 32u] = Sm.dirTab[lane + 32u];
+        dtab[lane] = D.dirTab[lane];
+        if (lane + 32u < kDirTab) dtab[lane + 32u] = D.dirTab[lane + 32u];
     }
     __syncwarp();
     if (!cur && !prev) return;
-    SysDev const& S = kMulti ? Sm : S1;
-    uint32_t const nAcc = __reduce_add_sync(0xffffffffu, perform_tile<W, true>(S, dtab, p, tile, cur, prev));
-    if (lane == 0) tally_flush(nAcc, S.stats, 2);
+    SysDev const& S = kMulti ? Sm[kMulti ? wid : 0] : S1;
+    uint32_t const nAcc =
+        __reduce_add_sync(0xffffffffu, perform_tile<W, true, Q>(S, dtab, p, tile, cur, prev, sub, (uint32_t)G));
+    if (lane == 0 && nAcc) atomicAdd(S.stats + 2 * kStatSlots + ((blockIdx.x * PW + wid) % kStatSlots),
+                                     (unsigned long long)nAcc);
 }
 
 // ---------------------------------------------------------------------------------- persistent
@@ -998,6 +1016,44 @@ int sm_count()
     return c;
 }
 
+// the perform's warps per CTA and per tile: BFM_PERFORM_WARPS (1, 2, 4, 8) and BFM_PERFORM_GROUP
+// (1, 2, 4; at most the warps per CTA) override the defaults
+int perform_env(char const* name, int dflt, int maxv)
+{
+    char const* e = std::getenv(name);
+    int const v = e ? std::atoi(e) : dflt;
+    return (v == 1 || v == 2 || v == 4 || v == 8) && v <= maxv ? v : dflt;
+}
+int perform_warps()
+{
+    static int const w = perform_env("BFM_PERFORM_WARPS", (int)kPerformWarpsDefault, 8);
+    return w;
+}
+int perform_group()
+{
+    static int const g = std::min(perform_env("BFM_PERFORM_GROUP", (int)kPerformGroupDefault, 4), perform_warps());
+    return g;
+}
+
+template <typename W, bool kMulti, int PW, int G>
+void launch_perform_k(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
+                      StepEntry const* dSteps, PerformArgs const& pa, cudaStream_t s)
+{
+    uint32_t const tilesPerCta = PW / G;
+    k_perform_bc<W, kMulti, PW, G><<<(nTiles + tilesPerCta - 1) / tilesPerCta, 32 * PW, 0, s>>>(
+        hostDesc, dSys, dTiles, dSteps, pa.parity, pa.scope, pa.next, nTiles);
+}
+
+template <typename W, bool kMulti, int PW>
+void launch_perform_g(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
+                      StepEntry const* dSteps, PerformArgs const& pa, cudaStream_t s)
+{
+    int const g = perform_group();
+    if (g >= 4 && PW >= 4) launch_perform_k<W, kMulti, PW, (PW >= 4 ? 4 : 1)>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s);
+    else if (g >= 2 && PW >= 2) launch_perform_k<W, kMulti, PW, (PW >= 2 ? 2 : 1)>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s);
+    else launch_perform_k<W, kMulti, PW, 1>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s);
+}
+
 template <typename W, bool kMulti, int B, int kMinCheck>
 void launch_grid_bc_k(bool check, SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles,
                       uint32_t nTiles, StepEntry const* dSteps, PerformArgs const& pa, cudaStream_t s)
@@ -1006,7 +1062,12 @@ void launch_grid_bc_k(bool check, SysDev const& hostDesc, SysDev const* dSys, Ti
         k_check_bc<W, B, kMulti, kMinCheck><<<nTiles, B, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
         return;
     }
-    k_perform_bc<W, kMulti><<<nTiles, 32, 0, s>>>(hostDesc, dSys, dTiles, dSteps, pa.parity, pa.scope, pa.next);
+    switch (perform_warps()) {
+    case 1: launch_perform_g<W, kMulti, 1>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
+    case 2: launch_perform_g<W, kMulti, 2>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
+    case 8: launch_perform_g<W, kMulti, 8>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
+    default: launch_perform_g<W, kMulti, 4>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
+    }
 }
 
 // shape: the check's register budget in resident threads per SM, 0: the compiler's choice, 1: 1536,
@@ -1153,9 +1214,6 @@ cudaError_t launch_sweep_bc_w(SysDev const& S, StepEntry const* dSteps, uint32_t
     case 0: return launch_sweep_bc_k<W, kCheckMpt, 4>(S, dSteps, nSteps, maxGroup, gs, allowCluster, s, gridOut);
     case 1: return launch_sweep_bc_k<W, kCheckMpt, 5>(S, dSteps, nSteps, maxGroup, gs, allowCluster, s, gridOut);
     case 2: return launch_sweep_bc_k<W, kCheckMpt, 6>(S, dSteps, nSteps, maxGroup, gs, allowCluster, s, gridOut);
-    // 128-thread CTAs, four monomers per thread, seven CTAs per SM: up to 7 x SMs tiles of 512
-    // monomers (a million-monomer colour group) each take a CTA of their own
-    case 3: return launch_sweep_bc_k<W, 4, 7, 128>(S, dSteps, nSteps, maxGroup, gs, allowCluster, s, gridOut);
     default: return cudaErrorInvalidValue;
     }
 }

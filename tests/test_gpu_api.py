@@ -199,6 +199,36 @@ def test_reference_adapter_over_engine_vs_oracle(build, steps, calls):
     assert np.array_equal(got, want)
 
 
+def test_stats_tickets_across_paths():
+    """Tickets taken after graph-path runs copy the counter snapshot the graph's last node took (on a
+    publishing stream of their own); after other paths they read the counters directly. Mixed,
+    back to back and repeated, every ticket equals a synchronous read after the same MCS."""
+    s = S.serpentine_chains(64, 32, 0.3, seed=5)
+    a = fresh()
+    a.load_system(s, mode=P.MODE_GRAPH)
+    b = fresh()
+    b.load_system(s, mode=P.MODE_GRAPH)
+    plan = [(P.MODE_GRAPH, 3), (P.MODE_LAUNCH, 2), (P.MODE_GRAPH, 5), (P.MODE_GRAPH, 0), (P.MODE_GRAPH, 1),
+            (P.MODE_LAUNCH, 1), (P.MODE_GRAPH, 2)]
+    tickets, done = [], []
+    total = 0
+    for mode, n in plan:
+        a.set_mode(mode)
+        if n:
+            a.run_async(n)
+        total += n
+        tickets.append(a.stats_async())
+        done.append(total)
+    got = [a.stats_wait(t) for t in tickets]
+    k = 0
+    for want_mcs, g in zip(done, got):
+        b.runSimulationOnGPU(want_mcs - k)
+        k = want_mcs
+        assert g == b.stats() and g["mcs"] == want_mcs
+    a.close()
+    b.close()
+
+
 def test_persistent_barrier_timeout_is_reported():
     """A persistent launch whose grid barrier cannot complete (injected on the host: the arrival
     count starts where no barrier's target is reached) ends at the barrier's time limit, the run
