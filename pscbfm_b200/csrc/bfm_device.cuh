@@ -169,6 +169,36 @@ __device__ __forceinline__ void write_next_step(StepGen* g, uint32_t const* grp,
     g->next = t + 1;
 }
 
+// Counter snapshots of graph replays: a device ring of kSnapRing slots of four words
+// {attempted, tentative, accepted, sequence}; `arrive` counts the CTAs of the snapshotting launch
+// that have finished, `seq` the snapshots taken so far.
+constexpr uint32_t kSnapRing = 64;
+struct SnapArgs {
+    unsigned long long* ring = nullptr;
+    unsigned long long* seq = nullptr;
+    unsigned int* arrive = nullptr;
+};
+
+// One warp: the sums of the three striped move counters into ring slot *seq % kSnapRing with the
+// sequence number *seq + 1, then ++*seq. The caller orders every counter update before it.
+__device__ __forceinline__ void snapshot_stats(unsigned long long const* stats, unsigned long long* ring,
+                                               unsigned long long* seq)
+{
+    uint32_t const lane = threadIdx.x & 31u;
+    unsigned long long const q = *seq;
+    unsigned long long* const slot = ring + 4ull * (q % kSnapRing);
+    for (uint32_t c = 0; c < 3; ++c) {
+        unsigned long long v = 0;
+        for (uint32_t k = lane; k < kStatSlots; k += 32) v += __ldcg(stats + c * kStatSlots + k);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) slot[c] = v;
+    }
+    if (lane == 0) {
+        slot[3] = q + 1;
+        *seq = q + 1;
+    }
+}
+
 // Move-direction hash, src/pscbfm/CRITICAL.cu:2-11 (Jenkins' 6-shift 32-bit integer hash).
 // The constants and shifts must stay as they are: they define the trajectory.
 __host__ __device__ __forceinline__ uint32_t move_hash(uint32_t a)

@@ -106,7 +106,7 @@ ArenaLayout arena_layout(uint32_t n, uint32_t npad, uint32_t maxc, uint32_t nwor
     // position read-back in the caller's order
     L.slotOf = take(4ull * n);
     L.xyzOut = take(12ull * n);
-    L.snap = take(8ull * (4 * kSnapRing + 1));   // counter snapshots of graph replays, then their count
+    L.snap = take(8ull * (4 * kSnapRing + 2));   // counter snapshots of graph replays, their count, arrivals
     L.bytes = off;
     return L;
 }
@@ -456,6 +456,7 @@ void Updater::initialize()
     dev_.xyzOut = reinterpret_cast<int32_t*>(base + L.xyzOut);
     dev_.snap = reinterpret_cast<unsigned long long*>(base + L.snap);
     dev_.snapSeq = dev_.snap + 4 * kSnapRing;
+    dev_.snapArrive = reinterpret_cast<unsigned int*>(dev_.snapSeq + 1);
     h.pk = reinterpret_cast<uint32_t*>(base + L.pk);
     h.code = base + L.code;
     h.nbrr = reinterpret_cast<uint32_t*>(base + L.nbrr);
@@ -516,7 +517,7 @@ void Updater::initialize()
     cuda_check(cudaMemsetAsync(dev_.dList, 0, 4, s), "memset list");
     cuda_check(cudaMemsetAsync(dev_.gs, 0, sizeof(GridSync), s), "memset grid barrier");
     cuda_check(cudaMemsetAsync(h.gen, 0, sizeof(StepGen), s), "memset step producer");   // off
-    cuda_check(cudaMemsetAsync(dev_.snap, 0, 8ull * (4 * kSnapRing + 1), s), "memset snapshots");
+    cuda_check(cudaMemsetAsync(dev_.snap, 0, 8ull * (4 * kSnapRing + 2), s), "memset snapshots");
     if (segs) {
         cuda_check(cudaMemsetAsync(h.mcount, 0, 4ull * 2 * segs, s), "memset mover counts");
         // the grid perform loads list slots past a list's end and ignores them: they start as zeros
@@ -921,9 +922,9 @@ cudaGraphExec_t Updater::graphFor(uint32_t nSteps, uint32_t parity0)
         pa.parity = (parity0 + t) & 1u;
         pa.scope = kPerfCur | kPerfPrev;   // a scrub with no marks pending only zeroes zero words
         pa.next = nSteps >= 2 ? dev_.dSteps + (t + 1) % nSteps : nullptr;
+        if (t + 1 == nSteps) pa.snap = SnapArgs{dev_.snap, dev_.snapSeq, dev_.snapArrive};   // the replay's counters
         if (err == cudaSuccess) err = launchPerform(dev_.dSteps + t, stream_, pa);
     }
-    if (err == cudaSuccess) err = launch_snapshot_stats(dev_.h.stats, dev_.snap, dev_.snapSeq, stream_);
     cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
     cuda_check(err, "capture launches");
     cuda_check(endErr, "end capture");
@@ -1003,11 +1004,11 @@ void Updater::enqueueGraph(uint32_t nSteps)
             cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         }
         cuda_check(cudaGraphLaunch(exec, stream_), "graph launch");
-        launches_ += 2ull * chunk + 1;
-        ++snapIssued_;
+        launches_ += 2ull * chunk;
+        if (codeMode_ != kCodeNone) ++snapIssued_;   // the bond-code perform takes the snapshot
         done += chunk;
     }
-    lastRunSnap_ = true;
+    lastRunSnap_ = codeMode_ != kCodeNone;
 }
 
 float Updater::runTimed(int32_t nMcs)

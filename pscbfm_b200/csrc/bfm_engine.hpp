@@ -182,6 +182,7 @@ private:
         int32_t* xyzOut = nullptr;     // [3 n] positions in the caller's order, for read-back
         unsigned long long* snap = nullptr;      // [kSnapRing][4] counter snapshots of graph replays
         unsigned long long* snapSeq = nullptr;   // snapshots taken so far
+        unsigned int* snapArrive = nullptr;      // CTAs of the snapshotting perform that have finished
     };
     void requireN(char const* who) const;
     void requireInit(char const* who) const;
@@ -242,7 +243,7 @@ private:
     unsigned long long* dStats_ = nullptr;     // hStats_ as the device addresses it
     cudaEvent_t statEv_[kStatRing] = {};
     uint64_t statTicket_[kStatRing] = {}, statMcs_[kStatRing] = {}, statNext_ = 0;
-    // every graph replay ends with a counter snapshot (k_snapshot_stats); a ticket taken right after
+    // every graph replay ends with a counter snapshot (its last perform's last CTA); a ticket taken right after
     // a graph-path run copies that snapshot into host memory on pubStream_, off the sweep's stream
     uint64_t statSeq_[kStatRing] = {};   // expected snapshot sequence of a ticket (0: direct read)
     uint64_t snapIssued_ = 0;            // graph replays enqueued (= the device's snapshot count)

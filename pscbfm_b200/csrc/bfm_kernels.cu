@@ -345,28 +345,6 @@ __global__ void k_publish_stats(unsigned long long const* __restrict__ stats, un
     }
 }
 
-// One warp, the last node of a captured sweep graph: the three counters' sums into slot
-// seq % kSnapRing of a device ring, {attempted, tentative, accepted, seq + 1}, then seq + 1 into
-// *seq. A later k_publish_snap on another stream copies the slot into host memory, so the write
-// into host memory does not hold up the sweep's stream.
-__global__ void k_snapshot_stats(unsigned long long const* __restrict__ stats, unsigned long long* __restrict__ snap,
-                                 unsigned long long* __restrict__ seq)
-{
-    uint32_t const lane = threadIdx.x;
-    unsigned long long const q = *seq;
-    unsigned long long* const slot = snap + 4ull * (q % kSnapRing);
-    for (uint32_t c = 0; c < 3; ++c) {
-        unsigned long long v = 0;
-        for (uint32_t k = lane; k < kStatSlots; k += 32) v += stats[c * kStatSlots + k];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) slot[c] = v;
-    }
-    if (lane == 0) {
-        slot[3] = q + 1;
-        *seq = q + 1;
-    }
-}
-
 // One thread: snapshot slot (4 words) into host memory (mapped), the sequence number included.
 __global__ void k_publish_snap(unsigned long long const* __restrict__ slot, unsigned long long* __restrict__ out)
 {
@@ -443,13 +421,6 @@ cudaError_t launch_gather_positions(SysDev const& h, uint32_t const* slotOf, uin
 cudaError_t launch_publish_stats(unsigned long long const* stats, unsigned long long* out, cudaStream_t s)
 {
     k_publish_stats<<<1, 32, 0, s>>>(stats, out);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_snapshot_stats(unsigned long long const* stats, unsigned long long* snap, unsigned long long* seq,
-                                  cudaStream_t s)
-{
-    k_snapshot_stats<<<1, 32, 0, s>>>(stats, snap, seq);
     return cudaGetLastError();
 }
 

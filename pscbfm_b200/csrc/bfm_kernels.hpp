@@ -64,12 +64,13 @@ cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef 
 // (several systems) always read each system's entry; parity, scope and next are ignored.
 constexpr uint32_t kParityFromEntry = 0xFFFFFFFFu;
 constexpr uint32_t kPerformWarpsDefault = 4;   // warps per CTA of the perform
-constexpr uint32_t kPerformGroupDefault = 4;   // warps per tile of the perform
+constexpr uint32_t kPerformGroupDefault = 2;   // warps per tile of the perform
 constexpr uint32_t kPerfCur = 1u, kPerfPrev = 2u;
 struct PerformArgs {
     uint32_t parity = kParityFromEntry;
     uint32_t scope = kPerfCur | kPerfPrev;
     StepEntry* next = nullptr;
+    SnapArgs snap{};   // ring != nullptr: the last CTA takes a counter snapshot (snapshot_stats)
 };
 cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
                               StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1,
@@ -121,12 +122,7 @@ cudaError_t launch_gather_positions(SysDev const& h, uint32_t const* slotOf, uin
 // Writes the sums over the kStatSlots slots of the three move counters (attempted, tentative,
 // accepted) into out[0..3), mapped pinned host memory.
 cudaError_t launch_publish_stats(unsigned long long const* stats, unsigned long long* out, cudaStream_t s);
-// The sweep graph's last node: the counters' sums into a device ring of kSnapRing slots of four
-// words ({attempted, tentative, accepted, sequence}), slot *seq % kSnapRing, and ++*seq. Then
-// k_publish_snap copies one slot into host memory on another stream.
-constexpr uint32_t kSnapRing = 64;
-cudaError_t launch_snapshot_stats(unsigned long long const* stats, unsigned long long* snap, unsigned long long* seq,
-                                  cudaStream_t s);
+// k_publish_snap copies one slot of the counter-snapshot ring (snapshot_stats) into host memory.
 cudaError_t launch_publish_snap(unsigned long long const* slot, unsigned long long* out, cudaStream_t s);
 
 }  // namespace bfm

@@ -199,15 +199,17 @@ def test_reference_adapter_over_engine_vs_oracle(build, steps, calls):
     assert np.array_equal(got, want)
 
 
-def test_stats_tickets_across_paths():
-    """Tickets taken after graph-path runs copy the counter snapshot the graph's last node took (on a
-    publishing stream of their own); after other paths they read the counters directly. Mixed,
-    back to back and repeated, every ticket equals a synchronous read after the same MCS."""
+@pytest.mark.parametrize("repr_", [P.REPR_AUTO, P.REPR_GATHER])
+def test_stats_tickets_across_paths(repr_):
+    """Tickets taken after bond-code graph-path runs copy the counter snapshot the graph's last
+    perform took (on a publishing stream of their own); after other paths, and on the gather
+    representation, they read the counters directly. Mixed, back to back and repeated, every ticket
+    equals a synchronous read after the same MCS."""
     s = S.serpentine_chains(64, 32, 0.3, seed=5)
     a = fresh()
-    a.load_system(s, mode=P.MODE_GRAPH)
+    a.load_system(s, mode=P.MODE_GRAPH, representation=repr_)
     b = fresh()
-    b.load_system(s, mode=P.MODE_GRAPH)
+    b.load_system(s, mode=P.MODE_GRAPH, representation=repr_)
     plan = [(P.MODE_GRAPH, 3), (P.MODE_LAUNCH, 2), (P.MODE_GRAPH, 5), (P.MODE_GRAPH, 0), (P.MODE_GRAPH, 1),
             (P.MODE_LAUNCH, 1), (P.MODE_GRAPH, 2)]
     tickets, done = [], []
