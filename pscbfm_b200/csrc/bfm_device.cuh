@@ -184,14 +184,18 @@ struct SnapArgs {
 __device__ __forceinline__ void snapshot_stats(unsigned long long const* stats, unsigned long long* ring,
                                                unsigned long long* seq)
 {
+    static_assert(kStatSlots == 64, "two slots per lane and counter");
     uint32_t const lane = threadIdx.x & 31u;
     unsigned long long const q = *seq;
     unsigned long long* const slot = ring + 4ull * (q % kSnapRing);
+    unsigned long long v[3];
+#pragma unroll
+    for (uint32_t c = 0; c < 3; ++c)   // the six loads go out together
+        v[c] = __ldcg(stats + c * kStatSlots + lane) + __ldcg(stats + c * kStatSlots + 32 + lane);
+#pragma unroll
     for (uint32_t c = 0; c < 3; ++c) {
-        unsigned long long v = 0;
-        for (uint32_t k = lane; k < kStatSlots; k += 32) v += __ldcg(stats + c * kStatSlots + k);
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) slot[c] = v;
+        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+        if (lane == 0) slot[c] = v[c];
     }
     if (lane == 0) {
         slot[3] = q + 1;

@@ -64,7 +64,7 @@ cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef 
 // (several systems) always read each system's entry; parity, scope and next are ignored.
 constexpr uint32_t kParityFromEntry = 0xFFFFFFFFu;
 constexpr uint32_t kPerformWarpsDefault = 4;   // warps per CTA of the perform
-constexpr uint32_t kPerformGroupDefault = 2;   // warps per tile of the perform
+constexpr uint32_t kPerformGroupDefault = 4;   // warps per tile of the perform
 constexpr uint32_t kPerfCur = 1u, kPerfPrev = 2u;
 struct PerformArgs {
     uint32_t parity = kParityFromEntry;
