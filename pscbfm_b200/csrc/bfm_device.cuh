@@ -148,10 +148,10 @@ struct StepGen {
 };
 static_assert(sizeof(StepGen) == sizeof(StepEntry), "StepGen takes one entry slot before the entries");
 
-// Written by one thread: the entry of sub-step g->next into *out (see StepGen).
-__device__ __forceinline__ void write_next_step(StepGen* g, uint32_t const* grp, StepEntry* out)
+// Written by one thread: the entry of sub-step g->next into *out (see StepGen). s: *g as the
+// caller loaded it (ahead of other work, so that its latency overlaps that work).
+__device__ __forceinline__ void write_next_step(StepGen* g, StepGen const& s, uint32_t const* grp, StepEntry* out)
 {
-    StepGen const s = *g;
     if (!s.on) return;
     uint64_t const t = s.next;
     uint32_t const c = counter_draw(s.seed, 2 * t) % s.nColors;

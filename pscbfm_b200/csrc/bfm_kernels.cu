@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(kGridBlock) k_perform(SysDev const* __restrict
     if (threadIdx.x == 0) tally = 0;
     __syncthreads();
     // one system in a captured graph: hand the next launch its entry (write_next_step)
-    if (next != nullptr && blockIdx.x == 0 && threadIdx.x == 0) write_next_step(S.gen, S.grp, next);
+    if (next != nullptr && blockIdx.x == 0 && threadIdx.x == 0) write_next_step(S.gen, *S.gen, S.grp, next);
 
     // scrub the marks of the previous sub-step of this system (other parity)
     if (st.prevColor != kNoColor) {

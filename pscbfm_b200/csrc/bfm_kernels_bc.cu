@@ -456,9 +456,13 @@ __global__ void __launch_bounds__(32 * PW) k_perform_bc(const __grid_constant__ 
     uint32_t* const dtab = dtabs[wid];
     uint32_t p = parity, tile = wt;
     bool cur = inRange && (scope & kPerfCur) != 0u, prev = inRange && (scope & kPerfPrev) != 0u;
+    // the next sub-step's entry (write_next_step): the producer's state is loaded now, the entry
+    // made and stored after this warp's share of the tile
+    bool const writer = !kMulti && next != nullptr && wt == 0 && sub == 0 && lane == 0;
+    StepGen gen{};
+    if (writer) gen = *S1.gen;
     if (inRange) {
         if (!kMulti) {
-            if (next != nullptr && wt == 0 && sub == 0 && lane == 0) write_next_step(S1.gen, S1.grp, next);
             uint32_t const d0 = S1.dirTab[lane];
             uint32_t const d1 = lane + 32u < kDirTab ? S1.dirTab[lane + 32u] : 0u;
             if (parity == kParityFromEntry) {
@@ -497,6 +501,7 @@ __global__ void __launch_bounds__(32 * PW) k_perform_bc(const __grid_constant__ 
         if (lane == 0 && nAcc)
             atomicAdd(S.stats + 2 * kStatSlots + ((blockIdx.x * PW + wid) % kStatSlots), (unsigned long long)nAcc);
     }
+    if (writer) write_next_step(S1.gen, gen, S1.grp, next);
     if (kMulti || snap.ring == nullptr) return;
     // the counter snapshot: every CTA counts its arrival after its counter updates; the last one
     // sums the counters (every earlier CTA's updates are visible to it)
