@@ -170,14 +170,8 @@ __device__ __forceinline__ void write_next_step(StepGen* g, StepGen const& s, ui
 }
 
 // Counter snapshots of graph replays: a device ring of kSnapRing slots of four words
-// {attempted, tentative, accepted, sequence}; `arrive` counts the CTAs of the snapshotting launch
-// that have finished, `seq` the snapshots taken so far.
+// {attempted, tentative, accepted, sequence}; `seq` counts the snapshots taken so far.
 constexpr uint32_t kSnapRing = 64;
-struct SnapArgs {
-    unsigned long long* ring = nullptr;
-    unsigned long long* seq = nullptr;
-    unsigned int* arrive = nullptr;
-};
 
 // One warp: the sums of the three striped move counters into ring slot *seq % kSnapRing with the
 // sequence number *seq + 1, then ++*seq. The caller orders every counter update before it.

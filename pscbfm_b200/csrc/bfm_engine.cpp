@@ -106,7 +106,7 @@ ArenaLayout arena_layout(uint32_t n, uint32_t npad, uint32_t maxc, uint32_t nwor
     // position read-back in the caller's order
     L.slotOf = take(4ull * n);
     L.xyzOut = take(12ull * n);
-    L.snap = take(8ull * (4 * kSnapRing + 2));   // counter snapshots of graph replays, their count, arrivals
+    L.snap = take(8ull * (4 * kSnapRing + 1));   // counter snapshots of graph replays, then their count
     L.bytes = off;
     return L;
 }
@@ -456,7 +456,6 @@ void Updater::initialize()
     dev_.xyzOut = reinterpret_cast<int32_t*>(base + L.xyzOut);
     dev_.snap = reinterpret_cast<unsigned long long*>(base + L.snap);
     dev_.snapSeq = dev_.snap + 4 * kSnapRing;
-    dev_.snapArrive = reinterpret_cast<unsigned int*>(dev_.snapSeq + 1);
     h.pk = reinterpret_cast<uint32_t*>(base + L.pk);
     h.code = base + L.code;
     h.nbrr = reinterpret_cast<uint32_t*>(base + L.nbrr);
@@ -517,7 +516,7 @@ void Updater::initialize()
     cuda_check(cudaMemsetAsync(dev_.dList, 0, 4, s), "memset list");
     cuda_check(cudaMemsetAsync(dev_.gs, 0, sizeof(GridSync), s), "memset grid barrier");
     cuda_check(cudaMemsetAsync(h.gen, 0, sizeof(StepGen), s), "memset step producer");   // off
-    cuda_check(cudaMemsetAsync(dev_.snap, 0, 8ull * (4 * kSnapRing + 2), s), "memset snapshots");
+    cuda_check(cudaMemsetAsync(dev_.snap, 0, 8ull * (4 * kSnapRing + 1), s), "memset snapshots");
     if (segs) {
         cuda_check(cudaMemsetAsync(h.mcount, 0, 4ull * 2 * segs, s), "memset mover counts");
         // the grid perform loads list slots past a list's end and ignores them: they start as zeros
@@ -537,6 +536,7 @@ void Updater::initialize()
     genOn_ = 0;
     snapIssued_ = 0;
     lastRunSnap_ = false;
+    snapMode_ = false;
 }
 
 void Updater::hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, std::vector<uint32_t>& nbrr) const
@@ -905,10 +905,10 @@ void Updater::enqueueLaunch(uint32_t nSteps)
     }
 }
 
-cudaGraphExec_t Updater::graphFor(uint32_t nSteps, uint32_t parity0)
+cudaGraphExec_t Updater::graphFor(uint32_t nSteps, uint32_t parity0, bool snap)
 {
     for (auto const& g : graphs_)
-        if (g.nSteps == nSteps && g.parity0 == parity0) return g.exec;
+        if (g.nSteps == nSteps && g.parity0 == parity0 && g.snap == snap) return g.exec;
     // node t performs the sub-step whose entry sits in slot t and, in a graph of two or more
     // sub-steps, writes the entry of the next one into slot t + 1 (the last node into slot 0,
     // where the next replay starts) when the device producer is on; the perform's parity is a
@@ -922,9 +922,10 @@ cudaGraphExec_t Updater::graphFor(uint32_t nSteps, uint32_t parity0)
         pa.parity = (parity0 + t) & 1u;
         pa.scope = kPerfCur | kPerfPrev;   // a scrub with no marks pending only zeroes zero words
         pa.next = nSteps >= 2 ? dev_.dSteps + (t + 1) % nSteps : nullptr;
-        if (t + 1 == nSteps) pa.snap = SnapArgs{dev_.snap, dev_.snapSeq, dev_.snapArrive};   // the replay's counters
         if (err == cudaSuccess) err = launchPerform(dev_.dSteps + t, stream_, pa);
     }
+    // once the counters are read by ticket, every replay ends with their snapshot
+    if (snap && err == cudaSuccess) err = launch_snapshot_stats(dev_.h.stats, dev_.snap, dev_.snapSeq, stream_);
     cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
     cuda_check(err, "capture launches");
     cuda_check(endErr, "end capture");
@@ -932,7 +933,7 @@ cudaGraphExec_t Updater::graphFor(uint32_t nSteps, uint32_t parity0)
     cudaError_t const instErr = cudaGraphInstantiate(&exec, g, 0);
     cudaGraphDestroy(g);
     cuda_check(instErr, "graph instantiate");
-    graphs_.push_back({nSteps, parity0, exec});
+    graphs_.push_back({nSteps, parity0, snap, exec});
     return exec;
 }
 
@@ -942,8 +943,8 @@ void Updater::prepareGraphs(uint32_t nSteps)
     // full chunks start at no more than two parities, then the tail
     uint32_t const G = std::min(kGraphMcs * (uint32_t)grpSize_.size(), hStepCap_);
     uint32_t const full = nSteps / G, rest = nSteps % G;
-    for (uint32_t k = 0; k < full && k < 2; ++k) graphFor(G, (uint32_t)((subStep_ + (uint64_t)k * G) & 1u));
-    if (rest) graphFor(rest, (uint32_t)((subStep_ + (uint64_t)full * G) & 1u));
+    for (uint32_t k = 0; k < full && k < 2; ++k) graphFor(G, (uint32_t)((subStep_ + (uint64_t)k * G) & 1u), snapMode_);
+    if (rest) graphFor(rest, (uint32_t)((subStep_ + (uint64_t)full * G) & 1u), snapMode_);
 }
 
 void Updater::seedChain(cudaStream_t s)
@@ -981,7 +982,7 @@ void Updater::enqueueGraph(uint32_t nSteps)
     uint32_t const G = std::min(kGraphMcs * nC, hStepCap_);
     for (uint32_t done = 0; done < nSteps;) {
         uint32_t const chunk = std::min(G, nSteps - done);
-        cudaGraphExec_t const exec = graphFor(chunk, (uint32_t)(subStep_ & 1u));
+        cudaGraphExec_t const exec = graphFor(chunk, (uint32_t)(subStep_ & 1u), snapMode_);
         if (drawKind_ == kDrawCounter && chunk >= 2) {
             uint32_t todo = chunk;
             if (!(chainValid_ && chainSub_ == subStep_ && chainPrev_ == lastColor_ && chainSeed_ == drawSeed_)) {
@@ -1004,11 +1005,11 @@ void Updater::enqueueGraph(uint32_t nSteps)
             cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         }
         cuda_check(cudaGraphLaunch(exec, stream_), "graph launch");
-        launches_ += 2ull * chunk;
-        if (codeMode_ != kCodeNone) ++snapIssued_;   // the bond-code perform takes the snapshot
+        launches_ += 2ull * chunk + (snapMode_ ? 1u : 0u);
+        if (snapMode_) ++snapIssued_;
         done += chunk;
     }
-    lastRunSnap_ = codeMode_ != kCodeNone;
+    lastRunSnap_ = snapMode_;
 }
 
 float Updater::runTimed(int32_t nMcs)
@@ -1432,6 +1433,8 @@ uint64_t Updater::statsEnqueue()
         cuda_check(launch_publish_stats(dev_.h.stats, dStatRing_ + 4ull * k, stream_), "stats");
         cuda_check(cudaEventRecord(statEv_[k], stream_), "event");
         statSeq_[k] = 0;
+        // this handle's counters are read by ticket: later graph-path runs end with a snapshot
+        snapMode_ = true;
     }
     d2hBytes_ += 3 * sizeof(unsigned long long);   // written into mapped host memory
     statTicket_[k] = t;

@@ -182,7 +182,6 @@ private:
         int32_t* xyzOut = nullptr;     // [3 n] positions in the caller's order, for read-back
         unsigned long long* snap = nullptr;      // [kSnapRing][4] counter snapshots of graph replays
         unsigned long long* snapSeq = nullptr;   // snapshots taken so far
-        unsigned int* snapArrive = nullptr;      // CTAs of the snapshotting perform that have finished
     };
     void requireN(char const* who) const;
     void requireInit(char const* who) const;
@@ -243,11 +242,13 @@ private:
     unsigned long long* dStats_ = nullptr;     // hStats_ as the device addresses it
     cudaEvent_t statEv_[kStatRing] = {};
     uint64_t statTicket_[kStatRing] = {}, statMcs_[kStatRing] = {}, statNext_ = 0;
-    // every graph replay ends with a counter snapshot (its last perform's last CTA); a ticket taken right after
+    // once a ticket has been taken, every graph replay ends with a counter snapshot
+    // (k_snapshot_stats, snapMode_); a ticket taken right after
     // a graph-path run copies that snapshot into host memory on pubStream_, off the sweep's stream
     uint64_t statSeq_[kStatRing] = {};   // expected snapshot sequence of a ticket (0: direct read)
     uint64_t snapIssued_ = 0;            // graph replays enqueued (= the device's snapshot count)
-    bool lastRunSnap_ = false;           // the last work changing the counters was a graph replay
+    bool lastRunSnap_ = false;           // the last work changing the counters was a snapshotting replay
+    bool snapMode_ = false;              // the graphs end with a counter snapshot
     cudaStream_t pubStream_ = nullptr;
     cudaEvent_t pubEv_ = nullptr;
     bool gsPending_ = false;                   // hGs_ is being refreshed by the stream
@@ -260,6 +261,7 @@ private:
     uint32_t hStepCap_ = 0;
     struct GraphExec {
         uint32_t nSteps, parity0;               // chunk length, parity of its first sub-step
+        bool snap;                              // ends with a counter snapshot
         cudaGraphExec_t exec;
     };
     std::vector<GraphExec> graphs_;
@@ -276,7 +278,7 @@ private:
     long long* dObsOut_ = nullptr;
     void buildObservables();
     std::vector<uint32_t> moleculeRoots() const;   // lowest monomer id of each monomer's molecule
-    cudaGraphExec_t graphFor(uint32_t nSteps, uint32_t parity0);
+    cudaGraphExec_t graphFor(uint32_t nSteps, uint32_t parity0, bool snap);
     void seedChain(cudaStream_t s);           // the device chain restarts at the host's position
     void producerOff(cudaStream_t s);         // the device producer stops writing entries
     int effectiveMode() const;                // the path run() takes (mode_ with AUTO resolved)

@@ -345,6 +345,12 @@ __global__ void k_publish_stats(unsigned long long const* __restrict__ stats, un
     }
 }
 
+__global__ void k_snapshot_stats(unsigned long long const* __restrict__ stats, unsigned long long* ring,
+                                 unsigned long long* seq)
+{
+    snapshot_stats(stats, ring, seq);
+}
+
 // One thread: snapshot slot (4 words) into host memory (mapped), the sequence number included.
 __global__ void k_publish_snap(unsigned long long const* __restrict__ slot, unsigned long long* __restrict__ out)
 {
@@ -421,6 +427,13 @@ cudaError_t launch_gather_positions(SysDev const& h, uint32_t const* slotOf, uin
 cudaError_t launch_publish_stats(unsigned long long const* stats, unsigned long long* out, cudaStream_t s)
 {
     k_publish_stats<<<1, 32, 0, s>>>(stats, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_snapshot_stats(unsigned long long const* stats, unsigned long long* ring, unsigned long long* seq,
+                                  cudaStream_t s)
+{
+    k_snapshot_stats<<<1, 32, 0, s>>>(stats, ring, seq);
     return cudaGetLastError();
 }
 

@@ -70,7 +70,6 @@ struct PerformArgs {
     uint32_t parity = kParityFromEntry;
     uint32_t scope = kPerfCur | kPerfPrev;
     StepEntry* next = nullptr;
-    SnapArgs snap{};   // ring != nullptr: the last CTA takes a counter snapshot (snapshot_stats)
 };
 cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
                               StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1,
@@ -122,7 +121,11 @@ cudaError_t launch_gather_positions(SysDev const& h, uint32_t const* slotOf, uin
 // Writes the sums over the kStatSlots slots of the three move counters (attempted, tentative,
 // accepted) into out[0..3), mapped pinned host memory.
 cudaError_t launch_publish_stats(unsigned long long const* stats, unsigned long long* out, cudaStream_t s);
-// k_publish_snap copies one slot of the counter-snapshot ring (snapshot_stats) into host memory.
+// A counter snapshot (snapshot_stats) as a one-warp launch: a captured sweep graph's last node
+// when its handle's counters are read by ticket; k_publish_snap copies one slot of the snapshot
+// ring into host memory, on another stream.
+cudaError_t launch_snapshot_stats(unsigned long long const* stats, unsigned long long* ring, unsigned long long* seq,
+                                  cudaStream_t s);
 cudaError_t launch_publish_snap(unsigned long long const* slot, unsigned long long* out, cudaStream_t s);
 
 }  // namespace bfm

@@ -427,73 +427,66 @@ __global__ void __launch_bounds__(B, kMinBlocks) k_check_bc(const __grid_constan
 }
 
 // Grid-phase perform: groups of G warps per tile of kBcTileSpan in-colour indices (perform_tile),
-// PW warps per CTA (PW / G tiles); the groups of a CTA share nothing and never wait for each other
-// during the walk. One system: `parity` and `scope` (kPerfCur: walk this sub-step's movers,
-// kPerfPrev: scrub the previous sub-step's marks) come with the launch, so no load precedes the
-// lists'; with parity == kParityFromEntry they come from the step entry (a launch captured once and
-// replayed on other entries). `next` != nullptr: the first warp of tile 0 also writes the following
-// sub-step's entry there (write_next_step). `snap` != nullptr (one system, the last perform of a
-// captured graph): the last CTA to finish sums the move counters into the snapshot ring
-// (snapshot_stats). A tile list (kMulti): group b takes tile tiles[b] of system tiles[b].sys, whose
-// step entry says what to do. nTiles: tiles of the launch. Every warp of a group has 32 x (4 / G)
-// list slots per pass.
+// PW warps per CTA (PW / G tiles); the groups of a CTA share nothing and never wait for each other.
+// One system: `parity` and `scope` (kPerfCur: walk this sub-step's movers, kPerfPrev: scrub the
+// previous sub-step's marks) come with the launch, so no load precedes the lists'; with parity ==
+// kParityFromEntry they come from the step entry (a launch captured once and replayed on other
+// entries). `next` != nullptr: the first warp of tile 0 also writes the following sub-step's entry
+// there (write_next_step; the producer's state is loaded first, the entry stored after the warp's
+// share of the tile). A tile list (kMulti): group b takes tile tiles[b] of system tiles[b].sys,
+// whose step entry says what to do. nTiles: tiles of the launch (groups past it leave at once).
+// Every warp of a group has 32 x (4 / G) list slots per pass.
 template <typename W, bool kMulti, int PW, int G>
 __global__ void __launch_bounds__(32 * PW) k_perform_bc(const __grid_constant__ SysDev S1, SysDev const* __restrict__ sysv,
                                                         TileRef const* __restrict__ tiles,
                                                         StepEntry const* __restrict__ steps, uint32_t parity,
-                                                        uint32_t scope, StepEntry* next, uint32_t nTiles,
-                                                        SnapArgs snap)
+                                                        uint32_t scope, StepEntry* next, uint32_t nTiles)
 {
     static_assert(PW % G == 0 && kPerfQ % G == 0, "whole groups, whole slots per lane");
     constexpr int Q = kPerfQ / G;
     __shared__ SysDev Sm[kMulti ? PW : 1];
     __shared__ __align__(16) uint32_t dtabs[PW][kDirTab];
-    __shared__ uint32_t lastCta;
     uint32_t const lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
     uint32_t const wt = (blockIdx.x * PW + wid) / G;   // this group's tile (single) or tile-list entry
     uint32_t const sub = wid % G;
-    bool const inRange = wt < nTiles;
-    uint32_t* const dtab = dtabs[wid];
-    uint32_t p = parity, tile = wt;
-    bool cur = inRange && (scope & kPerfCur) != 0u, prev = inRange && (scope & kPerfPrev) != 0u;
-    // the next sub-step's entry (write_next_step): the producer's state is loaded now, the entry
-    // made and stored after this warp's share of the tile
+    if (wt >= nTiles) return;
     bool const writer = !kMulti && next != nullptr && wt == 0 && sub == 0 && lane == 0;
     StepGen gen{};
     if (writer) gen = *S1.gen;
-    if (inRange) {
-        if (!kMulti) {
-            uint32_t const d0 = S1.dirTab[lane];
-            uint32_t const d1 = lane + 32u < kDirTab ? S1.dirTab[lane + 32u] : 0u;
-            if (parity == kParityFromEntry) {
-                StepEntry const st = steps[0];
-                uint32_t const start = tile * kBcTileSpan;
-                p = st.parity;
-                cur = st.color != kNoColor && start < st.cnt;
-                prev = st.prevColor != kNoColor && start < st.pcnt;
-            }
-            dtab[lane] = d0;
-            if (lane + 32u < kDirTab) dtab[lane + 32u] = d1;
-        } else {
-            TileRef const tr = tiles[wt];
-            SysDev& D = Sm[kMulti ? wid : 0];
-            {   // the warp copies its system's descriptor
-                static_assert(sizeof(SysDev) % 4 == 0, "SysDev is copied word by word");
-                uint32_t const* src = reinterpret_cast<uint32_t const*>(sysv + tr.sys);
-                uint32_t* dst = reinterpret_cast<uint32_t*>(&D);
-                for (uint32_t w = lane; w < sizeof(SysDev) / 4; w += 32u) dst[w] = src[w];
-            }
-            StepEntry const st = steps[tr.sys];
+    uint32_t* const dtab = dtabs[wid];
+    uint32_t p = parity, tile = wt;
+    bool cur = (scope & kPerfCur) != 0u, prev = (scope & kPerfPrev) != 0u;
+    if (!kMulti) {
+        uint32_t const d0 = S1.dirTab[lane];
+        uint32_t const d1 = lane + 32u < kDirTab ? S1.dirTab[lane + 32u] : 0u;
+        if (parity == kParityFromEntry) {
+            StepEntry const st = steps[0];
+            uint32_t const start = tile * kBcTileSpan;
             p = st.parity;
-            tile = tr.start / kBcTileSpan;
-            cur = st.color != kNoColor && tr.start < st.cnt;
-            prev = st.prevColor != kNoColor && tr.start < st.pcnt;
-            __syncwarp();
-            dtab[lane] = D.dirTab[lane];
-            if (lane + 32u < kDirTab) dtab[lane + 32u] = D.dirTab[lane + 32u];
+            cur = st.color != kNoColor && start < st.cnt;
+            prev = st.prevColor != kNoColor && start < st.pcnt;
         }
+        dtab[lane] = d0;
+        if (lane + 32u < kDirTab) dtab[lane + 32u] = d1;
+    } else {
+        TileRef const tr = tiles[wt];
+        SysDev& D = Sm[kMulti ? wid : 0];
+        {   // the warp copies its system's descriptor
+            static_assert(sizeof(SysDev) % 4 == 0, "SysDev is copied word by word");
+            uint32_t const* src = reinterpret_cast<uint32_t const*>(sysv + tr.sys);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&D);
+            for (uint32_t w = lane; w < sizeof(SysDev) / 4; w += 32u) dst[w] = src[w];
+        }
+        StepEntry const st = steps[tr.sys];
+        p = st.parity;
+        tile = tr.start / kBcTileSpan;
+        cur = st.color != kNoColor && tr.start < st.cnt;
+        prev = st.prevColor != kNoColor && tr.start < st.pcnt;
         __syncwarp();
+        dtab[lane] = D.dirTab[lane];
+        if (lane + 32u < kDirTab) dtab[lane + 32u] = D.dirTab[lane + 32u];
     }
+    __syncwarp();
     if (cur || prev) {
         SysDev const& S = kMulti ? Sm[kMulti ? wid : 0] : S1;
         uint32_t const nAcc =
@@ -502,20 +495,6 @@ __global__ void __launch_bounds__(32 * PW) k_perform_bc(const __grid_constant__ 
             atomicAdd(S.stats + 2 * kStatSlots + ((blockIdx.x * PW + wid) % kStatSlots), (unsigned long long)nAcc);
     }
     if (writer) write_next_step(S1.gen, gen, S1.grp, next);
-    if (kMulti || snap.ring == nullptr) return;
-    // the counter snapshot: every CTA counts its arrival after its counter updates; the last one
-    // sums the counters (every earlier CTA's updates are visible to it)
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        lastCta = atomicAdd(snap.arrive, 1u) == gridDim.x - 1u ? 1u : 0u;
-    }
-    __syncthreads();
-    if (lastCta && wid == 0) {
-        __threadfence();
-        snapshot_stats(S1.stats, snap.ring, snap.seq);
-        if (lane == 0) *snap.arrive = 0u;
-    }
 }
 
 // ---------------------------------------------------------------------------------- persistent
@@ -1067,7 +1046,7 @@ void launch_perform_k(SysDev const& hostDesc, SysDev const* dSys, TileRef const*
 {
     uint32_t const tilesPerCta = PW / G;
     k_perform_bc<W, kMulti, PW, G><<<(nTiles + tilesPerCta - 1) / tilesPerCta, 32 * PW, 0, s>>>(
-        hostDesc, dSys, dTiles, dSteps, pa.parity, pa.scope, pa.next, nTiles, pa.snap);
+        hostDesc, dSys, dTiles, dSteps, pa.parity, pa.scope, pa.next, nTiles);
 }
 
 template <typename W, bool kMulti, int PW>
