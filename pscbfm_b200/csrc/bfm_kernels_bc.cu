@@ -87,7 +87,7 @@ constexpr int kPerfQ = 4;
 
 template <typename W, int MPT, bool kNc = true>
 __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab, StepEntry const& st, uint32_t start,
-                                           uint32_t* segCount)
+                                           uint32_t* segCount, uint2* stage)
 {
     uint32_t const B = blockDim.x, tid = threadIdx.x;
     uint32_t const* const PK = S.pk;
@@ -110,46 +110,48 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
         code[q] = a ? ldm<kNc>(CODE + st.off + i) : W(0);
     }
     __syncthreads();
-    // stage 2: direction, walls, bonds, front-plane words; the target's address replaces the
-    // monomer's
-    uint32_t dir[MPT];
-    bool ok[MPT];
-    Plane pl[MPT];
+    // stage 2: direction, walls, bonds; the monomers that pass go to this warp's part of the
+    // stage (address, slot | direction << 27), packed, so that the front-plane and occupancy work
+    // below runs on full warps of candidates only (about half the monomers fail here)
+    uint32_t const lane = tid & 31u;
+    uint32_t const lanesBelow = (1u << lane) - 1u;
+    uint2* const ws = stage + (tid >> 5) * (32u * MPT);
+    uint32_t n = 0;
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
         uint32_t const i = start + tid + (uint32_t)q * B;
-        dir[q] = move_dir(i, st.seed);
-        DirParams const D = dir_params(dtab, dir[q]);
-        ok[q] = i < st.cnt && (pk[q] & D.ma) != D.wall && bonds_ok<W, false>(code[q], dir[q], S.moveOk);
-        front_plane<false>(pl[q], S.planeTab, D, pk[q], D.front, dir[q]);
-        pk[q] = addr_add(pk[q], D.ma, D.step);
+        uint32_t const dir = move_dir(i, st.seed);
+        DirParams const D = dir_params(dtab, dir);
+        bool const ok = i < st.cnt && (pk[q] & D.ma) != D.wall && bonds_ok<W, false>(code[q], dir, S.moveOk);
+        uint32_t const bal = __ballot_sync(0xffffffffu, ok);
+        if (ok) ws[n + __popc(bal & lanesBelow)] = make_uint2(pk[q], (st.off + i) | (dir << 27));
+        n += (uint32_t)__popc(bal);
     }
-    // stage 3: occupancy words
-    unsigned long long hit[MPT];
-#pragma unroll
-    for (int q = 0; q < MPT; ++q) {
-        hit[q] = 0ull;
+    __syncwarp();
+    // stage 3: per candidate, the front plane from its address, the occupancy words, and for a
+    // free plane the mark and the list entries (one shared-memory atomic per warp and pass)
+    for (uint32_t b = 0; b < n; b += 32u) {
+        bool const live = b + lane < n;
+        uint2 const it = live ? ws[b + lane] : make_uint2(0u, 0u);
+        uint32_t const dir = it.y >> 27;   // 0 for a dead lane: table reads stay in range
+        DirParams const D = dir_params(dtab, dir);
+        Plane pl;
+        front_plane<false>(pl, S.planeTab, D, it.x, D.front, dir);
+        uint32_t const to = addr_add(it.x, D.ma, D.step);
+        unsigned long long hit = 0ull;
 #pragma unroll
         for (int r = 0; r < 4; ++r)
-            if (ok[q] && ((pl[q].touch >> r) & 1u)) hit[q] |= ldm<kNc>(S.lat + pl[q].w[r]) & pl[q].m[r];
-    }
-    // stage 4: decisions; tentative movers go to this tile's list segment (one shared-memory
-    // atomic per warp reserves the warp's slots)
-    uint32_t const lane = tid & 31u;
-#pragma unroll
-    for (int q = 0; q < MPT; ++q) {
-        uint32_t const i = start + tid + (uint32_t)q * B;
-        bool const go = ok[q] && hit[q] == 0ull;
+            if (live && ((pl.touch >> r) & 1u)) hit |= ldm<kNc>(S.lat + pl.w[r]) & pl.m[r];
+        bool const go = live && hit == 0ull;
         uint32_t const bal = __ballot_sync(0xffffffffu, go);
         uint32_t base = 0;
         if (lane == 0 && bal) base = atomicAdd(segCount, (uint32_t)__popc(bal));
         base = __shfl_sync(0xffffffffu, base, 0);
         if (go) {
-            uint32_t const w = pk[q] >> 6;
-            atomicOr(tcur + w, 1ull << (pk[q] & 63u));
-            uint32_t const slot = base + __popc(bal & ((1u << lane) - 1u));
-            lcur[slot] = (st.off + i) | (dir[q] << 27);
-            wcur[slot] = pk[q];
+            atomicOr(tcur + (to >> 6), 1ull << (to & 63u));
+            uint32_t const slot = base + __popc(bal & lanesBelow);
+            lcur[slot] = it.y;
+            wcur[slot] = to;
         }
     }
 }
@@ -415,9 +417,10 @@ __global__ void __launch_bounds__(B, kMinBlocks) k_check_bc(const __grid_constan
     }
     SysDev const& S = kMulti ? Sm : S1;
     __shared__ uint32_t segCount;
+    __shared__ uint2 stage[kBcTileSpan];   // the warps' candidates (check_body)
     if (threadIdx.x < kDirTab) dtab[threadIdx.x] = dv;
     if (threadIdx.x == 0) segCount = 0;
-    check_body<W, MPT>(S, dtab, st, start, &segCount);   // publishes both with its first barrier
+    check_body<W, MPT>(S, dtab, st, start, &segCount, stage);   // publishes both with its first barrier
     __syncthreads();
     if (threadIdx.x == 0 && st.color != kNoColor) {
         S.mcount[(size_t)st.parity * S.countStride + start / kBcTileSpan] = segCount;
@@ -581,6 +584,7 @@ __global__ void __launch_bounds__(B, kMinBlocks)
     static_assert(B * MPT == (int)kBcTileSpan, "a tile is one list segment");
     __shared__ __align__(16) uint32_t dtab[kDirTab];
     __shared__ uint32_t tallyT, tallyA, okSm, segCount, pre[4];
+    __shared__ uint2 stage[kBcTileSpan];   // the warps' candidates (check_body)
     if (ld_acquire_gpu(&gs->fault) != 0u) return;   // an earlier launch failed: the state is not usable
     if (threadIdx.x < kDirTab) dtab[threadIdx.x] = S.dirTab[threadIdx.x];
     if (threadIdx.x == 0) {
@@ -600,7 +604,7 @@ __global__ void __launch_bounds__(B, kMinBlocks)
             uint32_t const start = k * span;
             if (!active || start >= st.cnt) break;
             if (threadIdx.x == 0) segCount = 0u;   // published by check_body's first barrier
-            check_body<W, MPT, false>(S, dtab, st, start, &segCount);
+            check_body<W, MPT, false>(S, dtab, st, start, &segCount, stage);
             __syncthreads();
             if (threadIdx.x == 0) {
                 S.mcount[(size_t)st.parity * S.countStride + k] = segCount;
