@@ -438,15 +438,15 @@ __global__ void __launch_bounds__(B, kMinBlocks) k_check_bc(const __grid_constan
 // there (write_next_step; the producer's state is loaded first, the entry stored after the warp's
 // share of the tile). A tile list (kMulti): group b takes tile tiles[b] of system tiles[b].sys,
 // whose step entry says what to do. nTiles: tiles of the launch (groups past it leave at once).
-// Every warp of a group has 32 x (4 / G) list slots per pass.
+// Every warp of a group has 32 x max(4 / G, 1) list slots per pass.
 template <typename W, bool kMulti, int PW, int G>
 __global__ void __launch_bounds__(32 * PW) k_perform_bc(const __grid_constant__ SysDev S1, SysDev const* __restrict__ sysv,
                                                         TileRef const* __restrict__ tiles,
                                                         StepEntry const* __restrict__ steps, uint32_t parity,
                                                         uint32_t scope, StepEntry* next, uint32_t nTiles)
 {
-    static_assert(PW % G == 0 && kPerfQ % G == 0, "whole groups, whole slots per lane");
-    constexpr int Q = kPerfQ / G;
+    static_assert(PW % G == 0, "whole groups per CTA");
+    constexpr int Q = kPerfQ / G > 0 ? kPerfQ / G : 1;   // list slots per lane and pass
     __shared__ SysDev Sm[kMulti ? PW : 1];
     __shared__ __align__(16) uint32_t dtabs[PW][kDirTab];
     uint32_t const lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
@@ -1026,7 +1026,7 @@ int sm_count()
 }
 
 // the perform's warps per CTA and per tile: BFM_PERFORM_WARPS (1, 2, 4, 8) and BFM_PERFORM_GROUP
-// (1, 2, 4; at most the warps per CTA) override the defaults
+// (1, 2, 4, 8; at most the warps per CTA) override the defaults
 int perform_env(char const* name, int dflt, int maxv)
 {
     char const* e = std::getenv(name);
@@ -1040,7 +1040,7 @@ int perform_warps()
 }
 int perform_group()
 {
-    static int const g = std::min(perform_env("BFM_PERFORM_GROUP", (int)kPerformGroupDefault, 4), perform_warps());
+    static int const g = std::min(perform_env("BFM_PERFORM_GROUP", (int)kPerformGroupDefault, 8), perform_warps());
     return g;
 }
 
@@ -1058,7 +1058,8 @@ void launch_perform_g(SysDev const& hostDesc, SysDev const* dSys, TileRef const*
                       StepEntry const* dSteps, PerformArgs const& pa, cudaStream_t s)
 {
     int const g = perform_group();
-    if (g >= 4 && PW >= 4) launch_perform_k<W, kMulti, PW, (PW >= 4 ? 4 : 1)>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s);
+    if (g >= 8 && PW >= 8) launch_perform_k<W, kMulti, PW, (PW >= 8 ? 8 : 1)>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s);
+    else if (g >= 4 && PW >= 4) launch_perform_k<W, kMulti, PW, (PW >= 4 ? 4 : 1)>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s);
     else if (g >= 2 && PW >= 2) launch_perform_k<W, kMulti, PW, (PW >= 2 ? 2 : 1)>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s);
     else launch_perform_k<W, kMulti, PW, 1>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s);
 }
