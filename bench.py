@@ -144,8 +144,8 @@ def profiled_traffic(kernel_key, tag="dram_bytes_per_launch:"):
 # ------------------------------------------------------------------ clocks
 
 class NvmlClockSampler:
-    """SM clock and throttle reasons read through NVML every 20 ms on a background thread (read
-    only; nothing is set)."""
+    """SM clock and throttle reasons read through NVML every millisecond on a background thread
+    (read only; nothing is set)."""
 
     REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
                "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
@@ -175,7 +175,7 @@ class NvmlClockSampler:
                         self.reasons.add(name)
             except Exception:
                 pass
-            self.stop_flag.wait(0.02)
+            self.stop_flag.wait(0.001)
 
     def stop(self):
         self.stop_flag.set()
@@ -185,7 +185,8 @@ class NvmlClockSampler:
         except Exception:
             pass
         return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.max,
-                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "nvml, 20 ms"}
+                "reasons": sorted(self.reasons), "samples": len(self.samples),
+                "sm_mhz_min": min(self.samples) if self.samples else None, "source": "nvml, every 1 ms"}
 
 
 def clock_sampler(gpu_index):
