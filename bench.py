@@ -612,10 +612,11 @@ def batched_vs_plain(mcs=ENSEMBLE_MCS, sample_mcs=200):
             "ratio_vs_plain_auto": batched_sample / rate["auto"],
             "batched_launches_per_mcs": launches_per_mcs, "parity": parity,
             "autotuned": {"shape": tuned["shape"], "resident": tuned["resident"], "cluster": tuned["cluster"],
-                          "block": tuned["block"],
-                          "trials": [[t["shape"], t["resident"], t["cluster"], t["block"], round(t["ms_per_mcs"], 4)]
-                                     for t in tuned["trials"]],
-                          "trial_fields": ["shape", "resident", "cluster", "block", "ms_per_mcs"]},
+                          "block": tuned["block"], "perform": list(tuned["perform"]),
+                          "trials": [[t["shape"], t["resident"], t["cluster"], t["block"], list(t["perform"]),
+                                      round(t["ms_per_mcs"], 4)] for t in tuned["trials"]],
+                          "trial_fields": ["shape", "resident", "cluster", "block",
+                                           "perform (warps per CTA, per tile; 0 = default 4)", "ms_per_mcs"]},
             "timing": (f"batched: CUDA events over MCS {done}-{done + sample_mcs} (batched_sample, compared with "
                        f"the plain samples) and {done + sample_mcs}-{mcs} (batched); plain: each system alone, "
                        f"CUDA events over its MCS 3-{3 + sample_mcs}"),

@@ -120,6 +120,10 @@ int bfm_set_mode(bfm_handle h, int mode);
  * the reference's runSimulationOnGPU times block sizes itself when built with
  * AUTO_CONFIGURE_BEST_SETTINGS_FOR_PSCBFM_ALGORITHM (CRITICAL.cu:445-487). */
 int bfm_set_grid_block(bfm_handle h, int block);
+/* Warps per CTA and warps per tile of the perform on this handle's grid paths (bond codes): each 1,
+ * 2, 4 or 8, the second at most the first (0, 0: the default, 4 and 4); results do not change. No
+ * reference counterpart (the reference's perform runs one thread per monomer of the colour). */
+int bfm_set_perform(bfm_handle h, int warps, int group);
 /* The path the next run takes (after bfm_initialize): the mode set by bfm_set_mode with
  * BFM_MODE_AUTO resolved, and a mode the system cannot use replaced by BFM_MODE_GRAPH. */
 int bfm_get_path(bfm_handle h, int* mode);
@@ -241,14 +245,19 @@ int bfm_batch_set_shape(bfm_batch_handle b, int shape);
 /* CTA size of the grid groups' check: 128, 256 or 512 threads over the same 512-monomer tile (0:
  * the default, 256); results do not change. */
 int bfm_batch_set_block(bfm_batch_handle b, int block);
-/* Autotuner: runs every configuration (kernel shape x resident path on / off x cluster path on /
- * off) for 1 + mcs_per_trial MCS, keeps the fastest and reports it (shape, paths, ms per MCS;
- * paths: bit 0 the resident path, bit 1 the cluster path). The trials are ordinary MCS of the run
- * (results do not depend on the configuration): every member advances by n_trials x
- * (1 + mcs_per_trial) MCS. Two stages: the paths (resident / cluster kernels on or off) with the
- * grid kernels' defaults, then for the best paths the grid check's register budget (shape) x CTA
- * size (128, 256, 512 threads; the reference sweeps its block size, CRITICAL.cu:445-487). trials
- * (may be NULL) receives up to capacity quadruples (shape, paths, block, ms per MCS). */
+/* Warps per CTA and per tile of the grid groups' perform, as bfm_set_perform (0, 0: the default). */
+int bfm_batch_set_perform(bfm_batch_handle b, int warps, int group);
+int bfm_batch_get_perform(bfm_batch_handle b, int* warps, int* group);
+/* Autotuner: runs configurations for 1 + mcs_per_trial MCS each, keeps the fastest and reports it
+ * (shape, paths, ms per MCS; paths: bit 0 the resident path, bit 1 the cluster path). The trials
+ * are ordinary MCS of the run (results do not depend on the configuration): every member advances
+ * by n_trials x (1 + mcs_per_trial) MCS. Three stages: the paths (resident / cluster kernels on or
+ * off) with the grid kernels' defaults; for the best paths the grid check's register budget
+ * (shape) x CTA size (128, 256, 512 threads; the reference sweeps its block size,
+ * CRITICAL.cu:445-487); for the best of those the perform's warps per CTA x per tile ((8,4),
+ * (4,2), (8,8), (2,2) beside the default (4,4)). The last two stages run only when some member is
+ * on the grid-phase kernels. trials (may be NULL) receives up to capacity sextuples (shape, paths,
+ * block, perform warps, perform warps per tile, ms per MCS; 0 for a default). */
 int bfm_batch_autotune(bfm_batch_handle b, int32_t mcs_per_trial, int* shape, int* paths, float* ms_per_mcs,
                        float* trials, uint32_t capacity, uint32_t* n_trials);
 const char* bfm_batch_last_error(bfm_batch_handle b);

@@ -108,7 +108,10 @@ _SIGS = {
     "bfm_batch_run_each": [H, _i32p],
     "bfm_batch_set_shape": [H, C.c_int],
     "bfm_batch_set_block": [H, C.c_int],
+    "bfm_batch_set_perform": [H, C.c_int, C.c_int],
+    "bfm_batch_get_perform": [H, C.POINTER(C.c_int), C.POINTER(C.c_int)],
     "bfm_set_grid_block": [H, C.c_int],
+    "bfm_set_perform": [H, C.c_int, C.c_int],
     "bfm_batch_autotune": [H, C.c_int32, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float),
                            np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"), C.c_uint32,
                            C.POINTER(C.c_uint32)],

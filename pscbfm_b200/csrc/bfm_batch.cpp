@@ -232,6 +232,9 @@ void Batch::rebuild()
 cudaError_t Batch::launchGrid(StepEntry const* e)
 {
     SysDev const unused{};   // multi-system launches read each CTA's descriptor from dSys_
+    PerformArgs pa;
+    pa.warps = perfWarps_;
+    pa.group = perfGroup_;
     for (auto const& g : grid_) {
         uint32_t const n = (uint32_t)g.tiles.size();
         if (g.members.size() == 1) {
@@ -246,7 +249,7 @@ cudaError_t Batch::launchGrid(StepEntry const* e)
             if (err != cudaSuccess) return err;
             err = g.codeMode == kCodeNone
                       ? launch_perform(u.deviceDesc(), nullptr, n, kGridBlock, e + m, stream_)
-                      : launch_perform_bc(u.desc(), u.deviceDesc(), nullptr, n, e + m, g.codeMode, stream_, shape_);
+                      : launch_perform_bc(u.desc(), u.deviceDesc(), nullptr, n, e + m, g.codeMode, stream_, shape_, pa);
             if (err != cudaSuccess) return err;
             continue;
         }
@@ -256,7 +259,7 @@ cudaError_t Batch::launchGrid(StepEntry const* e)
         if (err != cudaSuccess) return err;
         err = g.codeMode == kCodeNone
                   ? launch_perform(dSys_, g.dTiles, n, kGridBlock, e, stream_)
-                  : launch_perform_bc(unused, dSys_, g.dPTiles, (uint32_t)g.ptiles.size(), e, g.codeMode, stream_, shape_);
+                  : launch_perform_bc(unused, dSys_, g.dPTiles, (uint32_t)g.ptiles.size(), e, g.codeMode, stream_, shape_, pa);
         if (err != cudaSuccess) return err;
     }
     return cudaSuccess;
@@ -421,6 +424,16 @@ void Batch::setBlock(int block)
     block_ = block;
 }
 
+void Batch::setPerformShape(int warps, int group)
+{
+    if (!perform_shape_ok(warps, group))
+        throw std::invalid_argument("[Batch::setPerformShape] warps per CTA and per tile must be 1, 2, 4 or 8, "
+                                    "the second at most the first (0, 0: the default)");
+    if (warps != perfWarps_ || group != perfGroup_) built_ = false;   // the captured graph holds the old kernels
+    perfWarps_ = warps;
+    perfGroup_ = group;
+}
+
 std::vector<Batch::Trial> Batch::autotune(int32_t mcsPerTrial)
 {
     // Every configuration gives the same trajectories, so the trials are ordinary MCS of the run:
@@ -437,20 +450,23 @@ std::vector<Batch::Trial> Batch::autotune(int32_t mcsPerTrial)
         anyCluster[0] = anyCluster[0] || cl;
         anyCluster[1] = anyCluster[1] || (cl && !u->residentEligible());
     }
-    // Two stages, each configuration timed over the same kind of MCS: first the paths (resident
+    // Three stages, each configuration timed over the same kind of MCS: first the paths (resident
     // kernel on / off x cluster kernel on / off, where either can matter) with the grid kernels'
     // defaults; then, for the best paths and if some member runs on the grid-phase kernels, the
     // check's register budget (kGridShapes) x its CTA size (128, 256, 512 threads), as the
-    // reference sweeps its block size (CRITICAL.cu:445-487).
+    // reference sweeps its block size (CRITICAL.cu:445-487); last, for the best of those, the
+    // perform's warps per CTA x warps per tile.
     std::vector<Trial> trials;
-    auto time_it = [&](bool resident, bool cl, int shape, int block) {
+    auto time_it = [&](bool resident, bool cl, int shape, int block, int pw, int pg) {
         setResidentEnabled(resident);
         setClusterEnabled(cl);
         setShape(shape);
         setBlock(block);
+        setPerformShape(pw, pg);
         rebuild();
         runTimed(1);
-        trials.push_back(Trial{shape_, resident, cl, block_, runTimed(mcsPerTrial) / (float)mcsPerTrial});
+        trials.push_back(
+            Trial{shape_, resident, cl, block_, pw, pg, runTimed(mcsPerTrial) / (float)mcsPerTrial});
         return trials.back();
     };
     Trial best{};
@@ -459,7 +475,7 @@ std::vector<Batch::Trial> Batch::autotune(int32_t mcsPerTrial)
         if (!resident && !anyResident) break;   // the same configuration as resident on
         for (int cl = 1; cl >= 0; --cl) {
             if (!cl && !anyCluster[resident]) break;   // the same configuration as cluster on
-            Trial const t = time_it(resident != 0, cl != 0, -1, 0);
+            Trial const t = time_it(resident != 0, cl != 0, -1, 0, 0, 0);
             if (first || t.msPerMcs < best.msPerMcs) best = t;
             first = false;
         }
@@ -470,14 +486,20 @@ std::vector<Batch::Trial> Batch::autotune(int32_t mcsPerTrial)
     if (!grid_.empty()) {
         for (int block : {128, 256, 512})
             for (int sh = 0; sh < kGridShapes; ++sh) {
-                Trial const t = time_it(best.resident, best.cluster, sh, block);
+                Trial const t = time_it(best.resident, best.cluster, sh, block, 0, 0);
                 if (t.msPerMcs < best.msPerMcs) best = t;
             }
+        Trial const base = best;
+        for (auto pw : kPerformShapeTrials) {
+            Trial const t = time_it(base.resident, base.cluster, base.shape, base.block, pw[0], pw[1]);
+            if (t.msPerMcs < best.msPerMcs) best = t;
+        }
     }
     setResidentEnabled(best.resident);
     setClusterEnabled(best.cluster);
     setShape(best.shape);
     setBlock(best.block);
+    setPerformShape(best.perfWarps, best.perfGroup);
     return trials;
 }
 

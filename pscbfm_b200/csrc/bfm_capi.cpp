@@ -169,6 +169,7 @@ int bfm_get_representation(bfm_handle h, int* out)
     });
 }
 int bfm_set_grid_block(bfm_handle h, int block) { BFM_CALL(h, h->u.setGridBlock(block)); }
+int bfm_set_perform(bfm_handle h, int warps, int group) { BFM_CALL(h, h->u.setPerformShape(warps, group)); }
 int bfm_initialize(bfm_handle h) { BFM_CALL(h, h->u.initialize()); }
 int bfm_run(bfm_handle h, int32_t n) { BFM_CALL(h, h->u.runSimulationOnGPU(n)); }
 int bfm_run_async(bfm_handle h, int32_t n) { BFM_CALL(h, h->u.run(n)); }
@@ -432,6 +433,14 @@ int bfm_batch_run(bfm_batch_handle b, int32_t n)
 }
 int bfm_batch_set_shape(bfm_batch_handle b, int shape) { BFM_CALL(b, b->b.setShape(shape)); }
 int bfm_batch_set_block(bfm_batch_handle b, int block) { BFM_CALL(b, b->b.setBlock(block)); }
+int bfm_batch_set_perform(bfm_batch_handle b, int warps, int group) { BFM_CALL(b, b->b.setPerformShape(warps, group)); }
+int bfm_batch_get_perform(bfm_batch_handle b, int* warps, int* group)
+{
+    BFM_CALL(b, {
+        if (warps) *warps = b->b.performWarps();
+        if (group) *group = b->b.performGroup();
+    });
+}
 int bfm_batch_autotune(bfm_batch_handle b, int32_t mcsPerTrial, int* shape, int* paths, float* msPerMcs,
                        float* trials, uint32_t capacity, uint32_t* nTrials)
 {
@@ -447,10 +456,13 @@ int bfm_batch_autotune(bfm_batch_handle b, int32_t mcsPerTrial, int* shape, int*
         }
         if (trials)
             for (uint32_t i = 0; i < (uint32_t)t.size() && i < capacity; ++i) {
-                trials[4 * i] = (float)t[i].shape;
-                trials[4 * i + 1] = (float)((t[i].resident ? 1 : 0) | (t[i].cluster ? 2 : 0));
-                trials[4 * i + 2] = (float)t[i].block;
-                trials[4 * i + 3] = t[i].msPerMcs;
+                float* r = trials + 6 * i;
+                r[0] = (float)t[i].shape;
+                r[1] = (float)((t[i].resident ? 1 : 0) | (t[i].cluster ? 2 : 0));
+                r[2] = (float)t[i].block;
+                r[3] = (float)t[i].perfWarps;
+                r[4] = (float)t[i].perfGroup;
+                r[5] = t[i].msPerMcs;
             }
         if (nTrials) *nTrials = (uint32_t)t.size();
     });

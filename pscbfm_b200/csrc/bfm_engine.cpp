@@ -305,18 +305,34 @@ void Updater::setDrawCallback(DrawFn fn, void* ctx)
     drawCtx_ = ctx;
 }
 
+void Updater::dropGraphs()
+{
+    // the captured graphs hold the launches of the old configuration
+    if (graphs_.empty()) return;
+    if (stream_) cuda_check(cudaStreamSynchronize(stream_), "graph reset");
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
+    graphs_.clear();
+}
+
 void Updater::setGridBlock(int block)
 {
-    // CTA size of the bond-code check (0: the default); the captured graphs hold the old launches
+    // CTA size of the bond-code check (0: the default)
     if (block != 0 && !check_block_ok(block))
         throw std::invalid_argument("[setGridBlock] the check's CTA size must be 128, 256 or 512 threads");
     if (block == gridBlock_) return;
-    if (!graphs_.empty()) {
-        if (stream_) cuda_check(cudaStreamSynchronize(stream_), "setGridBlock");
-        for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
-        graphs_.clear();
-    }
+    dropGraphs();
     gridBlock_ = block;
+}
+
+void Updater::setPerformShape(int warps, int group)
+{
+    if (!perform_shape_ok(warps, group))
+        throw std::invalid_argument("[setPerformShape] warps per CTA and per tile must be 1, 2, 4 or 8, the "
+                                    "second at most the first (0, 0: the default)");
+    if (warps == perfWarps_ && group == perfGroup_) return;
+    dropGraphs();
+    perfWarps_ = warps;
+    perfGroup_ = group;
 }
 
 void Updater::setMode(int mode)
@@ -772,9 +788,11 @@ cudaError_t Updater::launchCheck(StepEntry const* e, cudaStream_t s) const
     return launch_check_bc(dev_.h, dev_.dDesc, nullptr, gridTiles(), e, codeMode_, s, -1, gridBlock_);
 }
 
-cudaError_t Updater::launchPerform(StepEntry const* e, cudaStream_t s, PerformArgs const& pa) const
+cudaError_t Updater::launchPerform(StepEntry const* e, cudaStream_t s, PerformArgs pa) const
 {
     if (codeMode_ == kCodeNone) return launch_perform(dev_.dDesc, nullptr, gridTiles(), kGridBlock, e, s, pa.next);
+    pa.warps = perfWarps_;
+    pa.group = perfGroup_;
     return launch_perform_bc(dev_.h, dev_.dDesc, nullptr, gridTiles(), e, codeMode_, s, -1, pa);
 }
 

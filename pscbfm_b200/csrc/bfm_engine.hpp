@@ -101,6 +101,8 @@ public:
     // CTA size of the bond-code check on the grid paths (128, 256, 512; 0: the default 256)
     void setGridBlock(int block);
     int gridBlock() const { return gridBlock_; }
+    // the bond-code perform's warps per CTA and per tile (perform_shape_ok; 0, 0: the default)
+    void setPerformShape(int warps, int group);
     // a system that only a Batch advances skips the pinned staging of its own run paths
     // (allocated on first use if it runs alone after all)
     void setBatchOnly(bool on) { batchOnly_ = on; }
@@ -269,6 +271,8 @@ private:
     uint64_t launches_ = 0;
     uint64_t h2dBytes_ = 0, d2hBytes_ = 0;
     int gridBlock_ = 0;
+    int perfWarps_ = 0, perfGroup_ = 0;
+    void dropGraphs();
     int repr_ = 0;
     uint32_t codeMode_ = kCodeNone;
     uint32_t nMol_ = 0;
@@ -294,7 +298,7 @@ public:
     uint32_t codeMode() const { return codeMode_; }
     uint32_t gridTiles() const;                               // CTAs of one grid-phase launch
     cudaError_t launchCheck(StepEntry const* e, cudaStream_t s) const;
-    cudaError_t launchPerform(StepEntry const* e, cudaStream_t s, PerformArgs const& pa) const;
+    cudaError_t launchPerform(StepEntry const* e, cudaStream_t s, PerformArgs pa) const;
     static PerformArgs performArgs(StepEntry const& e);   // parity and scope of a host-made entry
     size_t residentSmem() const;
 };
@@ -318,6 +322,10 @@ public:
     // CTA size of the grid groups' check (128, 256, 512; 0: the default)
     void setBlock(int block);
     int block() const { return block_; }
+    // the grid groups' perform: warps per CTA and per tile (perform_shape_ok; 0, 0: the default)
+    void setPerformShape(int warps, int group);
+    int performWarps() const { return perfWarps_; }
+    int performGroup() const { return perfGroup_; }
     bool residentEnabled() const { return residentOn_; }
     bool clusterEnabled() const { return clusterOn_; }
     // Runs the members under each configuration (kernel shape x resident path on / off x cluster
@@ -328,6 +336,7 @@ public:
         bool resident;
         bool cluster;
         int block;
+        int perfWarps, perfGroup;
         float msPerMcs;
     };
     std::vector<Trial> autotune(int32_t mcsPerTrial);
@@ -402,6 +411,7 @@ private:
     bool built_ = false;
     int shape_ = -1;
     int block_ = 0;
+    int perfWarps_ = 0, perfGroup_ = 0;
     cudaStream_t stream_ = nullptr, stream2_ = nullptr;
     cudaEvent_t join_ = nullptr, fork_ = nullptr, ready_ = nullptr;
     void* arena_ = nullptr;                    // descriptors, graph window, tiles, lists

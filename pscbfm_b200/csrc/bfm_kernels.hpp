@@ -65,12 +65,21 @@ cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef 
 constexpr uint32_t kParityFromEntry = 0xFFFFFFFFu;
 constexpr uint32_t kPerformWarpsDefault = 4;   // warps per CTA of the perform
 constexpr uint32_t kPerformGroupDefault = 4;   // warps per tile of the perform
+// the perform shapes (warps per CTA, warps per tile) an autotuner tries beside the default
+constexpr int kPerformShapeTrials[][2] = {{8, 4}, {4, 2}, {8, 8}, {2, 2}};
 constexpr uint32_t kPerfCur = 1u, kPerfPrev = 2u;
 struct PerformArgs {
     uint32_t parity = kParityFromEntry;
     uint32_t scope = kPerfCur | kPerfPrev;
     StepEntry* next = nullptr;
+    int warps = 0;   // warps per CTA (1, 2, 4, 8; 0: the default)
+    int group = 0;   // warps per tile (1, 2, 4, 8, at most `warps`; 0: the default)
 };
+inline bool perform_shape_ok(int warps, int group)
+{
+    auto ok = [](int v) { return v == 1 || v == 2 || v == 4 || v == 8; };
+    return (warps == 0 && group == 0) || (ok(warps) && ok(group) && group <= warps);
+}
 cudaError_t launch_perform_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
                               StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1,
                               PerformArgs const& pa = PerformArgs{});

@@ -1057,7 +1057,7 @@ template <typename W, bool kMulti, int PW>
 void launch_perform_g(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
                       StepEntry const* dSteps, PerformArgs const& pa, cudaStream_t s)
 {
-    int const g = perform_group();
+    int const g = pa.group > 0 ? pa.group : perform_group();
     if (g >= 8 && PW >= 8) launch_perform_k<W, kMulti, PW, (PW >= 8 ? 8 : 1)>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s);
     else if (g >= 4 && PW >= 4) launch_perform_k<W, kMulti, PW, (PW >= 4 ? 4 : 1)>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s);
     else if (g >= 2 && PW >= 2) launch_perform_k<W, kMulti, PW, (PW >= 2 ? 2 : 1)>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s);
@@ -1072,7 +1072,7 @@ void launch_grid_bc_k(bool check, SysDev const& hostDesc, SysDev const* dSys, Ti
         k_check_bc<W, B, kMulti, kMinCheck><<<nTiles, B, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
         return;
     }
-    switch (perform_warps()) {
+    switch (pa.warps > 0 ? pa.warps : perform_warps()) {
     case 1: launch_perform_g<W, kMulti, 1>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
     case 2: launch_perform_g<W, kMulti, 2>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
     case 8: launch_perform_g<W, kMulti, 8>(hostDesc, dSys, dTiles, nTiles, dSteps, pa, s); break;
@@ -1114,7 +1114,8 @@ cudaError_t launch_grid_bc(bool check, SysDev const& hostDesc, SysDev const* dSy
                            uint32_t nTiles, StepEntry const* dSteps, PerformArgs const& pa, int shape, int block,
                            cudaStream_t s)
 {
-    if (shape >= kGridShapes || !check_block_ok(block)) return cudaErrorInvalidValue;
+    if (shape >= kGridShapes || !check_block_ok(block) || !perform_shape_ok(pa.warps, pa.group))
+        return cudaErrorInvalidValue;
     if (dTiles) launch_grid_bc_m<W, true>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, block, s);
     else launch_grid_bc_m<W, false>(check, hostDesc, dSys, dTiles, nTiles, dSteps, pa, shape, block, s);
     return cudaGetLastError();

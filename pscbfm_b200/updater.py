@@ -208,6 +208,11 @@ class UpdaterGPUScBFM_AB_Type:
         """CTA size of the bond-code check on the grid paths (128, 256, 512; 0 = default 256)."""
         self._call("bfm_set_grid_block", block)
 
+    def set_perform(self, warps: int, group: int):
+        """Warps per CTA and per tile of the bond-code perform on the grid paths (1, 2, 4, 8, group <=
+        warps; 0, 0 = default 4, 4); results do not change."""
+        self._call("bfm_set_perform", warps, group)
+
     def set_mode(self, mode: int):
         self._call("bfm_set_mode", mode)
 
@@ -404,23 +409,33 @@ class Batch:
         """CTA size of the grid groups' check (128, 256, 512; 0 = default); results do not change."""
         self._call("bfm_batch_set_block", block)
 
+    def set_perform(self, warps: int, group: int):
+        """Warps per CTA and per tile of the grid groups' perform (1, 2, 4, 8, group <= warps; 0, 0 =
+        default); results do not change."""
+        self._call("bfm_batch_set_perform", warps, group)
+
+    def perform_shape(self) -> tuple:
+        w, g = C.c_int(), C.c_int()
+        self._call("bfm_batch_get_perform", C.byref(w), C.byref(g))
+        return w.value, g.value
+
     def autotune(self, mcs_per_trial: int = 10) -> dict:
-        """Times the configurations in two stages (the resident / cluster paths on or off, then the
-        grid check's register budget x CTA size for the best paths), 1 + mcs_per_trial MCS each,
-        and keeps the fastest. The trials advance every member (the results do not depend on the
-        configuration)."""
+        """Times the configurations in three stages (the resident / cluster paths on or off; the grid
+        check's register budget x CTA size for the best paths; the perform's warps per CTA x per
+        tile for the best of those), 1 + mcs_per_trial MCS each, and keeps the fastest. The trials
+        advance every member (the results do not depend on the configuration)."""
         cap = 64
-        trials = np.zeros(4 * cap, dtype=np.float32)
+        trials = np.zeros(6 * cap, dtype=np.float32)
         shape, paths, best, n = C.c_int(), C.c_int(), C.c_float(), C.c_uint32()
         self._call("bfm_batch_autotune", mcs_per_trial, C.byref(shape), C.byref(paths), C.byref(best), trials,
                    cap, C.byref(n))
-        rows = trials[:4 * min(n.value, cap)].reshape(-1, 4)
+        rows = trials[:6 * min(n.value, cap)].reshape(-1, 6)
         t = [{"shape": int(r[0]), "resident": bool(int(r[1]) & 1), "cluster": bool(int(r[1]) & 2),
-              "block": int(r[2]), "ms_per_mcs": float(r[3])} for r in rows]
+              "block": int(r[2]), "perform": (int(r[3]), int(r[4])), "ms_per_mcs": float(r[5])} for r in rows]
         bt = min(t, key=lambda q: q["ms_per_mcs"])
         return {"shape": shape.value, "resident": bool(paths.value & 1), "cluster": bool(paths.value & 2),
-                "block": bt["block"], "ms_per_mcs": best.value, "mcs_spent": n.value * (1 + mcs_per_trial),
-                "trials": t}
+                "block": bt["block"], "perform": self.perform_shape(), "ms_per_mcs": best.value,
+                "mcs_spent": n.value * (1 + mcs_per_trial), "trials": t}
 
     def set_cluster(self, on: bool):
         """Members too large for one CTA that a cluster of CTAs holds run in the cluster-resident

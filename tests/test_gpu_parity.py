@@ -264,11 +264,17 @@ def test_batch_autotune_keeps_trajectories():
     rep = b.autotune(3)
     # stage 1: the paths (the network runs in a cluster of CTAs alone, so the cluster path is a
     # dimension); stage 2: the grid check's register budget x CTA size for the best paths (the
-    # 128^3 members run on the grid-phase kernels under every path choice)
-    paths, grid = rep["trials"][:4], rep["trials"][4:]
+    # 128^3 members run on the grid-phase kernels under every path choice); stage 3: the perform's
+    # warps per CTA x per tile for the best of those
+    paths, grid, perf = rep["trials"][:4], rep["trials"][4:16], rep["trials"][16:]
     assert {(t["resident"], t["cluster"]) for t in paths} == {(r, c) for r in (True, False) for c in (True, False)}
     assert {(t["shape"], t["block"]) for t in grid} == {(s, bl) for s in range(4) for bl in (128, 256, 512)}
-    assert len(rep["trials"]) == 16 and rep["mcs_spent"] == 16 * 4
+    assert all(t["perform"] == (0, 0) for t in paths + grid)
+    assert [t["perform"] for t in perf] == [(8, 4), (4, 2), (8, 8), (2, 2)]
+    assert len({(t["shape"], t["block"]) for t in perf}) == 1
+    assert len(rep["trials"]) == 20 and rep["mcs_spent"] == 20 * 4
+    best = min(rep["trials"], key=lambda t: t["ms_per_mcs"])
+    assert rep["perform"] == best["perform"] and b.perform_shape() == best["perform"]
     assert rep["ms_per_mcs"] == min(t["ms_per_mcs"] for t in rep["trials"])
     b.run(17)
     for s, m in zip(systems, members):
@@ -409,4 +415,30 @@ def test_check_block_size_rejects_other_sizes():
     u = P.UpdaterGPUScBFM_AB_Type(0)
     with pytest.raises(ValueError, match="128, 256 or 512"):
         u.set_grid_block(64)
+    u.close()
+
+
+@pytest.mark.parametrize("warps,group", [(1, 1), (2, 2), (4, 2), (8, 4), (8, 8), (4, 1)])
+@pytest.mark.parametrize("name", ["melt256_16384x64_20mcs", "chains64_256x32_chunked"])
+def test_perform_shapes_vs_reference(name, warps, group):
+    """The bond-code perform with 1 to 8 warps per CTA and per tile, on the graph path and one
+    launch at a time: identical to the reference."""
+    g = json.load(open(GOLDEN_JSON))["cases"][name]
+    build, chunks = CASES[name]
+    s = build()
+    for mode in (P.MODE_GRAPH, P.MODE_LAUNCH):
+        u = P.UpdaterGPUScBFM_AB_Type(0)
+        u.load_system(s, mode=mode)
+        u.set_perform(warps, group)
+        for c in chunks:
+            u.runSimulationOnGPU(c)
+        assert positions_digest(u.get_coords()) == g["sha256"], (warps, group, mode)
+        u.close()
+
+
+def test_perform_shape_rejects_other_shapes():
+    u = P.UpdaterGPUScBFM_AB_Type(0)
+    for w, g in [(3, 1), (4, 8), (0, 4), (16, 16)]:
+        with pytest.raises(ValueError, match="1, 2, 4 or 8"):
+            u.set_perform(w, g)
     u.close()
