@@ -327,10 +327,13 @@ __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* dt
 // one round trip, so no length scan or barrier precedes the movers' own loads; entries past a
 // list's end lie inside the tile's segment and are ignored. The lengths are exact for every tile of
 // the launch: a check CTA whose tile lies beyond its colour group stores a zero length. Longer lists
-// take further passes. Returns the moves this warp applied.
+// take further passes. The warp's copy of the direction table (dtab) is written from d0, d1 (words
+// lane and lane + 32, loaded by the caller) once those loads are out, so the table's round trip
+// overlaps the lists'. Returns the moves this warp applied.
 template <typename W, bool kNc, int Q>
-__device__ __forceinline__ uint32_t perform_tile(SysDev const& S, uint32_t const* dtab, uint32_t p, uint32_t tile,
-                                                 bool doCur, bool doPrev, uint32_t sub, uint32_t G)
+__device__ __forceinline__ uint32_t perform_tile(SysDev const& S, uint32_t* dtab, uint32_t d0, uint32_t d1,
+                                                 uint32_t p, uint32_t tile, bool doCur, bool doPrev, uint32_t sub,
+                                                 uint32_t G)
 {
     uint32_t const lane = threadIdx.x & 31u;
     size_t const seg = (size_t)tile * kBcTileSpan;
@@ -351,6 +354,9 @@ __device__ __forceinline__ uint32_t perform_tile(SysDev const& S, uint32_t const
         to[q] = doCur ? ldm<kNc>(wc + e) : 0u;
         pw[q] = doPrev ? ldm<kNc>(wp + e) : 0u;
     }
+    dtab[lane] = d0;
+    if (lane + 32u < kDirTab) dtab[lane + 32u] = d1;
+    __syncwarp();
 #pragma unroll
     for (int q = 0; q < Q; ++q) live[q] = first + stride * (uint32_t)q < cnt;
     uint32_t nAcc = perform_movers<W, Q, kNc>(S, dtab, tcur, ent, to, live);
@@ -456,12 +462,11 @@ __global__ void __launch_bounds__(32 * PW) k_perform_bc(const __grid_constant__ 
     bool const writer = !kMulti && next != nullptr && wt == 0 && sub == 0 && lane == 0;
     StepGen gen{};
     if (writer) gen = *S1.gen;
-    uint32_t* const dtab = dtabs[wid];
-    uint32_t p = parity, tile = wt;
+    uint32_t p = parity, tile = wt, d0, d1;
     bool cur = (scope & kPerfCur) != 0u, prev = (scope & kPerfPrev) != 0u;
     if (!kMulti) {
-        uint32_t const d0 = S1.dirTab[lane];
-        uint32_t const d1 = lane + 32u < kDirTab ? S1.dirTab[lane + 32u] : 0u;
+        d0 = S1.dirTab[lane];
+        d1 = lane + 32u < kDirTab ? S1.dirTab[lane + 32u] : 0u;
         if (parity == kParityFromEntry) {
             StepEntry const st = steps[0];
             uint32_t const start = tile * kBcTileSpan;
@@ -469,8 +474,6 @@ __global__ void __launch_bounds__(32 * PW) k_perform_bc(const __grid_constant__ 
             cur = st.color != kNoColor && start < st.cnt;
             prev = st.prevColor != kNoColor && start < st.pcnt;
         }
-        dtab[lane] = d0;
-        if (lane + 32u < kDirTab) dtab[lane + 32u] = d1;
     } else {
         TileRef const tr = tiles[wt];
         SysDev& D = Sm[kMulti ? wid : 0];
@@ -486,14 +489,13 @@ __global__ void __launch_bounds__(32 * PW) k_perform_bc(const __grid_constant__ 
         cur = st.color != kNoColor && tr.start < st.cnt;
         prev = st.prevColor != kNoColor && tr.start < st.pcnt;
         __syncwarp();
-        dtab[lane] = D.dirTab[lane];
-        if (lane + 32u < kDirTab) dtab[lane + 32u] = D.dirTab[lane + 32u];
+        d0 = D.dirTab[lane];
+        d1 = lane + 32u < kDirTab ? D.dirTab[lane + 32u] : 0u;
     }
-    __syncwarp();
     if (cur || prev) {
         SysDev const& S = kMulti ? Sm[kMulti ? wid : 0] : S1;
-        uint32_t const nAcc =
-            __reduce_add_sync(0xffffffffu, perform_tile<W, true, Q>(S, dtab, p, tile, cur, prev, sub, (uint32_t)G));
+        uint32_t const nAcc = __reduce_add_sync(
+            0xffffffffu, perform_tile<W, true, Q>(S, dtabs[wid], d0, d1, p, tile, cur, prev, sub, (uint32_t)G));
         if (lane == 0 && nAcc)
             atomicAdd(S.stats + 2 * kStatSlots + ((blockIdx.x * PW + wid) % kStatSlots), (unsigned long long)nAcc);
     }
