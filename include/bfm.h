@@ -166,10 +166,13 @@ int bfm_n_colors(bfm_handle h, uint32_t* n_colors, uint32_t* sizes, uint32_t cap
  * MCS done. */
 int bfm_get_stats(bfm_handle h, uint64_t out[4]);
 /* The same counters without waiting for later work (no reference counterpart): bfm_stats_enqueue
- * queues their copy after the work queued so far on the handle's stream and returns a ticket;
- * bfm_stats_wait waits for that copy only, while work queued after it keeps running, and writes the
- * counters as they stood then. The last 8 tickets of a handle stay valid; an older or unknown
- * ticket is BFM_ERR_INVALID_ARGUMENT. */
+ * returns a ticket for the counters as the work queued so far on the handle leaves them;
+ * bfm_stats_wait waits for their copy only, while work queued after it keeps running, and writes
+ * the counters as they stood then. After a graph-path run (bond codes) the copy comes from the
+ * snapshot the next run's first kernel takes, so the sweep's stream carries no extra kernel; when
+ * no such run follows, the wait (or any other work on the handle) reads the counters directly.
+ * The last 8 tickets of a handle stay valid; an older or unknown ticket is
+ * BFM_ERR_INVALID_ARGUMENT. */
 int bfm_stats_enqueue(bfm_handle h, uint64_t* ticket);
 int bfm_stats_wait(bfm_handle h, uint64_t ticket, uint64_t out[4]);
 /* checkSystem (UpdaterGPUScBFM_AB_Type.cu:882-986): excluded volume and bond set on the host. */

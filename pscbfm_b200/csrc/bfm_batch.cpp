@@ -333,6 +333,7 @@ void Batch::run(int32_t const* mcs)
     for (uint32_t m = 0; m < M; ++m)
         if (wholeRun_[m]) members_[m]->scrubPending(members_[m]->stream());
     for (Updater* u : members_) {
+        u->flushTickets();   // a member's ticket still waiting for a snapshot reads its counters now
         cuda_check(cudaEventRecord(ready_, u->stream()), "event");
         cuda_check(cudaStreamWaitEvent(stream_, ready_, 0), "wait");
     }

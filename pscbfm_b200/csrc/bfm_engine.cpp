@@ -552,7 +552,9 @@ void Updater::initialize()
     genOn_ = 0;
     snapIssued_ = 0;
     lastRunSnap_ = false;
+    lastRunLead_ = false;
     snapMode_ = false;
+    pendingTickets_.clear();
 }
 
 void Updater::hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, std::vector<uint32_t>& nbrr) const
@@ -782,10 +784,10 @@ uint32_t Updater::gridTiles() const
     return std::max((maxGroup_ + span - 1) / span, 1u);
 }
 
-cudaError_t Updater::launchCheck(StepEntry const* e, cudaStream_t s) const
+cudaError_t Updater::launchCheck(StepEntry const* e, cudaStream_t s, unsigned long long* snap) const
 {
     if (codeMode_ == kCodeNone) return launch_check(dev_.dDesc, nullptr, gridTiles(), kGridBlock, e, s);
-    return launch_check_bc(dev_.h, dev_.dDesc, nullptr, gridTiles(), e, codeMode_, s, -1, gridBlock_);
+    return launch_check_bc(dev_.h, dev_.dDesc, nullptr, gridTiles(), e, codeMode_, s, -1, gridBlock_, snap);
 }
 
 cudaError_t Updater::launchPerform(StepEntry const* e, cudaStream_t s, PerformArgs pa) const
@@ -888,7 +890,9 @@ void Updater::scrubPending(cudaStream_t s)
     h2dBytes_ += sizeof(StepEntry);
     cuda_check(cudaEventRecord(stepsFree_, s), "event");
     chainValid_ = false;
+    flushTickets();
     lastRunSnap_ = false;
+    lastRunLead_ = false;
     // both representations scrub the previous sub-step's marks in the perform
     cuda_check(launchPerform(dev_.dSteps, s, performArgs(hSteps_[0])), "scrub");
     ++launches_;
@@ -899,6 +903,7 @@ void Updater::noteExternalRun(uint64_t subSteps, uint64_t mcs, bool pendingMarks
 {
     (void)subSteps;
     lastRunSnap_ = false;
+    lastRunLead_ = false;   // the batch flushed this system's waiting tickets before it ran
     mcsDone_ += mcs;
     hostStale_ = true;
     lastColor_ = pendingMarks ? lastColor : kNoColor;
@@ -931,19 +936,22 @@ cudaGraphExec_t Updater::graphFor(uint32_t nSteps, uint32_t parity0, bool snap)
     // sub-steps, writes the entry of the next one into slot t + 1 (the last node into slot 0,
     // where the next replay starts) when the device producer is on; the perform's parity is a
     // launch parameter, so a graph is captured per length and parity of its first sub-step
+    // snap: with bond codes the first check takes the counters' snapshot as the work before the
+    // replay left them, on the gather representation a node after the last perform takes it
+    bool const lead = snap && leadSnapshots();
     cudaGraph_t g;
     cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t err = cudaSuccess;
     for (uint32_t t = 0; t < nSteps && err == cudaSuccess; ++t) {
-        err = launchCheck(dev_.dSteps + t, stream_);
+        err = launchCheck(dev_.dSteps + t, stream_, lead && t == 0 ? dev_.snap : nullptr);
         PerformArgs pa;
         pa.parity = (parity0 + t) & 1u;
         pa.scope = kPerfCur | kPerfPrev;   // a scrub with no marks pending only zeroes zero words
         pa.next = nSteps >= 2 ? dev_.dSteps + (t + 1) % nSteps : nullptr;
         if (err == cudaSuccess) err = launchPerform(dev_.dSteps + t, stream_, pa);
     }
-    // once the counters are read by ticket, every replay ends with their snapshot
-    if (snap && err == cudaSuccess) err = launch_snapshot_stats(dev_.h.stats, dev_.snap, dev_.snapSeq, stream_);
+    if (snap && !lead && err == cudaSuccess)
+        err = launch_snapshot_stats(dev_.h.stats, dev_.snap, dev_.snapSeq, stream_);
     cudaError_t const endErr = cudaStreamEndCapture(stream_, &g);
     cuda_check(err, "capture launches");
     cuda_check(endErr, "end capture");
@@ -998,6 +1006,8 @@ void Updater::enqueueGraph(uint32_t nSteps)
     // when the device's chain does not continue from the host's position, otherwise nothing.
     uint32_t const nC = (uint32_t)grpSize_.size();
     uint32_t const G = std::min(kGraphMcs * nC, hStepCap_);
+    bool const lead = snapMode_ && leadSnapshots();
+    if (!lead) flushTickets();
     for (uint32_t done = 0; done < nSteps;) {
         uint32_t const chunk = std::min(G, nSteps - done);
         cudaGraphExec_t const exec = graphFor(chunk, (uint32_t)(subStep_ & 1u), snapMode_);
@@ -1023,11 +1033,13 @@ void Updater::enqueueGraph(uint32_t nSteps)
             cuda_check(cudaEventRecord(stepsFree_, stream_), "event");
         }
         cuda_check(cudaGraphLaunch(exec, stream_), "graph launch");
-        launches_ += 2ull * chunk + (snapMode_ ? 1u : 0u);
+        launches_ += 2ull * chunk + (snapMode_ && !lead ? 1u : 0u);
+        if (lead) publishPending(snapIssued_);   // this replay's first check wrote that snapshot
         if (snapMode_) ++snapIssued_;
         done += chunk;
     }
-    lastRunSnap_ = snapMode_;
+    lastRunSnap_ = snapMode_ && !lead;
+    lastRunLead_ = lead;
 }
 
 float Updater::runTimed(int32_t nMcs)
@@ -1060,7 +1072,9 @@ void Updater::timeKernels(int32_t nMcs, double out[4])
     // it runs on; sums per kernel
     requireInit("timeKernels");
     cuda_check(cudaSetDevice(gpu_), "cudaSetDevice");
+    flushTickets();
     lastRunSnap_ = false;
+    lastRunLead_ = false;
     ensureStaging();
     scrubPending(stream_);
     uint32_t const nSteps = (uint32_t)nMcs * (uint32_t)grpSize_.size();
@@ -1229,8 +1243,10 @@ void Updater::run(int32_t nMcs)
     if (total > 0xFFFFFFFFull) throw std::invalid_argument("[runSimulationOnGPU] too many sub-steps in one call");
     uint32_t const nSteps = (uint32_t)total;
     ensureStaging();
-    lastRunSnap_ = false;   // enqueueGraph sets it again
+    lastRunSnap_ = false;   // enqueueGraph sets both again
+    lastRunLead_ = false;
     int const m = effectiveMode();
+    if (m != kModeGraph) flushTickets();
     if (m == kModeResident) enqueueResident(nSteps);
     else if (m == kModeGraph) enqueueGraph(nSteps);
     else if (m == kModePersistent) enqueuePersistent(nSteps);
@@ -1432,7 +1448,13 @@ uint64_t Updater::statsEnqueue()
     // kernels); a slot's new write waits for its previous one, whichever stream made it
     uint64_t const t = ++statNext_;
     uint32_t const k = (uint32_t)(t % kStatRing);
-    if (lastRunSnap_) {
+    // a waiting ticket of this ring slot is older than the last kStatRing: it is dropped
+    pendingTickets_.erase(std::remove(pendingTickets_.begin(), pendingTickets_.end(), k), pendingTickets_.end());
+    if (lastRunLead_) {
+        // the next replay's first check takes the snapshot of the counters as they are now
+        pendingTickets_.push_back(k);
+        statSeq_[k] = 0;
+    } else if (lastRunSnap_) {
         // the last graph replay left its counters in snapshot slot (snapIssued_ - 1): copy that into
         // host memory on the publishing stream, so the sweep's stream goes on at once
         if (!pubStream_) {
@@ -1460,12 +1482,46 @@ uint64_t Updater::statsEnqueue()
     return t;
 }
 
+void Updater::publishPending(uint64_t snapSeq)
+{
+    // after the replay that writes snapshot snapSeq: the waiting tickets copy it on pubStream_
+    if (pendingTickets_.empty()) return;
+    if (!pubStream_) {
+        cuda_check(cudaStreamCreateWithFlags(&pubStream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaEventCreateWithFlags(&pubEv_, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    cuda_check(cudaEventRecord(pubEv_, stream_), "event");
+    cuda_check(cudaStreamWaitEvent(pubStream_, pubEv_, 0), "wait");
+    uint64_t const slot = snapSeq % kSnapRing;
+    for (uint32_t k : pendingTickets_) {
+        cuda_check(cudaStreamWaitEvent(pubStream_, statEv_[k], 0), "wait");
+        cuda_check(launch_publish_snap(dev_.snap + 4 * slot, dStatRing_ + 4ull * k, pubStream_), "stats");
+        cuda_check(cudaEventRecord(statEv_[k], pubStream_), "event");
+        statSeq_[k] = snapSeq + 1;
+    }
+    pendingTickets_.clear();
+}
+
+void Updater::flushTickets()
+{
+    // nothing has changed the counters since these tickets were taken: read them directly
+    if (pendingTickets_.empty()) return;
+    for (uint32_t k : pendingTickets_) {
+        cuda_check(cudaStreamWaitEvent(stream_, statEv_[k], 0), "wait");
+        cuda_check(launch_publish_stats(dev_.h.stats, dStatRing_ + 4ull * k, stream_), "stats");
+        cuda_check(cudaEventRecord(statEv_[k], stream_), "event");
+        statSeq_[k] = 0;
+    }
+    pendingTickets_.clear();
+}
+
 void Updater::statsWait(uint64_t ticket, uint64_t out[4])
 {
     requireInit("stats");
     uint32_t const k = (uint32_t)(ticket % kStatRing);
     if (ticket == 0 || !hStatRing_ || statTicket_[k] != ticket)
         throw std::invalid_argument("[stats] unknown ticket, or one older than the last 8 of this system");
+    if (std::find(pendingTickets_.begin(), pendingTickets_.end(), k) != pendingTickets_.end()) flushTickets();
     cuda_check(cudaEventSynchronize(statEv_[k]), "stats");
     std::atomic_thread_fence(std::memory_order_acquire);
     unsigned long long const volatile* const slot = hStatRing_ + 4ull * k;
@@ -1612,6 +1668,7 @@ void Updater::freeDevice()
         dStatRing_ = nullptr;
         for (uint32_t k = 0; k < kStatRing; ++k) statTicket_[k] = 0;
     }
+    pendingTickets_.clear();
 
 }
 

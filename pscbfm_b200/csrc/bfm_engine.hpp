@@ -148,6 +148,7 @@ public:
     void noteExternalRun(uint64_t subSteps, uint64_t mcs, bool pendingMarks, uint32_t lastColor);
     uint32_t lastColor() const { return lastColor_; }
     void streamWait(cudaEvent_t e);          // orders this system's later work after e
+    void flushTickets();                     // tickets waiting for a snapshot: from the counters, now
 
     // observables (bfm_observables.cu layout; molecules = connected components of the bonds)
     uint32_t nMolecules() const { return nMol_; }
@@ -244,13 +245,22 @@ private:
     unsigned long long* dStats_ = nullptr;     // hStats_ as the device addresses it
     cudaEvent_t statEv_[kStatRing] = {};
     uint64_t statTicket_[kStatRing] = {}, statMcs_[kStatRing] = {}, statNext_ = 0;
-    // once a ticket has been taken, every graph replay ends with a counter snapshot
-    // (k_snapshot_stats, snapMode_); a ticket taken right after
-    // a graph-path run copies that snapshot into host memory on pubStream_, off the sweep's stream
+    // Once a ticket has been taken (snapMode_), every graph replay takes a snapshot of the counters:
+    // with bond codes its first check does, of the counters as the work before the replay left
+    // them, so a ticket taken right after a replay waits (pendingTickets_) for the next replay and
+    // is then copied from that replay's snapshot into host memory on pubStream_, off the sweep's
+    // stream; any other work that changes the counters first publishes the waiting tickets from the
+    // counters themselves on the sweep's stream (flushTickets), as does a wait for such a ticket.
+    // On the gather representation the replay ends with a snapshot node (k_snapshot_stats) and a
+    // ticket taken right after it copies that snapshot at once.
     uint64_t statSeq_[kStatRing] = {};   // expected snapshot sequence of a ticket (0: direct read)
-    uint64_t snapIssued_ = 0;            // graph replays enqueued (= the device's snapshot count)
-    bool lastRunSnap_ = false;           // the last work changing the counters was a snapshotting replay
-    bool snapMode_ = false;              // the graphs end with a counter snapshot
+    uint64_t snapIssued_ = 0;            // snapshots enqueued (= the device's snapshot count)
+    bool lastRunSnap_ = false;           // the last work changing the counters ended with a snapshot
+    bool lastRunLead_ = false;           // ... was a replay whose successor's check takes the snapshot
+    bool snapMode_ = false;              // the graphs take counter snapshots
+    std::vector<uint32_t> pendingTickets_;   // ticket ring slots waiting for the next snapshot
+    void publishPending(uint64_t snapSeq);   // the waiting tickets from snapshot snapSeq, on pubStream_
+    bool leadSnapshots() const { return codeMode_ != kCodeNone; }
     cudaStream_t pubStream_ = nullptr;
     cudaEvent_t pubEv_ = nullptr;
     bool gsPending_ = false;                   // hGs_ is being refreshed by the stream
@@ -297,7 +307,7 @@ public:
     void setRepresentation(int r);
     uint32_t codeMode() const { return codeMode_; }
     uint32_t gridTiles() const;                               // CTAs of one grid-phase launch
-    cudaError_t launchCheck(StepEntry const* e, cudaStream_t s) const;
+    cudaError_t launchCheck(StepEntry const* e, cudaStream_t s, unsigned long long* snap = nullptr) const;
     cudaError_t launchPerform(StepEntry const* e, cudaStream_t s, PerformArgs pa) const;
     static PerformArgs performArgs(StepEntry const& e);   // parity and scope of a host-made entry
     size_t residentSmem() const;

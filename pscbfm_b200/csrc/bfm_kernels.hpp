@@ -54,9 +54,13 @@ inline bool check_block_ok(int block) { return block == 128 || block == 256 || b
 constexpr int kGridShapes = 4;
 // The perform launch's tile list for a check tile list of bond-code systems: one tile per entry.
 std::vector<TileRef> perform_tile_list(std::vector<TileRef> const& tiles);
+// snap != nullptr (one system): the check first writes the snapshot of the move counters as the
+// work before it left them into that ring (snapshot_stats; the sequence word follows the 4 x
+// kSnapRing slot words). The check counts attempted moves (CTA 0, after the snapshot) and the
+// perform the tentative ones (list lengths) and the accepted ones.
 cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
                             StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape = -1,
-                            int block = 0);
+                            int block = 0, unsigned long long* snap = nullptr);
 // The perform takes one warp per tile. A single-system launch may carry the sub-step's parity and
 // scope (kPerfCur: walk its tentative movers, kPerfPrev: zero the previous sub-step's marks), so
 // it reads no step entry; parity == kParityFromEntry reads both from dSteps[0]. next != nullptr
@@ -72,6 +76,7 @@ struct PerformArgs {
     uint32_t parity = kParityFromEntry;
     uint32_t scope = kPerfCur | kPerfPrev;
     StepEntry* next = nullptr;
+    unsigned long long* snap = nullptr;   // the check's counter snapshot ring (launch_check_bc)
     int warps = 0;   // warps per CTA (1, 2, 4, 8; 0: the default)
     int group = 0;   // warps per tile (1, 2, 4, 8, at most `warps`; 0: the default)
 };

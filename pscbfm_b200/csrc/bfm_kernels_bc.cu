@@ -333,7 +333,7 @@ __device__ __forceinline__ void perform_body(SysDev const& S, uint32_t const* dt
 template <typename W, bool kNc, int Q>
 __device__ __forceinline__ uint32_t perform_tile(SysDev const& S, uint32_t* dtab, uint32_t d0, uint32_t d1,
                                                  uint32_t p, uint32_t tile, bool doCur, bool doPrev, uint32_t sub,
-                                                 uint32_t G)
+                                                 uint32_t G, uint32_t& listLen)
 {
     uint32_t const lane = threadIdx.x & 31u;
     size_t const seg = (size_t)tile * kBcTileSpan;
@@ -344,6 +344,7 @@ __device__ __forceinline__ uint32_t perform_tile(SysDev const& S, uint32_t* dtab
     unsigned long long* const tprev = S.tmp + (size_t)(p ^ 1u) * S.nwords;
     uint32_t const cnt = doCur ? ldm<kNc>(S.mcount + (size_t)p * S.countStride + tile) : 0u;
     uint32_t const pcnt = doPrev ? ldm<kNc>(S.mcount + (size_t)(p ^ 1u) * S.countStride + tile) : 0u;
+    listLen = cnt;
     uint32_t const first = sub * 32u + lane, stride = 32u * G;
     uint32_t ent[Q], to[Q], pw[Q];
     bool live[Q];
@@ -394,12 +395,19 @@ template <typename W, int B, bool kMulti, int kMinBlocks = 1>
 __global__ void __launch_bounds__(B, kMinBlocks) k_check_bc(const __grid_constant__ SysDev S1,
                                                          SysDev const* __restrict__ sysv,
                                                          TileRef const* __restrict__ tiles,
-                                                         StepEntry const* __restrict__ steps)
+                                                         StepEntry const* __restrict__ steps,
+                                                         unsigned long long* snap)
 {
     __shared__ SysDev Sm;
     __shared__ __align__(16) uint32_t dtab[kDirTab];
     constexpr int MPT = (int)kBcTileSpan / B;
     static_assert(B * MPT == (int)kBcTileSpan, "a CTA covers one list segment");
+    // one system, snap != nullptr: the first warp of CTA 0 first takes the snapshot of the move
+    // counters as the work before this launch left them (snapshot_stats). No CTA of the check adds to
+    // the tentative count (the perform does) and CTA 0 adds the attempted count only after this, so
+    // no other update of this launch can reach the counters before it.
+    if (!kMulti && snap != nullptr && blockIdx.x == 0 && threadIdx.x < 32u)
+        snapshot_stats(S1.stats, snap, snap + 4 * kSnapRing);
     uint32_t sys = 0, start = blockIdx.x * kBcTileSpan;
     // one system: the direction table's load goes out with the step entry's
     uint32_t dv = (!kMulti && threadIdx.x < kDirTab) ? S1.dirTab[threadIdx.x] : 0u;
@@ -429,8 +437,8 @@ __global__ void __launch_bounds__(B, kMinBlocks) k_check_bc(const __grid_constan
     check_body<W, MPT>(S, dtab, st, start, &segCount, stage);   // publishes both with its first barrier
     __syncthreads();
     if (threadIdx.x == 0 && st.color != kNoColor) {
+        // the list length; the perform that walks the list counts its entries as tentative moves
         S.mcount[(size_t)st.parity * S.countStride + start / kBcTileSpan] = segCount;
-        tally_flush(segCount, S.stats, 1);
         if (start == 0) tally_flush(st.cnt, S.stats, 0);
     }
 }
@@ -494,10 +502,15 @@ __global__ void __launch_bounds__(32 * PW) k_perform_bc(const __grid_constant__ 
     }
     if (cur || prev) {
         SysDev const& S = kMulti ? Sm[kMulti ? wid : 0] : S1;
+        uint32_t listLen = 0;
         uint32_t const nAcc = __reduce_add_sync(
-            0xffffffffu, perform_tile<W, true, Q>(S, dtabs[wid], d0, d1, p, tile, cur, prev, sub, (uint32_t)G));
-        if (lane == 0 && nAcc)
-            atomicAdd(S.stats + 2 * kStatSlots + ((blockIdx.x * PW + wid) % kStatSlots), (unsigned long long)nAcc);
+            0xffffffffu,
+            perform_tile<W, true, Q>(S, dtabs[wid], d0, d1, p, tile, cur, prev, sub, (uint32_t)G, listLen));
+        uint32_t const stripe = (blockIdx.x * PW + wid) % kStatSlots;
+        // the tile's list length (its tentative moves) is counted once, by the group's first warp
+        if (lane == 0 && sub == 0 && listLen)
+            atomicAdd(S.stats + kStatSlots + stripe, (unsigned long long)listLen);
+        if (lane == 0 && nAcc) atomicAdd(S.stats + 2 * kStatSlots + stripe, (unsigned long long)nAcc);
     }
     if (writer) write_next_step(S1.gen, gen, S1.grp, next);
 }
@@ -1071,7 +1084,7 @@ void launch_grid_bc_k(bool check, SysDev const& hostDesc, SysDev const* dSys, Ti
                       uint32_t nTiles, StepEntry const* dSteps, PerformArgs const& pa, cudaStream_t s)
 {
     if (check) {
-        k_check_bc<W, B, kMulti, kMinCheck><<<nTiles, B, 0, s>>>(hostDesc, dSys, dTiles, dSteps);
+        k_check_bc<W, B, kMulti, kMinCheck><<<nTiles, B, 0, s>>>(hostDesc, dSys, dTiles, dSteps, pa.snap);
         return;
     }
     switch (pa.warps > 0 ? pa.warps : perform_warps()) {
@@ -1134,10 +1147,13 @@ std::vector<TileRef> perform_tile_list(std::vector<TileRef> const& tiles)
 }
 
 cudaError_t launch_check_bc(SysDev const& hostDesc, SysDev const* dSys, TileRef const* dTiles, uint32_t nTiles,
-                            StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape, int block)
+                            StepEntry const* dSteps, uint32_t codeMode, cudaStream_t s, int shape, int block,
+                            unsigned long long* snap)
 {
     if (nTiles == 0) return cudaSuccess;
-    PerformArgs const none{};
+    if (dTiles && snap) return cudaErrorInvalidValue;   // snapshots are taken for one system only
+    PerformArgs none{};
+    none.snap = snap;
     if (block <= 0) block = (int)kCheckBlockDefault;
     if (codeMode == kCode32)
         return launch_grid_bc<uint32_t>(true, hostDesc, dSys, dTiles, nTiles, dSteps, none, shape, block, s);

@@ -201,10 +201,10 @@ def test_reference_adapter_over_engine_vs_oracle(build, steps, calls):
 
 @pytest.mark.parametrize("repr_", [P.REPR_AUTO, P.REPR_GATHER])
 def test_stats_tickets_across_paths(repr_):
-    """Tickets taken after bond-code graph-path runs copy the counter snapshot the graph's last
-    perform took (on a publishing stream of their own); after other paths, and on the gather
-    representation, they read the counters directly. Mixed, back to back and repeated, every ticket
-    equals a synchronous read after the same MCS."""
+    """Tickets taken after graph-path runs copy a counter snapshot on a publishing stream of their
+    own (bond codes: the one the next replay's first check takes; gather representation: the one a
+    node at the end of the replay takes); after other paths they read the counters directly. Mixed,
+    back to back and repeated, every ticket equals a synchronous read after the same MCS."""
     s = S.serpentine_chains(64, 32, 0.3, seed=5)
     a = fresh()
     a.load_system(s, mode=P.MODE_GRAPH, representation=repr_)
@@ -227,6 +227,69 @@ def test_stats_tickets_across_paths(repr_):
         b.runSimulationOnGPU(want_mcs - k)
         k = want_mcs
         assert g == b.stats() and g["mcs"] == want_mcs
+    a.close()
+    b.close()
+
+
+def test_stats_tickets_in_flight_and_around_other_work():
+    """Tickets taken after graph replays of bond-code systems wait for the next replay's snapshot
+    (its first check takes it) or, when other work comes first or the ticket is waited for, read
+    the counters directly. Steps queued two ahead of the wait, as a serving loop does, two tickets
+    with no work between them, a timed kernel pass, a LAUNCH-path run and a Batch run between
+    replays: every ticket equals a synchronous read after the same MCS."""
+    import numpy as np
+    s = S.serpentine_chains(64, 32, 0.3, seed=5)
+    a = fresh()
+    a.load_system(s, mode=P.MODE_GRAPH)
+    b = fresh()
+    b.load_system(s, mode=P.MODE_GRAPH)
+    got, done, total = [], [], 0
+
+    def ticket():
+        done.append(total)
+        return a.stats_async()
+
+    pending = []
+    for k in range(12):                    # one MCS per step, the counters read two steps later
+        a.run_async(1)
+        total += 1
+        pending.append(ticket())
+        if len(pending) > 2:
+            got.append(a.stats_wait(pending.pop(0)))
+    got += [a.stats_wait(t) for t in pending]
+    t1, t2 = ticket(), ticket()            # no work between them
+    a.run_async(3)
+    total += 3
+    t3 = ticket()
+    a.time_kernels(2)                      # kernels timed one at a time change the counters too
+    total += 2
+    t4 = ticket()
+    a.set_mode(P.MODE_LAUNCH)
+    a.run_async(2)
+    total += 2
+    a.set_mode(P.MODE_GRAPH)
+    a.run_async(1)
+    total += 1
+    t5 = ticket()
+    other = fresh()
+    other.load_system(S.small_chains(), mode=P.MODE_GRAPH)
+    batch = P.Batch([a, other])
+    batch.run(2)
+    total += 2
+    t6 = ticket()
+    a.run_async(70)                        # more than one graph chunk
+    total += 70
+    t7 = ticket()
+    got += [a.stats_wait(t) for t in (t1, t2, t3, t4, t5, t6, t7)]
+    batch.close()
+    other.close()
+    k = 0
+    for want_mcs, g in zip(done, got):
+        if want_mcs > k:
+            b.runSimulationOnGPU(want_mcs - k)
+            k = want_mcs
+        assert g == b.stats() and g["mcs"] == want_mcs, (want_mcs, g, b.stats())
+    assert np.array_equal(a.get_coords(), b.get_coords())
     a.close()
     b.close()
 
