@@ -171,11 +171,14 @@ __device__ __forceinline__ uint32_t perform_movers(SysDev const& S, uint32_t con
     W* const CODE = static_cast<W*>(S.code);
     Plane pl[N];
     W code[N];
+    int32_t coord[N];   // the coordinate along the move's axis, loaded with the code word
     uint32_t nbr[N][CodeWord<W>::kSlots];
 #pragma unroll
     for (int q = 0; q < N; ++q) {
         uint32_t const g = live[q] ? ent[q] & kEntSlotMask : 0u;
         code[q] = live[q] ? CODE[g] : W(0);
+        uint32_t const ax = live[q] ? ((ent[q] >> 27) & 7u) >> 1 : 0u;
+        coord[q] = live[q] ? (ax == 0 ? S.x : (ax == 1 ? S.y : S.z))[g] : 0;
 #pragma unroll
         for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k)
             nbr[q][k] = (live[q] && k < S.maxc) ? __ldg(S.nbrr + (size_t)k * S.npad + g) : 0u;
@@ -216,7 +219,10 @@ __device__ __forceinline__ uint32_t perform_movers(SysDev const& S, uint32_t con
             atomicXor(S.lat + w1, 1ull << (pk1 & 63u));
         }
         PK[g] = pk1;
-        atomicAdd((a == 0 ? S.x : (a == 1 ? S.y : S.z)) + g, s);
+        // only the mover writes its own coordinates, so a plain store of the value loaded above
+        // suffices; an atomic add costs an L2 atomic operation per move (and, on a cold line, a DRAM
+        // round trip inside the atomic unit)
+        (a == 0 ? S.x : (a == 1 ? S.y : S.z))[g] = coord[q] + s;
         W const own = code[q];
         CODE[g] = code_shift(own, a, -s);
         uint32_t const n = uint32_t(own >> CodeWord<W>::kCountShift) & 7u;
