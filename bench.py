@@ -107,15 +107,16 @@ def perform_bytes_per_move(kbar, p_chk, p_acc, code_mode):
     the mover lists: per tentative move its list entry 4 B, its target address 4 B, its code word,
     kbar neighbour references (4 B) and 9 temporary-lattice bits; per tentative move of the
     previous sub-step (the scrub, same rate) its target address 4 B and one temporary bit
-    cleared; per accepted move 2 lattice bits read and written, the new lattice address 4 B, one
-    coordinate read+write 8 B, the own code word written and kbar neighbour code words read and
-    written. Gather representation (code_mode 0): flag 1 B, per tentative move xyz 12 B and 9
+    cleared; per accepted move 2 lattice bits read and written, the new lattice address 4 B, the
+    own code word written and kbar neighbour code words read and written (the coordinates are image
+    offsets, written only when a move wraps a periodic axis, about one move in a lattice side
+    along that axis, and not counted). Gather representation (code_mode 0): flag 1 B, per tentative move xyz 12 B and 9
     temporary bits, per accepted move 2 lattice bits read and written, one coordinate 8 B, flag
     1 B."""
     if code_mode == 0:
         return 1 + p_chk * (12 + 9 / 8) + p_acc * (0.5 + 8 + 1)
     w = 4 if code_mode == 1 else 8
-    return p_chk * (8 + w + 4 * kbar + 9 / 8) + p_chk * (4 + 1 / 8) + p_acc * (0.5 + 4 + 8 + w + 2 * w * kbar)
+    return p_chk * (8 + w + 4 * kbar + 9 / 8) + p_chk * (4 + 1 / 8) + p_acc * (0.5 + 4 + w + 2 * w * kbar)
 
 
 def measured_peaks():

@@ -45,6 +45,10 @@ __device__ __forceinline__ void tally_flush(uint32_t count, unsigned long long* 
     if (count) atomicAdd(stats + which * kStatSlots + (blockIdx.x % kStatSlots), (unsigned long long)count);
 }
 
+// x, y, z: the unfolded corner positions (gather representation). With bond codes they hold each
+// slot's image offsets instead: the unfolded coordinate minus the coordinate inside the lattice
+// (a multiple of the lattice side, zero along a walled axis), since the lattice address pk already
+// holds the rest; a move changes them only when it wraps a periodic axis (slot_coord).
 struct SysDev {
     int32_t* x;
     int32_t* y;
@@ -78,6 +82,7 @@ struct SysDev {
     uint32_t lim[3];                 // box side - 1: on a walled axis a moved corner stays below it
     uint32_t nb[3];                  // bricks per axis
     uint32_t mb, hx, hy;             // brick_index parameters
+    uint32_t amask[3];               // bond codes: the lattice-address bits of each axis (axis_address_mask)
     uint32_t forbid[16];             // bit i set <=> bond index i is forbidden
 };
 
@@ -447,6 +452,38 @@ __host__ __device__ __forceinline__ uint32_t addr_add(uint32_t p, uint32_t m, ui
 __host__ __device__ __forceinline__ uint32_t addr_back(uint32_t ma, uint32_t step)
 {
     return step ^ ma ^ (ma & (0u - ma));
+}
+
+// Coordinate along an axis of the lattice address p: the address bits under the axis's mask m,
+// packed in order (an axis's bits keep their significance in the address). A bit-by-bit extract,
+// for read-back and set-up, not for the sweep.
+__host__ __device__ __forceinline__ uint32_t axis_coord(uint32_t p, uint32_t m)
+{
+    uint32_t r = 0u, bit = 1u;
+    while (m) {
+        uint32_t const low = m & (0u - m);
+        if (p & low) r |= bit;
+        bit <<= 1;
+        m ^= low;
+    }
+    return r;
+}
+
+// Image offset of an unfolded coordinate c on an axis of lattice side P (a power of two): c minus
+// its coordinate inside the lattice, i.e. c with its low log2(P) bits cleared.
+__host__ __device__ __forceinline__ int32_t image_offset(int32_t c, uint32_t P)
+{
+    return int32_t(uint32_t(c) & ~(P - 1u));
+}
+
+// Unfolded coordinate along axis a of slot g (padding slots keep kPadCoord in x): with bond codes
+// the image offset in x/y/z plus the coordinate read from the lattice address.
+__device__ __forceinline__ int32_t slot_coord(SysDev const& S, uint32_t g, uint32_t a)
+{
+    int32_t const* const X = a == 0 ? S.x : (a == 1 ? S.y : S.z);
+    int32_t const off = X[g];
+    if (S.codeMode == kCodeNone) return off;
+    return off + int32_t(axis_coord(S.pk[g], S.amask[a]));
 }
 
 // The <= 2x2 brick words of the front plane of a move along dir and their masks. The plane's

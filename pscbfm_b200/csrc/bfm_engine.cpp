@@ -459,6 +459,7 @@ void Updater::initialize()
         h.nb[a] = nb[a];
     }
     brick_params(nb, h.mb, h.hx, h.hy);
+    for (uint32_t a = 0; a < 3; ++a) h.amask[a] = axis_address_mask(a, nb, tab.data());
     std::memset(h.forbid, 0, sizeof(h.forbid));
     for (uint32_t i = 0; i < 512; ++i)
         if (forbidden_[i]) h.forbid[i >> 5] |= 1u << (i & 31);
@@ -510,6 +511,7 @@ void Updater::initialize()
         cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(h.nbrr), hnbrr.data(), 4ull * hnbrr.size(),
                                    cudaMemcpyHostToDevice, s), "upload nbrr");
     }
+    if (codeMode_ != kCodeNone) toImageOffsets(hx, hy, hz);
     cuda_check(cudaMemcpyAsync(h.x, hx.data(), 4ull * npad_, cudaMemcpyHostToDevice, s), "upload x");
     cuda_check(cudaMemcpyAsync(h.y, hy.data(), 4ull * npad_, cudaMemcpyHostToDevice, s), "upload y");
     cuda_check(cudaMemcpyAsync(h.z, hz.data(), 4ull * npad_, cudaMemcpyHostToDevice, s), "upload z");
@@ -683,9 +685,26 @@ std::vector<uint32_t> Updater::moleculeSizes() const
     return molSize_;
 }
 
+void Updater::toImageOffsets(std::vector<int32_t>& hx, std::vector<int32_t>& hy, std::vector<int32_t>& hz) const
+{
+    // padding slots keep kPadCoord, whose low bits are zero
+    uint32_t const P[3] = {latticeSide(0), latticeSide(1), latticeSide(2)};
+    for (uint32_t g = 0; g < npad_; ++g) {
+        hx[g] = image_offset(hx[g], P[0]);
+        hy[g] = image_offset(hy[g], P[1]);
+        hz[g] = image_offset(hz[g], P[2]);
+    }
+}
+
 void Updater::resetReference()
 {
     requireInit("resetReference");
+    if (codeMode_ != kCodeNone) {
+        cuda_check(launch_unfold_positions(dev_.dDesc, npad_, const_cast<int32_t*>(obs_.rx), const_cast<int32_t*>(obs_.ry),
+                                           const_cast<int32_t*>(obs_.rz), stream_),
+                   "reference positions");
+        return;
+    }
     cuda_check(cudaMemcpyAsync(const_cast<int32_t*>(obs_.rx), dev_.h.x, 4ull * npad_, cudaMemcpyDeviceToDevice, stream_),
                "reference x");
     cuda_check(cudaMemcpyAsync(const_cast<int32_t*>(obs_.ry), dev_.h.y, 4ull * npad_, cudaMemcpyDeviceToDevice, stream_),
@@ -1401,6 +1420,11 @@ void Updater::setCoordinates(int32_t const* xyz, uint32_t n)
         cuda_check(cudaMemcpyAsync(dev_.h.pk, hpk.data(), 4ull * npad_, cudaMemcpyHostToDevice, stream_), "upload pk");
         cuda_check(cudaMemcpyAsync(dev_.h.code, hcode.data(), hcode.size(), cudaMemcpyHostToDevice, stream_),
                    "upload codes");
+        // the lattice above was built from the unfolded positions; bond codes keep image offsets
+        toImageOffsets(hx, hy, hz);
+        cuda_check(cudaMemcpyAsync(dev_.h.x, hx.data(), 4ull * npad_, cudaMemcpyHostToDevice, stream_), "upload x");
+        cuda_check(cudaMemcpyAsync(dev_.h.y, hy.data(), 4ull * npad_, cudaMemcpyHostToDevice, stream_), "upload y");
+        cuda_check(cudaMemcpyAsync(dev_.h.z, hz.data(), 4ull * npad_, cudaMemcpyHostToDevice, stream_), "upload z");
     }
     cuda_check(cudaStreamSynchronize(stream_), "setCoordinates");
 }

@@ -298,6 +298,8 @@ private:
     int effectiveMode() const;                // the path run() takes (mode_ with AUTO resolved)
     int autoMode() const;                     // the path BFM_MODE_AUTO takes for this system
     void prepareGraphs(uint32_t nSteps);      // capture the graphs a graph-path run of nSteps replays
+    // bond codes: unfolded positions (slot order) to image offsets in place (SysDev x, y, z)
+    void toImageOffsets(std::vector<int32_t>& hx, std::vector<int32_t>& hy, std::vector<int32_t>& hz) const;
     void hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, std::vector<uint32_t>& nbrr) const;
 
 public:

@@ -319,16 +319,38 @@ __global__ void k_build_lattice(SysDev const* __restrict__ sysv, uint32_t n)
 // ------------------------------------------------------------------------ position read-back
 
 // Positions in the caller's monomer order, x y z interleaved: out[3 i + a] is coordinate a of the
-// monomer in sorted slot slotOf[i]. One copy of out then gives the caller's array.
+// monomer in sorted slot slotOf[i]. One copy of out then gives the caller's array. With bond codes
+// (pk != nullptr) x, y, z hold image offsets and the lattice address the rest (slot_coord).
 __global__ void k_gather_positions(int32_t const* __restrict__ x, int32_t const* __restrict__ y,
-                                   int32_t const* __restrict__ z, uint32_t const* __restrict__ slotOf, uint32_t n,
+                                   int32_t const* __restrict__ z, uint32_t const* __restrict__ pk, uint32_t m0,
+                                   uint32_t m1, uint32_t m2, uint32_t const* __restrict__ slotOf, uint32_t n,
                                    int32_t* __restrict__ out)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t const g = slotOf[i];
-        out[3ull * i] = x[g];
-        out[3ull * i + 1] = y[g];
-        out[3ull * i + 2] = z[g];
+        int32_t cx = x[g], cy = y[g], cz = z[g];
+        if (pk != nullptr) {
+            uint32_t const p = pk[g];
+            cx += int32_t(axis_coord(p, m0));
+            cy += int32_t(axis_coord(p, m1));
+            cz += int32_t(axis_coord(p, m2));
+        }
+        out[3ull * i] = cx;
+        out[3ull * i + 1] = cy;
+        out[3ull * i + 2] = cz;
+    }
+}
+
+// Unfolded positions of every slot of a bond-code system in slot order (the MSD reference of the
+// observables); padding slots keep kPadCoord.
+__global__ void k_unfold_positions(SysDev const* __restrict__ sysv, int32_t* __restrict__ ox,
+                                   int32_t* __restrict__ oy, int32_t* __restrict__ oz)
+{
+    SysDev const& S = sysv[0];
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < S.npad; g += gridDim.x * blockDim.x) {
+        ox[g] = slot_coord(S, g, 0);
+        oy[g] = slot_coord(S, g, 1);
+        oz[g] = slot_coord(S, g, 2);
     }
 }
 
@@ -420,7 +442,19 @@ cudaError_t launch_gather_positions(SysDev const& h, uint32_t const* slotOf, uin
     uint32_t const block = 256;
     uint32_t const grid = std::min((n + block - 1) / block, 148u * 8u);
     if (grid == 0) return cudaSuccess;
-    k_gather_positions<<<grid, block, 0, s>>>(h.x, h.y, h.z, slotOf, n, out);
+    bool const codes = h.codeMode != kCodeNone;
+    k_gather_positions<<<grid, block, 0, s>>>(h.x, h.y, h.z, codes ? h.pk : nullptr, h.amask[0], h.amask[1],
+                                              h.amask[2], slotOf, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unfold_positions(SysDev const* dSys, uint32_t npad, int32_t* ox, int32_t* oy, int32_t* oz,
+                                    cudaStream_t s)
+{
+    uint32_t const block = 256;
+    uint32_t const grid = std::min((npad + block - 1) / block, 148u * 8u);
+    if (grid == 0) return cudaSuccess;
+    k_unfold_positions<<<grid, block, 0, s>>>(dSys, ox, oy, oz);
     return cudaGetLastError();
 }
 

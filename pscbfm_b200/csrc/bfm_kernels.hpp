@@ -132,6 +132,10 @@ cudaError_t launch_build_lattice(SysDev const* dSys, uint32_t npad, cudaStream_t
 // Positions in the caller's order, x y z interleaved (out[3 i + a] from sorted slot slotOf[i]).
 cudaError_t launch_gather_positions(SysDev const& h, uint32_t const* slotOf, uint32_t n, int32_t* out,
                                     cudaStream_t s);
+// Unfolded positions of every slot of bond-code system dSys[0] (image offsets plus the coordinates
+// of the lattice addresses) into ox, oy, oz, in slot order.
+cudaError_t launch_unfold_positions(SysDev const* dSys, uint32_t npad, int32_t* ox, int32_t* oy, int32_t* oz,
+                                    cudaStream_t s);
 // Writes the sums over the kStatSlots slots of the three move counters (attempted, tentative,
 // accepted) into out[0..3), mapped pinned host memory.
 cudaError_t launch_publish_stats(unsigned long long const* stats, unsigned long long* out, cudaStream_t s);

@@ -158,6 +158,17 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
 
 // ---------------------------------------------------------------------------------- perform
 
+// Image offsets (x, y, z with bond codes, see SysDev) of slot g after a move along axis a by s from
+// lattice address p0 to p1 (ma: the axis's address bits): they change only when the move wraps the
+// periodic axis, i.e. reaches coordinate 0 going up or leaves it going down; a walled axis never
+// wraps. About one move in a lattice side along that axis writes here.
+__device__ __forceinline__ void image_step(SysDev const& S, uint32_t g, uint32_t a, int32_t s, uint32_t p0,
+                                           uint32_t p1, uint32_t ma)
+{
+    if (((s > 0 ? p1 : p0) & ma) == 0u)
+        atomicAdd((a == 0 ? S.x : (a == 1 ? S.y : S.z)) + g, s * int32_t(S.mask[a] + 1u));
+}
+
 // Movers ent[q] (list entries: slot | direction << 27) with targets to[q], for the q with
 // live[q]: re-test the front plane on the temporary lattice and apply the free moves. The plane
 // and the old position follow from the target's address, so the monomer's own address is not
@@ -171,14 +182,11 @@ __device__ __forceinline__ uint32_t perform_movers(SysDev const& S, uint32_t con
     W* const CODE = static_cast<W*>(S.code);
     Plane pl[N];
     W code[N];
-    int32_t coord[N];   // the coordinate along the move's axis, loaded with the code word
     uint32_t nbr[N][CodeWord<W>::kSlots];
 #pragma unroll
     for (int q = 0; q < N; ++q) {
         uint32_t const g = live[q] ? ent[q] & kEntSlotMask : 0u;
         code[q] = live[q] ? CODE[g] : W(0);
-        uint32_t const ax = live[q] ? ((ent[q] >> 27) & 7u) >> 1 : 0u;
-        coord[q] = live[q] ? (ax == 0 ? S.x : (ax == 1 ? S.y : S.z))[g] : 0;
 #pragma unroll
         for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k)
             nbr[q][k] = (live[q] && k < S.maxc) ? __ldg(S.nbrr + (size_t)k * S.npad + g) : 0u;
@@ -219,10 +227,7 @@ __device__ __forceinline__ uint32_t perform_movers(SysDev const& S, uint32_t con
             atomicXor(S.lat + w1, 1ull << (pk1 & 63u));
         }
         PK[g] = pk1;
-        // only the mover writes its own coordinates, so a plain store of the value loaded above
-        // suffices; an atomic add costs an L2 atomic operation per move (and, on a cold line, a DRAM
-        // round trip inside the atomic unit)
-        (a == 0 ? S.x : (a == 1 ? S.y : S.z))[g] = coord[q] + s;
+        image_step(S, g, a, s, pk0, pk1, ms.x);
         W const own = code[q];
         CODE[g] = code_shift(own, a, -s);
         uint32_t const n = uint32_t(own >> CodeWord<W>::kCountShift) & 7u;
@@ -777,7 +782,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
                 atomicXor(lat + w1, 1ull << (p1 & 63u));
             }
             pk[g] = p1;
-            atomicAdd((a == 0 ? S.x : (a == 1 ? S.y : S.z)) + g, s);
+            image_step(S, g, a, s, p, p1, D.ma);
             W const own = code[g];
             code[g] = code_shift(own, a, -s);
             uint32_t const n = uint32_t(own >> CodeWord<W>::kCountShift) & 7u;
@@ -979,7 +984,7 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
                 dsmem_xor64(latAt(w1), 1ull << (p1 & 63u));
             }
             pk[l] = p1;
-            atomicAdd((a == 0 ? S.x : (a == 1 ? S.y : S.z)) + g, s);
+            image_step(S, g, a, s, p, p1, D.ma);
             W const own = code[l];
             code[l] = code_shift(own, a, -s);
             uint32_t const n = uint32_t(own >> CodeWord<W>::kCountShift) & 7u;

@@ -36,7 +36,8 @@ __global__ void __launch_bounds__(256) k_observables(SysDev const* __restrict__ 
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < S.npad; g += gridDim.x * blockDim.x) {
         uint32_t const m = o.molOfSlot[g];
         if (m == kNoColor) continue;   // padding slot
-        long long const x = S.x[g], y = S.y[g], z = S.z[g];
+        int32_t const ix = slot_coord(S, g, 0), iy = slot_coord(S, g, 1), iz = slot_coord(S, g, 2);
+        long long const x = ix, y = iy, z = iz;
         atomicAdd(reinterpret_cast<unsigned long long*>(mom + 4ull * m + 0), (unsigned long long)x);
         atomicAdd(reinterpret_cast<unsigned long long*>(mom + 4ull * m + 1), (unsigned long long)y);
         atomicAdd(reinterpret_cast<unsigned long long*>(mom + 4ull * m + 2), (unsigned long long)z);
@@ -46,7 +47,8 @@ __global__ void __launch_bounds__(256) k_observables(SysDev const* __restrict__ 
         uint32_t const nn = S.nnb[g];
         for (uint32_t k = 0; k < nn; ++k) {
             uint32_t const j = S.nbr[(size_t)k * S.npad + g];
-            atomicAdd(&hist[bond_index(S.x[j] - (int32_t)x, S.y[j] - (int32_t)y, S.z[j] - (int32_t)z)], 1u);
+            atomicAdd(&hist[bond_index(slot_coord(S, j, 0) - ix, slot_coord(S, j, 1) - iy, slot_coord(S, j, 2) - iz)],
+                      1u);
         }
     }
     for (int sh = 16; sh > 0; sh >>= 1) myMsd += __shfl_down_sync(0xffffffffu, myMsd, sh);
@@ -54,7 +56,9 @@ __global__ void __launch_bounds__(256) k_observables(SysDev const* __restrict__ 
     // end-to-end vectors, one thread per molecule
     for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < o.nMol; m += gridDim.x * blockDim.x) {
         uint32_t const a = o.ends[2 * m], b = o.ends[2 * m + 1];
-        long long const dx = (long long)S.x[b] - S.x[a], dy = (long long)S.y[b] - S.y[a], dz = (long long)S.z[b] - S.z[a];
+        long long const dx = (long long)slot_coord(S, b, 0) - slot_coord(S, a, 0);
+        long long const dy = (long long)slot_coord(S, b, 1) - slot_coord(S, a, 1);
+        long long const dz = (long long)slot_coord(S, b, 2) - slot_coord(S, a, 2);
         ree[m] = dx * dx + dy * dy + dz * dz;
     }
     __syncthreads();
