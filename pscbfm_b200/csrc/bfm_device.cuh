@@ -45,6 +45,25 @@ __device__ __forceinline__ void tally_flush(uint32_t count, unsigned long long* 
     if (count) atomicAdd(stats + which * kStatSlots + (blockIdx.x % kStatSlots), (unsigned long long)count);
 }
 
+// Per-slot state of the bond-code representation, one record per slot so that the check reads
+// it with one load and the perform writes it with one store: the lattice address of the corner
+// (pk: brick word << 6 | bit, lattice_address) and the bond-code word (CodeWord). 3 fields
+// (uint32 code): {pk, code} in 8 bytes; 6 fields (uint64 code): {pk, 0, code} in 16 bytes.
+template <typename W>
+struct SlotRec;
+template <>
+struct SlotRec<uint32_t> {
+    using V = uint2;
+    static constexpr uint32_t kWords = 2;
+};
+template <>
+struct SlotRec<unsigned long long> {
+    using V = uint4;
+    static constexpr uint32_t kWords = 4;
+};
+// 32-bit words per record of a code mode
+__host__ __device__ __forceinline__ uint32_t rec_words(uint32_t codeMode) { return codeMode == 2u ? 4u : 2u; }
+
 // x, y, z: the unfolded corner positions (gather representation). With bond codes they hold each
 // slot's image offsets instead: the unfolded coordinate minus the coordinate inside the lattice
 // (a multiple of the lattice side, zero along a walled axis), since the lattice address pk already
@@ -63,8 +82,7 @@ struct SysDev {
     uint32_t const* grp;             // [2 * nColors]: offset, size
     unsigned long long* stats;       // [3][kStatSlots]: attempted, tentative, accepted (striped)
     // bond-code representation (codeMode != kCodeNone)
-    uint32_t* pk;                    // [npad] lattice address of the corner: brick word << 6 | bit (lattice_address)
-    void* code;                      // [npad] uint32 (3 slots) or uint64 (6 slots) bond codes
+    uint32_t* rec;                   // [npad] records {lattice address, bond code} (SlotRec, rec_words each)
     uint32_t const* nbrr;            // [maxc][npad] neighbour slot | reverse slot << 28
     unsigned long long const* planeTab;   // [3][64][4] front-plane masks (see plane_table_fill)
     uint8_t const* moveOk;           // [512] bit d: a bond with this index stays allowed after move d
@@ -100,6 +118,7 @@ struct GridSync {
 // the count of fields sits above them. Valid only with symmetric neighbour lists, where the
 // reverse slot of every bond exists and bonded monomers never share a colour.
 constexpr uint32_t kCodeNone = 0, kCode32 = 1, kCode64 = 2;
+static_assert(kCode64 == 2u, "rec_words names the 64-bit code mode by its value");
 template <typename W>
 struct CodeWord;
 template <>
@@ -221,6 +240,7 @@ __device__ __forceinline__ uint32_t move_dir(uint32_t iLocal, uint32_t seed)
 {
     return move_hash(move_hash(iLocal) ^ seed) % 6u;
 }
+
 
 // Position of value v (0..3) of axis a inside a brick word: bit = x + 4 y + 16 z.
 // CRITICAL.cu:334-341 (the reference's NONPERIODICITY build): along an axis with walls the moved
@@ -483,7 +503,31 @@ __device__ __forceinline__ int32_t slot_coord(SysDev const& S, uint32_t g, uint3
     int32_t const* const X = a == 0 ? S.x : (a == 1 ? S.y : S.z);
     int32_t const off = X[g];
     if (S.codeMode == kCodeNone) return off;
-    return off + int32_t(axis_coord(S.pk[g], S.amask[a]));
+    return off + int32_t(axis_coord(S.rec[(size_t)g * rec_words(S.codeMode)], S.amask[a]));
+}
+
+// The lattice address and the bond-code word of slot g inside its record.
+template <typename W>
+__host__ __device__ __forceinline__ uint32_t* rec_pk(uint32_t* r, uint32_t g)
+{
+    return r + (size_t)g * SlotRec<W>::kWords;
+}
+template <typename W>
+__host__ __device__ __forceinline__ W* rec_code(uint32_t* r, uint32_t g)
+{
+    return reinterpret_cast<W*>(r + (size_t)g * SlotRec<W>::kWords + SlotRec<W>::kWords / 2);
+}
+// The code word of a record as loaded (V: uint2 or uint4).
+__host__ __device__ __forceinline__ uint32_t rec_code_of(uint2 v) { return v.y; }
+__host__ __device__ __forceinline__ unsigned long long rec_code_of(uint4 v)
+{
+    return v.z | ((unsigned long long)v.w << 32);
+}
+// A record with address p and code word c.
+__host__ __device__ __forceinline__ uint2 make_rec(uint32_t p, uint32_t c) { return make_uint2(p, c); }
+__host__ __device__ __forceinline__ uint4 make_rec(uint32_t p, unsigned long long c)
+{
+    return make_uint4(p, 0u, uint32_t(c), uint32_t(c >> 32));
 }
 
 // The <= 2x2 brick words of the front plane of a move along dir and their masks. The plane's

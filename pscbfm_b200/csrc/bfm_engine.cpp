@@ -75,7 +75,6 @@ ArenaLayout arena_layout(uint32_t n, uint32_t npad, uint32_t maxc, uint32_t nwor
         off = align256(off + bytes);
         return o;
     };
-    size_t const codeBytes = codeMode == kCode64 ? 8 : 4;
     L.x = take(4ull * npad);
     L.y = take(4ull * npad);
     L.z = take(4ull * npad);
@@ -92,8 +91,7 @@ ArenaLayout arena_layout(uint32_t n, uint32_t npad, uint32_t maxc, uint32_t nwor
     L.steps = take(sizeof(StepEntry) * (kStepCap + 1));   // the StepGen, then the entries
     L.list = take(4);
     L.gs = take(sizeof(GridSync));
-    L.pk = take(4ull * npad);
-    L.code = take(codeBytes * npad);
+    L.rec = take(codeMode == kCodeNone ? 0 : 4ull * rec_words(codeMode) * npad);
     L.nbrr = take(4ull * maxc * npad);
     L.plane = take(8ull * 768);
     L.moveOk = take(512);
@@ -426,6 +424,7 @@ void Updater::initialize()
     std::vector<uint32_t> hpk;
     std::vector<uint8_t> hcode;
     std::vector<uint32_t> hnbrr;
+    std::vector<uint32_t> hrec;
 
     // one arena for every device array of this system
     ArenaLayout const L = arena_layout(n_, npad_, maxc_, nwords, (uint32_t)tab.size(), nC, maxGroup_, codeMode_);
@@ -473,8 +472,7 @@ void Updater::initialize()
     dev_.xyzOut = reinterpret_cast<int32_t*>(base + L.xyzOut);
     dev_.snap = reinterpret_cast<unsigned long long*>(base + L.snap);
     dev_.snapSeq = dev_.snap + 4 * kSnapRing;
-    h.pk = reinterpret_cast<uint32_t*>(base + L.pk);
-    h.code = base + L.code;
+    h.rec = codeMode_ == kCodeNone ? nullptr : reinterpret_cast<uint32_t*>(base + L.rec);
     h.nbrr = reinterpret_cast<uint32_t*>(base + L.nbrr);
     h.planeTab = reinterpret_cast<unsigned long long*>(base + L.plane);
     h.moveOk = reinterpret_cast<uint8_t*>(base + L.moveOk);
@@ -506,8 +504,9 @@ void Updater::initialize()
                                cudaMemcpyHostToDevice, s), "upload direction table");
     if (codeMode_ != kCodeNone) {
         hostCodes(hpk, hcode, hnbrr);
-        cuda_check(cudaMemcpyAsync(h.pk, hpk.data(), 4ull * npad_, cudaMemcpyHostToDevice, s), "upload pk");
-        cuda_check(cudaMemcpyAsync(h.code, hcode.data(), hcode.size(), cudaMemcpyHostToDevice, s), "upload codes");
+        hrec = slotRecords(hpk, hcode);
+        cuda_check(cudaMemcpyAsync(h.rec, hrec.data(), 4ull * hrec.size(), cudaMemcpyHostToDevice, s),
+                   "upload slot records");
         cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(h.nbrr), hnbrr.data(), 4ull * hnbrr.size(),
                                    cudaMemcpyHostToDevice, s), "upload nbrr");
     }
@@ -599,6 +598,20 @@ void Updater::hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, s
         }
         std::memcpy(&code[w * s], &c, w);
     }
+}
+
+std::vector<uint32_t> Updater::slotRecords(std::vector<uint32_t> const& pk, std::vector<uint8_t> const& code) const
+{
+    // the records of every slot (SlotRec; padding: zeros): the lattice address in the first word,
+    // the code word in the second half
+    uint32_t const rw = rec_words(codeMode_);
+    size_t const w = codeMode_ == kCode64 ? 8 : 4;
+    std::vector<uint32_t> r((size_t)rw * npad_, 0u);
+    for (uint32_t g = 0; g < npad_; ++g) {
+        r[(size_t)g * rw] = pk[g];
+        std::memcpy(&r[(size_t)g * rw + rw / 2], &code[w * g], w);
+    }
+    return r;
 }
 
 std::vector<uint32_t> Updater::moleculeRoots() const
@@ -1415,11 +1428,12 @@ void Updater::setCoordinates(int32_t const* xyz, uint32_t n)
     cuda_check(launch_build_lattice(dev_.dDesc, npad_, stream_), "build lattice");
     std::vector<uint32_t> hpk, hnbrr;
     std::vector<uint8_t> hcode;
+    std::vector<uint32_t> hrec;
     if (codeMode_ != kCodeNone) {
         hostCodes(hpk, hcode, hnbrr);
-        cuda_check(cudaMemcpyAsync(dev_.h.pk, hpk.data(), 4ull * npad_, cudaMemcpyHostToDevice, stream_), "upload pk");
-        cuda_check(cudaMemcpyAsync(dev_.h.code, hcode.data(), hcode.size(), cudaMemcpyHostToDevice, stream_),
-                   "upload codes");
+        hrec = slotRecords(hpk, hcode);
+        cuda_check(cudaMemcpyAsync(dev_.h.rec, hrec.data(), 4ull * hrec.size(), cudaMemcpyHostToDevice, stream_),
+                   "upload slot records");
         // the lattice above was built from the unfolded positions; bond codes keep image offsets
         toImageOffsets(hx, hy, hz);
         cuda_check(cudaMemcpyAsync(dev_.h.x, hx.data(), 4ull * npad_, cudaMemcpyHostToDevice, stream_), "upload x");
@@ -1618,14 +1632,21 @@ void Updater::validate()
         }
         if (lat != want) throw std::runtime_error("[checkSystem] device occupancy lattice disagrees with the positions");
         if (codeMode_ != kCodeNone) {
-            std::vector<uint32_t> hpk, hnbrr, dpk(npad_);
-            std::vector<uint8_t> hcode, dcode;
+            std::vector<uint32_t> hpk, hnbrr;
+            std::vector<uint8_t> hcode;
             hostCodes(hpk, hcode, hnbrr);
-            dcode.resize(hcode.size());
-            cuda_check(cudaMemcpy(dpk.data(), dev_.h.pk, 4ull * npad_, cudaMemcpyDeviceToHost), "download pk");
-            cuda_check(cudaMemcpy(dcode.data(), dev_.h.code, dcode.size(), cudaMemcpyDeviceToHost), "download codes");
-            if (dpk != hpk) throw std::runtime_error("[checkSystem] packed coordinates disagree with the positions");
-            if (dcode != hcode) throw std::runtime_error("[checkSystem] bond codes disagree with the positions");
+            std::vector<uint32_t> const want = slotRecords(hpk, hcode);
+            std::vector<uint32_t> drec(want.size());
+            cuda_check(cudaMemcpy(drec.data(), dev_.h.rec, 4ull * drec.size(), cudaMemcpyDeviceToHost),
+                       "download slot records");
+            uint32_t const rw = rec_words(codeMode_);
+            for (uint32_t g = 0; g < npad_; ++g) {
+                if (drec[(size_t)g * rw] != want[(size_t)g * rw])
+                    throw std::runtime_error("[checkSystem] packed coordinates disagree with the positions");
+                uint32_t const* const dc = drec.data() + (size_t)g * rw + rw / 2;
+                if (!std::equal(dc, dc + rw / 2, want.data() + (size_t)g * rw + rw / 2))
+                    throw std::runtime_error("[checkSystem] bond codes disagree with the positions");
+            }
         }
     }
 }

@@ -33,7 +33,7 @@ std::vector<uint8_t> colour_bond_graph(uint32_t n, uint32_t const* cnt, uint32_t
 // job's device bytes with it before the job is coloured.
 struct ArenaLayout {
     size_t x, y, z, nbr, nnb, flags, mark, lat, tmp, tab, grp, stats, desc, steps, list, gs;
-    size_t pk, code, nbrr, plane, moveOk, dir, mlist, mword, mcount, slotOf, xyzOut, snap;
+    size_t rec, nbrr, plane, moveOk, dir, mlist, mword, mcount, slotOf, xyzOut, snap;
     uint32_t segs;   // mover-list segments (tiles) per parity
     size_t bytes;
 };
@@ -301,6 +301,9 @@ private:
     // bond codes: unfolded positions (slot order) to image offsets in place (SysDev x, y, z)
     void toImageOffsets(std::vector<int32_t>& hx, std::vector<int32_t>& hy, std::vector<int32_t>& hz) const;
     void hostCodes(std::vector<uint32_t>& pk, std::vector<uint8_t>& code, std::vector<uint32_t>& nbrr) const;
+    // bond codes: the device records (SlotRec, rec_words 32-bit words each) of host lattice
+    // addresses and code words
+    std::vector<uint32_t> slotRecords(std::vector<uint32_t> const& pk, std::vector<uint8_t> const& code) const;
 
 public:
     // representation of the bonds on the device: auto (bond codes when the neighbour lists are

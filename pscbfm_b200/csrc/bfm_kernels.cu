@@ -320,17 +320,17 @@ __global__ void k_build_lattice(SysDev const* __restrict__ sysv, uint32_t n)
 
 // Positions in the caller's monomer order, x y z interleaved: out[3 i + a] is coordinate a of the
 // monomer in sorted slot slotOf[i]. One copy of out then gives the caller's array. With bond codes
-// (pk != nullptr) x, y, z hold image offsets and the lattice address the rest (slot_coord).
+// (rec != nullptr) x, y, z hold image offsets and the lattice address the rest (slot_coord).
 __global__ void k_gather_positions(int32_t const* __restrict__ x, int32_t const* __restrict__ y,
-                                   int32_t const* __restrict__ z, uint32_t const* __restrict__ pk, uint32_t m0,
-                                   uint32_t m1, uint32_t m2, uint32_t const* __restrict__ slotOf, uint32_t n,
-                                   int32_t* __restrict__ out)
+                                   int32_t const* __restrict__ z, uint32_t const* __restrict__ rec, uint32_t recWords,
+                                   uint32_t m0, uint32_t m1, uint32_t m2, uint32_t const* __restrict__ slotOf,
+                                   uint32_t n, int32_t* __restrict__ out)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t const g = slotOf[i];
         int32_t cx = x[g], cy = y[g], cz = z[g];
-        if (pk != nullptr) {
-            uint32_t const p = pk[g];
+        if (rec != nullptr) {
+            uint32_t const p = rec[(size_t)g * recWords];
             cx += int32_t(axis_coord(p, m0));
             cy += int32_t(axis_coord(p, m1));
             cz += int32_t(axis_coord(p, m2));
@@ -443,8 +443,8 @@ cudaError_t launch_gather_positions(SysDev const& h, uint32_t const* slotOf, uin
     uint32_t const grid = std::min((n + block - 1) / block, 148u * 8u);
     if (grid == 0) return cudaSuccess;
     bool const codes = h.codeMode != kCodeNone;
-    k_gather_positions<<<grid, block, 0, s>>>(h.x, h.y, h.z, codes ? h.pk : nullptr, h.amask[0], h.amask[1],
-                                              h.amask[2], slotOf, n, out);
+    k_gather_positions<<<grid, block, 0, s>>>(h.x, h.y, h.z, codes ? h.rec : nullptr, rec_words(h.codeMode),
+                                              h.amask[0], h.amask[1], h.amask[2], slotOf, n, out);
     return cudaGetLastError();
 }
 

@@ -90,8 +90,8 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
                                            uint32_t* segCount, uint2* stage)
 {
     uint32_t const B = blockDim.x, tid = threadIdx.x;
-    uint32_t const* const PK = S.pk;
-    W const* const CODE = static_cast<W const*>(S.code);
+    using RV = typename SlotRec<W>::V;
+    RV const* const REC = reinterpret_cast<RV const*>(S.rec);
     uint32_t const tile = start / kBcTileSpan;
     unsigned long long* const tcur = S.tmp + (size_t)st.parity * S.nwords;
     size_t const seg = (size_t)st.parity * S.listStride + (size_t)tile * kBcTileSpan;
@@ -105,9 +105,9 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
         uint32_t const i = start + tid + (uint32_t)q * B;
-        bool const a = i < st.cnt;
-        pk[q] = a ? ldm<kNc>(PK + st.off + i) : 0u;
-        code[q] = a ? ldm<kNc>(CODE + st.off + i) : W(0);
+        RV const r = i < st.cnt ? ldm<kNc>(REC + st.off + i) : RV{};
+        pk[q] = r.x;
+        code[q] = rec_code_of(r);
     }
     __syncthreads();
     // stage 2: direction, walls, bonds; the monomers that pass go to this warp's part of the
@@ -178,15 +178,15 @@ __device__ __forceinline__ uint32_t perform_movers(SysDev const& S, uint32_t con
                                                    unsigned long long const* tcur, uint32_t const (&ent)[N],
                                                    uint32_t const (&to)[N], bool const (&live)[N])
 {
-    uint32_t* const PK = S.pk;
-    W* const CODE = static_cast<W*>(S.code);
+    using RV = typename SlotRec<W>::V;
+    RV* const REC = reinterpret_cast<RV*>(S.rec);
     Plane pl[N];
     W code[N];
     uint32_t nbr[N][CodeWord<W>::kSlots];
 #pragma unroll
     for (int q = 0; q < N; ++q) {
         uint32_t const g = live[q] ? ent[q] & kEntSlotMask : 0u;
-        code[q] = live[q] ? CODE[g] : W(0);
+        code[q] = live[q] ? *rec_code<W>(S.rec, g) : W(0);
 #pragma unroll
         for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k)
             nbr[q][k] = (live[q] && k < S.maxc) ? __ldg(S.nbrr + (size_t)k * S.npad + g) : 0u;
@@ -226,10 +226,9 @@ __device__ __forceinline__ uint32_t perform_movers(SysDev const& S, uint32_t con
             atomicXor(S.lat + w0, 1ull << (pk0 & 63u));
             atomicXor(S.lat + w1, 1ull << (pk1 & 63u));
         }
-        PK[g] = pk1;
         image_step(S, g, a, s, pk0, pk1, ms.x);
         W const own = code[q];
-        CODE[g] = code_shift(own, a, -s);
+        REC[g] = make_rec(pk1, code_shift(own, a, -s));   // new address and code word in one store
         uint32_t const n = uint32_t(own >> CodeWord<W>::kCountShift) & 7u;
 #pragma unroll
         for (uint32_t k = 0; k < CodeWord<W>::kSlots; ++k) {
@@ -237,7 +236,7 @@ __device__ __forceinline__ uint32_t perform_movers(SysDev const& S, uint32_t con
                 uint32_t const nb = nbr[q][k];
                 uint32_t const c = (0u - (uint32_t(own >> (9u * k + 3u * a)) & 7u)) & 7u;   // reverse field
                 uint32_t const nc = uint32_t(int32_t(c) + s) & 7u;
-                atomicXor(CODE + (nb & kSlotMask), W(c ^ nc) << (9u * (nb >> kSlotShift) + 3u * a));
+                atomicXor(rec_code<W>(S.rec, nb & kSlotMask), W(c ^ nc) << (9u * (nb >> kSlotShift) + 3u * a));
             }
         }
     }
@@ -686,7 +685,6 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
     uint32_t* const pk = reinterpret_cast<uint32_t*>(code + np);
     uint8_t* const mok = reinterpret_cast<uint8_t*>(pk + np);   // 512 move-table bytes
     uint32_t* const list = reinterpret_cast<uint32_t*>(mok + 512);
-    W const* const gcode = static_cast<W const*>(S.code);
     for (uint32_t w = tid; w < 768; w += B) ptab[w] = S.planeTab[w];
     if (tid < kDirTab) dtab[tid] = S.dirTab[tid];
     for (uint32_t w = tid; w < 512; w += B) mok[w] = S.moveOk[w];
@@ -696,8 +694,8 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
         tmp[nw + w] = 0ull;
     }
     for (uint32_t g = tid; g < np; g += B) {
-        code[g] = gcode[g];
-        pk[g] = S.pk[g];
+        code[g] = *rec_code<W>(S.rec, g);
+        pk[g] = *rec_pk<W>(S.rec, g);
     }
     if (tid < 2) listCount[tid] = 0;
     uint32_t nTent = 0, nAcc = 0;
@@ -800,11 +798,10 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_resident_bc(SysDev const*
         __syncthreads();   // every perform is done: the lattice is settled for the next check
         par ^= 1u;
     }
-    W* const gcodeOut = static_cast<W*>(S.code);
     for (uint32_t w = tid; w < nw; w += B) S.lat[w] = lat[w];
     for (uint32_t g = tid; g < np; g += B) {
-        gcodeOut[g] = code[g];
-        S.pk[g] = pk[g];
+        *rec_code<W>(S.rec, g) = code[g];
+        *rec_pk<W>(S.rec, g) = pk[g];
     }
     uint32_t const tsum = __reduce_add_sync(0xffffffffu, nTent);
     uint32_t const asum = __reduce_add_sync(0xffffffffu, nAcc);
@@ -874,7 +871,6 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
     uint32_t* const pk = reinterpret_cast<uint32_t*>(code + cap);            // cap slots
     uint8_t* const mok = reinterpret_cast<uint8_t*>(pk + cap);               // 512 move-table bytes
     uint32_t* const list = reinterpret_cast<uint32_t*>(mok + 512);           // K x 1024 entries
-    W const* const gcode = static_cast<W const*>(S.code);
     for (uint32_t w = tid; w < 768; w += B) ptab[w] = S.planeTab[w];
     if (tid < kDirTab) dtab[tid] = S.dirTab[tid];
     for (uint32_t w = tid; w < 512; w += B) mok[w] = S.moveOk[w];
@@ -886,8 +882,8 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
     for (uint32_t l = tid; l < cap; l += B) {
         uint32_t const g = cluster_slot_of(l, rank, logC);
         bool const in = g < np;
-        code[l] = in ? gcode[g] : W(0);
-        pk[l] = in ? S.pk[g] : 0u;
+        code[l] = in ? *rec_code<W>(S.rec, g) : W(0);
+        pk[l] = in ? *rec_pk<W>(S.rec, g) : 0u;
     }
     if (tid < 2) listCount[tid] = 0;
     cluster.sync();   // every CTA's part of the state is in place before any remote access
@@ -1003,13 +999,12 @@ __global__ void __launch_bounds__(kResidentBlock, 1) k_cluster_bc(SysDev const* 
         par ^= 1u;
     }
     // after the last cluster barrier no CTA reaches into another's shared memory
-    W* const gcodeOut = static_cast<W*>(S.code);
     for (uint32_t l = tid; l < nwC; l += B) S.lat[(l << logC) | rank] = lat[l];
     for (uint32_t l = tid; l < cap; l += B) {
         uint32_t const g = cluster_slot_of(l, rank, logC);
         if (g < np) {
-            gcodeOut[g] = code[l];
-            S.pk[g] = pk[l];
+            *rec_code<W>(S.rec, g) = code[l];
+            *rec_pk<W>(S.rec, g) = pk[l];
         }
     }
     uint32_t const tsum = __reduce_add_sync(0xffffffffu, nTent);
