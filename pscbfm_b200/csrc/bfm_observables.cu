@@ -45,10 +45,17 @@ __global__ void __launch_bounds__(256) k_observables(SysDev const* __restrict__ 
         long long const dx = x - o.rx[g], dy = y - o.ry[g], dz = z - o.rz[g];
         myMsd += dx * dx + dy * dy + dz * dz;
         uint32_t const nn = S.nnb[g];
-        for (uint32_t k = 0; k < nn; ++k) {
-            uint32_t const j = S.nbr[(size_t)k * S.npad + g];
-            atomicAdd(&hist[bond_index(slot_coord(S, j, 0) - ix, slot_coord(S, j, 1) - iy, slot_coord(S, j, 2) - iz)],
-                      1u);
+        if (S.codeMode == kCodeNone) {
+            for (uint32_t k = 0; k < nn; ++k) {
+                uint32_t const j = S.nbr[(size_t)k * S.npad + g];
+                atomicAdd(&hist[bond_index(S.x[j] - ix, S.y[j] - iy, S.z[j] - iz)], 1u);
+            }
+        } else {
+            // field k of the slot's bond-code word is the bond index of (neighbour k - monomer), in
+            // the order of the neighbour list
+            unsigned long long const code = S.codeMode == kCode32 ? (unsigned long long)*rec_code<uint32_t>(S.rec, g)
+                                                                  : *rec_code<unsigned long long>(S.rec, g);
+            for (uint32_t k = 0; k < nn; ++k) atomicAdd(&hist[uint32_t(code >> (9u * k)) & 511u], 1u);
         }
     }
     for (int sh = 16; sh > 0; sh >>= 1) myMsd += __shfl_down_sync(0xffffffffu, myMsd, sh);
