@@ -117,12 +117,17 @@ __device__ __forceinline__ void check_body(SysDev const& S, uint32_t const* dtab
     uint32_t const lanesBelow = (1u << lane) - 1u;
     uint2* const ws = stage + (tid >> 5) * (32u * MPT);
     uint32_t n = 0;
+    bool const walled = S.walls != 0u;   // uniform: a periodic box skips the wall test's table reads
 #pragma unroll
     for (int q = 0; q < MPT; ++q) {
         uint32_t const i = start + tid + (uint32_t)q * B;
         uint32_t const dir = move_dir(i, st.seed);
-        DirParams const D = dir_params(dtab, dir);
-        bool const ok = i < st.cnt && (pk[q] & D.ma) != D.wall && bonds_ok<W, false>(code[q], dir, S.moveOk);
+        bool free = true;
+        if (walled) {
+            uint2 const mw = make_uint2(dtab[dir * 4u], dtab[kDirHalf + dir * 4u + 3u]);   // Ma, wall
+            free = (pk[q] & mw.x) != mw.y;
+        }
+        bool const ok = i < st.cnt && free && bonds_ok<W, false>(code[q], dir, S.moveOk);
         uint32_t const bal = __ballot_sync(0xffffffffu, ok);
         if (ok) ws[n + __popc(bal & lanesBelow)] = make_uint2(pk[q], (st.off + i) | (dir << 27));
         n += (uint32_t)__popc(bal);
