@@ -5,7 +5,11 @@
 //   2. the front plane's words and masks name exactly the nine cells p + 2 s e_a + i e_u + j e_v,
 //      i, j in {-1, 0, 1}: the cells whose corners the moved cube would newly overlap;
 //   3. on a walled axis the wall entry blocks exactly the moves that leave [0, L-2], and on a
-//      periodic axis it blocks none.
+//      periodic axis it blocks none;
+//   4. read-back: the coordinate extracted from the address (axis_coord under the axis's address
+//      mask) is the coordinate, the image offset of an unfolded coordinate plus it gives the
+//      unfolded coordinate back, and a move wraps the periodic axis (the image-offset update)
+//      exactly when the address bits of the axis are zero after a + move or before a - move.
 // Prints "ok" and exits 0, or prints the first disagreement and exits 1.
 #include <cstdio>
 #include <set>
@@ -35,11 +39,33 @@ int check_box(uint32_t const box[3])
     alignas(16) uint32_t dirP[kDirTab], dirW[kDirTab];
     dir_table_fill(nb, tab.data(), hi, 0u, dirP);
     dir_table_fill(nb, tab.data(), hi, 7u, dirW);
+    uint32_t amask[3];
+    for (uint32_t a = 0; a < 3; ++a) amask[a] = axis_address_mask(a, nb, tab.data());
     for (uint32_t z = 0; z < box[2]; ++z)
         for (uint32_t y = 0; y < box[1]; ++y)
             for (uint32_t x = 0; x < box[0]; ++x) {
                 uint32_t const c0[3] = {x, y, z};
                 uint32_t const p = address(c0, nb, tab);
+                for (uint32_t a = 0; a < 3; ++a) {
+                    if (axis_coord(p, amask[a]) != c0[a]) {
+                        std::printf("axis_coord: box %u %u %u at %u %u %u axis %u\n", box[0], box[1], box[2], x, y, z, a);
+                        return 1;
+                    }
+                    for (int32_t k = -3; k <= 3; ++k) {
+                        int32_t const unfolded = int32_t(c0[a]) + k * int32_t(box[a]);
+                        if (image_offset(unfolded, box[a]) + int32_t(axis_coord(p, amask[a])) != unfolded) {
+                            std::printf("image offset: box %u %u %u coordinate %d axis %u\n", box[0], box[1], box[2],
+                                        unfolded, a);
+                            return 1;
+                        }
+                    }
+                    DirParams const U = dir_params(dirP, 2 * a + 1);
+                    bool const upWraps = (addr_add(p, U.ma, U.step) & U.ma) == 0u, downWraps = (p & U.ma) == 0u;
+                    if (upWraps != (c0[a] == box[a] - 1) || downWraps != (c0[a] == 0)) {
+                        std::printf("wrap test: box %u %u %u at %u %u %u axis %u\n", box[0], box[1], box[2], x, y, z, a);
+                        return 1;
+                    }
+                }
                 for (uint32_t d = 0; d < 6; ++d) {
                     uint32_t const a = d >> 1, u = a == 0 ? 1u : 0u, v = a == 2 ? 1u : 2u;
                     int32_t const s = (d & 1u) ? 1 : -1;
@@ -136,6 +162,8 @@ int main()
     uint32_t const top[3] = {1023, 1023, 1023}, zero[3] = {0, 0, 0};
     uint32_t const pt = address(top, nb, tab);
     if (pt >= (1u << 30)) return std::printf("address of the top corner exceeds 30 bits\n"), 1;
+    for (uint32_t a = 0; a < 3; ++a)
+        if (axis_coord(pt, axis_address_mask(a, nb, tab.data())) != 1023u) return std::printf("axis_coord at 1023\n"), 1;
     for (uint32_t d = 1; d < 6; d += 2) {
         DirParams const D = dir_params(dir, d);
         uint32_t c[3] = {1023, 1023, 1023};

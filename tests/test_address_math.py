@@ -1,7 +1,10 @@
 """The lattice-address arithmetic of the bond-code kernels (a monomer's corner stored as its
 occupancy-lattice address; moves and the front plane as adds confined to one axis's address bits),
 checked on the host against plain coordinates for several box shapes: every position, every
-direction, the step, the nine front-plane cells and the walls (tests/address_check.cu)."""
+direction, the step, the nine front-plane cells and the walls; and the read-back of bond-code
+systems, whose x/y/z hold image offsets: the coordinate extracted from an address, the offset plus
+it giving the unfolded coordinate back, and the wrap test behind the offset update
+(tests/address_check.cu)."""
 import os
 import shutil
 import subprocess
