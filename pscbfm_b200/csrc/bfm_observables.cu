@@ -33,15 +33,37 @@ __global__ void __launch_bounds__(256) k_observables(SysDev const* __restrict__ 
     long long* const gh = out + 5ull * o.nMol;
     long long* const gmsd = gh + 512;
     long long myMsd = 0;
+    uint32_t const lane = threadIdx.x & 31u;
+    // npad is a multiple of 32 and so is the grid's stride: every lane of a warp runs the same
+    // iterations, so the warp-wide reduction below sees all 32 lanes
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < S.npad; g += gridDim.x * blockDim.x) {
         uint32_t const m = o.molOfSlot[g];
-        if (m == kNoColor) continue;   // padding slot
-        int32_t const ix = slot_coord(S, g, 0), iy = slot_coord(S, g, 1), iz = slot_coord(S, g, 2);
+        bool const real = m != kNoColor;   // padding slots add nothing
+        int32_t const ix = real ? slot_coord(S, g, 0) : 0, iy = real ? slot_coord(S, g, 1) : 0,
+                      iz = real ? slot_coord(S, g, 2) : 0;
         long long const x = ix, y = iy, z = iz;
-        atomicAdd(reinterpret_cast<unsigned long long*>(mom + 4ull * m + 0), (unsigned long long)x);
-        atomicAdd(reinterpret_cast<unsigned long long*>(mom + 4ull * m + 1), (unsigned long long)y);
-        atomicAdd(reinterpret_cast<unsigned long long*>(mom + 4ull * m + 2), (unsigned long long)z);
-        atomicAdd(reinterpret_cast<unsigned long long*>(mom + 4ull * m + 3), (unsigned long long)(x * x + y * y + z * z));
+        // per-molecule sums: the lanes of a warp mostly hold monomers of one or two chains, so they
+        // are summed over each run of equal molecule ids first (a segmented scan; run r starts at
+        // the highest run head at or below the lane) and the run's last lane adds them, one atomic
+        // per run and sum instead of one per monomer; integer sums are exact in any order
+        uint32_t const mPrev = __shfl_up_sync(0xffffffffu, m, 1);
+        unsigned const heads = __ballot_sync(0xffffffffu, lane == 0 || mPrev != m);
+        uint32_t const runStart = 31u - __clz(heads & (0xffffffffu >> (31u - lane)));
+        bool const runEnd = lane == 31u || ((heads >> (lane + 1u)) & 1u);
+        long long sum[4] = {x, y, z, x * x + y * y + z * z};
+#pragma unroll
+        for (uint32_t off = 1; off < 32u; off <<= 1) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                long long const v = __shfl_up_sync(0xffffffffu, sum[c], off);
+                if (lane >= runStart + off) sum[c] += v;
+            }
+        }
+        if (real && runEnd)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                atomicAdd(reinterpret_cast<unsigned long long*>(mom + 4ull * m + c), (unsigned long long)sum[c]);
+        if (!real) continue;
         long long const dx = x - o.rx[g], dy = y - o.ry[g], dz = z - o.rz[g];
         myMsd += dx * dx + dy * dy + dz * dz;
         uint32_t const nn = S.nnb[g];
